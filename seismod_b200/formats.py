@@ -1,0 +1,128 @@
+"""Writers and readers for the reference's input and output file formats.
+
+The formats are the ones the reference programs read and write:
+
+* parameter file   ``value  # keyword, comment`` lines (io_utils.c:214-292);
+                   the comma is required by the reference parser.
+* e_iso model      ``nx nz / dx dz / x0 z0 / isotropic_elastic`` then one
+                   ``vp vs rho`` line per node, x slow, z fast; a single
+                   column (nz lines) is a 1-D profile (io_utils.c:892-947).
+* a_iso_3d model   ``nx ny nz / dx dy dz / x0 y0 z0 / isotropic_acoustic_3d``
+                   then ``vp rho`` per node, x slowest, z fastest; a single
+                   column is a 1-D profile (io_utils.c:1029-1153).
+* source file      ``nsrc / ntemplate`` then per source ``type / A / f /
+                   coordinates`` (io_utils.c:1432-1589).
+* output file      ``nrec`` then per record ``comp / Trace / coordinates /
+                   t0 (s) / dt (ms)`` (io_utils.c:1592-1741).
+* trace file       ``trc/<base>/<base>_<n>.trc``: ``"%le    %le"`` of time
+                   and 1e3 * velocity (io_utils.c:1744-1768).
+"""
+from __future__ import annotations
+
+import os
+
+import numpy as np
+
+
+def _num(x):
+    """Shortest text that parses back to the same double."""
+    return repr(float(x))
+
+
+def write_par(path, model, source, output, basename, duration, dt_ms, abs_=1, nl=20,
+              **extra):
+    lines = [
+        f"{model}    # model, model file",
+        f"{source}    # source, source file",
+        f"{output}    # output, description of output records",
+        f"{basename}    # basename, common for all output files",
+        f"{_num(duration)}    # time, length of time window in s",
+        f"{_num(dt_ms)}    # dt, time step in ms",
+        f"{int(abs_)}    # abs, apply absorbing boundary",
+        f"{int(nl)}    # nl, number of absorbing layers",
+    ]
+    for k, v in extra.items():
+        lines.append(f"{v}    # {k}, extra")
+    with open(path, "w") as f:
+        f.write("\n".join(lines) + "\n")
+
+
+def _write_rows(f, cols):
+    data = np.column_stack([np.asarray(c, dtype=np.float64).reshape(-1) for c in cols])
+    np.savetxt(f, data, fmt="%.17g")
+
+
+def write_model_e(path, vp, vs, rho, dx, x0=0.0, z0=0.0):
+    """vp, vs, rho: (nx, nz) arrays, or (nz,) 1-D profiles with nx given by
+    passing a tuple (nx, profile) is not supported: use write_model_e_1d."""
+    nx, nz = vp.shape
+    with open(path, "w") as f:
+        f.write(f"{nx} {nz}\n{_num(dx)} {_num(dx)}\n{_num(x0)} {_num(z0)}\nisotropic_elastic\n")
+        _write_rows(f, (vp, vs, rho))
+
+
+def write_model_e_1d(path, nx, vp, vs, rho, dx, x0=0.0, z0=0.0):
+    nz = len(vp)
+    with open(path, "w") as f:
+        f.write(f"{nx} {nz}\n{_num(dx)} {_num(dx)}\n{_num(x0)} {_num(z0)}\nisotropic_elastic\n")
+        _write_rows(f, (vp, vs, rho))
+
+
+def write_model_a(path, vp, rho, d, origin=(0.0, 0.0, 0.0)):
+    """vp, rho: (nx, ny, nz); d = (dx, dy, dz)."""
+    nx, ny, nz = vp.shape
+    with open(path, "w") as f:
+        f.write(f"{nx} {ny} {nz}\n{_num(d[0])} {_num(d[1])} {_num(d[2])}\n"
+                f"{_num(origin[0])} {_num(origin[1])} {_num(origin[2])}\nisotropic_acoustic_3d\n")
+        # chunked so very large models do not need one giant text buffer
+        v = vp.reshape(nx, -1)
+        r = rho.reshape(nx, -1)
+        for i in range(nx):
+            _write_rows(f, (v[i], r[i]))
+
+
+def write_model_a_1d(path, shape, vp, rho, d, origin=(0.0, 0.0, 0.0)):
+    nx, ny, nz = shape
+    assert len(vp) == nz
+    with open(path, "w") as f:
+        f.write(f"{nx} {ny} {nz}\n{_num(d[0])} {_num(d[1])} {_num(d[2])}\n"
+                f"{_num(origin[0])} {_num(origin[1])} {_num(origin[2])}\nisotropic_acoustic_3d\n")
+        _write_rows(f, (vp, rho))
+
+
+def write_src(path, sources, ntemplate=1):
+    """sources: list of (type, A, f, coords...) with 2 (x, z) or 3 (x, y, z) coords."""
+    with open(path, "w") as f:
+        f.write(f"{len(sources)}\n{ntemplate}\n")
+        for s in sources:
+            typ, A, fr, *xyz = s
+            f.write(f"\n{typ}\n{_num(A)}\n{_num(fr)}\n{' '.join(_num(c) for c in xyz)}\n")
+
+
+def write_rcv(path, records):
+    """records: list of (comp, coords tuple, t0_s, dt_ms)."""
+    with open(path, "w") as f:
+        f.write(f"{len(records)}\n")
+        for comp, xyz, t0, dtms in records:
+            f.write(f"\n{comp}\nTrace\n{' '.join(_num(c) for c in xyz)}\n{_num(t0)}\n{_num(dtms)}\n")
+
+
+def trace_path(workdir, basename, n):
+    """Path of record n (1-based) as write_trace names it (io_utils.c:1759)."""
+    return os.path.join(workdir, "trc", basename, f"{basename}_{n}.trc")
+
+
+def read_trc(path):
+    a = np.loadtxt(path, ndmin=2)
+    return a[:, 0], a[:, 1]
+
+
+def read_traces(workdir, basename, nrec):
+    """All .trc records -> (list of time arrays, list of value arrays); the
+    records may have different sample counts."""
+    ts, vs = [], []
+    for n in range(1, nrec + 1):
+        t, v = read_trc(trace_path(workdir, basename, n))
+        ts.append(t)
+        vs.append(v)
+    return ts, vs
