@@ -1,0 +1,225 @@
+/*
+ * seismod_gpu.h -- C ABI of the B200 (sm_100a) FDTD library.
+ *
+ * Drop-in for the time loops of two seismod programs:
+ *
+ *   e_iso     2D P-SV elastic, velocity-stress staggered grid, split-field
+ *             PML (Collino & Tsogka 2001)
+ *   a_iso_3d  3D acoustic, velocity-pressure staggered grid, CPML
+ *
+ * The reference has no library interface: its time loops call C functions on
+ * raw double arrays from main().  Each entry point below names the reference
+ * code it replaces (file:line in the seismod sources).  Every function returns
+ * an int status (SM_OK = 0); none exits or aborts; sm_last_error() gives a
+ * message for the last failure on the calling thread.  Handles are not
+ * thread-safe: use one handle per thread, or serialise calls on it.
+ *
+ * All array arguments are host pointers.  Layouts are the reference's:
+ *   e_iso     interior arrays nx*nz, index i*nz + j (x slow, z fast),
+ *             e_iso.c:384-393
+ *   a_iso_3d  padded arrays nx2*ny2*nz2, index (i*ny2 + j)*nz2 + k,
+ *             a_iso_3d.c:317-335 (nx2 = nx + 2*np, io_utils.c:396-398)
+ */
+#ifndef SEISMOD_GPU_H
+#define SEISMOD_GPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define SM_ABI_VERSION 1
+
+/* status codes */
+#define SM_OK        0
+#define SM_EINVAL    1   /* bad argument                                    */
+#define SM_ENOMEM    2   /* device or host allocation failed                */
+#define SM_ECUDA     3   /* CUDA runtime error                              */
+#define SM_ECFL      4   /* time step violates the reference's CFL test     */
+#define SM_EIO       5   /* file could not be opened / parsed               */
+#define SM_ETIMEOUT  6   /* a bounded wait gave up                          */
+#define SM_EBUSY     7   /* admission refused: not enough device memory     */
+#define SM_ESTATE    8   /* call not valid in the handle's current state    */
+#define SM_ENOTFOUND 9   /* unknown ticket / index                          */
+
+/* storage precision of wavefields and PML/CPML memory variables.
+ * FP32 and FP64 compute in their own type; FP16 and BF16 store 16-bit values
+ * with one power-of-two scale per field and compute in FP32. */
+#define SM_FP32 0
+#define SM_FP64 1
+#define SM_FP16 2
+#define SM_BF16 3
+
+/* source types, numbered as enum sourceType (structs.h:44) */
+#define SM_SRC_SX   0
+#define SM_SRC_SZ   2
+#define SM_SRC_SXZ  4
+#define SM_SRC_BULK 6
+
+/* record components, numbered as enum component (structs.h:45) */
+#define SM_VX  0
+#define SM_VY  1
+#define SM_VZ  2
+#define SM_TXX 5
+#define SM_TZZ 6
+#define SM_TXZ 7
+#define SM_P   8
+
+/* which part of an e_iso field: the total, or the x / z split part that the
+ * PML frame carries (pml.c keeps q_x and q_z, q = q_x + q_z) */
+#define SM_PART_TOTAL 0
+#define SM_PART_X     1
+#define SM_PART_Z     2
+
+/* pass as `shot` to apply a call to every shot of a batch */
+#define SM_ALL_SHOTS ((size_t)-1)
+
+const char *sm_last_error(void);
+int sm_abi_version(void);
+/* device count and the SM count / HBM size of one device */
+int sm_device_info(int device, int *sm_count, size_t *hbm_bytes, size_t *hbm_free);
+
+/* ======================================================================
+ * host-side set-up, FP64, identical in arithmetic to the reference
+ * ====================================================================== */
+
+/* Ricker wavelets of n sources, src.c:43-65 compute_src_fct (including its
+ * normalisation order: every pass rescales wavelet 0).  Row s of fct (stride
+ * doubles) receives length[s] samples.  sm_ricker_length gives the length
+ * the reference allocates for one source. */
+size_t sm_ricker_length(double f, double dt, double fac);
+int sm_ricker(size_t n, const double *A, const double *f, double dt, double fac,
+              size_t stride, double *fct, size_t *length);
+/* time-step count, e_iso.c:575-576 */
+size_t sm_nsteps(double duration, double dt);
+/* receiver sampling predicate at step it, e_iso.c:643-658 */
+int sm_sample_predicate(size_t it, double dt, double t0, double rdt);
+
+/* e_iso material averaging e_iso.c:423-462 (returns max vp through vpmax)
+ * and PML damping profiles e_iso.c:482-500 (d, dh: np values; dH: np+1) */
+int sm_eiso_materials(size_t nx, size_t nz, const double *vp, const double *vs,
+                      const double *rho, double *la, double *mu, double *l2m,
+                      double *b, double *bm, double *vpmax);
+int sm_eiso_profiles(size_t np, double h, size_t ncell, const double *vp,
+                     double *d, double *dh, double *dH);
+
+/* a_iso_3d model padding by edge replication (io_utils.c:1096-1143), the
+ * vp maximum its CFL test uses (a_iso_3d.c:368-374) and its CPML
+ * coefficients (a_iso_3d.c:500-576).  coef: 18 arrays in the order
+ * ax bx kx ay by ky az bz kz (n2 values each) then ax_h ... kz_h (n2-1). */
+int sm_a3d_pad_model(size_t nx, size_t ny, size_t nz, size_t np,
+                     const double *vp, const double *rho, double *vp_pad, double *rho_pad);
+double sm_a3d_cfl_vpmax(size_t nx, size_t nz, const double *vp_pad);
+int sm_a3d_cpml(size_t np, size_t nx2, size_t ny2, size_t nz2,
+                double dx, double dy, double dz, double dt,
+                double pml_order, double vmax, double Rc, double kappa_max,
+                int alpha_max_flag, double f0, double *const *coef);
+
+/* ======================================================================
+ * e_iso on the device
+ * ====================================================================== */
+
+typedef struct sm_eiso *sm_eiso_t;
+
+/* Replaces the allocations of e_iso.c:384-411 and the state the time loop
+ * e_iso.c:589-670 updates.  la, mu, l2m, b, bm are the averaged materials
+ * that update_vx/update_vz/update_txxzz/update_txz (propagate.c:2511-2670)
+ * and pml_v/pml_t (pml.c:39,684) receive; d, dh, dH the PML profiles.
+ * nshots independent shots share the model (batched launch).  npml >= 1
+ * (the reference indexes [npml-1] and fails for npml = 0,
+ * propagate.c:2519). */
+int sm_eiso_create(int device, size_t nx, size_t nz, size_t npml, double h, double dt,
+                   const double *la, const double *mu, const double *l2m,
+                   const double *b, const double *bm,
+                   const double *d, const double *dh, const double *dH,
+                   int precision, size_t nshots, sm_eiso_t *out);
+
+/* Sources of one shot (or SM_ALL_SHOTS), add_src src.c:170-184: at step it
+ * every source with it < length[s] adds scale * fct[s*stride + it] to txx
+ * (Sx, Bulk), tzz (Sz, Bulk) or txz (Sxz) at interior index[s] = i*nz + j.
+ * The reference uses scale = dt.  Replaces the previous source set. */
+int sm_eiso_set_sources(sm_eiso_t h, size_t shot, size_t nsrc, const size_t *index,
+                        const int *type, const double *fct, const size_t *length,
+                        size_t stride, double scale);
+
+/* Trace records of one shot (or SM_ALL_SHOTS), e_iso.c:641-669: receiver r
+ * reads component comp[r] (SM_VX or SM_VZ; SM_TXX/SM_TZZ/SM_TXZ also work)
+ * at interior index[r] after every step it for which
+ * sm_sample_predicate(it, dt, t0[r], rdt[r]) holds, for it < nsteps_max.
+ * Resets the sample counters. */
+int sm_eiso_set_receivers(sm_eiso_t h, size_t shot, size_t nrec, const size_t *index,
+                          const int *comp, const double *t0, const double *rdt,
+                          size_t nsteps_max);
+
+/* Advance every shot by nsteps time steps (the body of e_iso.c:589-670).
+ * Asynchronous: returns once the work is queued. */
+int sm_eiso_run(sm_eiso_t h, size_t nsteps);
+int sm_eiso_sync(sm_eiso_t h);
+/* steps taken so far */
+int sm_eiso_step_count(sm_eiso_t h, size_t *it);
+
+/* Copy the samples taken so far: values (raw field values; the reference
+ * writes 1e3*v, io_utils.c:1767) of receivers [rec0, rec0+nrec) into
+ * out[r*ld + s]; counts[r] receives the number of samples.  Synchronises. */
+int sm_eiso_read_traces(sm_eiso_t h, size_t shot, size_t rec0, size_t nrec,
+                        double *out, size_t ld, size_t *counts);
+
+/* Whole padded field (NX*NZ, NX = nx+2*npml, NZ = nz+2*npml, index X*NZ+Z)
+ * of one shot: SM_PART_TOTAL, or a split part (zero inside the interior).
+ * set_field loads a state (tests, restarts); for SM_PART_TOTAL it writes
+ * interior cells only, PML totals follow from the parts. */
+int sm_eiso_get_field(sm_eiso_t h, size_t shot, int comp, int part, double *out);
+int sm_eiso_set_field(sm_eiso_t h, size_t shot, int comp, int part, const double *in);
+/* zero all wavefields and counters of every shot (e_iso.c:565-572) */
+int sm_eiso_reset(sm_eiso_t h);
+int sm_eiso_destroy(sm_eiso_t h);
+
+/* ======================================================================
+ * a_iso_3d on the device
+ * ====================================================================== */
+
+typedef struct sm_a3d *sm_a3d_t;
+
+/* Replaces the allocations of a_iso_3d.c:317-355, the material set-up
+ * a_iso_3d.c:379-409 and the state of the time loop a_iso_3d.c:593-741.
+ * vp, rho: padded, edge-replicated model (as read_model_a leaves it);
+ * coef: the 18 CPML arrays of sm_a3d_cpml.  Outside the np-node frame the
+ * coefficients must be a = 0, b = k = 1 (the reference's defaults). */
+int sm_a3d_create(int device, size_t nx2, size_t ny2, size_t nz2, size_t np,
+                  double dx, double dy, double dz, double dt,
+                  const double *vp, const double *rho, const double *const *coef,
+                  int precision, sm_a3d_t *out);
+/* a_iso_3d.c:689-693: P[index[s]] += scale * fct[s*stride + it] while
+ * it < length[s]; the reference uses scale = dt * 1e6 for every source type */
+int sm_a3d_set_sources(sm_a3d_t h, size_t nsrc, const size_t *index, const double *fct,
+                       const size_t *length, size_t stride, double scale);
+/* a_iso_3d.c:698-741; comp SM_VX, SM_VY, SM_VZ (SM_P also works) */
+int sm_a3d_set_receivers(sm_a3d_t h, size_t nrec, const size_t *index, const int *comp,
+                         const double *t0, const double *rdt, size_t nsteps_max);
+int sm_a3d_run(sm_a3d_t h, size_t nsteps);
+int sm_a3d_sync(sm_a3d_t h);
+int sm_a3d_step_count(sm_a3d_t h, size_t *it);
+int sm_a3d_read_traces(sm_a3d_t h, size_t rec0, size_t nrec, double *out, size_t ld,
+                       size_t *counts);
+/* whole padded field nx2*ny2*nz2 */
+int sm_a3d_get_field(sm_a3d_t h, int comp, double *out);
+int sm_a3d_set_field(sm_a3d_t h, int comp, const double *in);
+int sm_a3d_reset(sm_a3d_t h);
+int sm_a3d_destroy(sm_a3d_t h);
+
+/* ======================================================================
+ * drop-in programs: the whole of e_iso / a_iso_3d main() on the device,
+ * reading the reference's .par / model / source / output files and writing
+ * its trc/<base>/<base>_<n>.trc files.  argv as the reference takes it
+ * (io_utils.c:156-202: -p file.par, -v, -h); an added "-P fp32|fp64|fp16|bf16"
+ * picks the storage precision (default fp32).  Returns 0 on success.
+ * ====================================================================== */
+int sm_e_iso_main(int argc, char **argv);
+int sm_a_iso_3d_main(int argc, char **argv);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* SEISMOD_GPU_H */

@@ -1,0 +1,332 @@
+"""Python front end of the C ABI: device handles for e_iso and a_iso_3d and
+helpers that take a whole shot from a workload description to traces.
+
+Everything here calls libseismod_gpu.so; the arithmetic of the set-up
+(materials, PML/CPML profiles, Ricker wavelets, sampling predicate) is the
+library's C host code, identical to the reference's, and the time loop runs
+on the GPU.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import math
+
+import numpy as np
+
+from . import _lib as L
+
+
+def c_round(v):
+    """C round() / lround(): half away from zero (io_utils.c:1488, 1650)."""
+    return int(math.copysign(math.floor(abs(v) + 0.5), v))
+
+
+def _f64(a):
+    return np.ascontiguousarray(a, dtype=np.float64)
+
+
+# ----------------------------------------------------------------------------
+# host set-up helpers (C, FP64)
+# ----------------------------------------------------------------------------
+
+def ricker(A, f, dt, fac=1.0):
+    """src.c:43-65 -> (fct [n, stride], lengths)."""
+    lib = L.load()
+    A, f = _f64(np.atleast_1d(A)), _f64(np.atleast_1d(f))
+    stride = max(int(lib.sm_ricker_length(float(x), dt, fac)) for x in f)
+    fct = np.zeros((len(A), stride))
+    ln = np.zeros(len(A), dtype=np.uintp)
+    L.check(lib.sm_ricker(len(A), L.dptr(A), L.dptr(f), dt, fac, stride, L.dptr(fct),
+                          L.szptr(ln)))
+    return fct, ln.astype(np.int64)
+
+
+def nsteps(duration, dt):
+    return int(L.load().sm_nsteps(duration, dt))
+
+
+def sample_predicate(it, dt, t0, rdt):
+    return bool(L.load().sm_sample_predicate(it, dt, t0, rdt))
+
+
+def eiso_materials(vp, vs, rho):
+    lib = L.load()
+    nx, nz = vp.shape
+    vp, vs, rho = _f64(vp), _f64(vs), _f64(rho)
+    out = [np.zeros((nx, nz)) for _ in range(5)]
+    vmax = C.c_double()
+    L.check(lib.sm_eiso_materials(nx, nz, L.dptr(vp), L.dptr(vs), L.dptr(rho),
+                                  *[L.dptr(a) for a in out], C.byref(vmax)))
+    return (*out, vmax.value)
+
+
+def eiso_profiles(npml, h, vp):
+    vp = _f64(vp)
+    d, dh, dH = np.zeros(npml), np.zeros(npml), np.zeros(npml + 1)
+    L.check(L.load().sm_eiso_profiles(npml, h, vp.size, L.dptr(vp), L.dptr(d), L.dptr(dh),
+                                      L.dptr(dH)))
+    return d, dh, dH
+
+
+def a3d_pad_model(vp, rho, npml):
+    nx, ny, nz = vp.shape
+    vp, rho = _f64(vp), _f64(rho)
+    shp = (nx + 2 * npml, ny + 2 * npml, nz + 2 * npml)
+    vpp, rhop = np.zeros(shp), np.zeros(shp)
+    L.check(L.load().sm_a3d_pad_model(nx, ny, nz, npml, L.dptr(vp), L.dptr(rho), L.dptr(vpp),
+                                      L.dptr(rhop)))
+    return vpp, rhop
+
+
+def a3d_cfl_vpmax(nx, nz, vp_pad):
+    return L.load().sm_a3d_cfl_vpmax(nx, nz, L.dptr(_f64(vp_pad)))
+
+
+def a3d_cpml(npml, shape2, d, dt, pml_order=2.0, vmax=5000.0, Rc=1e-5, kappa_max=1.0,
+             alpha_max_flag=1, f0=0.0):
+    n2 = list(shape2)
+    arrs = [np.zeros(n2[c // 3]) for c in range(9)] + \
+           [np.zeros(n2[(c - 9) // 3] - 1) for c in range(9, 18)]
+    P = (L._dp * 18)(*[L.dptr(a) for a in arrs])
+    L.check(L.load().sm_a3d_cpml(npml, n2[0], n2[1], n2[2], d[0], d[1], d[2], dt, pml_order,
+                                 vmax, Rc, kappa_max, alpha_max_flag, f0, P))
+    return arrs
+
+
+# ----------------------------------------------------------------------------
+# device handles
+# ----------------------------------------------------------------------------
+
+class EIsoDevice:
+    """An e_iso state on the GPU: nshots shots over one model."""
+
+    def __init__(self, nx, nz, npml, h, dt, la, mu, l2m, b, bm, d, dh, dH,
+                 precision="fp32", nshots=1, device=0):
+        lib = L.load()
+        self.nx, self.nz, self.npml, self.h, self.dt = nx, nz, npml, h, dt
+        self.NX, self.NZ = nx + 2 * npml, nz + 2 * npml
+        self.nshots = nshots
+        self.precision = precision
+        arrs = [_f64(a) for a in (la, mu, l2m, b, bm, d, dh, dH)]
+        hnd = C.c_void_p()
+        L.check(lib.sm_eiso_create(device, nx, nz, npml, h, dt, *[L.dptr(a) for a in arrs],
+                                   L.PRECISIONS[precision], nshots, C.byref(hnd)))
+        self._h = hnd
+        self.nrec = [0] * nshots
+
+    def close(self):
+        if getattr(self, "_h", None) and self._h.value:
+            L.load().sm_eiso_destroy(self._h)
+            self._h = None
+
+    __del__ = close
+
+    def set_sources(self, shot, index, types, fct, lengths, scale):
+        index = np.ascontiguousarray(index, dtype=np.uintp)
+        types = np.ascontiguousarray(types, dtype=np.int32)
+        fct = _f64(fct)
+        lengths = np.ascontiguousarray(lengths, dtype=np.uintp)
+        shot = L.SM_ALL_SHOTS if shot is None else shot
+        L.check(L.load().sm_eiso_set_sources(self._h, shot, len(index), L.szptr(index),
+                                             L.iptr(types), L.dptr(fct), L.szptr(lengths),
+                                             fct.shape[1] if fct.ndim == 2 else fct.size, scale))
+
+    def set_receivers(self, shot, index, comps, t0, rdt, nsteps_max):
+        index = np.ascontiguousarray(index, dtype=np.uintp)
+        comps = np.ascontiguousarray(comps, dtype=np.int32)
+        t0, rdt = _f64(t0), _f64(rdt)
+        L.check(L.load().sm_eiso_set_receivers(
+            self._h, L.SM_ALL_SHOTS if shot is None else shot, len(index), L.szptr(index),
+            L.iptr(comps), L.dptr(t0), L.dptr(rdt), nsteps_max))
+        for s in (range(self.nshots) if shot is None else [shot]):
+            self.nrec[s] = len(index)
+
+    def run(self, n):
+        L.check(L.load().sm_eiso_run(self._h, n))
+
+    def sync(self):
+        L.check(L.load().sm_eiso_sync(self._h))
+
+    def traces(self, shot=0, max_samples=None):
+        n = self.nrec[shot]
+        counts = np.zeros(n, dtype=np.uintp)
+        L.check(L.load().sm_eiso_read_traces(self._h, shot, 0, n, None, 0, L.szptr(counts)))
+        ld = int(counts.max()) if n else 0
+        out = np.zeros((n, max(ld, 1)))
+        if n and ld:
+            L.check(L.load().sm_eiso_read_traces(self._h, shot, 0, n, L.dptr(out), ld,
+                                                 L.szptr(counts)))
+        return [out[r, :int(counts[r])].copy() for r in range(n)]
+
+    def get_field(self, comp, shot=0, part="total"):
+        out = np.zeros((self.NX, self.NZ))
+        L.check(L.load().sm_eiso_get_field(self._h, shot, L.SM_COMP[comp], L.SM_PART[part],
+                                           L.dptr(out)))
+        return out
+
+    def set_field(self, comp, arr, shot=0, part="total"):
+        a = _f64(arr).reshape(self.NX, self.NZ)
+        L.check(L.load().sm_eiso_set_field(self._h, shot, L.SM_COMP[comp], L.SM_PART[part],
+                                           L.dptr(a)))
+
+    def reset(self):
+        L.check(L.load().sm_eiso_reset(self._h))
+
+
+class A3DDevice:
+    """An a_iso_3d state on the GPU."""
+
+    def __init__(self, vp_pad, rho_pad, npml, d, dt, coef, precision="fp32", device=0):
+        lib = L.load()
+        self.shape = vp_pad.shape
+        self.npml, self.d, self.dt, self.precision = npml, d, dt, precision
+        vp_pad, rho_pad = _f64(vp_pad), _f64(rho_pad)
+        cf = [_f64(c) for c in coef]
+        P = (L._dp * 18)(*[L.dptr(c) for c in cf])
+        hnd = C.c_void_p()
+        n = self.shape
+        L.check(lib.sm_a3d_create(device, n[0], n[1], n[2], npml, d[0], d[1], d[2], dt,
+                                  L.dptr(vp_pad), L.dptr(rho_pad), P, L.PRECISIONS[precision],
+                                  C.byref(hnd)))
+        self._h = hnd
+        self.nrec = 0
+
+    def close(self):
+        if getattr(self, "_h", None) and self._h.value:
+            L.load().sm_a3d_destroy(self._h)
+            self._h = None
+
+    __del__ = close
+
+    def set_sources(self, index, fct, lengths, scale):
+        index = np.ascontiguousarray(index, dtype=np.uintp)
+        fct = _f64(fct)
+        lengths = np.ascontiguousarray(lengths, dtype=np.uintp)
+        L.check(L.load().sm_a3d_set_sources(self._h, len(index), L.szptr(index), L.dptr(fct),
+                                            L.szptr(lengths), fct.shape[1], scale))
+
+    def set_receivers(self, index, comps, t0, rdt, nsteps_max):
+        index = np.ascontiguousarray(index, dtype=np.uintp)
+        comps = np.ascontiguousarray(comps, dtype=np.int32)
+        t0, rdt = _f64(t0), _f64(rdt)
+        L.check(L.load().sm_a3d_set_receivers(self._h, len(index), L.szptr(index),
+                                              L.iptr(comps), L.dptr(t0), L.dptr(rdt),
+                                              nsteps_max))
+        self.nrec = len(index)
+
+    def run(self, n):
+        L.check(L.load().sm_a3d_run(self._h, n))
+
+    def sync(self):
+        L.check(L.load().sm_a3d_sync(self._h))
+
+    def traces(self):
+        n = self.nrec
+        counts = np.zeros(n, dtype=np.uintp)
+        L.check(L.load().sm_a3d_read_traces(self._h, 0, n, None, 0, L.szptr(counts)))
+        ld = int(counts.max()) if n else 0
+        out = np.zeros((n, max(ld, 1)))
+        if n and ld:
+            L.check(L.load().sm_a3d_read_traces(self._h, 0, n, L.dptr(out), ld, L.szptr(counts)))
+        return [out[r, :int(counts[r])].copy() for r in range(n)]
+
+    def traces_array(self):
+        """Traces as one [nrec, nsamples] array (all receivers equally sampled)."""
+        n = self.nrec
+        counts = np.zeros(n, dtype=np.uintp)
+        L.check(L.load().sm_a3d_read_traces(self._h, 0, n, None, 0, L.szptr(counts)))
+        ld = int(counts.max()) if n else 0
+        out = np.zeros((n, max(ld, 1)))
+        if n and ld:
+            L.check(L.load().sm_a3d_read_traces(self._h, 0, n, L.dptr(out), ld, L.szptr(counts)))
+        return out
+
+    def get_field(self, comp):
+        out = np.zeros(self.shape)
+        L.check(L.load().sm_a3d_get_field(self._h, L.SM_COMP[comp], L.dptr(out)))
+        return out
+
+    def set_field(self, comp, arr):
+        L.check(L.load().sm_a3d_set_field(self._h, L.SM_COMP[comp], L.dptr(_f64(arr))))
+
+    def reset(self):
+        L.check(L.load().sm_a3d_reset(self._h))
+
+
+# ----------------------------------------------------------------------------
+# whole shots from workload descriptions (seismod_b200.workloads)
+# ----------------------------------------------------------------------------
+
+def eiso_device(p, precision="fp32", shots=None, device=0):
+    """Build an EIsoDevice for problem p with sources of `shots` (default:
+    all shots of p) and p's receivers.  Returns (dev, nsteps)."""
+    la, mu, l2m, b, bm, vpmax = eiso_materials(p.vp, p.vs, p.rho)
+    dt = p.dt
+    if dt > p.h / (math.sqrt(2.0) * vpmax):
+        raise L.SeismodError(L.SM_ECFL, "time step too large (e_iso.c:476)")
+    d, dh, dH = eiso_profiles(p.npml, p.h, p.vp)
+    shots = list(range(len(p.shots))) if shots is None else list(shots)
+    dev = EIsoDevice(p.nx, p.nz, p.npml, p.h, dt, la, mu, l2m, b, bm, d, dh, dH, precision,
+                     len(shots), device)
+    n = nsteps(p.duration, dt)
+    for k, s in enumerate(shots):
+        srcs = p.shots[s]
+        fct, ln = ricker([q[1] for q in srcs], [q[2] for q in srcs], dt)
+        idx = [c_round((q[3] - p.x0) / p.h) * p.nz + c_round((q[4] - p.z0) / p.h) for q in srcs]
+        typ = [L.SM_SRC[q[0].lower()] for q in srcs]
+        dev.set_sources(k, idx, typ, fct, ln, dt)
+    ridx = [c_round((x - p.x0) / p.h) * p.nz + c_round((z - p.z0) / p.h)
+            for (_, x, z, _, _) in p.receivers]
+    comps = [L.SM_COMP[c.lower()] for (c, _, _, _, _) in p.receivers]
+    t0 = [r[3] for r in p.receivers]
+    rdt = [r[4] * 1e-3 for r in p.receivers]
+    dev.set_receivers(None, ridx, comps, t0, rdt, n)
+    return dev, n
+
+
+def run_eiso(p, precision="fp32", shots=None, device=0, nsteps_override=None):
+    """Whole shots on the GPU -> list (per shot) of lists of trace arrays
+    (raw velocities; the reference's .trc files hold 1e3 * v)."""
+    dev, n = eiso_device(p, precision, shots, device)
+    dev.run(n if nsteps_override is None else nsteps_override)
+    out = [dev.traces(s) for s in range(dev.nshots)]
+    dev.close()
+    return out
+
+
+def a3d_index(p, x, y, z):
+    nx2, ny2, nz2 = (n + 2 * p.npml for n in p.shape)
+    i = c_round((x - p.origin[0]) / p.d[0]) + p.npml
+    j = c_round((y - p.origin[1]) / p.d[1]) + p.npml
+    k = c_round((z - p.origin[2]) / p.d[2]) + p.npml
+    return (i * ny2 + j) * nz2 + k
+
+
+def a3d_device(p, precision="fp32", device=0):
+    nx, ny, nz = p.shape
+    vpp, rhop = a3d_pad_model(p.vp, p.rho, p.npml)
+    dt = p.dt
+    vpmax = a3d_cfl_vpmax(nx, nz, vpp)
+    dx, dy, dz = p.d
+    if dt * vpmax * math.sqrt(1. / dx ** 2 + 1. / dy ** 2 + 1. / dz ** 2) > 1.:
+        raise L.SeismodError(L.SM_ECFL, "time step too large (a_iso_3d.c:411-417)")
+    coef = a3d_cpml(p.npml, vpp.shape, p.d, dt, 2.0, 5000.0, p.Rc, p.kappa_max, p.alpha_max,
+                    p.sources[0][2])
+    dev = A3DDevice(vpp, rhop, p.npml, p.d, dt, coef, precision, device)
+    n = nsteps(p.duration, dt)
+    fct, ln = ricker([q[1] for q in p.sources], [q[2] for q in p.sources], dt)
+    idx = [a3d_index(p, q[3], q[4], q[5]) for q in p.sources]
+    dev.set_sources(idx, fct, ln, dt * 1e6)
+    ridx = [a3d_index(p, x, y, z) for (_, x, y, z, _, _) in p.receivers]
+    comps = [L.SM_COMP[c.lower()] for (c, _, _, _, _, _) in p.receivers]
+    dev.set_receivers(ridx, comps, [r[4] for r in p.receivers],
+                      [r[5] * 1e-3 for r in p.receivers], n)
+    return dev, n
+
+
+def run_a3d(p, precision="fp32", device=0, nsteps_override=None):
+    dev, n = a3d_device(p, precision, device)
+    dev.run(n if nsteps_override is None else nsteps_override)
+    out = dev.traces()
+    dev.close()
+    return out

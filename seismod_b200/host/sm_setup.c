@@ -1,0 +1,229 @@
+/*
+ * sm_setup.c -- host-side set-up of the e_iso / a_iso_3d paths, in FP64.
+ *
+ * These run once per shot before the time loop and must produce exactly the
+ * numbers the reference feeds its loops: the same formulas in the same
+ * order of operations, so results match bit for bit.
+ */
+#include "sm_host.h"
+
+#include <math.h>
+#include <stdlib.h>
+#include <string.h>
+
+size_t sm_ricker_length(double f, double dt, double fac)
+{
+    /* src.c:47-48 */
+    double tcut = 1.0 / f;
+    return (size_t)ceil(tcut * 2.0 / (fac * dt));
+}
+
+int sm_ricker(size_t n, const double *A, const double *f, double dt0, double fac,
+              size_t stride, double *fct, size_t *length)
+{
+    if (n == 0) return SM_OK;
+    if (!A || !f || !fct || !length || !(dt0 > 0.0) || !(fac > 0.0)) {
+        return sm_fail(SM_EINVAL, "sm_ricker: bad argument");
+    }
+    const double pi = 4.0 * atan(1.0);
+    const double pi2 = pi * pi;
+    const double dt = fac * dt0;
+    for (size_t s = 0; s < n; ++s) {
+        if (!(f[s] > 0.0)) return sm_fail(SM_EINVAL, "sm_ricker: frequency must be > 0");
+        if (sm_ricker_length(f[s], dt0, fac) > stride)
+            return sm_fail(SM_EINVAL, "sm_ricker: stride shorter than the wavelet");
+    }
+    /* src.c:43-65.  Pass s writes wavelet s, takes the peak of wavelet 0 over
+     * the first length[s] samples, and rescales wavelet 0 by A[s] / peak.
+     * Where the reference would read wavelet 0 past its end (length[s] >
+     * length[0]) the scan stops at length[0]. */
+    for (size_t s = 0; s < n; ++s) {
+        const double tcut = 1.0 / f[s];
+        length[s] = sm_ricker_length(f[s], dt0, fac);
+        double *w = fct + s * stride;
+        double peak = 0.0;
+        for (size_t i = 0; i < length[s]; ++i) {
+            double time = i * dt - tcut;
+            /* same left-to-right products as the reference */
+            double K = pi2 * f[s] * f[s] * time * time;
+            w[i] = A[s] * 2. * pi2 * f[s] * f[s] * (1.0 - 2.0 * K) * exp(-K);
+            if (i < length[0]) {
+                double a = fabs(fct[i]);
+                if (a > peak) peak = a;
+            }
+        }
+        for (size_t i = 0; i < length[0]; ++i) fct[i] *= A[s] / peak;
+    }
+    return SM_OK;
+}
+
+size_t sm_nsteps(double duration, double dt)
+{
+    size_t n = (size_t)(duration / dt);
+    if (n * dt < duration) n++;
+    return n;
+}
+
+int sm_sample_predicate(size_t it, double dt, double t0, double rdt)
+{
+    /* e_iso.c:643-658, a_iso_3d.c:700-719 */
+    const double t = dt * (it + 1);
+    const double dt2 = t - t0 + 1.e-15;
+    const double rem = fmod(1.e6 * dt2, 1.e6 * rdt);
+    return (fabs(dt2) < 0.99 * dt) || (t > t0 && rdt > 0.0 && fabs(rem) < 1.e-8);
+}
+
+int sm_eiso_materials(size_t nx, size_t nz, const double *vp, const double *vs,
+                      const double *rho, double *la, double *mu, double *l2m,
+                      double *b, double *bm, double *vpmax)
+{
+    if (nx < 2 || nz < 2 || !vp || !vs || !rho || !la || !mu || !l2m || !b || !bm)
+        return sm_fail(SM_EINVAL, "sm_eiso_materials: bad argument (nx, nz >= 2)");
+    const size_t n = nx * nz;
+    /* nodal lambda, mu, lambda + 2 mu kept in the outputs' spare room:
+     * la <- nodal lambda first, then averaged along x in place, column by
+     * column from the front (each average reads i and i+1 before i+1 is
+     * rewritten).  mu and l2m likewise. */
+    double vmax = 0.0;
+    for (size_t q = 0; q < n; ++q) {
+        if (vp[q] > vmax) vmax = vp[q];
+        double lam = rho[q] * (vp[q] * vp[q] - 2. * vs[q] * vs[q]);  /* e_iso.c:428 */
+        double m = rho[q] * vs[q] * vs[q];                           /* :429 */
+        la[q] = lam;
+        mu[q] = m;
+        l2m[q] = lam + 2. * m;                                       /* :430 */
+        b[q] = 1. / rho[q];                                          /* :431 */
+    }
+    /* mu: average along z, last row nodal (e_iso.c:438-443) */
+    for (size_t i = 0; i < nx; ++i)
+        for (size_t j = 0; j + 1 < nz; ++j)
+            mu[i * nz + j] = (mu[i * nz + j] + mu[i * nz + j + 1]) / 2.0;
+    /* lambda, lambda + 2 mu: average along x, last column nodal (:444-451) */
+    for (size_t i = 0; i + 1 < nx; ++i)
+        for (size_t j = 0; j < nz; ++j) {
+            la[i * nz + j] = (la[i * nz + j] + la[(i + 1) * nz + j]) / 2.0;
+            l2m[i * nz + j] = (l2m[i * nz + j] + l2m[(i + 1) * nz + j]) / 2.0;
+        }
+    /* 1/rho at the vz node: 4-point mean, 2-point on the last row/column,
+     * nodal in the last corner (:452-462) */
+    for (size_t i = 0; i + 1 < nx; ++i) {
+        for (size_t j = 0; j + 1 < nz; ++j)
+            bm[i * nz + j] = (b[i * nz + j] + b[(i + 1) * nz + j] +
+                              b[i * nz + j + 1] + b[(i + 1) * nz + j + 1]) / 4.0;
+        bm[i * nz + nz - 1] = (b[i * nz + nz - 1] + b[(i + 1) * nz + nz - 1]) / 2.0;
+    }
+    for (size_t j = 0; j + 1 < nz; ++j)
+        bm[(nx - 1) * nz + j] = (b[(nx - 1) * nz + j] + b[(nx - 1) * nz + j + 1]) / 2.0;
+    bm[n - 1] = b[n - 1];
+    if (vpmax) *vpmax = vmax;
+    return SM_OK;
+}
+
+int sm_eiso_profiles(size_t np, double h, size_t ncell, const double *vp,
+                     double *d, double *dh, double *dH)
+{
+    if (np == 0 || ncell == 0 || !vp || !d || !dh || !dH || !(h > 0.0))
+        return sm_fail(SM_EINVAL, "sm_eiso_profiles: bad argument");
+    /* e_iso.c:486-500: d0 from the MEAN vp, R = 1e-3, quadratic profile */
+    double vbar = 0.0;
+    for (size_t q = 0; q < ncell; ++q) vbar += vp[q];
+    vbar /= (double)ncell;
+    const double R = 0.001;
+    const double delta = np * h;
+    const double d0 = log(1. / R) * 3. / 2. * vbar / delta;
+    for (size_t n = 0; n < np; ++n) {
+        d[n] = d0 * pow(((np - n) * h / delta), 2);
+        dh[n] = d0 * pow((((np - n) * h - h / 2.) / delta), 2);
+    }
+    for (size_t n = 0; n < np + 1; ++n) dH[n] = d0 * pow((((np - n) * h + h / 2.) / delta), 2);
+    return SM_OK;
+}
+
+int sm_a3d_pad_model(size_t nx, size_t ny, size_t nz, size_t np,
+                     const double *vp, const double *rho, double *vp_pad, double *rho_pad)
+{
+    if (!nx || !ny || !nz || !vp || !rho || !vp_pad || !rho_pad)
+        return sm_fail(SM_EINVAL, "sm_a3d_pad_model: bad argument");
+    /* io_utils.c:1096-1143: every padded node takes the value of the nearest
+     * interior node (replication along z, then y, then x) */
+    const size_t nx2 = nx + 2 * np, ny2 = ny + 2 * np, nz2 = nz + 2 * np;
+    for (size_t i = 0; i < nx2; ++i) {
+        size_t ii = i < np ? 0 : (i - np >= nx ? nx - 1 : i - np);
+        for (size_t j = 0; j < ny2; ++j) {
+            size_t jj = j < np ? 0 : (j - np >= ny ? ny - 1 : j - np);
+            const double *sv = vp + (ii * ny + jj) * nz;
+            const double *sr = rho + (ii * ny + jj) * nz;
+            double *dv = vp_pad + (i * ny2 + j) * nz2;
+            double *dr = rho_pad + (i * ny2 + j) * nz2;
+            for (size_t k = 0; k < nz2; ++k) {
+                size_t kk = k < np ? 0 : (k - np >= nz ? nz - 1 : k - np);
+                dv[k] = sv[kk];
+                dr[k] = sr[kk];
+            }
+        }
+    }
+    return SM_OK;
+}
+
+double sm_a3d_cfl_vpmax(size_t nx, size_t nz, const double *vp_pad)
+{
+    /* a_iso_3d.c:368-374 scans index i*nz + j (i < nx, j < nz) of the padded
+     * 3-D array; kept as is so the same inputs pass or fail the test */
+    double v = 0.0;
+    for (size_t i = 0; i < nx; ++i)
+        for (size_t j = 0; j < nz; ++j) {
+            double a = vp_pad[i * nz + j];
+            if (a > v) v = a;
+        }
+    return v;
+}
+
+int sm_a3d_cpml(size_t np, size_t nx2, size_t ny2, size_t nz2,
+                double dx, double dy, double dz, double dt,
+                double pml_order, double vmax, double Rc, double kappa_max,
+                int alpha_max_flag, double f0, double *const *coef)
+{
+    if (!coef) return sm_fail(SM_EINVAL, "sm_a3d_cpml: coef is NULL");
+    const size_t n2[3] = {nx2, ny2, nz2};
+    const double hh[3] = {dx, dy, dz};
+    for (int c = 0; c < 18; ++c)
+        if (!coef[c]) return sm_fail(SM_EINVAL, "sm_a3d_cpml: coefficient array is NULL");
+    for (int a = 0; a < 3; ++a) {
+        if (n2[a] < 2 * np + 2) return sm_fail(SM_EINVAL, "sm_a3d_cpml: grid smaller than the frame");
+        double *A = coef[3 * a], *B = coef[3 * a + 1], *K = coef[3 * a + 2];
+        double *Ah = coef[9 + 3 * a], *Bh = coef[9 + 3 * a + 1], *Kh = coef[9 + 3 * a + 2];
+        /* a_iso_3d.c:525-548 */
+        for (size_t n = 0; n < n2[a]; ++n) { A[n] = 0.0; B[n] = 1.0; K[n] = 1.0; }
+        for (size_t n = 0; n + 1 < n2[a]; ++n) { Ah[n] = 0.0; Bh[n] = 1.0; Kh[n] = 1.0; }
+    }
+    if (np == 0) return SM_OK;
+    /* a_iso_3d.c:550-576 */
+    const double pi = 4.0 * atan(1.0);
+    const double amax = alpha_max_flag == 0 ? 0.0 : pi * f0;
+    const double da = amax / np;
+    for (int a = 0; a < 3; ++a) {
+        double *A = coef[3 * a], *B = coef[3 * a + 1], *K = coef[3 * a + 2];
+        double *Ah = coef[9 + 3 * a], *Bh = coef[9 + 3 * a + 1], *Kh = coef[9 + 3 * a + 2];
+        const size_t N = n2[a];
+        const double L = np * hh[a];
+        const double d0 = -(pml_order + 1.) * vmax * log(Rc) / (2. * L);
+        for (size_t n = 0; n < np; ++n) {
+            double k = 1. + (kappa_max - 1.) * pow(((np - n) * hh[a] / L), pml_order);
+            double kh = 1. + (kappa_max - 1.) * pow(((np - n - 0.5) * hh[a] / L), pml_order);
+            double al = n * da, alh = (n + 0.5) * da;
+            double dd = d0 * pow(((np - n) * hh[a] / L), pml_order);
+            double ddh = d0 * pow(((np - n - 0.5) * hh[a] / L), pml_order);
+            double b = exp(-(dd / k + al) * dt);
+            double bh = exp(-(ddh / kh + alh) * dt);
+            double c = dd * (b - 1.) / (k * (dd + k * al));
+            double ch = ddh * (bh - 1.) / (kh * (ddh + kh * alh));
+            K[n] = K[N - 1 - n] = k;
+            Kh[n] = Kh[N - 2 - n] = kh;
+            B[n] = B[N - 1 - n] = b;
+            Bh[n] = Bh[N - 2 - n] = bh;
+            A[n] = A[N - 1 - n] = c;
+            Ah[n] = Ah[N - 2 - n] = ch;
+        }
+    }
+    return SM_OK;
+}

@@ -1,0 +1,84 @@
+"""a_iso_3d on the GPU against the FP64 oracle and the reference's golden
+traces.  Tolerances as for e_iso: FP64 1e-10, FP32 1e-5 relative L2."""
+import glob
+import os
+
+import numpy as np
+import pytest
+
+import harness as H
+from golden import make_golden as G
+from oracle import oracle as O
+from seismod_b200 import api
+from seismod_b200 import workloads as W
+
+pytestmark = pytest.mark.gpu
+
+TOL = {"fp64": 1e-10, "fp32": 1e-5}
+GOLDEN = sorted(glob.glob(os.path.join(os.path.dirname(__file__), "golden", "a3d_*.npz")))
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+@pytest.mark.parametrize("shape", [((12, 10, 14), 2), ((20, 20, 20), 5), ((9, 17, 33), 3)])
+def test_steps_from_random_state(shape, precision):
+    (nx, ny, nz), npml = shape
+    rng = np.random.default_rng(nx * ny + nz)
+    vp = 1500 + 3000 * rng.random((nx, ny, nz))
+    rho = 1800 + 600 * rng.random((nx, ny, nz))
+    p = W.A3DProblem(vp, rho, (4.0, 5.0, 3.0), npml, 0.2, 1.0, [("Bulk", 1.0, 30.0, 0, 0, 0)],
+                     [], Rc=1e-3, kappa_max=2.0, alpha_max=1)
+    vmax = vp.max()
+    p.dt_ms = 0.5 / (vmax * np.sqrt(1 / 16 + 1 / 25 + 1 / 9)) * 1e3
+    s = H.a3d_setup(p)
+    orc = O.A3D(s["vpp"], s["rhop"], *p.d, s["dt"], s["coef"])
+    dev = api.A3DDevice(s["vpp"], s["rhop"], npml, p.d, s["dt"], s["coef"], precision)
+    shp = s["vpp"].shape
+    for f, sc in (("p", 1e5), ("vx", 1e-2), ("vy", 1e-2), ("vz", 1e-2)):
+        a = sc * rng.standard_normal(shp)
+        orc.set(f, a)
+        dev.set_field(f, a)
+    for _ in range(4):
+        orc.velocity()
+        orc.pressure()
+    dev.run(4)
+    for f in ("p", "vx", "vy", "vz"):
+        e = O.rel_l2(dev.get_field(f), orc.get(f))
+        assert e < TOL[precision], (f, e)
+    dev.close()
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+@pytest.mark.parametrize("path", GOLDEN, ids=[os.path.basename(p)[:-4] for p in GOLDEN])
+def test_golden_traces(path, precision):
+    p, kind, program, ref_t, ref_v = G.load(path)
+    got = [1e3 * t for t in api.run_a3d(p, precision)]
+    assert [len(a) for a in got] == [len(a) for a in ref_v]
+    assert H.rel_l2(got, ref_v) < max(TOL[precision], 2e-6)
+    if precision == "fp64":
+        orc, _, _ = H.run_a3d_oracle(p)
+        assert H.rel_l2(got, orc) < TOL["fp64"]
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+def test_cfg1_family_against_oracle(precision):
+    # the cfg1 model family at 48^3 (+2x8 CPML), 300 steps, 16x16 surface receivers
+    p = W.cfg1(n=48, npml=8, nsteps=300, seed=21, rec_stride=3, nrec_side=16)
+    got = [1e3 * t for t in api.run_a3d(p, precision)]
+    orc, _, _ = H.run_a3d_oracle(p)
+    assert H.rel_l2(got, orc) < TOL[precision]
+
+
+def test_pressure_receivers_and_reset():
+    p = W.cfg1(n=24, npml=4, nsteps=100, seed=5, rec_stride=6, nrec_side=3)
+    p.receivers = p.receivers + [("P", 60.0, 60.0, 60.0, 0.0, p.dt_ms)]
+    dev, n = api.a3d_device(p, "fp64")
+    dev.run(n)
+    a = dev.traces()
+    orc, _, _ = H.run_a3d_oracle(p)
+    assert H.rel_l2([1e3 * t for t in a], orc) < TOL["fp64"]
+    dev.reset()
+    dev.run(n)
+    b = dev.traces()
+    for x, y in zip(a, b):
+        np.testing.assert_array_equal(x, y)
+    dev.close()

@@ -1,0 +1,139 @@
+"""e_iso on the GPU against the FP64 oracle and the reference's golden traces.
+
+Tolerances (relative L2 over all compared values):
+  FP64 device vs FP64 oracle      1e-10  (same arithmetic up to operation order)
+  FP32 device vs oracle/reference 1e-5   (the FP32 bound stated for this path)
+"""
+import glob
+import math
+import os
+
+import numpy as np
+import pytest
+
+import harness as H
+from golden import make_golden as G
+from oracle import oracle as O
+from seismod_b200 import api
+from seismod_b200 import workloads as W
+
+pytestmark = pytest.mark.gpu
+
+TOL = {"fp64": 1e-10, "fp32": 1e-5}
+GOLDEN = sorted(glob.glob(os.path.join(os.path.dirname(__file__), "golden", "eiso_*.npz")))
+FIELDS = ("vx", "vz", "txx", "tzz", "txz")
+
+
+def _pair(nx, nz, P, seed, precision):
+    rng = np.random.default_rng(seed)
+    vp = 3000 + 1000 * rng.random((nx, nz))
+    vs = vp / (1.6 + 0.3 * rng.random((nx, nz)))
+    rho = 2000 + 400 * rng.random((nx, nz))
+    la, mu, l2m, b, bm, vpmax = O.eiso_materials(vp, vs, rho)
+    h = 1.0
+    dt = 0.5 * h / (math.sqrt(2) * vpmax)
+    d, dh, dH = O.eiso_profiles(P, h, vp)
+    orc = O.EIso(nx, nz, P, h, dt, la, mu, l2m, b, bm, d, dh, dH)
+    dev = api.EIsoDevice(nx, nz, P, h, dt, la, mu, l2m, b, bm, d, dh, dH, precision)
+    NX, NZ = nx + 2 * P, nz + 2 * P
+    inter = np.zeros((NX, NZ), bool)
+    inter[P:P + nx, P:P + nz] = True
+    for f in FIELDS:
+        scale = 1e-3 if f.startswith("v") else 1e4
+        tot, xp, zp = (scale * rng.standard_normal((NX, NZ)) for _ in range(3))
+        xp[inter] = 0
+        zp[inter] = 0
+        for tgt in (orc, dev):
+            if tgt is orc:
+                orc.set(f, "x", xp)
+                orc.set(f, "z", zp)
+                orc.set(f, "total", np.where(inter, tot, 0))
+            else:
+                dev.set_field(f, xp, part="x")
+                dev.set_field(f, zp, part="z")
+                dev.set_field(f, np.where(inter, tot, 0), part="total")
+    return orc, dev
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+@pytest.mark.parametrize("shape", [(13, 9, 3), (9, 14, 4), (33, 40, 8), (8, 8, 1), (40, 12, 2)])
+def test_steps_from_random_state(shape, precision):
+    nx, nz, P = shape
+    orc, dev = _pair(nx, nz, P, sum(shape), precision)
+    for _ in range(4):
+        orc.velocity()
+        orc.stress()
+    dev.run(4)
+    for f in FIELDS:
+        for part in ("total", "x", "z"):
+            a, b = dev.get_field(f, part=part), orc.get(f, part)
+            assert O.rel_l2(a, b) < TOL[precision], (f, part, O.rel_l2(a, b))
+    dev.close()
+
+
+def _dev_traces_mm(p, precision):
+    return [1e3 * t for t in api.run_eiso(p, precision, shots=[0])[0]]
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+@pytest.mark.parametrize("path", GOLDEN, ids=[os.path.basename(p)[:-4] for p in GOLDEN])
+def test_golden_traces(path, precision):
+    p, kind, program, ref_t, ref_v = G.load(path)
+    got = _dev_traces_mm(p, precision)
+    assert [len(a) for a in got] == [len(a) for a in ref_v]
+    # reference values carry 7 printed digits
+    assert H.rel_l2(got, ref_v) < max(TOL[precision], 2e-6)
+    if precision == "fp64":
+        orc, _, _ = H.run_eiso_oracle(p)
+        assert H.rel_l2(got, orc) < TOL["fp64"]
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+def test_cfg0_full_size_against_oracle(precision):
+    p = W.cfg0()
+    got = api.run_eiso(p, precision)[0]
+    orc, _, _ = H.run_eiso_oracle(p)
+    assert [len(a) for a in got] == [len(a) for a in orc]
+    assert H.rel_l2([1e3 * g for g in got], orc) < TOL[precision]
+
+
+def test_batched_shots_equal_single_shots():
+    p = W.cfg2(nx=120, nz=80, npml=10, nsteps=250, nshots=5, nrec=12)
+    batch = api.run_eiso(p, "fp32")
+    for s in (0, 2, 4):
+        alone = api.run_eiso(p, "fp32", shots=[s])[0]
+        for a, b in zip(batch[s], alone):
+            np.testing.assert_array_equal(a, b)
+    # and each shot matches the oracle
+    for s in (1, 3):
+        q = W.cfg2(nx=120, nz=80, npml=10, nsteps=250, nshots=5, nrec=12)
+        q.shots = [q.shots[s]]
+        orc, _, _ = H.run_eiso_oracle(q)
+        assert H.rel_l2([1e3 * g for g in batch[s]], orc) < TOL["fp32"]
+
+
+def test_every_source_type_and_edge_positions():
+    p = W.cfg0(nx=48, nz=56, npml=5, nsteps=220, nrec=4)
+    p.shots = [[("Sx", 1.0, 80.0, 0.0, 0.0), ("Sz", 2.0, 80.0, 47.0, 55.0),
+                ("Sxz", 0.7, 80.0, 10.0, 55.0), ("Bulk", 1.3, 80.0, 47.0, 0.0)]]
+    p.receivers = [("Vx", 0.0, 0.0, 0.0, p.dt_ms), ("Vz", 47.0, 55.0, 0.0, p.dt_ms),
+                   ("txx", 20.0, 20.0, 0.0, p.dt_ms), ("Vx", 47.0, 0.0, 0.0, 2 * p.dt_ms)]
+    got = api.run_eiso(p, "fp64")[0]
+    orc, _, _ = H.run_eiso_oracle(p)
+    assert H.rel_l2([1e3 * g for g in got], orc) < TOL["fp64"]
+    got32 = api.run_eiso(p, "fp32")[0]
+    assert H.rel_l2([1e3 * g for g in got32], orc) < TOL["fp32"]
+
+
+def test_reset_reproduces_run_and_step_count():
+    p = W.cfg0(nx=40, nz=40, npml=6, nsteps=120, nrec=3)
+    dev, n = api.eiso_device(p, "fp32")
+    dev.run(n)
+    a = dev.traces(0)
+    dev.reset()
+    dev.run(n // 2)
+    dev.run(n - n // 2)
+    b = dev.traces(0)
+    for x, y in zip(a, b):
+        np.testing.assert_array_equal(x, y)
+    dev.close()
