@@ -1,0 +1,396 @@
+#!/usr/bin/env python
+"""Benchmark of the seismod FDTD hot path on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--workload a3d|a3d512|eiso|eiso1] [--precision fp32|fp16|bf16|fp64]
+
+A "step" is one FDTD time step of the whole workload (velocity + pressure /
+stress update, CPML/PML memory variables, source injection, receiver
+sampling).  Default workload: the 256^3 a_iso_3d shot (+2x16 CPML = 288^3,
+FP32, 16,384 surface receivers).  Inputs (wavefields, materials) stay
+resident in HBM; the state (~0.4 GB in FP32) is larger than the 126 MB L2,
+so no flush is needed between timed steps.
+
+Prints ONE JSON line (rank 0).  N > 1 (torchrun): every rank runs its own
+shot (replicas, no collective in the data path); the time is the max over
+ranks; value = all ranks' cell-updates / that time.
+
+--impl reference times the reference's own CPU program (oracle/_ref, built
+from its sources) on the host cores for a bounded number of steps of the
+same workload.
+"""
+from __future__ import annotations
+
+import argparse
+import dataclasses
+import json
+import math
+import os
+import resource
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = ("shots/s & Gcell/s, batched+FP16 vs plain FP32 (trace err≤1e-3); "
+          "HBM %peak; p50/p99")
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            m = json.load(f)
+        return float(m["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+# ----------------------------------------------------------------------------
+# clocks sampled during the timed region
+# ----------------------------------------------------------------------------
+
+class Clocks:
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu):
+        self.gpu = gpu
+        self.rows = []
+        self.p = None
+
+    def __enter__(self):
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.Q}",
+                                       "--format=csv,noheader,nounits", "-lms", "100"],
+                                      stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.p = None
+        return self
+
+    def _read(self):
+        for line in self.p.stdout:
+            self.rows.append([c.strip() for c in line.split(",")])
+
+    def __exit__(self, *a):
+        if self.p:
+            time.sleep(0.25)
+            self.p.terminate()
+            try:
+                self.p.wait(timeout=5)
+            except Exception:
+                self.p.kill()
+
+    def summary(self):
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in self.rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({n for r in self.rows for n, v in zip(names, r[5:9]) if v == "Active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(mx) if mx else None, "reasons": reasons,
+                "samples": len(self.rows)}
+
+
+# ----------------------------------------------------------------------------
+# workloads and algorithmic bytes
+# ----------------------------------------------------------------------------
+
+def a3d_bytes_per_step(p, s, m=4, psi=None):
+    """Ncell (8 s + 2 m) + sum over axes of N_slab 4 p (state R+W, rho & K read
+    once, both CPML memory variables R+W on their slabs)."""
+    psi = s if psi is None else psi
+    n2 = [n + 2 * p.npml for n in p.shape]
+    ncell = n2[0] * n2[1] * n2[2]
+    slab = sum(2 * p.npml * (ncell // n2[a]) for a in range(3))
+    return ncell * (8 * s + 2 * m) + slab * 4 * psi
+
+
+def eiso_bytes_per_step(p, nshots, s, m=4):
+    """shots (N_int 10 s + N_pml 20 s) + N_all 3 m."""
+    nall = p.cells
+    nint = p.nx * p.nz
+    return nshots * (nint * 10 * s + (nall - nint) * 20 * s) + nall * 3 * m
+
+
+def make_workload(name):
+    from seismod_b200 import workloads as W
+    if name == "a3d":
+        return "a3d", W.cfg1(), "a_iso_3d 256^3 (+2x16 CPML = 288^3), dx 5 m, 1000-step shot"
+    if name == "a3d512":
+        return "a3d", W.cfg3(), "a_iso_3d 512^3 (+2x16 CPML = 544^3), dx 5 m, 2000-step shot"
+    if name == "eiso":
+        return ("eiso", W.cfg2(),
+                "e_iso 1000x500 (+2x20 PML), 64 shots batched, 2000-step shots")
+    if name == "eiso1":
+        return "eiso", W.cfg0(), "e_iso 400x400 (+2x20 PML), single shot, 1500-step shot"
+    raise SystemExit(f"unknown workload {name}")
+
+
+# ----------------------------------------------------------------------------
+# our arm
+# ----------------------------------------------------------------------------
+
+def trace_err(a, b):
+    a = np.concatenate([np.ravel(x) for x in a])
+    b = np.concatenate([np.ravel(x) for x in b])
+    return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))
+
+
+def device_for(kind, p, precision, dev_id):
+    from seismod_b200 import api
+    if kind == "a3d":
+        return api.a3d_device(p, precision, dev_id)
+    return api.eiso_device(p, precision, None, dev_id)
+
+
+def time_steps(dev, K, torch):
+    ext = torch.cuda.ExternalStream(dev.stream())
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    dev.sync()
+    e0.record(ext)
+    dev.run(K)
+    e1.record(ext)
+    e1.synchronize()
+    return e0.elapsed_time(e1)
+
+
+def run_ours(args, rank, world, local_rank, torch, dist):
+    from seismod_b200 import api
+    kind, p, desc = make_workload(args.workload)
+    prec = args.precision
+    sbytes = {"fp32": 4, "fp64": 8, "fp16": 2, "bf16": 2}[prec]
+    mbytes = 8 if prec == "fp64" else 4
+    nshots = len(p.shots) if kind == "eiso" else 1
+    if kind == "a3d":
+        bps = a3d_bytes_per_step(p, sbytes, mbytes)
+        cells = p.cells
+    else:
+        bps = eiso_bytes_per_step(p, nshots, sbytes, mbytes)
+        cells = p.cells * nshots
+    dev, nsteps_shot = device_for(kind, p, prec, local_rank)
+    K, Wm = args.steps, args.warmup
+    dev.run(Wm)
+    dev.sync()
+    dev.kernel_stats(reset=True)
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    with Clocks(local_rank) as clk:
+        ms = time_steps(dev, K, torch)
+    _, _, launches = dev.kernel_stats(reset=True)
+    if world > 1:
+        t = torch.tensor([ms], device=f"cuda:{local_rank}")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    # dominant-kernel duration: separate pass with per-launch events
+    dev.set_timing(True)
+    Kr = min(K, 400)
+    dev.run(Kr)
+    upd_ms, upd_n, _ = dev.kernel_stats(reset=True)
+    dev.set_timing(False)
+    dev.close()
+    total_cells = cells * K * world
+    value = total_cells / (ms * 1e-3) / 1e9
+    hbm, how = peaks()
+    achieved = bps / (upd_ms / upd_n * 1e-3) / 1e9
+    out = {
+        "metric": METRIC, "value": round(value, 3), "unit": "Gcell/s",
+        "n_gpus": world, "steps": K, "warmup": Wm, "ms_per_step": round(ms / K, 5),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64" if prec == "fp64" else "f32",
+        "data": "synthetic (seeded generator of the named configuration; no dataset exists)",
+        "config": {"workload": desc, "precision": f"{prec} storage",
+                   "cells_per_shot": p.cells, "shots": nshots * world,
+                   "parallelism": f"replicas x{world} (shot-parallel, no collective)",
+                   "l2": "inputs larger than L2 (state %.0f MB)" % (bps / 1e6)},
+        "shots_per_s": round(nshots * world / (ms / K * 1e-3 * nsteps_shot), 3),
+        "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": hbm,
+                     "unit": "GB/s", "frac": round(achieved / hbm, 4), "traffic": None,
+                     "peak_source": how, "algorithmic_bytes_per_step": bps,
+                     "kernel": "wavefield update (velocity + stress/pressure, PML/CPML)"},
+        "gpu_launches": int(launches),
+        "clocks": clk.summary(),
+    }
+    return out, kind, p, desc, cells
+
+
+def precision_side(kind, p, local_rank, K):
+    """Throughput of the other storage precisions and every trace error
+    against an FP64 device run of the whole shot."""
+    from seismod_b200 import api
+    import torch
+    run = api.run_a3d if kind == "a3d" else (lambda q, pr, d: api.run_eiso(q, pr, [0], d)[0])
+    ref64 = run(p, "fp64", local_rank)
+    res = {}
+    for prec in ("fp32", "fp16", "bf16"):
+        try:
+            tr = run(p, prec, local_rank)
+            err = trace_err(tr, ref64)
+            dev, _ = device_for(kind, p, prec, local_rank)
+            dev.run(10)
+            ms = time_steps(dev, min(K, 500), torch)
+            dev.close()
+            res[prec] = {"trace_err_vs_fp64": err, "ms_per_step": round(ms / min(K, 500), 5)}
+        except Exception as e:  # report, do not hide
+            res[prec] = {"error": str(e)[:200]}
+    return res
+
+
+def e2e(kind, p, K, local_rank):
+    """Whole user call through the public API from host arrays: set-up and
+    upload, K steps, traces back to the host, teardown."""
+    from seismod_b200 import api
+    t0 = time.perf_counter()
+    dev, _ = device_for(kind, p, "fp32", local_rank)
+    dev.run(K)
+    if kind == "a3d":
+        tr = dev.traces_array()
+        d2h = tr.size * 8
+    else:
+        tr = [dev.traces(s) for s in range(dev.nshots)]
+        d2h = sum(sum(len(x) for x in t) for t in tr) * 8
+    dev.close()
+    wall = time.perf_counter() - t0
+    if kind == "a3d":
+        n2 = [n + 2 * p.npml for n in p.shape]
+        pitch = math.ceil(n2[2] / 32) * 32
+        h2d = 2 * n2[0] * n2[1] * pitch * 4
+        cells = p.cells
+    else:
+        pitch = math.ceil((p.nz + 2 * p.npml) / 32) * 32
+        h2d = 5 * (p.nx + 2 * p.npml) * pitch * 4
+        cells = p.cells * len(p.shots)
+    return {"value": round(cells * K / wall / 1e9, 3), "unit": "Gcell/s",
+            "h2d_bytes_per_step": int(h2d / K), "d2h_bytes_per_step": int(d2h / K),
+            "wall_s": round(wall, 3)}
+
+
+# ----------------------------------------------------------------------------
+# the reference on the host cores
+# ----------------------------------------------------------------------------
+
+def _raise_nofile():
+    soft, hard = resource.getrlimit(resource.RLIMIT_NOFILE)
+    try:
+        resource.setrlimit(resource.RLIMIT_NOFILE, (hard, hard))
+    except Exception:
+        pass
+    return resource.getrlimit(resource.RLIMIT_NOFILE)[0]
+
+
+def reference_rate(kind, p, steps):
+    """Gcell/s of the reference program over `steps` steps of p (time of a
+    (2 + steps)-step run minus a 2-step run, same inputs).  The model is
+    written as a 1-D profile file (the reference's own shortcut) so parsing
+    stays short; the arithmetic per step does not depend on the values."""
+    from oracle import oracle as O
+    from seismod_b200 import workloads as W
+    if not O.ref_available():
+        return None, "reference build absent (oracle/_ref)"
+    nofile = _raise_nofile()
+    d = tempfile.mkdtemp(prefix="refbench_")
+    q = p
+    nrec = len(p.receivers)
+    if nrec + 64 > nofile:  # the reference keeps one open file per trace
+        q = dataclasses.replace(p, receivers=p.receivers[: max(nofile - 64, 1)])
+    prog = "a_iso_3d" if kind == "a3d" else ("e_iso" if p.nx <= p.nz else "e_iso_lrfix")
+    times = []
+    for n in (2, 2 + steps):
+        r = dataclasses.replace(q, duration=W.steps_duration(n, q.dt_ms))
+        if kind == "a3d":
+            par = r.write(os.path.join(d, f"n{n}"), profile_1d=True)
+        else:
+            par = r.write(os.path.join(d, f"n{n}"), shot=0, profile_1d=True)
+        times.append(O.run_reference(prog, par, os.path.dirname(par), timeout=3600))
+    dt = (times[1] - times[0]) / steps
+    cells = p.cells
+    sample = (f"{prog} (oracle/_ref, gcc -O3, OpenMP, 3 threads as hard-coded), "
+              f"{steps} steps of the full grid, {len(q.receivers)} receivers, "
+              f"1-D profile model file; time(2+{steps} steps) - time(2 steps)")
+    return cells / dt / 1e9, sample
+
+
+def run_reference_arm(args, rank, world):
+    if rank != 0:
+        return None
+    kind, p, desc = make_workload(args.workload)
+    steps = max(1, min(args.steps, 12 if kind == "a3d" else 200))
+    rate, sample = reference_rate(kind, p, steps)
+    if rate is None:
+        return {"impl": "reference", "unavailable": sample}
+    return {"impl": "reference", "metric": METRIC, "value": round(rate, 4), "unit": "Gcell/s",
+            "n_gpus": world, "steps": steps, "warmup": args.warmup,
+            "ms_per_step": round(p.cells / (rate * 1e9) * 1e3, 3),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic", "config": {"workload": desc},
+            "cpu_baseline": {"value": round(rate, 4), "unit": "Gcell/s", "cores": 3,
+                             "kind": "reference", "sample": sample},
+            "e2e": {"value": round(rate, 4), "unit": "Gcell/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+
+
+# ----------------------------------------------------------------------------
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=1000)
+    ap.add_argument("--warmup", type=int, default=20)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="a3d", choices=["a3d", "a3d512", "eiso", "eiso1"])
+    ap.add_argument("--precision", default="fp32", choices=["fp32", "fp64", "fp16", "bf16"])
+    ap.add_argument("--no-side", action="store_true", help="skip precision / CPU side runs")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+
+    if args.impl == "reference":
+        out = run_reference_arm(args, rank, world)
+        if out is not None:
+            print(json.dumps(out), flush=True)
+        return 0
+
+    import torch
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        torch.cuda.set_device(local_rank)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    out, kind, p, desc, cells = run_ours(args, rank, world, local_rank, torch, dist)
+    if rank == 0 and not args.no_side:
+        out["precisions"] = precision_side(kind, p, local_rank, args.steps)
+        out["e2e"] = e2e(kind, p, args.steps, local_rank)
+        steps = 12 if kind == "a3d" else 200
+        rate, sample = reference_rate(kind, p, steps)
+        if rate is not None:
+            out["cpu_baseline"] = {"value": round(rate, 4), "unit": "Gcell/s", "cores": 3,
+                                   "kind": "reference", "sample": sample}
+        else:
+            out["cpu_baseline"] = {"value": None, "unit": "Gcell/s", "cores": 0,
+                                   "kind": "reference", "sample": sample}
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(out), flush=True)
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -175,6 +175,16 @@ int sm_eiso_set_field(sm_eiso_t h, size_t shot, int comp, int part, const double
 /* zero all wavefields and counters of every shot (e_iso.c:565-572) */
 int sm_eiso_reset(sm_eiso_t h);
 int sm_eiso_destroy(sm_eiso_t h);
+/* the cudaStream_t the handle launches on (for timing with CUDA events) */
+int sm_eiso_stream(sm_eiso_t h, void **stream);
+/* Per-kernel timing.  With timing on, every launch of the wavefield update
+ * kernel(s) is bracketed by CUDA events on the handle's stream;
+ * sm_eiso_kernel_stats synchronises and returns their summed duration and
+ * launch count since the last reset, plus the number of kernels of every
+ * kind launched (update, sources, receivers). */
+int sm_eiso_set_timing(sm_eiso_t h, int on);
+int sm_eiso_kernel_stats(sm_eiso_t h, int reset, double *update_ms, size_t *update_launches,
+                         size_t *all_launches);
 
 /* ======================================================================
  * a_iso_3d on the device
@@ -208,6 +218,16 @@ int sm_a3d_get_field(sm_a3d_t h, int comp, double *out);
 int sm_a3d_set_field(sm_a3d_t h, int comp, const double *in);
 int sm_a3d_reset(sm_a3d_t h);
 int sm_a3d_destroy(sm_a3d_t h);
+int sm_a3d_stream(sm_a3d_t h, void **stream);
+/* launch configuration of the fused step kernel (tile rows, pipeline
+ * depth): index in [0, nconfigs).  Results do not depend on it. */
+int sm_a3d_set_config(sm_a3d_t h, int config);
+/* x planes each CTA marches through (<= 0: the library's choice) */
+int sm_a3d_set_chunk(sm_a3d_t h, int chunk);
+int sm_a3d_get_config(sm_a3d_t h, int *config, int *nconfigs);
+int sm_a3d_set_timing(sm_a3d_t h, int on);
+int sm_a3d_kernel_stats(sm_a3d_t h, int reset, double *update_ms, size_t *update_launches,
+                        size_t *all_launches);
 
 /* ======================================================================
  * drop-in programs: the whole of e_iso / a_iso_3d main() on the device,

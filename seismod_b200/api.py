@@ -172,6 +172,23 @@ class EIsoDevice:
     def reset(self):
         L.check(L.load().sm_eiso_reset(self._h))
 
+    def stream(self):
+        p = C.c_void_p()
+        L.check(L.load().sm_eiso_stream(self._h, C.byref(p)))
+        return p.value
+
+    def set_timing(self, on=True):
+        L.check(L.load().sm_eiso_set_timing(self._h, 1 if on else 0))
+
+    def kernel_stats(self, reset=False):
+        """(summed update-kernel ms, timed launches, all kernel launches)."""
+        ms = C.c_double()
+        n = C.c_size_t()
+        a = C.c_size_t()
+        L.check(L.load().sm_eiso_kernel_stats(self._h, 1 if reset else 0, C.byref(ms),
+                                              C.byref(n), C.byref(a)))
+        return ms.value, n.value, a.value
+
 
 class A3DDevice:
     """An a_iso_3d state on the GPU."""
@@ -241,6 +258,17 @@ class A3DDevice:
             L.check(L.load().sm_a3d_read_traces(self._h, 0, n, L.dptr(out), ld, L.szptr(counts)))
         return out
 
+    def set_config(self, config):
+        L.check(L.load().sm_a3d_set_config(self._h, int(config)))
+
+    def set_chunk(self, chunk):
+        L.check(L.load().sm_a3d_set_chunk(self._h, int(chunk)))
+
+    def get_config(self):
+        c, n = C.c_int(), C.c_int()
+        L.check(L.load().sm_a3d_get_config(self._h, C.byref(c), C.byref(n)))
+        return c.value, n.value
+
     def get_field(self, comp):
         out = np.zeros(self.shape)
         L.check(L.load().sm_a3d_get_field(self._h, L.SM_COMP[comp], L.dptr(out)))
@@ -251,6 +279,23 @@ class A3DDevice:
 
     def reset(self):
         L.check(L.load().sm_a3d_reset(self._h))
+
+    def stream(self):
+        p = C.c_void_p()
+        L.check(L.load().sm_a3d_stream(self._h, C.byref(p)))
+        return p.value
+
+    def set_timing(self, on=True):
+        L.check(L.load().sm_a3d_set_timing(self._h, 1 if on else 0))
+
+    def kernel_stats(self, reset=False):
+        """(summed update-kernel ms, timed launches, all kernel launches)."""
+        ms = C.c_double()
+        n = C.c_size_t()
+        a = C.c_size_t()
+        L.check(L.load().sm_a3d_kernel_stats(self._h, 1 if reset else 0, C.byref(ms),
+                                              C.byref(n), C.byref(a)))
+        return ms.value, n.value, a.value
 
 
 # ----------------------------------------------------------------------------

@@ -26,6 +26,11 @@
 
 namespace sm {
 
+// mbarriers reserved at the head of the step kernel's shared memory
+#define D_HEAD_BARS 16
+// most x planes one CTA marches through
+#define A3_CHMAX 64
+
 enum { A_VX = 0, A_VY = 1, A_VZ = 2, A_P = 3 };
 enum { PS_PX = 0, PS_PY = 1, PS_PZ = 2, PS_VX = 3, PS_VY = 4, PS_VZ = 5 };
 
@@ -45,9 +50,13 @@ struct A3Coef {
 
 struct A3Args {
     int nx2, ny2, nz2, pitch, np;
-    long long sx, sy;          // strides of i and j in elements
-    void *f[4];
-    void *psi[6];
+    int sx, sy;                // strides of i and j in elements (grids < 2^31 cells)
+    int *err;                  // set by a kernel whose bounded wait gave up
+    void *f[4];                // wavefields read this step
+    void *psi[6];              // CPML memory variables read this step
+    void *fo[4];               // ... and written this step (the other buffer)
+    void *pso[6];
+    int chunk;                 // x planes per CTA
     const void *rho;           // compute type, padded layout
     const void *K;
     const void *coef;
@@ -70,117 +79,412 @@ __device__ __forceinline__ int node_slab(int n, int n2, int np) {
     return -1;
 }
 
-template <typename S>
-__global__ void __launch_bounds__(256) a3d_velocity_kernel(A3Args a) {
+// Shared-memory stage of the fused step: one x plane of every input the
+// step reads, delivered by six TMA box loads.  P and rho carry a one-cell
+// halo in j (rows j0-1 .. j0+TY) and the 16-byte chunks around the tile in
+// k (elements k0-H .. k0+32+H, H = 16 bytes / element size); vy starts at
+// row j0-1 and vz at column k0-H, which hold the recomputed halo cells.
+template <typename S, int TY>
+struct A3Lay {
+    using C = typename Store<S>::C;
+    static constexpr int HS = 16 / (int)sizeof(S), HC = 16 / (int)sizeof(C);
+    static constexpr int WS = 32 + 2 * HS, WC = 32 + 2 * HC, WZ = 32 + HS;
+    __host__ __device__ static constexpr size_t al(size_t x) { return (x + 127) / 128 * 128; }
+    static constexpr size_t bP = (size_t)(TY + 2) * WS * sizeof(S);
+    static constexpr size_t bR = (size_t)(TY + 2) * WC * sizeof(C);
+    static constexpr size_t bX = (size_t)TY * 32 * sizeof(S);
+    static constexpr size_t bY = (size_t)(TY + 1) * 32 * sizeof(S);
+    static constexpr size_t bZ = (size_t)TY * WZ * sizeof(S);
+    static constexpr size_t bK = (size_t)TY * 32 * sizeof(C);
+    static constexpr size_t oP = 0, oR = al(bP), oX = oR + al(bR), oY = oX + al(bX);
+    static constexpr size_t oZ = oY + al(bY), oK = oZ + al(bZ);
+    static constexpr size_t stage = oK + al(bK);
+    static constexpr unsigned tx = (unsigned)(bP + bR + bX + bY + bZ + bK);
+    // head: the stage mbarriers, two vy row buffers [TY+1][32], and the
+    // CPML coefficient tables of the chunk's planes, the tile's rows and columns
+    static constexpr size_t oVY = al(D_HEAD_BARS * 8);
+    static constexpr size_t oCX = oVY + al((size_t)2 * (TY + 1) * 32 * sizeof(C));
+    static constexpr size_t oCY = oCX + al((size_t)6 * (A3_CHMAX + 2) * sizeof(C));
+    static constexpr size_t oCZ = oCY + al((size_t)6 * (TY + 1) * sizeof(C));
+    static constexpr size_t head = oCZ + al((size_t)6 * 33 * sizeof(C));
+};
+
+// one velocity component (a_iso_3d.c:605-651):
+//   g = (P_hi - P_lo)/h;  psi = b psi + a g;  g = g/k + psi (frame only);
+//   v -= 2 dt/(rho_lo + rho_hi) g
+// The owner of a cell and a tile that recomputes it as halo call this same
+// function, so both round identically.
+template <typename C>
+__device__ __forceinline__ C a3_vel(C vold, C p_lo, C p_hi, C r_lo, C r_hi, C ih, C two_dt,
+                                    bool frame, C ca, C cb, C cik, C psi_old, C &psi_new) {
+    C g = r_mul(r_sub(p_hi, p_lo), ih);
+    if (frame) {
+        psi_new = r_fma(cb, psi_old, r_mul(ca, g));
+        g = r_fma(g, cik, psi_new);
+    }
+    return r_fma(-r_quot(two_dt, r_add(r_lo, r_hi)), g, vold);
+}
+
+// the same update outside the frame (psi = 0, k = 1): identical rounding to
+// a3_vel with frame = false
+template <typename C>
+__device__ __forceinline__ C a3_vel0(C vold, C p_lo, C p_hi, C r_lo, C r_hi, C ih, C two_dt) {
+    const C g = r_mul(r_sub(p_hi, p_lo), ih);
+    return r_fma(-r_quot(two_dt, r_add(r_lo, r_hi)), g, vold);
+}
+
+// the frame correction of one pressure derivative (a_iso_3d.c:667-676)
+template <typename C>
+__device__ __forceinline__ C a3_dv(C g, C ca, C cb, C cik, C psi_old, C &psi_new) {
+    psi_new = r_fma(cb, psi_old, r_mul(ca, g));
+    return r_fma(g, cik, psi_new);
+}
+
+struct A3Maps {
+    CUtensorMap P, vx, vy, vz, rho, K;
+};
+
+// One time step, fused (a_iso_3d.c:599-684).  A CTA of W warps owns a
+// 32 (k) x TY (j) column tile, TY = W*R (each warp R consecutive rows), and
+// marches along x over planes [i0, i1), i1 - i0 <= A3_CHMAX:
+//   * thread 0 keeps a D-stage ring of shared-memory planes filled by TMA
+//     (D-2 planes ahead); each stage completes on its own mbarrier;
+//   * iteration i computes the velocities of plane i (vx needs P and rho of
+//     plane i+1, already in the ring) and the pressure of plane i-1, whose
+//     velocities were computed one iteration earlier: vx and vz stay in
+//     registers, vy is kept in a shared row buffer (double-buffered by plane
+//     parity), so one __syncthreads per plane suffices;
+//   * vy on row j0-1 and vz on column k0-1 are recomputed from old values
+//     (owned by the neighbouring tiles, which write them to the other
+//     buffer, so nothing races): the row by warp 0, the column by lanes
+//     0..R-1 of every warp, one row each;
+//   * inside the CPML frame the memory variables of the next plane are
+//     loaded one iteration ahead, and the coefficients of the tile's planes,
+//     rows and columns sit in shared memory, so no global load waits in the
+//     loop; tiles and planes clear of the frame take a lean path.
+// Old and new wavefields and CPML memory variables live in separate buffers
+// (ping-pong): every stored value is read once and written once per step.
+template <typename S, int W, int R, int D, int MINB>
+__global__ void __launch_bounds__(32 * W, MINB)
+    a3d_step_kernel(const A3Args a, const __grid_constant__ A3Maps m) {
+    constexpr int TY = W * R;
     using C = typename Store<S>::C;
     using St = Store<S>;
-    const int k = blockIdx.x * blockDim.x + threadIdx.x;
-    const int j = blockIdx.y * blockDim.y + threadIdx.y;
-    const int i = blockIdx.z;
-    if (k >= a.nz2 || j >= a.ny2) return;
-    const long long q = (long long)i * a.sx + (long long)j * a.sy + k;
-    const S *P = static_cast<const S *>(a.f[A_P]);
+    using L = A3Lay<S, TY>;
+    static_assert(D >= 4 && D <= D_HEAD_BARS, "ring depth");
+    static_assert(R <= 32, "rows per warp");
+    constexpr int HS = L::HS, HC = L::HC, WS = L::WS, WC = L::WC, WZ = L::WZ;
+    constexpr int NXT = A3_CHMAX + 2;   // coefficient table: planes i0-1 .. i1
+    extern __shared__ __align__(128) unsigned char smem[];
+    uint64_t *bars = reinterpret_cast<uint64_t *>(smem);
+    C(*VYs)[TY + 1][32] = reinterpret_cast<C(*)[TY + 1][32]>(smem + L::oVY);
+    C(*CX)[NXT] = reinterpret_cast<C(*)[NXT]>(smem + L::oCX);     // [6][NXT]
+    C(*CY)[TY + 1] = reinterpret_cast<C(*)[TY + 1]>(smem + L::oCY);  // [6][TY+1]
+    C(*CZ)[33] = reinterpret_cast<C(*)[33]>(smem + L::oCZ);          // [6][33]
+    unsigned char *ring = smem + L::head;
+
+    const int lane = threadIdx.x, w = threadIdx.y;
+    const int tid = w * 32 + lane;
+    const int k0 = blockIdx.x * 32, j0 = blockIdx.y * TY;
+    const int k = k0 + lane;
+    const int i0 = blockIdx.z * a.chunk;
+    const int i1 = min(i0 + a.chunk, a.nx2);
+    const int nx2 = a.nx2, ny2 = a.ny2, nz2 = a.nz2, np = a.np, pitch = a.pitch;
+    const int sx = a.sx, sy = a.sy;   // element strides (all indices fit 31 bits)
+    const bool kin = k < nz2;
+    const S *Pin = static_cast<const S *>(a.f[A_P]);
+    const S *Vxin = static_cast<const S *>(a.f[A_VX]);
+    S *Pout = static_cast<S *>(a.fo[A_P]);
+    S *Vxout = static_cast<S *>(a.fo[A_VX]);
+    S *Vyout = static_cast<S *>(a.fo[A_VY]);
+    S *Vzout = static_cast<S *>(a.fo[A_VZ]);
     const C *rho = static_cast<const C *>(a.rho);
     const C *cf = static_cast<const C *>(a.coef);
-    const C p = St::ld(P + q, a.isc[A_P]);
-    const C r = rho[q];
     const C two_dt = static_cast<C>(a.two_dt);
-    const int np = a.np;
-    // vx, a_iso_3d.c:605-617 (i < nx2-1)
-    if (i < a.nx2 - 1) {
-        C g = (St::ld(P + q + a.sx, a.isc[A_P]) - p) * static_cast<C>(a.idx);
-        const int s = half_slab(i, a.nx2, np);
-        if (s >= 0) {
-            S *m = static_cast<S *>(a.psi[PS_PX]);
-            const long long c = ((long long)s * a.ny2 + j) * a.pitch + k;
-            const C mm = cf[a.cf.at(0, 4) + i] * St::ld(m + c, a.pisc[PS_PX]) +
-                         cf[a.cf.at(0, 3) + i] * g;
-            St::st(m + c, mm, a.psc[PS_PX]);
-            g = g * cf[a.cf.at(0, 5) + i] + mm;
-        }
-        S *v = static_cast<S *>(a.f[A_VX]);
-        const C ir = two_dt / (r + rho[q + a.sx]);
-        St::st(v + q, St::ld(v + q, a.isc[A_VX]) - ir * g, a.sc[A_VX]);
+    const C idx = static_cast<C>(a.idx), idy = static_cast<C>(a.idy), idz = static_cast<C>(a.idz);
+    const float isP = a.isc[A_P], isX = a.isc[A_VX], isY = a.isc[A_VY], isZ = a.isc[A_VZ];
+    const S *psPx = static_cast<const S *>(a.psi[PS_PX]);
+    const S *psPy = static_cast<const S *>(a.psi[PS_PY]);
+    const S *psPz = static_cast<const S *>(a.psi[PS_PZ]);
+    const S *psVx = static_cast<const S *>(a.psi[PS_VX]);
+    const S *psVy = static_cast<const S *>(a.psi[PS_VY]);
+    const S *psVz = static_cast<const S *>(a.psi[PS_VZ]);
+    S *poPx = static_cast<S *>(a.pso[PS_PX]);
+    S *poPy = static_cast<S *>(a.pso[PS_PY]);
+    S *poPz = static_cast<S *>(a.pso[PS_PZ]);
+    S *poVx = static_cast<S *>(a.pso[PS_VX]);
+    S *poVy = static_cast<S *>(a.pso[PS_VY]);
+    S *poVz = static_cast<S *>(a.pso[PS_VZ]);
+
+    // coefficient tables: rows 0..2 half node (a, b, 1/k), 3..5 node
+    for (int t = tid; t < 6 * NXT; t += 32 * W) {
+        const int wch = t / NXT, e = t % NXT, p = i0 - 1 + e;
+        const bool half = wch < 3;
+        const bool ok = p >= 0 && p < (half ? nx2 - 1 : nx2);
+        CX[wch][e] = ok ? cf[a.cf.at(0, half ? 3 + wch : wch - 3) + p] : C(wch % 3 == 0 ? 0 : 1);
     }
-    // vy, :620-634 (j < ny2-1)
-    if (j < a.ny2 - 1) {
-        C g = (St::ld(P + q + a.sy, a.isc[A_P]) - p) * static_cast<C>(a.idy);
-        const int s = half_slab(j, a.ny2, np);
-        if (s >= 0) {
-            S *m = static_cast<S *>(a.psi[PS_PY]);
-            const long long c = ((long long)i * 2 * np + s) * a.pitch + k;
-            const C mm = cf[a.cf.at(1, 4) + j] * St::ld(m + c, a.pisc[PS_PY]) +
-                         cf[a.cf.at(1, 3) + j] * g;
-            St::st(m + c, mm, a.psc[PS_PY]);
-            g = g * cf[a.cf.at(1, 5) + j] + mm;
-        }
-        S *v = static_cast<S *>(a.f[A_VY]);
-        const C ir = two_dt / (r + rho[q + a.sy]);
-        St::st(v + q, St::ld(v + q, a.isc[A_VY]) - ir * g, a.sc[A_VY]);
+    for (int t = tid; t < 6 * (TY + 1); t += 32 * W) {
+        const int wch = t / (TY + 1), e = t % (TY + 1), p = j0 - 1 + e;
+        const bool half = wch < 3;
+        const bool ok = p >= 0 && p < (half ? ny2 - 1 : ny2);
+        CY[wch][e] = ok ? cf[a.cf.at(1, half ? 3 + wch : wch - 3) + p] : C(wch % 3 == 0 ? 0 : 1);
     }
-    // vz, :637-651 (k < nz2-1)
-    if (k < a.nz2 - 1) {
-        C g = (St::ld(P + q + 1, a.isc[A_P]) - p) * static_cast<C>(a.idz);
-        const int s = half_slab(k, a.nz2, np);
-        if (s >= 0) {
-            S *m = static_cast<S *>(a.psi[PS_PZ]);
-            const long long c = ((long long)i * a.ny2 + j) * 2 * np + s;
-            const C mm = cf[a.cf.at(2, 4) + k] * St::ld(m + c, a.pisc[PS_PZ]) +
-                         cf[a.cf.at(2, 3) + k] * g;
-            St::st(m + c, mm, a.psc[PS_PZ]);
-            g = g * cf[a.cf.at(2, 5) + k] + mm;
+    for (int t = tid; t < 6 * 33; t += 32 * W) {
+        const int wch = t / 33, e = t % 33, p = k0 - 1 + e;
+        const bool half = wch < 3;
+        const bool ok = p >= 0 && p < (half ? nz2 - 1 : nz2);
+        CZ[wch][e] = ok ? cf[a.cf.at(2, half ? 3 + wch : wch - 3) + p] : C(wch % 3 == 0 ? 0 : 1);
+    }
+    if (tid == 0) {
+        for (int d = 0; d < D; ++d) mbar_init(&bars[d], 1);
+        fence_proxy_async();
+    }
+
+    // ring of planes i0 .. min(i1, nx2-1), local index l = plane - i0
+    const int nload = min(i1 + 1, nx2) - i0;
+    auto issue = [&](int l) {   // thread 0 only
+        if (l >= nload) return;
+        unsigned char *b = ring + (size_t)(l % D) * L::stage;
+        uint64_t *bar = &bars[l % D];
+        const int ip = i0 + l;
+        fence_proxy_async();
+        mbar_expect_tx(bar, L::tx);
+        tma_load_3d(b + L::oP, &m.P, k0 - HS, j0 - 1, ip, bar);
+        tma_load_3d(b + L::oR, &m.rho, k0 - HC, j0 - 1, ip, bar);
+        tma_load_3d(b + L::oX, &m.vx, k0, j0, ip, bar);
+        tma_load_3d(b + L::oY, &m.vy, k0, j0 - 1, ip, bar);
+        tma_load_3d(b + L::oZ, &m.vz, k0 - HS, j0, ip, bar);
+        tma_load_3d(b + L::oK, &m.K, k0, j0, ip, bar);
+    };
+    __syncthreads();   // barriers initialised, tables filled
+    if (tid == 0)
+        for (int l = 0; l < D - 2; ++l) issue(l);
+
+    // per-row / per-column frame membership (fixed over the march)
+    int jh[R], jn[R], joff[R];
+    bool rin[R];
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+        const int j = j0 + w * R + r;
+        rin[r] = kin && j < ny2;
+        jh[r] = j < ny2 ? half_slab(j, ny2, np) : -1;
+        jn[r] = j < ny2 ? node_slab(j, ny2, np) : -1;
+        joff[r] = j * sy + k;
+    }
+    const int kh = kin ? half_slab(k, nz2, np) : -1;
+    const int kn = kin ? node_slab(k, nz2, np) : -1;
+    const int jm = j0 - 1, km = k0 - 1;
+    const int jmh = (jm >= 0) ? half_slab(jm, ny2, np) : -1;
+    const int hrow = w * R + lane;                 // halo-column row of lanes 0..R-1
+    const bool hcol = lane < R && km >= 0 && j0 + hrow < ny2;
+    const int kmh = (km >= 0) ? half_slab(km, nz2, np) : -1;
+    const bool tile_fast = (j0 - 1 >= np) && (j0 + TY - 1 <= ny2 - 2 - np) &&
+                           (k0 - 1 >= np) && (k0 + 31 <= nz2 - 2 - np);
+
+    // memory variables prefetched one plane ahead
+    C fPx[R], fPy[R], fPz[R], fVx[R], fVy[R], fVz[R], fHy = C(0), fHz = C(0);
+    auto load_vpsi = [&](int ip) {   // for the velocities of plane ip
+        const int s = (ip < nx2 - 1) ? half_slab(ip, nx2, np) : -1;
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+            const int j = j0 + w * R + r;
+            fPx[r] = (rin[r] && s >= 0) ? St::ld(psPx + s * sx + joff[r], a.pisc[PS_PX]) : C(0);
+            fPy[r] = (rin[r] && jh[r] >= 0) ? St::ld(psPy + (ip * 2 * np + jh[r]) * pitch + k, a.pisc[PS_PY]) : C(0);
+            fPz[r] = (rin[r] && kh >= 0) ? St::ld(psPz + (ip * ny2 + j) * 2 * np + kh, a.pisc[PS_PZ]) : C(0);
         }
-        S *v = static_cast<S *>(a.f[A_VZ]);
-        const C ir = two_dt / (r + rho[q + 1]);
-        St::st(v + q, St::ld(v + q, a.isc[A_VZ]) - ir * g, a.sc[A_VZ]);
+        fHy = (w == 0 && kin && jmh >= 0) ? St::ld(psPy + (ip * 2 * np + jmh) * pitch + k, a.pisc[PS_PY]) : C(0);
+        fHz = (hcol && kmh >= 0) ? St::ld(psPz + (ip * ny2 + j0 + hrow) * 2 * np + kmh, a.pisc[PS_PZ]) : C(0);
+    };
+    auto load_ppsi = [&](int ip) {   // for the pressure of plane ip
+        const int s = node_slab(ip, nx2, np);
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+            const int j = j0 + w * R + r;
+            fVx[r] = (rin[r] && s >= 0) ? St::ld(psVx + s * sx + joff[r], a.pisc[PS_VX]) : C(0);
+            fVy[r] = (rin[r] && jn[r] >= 0) ? St::ld(psVy + (ip * 2 * np + jn[r]) * pitch + k, a.pisc[PS_VY]) : C(0);
+            fVz[r] = (rin[r] && kn >= 0) ? St::ld(psVz + (ip * ny2 + j) * 2 * np + kn, a.pisc[PS_VZ]) : C(0);
+        }
+    };
+
+    // per-thread state carried between planes, one entry per row
+    C vxa[R], vxb[R], vzp[R], vzhp[R];
+#pragma unroll
+    for (int r = 0; r < R; ++r) { vxa[r] = C(0); vxb[r] = C(0); vzp[r] = C(0); vzhp[r] = C(0); }
+    // vx(i0-1) (direct loads, once per CTA): the pressure of plane i0 needs it
+    if (i0 >= 1) {
+        const int s = half_slab(i0 - 1, nx2, np);
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+            if (!rin[r]) continue;
+            const int qm = (i0 - 1) * sx + joff[r], q0 = qm + sx;
+            C psi_old = C(0), psi_new;
+            if (s >= 0) psi_old = St::ld(psPx + s * sx + joff[r], a.pisc[PS_PX]);
+            vxa[r] = a3_vel<C>(St::ld(Vxin + qm, isX), St::ld(Pin + qm, isP), St::ld(Pin + q0, isP),
+                               rho[qm], rho[q0], idx, two_dt, s >= 0, CX[0][0], CX[1][0], CX[2][0],
+                               psi_old, psi_new);
+        }
+    }
+    load_vpsi(i0);
+
+    // ---- the lagged pressure half step of plane ip (a_iso_3d.c:659-683) ----
+    auto pressure = [&](int ip, int lp, bool fast) {
+        const unsigned char *pb = ring + (size_t)(lp % D) * L::stage;
+        const S *pP = reinterpret_cast<const S *>(pb + L::oP);
+        const C *pK = reinterpret_cast<const C *>(pb + L::oK);
+        const C(*vy)[32] = VYs[ip & 1];
+        const int sxn = node_slab(ip, nx2, np);
+        const int e = ip - (i0 - 1);
+        S *po = Pout + ip * sx;
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+            const int row = w * R + r, j = j0 + row;
+            C vzm = __shfl_up_sync(0xffffffffu, vzp[r], 1);
+            const C hal = __shfl_sync(0xffffffffu, vzhp[r], r);
+            if (lane == 0) vzm = hal;
+            if (!rin[r]) continue;
+            const C p_c = St::ld(pP + (row + 1) * WS + HS + lane, isP);
+            C pn = p_c;
+            if (fast || (ip >= 1 && j >= 1 && k >= 1)) {
+                C gx = r_mul(r_sub(vxa[r], vxb[r]), idx);
+                C gy = r_mul(r_sub(vy[row + 1][lane], vy[row][lane]), idy);
+                C gz = r_mul(r_sub(vzp[r], vzm), idz);
+                if (!fast) {
+                    C psi_new;
+                    if (sxn >= 0) {
+                        gx = a3_dv<C>(gx, CX[3][e], CX[4][e], CX[5][e], fVx[r], psi_new);
+                        St::st(poVx + sxn * sx + joff[r], psi_new, a.psc[PS_VX]);
+                    }
+                    if (jn[r] >= 0) {
+                        gy = a3_dv<C>(gy, CY[3][row + 1], CY[4][row + 1], CY[5][row + 1], fVy[r], psi_new);
+                        St::st(poVy + (ip * 2 * np + jn[r]) * pitch + k, psi_new, a.psc[PS_VY]);
+                    }
+                    if (kn >= 0) {
+                        gz = a3_dv<C>(gz, CZ[3][lane + 1], CZ[4][lane + 1], CZ[5][lane + 1], fVz[r], psi_new);
+                        St::st(poVz + (ip * ny2 + j) * 2 * np + kn, psi_new, a.psc[PS_VZ]);
+                    }
+                }
+                pn = r_fma(-pK[row * 32 + lane], r_add(r_add(gx, gy), gz), p_c);
+            }
+            // written whether updated or not: both buffers always hold a
+            // complete state
+            St::st(po + joff[r], pn, a.sc[A_P]);
+        }
+    };
+
+    for (int i = i0; i < i1; ++i) {
+        const int l = i - i0;
+        if (tid == 0) issue(l + D - 2);
+        if (!mbar_wait(&bars[l % D], (l / D) & 1, a.err, 1)) return;
+        if (i + 1 < nx2 && !mbar_wait(&bars[(l + 1) % D], ((l + 1) / D) & 1, a.err, 1)) return;
+        const unsigned char *cbuf = ring + (size_t)(l % D) * L::stage;
+        const unsigned char *nbuf = ring + (size_t)((l + 1) % D) * L::stage;
+        const S *cP = reinterpret_cast<const S *>(cbuf + L::oP);
+        const C *cR = reinterpret_cast<const C *>(cbuf + L::oR);
+        const S *cX = reinterpret_cast<const S *>(cbuf + L::oX);
+        const S *cY = reinterpret_cast<const S *>(cbuf + L::oY);
+        const S *cZ = reinterpret_cast<const S *>(cbuf + L::oZ);
+        const S *nP = reinterpret_cast<const S *>(nbuf + L::oP);
+        const C *nR = reinterpret_cast<const C *>(nbuf + L::oR);
+        C(*vyw)[32] = VYs[i & 1];
+        const bool fast = tile_fast && i >= np && i <= nx2 - 2 - np;
+        const int sxh = (i < nx2 - 1) ? half_slab(i, nx2, np) : -1;
+        const int e = i - (i0 - 1);
+        S *ox = Vxout + i * sx, *oy = Vyout + i * sx, *oz = Vzout + i * sx;
+
+        // ---- velocity half step at plane i (a_iso_3d.c:605-651) ----
+        C vxn[R], vzn[R];
+        C vzh = C(0);
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+            const int row = w * R + r, j = j0 + row;
+            const int cc = (row + 1) * WS + HS + lane;
+            const int rc = (row + 1) * WC + HC + lane;
+            const C p_c = St::ld(cP + cc, isP);
+            const C r_c = cR[rc];
+            C vx = St::ld(cX + row * 32 + lane, isX);
+            C vy = St::ld(cY + (row + 1) * 32 + lane, isY);
+            C vz = St::ld(cZ + row * WZ + HS + lane, isZ);
+            if (fast) {
+                vx = a3_vel0<C>(vx, p_c, St::ld(nP + cc, isP), r_c, nR[rc], idx, two_dt);
+                vy = a3_vel0<C>(vy, p_c, St::ld(cP + cc + WS, isP), r_c, cR[rc + WC], idy, two_dt);
+                vz = a3_vel0<C>(vz, p_c, St::ld(cP + cc + 1, isP), r_c, cR[rc + 1], idz, two_dt);
+            } else if (rin[r]) {
+                C psi_new;
+                if (i < nx2 - 1) {
+                    vx = a3_vel<C>(vx, p_c, St::ld(nP + cc, isP), r_c, nR[rc], idx, two_dt, sxh >= 0,
+                                   CX[0][e], CX[1][e], CX[2][e], fPx[r], psi_new);
+                    if (sxh >= 0) St::st(poPx + sxh * sx + joff[r], psi_new, a.psc[PS_PX]);
+                }
+                if (j < ny2 - 1) {
+                    vy = a3_vel<C>(vy, p_c, St::ld(cP + cc + WS, isP), r_c, cR[rc + WC], idy, two_dt,
+                                   jh[r] >= 0, CY[0][row + 1], CY[1][row + 1], CY[2][row + 1], fPy[r],
+                                   psi_new);
+                    if (jh[r] >= 0)
+                        St::st(poPy + (i * 2 * np + jh[r]) * pitch + k, psi_new, a.psc[PS_PY]);
+                }
+                if (k < nz2 - 1) {
+                    vz = a3_vel<C>(vz, p_c, St::ld(cP + cc + 1, isP), r_c, cR[rc + 1], idz, two_dt,
+                                   kh >= 0, CZ[0][lane + 1], CZ[1][lane + 1], CZ[2][lane + 1], fPz[r],
+                                   psi_new);
+                    if (kh >= 0) St::st(poPz + (i * ny2 + j) * 2 * np + kh, psi_new, a.psc[PS_PZ]);
+                }
+            }
+            vyw[row + 1][lane] = vy;
+            vxn[r] = vx;
+            vzn[r] = vz;
+            if (rin[r]) {
+                St::st(ox + joff[r], vx, a.sc[A_VX]);
+                St::st(oy + joff[r], vy, a.sc[A_VY]);
+                St::st(oz + joff[r], vz, a.sc[A_VZ]);
+            }
+        }
+        // halo row: vy(i, j0-1, k), by warp 0
+        if (w == 0) {
+            C vyh = C(0);
+            if (jm >= 0 && kin) {
+                C psi_new;
+                vyh = a3_vel<C>(St::ld(cY + lane, isY), St::ld(cP + HS + lane, isP),
+                                St::ld(cP + WS + HS + lane, isP), cR[HC + lane], cR[WC + HC + lane],
+                                idy, two_dt, jmh >= 0, CY[0][0], CY[1][0], CY[2][0], fHy, psi_new);
+            }
+            vyw[0][lane] = vyh;
+        }
+        // halo column: vz(i, j, k0-1) of row w*R + lane, by lanes 0..R-1
+        if (hcol) {
+            const int cc = (hrow + 1) * WS + HS, rc = (hrow + 1) * WC + HC;
+            C psi_new;
+            vzh = a3_vel<C>(St::ld(cZ + hrow * WZ + HS - 1, isZ), St::ld(cP + cc - 1, isP),
+                            St::ld(cP + cc, isP), cR[rc - 1], cR[rc], idz, two_dt, kmh >= 0, CZ[0][0],
+                            CZ[1][0], CZ[2][0], fHz, psi_new);
+        }
+        // memory variables for the next plane's velocities
+        if (i + 1 < i1 && (!tile_fast || i + 1 < np || i + 1 > nx2 - 2 - np)) load_vpsi(i + 1);
+        // the pressure of the previous plane (its velocities are complete)
+        if (i > i0) {
+            const int ip = i - 1;
+            pressure(ip, l - 1, tile_fast && ip >= np && ip <= nx2 - 1 - np);
+        }
+        if (!tile_fast || i < np || i > nx2 - 1 - np) load_ppsi(i);
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+            vxb[r] = vxa[r];
+            vxa[r] = vxn[r];
+            vzp[r] = vzn[r];
+        }
+#pragma unroll
+        for (int r = 0; r < R; ++r) vzhp[r] = (lane == r) ? vzh : vzhp[r];
+        __syncthreads();   // vy rows of plane i visible; the oldest stage may be refilled
+    }
+    // the last plane's pressure
+    if (i1 > i0) {
+        const int ip = i1 - 1;
+        pressure(ip, ip - i0, tile_fast && ip >= np && ip <= nx2 - 1 - np);
     }
 }
 
-template <typename S>
-__global__ void __launch_bounds__(256) a3d_pressure_kernel(A3Args a) {
-    using C = typename Store<S>::C;
-    using St = Store<S>;
-    const int k = blockIdx.x * blockDim.x + threadIdx.x;
-    const int j = blockIdx.y * blockDim.y + threadIdx.y;
-    const int i = blockIdx.z;
-    // a_iso_3d.c:659-683: i, j, k >= 1
-    if (k >= a.nz2 || j >= a.ny2 || i < 1 || j < 1 || k < 1) return;
-    const long long q = (long long)i * a.sx + (long long)j * a.sy + k;
-    const S *vx = static_cast<const S *>(a.f[A_VX]);
-    const S *vy = static_cast<const S *>(a.f[A_VY]);
-    const S *vz = static_cast<const S *>(a.f[A_VZ]);
-    const C *cf = static_cast<const C *>(a.coef);
-    const int np = a.np;
-    C dx = (St::ld(vx + q, a.isc[A_VX]) - St::ld(vx + q - a.sx, a.isc[A_VX])) * static_cast<C>(a.idx);
-    C dy = (St::ld(vy + q, a.isc[A_VY]) - St::ld(vy + q - a.sy, a.isc[A_VY])) * static_cast<C>(a.idy);
-    C dz = (St::ld(vz + q, a.isc[A_VZ]) - St::ld(vz + q - 1, a.isc[A_VZ])) * static_cast<C>(a.idz);
-    int s = node_slab(i, a.nx2, np);
-    if (s >= 0) {
-        S *m = static_cast<S *>(a.psi[PS_VX]);
-        const long long c = ((long long)s * a.ny2 + j) * a.pitch + k;
-        const C mm = cf[a.cf.at(0, 1) + i] * St::ld(m + c, a.pisc[PS_VX]) + cf[a.cf.at(0, 0) + i] * dx;
-        St::st(m + c, mm, a.psc[PS_VX]);
-        dx = dx * cf[a.cf.at(0, 2) + i] + mm;
-    }
-    s = node_slab(j, a.ny2, np);
-    if (s >= 0) {
-        S *m = static_cast<S *>(a.psi[PS_VY]);
-        const long long c = ((long long)i * 2 * np + s) * a.pitch + k;
-        const C mm = cf[a.cf.at(1, 1) + j] * St::ld(m + c, a.pisc[PS_VY]) + cf[a.cf.at(1, 0) + j] * dy;
-        St::st(m + c, mm, a.psc[PS_VY]);
-        dy = dy * cf[a.cf.at(1, 2) + j] + mm;
-    }
-    s = node_slab(k, a.nz2, np);
-    if (s >= 0) {
-        S *m = static_cast<S *>(a.psi[PS_VZ]);
-        const long long c = ((long long)i * a.ny2 + j) * 2 * np + s;
-        const C mm = cf[a.cf.at(2, 1) + k] * St::ld(m + c, a.pisc[PS_VZ]) + cf[a.cf.at(2, 0) + k] * dz;
-        St::st(m + c, mm, a.psc[PS_VZ]);
-        dz = dz * cf[a.cf.at(2, 2) + k] + mm;
-    }
-    S *P = static_cast<S *>(a.f[A_P]);
-    const C K = static_cast<const C *>(a.K)[q];
-    St::st(P + q, St::ld(P + q, a.isc[A_P]) - K * (dx + dy + dz), a.sc[A_P]);
+template <typename S, int TY, int D>
+constexpr size_t a3d_step_smem() {
+    return A3Lay<S, TY>::head + (size_t)D * A3Lay<S, TY>::stage;
 }
 
 struct A3Src {
@@ -237,7 +541,10 @@ struct sm_a3d {
     size_t it = 0;
     cudaStream_t stream = nullptr;
     A3Args args{};
-    DevBuf f[4], psi[6], rho, K, coef;
+    DevBuf f[2][4], psi[2][6], rho, K, coef;   // two buffer sets (ping-pong)
+    int cur = 0;                               // set holding the current state
+    int config = 6;                            // index into kA3Configs
+    int sms = 148;
     std::vector<A3Src> src;
     std::vector<double> vals;
     DevBuf d_src, d_vals;
@@ -248,6 +555,10 @@ struct sm_a3d {
     int rec_dirty = 1;
     size_t elem = 4;
     size_t psi_cells[6] = {0, 0, 0, 0, 0, 0};
+    KernelTimer timer;
+    A3Maps maps[2];                            // TMA maps with set b as input
+    int maps_ty = -1;                          // tile rows the maps were made for
+    DevBuf err;                                // kernel timeout flag
 };
 
 namespace {
@@ -257,12 +568,136 @@ int a3d_check(sm_a3d_t h) {
     return SM_OK;
 }
 
+void a3d_bind(sm_a3d *h, int in) {
+    for (int f = 0; f < 4; ++f) {
+        h->args.f[f] = h->f[in][f].p;
+        h->args.fo[f] = h->f[1 - in][f].p;
+    }
+    for (int p = 0; p < 6; ++p) {
+        h->args.psi[p] = h->psi[in][p].p;
+        h->args.pso[p] = h->psi[1 - in][p].p;
+    }
+}
+
+// launch configurations of the fused step: tile rows, ring stages and the
+// minimum resident CTAs per SM the register budget is fitted to
+struct A3Config {
+    int warps, rows, stages, minb;
+    int ty() const { return warps * rows; }
+};
+static const A3Config kA3Configs[] = {
+    {8, 2, 5, 2}, {4, 4, 5, 3}, {8, 4, 4, 1}, {8, 1, 6, 3},
+    {16, 2, 4, 1}, {4, 2, 6, 4}, {8, 2, 4, 3}, {4, 8, 4, 2},
+};
+static const int kA3NumConfigs = sizeof(kA3Configs) / sizeof(kA3Configs[0]);
+
+template <typename S, int W, int R, int D, int MINB>
+void a3d_launch_cfg(sm_a3d *h) {
+    constexpr int TY = W * R;
+    constexpr size_t smem = a3d_step_smem<S, TY, D>();
+    static bool configured = false;   // once per instantiation and process
+    if (!configured) {
+        cudaFuncSetAttribute(a3d_step_kernel<S, W, R, D, MINB>,
+                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        configured = true;
+    }
+    dim3 blk(32, W, 1);
+    dim3 grd((unsigned)((h->nz2 + 31) / 32), (unsigned)((h->ny2 + TY - 1) / TY),
+             (unsigned)((h->nx2 + h->args.chunk - 1) / h->args.chunk));
+    a3d_step_kernel<S, W, R, D, MINB><<<grd, blk, smem, h->stream>>>(h->args, h->maps[h->cur]);
+}
+
+// TMA maps of one buffer set (as the step's input) for tile rows ty; box
+// shapes follow A3Lay
+template <typename S>
+int a3d_make_maps(sm_a3d *h, int ty) {
+    using C = typename Store<S>::C;
+    const int HS = 16 / (int)sizeof(S), HC = 16 / (int)sizeof(C);
+    const CUtensorMapDataType ds = MapType<S>::v, dc = MapType<C>::v;
+    const size_t n0 = h->nz2, n1 = h->ny2, n2 = h->nx2, pt = h->pitch;
+    int rc;
+    for (int b = 0; b < 2; ++b) {
+        A3Maps &m = h->maps[b];
+        if ((rc = make_map_3d(&m.P, h->f[b][A_P].p, ds, sizeof(S), n0, n1, n2, pt, 32 + 2 * HS, ty + 2)))
+            return rc;
+        if ((rc = make_map_3d(&m.vx, h->f[b][A_VX].p, ds, sizeof(S), n0, n1, n2, pt, 32, ty))) return rc;
+        if ((rc = make_map_3d(&m.vy, h->f[b][A_VY].p, ds, sizeof(S), n0, n1, n2, pt, 32, ty + 1)))
+            return rc;
+        if ((rc = make_map_3d(&m.vz, h->f[b][A_VZ].p, ds, sizeof(S), n0, n1, n2, pt, 32 + HS, ty)))
+            return rc;
+        if ((rc = make_map_3d(&m.rho, h->rho.p, dc, sizeof(C), n0, n1, n2, pt, 32 + 2 * HC, ty + 2)))
+            return rc;
+        if ((rc = make_map_3d(&m.K, h->K.p, dc, sizeof(C), n0, n1, n2, pt, 32, ty))) return rc;
+    }
+    h->maps_ty = ty;
+    return SM_OK;
+}
+
+int a3d_ensure_maps(sm_a3d *h) {
+    const int ty = kA3Configs[h->config].ty();
+    if (h->maps_ty == ty) return SM_OK;
+    switch (h->precision) {
+    case SM_FP64: return a3d_make_maps<double>(h, ty);
+    case SM_FP16: return a3d_make_maps<__half>(h, ty);
+    case SM_BF16: return a3d_make_maps<__nv_bfloat16>(h, ty);
+    default: return a3d_make_maps<float>(h, ty);
+    }
+}
+
+int a3d_check_err(sm_a3d *h) {
+    int e = 0;
+    SM_CUDA_TRY(cudaMemcpy(&e, h->err.p, sizeof(int), cudaMemcpyDeviceToHost));
+    if (e) return sm_fail(SM_ETIMEOUT, "a_iso_3d step kernel: a bounded wait for a TMA load gave up");
+    return SM_OK;
+}
+
+template <typename S>
+size_t a3d_config_smem(int config) {
+    switch (config) {
+    case 0: return a3d_step_smem<S, 16, 5>();
+    case 1: return a3d_step_smem<S, 16, 5>();
+    case 2: return a3d_step_smem<S, 32, 4>();
+    case 3: return a3d_step_smem<S, 8, 6>();
+    case 4: return a3d_step_smem<S, 32, 4>();
+    case 5: return a3d_step_smem<S, 8, 6>();
+    case 6: return a3d_step_smem<S, 16, 4>();
+    default: return a3d_step_smem<S, 32, 4>();
+    }
+}
+
+size_t a3d_config_smem_prec(int precision, int config) {
+    switch (precision) {
+    case SM_FP64: return a3d_config_smem<double>(config);
+    case SM_FP16: return a3d_config_smem<__half>(config);
+    case SM_BF16: return a3d_config_smem<__nv_bfloat16>(config);
+    default: return a3d_config_smem<float>(config);
+    }
+}
+
+template <typename S>
+void a3d_launch_step(sm_a3d *h) {
+    switch (h->config) {
+    case 0: a3d_launch_cfg<S, 8, 2, 5, 2>(h); break;
+    case 1: a3d_launch_cfg<S, 4, 4, 5, 3>(h); break;
+    case 2: a3d_launch_cfg<S, 8, 4, 4, 1>(h); break;
+    case 3: a3d_launch_cfg<S, 8, 1, 6, 3>(h); break;
+    case 4: a3d_launch_cfg<S, 16, 2, 4, 1>(h); break;
+    case 5: a3d_launch_cfg<S, 4, 2, 6, 4>(h); break;
+    case 6: a3d_launch_cfg<S, 8, 2, 4, 3>(h); break;
+    default: a3d_launch_cfg<S, 4, 8, 4, 2>(h); break;
+    }
+}
+
 template <typename S>
 void a3d_launch(sm_a3d *h) {
-    dim3 blk(32, 8, 1);
-    dim3 grd((unsigned)((h->nz2 + 31) / 32), (unsigned)((h->ny2 + 7) / 8), (unsigned)h->nx2);
-    a3d_velocity_kernel<S><<<grd, blk, 0, h->stream>>>(h->args);
-    a3d_pressure_kernel<S><<<grd, blk, 0, h->stream>>>(h->args);
+    a3d_bind(h, h->cur);
+    cudaEvent_t t0 = h->timer.begin(h->stream);
+    a3d_launch_step<S>(h);
+    h->timer.end(t0, h->stream);
+    h->cur = 1 - h->cur;
+    // sources and receivers act on the state just written
+    a3d_bind(h, h->cur);
+    h->timer.launches += 1 + (h->src.empty() ? 0 : 1) + (h->rec.empty() ? 0 : 1);
     if (!h->src.empty())
         a3d_source_kernel<S><<<1, 32, 0, h->stream>>>(h->args, h->d_src.as<A3Src>(),
                                                       (int)h->src.size(), h->d_vals.as<double>(),
@@ -273,6 +708,21 @@ void a3d_launch(sm_a3d *h) {
             h->args, h->d_rec.as<A3Rec>(), n, h->d_table.as<int32_t>(),
             (long long)h->plan.nsteps_max, (long long)h->it, h->d_traces.as<double>());
     }
+}
+
+// x planes per CTA: enough CTAs for a few waves on the device, at least
+// 16 planes per chunk so the recomputed plane i0-1 and the pipeline fill stay
+// cheap
+int a3d_pick_chunk(size_t nx2, size_t ny2, size_t nz2, int sms, int ty) {
+    const size_t tiles = ((nz2 + 31) / 32) * ((ny2 + ty - 1) / ty);
+    const size_t want = (size_t)sms * 16;
+    size_t nch = (want + tiles - 1) / tiles;
+    if (nch < 1) nch = 1;
+    size_t chunk = (nx2 + nch - 1) / nch;
+    if (chunk < 16) chunk = 16;
+    if (chunk > A3_CHMAX) chunk = A3_CHMAX;
+    if (chunk > nx2) chunk = nx2;
+    return (int)chunk;
 }
 
 int a3d_field_id(int comp) {
@@ -321,8 +771,8 @@ extern "C" int sm_a3d_create(int device, size_t nx2, size_t ny2, size_t nz2, siz
         return sm_fail(SM_EINVAL, "sm_a3d_create: spacings and dt must be > 0");
     if (precision < SM_FP32 || precision > SM_BF16)
         return sm_fail(SM_EINVAL, "sm_a3d_create: unknown precision %d", precision);
-    if (ny2 > 65535 * 8 || nx2 > 65535)
-        return sm_fail(SM_EINVAL, "sm_a3d_create: grid too large");
+    if (ny2 > 65535 * 4 || nx2 > 65535 || (double)nx2 * ny2 * (nz2 + 31) >= 2147483647.0)
+        return sm_fail(SM_EINVAL, "sm_a3d_create: grid too large (cells must stay below 2^31)");
     // outside the frame the coefficients must be the reference defaults
     const size_t n2[3] = {nx2, ny2, nz2};
     for (int ax = 0; ax < 3; ++ax) {
@@ -354,13 +804,15 @@ extern "C" int sm_a3d_create(int device, size_t nx2, size_t ny2, size_t nz2, siz
     const size_t cb = precision == SM_FP64 ? 8 : 4;
     const size_t ncell = nx2 * ny2 * (size_t)h->pitch;
     int rc;
-    for (int f = 0; f < 4; ++f)
-        if ((rc = h->f[f].alloc(ncell * h->elem))) return rc;
+    for (int b = 0; b < 2; ++b)
+        for (int f = 0; f < 4; ++f)
+            if ((rc = h->f[b][f].alloc(ncell * h->elem))) return rc;
     h->psi_cells[PS_PX] = h->psi_cells[PS_VX] = 2 * np * ny2 * (size_t)h->pitch;
     h->psi_cells[PS_PY] = h->psi_cells[PS_VY] = nx2 * 2 * np * (size_t)h->pitch;
     h->psi_cells[PS_PZ] = h->psi_cells[PS_VZ] = nx2 * ny2 * 2 * np;
-    for (int p = 0; p < 6; ++p)
-        if ((rc = h->psi[p].alloc(h->psi_cells[p] * h->elem))) return rc;
+    for (int b = 0; b < 2; ++b)
+        for (int p = 0; p < 6; ++p)
+            if ((rc = h->psi[b][p].alloc(h->psi_cells[p] * h->elem))) return rc;
     if ((rc = h->rho.alloc(ncell * cb))) return rc;
     if ((rc = h->K.alloc(ncell * cb))) return rc;
     {
@@ -410,9 +862,15 @@ extern "C" int sm_a3d_create(int device, size_t nx2, size_t ny2, size_t nz2, siz
     A3Args &a = h->args;
     a.nx2 = (int)nx2; a.ny2 = (int)ny2; a.nz2 = (int)nz2; a.pitch = h->pitch; a.np = (int)np;
     a.sy = h->pitch;
-    a.sx = (long long)ny2 * h->pitch;
-    for (int f = 0; f < 4; ++f) { a.f[f] = h->f[f].p; a.sc[f] = 1.f; a.isc[f] = 1.f; }
-    for (int p = 0; p < 6; ++p) { a.psi[p] = h->psi[p].p; a.psc[p] = 1.f; a.pisc[p] = 1.f; }
+    a.sx = (int)(ny2 * h->pitch);
+    if ((rc = h->err.alloc(sizeof(int)))) return rc;
+    if ((rc = h->err.zero(h->stream))) return rc;
+    a.err = h->err.as<int>();
+    for (int f = 0; f < 4; ++f) { a.sc[f] = 1.f; a.isc[f] = 1.f; }
+    for (int p = 0; p < 6; ++p) { a.psc[p] = 1.f; a.pisc[p] = 1.f; }
+    cudaDeviceGetAttribute(&h->sms, cudaDevAttrMultiProcessorCount, device);
+    a.chunk = a3d_pick_chunk(nx2, ny2, nz2, h->sms, kA3Configs[h->config].ty());
+    a3d_bind(h.get(), 0);
     a.rho = h->rho.p;
     a.K = h->K.p;
     a.coef = h->coef.p;
@@ -427,10 +885,13 @@ extern "C" int sm_a3d_create(int device, size_t nx2, size_t ny2, size_t nz2, siz
 extern "C" int sm_a3d_reset(sm_a3d_t h) {
     if (int rc = a3d_check(h)) return rc;
     DeviceGuard g(h->device);
-    for (int f = 0; f < 4; ++f)
-        if (int rc = h->f[f].zero(h->stream)) return rc;
-    for (int p = 0; p < 6; ++p)
-        if (int rc = h->psi[p].zero(h->stream)) return rc;
+    for (int b = 0; b < 2; ++b) {
+        for (int f = 0; f < 4; ++f)
+            if (int rc = h->f[b][f].zero(h->stream)) return rc;
+        for (int p = 0; p < 6; ++p)
+            if (int rc = h->psi[b][p].zero(h->stream)) return rc;
+    }
+    h->cur = 0;
     if (int rc = h->d_traces.zero(h->stream)) return rc;
     SM_CUDA_TRY(cudaStreamSynchronize(h->stream));
     h->it = 0;
@@ -525,6 +986,7 @@ int a3d_upload(sm_a3d *h) {
 extern "C" int sm_a3d_run(sm_a3d_t h, size_t nsteps) {
     if (int rc = a3d_check(h)) return rc;
     DeviceGuard g(h->device);
+    if (int rc = a3d_ensure_maps(h)) return rc;
     if (h->src_dirty || h->rec_dirty)
         if (int rc = a3d_upload(h)) return rc;
     for (size_t s = 0; s < nsteps; ++s) {
@@ -542,8 +1004,9 @@ extern "C" int sm_a3d_run(sm_a3d_t h, size_t nsteps) {
 
 extern "C" int sm_a3d_sync(sm_a3d_t h) {
     if (int rc = a3d_check(h)) return rc;
+    DeviceGuard g(h->device);
     SM_CUDA_TRY(cudaStreamSynchronize(h->stream));
-    return SM_OK;
+    return a3d_check_err(h);
 }
 
 extern "C" int sm_a3d_step_count(sm_a3d_t h, size_t *it) {
@@ -561,6 +1024,7 @@ extern "C" int sm_a3d_read_traces(sm_a3d_t h, size_t rec0, size_t nrec, double *
     if (h->rec_dirty)
         if (int rc = a3d_upload(h)) return rc;
     SM_CUDA_TRY(cudaStreamSynchronize(h->stream));
+    if (int rc = a3d_check_err(h)) return rc;
     const size_t lim = std::min(h->it, h->plan.nsteps_max);
     std::vector<size_t> gcount(h->plan.count_total.size(), 0);
     for (size_t gi = 0; gi < gcount.size(); ++gi)
@@ -591,7 +1055,7 @@ extern "C" int sm_a3d_get_field(sm_a3d_t h, int comp, double *out) {
     SM_CUDA_TRY(cudaStreamSynchronize(h->stream));
     const size_t ncell = h->nx2 * h->ny2 * (size_t)h->pitch;
     std::vector<unsigned char> buf(ncell * h->elem);
-    SM_CUDA_TRY(cudaMemcpy(buf.data(), h->f[f].p, buf.size(), cudaMemcpyDeviceToHost));
+    SM_CUDA_TRY(cudaMemcpy(buf.data(), h->f[h->cur][f].p, buf.size(), cudaMemcpyDeviceToHost));
     for (size_t i = 0; i < h->nx2; ++i)
         for (size_t j = 0; j < h->ny2; ++j)
             for (size_t k = 0; k < h->nz2; ++k)
@@ -614,7 +1078,7 @@ extern "C" int sm_a3d_set_field(sm_a3d_t h, int comp, const double *in) {
             for (size_t k = 0; k < h->nz2; ++k)
                 a3_from_double(buf.data(), (i * h->ny2 + j) * h->pitch + k, h->precision,
                                in[(i * h->ny2 + j) * h->nz2 + k], h->args.sc[f]);
-    SM_CUDA_TRY(cudaMemcpy(h->f[f].p, buf.data(), buf.size(), cudaMemcpyHostToDevice));
+    SM_CUDA_TRY(cudaMemcpy(h->f[h->cur][f].p, buf.data(), buf.size(), cudaMemcpyHostToDevice));
     return SM_OK;
 }
 
@@ -641,5 +1105,58 @@ extern "C" int sm_device_info(int device, int *sm_count, size_t *hbm_bytes, size
     SM_CUDA_TRY(cudaMemGetInfo(&fr, &tot));
     if (hbm_bytes) *hbm_bytes = tot;
     if (hbm_free) *hbm_free = fr;
+    return SM_OK;
+}
+
+extern "C" int sm_a3d_stream(sm_a3d_t h, void **stream) {
+    if (int rc = a3d_check(h)) return rc;
+    if (!stream) return sm_fail(SM_EINVAL, "sm_a3d_stream: NULL");
+    *stream = (void *)h->stream;
+    return SM_OK;
+}
+
+extern "C" int sm_a3d_set_timing(sm_a3d_t h, int on) {
+    if (int rc = a3d_check(h)) return rc;
+    h->timer.on = on != 0;
+    return SM_OK;
+}
+
+extern "C" int sm_a3d_kernel_stats(sm_a3d_t h, int reset, double *update_ms,
+                                   size_t *update_launches, size_t *all_launches) {
+    if (int rc = a3d_check(h)) return rc;
+    DeviceGuard g(h->device);
+    return h->timer.stats(reset, update_ms, update_launches, all_launches);
+}
+
+extern "C" int sm_a3d_set_config(sm_a3d_t h, int config) {
+    if (int rc = a3d_check(h)) return rc;
+    if (config < 0 || config >= kA3NumConfigs)
+        return sm_fail(SM_EINVAL, "sm_a3d_set_config: config %d not in [0, %d)", config,
+                       kA3NumConfigs);
+    int maxsm = 0;
+    cudaDeviceGetAttribute(&maxsm, cudaDevAttrMaxSharedMemoryPerBlockOptin, h->device);
+    if (a3d_config_smem_prec(h->precision, config) > (size_t)maxsm)
+        return sm_fail(SM_EINVAL, "sm_a3d_set_config: config %d needs %zu bytes of shared memory "
+                                  "in this precision (device limit %d)", config,
+                       a3d_config_smem_prec(h->precision, config), maxsm);
+    h->config = config;
+    h->args.chunk = a3d_pick_chunk(h->nx2, h->ny2, h->nz2, h->sms, kA3Configs[config].ty());
+    // maps are rebuilt for the new tile height at the next run
+    return SM_OK;
+}
+
+extern "C" int sm_a3d_set_chunk(sm_a3d_t h, int chunk) {
+    if (int rc = a3d_check(h)) return rc;
+    if (chunk <= 0)
+        h->args.chunk = a3d_pick_chunk(h->nx2, h->ny2, h->nz2, h->sms, kA3Configs[h->config].ty());
+    else
+        h->args.chunk = chunk > A3_CHMAX ? A3_CHMAX : (chunk > (int)h->nx2 ? (int)h->nx2 : chunk);
+    return SM_OK;
+}
+
+extern "C" int sm_a3d_get_config(sm_a3d_t h, int *config, int *nconfigs) {
+    if (int rc = a3d_check(h)) return rc;
+    if (config) *config = h->config;
+    if (nconfigs) *nconfigs = kA3NumConfigs;
     return SM_OK;
 }

@@ -1,6 +1,8 @@
 // sm_common.cuh -- shared device helpers of libseismod_gpu (sm_100a).
 #pragma once
 
+#include <cuda.h>
+#include <cudaTypedefs.h>
 #include <cuda_bf16.h>
 #include <cuda_fp16.h>
 #include <cuda_runtime.h>
@@ -151,6 +153,59 @@ int upload_convert(void *dst, const double *src, size_t n, cudaStream_t s) {
 
 inline size_t round_up(size_t a, size_t b) { return (a + b - 1) / b * b; }
 
+// CUDA-event timing of the update kernel(s) plus launch counters
+struct KernelTimer {
+    bool on = false;
+    std::vector<cudaEvent_t> pool;
+    std::vector<std::pair<cudaEvent_t, cudaEvent_t>> pending;
+    double ms = 0.0;
+    size_t timed = 0;
+    size_t launches = 0;        // every kernel this handle launched
+    ~KernelTimer() {
+        for (auto e : pool) cudaEventDestroy(e);
+        for (auto &p : pending) { cudaEventDestroy(p.first); cudaEventDestroy(p.second); }
+    }
+    cudaEvent_t get() {
+        if (!pool.empty()) { cudaEvent_t e = pool.back(); pool.pop_back(); return e; }
+        cudaEvent_t e = nullptr;
+        cudaEventCreate(&e);
+        return e;
+    }
+    cudaEvent_t begin(cudaStream_t s) {
+        if (!on) return nullptr;
+        cudaEvent_t a = get();
+        cudaEventRecord(a, s);
+        return a;
+    }
+    void end(cudaEvent_t a, cudaStream_t s) {
+        if (!a) return;
+        cudaEvent_t b = get();
+        cudaEventRecord(b, s);
+        pending.emplace_back(a, b);
+        if (pending.size() > 4096) collect();
+    }
+    void collect() {
+        for (auto &p : pending) {
+            cudaEventSynchronize(p.second);
+            float t = 0.f;
+            cudaEventElapsedTime(&t, p.first, p.second);
+            ms += t;
+            ++timed;
+            pool.push_back(p.first);
+            pool.push_back(p.second);
+        }
+        pending.clear();
+    }
+    int stats(int reset, double *out_ms, size_t *out_timed, size_t *out_all) {
+        collect();
+        if (out_ms) *out_ms = ms;
+        if (out_timed) *out_timed = timed;
+        if (out_all) *out_all = launches;
+        if (reset) { ms = 0.0; timed = 0; launches = 0; }
+        return SM_OK;
+    }
+};
+
 // receiver sampling plan shared by both paths: receivers with the same
 // (t0, rdt) share one step -> slot table.
 struct SamplePlan {
@@ -189,5 +244,122 @@ struct SamplePlan {
         return SM_OK;
     }
 };
+
+// ---------------------------------------------------------------------------
+// arithmetic with fixed rounding: no contraction is left to the compiler, so
+// the same formula evaluated in two code paths (a cell and its recomputed
+// halo copy) rounds identically, and results do not depend on the launch
+// configuration
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ float r_add(float a, float b) { return __fadd_rn(a, b); }
+__device__ __forceinline__ float r_sub(float a, float b) { return __fsub_rn(a, b); }
+__device__ __forceinline__ float r_mul(float a, float b) { return __fmul_rn(a, b); }
+__device__ __forceinline__ float r_fma(float a, float b, float c) { return __fmaf_rn(a, b, c); }
+// 2 dt / (a + b): fast reciprocal in FP32 (within 2 ulp), exact in FP64
+__device__ __forceinline__ float r_quot(float num, float den) { return __fdividef(num, den); }
+__device__ __forceinline__ double r_add(double a, double b) { return __dadd_rn(a, b); }
+__device__ __forceinline__ double r_sub(double a, double b) { return __dsub_rn(a, b); }
+__device__ __forceinline__ double r_mul(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ double r_fma(double a, double b, double c) { return __fma_rn(a, b, c); }
+__device__ __forceinline__ double r_quot(double num, double den) { return __ddiv_rn(num, den); }
+
+// ---------------------------------------------------------------------------
+// TMA tile loads (cp.async.bulk.tensor, no multicast) completing on an
+// mbarrier, and bounded waits on it
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ unsigned smem_u32(const void *p) {
+    return static_cast<unsigned>(__cvta_generic_to_shared(p));
+}
+__device__ __forceinline__ void mbar_init(uint64_t *bar, unsigned count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(smem_u32(bar)), "r"(count)
+                 : "memory");
+}
+__device__ __forceinline__ void fence_proxy_async() {
+    asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, unsigned bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(smem_u32(bar)),
+                 "r"(bytes)
+                 : "memory");
+}
+__device__ __forceinline__ void tma_load_3d(void *dst, const CUtensorMap *map, int c0, int c1,
+                                            int c2, uint64_t *bar) {
+    asm volatile(
+        "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
+        " [%0], [%1, {%2, %3, %4}], [%5];\n" ::"r"(smem_u32(dst)),
+        "l"(reinterpret_cast<uint64_t>(map)), "r"(c0), "r"(c1), "r"(c2), "r"(smem_u32(bar))
+        : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, unsigned parity) {
+    unsigned ok;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+        " selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+// Wait for the phase with this parity; gives up after ~2^22 polls (each
+// try_wait may suspend for a while), records `code` in *err and returns
+// false.  A normal load lands within microseconds.
+__device__ __forceinline__ bool mbar_wait(uint64_t *bar, unsigned parity, int *err, int code) {
+    for (int n = 0; n < (1 << 22); ++n)
+        if (mbar_try_wait(bar, parity)) return true;
+    atomicExch(err, code);
+    return false;
+}
+
+}  // namespace sm
+
+// ---------------------------------------------------------------------------
+// host: TMA descriptors through the driver entry point (no -lcuda needed)
+// ---------------------------------------------------------------------------
+namespace sm {
+
+inline PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+    if (!fn) {
+        cudaDriverEntryPointQueryResult q;
+        void *p = nullptr;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) ==
+                cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+    }
+    return fn;
+}
+
+// 3-D tiled map over a padded array [n2][n1][pitch] of `elem`-byte values
+// whose valid extent is n0 x n1 x n2; box b0 x b1 x 1.  Loads outside the
+// extent read zeros.  The box row must be a multiple of 16 bytes and every
+// load's first coordinate a multiple of 16 bytes / elem (callers ensure it).
+inline int make_map_3d(CUtensorMap *m, const void *base, CUtensorMapDataType dt, size_t elem,
+                       size_t n0, size_t n1, size_t n2, size_t pitch, unsigned b0, unsigned b1) {
+    auto enc = tensor_map_encoder();
+    if (!enc) return sm_fail(SM_ECUDA, "cuTensorMapEncodeTiled is not available");
+    if ((b0 * elem) % 16 || (pitch * elem) % 16 || (reinterpret_cast<uintptr_t>(base) % 16))
+        return sm_fail(SM_EINVAL, "tensor map: 16-byte alignment rule violated");
+    cuuint64_t dims[3] = {n0, n1, n2};
+    cuuint64_t strides[2] = {pitch * elem, n1 * pitch * elem};
+    cuuint32_t box[3] = {b0, b1, 1};
+    cuuint32_t es[3] = {1, 1, 1};
+    CUresult r = enc(m, dt, 3, const_cast<void *>(base), dims, strides, box, es,
+                     CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                     CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) return sm_fail(SM_ECUDA, "cuTensorMapEncodeTiled failed (%d)", (int)r);
+    return SM_OK;
+}
+
+template <typename T>
+struct MapType;
+template <>
+struct MapType<float> { static constexpr CUtensorMapDataType v = CU_TENSOR_MAP_DATA_TYPE_FLOAT32; };
+template <>
+struct MapType<double> { static constexpr CUtensorMapDataType v = CU_TENSOR_MAP_DATA_TYPE_FLOAT64; };
+template <>
+struct MapType<__half> { static constexpr CUtensorMapDataType v = CU_TENSOR_MAP_DATA_TYPE_FLOAT16; };
+template <>
+struct MapType<__nv_bfloat16> { static constexpr CUtensorMapDataType v = CU_TENSOR_MAP_DATA_TYPE_BFLOAT16; };
 
 }  // namespace sm

@@ -276,6 +276,7 @@ struct sm_eiso {
     long long table_steps = 0;
     int rec_dirty = 1;
     size_t elem = 4;
+    KernelTimer timer;
 };
 
 namespace {
@@ -289,14 +290,18 @@ template <typename S>
 void launch_step(sm_eiso *h) {
     dim3 blk(32, 8, 1);
     dim3 grd((h->NZ + 31) / 32, (h->NX + 7) / 8, (unsigned)h->nshots);
+    cudaEvent_t t0 = h->timer.begin(h->stream);
     eiso_velocity_kernel<S><<<grd, blk, 0, h->stream>>>(h->args);
     eiso_stress_kernel<S><<<grd, blk, 0, h->stream>>>(h->args);
+    h->timer.end(t0, h->stream);
+    h->timer.launches += 2;
 }
 
 template <typename S>
 void launch_src(sm_eiso *h) {
     if (h->d_src.bytes == 0) return;
     int n = (int)h->nshots;
+    h->timer.launches += 1;
     eiso_source_kernel<S><<<(n + 127) / 128, 128, 0, h->stream>>>(
         h->args, h->d_src.as<SrcEntry>(), h->d_src_first.as<int>(), h->d_vals.as<double>(), n,
         (long long)h->it);
@@ -306,6 +311,7 @@ template <typename S>
 void launch_gather(sm_eiso *h) {
     if (h->n_rec_total == 0) return;
     int n = h->n_rec_total;
+    h->timer.launches += 1;
     eiso_gather_kernel<S><<<(n + 127) / 128, 128, 0, h->stream>>>(
         h->args, h->d_rec.as<RecEntry>(), n, h->d_table.as<int32_t>(), h->table_steps,
         (long long)h->it, h->d_traces.as<double>());
@@ -794,4 +800,24 @@ extern "C" int sm_eiso_destroy(sm_eiso_t h) {
         delete h;
     }
     return SM_OK;
+}
+
+extern "C" int sm_eiso_stream(sm_eiso_t h, void **stream) {
+    if (int rc = eiso_check(h)) return rc;
+    if (!stream) return sm_fail(SM_EINVAL, "sm_eiso_stream: NULL");
+    *stream = (void *)h->stream;
+    return SM_OK;
+}
+
+extern "C" int sm_eiso_set_timing(sm_eiso_t h, int on) {
+    if (int rc = eiso_check(h)) return rc;
+    h->timer.on = on != 0;
+    return SM_OK;
+}
+
+extern "C" int sm_eiso_kernel_stats(sm_eiso_t h, int reset, double *update_ms,
+                                    size_t *update_launches, size_t *all_launches) {
+    if (int rc = eiso_check(h)) return rc;
+    DeviceGuard g(h->device);
+    return h->timer.stats(reset, update_ms, update_launches, all_launches);
 }
