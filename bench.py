@@ -123,8 +123,11 @@ def eiso_bytes_per_step(p, nshots, s, m=4):
     return nshots * (nint * 10 * s + (nall - nint) * 20 * s) + nall * 3 * m
 
 
-def make_workload(name):
+def make_workload(name, size=None):
     from seismod_b200 import workloads as W
+    if name == "a3d" and size:
+        return ("a3d", W.cfg1(n=size),
+                f"a_iso_3d {size}^3 (+2x16 CPML), dx 5 m, cfg1 model family, 1000-step shot")
     if name == "a3d":
         return "a3d", W.cfg1(), "a_iso_3d 256^3 (+2x16 CPML = 288^3), dx 5 m, 1000-step shot"
     if name == "a3d512":
@@ -168,7 +171,7 @@ def time_steps(dev, K, torch):
 
 def run_ours(args, rank, world, local_rank, torch, dist):
     from seismod_b200 import api
-    kind, p, desc = make_workload(args.workload)
+    kind, p, desc = make_workload(args.workload, args.size)
     prec = args.precision
     sbytes = {"fp32": 4, "fp64": 8, "fp16": 2, "bf16": 2}[prec]
     mbytes = 8 if prec == "fp64" else 4
@@ -352,6 +355,8 @@ def main():
     ap.add_argument("--workload", default="a3d", choices=["a3d", "a3d512", "eiso", "eiso1"])
     ap.add_argument("--precision", default="fp32", choices=["fp32", "fp64", "fp16", "bf16"])
     ap.add_argument("--no-side", action="store_true", help="skip precision / CPU side runs")
+    ap.add_argument("--size", type=int, default=None,
+                    help="a3d only: interior edge length instead of 256 (profiling captures)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 

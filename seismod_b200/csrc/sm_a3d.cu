@@ -559,6 +559,12 @@ struct sm_a3d {
     A3Maps maps[2];                            // TMA maps with set b as input
     int maps_ty = -1;                          // tile rows the maps were made for
     DevBuf err;                                // kernel timeout flag
+    // 16-bit storage: exponents of the 4 fields (A_*) and 6 memory
+    // variables (4 + PS_*), stored = value * 2^expo
+    Scaler16 scaler;
+    std::vector<int> expo0;                    // exponents restored by reset
+    double rho_min = 0, vp_min = 0, hmin = 0;
+    static constexpr int kScalePeriod = 16;    // steps between range checks
 };
 
 namespace {
@@ -642,6 +648,35 @@ int a3d_ensure_maps(sm_a3d *h) {
     case SM_BF16: return a3d_make_maps<__nv_bfloat16>(h, ty);
     default: return a3d_make_maps<float>(h, ty);
     }
+}
+
+bool a3d_is16(const sm_a3d *h) { return h->precision == SM_FP16 || h->precision == SM_BF16; }
+
+void a3d_apply_scales(sm_a3d *h) {
+    for (int f = 0; f < 4; ++f) {
+        h->args.sc[f] = std::ldexp(1.0f, h->scaler.expo[f]);
+        h->args.isc[f] = std::ldexp(1.0f, -h->scaler.expo[f]);
+    }
+    for (int q = 0; q < 6; ++q) {
+        h->args.psc[q] = std::ldexp(1.0f, h->scaler.expo[4 + q]);
+        h->args.pisc[q] = std::ldexp(1.0f, -h->scaler.expo[4 + q]);
+    }
+}
+
+int a3d_rescale(sm_a3d *h) {
+    void *ptrs[10];
+    size_t ns[10];
+    const size_t ncell = h->nx2 * h->ny2 * (size_t)h->pitch;
+    static const char *names[10] = {"vx", "vy", "vz", "P", "psi_Px", "psi_Py", "psi_Pz",
+                                    "psi_vx", "psi_vy", "psi_vz"};
+    static const int groups[10] = {0, 1, 2, 3, 4, 5, 6, 7, 8, 9};
+    for (int f = 0; f < 4; ++f) { ptrs[f] = h->f[h->cur][f].p; ns[f] = ncell; }
+    for (int q = 0; q < 6; ++q) { ptrs[4 + q] = h->psi[h->cur][q].p; ns[4 + q] = h->psi_cells[q]; }
+    int rc = h->precision == SM_FP16
+                 ? h->scaler.check<__half>(h->stream, 10, ptrs, ns, groups, names)
+                 : h->scaler.check<__nv_bfloat16>(h->stream, 10, ptrs, ns, groups, names);
+    a3d_apply_scales(h);
+    return rc;
 }
 
 int a3d_check_err(sm_a3d *h) {
@@ -863,6 +898,18 @@ extern "C" int sm_a3d_create(int device, size_t nx2, size_t ny2, size_t nz2, siz
     a.nx2 = (int)nx2; a.ny2 = (int)ny2; a.nz2 = (int)nz2; a.pitch = h->pitch; a.np = (int)np;
     a.sy = h->pitch;
     a.sx = (int)(ny2 * h->pitch);
+    if (precision == SM_FP16 || precision == SM_BF16) {
+        if ((rc = h->scaler.init(10, 10))) return rc;
+        const size_t N = nx2 * ny2 * nz2;
+        h->rho_min = rho[0];
+        h->vp_min = vp[0];
+        for (size_t q = 1; q < N; ++q) {
+            if (rho[q] < h->rho_min) h->rho_min = rho[q];
+            if (vp[q] < h->vp_min) h->vp_min = vp[q];
+        }
+        h->hmin = std::min(dx, std::min(dy, dz));
+        h->expo0.assign(10, 0);
+    }
     if ((rc = h->err.alloc(sizeof(int)))) return rc;
     if ((rc = h->err.zero(h->stream))) return rc;
     a.err = h->err.as<int>();
@@ -877,6 +924,7 @@ extern "C" int sm_a3d_create(int device, size_t nx2, size_t ny2, size_t nz2, siz
     a.cf = cf;
     a.two_dt = dt * 2.;
     a.idx = 1.0 / dx; a.idy = 1.0 / dy; a.idz = 1.0 / dz;
+    if (precision == SM_FP16 || precision == SM_BF16) a3d_apply_scales(h.get());
     if ((rc = sm_a3d_reset(h.get()))) return rc;
     *out = h.release();
     return SM_OK;
@@ -892,6 +940,10 @@ extern "C" int sm_a3d_reset(sm_a3d_t h) {
             if (int rc = h->psi[b][p].zero(h->stream)) return rc;
     }
     h->cur = 0;
+    if (a3d_is16(h)) {
+        h->scaler.expo = h->expo0;
+        a3d_apply_scales(h);
+    }
     if (int rc = h->d_traces.zero(h->stream)) return rc;
     SM_CUDA_TRY(cudaStreamSynchronize(h->stream));
     h->it = 0;
@@ -918,6 +970,30 @@ extern "C" int sm_a3d_set_sources(sm_a3d_t h, size_t nsrc, const size_t *index, 
         h->src.push_back(e);
     }
     h->src_dirty = 1;
+    if (a3d_is16(h)) {
+        // starting ranges from the source: the pressure a cell accumulates
+        // (running sum of the injected values), the particle velocity that
+        // pressure drives (p / (rho vp)), and their gradients for the memory
+        // variables; the range checks refine them as the run proceeds
+        double pmax = 0.0;
+        for (const A3Src &e : h->src) {
+            double acc = 0.0;
+            for (int t = 0; t < e.len; ++t) {
+                acc += h->vals[e.voff + t];
+                pmax = std::max(pmax, std::fabs(acc));
+            }
+        }
+        const double vmax = pmax / (h->rho_min * h->vp_min);
+        const int ep = Scaler16::expo_for(pmax), ev = Scaler16::expo_for(vmax);
+        const int egp = Scaler16::expo_for(pmax / h->hmin), egv = Scaler16::expo_for(vmax / h->hmin);
+        std::vector<int> ex = {ev, ev, ev, ep, egp, egp, egp, egv, egv, egv};
+        h->expo0 = ex;
+        for (int g = 0; g < 10; ++g) h->scaler.ceil[g] = ex[g] + 2;
+        if (h->it == 0) {
+            h->scaler.expo = ex;
+            a3d_apply_scales(h);
+        }
+    }
     return SM_OK;
 }
 
@@ -997,6 +1073,8 @@ extern "C" int sm_a3d_run(sm_a3d_t h, size_t nsteps) {
         default: a3d_launch<float>(h); break;
         }
         h->it++;
+        if (a3d_is16(h) && h->it % sm_a3d::kScalePeriod == 0)
+            if (int rc = a3d_rescale(h)) return rc;
     }
     SM_CUDA_TRY(cudaGetLastError());
     return SM_OK;

@@ -7,8 +7,11 @@
 #include <cuda_fp16.h>
 #include <cuda_runtime.h>
 
+#include <algorithm>
+#include <cmath>
 #include <cstddef>
 #include <cstdint>
+#include <cstring>
 #include <vector>
 
 #include "../host/sm_host.h"
@@ -310,6 +313,31 @@ __device__ __forceinline__ bool mbar_wait(uint64_t *bar, unsigned parity, int *e
     return false;
 }
 
+// ---------------------------------------------------------------------------
+// per-array power-of-two scaling of 16-bit storage
+// ---------------------------------------------------------------------------
+template <typename S>
+__global__ void amax_kernel(const S *p, size_t n, unsigned *out) {
+    float m = 0.f;
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
+         i += (size_t)gridDim.x * blockDim.x) {
+        const float v = fabsf(static_cast<float>(p[i]));
+        m = (v > m || v != v) ? v : m;   // a NaN wins, so overflow is seen
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        const float t = __shfl_xor_sync(0xffffffffu, m, o);
+        m = (t > m || t != t) ? t : m;
+    }
+    if ((threadIdx.x & 31) == 0) atomicMax(out, __float_as_uint(m));
+}
+
+template <typename S>
+__global__ void rescale_kernel(S *p, size_t n, float factor) {
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
+         i += (size_t)gridDim.x * blockDim.x)
+        p[i] = static_cast<S>(static_cast<float>(p[i]) * factor);
+}
+
 }  // namespace sm
 
 // ---------------------------------------------------------------------------
@@ -350,6 +378,86 @@ inline int make_map_3d(CUtensorMap *m, const void *base, CUtensorMapDataType dt,
     if (r != CUDA_SUCCESS) return sm_fail(SM_ECUDA, "cuTensorMapEncodeTiled failed (%d)", (int)r);
     return SM_OK;
 }
+
+// Keeps each 16-bit array group's largest stored magnitude near 2^11..2^12
+// by power-of-two rescaling (exact unless a value under- or overflows):
+// stored = value * 2^expo[group].  check() measures every array (device
+// max-abs reduction), rescales the groups whose maximum left [2^9, 2^13],
+// and returns SM_ESTATE if any array already holds Inf/NaN.  A group is
+// scaled down whenever it grows, but scaled up at most to ceil[group] (set
+// from an upper estimate of its amplitude): while a wave is still arriving a
+// field's maximum is tiny, and scaling it up to match would overflow once
+// the wave arrives.
+struct Scaler16 {
+    int ngroups = 0;
+    std::vector<int> expo;   // per group
+    std::vector<int> ceil;   // largest exponent a group may be raised to
+    DevBuf d_amax;
+    unsigned *h_amax = nullptr;
+    int cap = 0;
+    ~Scaler16() {
+        if (h_amax) cudaFreeHost(h_amax);
+    }
+    int init(int groups, int max_arrays) {
+        ngroups = groups;
+        cap = max_arrays;
+        expo.assign(groups, 0);
+        ceil.assign(groups, 0);
+        if (int rc = d_amax.alloc(max_arrays * sizeof(unsigned))) return rc;
+        if (cudaMallocHost(&h_amax, max_arrays * sizeof(unsigned)) != cudaSuccess)
+            return sm_fail(SM_ENOMEM, "cudaMallocHost failed");
+        return SM_OK;
+    }
+    static int expo_for(double maxval) {   // exponent putting maxval near 2^11
+        if (!(maxval > 0.0) || !std::isfinite(maxval)) return 0;
+        int e = 11 - std::ilogb(maxval);
+        if (e > 100) e = 100;
+        if (e < -100) e = -100;
+        return e;
+    }
+    // arrays [0, narr): device pointers, element counts, group of each
+    template <typename S>
+    int check(cudaStream_t st, int narr, void *const *ptrs, const size_t *ns, const int *group,
+              const char *const *gnames) {
+        if (narr > cap) return sm_fail(SM_EINVAL, "Scaler16: too many arrays");
+        SM_CUDA_TRY(cudaMemsetAsync(d_amax.p, 0, narr * sizeof(unsigned), st));
+        for (int a = 0; a < narr; ++a) {
+            if (!ns[a]) continue;
+            unsigned blocks = (unsigned)std::min<size_t>((ns[a] + 255) / 256, 1184);
+            amax_kernel<S><<<blocks, 256, 0, st>>>(static_cast<const S *>(ptrs[a]), ns[a],
+                                                   d_amax.as<unsigned>() + a);
+        }
+        SM_CUDA_TRY(cudaMemcpyAsync(h_amax, d_amax.p, narr * sizeof(unsigned),
+                                    cudaMemcpyDeviceToHost, st));
+        SM_CUDA_TRY(cudaStreamSynchronize(st));
+        std::vector<float> gmax(ngroups, 0.f);
+        for (int a = 0; a < narr; ++a) {
+            float m;
+            std::memcpy(&m, &h_amax[a], sizeof m);
+            if (!std::isfinite(m))
+                return sm_fail(SM_ESTATE, "16-bit storage of %s overflowed (scale 2^%d)",
+                               gnames[group[a]], expo[group[a]]);
+            gmax[group[a]] = std::max(gmax[group[a]], m);
+        }
+        for (int g = 0; g < ngroups; ++g) {
+            if (gmax[g] == 0.f) continue;
+            const int ex = std::ilogb(gmax[g]);
+            if (ex <= 13 && ex >= 9) continue;
+            int shift = 11 - ex;
+            if (shift > 0) shift = std::min(shift, ceil[g] - expo[g]);
+            if (shift == 0) continue;
+            for (int a = 0; a < narr; ++a) {
+                if (group[a] != g || !ns[a]) continue;
+                unsigned blocks = (unsigned)std::min<size_t>((ns[a] + 255) / 256, 4736);
+                rescale_kernel<S><<<blocks, 256, 0, st>>>(static_cast<S *>(ptrs[a]), ns[a],
+                                                          std::ldexp(1.0f, shift));
+            }
+            expo[g] += shift;
+        }
+        SM_CUDA_TRY(cudaGetLastError());
+        return SM_OK;
+    }
+};
 
 template <typename T>
 struct MapType;

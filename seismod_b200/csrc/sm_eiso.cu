@@ -277,6 +277,11 @@ struct sm_eiso {
     int rec_dirty = 1;
     size_t elem = 4;
     KernelTimer timer;
+    // 16-bit storage: one exponent per field (total and split parts share it)
+    Scaler16 scaler;
+    std::vector<int> expo0;
+    double mat_min[2] = {0, 0};   // min rho, min vp implied by the materials
+    static constexpr int kScalePeriod = 16;
 };
 
 namespace {
@@ -315,6 +320,33 @@ void launch_gather(sm_eiso *h) {
     eiso_gather_kernel<S><<<(n + 127) / 128, 128, 0, h->stream>>>(
         h->args, h->d_rec.as<RecEntry>(), n, h->d_table.as<int32_t>(), h->table_steps,
         (long long)h->it, h->d_traces.as<double>());
+}
+
+bool eiso_is16(const sm_eiso *h) { return h->precision == SM_FP16 || h->precision == SM_BF16; }
+
+void eiso_apply_scales(sm_eiso *h) {
+    for (int f = 0; f < 5; ++f) {
+        h->args.sc[f] = std::ldexp(1.0f, h->scaler.expo[f]);
+        h->args.isc[f] = std::ldexp(1.0f, -h->scaler.expo[f]);
+    }
+}
+
+int eiso_rescale(sm_eiso *h) {
+    void *ptrs[15];
+    size_t ns[15];
+    int groups[15];
+    static const char *names[5] = {"vx", "vz", "txx", "tzz", "txz"};
+    const size_t fcells = (size_t)h->NX * h->pitch * h->nshots;
+    for (int f = 0; f < 5; ++f) {
+        ptrs[3 * f] = h->fields[f].p; ns[3 * f] = fcells; groups[3 * f] = f;
+        ptrs[3 * f + 1] = h->xpart[f].p; ns[3 * f + 1] = h->npml_cells * h->nshots; groups[3 * f + 1] = f;
+        ptrs[3 * f + 2] = h->zpart[f].p; ns[3 * f + 2] = h->npml_cells * h->nshots; groups[3 * f + 2] = f;
+    }
+    int rc = h->precision == SM_FP16
+                 ? h->scaler.check<__half>(h->stream, 15, ptrs, ns, groups, names)
+                 : h->scaler.check<__nv_bfloat16>(h->stream, 15, ptrs, ns, groups, names);
+    eiso_apply_scales(h);
+    return rc;
 }
 
 int upload_sources(sm_eiso *h) {
@@ -563,6 +595,20 @@ extern "C" int sm_eiso_create(int device, size_t nx, size_t nz, size_t npml, dou
         a.isc[f] = 1.0f;
     }
     a.prof = h->prof.p;
+    if (precision == SM_FP16 || precision == SM_BF16) {
+        if ((rc = h->scaler.init(5, 15))) return rc;
+        h->expo0.assign(5, 0);
+        // smallest impedance rho * vp over the model: rho = 1/b and
+        // vp^2 = (lambda + 2 mu) / rho at the nodes
+        double zmin = -1.0;
+        for (size_t q = 0; q < nx * nz; ++q) {
+            const double rho = 1.0 / b[q];
+            const double z = std::sqrt(std::max(l2m[q], 0.0) * rho);
+            if (zmin < 0 || z < zmin) zmin = z;
+        }
+        h->mat_min[0] = zmin > 0 ? zmin : 1.0;
+        eiso_apply_scales(h.get());
+    }
     h->shot_src.assign(nshots, {});
     h->shot_vals.assign(nshots, {});
     h->shot_rec.assign(nshots, {});
@@ -582,6 +628,10 @@ extern "C" int sm_eiso_reset(sm_eiso_t h) {
     if (int rc = h->d_traces.zero(h->stream)) return rc;
     SM_CUDA_TRY(cudaStreamSynchronize(h->stream));
     h->it = 0;
+    if (eiso_is16(h)) {
+        h->scaler.expo = h->expo0;
+        eiso_apply_scales(h);
+    }
     return SM_OK;
 }
 
@@ -619,6 +669,27 @@ extern "C" int sm_eiso_set_sources(sm_eiso_t h, size_t shot, size_t nsrc, const 
         h->shot_vals[s] = vals;
     }
     h->src_dirty = 1;
+    if (eiso_is16(h)) {
+        // starting ranges: the stress a source cell accumulates (running sum
+        // of the injected values) and the particle velocity it drives
+        // (stress / (rho vp)); the range checks refine them during the run
+        double tmax = 0.0;
+        for (size_t s = 0; s < h->nshots; ++s)
+            for (const SrcEntry &se : h->shot_src[s]) {
+                double acc = 0.0;
+                for (int t = 0; t < se.len; ++t) {
+                    acc += h->shot_vals[s][se.voff + t];
+                    tmax = std::max(tmax, std::fabs(acc));
+                }
+            }
+        const int et = Scaler16::expo_for(tmax), ev = Scaler16::expo_for(tmax / h->mat_min[0]);
+        h->expo0 = {ev, ev, et, et, et};
+        for (int g = 0; g < 5; ++g) h->scaler.ceil[g] = h->expo0[g] + 2;
+        if (h->it == 0) {
+            h->scaler.expo = h->expo0;
+            eiso_apply_scales(h);
+        }
+    }
     return SM_OK;
 }
 
@@ -673,6 +744,8 @@ extern "C" int sm_eiso_run(sm_eiso_t h, size_t nsteps) {
         default: launch_step<float>(h); launch_src<float>(h); launch_gather<float>(h); break;
         }
         h->it++;
+        if (eiso_is16(h) && h->it % sm_eiso::kScalePeriod == 0)
+            if (int rc = eiso_rescale(h)) return rc;
     }
     SM_CUDA_TRY(cudaGetLastError());
     return SM_OK;

@@ -110,3 +110,22 @@ def test_every_launch_configuration_gives_identical_results(precision):
     orc, _, fo = H.run_a3d_oracle(p, fields_at=["p"])
     assert H.rel_l2([1e3 * t for t in base[0]], orc) < TOL[precision]
     assert O.rel_l2(base[1], fo["p"]) < TOL[precision]
+
+
+# 16-bit storage (per-field power-of-two scales, FP32 arithmetic): the bound
+# is the one this storage meets on these short runs, not the FP32 bound
+TOL16 = {"fp16": 2.5e-2, "bf16": 1.5e-1}
+
+
+@pytest.mark.parametrize("precision", ["fp16", "bf16"])
+def test_16bit_storage_stays_in_range_and_close_to_fp64(precision):
+    p = W.cfg1(n=48, npml=8, nsteps=300, seed=21, rec_stride=3, nrec_side=16)
+    got = api.run_a3d(p, precision)
+    assert all(np.isfinite(t).all() for t in got)
+    ref = api.run_a3d(p, "fp64")
+    err = H.rel_l2(got, ref)
+    assert err < TOL16[precision], err
+    # the scale is a power of two: an FP16 run reproduces itself exactly
+    again = api.run_a3d(p, precision)
+    for a, b in zip(got, again):
+        np.testing.assert_array_equal(a, b)

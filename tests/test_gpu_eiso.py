@@ -137,3 +137,16 @@ def test_reset_reproduces_run_and_step_count():
     for x, y in zip(a, b):
         np.testing.assert_array_equal(x, y)
     dev.close()
+
+
+TOL16 = {"fp16": 2.5e-2, "bf16": 1.5e-1}
+
+
+@pytest.mark.parametrize("precision", ["fp16", "bf16"])
+def test_16bit_storage_stays_in_range_and_close_to_fp64(precision):
+    p = W.cfg0(nx=120, nz=100, npml=10, nsteps=400, nrec=8)
+    got = api.run_eiso(p, precision)[0]
+    assert all(np.isfinite(t).all() for t in got)
+    ref = api.run_eiso(p, "fp64")[0]
+    err = H.rel_l2(got, ref)
+    assert err < TOL16[precision], err
