@@ -798,7 +798,6 @@ extern "C" int sm_a3d_create(int device, size_t nx2, size_t ny2, size_t nz2, siz
     *out = nullptr;
     if (nx2 < 2 * np + 2 || ny2 < 2 * np + 2 || nz2 < 2 * np + 2)
         return sm_fail(SM_EINVAL, "sm_a3d_create: grid smaller than the CPML frame");
-    if (np < 1) return sm_fail(SM_EINVAL, "sm_a3d_create: np must be >= 1");
     if (!vp || !rho || !coef) return sm_fail(SM_EINVAL, "sm_a3d_create: NULL array");
     for (int c = 0; c < 18; ++c)
         if (!coef[c]) return sm_fail(SM_EINVAL, "sm_a3d_create: NULL coefficient array");

@@ -1,4 +1,302 @@
-/* placeholder, replaced below */
-#include "sm_host.h"
-int sm_e_iso_main(int argc, char **argv) { (void)argc; (void)argv; return 1; }
-int sm_a_iso_3d_main(int argc, char **argv) { (void)argc; (void)argv; return 1; }
+/*
+ * sm_drivers.c -- the e_iso and a_iso_3d programs with their time loops on
+ * the GPU: same arguments, same input files, same trace files.
+ *
+ * The set-up follows the reference drivers step by step (e_iso.c:342-587,
+ * a_iso_3d/a_iso_3d.c:240-591) in FP64 through the library's host
+ * functions; the loop (e_iso.c:589-670, a_iso_3d.c:593-741) runs through
+ * the C ABI.  Differences: errors return a non-zero status with a message
+ * instead of abort()/exit(); snapshot records (netCDF) are skipped with a
+ * warning; the 8 outer points of a 9-point source template take the
+ * centre's type (io_utils.c:1494-1535 leaves them unset).
+ */
+#include <math.h>
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+
+#include "sm_io.h"
+
+static int report(int rc, const char *prog)
+{
+    if (rc != SM_OK) fprintf(stderr, "%s: %s\n", prog, sm_last_error());
+    return rc;
+}
+
+/* trace records -> receiver arrays for the device (trace records only) */
+typedef struct {
+    size_t n;
+    size_t *index, *recno;
+    int *comp;
+    double *t0, *rdt;
+} rec_plan;
+
+static void rec_plan_free(rec_plan *r)
+{
+    free(r->index); free(r->recno); free(r->comp); free(r->t0); free(r->rdt);
+}
+
+static int write_traces(const char *base, const rec_plan *rp, const double *vals, size_t ld,
+                        const size_t *counts, double dt, size_t nsteps)
+{
+    double *t = malloc((ld ? ld : 1) * sizeof(double));
+    if (!t) return sm_fail(SM_ENOMEM, "out of host memory");
+    for (size_t r = 0; r < rp->n; ++r) {
+        size_t s = 0;
+        for (size_t it = 0; it < nsteps && s < counts[r]; ++it)
+            if (sm_sample_predicate(it, dt, rp->t0[r], rp->rdt[r])) t[s++] = dt * (it + 1);
+        int rc = sm_write_trace_file(base, rp->recno[r] + 1, t, vals + r * ld, counts[r]);
+        if (rc) { free(t); return rc; }
+    }
+    free(t);
+    return SM_OK;
+}
+
+static void check_dt_trc(const sm_record *rec, size_t nrec, double dt)
+{
+    /* io_utils.c:3561-3575 */
+    for (size_t n = 0; n < nrec; ++n)
+        if (rec[n].is_trace) {
+            double rem = fmod(1000000.0 * rec[n].dt, 1000000.0 * dt);
+            if (rem > 1.e-9) {
+                fprintf(stdout, "\n *** Warning ***\n");
+                fprintf(stdout, "Time step of receiver %zu not a multiple of modeling time step\n", n + 1);
+                fprintf(stdout, " *** Warning ***\n");
+            }
+        }
+}
+
+/* Ricker wavelets of every source (src.c:43-65); *fct is n x stride */
+static int make_wavelets(const sm_source *s, size_t n, double dt, double **fct, size_t **len,
+                         size_t *stride)
+{
+    double *A = malloc(n * sizeof(double)), *f = malloc(n * sizeof(double));
+    size_t st = 0;
+    for (size_t q = 0; q < n; ++q) {
+        A[q] = s[q].A;
+        f[q] = s[q].f;
+        size_t l = sm_ricker_length(s[q].f, dt, 1.0);
+        if (l > st) st = l;
+    }
+    *fct = calloc(n * (st ? st : 1), sizeof(double));
+    *len = calloc(n, sizeof(size_t));
+    int rc = sm_ricker(n, A, f, dt, 1.0, st, *fct, *len);
+    free(A);
+    free(f);
+    *stride = st;
+    return rc;
+}
+
+int sm_e_iso_main(int argc, char **argv)
+{
+    const char *prog = "e_iso_gpu";
+    sm_params p;
+    sm_grid g;
+    double *vp = NULL, *vs = NULL, *rho = NULL, *la = NULL, *mu = NULL, *l2m = NULL, *b = NULL, *bm = NULL;
+    double *d = NULL, *dh = NULL, *dH = NULL, *fct = NULL, *vals = NULL;
+    size_t *len = NULL, *counts = NULL;
+    sm_source *src = NULL;
+    sm_record *rec = NULL;
+    rec_plan rp = {0};
+    sm_eiso_t h = NULL;
+    size_t nsrc = 0, ntpl = 1, nrec = 0, stride = 0;
+    int rc;
+
+    sm_params_defaults(&p);
+    if ((rc = sm_parse_args(argc, argv, &p, prog))) return report(rc, prog);
+    const size_t npml = p.np;   /* e_iso.c:346: the frame is kept outside the grid */
+    if (p.verbose) fprintf(stdout, "\n *** e_iso - Elastic wave propagation in 2D isotropic media (GPU) ***\n\n");
+    if ((rc = sm_read_model_e(p.modelfile, &g, &vp, &vs, &rho))) goto out;
+    if (g.dx != g.dz) { rc = sm_fail(SM_EINVAL, "grid cell size must be equal in X and Z"); goto out; }
+    if (npml == 0) {
+        rc = sm_fail(SM_EINVAL, "e_iso needs its PML (abs 1, nl >= 1): with none the reference "
+                                "indexes outside its arrays (propagate.c:2519)");
+        goto out;
+    }
+    const double h_ = g.dx, dt = p.dt;
+    const size_t nx = g.nx, nz = g.nz, ncell = nx * nz;
+    la = malloc(ncell * sizeof(double)); mu = malloc(ncell * sizeof(double));
+    l2m = malloc(ncell * sizeof(double)); b = malloc(ncell * sizeof(double));
+    bm = malloc(ncell * sizeof(double));
+    double vpmax = 0.0;
+    if ((rc = sm_eiso_materials(nx, nz, vp, vs, rho, la, mu, l2m, b, bm, &vpmax))) goto out;
+    if (dt > h_ / (sqrt(2.0) * vpmax)) {   /* e_iso.c:476-479 */
+        rc = sm_fail(SM_ECFL, "Time step too large (dt > h / (sqrt(2) vpmax))");
+        goto out;
+    }
+    d = malloc(npml * sizeof(double)); dh = malloc(npml * sizeof(double));
+    dH = malloc((npml + 1) * sizeof(double));
+    if ((rc = sm_eiso_profiles(npml, h_, ncell, vp, d, dh, dH))) goto out;
+    if ((rc = sm_read_sources(p.sourcefile, &g, 0, &src, &nsrc, &ntpl))) goto out;
+    if ((rc = make_wavelets(src, nsrc, dt, &fct, &len, &stride))) goto out;
+    if ((rc = sm_read_records(p.outputfile, &g, 0, &rec, &nrec))) goto out;
+    check_dt_trc(rec, nrec, dt);
+    const size_t nsteps = sm_nsteps(p.duration, dt);
+
+    if ((rc = sm_eiso_create(0, nx, nz, npml, h_, dt, la, mu, l2m, b, bm, d, dh, dH, p.precision, 1, &h)))
+        goto out;
+    {   /* sources: add_src (src.c:170-184) acts on Sx, Sz, Sxz and Bulk only */
+        size_t *idx = malloc(nsrc * sizeof(size_t)), *ln = malloc(nsrc * sizeof(size_t));
+        int *ty = malloc(nsrc * sizeof(int));
+        double *w = malloc(nsrc * (stride ? stride : 1) * sizeof(double));
+        size_t m = 0;
+        for (size_t q = 0; q < nsrc; ++q) {
+            int t = src[q].type;
+            if (t != SM_SRC_SX && t != SM_SRC_SZ && t != SM_SRC_SXZ && t != SM_SRC_BULK) continue;
+            if (src[q].i < 0 || src[q].k < 0 || (size_t)src[q].i >= nx || (size_t)src[q].k >= nz) {
+                free(idx); free(ln); free(ty); free(w);
+                rc = sm_fail(SM_EINVAL, "source %zu lies outside the grid", q + 1);
+                goto out;
+            }
+            idx[m] = (size_t)src[q].i * nz + (size_t)src[q].k;
+            ty[m] = t;
+            ln[m] = len[q];
+            memcpy(w + m * stride, fct + q * stride, stride * sizeof(double));
+            ++m;
+        }
+        rc = sm_eiso_set_sources(h, 0, m, idx, ty, w, ln, stride, dt);
+        free(idx); free(ln); free(ty); free(w);
+        if (rc) goto out;
+    }
+    rp.index = malloc((nrec ? nrec : 1) * sizeof(size_t)); rp.recno = malloc((nrec ? nrec : 1) * sizeof(size_t));
+    rp.comp = malloc((nrec ? nrec : 1) * sizeof(int));
+    rp.t0 = malloc((nrec ? nrec : 1) * sizeof(double)); rp.rdt = malloc((nrec ? nrec : 1) * sizeof(double));
+    for (size_t n = 0; n < nrec; ++n) {
+        if (!rec[n].is_trace) {
+            fprintf(stderr, "%s: record %zu is a snapshot (netCDF); skipped\n", prog, n + 1);
+            continue;
+        }
+        if (rec[n].i < 0 || rec[n].k < 0 || (size_t)rec[n].i >= nx || (size_t)rec[n].k >= nz) {
+            rc = sm_fail(SM_EINVAL, "record %zu lies outside the grid", n + 1);
+            goto out;
+        }
+        rp.index[rp.n] = (size_t)rec[n].i * nz + (size_t)rec[n].k;
+        rp.comp[rp.n] = rec[n].comp;
+        rp.t0[rp.n] = rec[n].t0;
+        rp.rdt[rp.n] = rec[n].dt;
+        rp.recno[rp.n] = n;
+        rp.n++;
+    }
+    if ((rc = sm_eiso_set_receivers(h, 0, rp.n, rp.index, rp.comp, rp.t0, rp.rdt, nsteps))) goto out;
+    if (p.verbose) fprintf(stdout, "Starting main loop (%zu iterations)\n", nsteps);
+    if ((rc = sm_eiso_run(h, nsteps))) goto out;
+    counts = calloc(rp.n ? rp.n : 1, sizeof(size_t));
+    if ((rc = sm_eiso_read_traces(h, 0, 0, rp.n, NULL, 0, counts))) goto out;
+    size_t ld = 1;
+    for (size_t r = 0; r < rp.n; ++r) ld = counts[r] > ld ? counts[r] : ld;
+    vals = malloc(rp.n * ld * sizeof(double) + 1);
+    if ((rc = sm_eiso_read_traces(h, 0, 0, rp.n, vals, ld, counts))) goto out;
+    rc = write_traces(p.basename, &rp, vals, ld, counts, dt, nsteps);
+    if (p.verbose) fprintf(stdout, "\nEnd of computation\n");
+out:
+    sm_eiso_destroy(h);
+    free(vp); free(vs); free(rho); free(la); free(mu); free(l2m); free(b); free(bm);
+    free(d); free(dh); free(dH); free(fct); free(len); free(src); free(rec); free(vals); free(counts);
+    rec_plan_free(&rp);
+    return report(rc, prog);
+}
+
+int sm_a_iso_3d_main(int argc, char **argv)
+{
+    const char *prog = "a_iso_3d_gpu";
+    sm_params p;
+    sm_grid g;
+    double *vp = NULL, *rho = NULL, *vpp = NULL, *rhop = NULL, *fct = NULL, *vals = NULL;
+    double *coef[18] = {0};
+    size_t *len = NULL, *counts = NULL;
+    sm_source *src = NULL;
+    sm_record *rec = NULL;
+    rec_plan rp = {0};
+    sm_a3d_t h = NULL;
+    size_t nsrc = 0, ntpl = 1, nrec = 0, stride = 0;
+    int rc;
+
+    sm_params_defaults(&p);
+    if ((rc = sm_parse_args(argc, argv, &p, prog))) return report(rc, prog);
+    if (p.verbose) fprintf(stdout, "\n *** a_iso_3d - Acoustic wave propagation in 3D isotropic media (GPU) ***\n\n");
+    if ((rc = sm_read_model_a(p.modelfile, &g, &vp, &rho))) goto out;
+    if (g.dx != g.dz) { rc = sm_fail(SM_EINVAL, "grid cell size must be equal in X and Z"); goto out; }
+    if (p.segy) { rc = sm_fail(SM_EINVAL, "SEG-Y output (segy 1) is not supported; use segy 0"); goto out; }
+    const size_t np = p.np, nx2 = g.nx + 2 * np, ny2 = g.ny + 2 * np, nz2 = g.nz + 2 * np;
+    const size_t n3 = nx2 * ny2 * nz2;
+    const double dt = p.dt;
+    vpp = malloc(n3 * sizeof(double));
+    rhop = malloc(n3 * sizeof(double));
+    if (!vpp || !rhop) { rc = sm_fail(SM_ENOMEM, "out of host memory"); goto out; }
+    if ((rc = sm_a3d_pad_model(g.nx, g.ny, g.nz, np, vp, rho, vpp, rhop))) goto out;
+    {   /* a_iso_3d.c:368-374 and 411-417 */
+        double vpmax = sm_a3d_cfl_vpmax(g.nx, g.nz, vpp);
+        if (dt * vpmax * sqrt(1. / (g.dx * g.dx) + 1. / (g.dy * g.dy) + 1. / (g.dz * g.dz)) > 1.) {
+            rc = sm_fail(SM_ECFL, "Time step too large");
+            goto out;
+        }
+    }
+    if ((rc = sm_read_sources(p.sourcefile, &g, 1, &src, &nsrc, &ntpl))) goto out;
+    if ((rc = make_wavelets(src, nsrc, dt, &fct, &len, &stride))) goto out;
+    if ((rc = sm_read_records(p.outputfile, &g, 1, &rec, &nrec))) goto out;
+    check_dt_trc(rec, nrec, dt);
+    {
+        const size_t n2[3] = {nx2, ny2, nz2};
+        for (int c = 0; c < 18; ++c) coef[c] = malloc((c < 9 ? n2[c / 3] : n2[(c - 9) / 3]) * sizeof(double));
+        if ((rc = sm_a3d_cpml(np, nx2, ny2, nz2, g.dx, g.dy, g.dz, dt, p.pml_order, p.vmax, p.Rc,
+                              p.kappa_max, p.alpha_max, src[0].f, coef)))
+            goto out;
+    }
+    const size_t nsteps = sm_nsteps(p.duration, dt);
+    if ((rc = sm_a3d_create(0, nx2, ny2, nz2, np, g.dx, g.dy, g.dz, dt, vpp, rhop,
+                            (const double *const *)coef, p.precision, &h)))
+        goto out;
+    {   /* a_iso_3d.c:689-693: P += dt fct 1e6 for every source type */
+        size_t *idx = malloc(nsrc * sizeof(size_t));
+        for (size_t q = 0; q < nsrc; ++q) {
+            long i = src[q].i + (long)np, j = src[q].j + (long)np, k = src[q].k + (long)np;
+            if (i < 0 || j < 0 || k < 0 || (size_t)i >= nx2 || (size_t)j >= ny2 || (size_t)k >= nz2) {
+                free(idx);
+                rc = sm_fail(SM_EINVAL, "source %zu lies outside the grid", q + 1);
+                goto out;
+            }
+            idx[q] = ((size_t)i * ny2 + (size_t)j) * nz2 + (size_t)k;
+        }
+        rc = sm_a3d_set_sources(h, nsrc, idx, fct, len, stride, dt * 1.e6);
+        free(idx);
+        if (rc) goto out;
+    }
+    rp.index = malloc((nrec ? nrec : 1) * sizeof(size_t)); rp.recno = malloc((nrec ? nrec : 1) * sizeof(size_t));
+    rp.comp = malloc((nrec ? nrec : 1) * sizeof(int));
+    rp.t0 = malloc((nrec ? nrec : 1) * sizeof(double)); rp.rdt = malloc((nrec ? nrec : 1) * sizeof(double));
+    for (size_t n = 0; n < nrec; ++n) {
+        if (!rec[n].is_trace) {
+            fprintf(stderr, "%s: record %zu is a snapshot (netCDF); skipped\n", prog, n + 1);
+            continue;
+        }
+        long i = rec[n].i + (long)np, j = rec[n].j + (long)np, k = rec[n].k + (long)np;
+        if (i < 0 || j < 0 || k < 0 || (size_t)i >= nx2 || (size_t)j >= ny2 || (size_t)k >= nz2) {
+            rc = sm_fail(SM_EINVAL, "record %zu lies outside the grid", n + 1);
+            goto out;
+        }
+        rp.index[rp.n] = ((size_t)i * ny2 + (size_t)j) * nz2 + (size_t)k;
+        rp.comp[rp.n] = rec[n].comp;
+        rp.t0[rp.n] = rec[n].t0;
+        rp.rdt[rp.n] = rec[n].dt;
+        rp.recno[rp.n] = n;
+        rp.n++;
+    }
+    if ((rc = sm_a3d_set_receivers(h, rp.n, rp.index, rp.comp, rp.t0, rp.rdt, nsteps))) goto out;
+    if (p.verbose) fprintf(stdout, "Starting main loop (%zu iterations)\n", nsteps);
+    if ((rc = sm_a3d_run(h, nsteps))) goto out;
+    counts = calloc(rp.n ? rp.n : 1, sizeof(size_t));
+    if ((rc = sm_a3d_read_traces(h, 0, rp.n, NULL, 0, counts))) goto out;
+    size_t ld = 1;
+    for (size_t r = 0; r < rp.n; ++r) ld = counts[r] > ld ? counts[r] : ld;
+    vals = malloc(rp.n * ld * sizeof(double) + 1);
+    if ((rc = sm_a3d_read_traces(h, 0, rp.n, vals, ld, counts))) goto out;
+    rc = write_traces(p.basename, &rp, vals, ld, counts, dt, nsteps);
+    if (p.verbose) fprintf(stdout, "\nEnd of computation\n");
+out:
+    sm_a3d_destroy(h);
+    free(vp); free(rho); free(vpp); free(rhop); free(fct); free(len); free(src); free(rec);
+    free(vals); free(counts);
+    for (int c = 0; c < 18; ++c) free(coef[c]);
+    rec_plan_free(&rp);
+    return report(rc, prog);
+}

@@ -1,0 +1,403 @@
+/*
+ * sm_io.c -- readers of the reference's input files and its trace writer.
+ *
+ * Formats and semantics follow io_utils.c (cited per function); where the
+ * reference would read past a buffer or dereference NULL on a malformed
+ * file, these return SM_EIO with a message instead.
+ */
+#define _GNU_SOURCE
+#include "sm_io.h"
+
+#include <ctype.h>
+#include <errno.h>
+#include <getopt.h>
+#include <math.h>
+#include <stdlib.h>
+#include <string.h>
+#include <sys/stat.h>
+#include <sys/types.h>
+
+void sm_params_defaults(sm_params *p)
+{
+    /* io_utils.c:63-98 / 100-135 (the fields the two programs read) */
+    memset(p, 0, sizeof *p);
+    p->dt = 1.e-4;
+    p->duration = 1.2;
+    strcpy(p->basename, "run01");
+    p->iwipe = 0;
+    p->np = 20;
+    p->segy = 0;
+    p->shotpt_no = 1;
+    p->Rc = 1.e-5;
+    p->kappa_max = 1.;
+    p->alpha_max = 1;
+    p->vmax = 5000.0;
+    p->pml_order = 2.;
+    p->precision = SM_FP32;
+}
+
+static int parse_precision(const char *s, int *out)
+{
+    if (!strcmp(s, "fp32")) *out = SM_FP32;
+    else if (!strcmp(s, "fp64")) *out = SM_FP64;
+    else if (!strcmp(s, "fp16")) *out = SM_FP16;
+    else if (!strcmp(s, "bf16")) *out = SM_BF16;
+    else return 0;
+    return 1;
+}
+
+int sm_parse_args(int argc, char **argv, sm_params *p, const char *prog)
+{
+    /* io_utils.c:156-202: -p file.par, -v (repeatable), -h; -c (checkpoint
+     * restart) belongs to the PSTD programs and is refused here */
+    const char *par = NULL;
+    int c;
+    optind = 1;
+    while ((c = getopt(argc, argv, "c:hp:vP:")) != -1) {
+        switch (c) {
+        case 'p': par = optarg; break;
+        case 'v': p->verbose++; break;
+        case 'P':
+            if (!parse_precision(optarg, &p->precision))
+                return sm_fail(SM_EINVAL, "%s: -P takes fp32, fp64, fp16 or bf16", prog);
+            break;
+        case 'c':
+            return sm_fail(SM_EINVAL, "%s: checkpoint restart (-c) is not part of this program", prog);
+        case 'h':
+            return sm_fail(SM_EINVAL, "usage: %s [-v] [-h] [-P fp32|fp64|fp16|bf16] -p parameter_file",
+                           prog);
+        default:
+            return sm_fail(SM_EINVAL, "usage: %s [-v] [-h] [-P fp32|fp64|fp16|bf16] -p parameter_file",
+                           prog);
+        }
+    }
+    if (!par) return sm_fail(SM_EINVAL, "usage: %s [-v] [-h] -p parameter_file", prog);
+    return sm_read_par(par, p);
+}
+
+int sm_read_par(const char *path, sm_params *p)
+{
+    /* io_utils.c:204-294: "value  # keyword, comment" per line */
+    FILE *fid = fopen(path, "r");
+    if (!fid) return sm_fail(SM_EIO, "cannot open parameter file %s for reading", path);
+    char line[512], value[256], keyword[256];
+    int lineno = 0;
+    while (fgets(line, sizeof line, fid)) {
+        ++lineno;
+        if (sscanf(line, "%255s", value) <= 0) continue;
+        char *s1 = strchr(line, '#');
+        char *s2 = strchr(line, ',');
+        if (!s1 || !s2 || s2 < s1) {
+            fclose(fid);
+            return sm_fail(SM_EIO, "%s:%d: expected \"value  # keyword, comment\"", path, lineno);
+        }
+        *s2 = '\0';
+        if (sscanf(s1 + 1, "%255s", keyword) != 1) continue;
+        if (!strcmp(keyword, "model")) snprintf(p->modelfile, sizeof p->modelfile, "%s", value);
+        else if (!strcmp(keyword, "source")) snprintf(p->sourcefile, sizeof p->sourcefile, "%s", value);
+        else if (!strcmp(keyword, "output")) snprintf(p->outputfile, sizeof p->outputfile, "%s", value);
+        else if (!strcmp(keyword, "basename")) snprintf(p->basename, sizeof p->basename, "%s", value);
+        else if (!strcmp(keyword, "time")) p->duration = strtod(value, NULL);
+        else if (!strcmp(keyword, "dt")) p->dt = strtod(value, NULL) * 0.001;  /* ms -> s */
+        else if (!strcmp(keyword, "abs")) p->iwipe = (short)atoi(value);
+        else if (!strcmp(keyword, "nl")) p->np = (size_t)atoi(value);
+        else if (!strcmp(keyword, "segy")) p->segy = (short)atoi(value);
+        else if (!strcmp(keyword, "shotpoint")) p->shotpt_no = atoi(value);
+        else if (!strcmp(keyword, "Rc")) p->Rc = strtod(value, NULL);
+        else if (!strcmp(keyword, "kappa_max")) p->kappa_max = strtod(value, NULL);
+        else if (!strcmp(keyword, "alpha_max")) p->alpha_max = (short)atoi(value);
+        /* plstr, check_model, chkpt_inc, pml_median, saveEnergy, EnergyROI,
+         * simulateCMP, azimuthal_mode: accepted, unused by these programs */
+    }
+    fclose(fid);
+    if (p->iwipe == 0) p->np = 0;   /* io_utils.c:293 */
+    return SM_OK;
+}
+
+int sm_read_model_e(const char *path, sm_grid *g, double **pvp, double **pvs, double **prho)
+{
+    /* io_utils.c:296-328 (grid) and 892-947 (values; one column = 1-D profile) */
+    FILE *fid = fopen(path, "r");
+    if (!fid) return sm_fail(SM_EIO, "cannot open %s for reading", path);
+    char type[64];
+    memset(g, 0, sizeof *g);
+    g->ny = 1;
+    g->dy = 1.0;
+    if (fscanf(fid, "%zu %zu", &g->nx, &g->nz) != 2 || fscanf(fid, "%lf %lf", &g->dx, &g->dz) != 2 ||
+        fscanf(fid, "%lf %lf", &g->x0, &g->z0) != 2 || fscanf(fid, "%63s", type) != 1) {
+        fclose(fid);
+        return sm_fail(SM_EIO, "%s: bad header", path);
+    }
+    if (strcmp(type, "isotropic_elastic") != 0) {
+        fclose(fid);
+        return sm_fail(SM_EIO, "model in %s not isotropic_elastic", path);
+    }
+    const size_t nx = g->nx, nz = g->nz;
+    if (nx < 2 || nz < 2) {
+        fclose(fid);
+        return sm_fail(SM_EIO, "%s: grid must be at least 2 x 2", path);
+    }
+    double *vp = malloc(nx * nz * sizeof(double)), *vs = malloc(nx * nz * sizeof(double));
+    double *rho = malloc(nx * nz * sizeof(double));
+    if (!vp || !vs || !rho) {
+        free(vp); free(vs); free(rho); fclose(fid);
+        return sm_fail(SM_ENOMEM, "out of host memory");
+    }
+    int flag1d = 0;
+    for (size_t i = 0; i < nx && !flag1d; ++i) {
+        size_t q = i * nz;
+        int nread = fscanf(fid, "%lf %lf %lf", &vp[q], &vs[q], &rho[q]);
+        if (nread <= 0 && i == 1) { flag1d = 1; break; }
+        if (nread != 3) goto bad;
+        for (size_t j = 1; j < nz; ++j) {
+            q = i * nz + j;
+            if (fscanf(fid, "%lf %lf %lf", &vp[q], &vs[q], &rho[q]) != 3) goto bad;
+        }
+    }
+    fclose(fid);
+    if (flag1d)
+        for (size_t i = 1; i < nx; ++i)
+            for (size_t j = 0; j < nz; ++j) {
+                vp[i * nz + j] = vp[j];
+                vs[i * nz + j] = vs[j];
+                rho[i * nz + j] = rho[j];
+            }
+    *pvp = vp; *pvs = vs; *prho = rho;
+    return SM_OK;
+bad:
+    fclose(fid);
+    free(vp); free(vs); free(rho);
+    return sm_fail(SM_EIO, "something wrong with file %s", path);
+}
+
+int sm_read_model_a(const char *path, sm_grid *g, double **pvp, double **prho)
+{
+    /* io_utils.c:384-401 (grid) and 1029-1094 (values; one (x,y) column is
+     * a 1-D profile).  Returns the nx*ny*nz interior. */
+    FILE *fid = fopen(path, "r");
+    if (!fid) return sm_fail(SM_EIO, "cannot open %s for reading", path);
+    char type[64];
+    memset(g, 0, sizeof *g);
+    if (fscanf(fid, "%zu %zu %zu", &g->nx, &g->ny, &g->nz) != 3 ||
+        fscanf(fid, "%lf %lf %lf", &g->dx, &g->dy, &g->dz) != 3 ||
+        fscanf(fid, "%lf %lf %lf", &g->x0, &g->y0, &g->z0) != 3 || fscanf(fid, "%63s", type) != 1) {
+        fclose(fid);
+        return sm_fail(SM_EIO, "%s: bad header", path);
+    }
+    if (strcmp(type, "isotropic_acoustic_3d") != 0) {
+        fclose(fid);
+        return sm_fail(SM_EIO, "model in %s not isotropic_acoustic_3d", path);
+    }
+    const size_t nx = g->nx, ny = g->ny, nz = g->nz, n = nx * ny * nz;
+    if (!nx || !ny || !nz) {
+        fclose(fid);
+        return sm_fail(SM_EIO, "%s: empty grid", path);
+    }
+    double *vp = malloc(n * sizeof(double)), *rho = malloc(n * sizeof(double));
+    if (!vp || !rho) {
+        free(vp); free(rho); fclose(fid);
+        return sm_fail(SM_ENOMEM, "out of host memory");
+    }
+    int flag1d = 0;
+    for (size_t i = 0; i < nx && !flag1d; ++i)
+        for (size_t j = 0; j < ny; ++j) {
+            size_t q = (i * ny + j) * nz;
+            int nread = fscanf(fid, "%lf %lf", &vp[q], &rho[q]);
+            if (nread <= 0 && j == 1) { flag1d = 1; break; }
+            if (nread != 2) goto bad;
+            for (size_t k = 1; k < nz; ++k)
+                if (fscanf(fid, "%lf %lf", &vp[q + k], &rho[q + k]) != 2) goto bad;
+        }
+    fclose(fid);
+    if (flag1d)
+        for (size_t q = nz; q < n; ++q) {
+            vp[q] = vp[q % nz];
+            rho[q] = rho[q % nz];
+        }
+    *pvp = vp; *prho = rho;
+    return SM_OK;
+bad:
+    fclose(fid);
+    free(vp); free(rho);
+    return sm_fail(SM_EIO, "something wrong with file %s", path);
+}
+
+static int source_type(const char *t, int three_d)
+{
+    /* io_utils.c:1452-1481 (2-D) and 1561-1575 (3-D) */
+    char s[64];
+    snprintf(s, sizeof s, "%s", t);
+    struct { const char *a, *b, *c; int v; int in3d; } tab[] = {
+        {"sx", "SX", "Sx", 0, 1}, {"sz", "SZ", "Sz", 2, 1}, {"sxy", "SXY", "Sxy", 3, 0},
+        {"sxz", "SXZ", "Sxz", 4, 1}, {"srz", "SRZ", "Srz", 4, 0}, {"syz", "SYZ", "Syz", 5, 0},
+        {"sf", "SF", "Sf", 7, 1}, {"bulk", "BULK", "Bulk", 6, 1}, {"bulk_s", "BULK_S", "Bulk_s", 8, 0},
+        {"fr", "FR", "Fr", 9, 0}, {"fz", "FZ", "Fz", 11, 0}, {"ftheta", "FTHETA", "Ftheta", 10, 0},
+        {"kurkjian", "Kurkjian", "Kurkjian", 12, 0},
+    };
+    for (size_t q = 0; q < sizeof tab / sizeof tab[0]; ++q)
+        if ((!three_d || tab[q].in3d) &&
+            (!strcmp(s, tab[q].a) || !strcmp(s, tab[q].b) || !strcmp(s, tab[q].c)))
+            return tab[q].v;
+    return -1;
+}
+
+static long c_round(double v) { return lround(v); }
+
+int sm_read_sources(const char *path, const sm_grid *g, int three_d, sm_source **out,
+                    size_t *nout, size_t *ntemplate)
+{
+    /* io_utils.c:1432-1538 (2-D, 1- or 9-point template) and 1540-1589 (3-D) */
+    FILE *fid = fopen(path, "r");
+    if (!fid) return sm_fail(SM_EIO, "cannot open %s for reading", path);
+    size_t nsrc = 0, ntpl = 1;
+    if (fscanf(fid, "%zu", &nsrc) != 1 || nsrc == 0) {
+        fclose(fid);
+        return sm_fail(SM_EIO, "%s: bad source count", path);
+    }
+    if (fscanf(fid, "%zu", &ntpl) != 1) ntpl = 1;
+    if (three_d && ntpl != 1) {
+        fprintf(stdout, "Warning, source template parameter ignored.\n");
+        ntpl = 1;
+    }
+    if (ntpl != 1 && ntpl != 9) {
+        fclose(fid);
+        return sm_fail(SM_EIO, "%s: template must have 1 or 9 points", path);
+    }
+    sm_source *s = calloc(nsrc * ntpl, sizeof *s);
+    if (!s) { fclose(fid); return sm_fail(SM_ENOMEM, "out of host memory"); }
+    char t[64];
+    for (size_t n = 0; n < nsrc * ntpl; n += ntpl) {
+        if (fscanf(fid, "%63s", t) != 1) goto bad;
+        int ty = source_type(t, three_d);
+        if (ty < 0) {
+            fclose(fid); free(s);
+            return sm_fail(SM_EIO, "type of source (%s) not implemented", t);
+        }
+        s[n].type = ty;
+        if (fscanf(fid, "%lf", &s[n].A) != 1 || fscanf(fid, "%lf", &s[n].f) != 1) goto bad;
+        if (three_d) {
+            if (fscanf(fid, "%lf %lf %lf", &s[n].x, &s[n].y, &s[n].z) != 3) goto bad;
+        } else if (fscanf(fid, "%lf %lf", &s[n].x, &s[n].z) != 2) goto bad;
+        s[n].i = c_round((s[n].x - g->x0) / g->dx);
+        s[n].j = three_d ? c_round((s[n].y - g->y0) / g->dy) : 0;
+        s[n].k = c_round((s[n].z - g->z0) / g->dz);
+        if (ntpl == 9) {
+            /* io_utils.c:1494-1535: centre 1/2, edges 1/4, corners 1/8 */
+            const double A = s[n].A;
+            static const double w[9] = {0.5, 0.125, 0.25, 0.125, 0.25, 0.25, 0.125, 0.25, 0.125};
+            static const int di[9] = {0, -1, 0, 1, -1, 1, -1, 0, 1};
+            static const int dk[9] = {0, -1, -1, -1, 0, 0, 1, 1, 1};
+            for (int q = 0; q < 9; ++q) {
+                s[n + q].type = s[n].type;
+                s[n + q].f = s[n].f;
+                s[n + q].x = s[n].x;
+                s[n + q].z = s[n].z;
+                s[n + q].A = w[q] * A;
+                s[n + q].i = c_round((s[n].x - g->x0 + di[q] * g->dx) / g->dx);
+                s[n + q].k = c_round((s[n].z - g->z0 + dk[q] * g->dz) / g->dz);
+            }
+        }
+    }
+    fclose(fid);
+    *out = s;
+    *nout = nsrc * ntpl;
+    *ntemplate = ntpl;
+    return SM_OK;
+bad:
+    fclose(fid);
+    free(s);
+    return sm_fail(SM_EIO, "something wrong with file %s", path);
+}
+
+static int record_comp(const char *t, int three_d)
+{
+    /* io_utils.c:1607-1649 (2-D) and 1699-1711 (3-D) */
+    struct { const char *a, *b, *c; int v; int in3d; } tab[] = {
+        {"Vx", "vx", "VX", 0, 1}, {"Vy", "vy", "VY", 1, 1}, {"Vz", "vz", "VZ", 2, 1},
+        {"Qx", "qx", "QX", 3, 0}, {"Qz", "qz", "QZ", 4, 0}, {"txx", "TXX", "TXX", 5, 0},
+        {"tzz", "TZZ", "TZZ", 6, 0}, {"txy", "TXY", "TXY", 9, 0}, {"tyz", "TYZ", "TYZ", 10, 0},
+        {"txz", "TXZ", "TXZ", 7, 0}, {"p", "P", "P", 8, 1}, {"div", "Div", "DIV", 11, 0},
+        {"curl", "Curl", "CURL", 12, 0},
+    };
+    for (size_t q = 0; q < sizeof tab / sizeof tab[0]; ++q)
+        if ((!three_d || tab[q].in3d) &&
+            (!strcmp(t, tab[q].a) || !strcmp(t, tab[q].b) || !strcmp(t, tab[q].c)))
+            return tab[q].v;
+    return -1;
+}
+
+int sm_read_records(const char *path, const sm_grid *g, int three_d, sm_record **out, size_t *nout)
+{
+    /* io_utils.c:1592-1682 (2-D) and 1684-1741 (3-D) */
+    FILE *fid = fopen(path, "r");
+    if (!fid) return sm_fail(SM_EIO, "cannot open %s for reading", path);
+    size_t nrec = 0;
+    if (fscanf(fid, "%zu", &nrec) != 1) {
+        fclose(fid);
+        return sm_fail(SM_EIO, "%s: bad record count", path);
+    }
+    sm_record *r = calloc(nrec ? nrec : 1, sizeof *r);
+    if (!r) { fclose(fid); return sm_fail(SM_ENOMEM, "out of host memory"); }
+    char t[80];
+    for (size_t n = 0; n < nrec; ++n) {
+        if (fscanf(fid, "%79s", t) != 1) goto bad;
+        int c = record_comp(t, three_d);
+        if (c < 0) {
+            fclose(fid); free(r);
+            return sm_fail(SM_EIO, "particle velocity component (%s) does not exists", t);
+        }
+        r[n].comp = c;
+        if (fscanf(fid, "%79s", t) != 1) goto bad;
+        if (!strcmp(t, "Trace") || !strcmp(t, "trace") || !strcmp(t, "TRACE")) {
+            r[n].is_trace = 1;
+            if (three_d) {
+                if (fscanf(fid, "%lf %lf %lf", &r[n].x, &r[n].y, &r[n].z) != 3) goto bad;
+            } else if (fscanf(fid, "%lf %lf", &r[n].x, &r[n].z) != 2) goto bad;
+            if (fscanf(fid, "%lf", &r[n].t0) != 1 || fscanf(fid, "%lf", &r[n].dt) != 1) goto bad;
+            r[n].dt *= 1.e-3;   /* ms -> s */
+            r[n].i = c_round((r[n].x - g->x0) / g->dx);
+            r[n].j = three_d ? c_round((r[n].y - g->y0) / g->dy) : 0;
+            r[n].k = c_round((r[n].z - g->z0) / g->dz);
+        } else if (!strcmp(t, "Snapshot") || !strcmp(t, "snapshot") || !strcmp(t, "SNAPSHOT")) {
+            r[n].is_trace = 0;
+            if (fscanf(fid, "%lf", &r[n].t0) != 1 || fscanf(fid, "%lf", &r[n].dt) != 1) goto bad;
+            r[n].dt *= 1.e-3;
+        } else {
+            fclose(fid); free(r);
+            return sm_fail(SM_EIO, "type of record (%s) not implemented", t);
+        }
+    }
+    fclose(fid);
+    *out = r;
+    *nout = nrec;
+    return SM_OK;
+bad:
+    fclose(fid);
+    free(r);
+    return sm_fail(SM_EIO, "something wrong with file %s", path);
+}
+
+static int ensure_dir(const char *d)
+{
+    struct stat sb;
+    if (stat(d, &sb) == 0) return S_ISDIR(sb.st_mode) ? SM_OK : sm_fail(SM_EIO, "%s is not a directory", d);
+    if (mkdir(d, S_IRWXU) != 0 && errno != EEXIST)
+        return sm_fail(SM_EIO, "cannot create %s (%s)", d, strerror(errno));
+    return SM_OK;
+}
+
+int sm_write_trace_file(const char *base, size_t n, const double *t, const double *v, size_t ns)
+{
+    /* io_utils.c:1744-1768 */
+    char path[512];
+    int rc;
+    if ((rc = ensure_dir("trc"))) return rc;
+    snprintf(path, sizeof path, "trc/%s", base);
+    if ((rc = ensure_dir(path))) return rc;
+    snprintf(path, sizeof path, "trc/%s/%s_%zu.trc", base, base, n);
+    FILE *f = fopen(path, "w+");
+    if (!f) return sm_fail(SM_EIO, "cannot open %s for output (%s)", path, strerror(errno));
+    for (size_t s = 0; s < ns; ++s) fprintf(f, "%le    %le\n", t[s], 1.e3 * v[s]);
+    if (fclose(f) != 0) return sm_fail(SM_EIO, "write error on %s", path);
+    return SM_OK;
+}

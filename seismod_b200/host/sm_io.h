@@ -1,0 +1,72 @@
+/*
+ * sm_io.h -- readers of the reference's input files and the trace writer,
+ * for the drop-in programs (sm_drivers.c).  Same formats and semantics as
+ * io_utils.c; failures return a status instead of exiting.
+ */
+#ifndef SM_IO_H
+#define SM_IO_H
+
+#include <stddef.h>
+#include <stdio.h>
+
+#include "sm_host.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* inputParams + abs_params, structs.h:49-60, 80-105 (the fields this path uses) */
+typedef struct {
+    double dt;           /* s (the file holds ms) */
+    double duration;     /* s */
+    char modelfile[256], sourcefile[256], outputfile[256], basename[256];
+    int iwipe;           /* "abs" */
+    size_t np;           /* "nl" */
+    int segy, shotpt_no;
+    double Rc, kappa_max, vmax, pml_order;
+    int alpha_max;
+    int verbose;
+    int precision;       /* SM_FP32 by default; "-P" */
+} sm_params;
+
+typedef struct {
+    size_t nx, ny, nz;   /* ny = 1 for 2-D models */
+    double dx, dy, dz, x0, y0, z0;
+} sm_grid;
+
+typedef struct {
+    int type;            /* enum sourceType numbering (SM_SRC_*) */
+    double A, f, x, y, z;
+    long i, j, k;        /* node indices (interior, before any padding) */
+} sm_source;
+
+typedef struct {
+    int comp;            /* enum component numbering (SM_VX ...) */
+    int is_trace;        /* 0: snapshot record */
+    double x, y, z, t0, dt;
+    long i, j, k;
+} sm_record;
+
+/* defaults of set_defaults / set_defaults_3d (io_utils.c:63-135) */
+void sm_params_defaults(sm_params *p);
+/* command line + parameter file, io_utils.c:156-294 ("-P" added) */
+int sm_parse_args(int argc, char **argv, sm_params *p, const char *prog);
+int sm_read_par(const char *path, sm_params *p);
+/* model files: e_iso (io_utils.c:296-328, 892-947) and a_iso_3d
+ * (io_utils.c:384-401, 1029-1153, interior values only: padding is done by
+ * sm_a3d_pad_model).  Arrays are malloc'ed; the caller frees them. */
+int sm_read_model_e(const char *path, sm_grid *g, double **vp, double **vs, double **rho);
+int sm_read_model_a(const char *path, sm_grid *g, double **vp, double **rho);
+/* source and output files (io_utils.c:1432-1741); *src / *rec malloc'ed */
+int sm_read_sources(const char *path, const sm_grid *g, int three_d, sm_source **src,
+                    size_t *nsrc, size_t *ntemplate);
+int sm_read_records(const char *path, const sm_grid *g, int three_d, sm_record **rec,
+                    size_t *nrec);
+/* trc/<base>/<base>_<n>.trc, "%le    %le" of t and 1e3 * v (io_utils.c:1744-1768) */
+int sm_write_trace_file(const char *base, size_t n, const double *t, const double *v,
+                        size_t ns);
+
+#ifdef __cplusplus
+}
+#endif
+#endif
