@@ -177,6 +177,15 @@ int sm_eiso_reset(sm_eiso_t h);
 int sm_eiso_destroy(sm_eiso_t h);
 /* the cudaStream_t the handle launches on (for timing with CUDA events) */
 int sm_eiso_stream(sm_eiso_t h, void **stream);
+/* Rows of x each warp of the fused step kernel marches through (>= 1; 0
+ * restores the automatic choice, which gives every SM about 48 warps).
+ * Results do not depend on it.  get_chunk returns the value in use. */
+int sm_eiso_set_chunk(sm_eiso_t h, int chunk);
+int sm_eiso_get_chunk(sm_eiso_t h, int *chunk);
+/* launch configuration of the step kernel (warps per CTA, register cap),
+ * an index in [0, *nconfigs); results do not depend on it */
+int sm_eiso_set_config(sm_eiso_t h, int config);
+int sm_eiso_get_config(sm_eiso_t h, int *config, int *nconfigs);
 /* Per-kernel timing.  With timing on, every launch of the wavefield update
  * kernel(s) is bracketed by CUDA events on the handle's stream;
  * sm_eiso_kernel_stats synchronises and returns their summed duration and

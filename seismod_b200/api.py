@@ -180,6 +180,23 @@ class EIsoDevice:
     def set_timing(self, on=True):
         L.check(L.load().sm_eiso_set_timing(self._h, 1 if on else 0))
 
+    def set_chunk(self, chunk):
+        L.check(L.load().sm_eiso_set_chunk(self._h, int(chunk)))
+
+    def get_chunk(self):
+        c = C.c_int()
+        L.check(L.load().sm_eiso_get_chunk(self._h, C.byref(c)))
+        return c.value
+
+    def set_config(self, config):
+        L.check(L.load().sm_eiso_set_config(self._h, int(config)))
+
+    def get_config(self):
+        """(current config, number of configs)."""
+        c, n = C.c_int(), C.c_int()
+        L.check(L.load().sm_eiso_get_config(self._h, C.byref(c), C.byref(n)))
+        return c.value, n.value
+
     def kernel_stats(self, reset=False):
         """(summed update-kernel ms, timed launches, all kernel launches)."""
         ms = C.c_double()

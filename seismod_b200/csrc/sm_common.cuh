@@ -273,6 +273,11 @@ __device__ __forceinline__ double r_quot(double num, double den) { return __ddiv
 __device__ __forceinline__ unsigned smem_u32(const void *p) {
     return static_cast<unsigned>(__cvta_generic_to_shared(p));
 }
+// hint: bring the line holding p into L2 (p must be a valid global address)
+__device__ __forceinline__ void prefetch_l2(const void *p) {
+    asm volatile("prefetch.global.L2 [%0];" ::"l"(p));
+}
+
 __device__ __forceinline__ void mbar_init(uint64_t *bar, unsigned count) {
     asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(smem_u32(bar)), "r"(count)
                  : "memory");

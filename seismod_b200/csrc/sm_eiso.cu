@@ -54,9 +54,15 @@ struct EisoArgs {
     long long fstride;   // elements between shots, field arrays
     long long sstride;   // elements between shots, split arrays
     int mid_off, right_off;
-    void *f[5];
-    void *fx[5];
+    void *f[5];          // wavefields read this step (totals)
+    void *fx[5];         // ... and their x / z split parts in the frame
     void *fz[5];
+    void *fo[5];         // written this step (the other buffer set)
+    void *fxo[5];
+    void *fzo[5];
+    int chunk;           // rows (x) each warp marches through
+    int pfd;             // rows ahead the march asks L2 to fetch (0: none)
+    int *err;            // set by a bounded wait that gave up
     const void *mat[5];
     const void *prof;
     float sc[5], isc[5];
@@ -72,115 +78,539 @@ __device__ __forceinline__ int e_pml_index(const EisoArgs &a, int X, int Z) {
     return a.mid_off + (X - a.np) * 2 * a.np + (Z < a.np ? Z : Z - a.nz);
 }
 
-template <typename S>
-__global__ void __launch_bounds__(256) eiso_velocity_kernel(EisoArgs a) {
-    using C = typename Store<S>::C;
+// values of one grid row (x = X) at this lane's z: the five wavefields of
+// the old state and the five (scaled) materials
+template <typename C>
+struct ERow {
+    C txx, tzz, txz, vx, vz, b, bm, la, l2m, mu;
+};
+
+template <typename S, typename C = typename Store<S>::C>
+__device__ __forceinline__ ERow<C> e_load_row(const EisoArgs &a, long long fb, int X, int Z) {
+    ERow<C> r;
     using St = Store<S>;
-    const int Z = blockIdx.x * blockDim.x + threadIdx.x;
-    const int X = blockIdx.y * blockDim.y + threadIdx.y;
-    if (X >= a.NX || Z >= a.NZ) return;
-    const long long fb = (long long)blockIdx.z * a.fstride;
-    const long long q = (long long)X * a.pitch + Z;
-    const S *txx = static_cast<const S *>(a.f[F_TXX]) + fb;
-    const S *tzz = static_cast<const S *>(a.f[F_TZZ]) + fb;
-    const S *txz = static_cast<const S *>(a.f[F_TXZ]) + fb;
-    S *vx = static_cast<S *>(a.f[F_VX]) + fb;
-    S *vz = static_cast<S *>(a.f[F_VZ]) + fb;
-    const C zero = C(0);
-    // vx at (X, Z): backward x of txx, backward z of txz
-    const C txx_c = St::ld(txx + q, a.isc[F_TXX]);
-    const C txx_m = X > 0 ? St::ld(txx + q - a.pitch, a.isc[F_TXX]) : zero;
-    const C txz_c = St::ld(txz + q, a.isc[F_TXZ]);
-    const C txz_zm = Z > 0 ? St::ld(txz + q - 1, a.isc[F_TXZ]) : zero;
-    // vz at (X+1/2, Z+1/2): forward x of txz, forward z of tzz
-    const C txz_xp = X + 1 < a.NX ? St::ld(txz + q + a.pitch, a.isc[F_TXZ]) : zero;
-    const C tzz_c = St::ld(tzz + q, a.isc[F_TZZ]);
-    const C tzz_zp = Z + 1 < a.NZ ? St::ld(tzz + q + 1, a.isc[F_TZZ]) : zero;
-    const C ax = txx_c - txx_m, az = txz_c - txz_zm;
-    const C bx = txz_xp - txz_c, bz = tzz_zp - tzz_c;
-    const C mb = static_cast<const C *>(a.mat[M_B])[q];
-    const C mbm = static_cast<const C *>(a.mat[M_BM])[q];
-    if (e_inside(a, X, Z)) {
-        St::st(vx + q, St::ld(vx + q, a.isc[F_VX]) + mb * (ax + az), a.sc[F_VX]);
-        St::st(vz + q, St::ld(vz + q, a.isc[F_VZ]) + mbm * (bx + bz), a.sc[F_VZ]);
-        return;
+    if (X < 0 || X >= a.NX || Z < 0 || Z >= a.NZ) {
+        r.txx = r.tzz = r.txz = r.vx = r.vz = C(0);
+        r.b = r.bm = r.la = r.l2m = r.mu = C(0);
+        return r;
     }
-    const C *pr = static_cast<const C *>(a.prof);
-    const EisoProf P{a.NX, a.NZ};
-    const long long sb = (long long)blockIdx.z * a.sstride;
-    const long long c = sb + e_pml_index(a, X, Z);
-    S *vxx = static_cast<S *>(a.fx[F_VX]), *vxz = static_cast<S *>(a.fz[F_VX]);
-    S *vzx = static_cast<S *>(a.fx[F_VZ]), *vzz = static_cast<S *>(a.fz[F_VZ]);
-    const C px = pr[P.axn() + X] * St::ld(vxx + c, a.isc[F_VX]) + pr[P.bxn() + X] * (mb * ax);
-    const C pz = pr[P.azn() + Z] * St::ld(vxz + c, a.isc[F_VX]) + pr[P.bzn() + Z] * (mb * az);
-    const C qx = pr[P.axh() + X] * St::ld(vzx + c, a.isc[F_VZ]) + pr[P.bxh() + X] * (mbm * bx);
-    const C qz = pr[P.azh() + Z] * St::ld(vzz + c, a.isc[F_VZ]) + pr[P.bzh() + Z] * (mbm * bz);
-    St::st(vxx + c, px, a.sc[F_VX]);
-    St::st(vxz + c, pz, a.sc[F_VX]);
-    St::st(vzx + c, qx, a.sc[F_VZ]);
-    St::st(vzz + c, qz, a.sc[F_VZ]);
-    St::st(vx + q, px + pz, a.sc[F_VX]);
-    St::st(vz + q, qx + qz, a.sc[F_VZ]);
+    const long long q = (long long)X * a.pitch + Z;
+    r.txx = St::ld(static_cast<const S *>(a.f[F_TXX]) + fb + q, a.isc[F_TXX]);
+    r.tzz = St::ld(static_cast<const S *>(a.f[F_TZZ]) + fb + q, a.isc[F_TZZ]);
+    r.txz = St::ld(static_cast<const S *>(a.f[F_TXZ]) + fb + q, a.isc[F_TXZ]);
+    r.vx = St::ld(static_cast<const S *>(a.f[F_VX]) + fb + q, a.isc[F_VX]);
+    r.vz = St::ld(static_cast<const S *>(a.f[F_VZ]) + fb + q, a.isc[F_VZ]);
+    r.b = static_cast<const C *>(a.mat[M_B])[q];
+    r.bm = static_cast<const C *>(a.mat[M_BM])[q];
+    r.la = static_cast<const C *>(a.mat[M_LA])[q];
+    r.l2m = static_cast<const C *>(a.mat[M_L2M])[q];
+    r.mu = static_cast<const C *>(a.mat[M_MU])[q];
+    return r;
 }
 
-template <typename S>
-__global__ void __launch_bounds__(256) eiso_stress_kernel(EisoArgs a) {
-    using C = typename Store<S>::C;
+// e_load_row for a row and lane known to lie on the grid
+template <typename S, typename C = typename Store<S>::C>
+__device__ __forceinline__ ERow<C> e_load_row_in(const EisoArgs &a, long long fb, int X, int Z) {
+    ERow<C> r;
     using St = Store<S>;
-    const int Z = blockIdx.x * blockDim.x + threadIdx.x;
-    const int X = blockIdx.y * blockDim.y + threadIdx.y;
-    if (X >= a.NX || Z >= a.NZ) return;
-    const long long fb = (long long)blockIdx.z * a.fstride;
     const long long q = (long long)X * a.pitch + Z;
-    const S *vx = static_cast<const S *>(a.f[F_VX]) + fb;
-    const S *vz = static_cast<const S *>(a.f[F_VZ]) + fb;
-    S *txx = static_cast<S *>(a.f[F_TXX]) + fb;
-    S *tzz = static_cast<S *>(a.f[F_TZZ]) + fb;
-    S *txz = static_cast<S *>(a.f[F_TXZ]) + fb;
-    const C zero = C(0);
-    const C vx_c = St::ld(vx + q, a.isc[F_VX]);
-    const C vx_xp = X + 1 < a.NX ? St::ld(vx + q + a.pitch, a.isc[F_VX]) : zero;
-    const C vx_zp = Z + 1 < a.NZ ? St::ld(vx + q + 1, a.isc[F_VX]) : zero;
-    const C vz_c = St::ld(vz + q, a.isc[F_VZ]);
-    const C vz_zm = Z > 0 ? St::ld(vz + q - 1, a.isc[F_VZ]) : zero;
-    const C vz_xm = X > 0 ? St::ld(vz + q - a.pitch, a.isc[F_VZ]) : zero;
-    // txx, tzz at (X+1/2, Z): forward x of vx, backward z of vz
-    const C ax = vx_xp - vx_c, az = vz_c - vz_zm;
-    // txz at (X, Z+1/2): forward z of vx, backward x of vz
-    const C bz = vx_zp - vx_c, bx = vz_c - vz_xm;
-    const C la = static_cast<const C *>(a.mat[M_LA])[q];
-    const C l2m = static_cast<const C *>(a.mat[M_L2M])[q];
-    const C mu = static_cast<const C *>(a.mat[M_MU])[q];
-    if (e_inside(a, X, Z)) {
-        St::st(txx + q, St::ld(txx + q, a.isc[F_TXX]) + (l2m * ax + la * az), a.sc[F_TXX]);
-        St::st(tzz + q, St::ld(tzz + q, a.isc[F_TZZ]) + (l2m * az + la * ax), a.sc[F_TZZ]);
-        St::st(txz + q, St::ld(txz + q, a.isc[F_TXZ]) + mu * (bz + bx), a.sc[F_TXZ]);
-        return;
+    r.txx = St::ld(static_cast<const S *>(a.f[F_TXX]) + fb + q, a.isc[F_TXX]);
+    r.tzz = St::ld(static_cast<const S *>(a.f[F_TZZ]) + fb + q, a.isc[F_TZZ]);
+    r.txz = St::ld(static_cast<const S *>(a.f[F_TXZ]) + fb + q, a.isc[F_TXZ]);
+    r.vx = St::ld(static_cast<const S *>(a.f[F_VX]) + fb + q, a.isc[F_VX]);
+    r.vz = St::ld(static_cast<const S *>(a.f[F_VZ]) + fb + q, a.isc[F_VZ]);
+    r.b = static_cast<const C *>(a.mat[M_B])[q];
+    r.bm = static_cast<const C *>(a.mat[M_BM])[q];
+    r.la = static_cast<const C *>(a.mat[M_LA])[q];
+    r.l2m = static_cast<const C *>(a.mat[M_L2M])[q];
+    r.mu = static_cast<const C *>(a.mat[M_MU])[q];
+    return r;
+}
+
+// ask L2 for row X (fields of the old state and materials) of this lane
+template <typename S, typename C>
+__device__ __forceinline__ void e_prefetch_row(const EisoArgs &a, long long fb, int X, int Z) {
+    const long long q = (long long)X * a.pitch + Z;
+#pragma unroll
+    for (int f = 0; f < 5; ++f) prefetch_l2(static_cast<const S *>(a.f[f]) + fb + q);
+#pragma unroll
+    for (int m = 0; m < 5; ++m) prefetch_l2(static_cast<const C *>(a.mat[m]) + q);
+}
+
+// One march iteration at row X for a warp whose cells and rows X-1 .. X+3
+// all lie inside the interior-update region: no frame test, no bounds test.
+// c, n = rows X, X+1; row X+3 is loaded into `ahead`.  The arithmetic is the
+// general iteration's interior branch, operation for operation.
+template <typename S, typename C>
+__device__ __forceinline__ void e_fast_row(const EisoArgs &a, long long fb, int X, int Z, bool own,
+                                           const ERow<C> &c, const ERow<C> &n, ERow<C> &ahead,
+                                           C &vxc, C &vzp) {
+    using St = Store<S>;
+    const unsigned full = 0xffffffffu;
+    ahead = e_load_row_in<S, C>(a, fb, X + 3, Z);
+    if (a.pfd > 0 && X + a.pfd < a.NX) e_prefetch_row<S, C>(a, fb, X + a.pfd, Z);
+    const C txz_zm = __shfl_up_sync(full, n.txz, 1);
+    const C tzz_zp = __shfl_down_sync(full, c.tzz, 1);
+    const C ax = r_sub(n.txx, c.txx), az = r_sub(n.txz, txz_zm);
+    const C bx = r_sub(n.txz, c.txz), bz = r_sub(tzz_zp, c.tzz);
+    const C vxn = r_fma(n.b, r_add(ax, az), n.vx);
+    const C vzn = r_fma(c.bm, r_add(bx, bz), c.vz);
+    const C vz_zm = __shfl_up_sync(full, vzn, 1);
+    const C vx_zp = __shfl_down_sync(full, vxc, 1);
+    const C sax = r_sub(vxn, vxc), saz = r_sub(vzn, vz_zm);
+    const C sbz = r_sub(vx_zp, vxc), sbx = r_sub(vzn, vzp);
+    const C txx = r_add(c.txx, r_fma(c.l2m, sax, r_mul(c.la, saz)));
+    const C tzz = r_add(c.tzz, r_fma(c.l2m, saz, r_mul(c.la, sax)));
+    const C txz = r_fma(c.mu, r_add(sbz, sbx), c.txz);
+    if (own) {
+        const long long q = fb + (long long)X * a.pitch + Z;
+        St::st(static_cast<S *>(a.fo[F_VX]) + q + a.pitch, vxn, a.sc[F_VX]);
+        St::st(static_cast<S *>(a.fo[F_VZ]) + q, vzn, a.sc[F_VZ]);
+        St::st(static_cast<S *>(a.fo[F_TXX]) + q, txx, a.sc[F_TXX]);
+        St::st(static_cast<S *>(a.fo[F_TZZ]) + q, tzz, a.sc[F_TZZ]);
+        St::st(static_cast<S *>(a.fo[F_TXZ]) + q, txz, a.sc[F_TXZ]);
     }
+    vxc = vxn;
+    vzp = vzn;
+}
+
+// split-part update in the frame: q' = A q + B (m * delta)  (pml.c, see above)
+template <typename C>
+__device__ __forceinline__ C e_split(C A, C B, C q, C m, C delta) {
+    return r_fma(A, q, r_mul(B, r_mul(m, delta)));
+}
+
+// The old x / z split parts one march iteration at row X needs: vx at
+// (X+1, Z), vz and the three stresses at (X, Z); zero where the cell is not
+// in the frame.  Loaded one iteration ahead, like the rows.
+template <typename C>
+struct ESplit {
+    C vx[2], vz[2], t[6];   // t: txx x, txx z, tzz x, tzz z, txz x, txz z
+};
+
+template <typename S, typename C>
+__device__ __forceinline__ void e_load_split(const EisoArgs &a, long long sb, int X, int Z,
+                                             bool zin, ESplit<C> &s) {
+    using St = Store<S>;
+    s.vx[0] = s.vx[1] = s.vz[0] = s.vz[1] = C(0);
+#pragma unroll
+    for (int k = 0; k < 6; ++k) s.t[k] = C(0);
+    if (!zin) return;
+    if (X + 1 >= 0 && X + 1 < a.NX && !e_inside(a, X + 1, Z)) {
+        const long long c = sb + e_pml_index(a, X + 1, Z);
+        s.vx[0] = St::ld(static_cast<const S *>(a.fx[F_VX]) + c, a.isc[F_VX]);
+        s.vx[1] = St::ld(static_cast<const S *>(a.fz[F_VX]) + c, a.isc[F_VX]);
+    }
+    if (X >= 0 && X < a.NX && !e_inside(a, X, Z)) {
+        const long long c = sb + e_pml_index(a, X, Z);
+        s.vz[0] = St::ld(static_cast<const S *>(a.fx[F_VZ]) + c, a.isc[F_VZ]);
+        s.vz[1] = St::ld(static_cast<const S *>(a.fz[F_VZ]) + c, a.isc[F_VZ]);
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+            const int f = F_TXX + k;
+            s.t[2 * k] = St::ld(static_cast<const S *>(a.fx[f]) + c, a.isc[f]);
+            s.t[2 * k + 1] = St::ld(static_cast<const S *>(a.fz[f]) + c, a.isc[f]);
+        }
+    }
+}
+
+// a frame cell's two split parts, updated, optionally stored to the new set;
+// returns their sum, the total
+template <typename S, typename C>
+__device__ __forceinline__ C e_frame(const EisoArgs &a, int f, long long c, C Ax, C Bx, C Az,
+                                     C Bz, C qx, C qz, C mx, C mz, C dx, C dz, bool store) {
+    using St = Store<S>;
+    const C px = e_split<C>(Ax, Bx, qx, mx, dx);
+    const C pz = e_split<C>(Az, Bz, qz, mz, dz);
+    if (store) {
+        St::st(static_cast<S *>(a.fxo[f]) + c, px, a.sc[f]);
+        St::st(static_cast<S *>(a.fzo[f]) + c, pz, a.sc[f]);
+    }
+    return r_add(px, pz);
+}
+
+// z profiles of one lane's cell: A / B at the node and at the half node
+template <typename C>
+struct EZProf {
+    C An, Bn, Ah, Bh;
+};
+
+// vx at (X, Z) from its x / z differences of txx / txz (propagate.c:2511-2550,
+// pml.c:39-360); q = the old split parts
+template <typename S, typename C>
+__device__ __forceinline__ C e_vx(const EisoArgs &a, long long sb, int X, int Z, C vold, C mb,
+                                  C ax, C az, const C *q, const EZProf<C> &zp, bool store) {
+    if (e_inside(a, X, Z)) return r_fma(mb, r_add(ax, az), vold);
     const C *pr = static_cast<const C *>(a.prof);
     const EisoProf P{a.NX, a.NZ};
+    return e_frame<S, C>(a, F_VX, sb + e_pml_index(a, X, Z), pr[P.axn() + X], pr[P.bxn() + X],
+                         zp.An, zp.Bn, q[0], q[1], mb, mb, ax, az, store);
+}
+
+// vz at (X+1/2, Z+1/2) (propagate.c:2552-2588, pml.c:371-680)
+template <typename S, typename C>
+__device__ __forceinline__ C e_vz(const EisoArgs &a, long long sb, int X, int Z, C vold, C mbm,
+                                  C bx, C bz, const C *q, const EZProf<C> &zp, bool store) {
+    if (e_inside(a, X, Z)) return r_fma(mbm, r_add(bx, bz), vold);
+    const C *pr = static_cast<const C *>(a.prof);
+    const EisoProf P{a.NX, a.NZ};
+    return e_frame<S, C>(a, F_VZ, sb + e_pml_index(a, X, Z), pr[P.axh() + X], pr[P.bxh() + X],
+                         zp.Ah, zp.Bh, q[0], q[1], mbm, mbm, bx, bz, store);
+}
+
+// One time step, fused (e_iso.c:595-636).  Each warp owns 30 consecutive z
+// cells of one shot and marches along x over rows [X0, X1); lane l computes
+// z = Z0 - 1 + l, lanes 0 and 31 being the halo cells, so every z neighbour
+// comes from a warp shuffle and warps never wait on one another.
+// Iteration X computes vx of row X+1 and vz of row X (velocity half step),
+// then txx, tzz, txz of row X (stress half step) from them, with vx of row
+// X and vz of row X-1 carried in registers.  Rows are prefetched two ahead,
+// frame split parts one ahead.  Old and new state live in separate buffer
+// sets (ping-pong), so halo reads of neighbouring warps' cells never race
+// with their writes.
+template <typename S, int W, int MINB>
+__global__ void __launch_bounds__(32 * W, MINB) eiso_step_kernel(const EisoArgs a) {
+    using C = typename Store<S>::C;
+    using St = Store<S>;
+    const int lane = threadIdx.x & 31;
+    const int wcol = blockIdx.x * W + (threadIdx.x >> 5);
+    const int Z0 = wcol * 30;
+    if (Z0 >= a.NZ) return;                          // whole warp idle
+    const int Z = Z0 - 1 + lane;
+    const bool zin = Z >= 0 && Z < a.NZ;
+    const bool own = lane >= 1 && lane <= 30 && Z < a.NZ;
+    const int X0 = blockIdx.y * a.chunk;
+    const int X1 = min(X0 + a.chunk, a.NX);
+    const long long fb = (long long)blockIdx.z * a.fstride;
     const long long sb = (long long)blockIdx.z * a.sstride;
-    const long long c = sb + e_pml_index(a, X, Z);
-    S *xxx = static_cast<S *>(a.fx[F_TXX]), *xxz = static_cast<S *>(a.fz[F_TXX]);
-    S *zzx = static_cast<S *>(a.fx[F_TZZ]), *zzz = static_cast<S *>(a.fz[F_TZZ]);
-    S *xzx = static_cast<S *>(a.fx[F_TXZ]), *xzz = static_cast<S *>(a.fz[F_TXZ]);
-    const C Axh = pr[P.axh() + X], Bxh = pr[P.bxh() + X];
-    const C Azn = pr[P.azn() + Z], Bzn = pr[P.bzn() + Z];
-    const C s1 = Axh * St::ld(xxx + c, a.isc[F_TXX]) + Bxh * (l2m * ax);
-    const C s2 = Azn * St::ld(xxz + c, a.isc[F_TXX]) + Bzn * (la * az);
-    const C s3 = Axh * St::ld(zzx + c, a.isc[F_TZZ]) + Bxh * (la * ax);
-    const C s4 = Azn * St::ld(zzz + c, a.isc[F_TZZ]) + Bzn * (l2m * az);
-    const C s5 = pr[P.axn() + X] * St::ld(xzx + c, a.isc[F_TXZ]) + pr[P.bxn() + X] * (mu * bx);
-    const C s6 = pr[P.azh() + Z] * St::ld(xzz + c, a.isc[F_TXZ]) + pr[P.bzh() + Z] * (mu * bz);
-    St::st(xxx + c, s1, a.sc[F_TXX]);
-    St::st(xxz + c, s2, a.sc[F_TXX]);
-    St::st(zzx + c, s3, a.sc[F_TZZ]);
-    St::st(zzz + c, s4, a.sc[F_TZZ]);
-    St::st(xzx + c, s5, a.sc[F_TXZ]);
-    St::st(xzz + c, s6, a.sc[F_TXZ]);
-    St::st(txx + q, s1 + s2, a.sc[F_TXX]);
-    St::st(tzz + q, s3 + s4, a.sc[F_TZZ]);
-    St::st(txz + q, s5 + s6, a.sc[F_TXZ]);
+    const unsigned full = 0xffffffffu;
+    const C zero = C(0);
+    // a warp whose 32 cells all lie inside the frame's interior in z takes
+    // the lean path on rows that are interior in x
+    const bool zint = (Z0 - 1 >= a.np) && (Z0 + 30 <= a.np + a.nz - 1);
+    S *vxo = static_cast<S *>(a.fo[F_VX]) + fb;
+    S *vzo = static_cast<S *>(a.fo[F_VZ]) + fb;
+    S *txxo = static_cast<S *>(a.fo[F_TXX]) + fb;
+    S *tzzo = static_cast<S *>(a.fo[F_TZZ]) + fb;
+    S *txzo = static_cast<S *>(a.fo[F_TXZ]) + fb;
+    EZProf<C> zp{C(1), C(1), C(1), C(1)};
+    if (zin) {
+        const C *pr = static_cast<const C *>(a.prof);
+        const EisoProf P{a.NX, a.NZ};
+        zp = EZProf<C>{pr[P.azn() + Z], pr[P.bzn() + Z], pr[P.azh() + Z], pr[P.bzh() + Z]};
+    }
+
+    // ---- prologue: vx of row X0 and vz of row X0-1 (recomputed; stored
+    // only for X0 == 0, the row no other warp's march reaches) ----
+    ERow<C> p = e_load_row<S>(a, fb, X0 - 1, Z);
+    ERow<C> c = e_load_row<S>(a, fb, X0, Z);
+    ERow<C> n = e_load_row<S>(a, fb, X0 + 1, Z);
+    ESplit<C> sp;
+    e_load_split<S, C>(a, sb, X0 - 1, Z, zin, sp);
+    C vxc, vzp;
+    {
+        const C txz_zm = __shfl_up_sync(full, c.txz, 1);
+        vxc = zin ? e_vx<S, C>(a, sb, X0, Z, c.vx, c.b, r_sub(c.txx, p.txx),
+                               r_sub(c.txz, txz_zm), sp.vx, zp, X0 == 0 && own)
+                  : zero;
+        if (X0 == 0 && own) St::st(vxo + (long long)X0 * a.pitch + Z, vxc, a.sc[F_VX]);
+        const C tzz_zp = __shfl_down_sync(full, p.tzz, 1);
+        vzp = zero;
+        if (X0 >= 1 && zin)
+            vzp = e_vz<S, C>(a, sb, X0 - 1, Z, p.vz, p.bm, r_sub(c.txz, p.txz),
+                             r_sub(tzz_zp, p.tzz), sp.vz, zp, false);
+    }
+    ERow<C> nn = e_load_row<S>(a, fb, X0 + 2, Z);
+    e_load_split<S, C>(a, sb, X0, Z, zin, sp);
+    // rows [Xf0, Xf1) take e_fast_row, four at a time: X >= np, X + 1 still
+    // interior, X + 3 on the grid
+    const int Xf1 = zint ? min(X1, min(a.np + a.nx - 1, a.NX - 3)) : X1;
+
+    for (int X = X0; X < X1;) {
+        if (zint && X >= a.np && X + 4 <= Xf1) {
+            ERow<C> r3;
+            do {
+                e_fast_row<S, C>(a, fb, X, Z, own, c, n, r3, vxc, vzp);
+                e_fast_row<S, C>(a, fb, X + 1, Z, own, n, nn, c, vxc, vzp);
+                e_fast_row<S, C>(a, fb, X + 2, Z, own, nn, r3, n, vxc, vzp);
+                e_fast_row<S, C>(a, fb, X + 3, Z, own, r3, c, nn, vxc, vzp);
+                // rows X+4, X+5, X+6 now sit in c, n, nn
+                X += 4;
+            } while (X + 4 <= Xf1);
+            if (X >= X1) break;
+            e_load_split<S, C>(a, sb, X, Z, zin, sp);
+            continue;
+        }
+        ERow<C> n3 = e_load_row<S>(a, fb, X + 3, Z);   // prefetch
+        if (a.pfd > 0 && zin && X + a.pfd < a.NX) e_prefetch_row<S, C>(a, fb, X + a.pfd, Z);
+        ESplit<C> sn;
+        e_load_split<S, C>(a, sb, X + 1, Z, zin && X + 1 < X1, sn);
+        const bool fast = zint && X >= a.np && X + 1 <= a.np + a.nx - 1;
+        const long long q = (long long)X * a.pitch + Z;
+        // ---- velocities: vx(X+1), vz(X) ----
+        const C txz_zm = __shfl_up_sync(full, n.txz, 1);
+        const C tzz_zp = __shfl_down_sync(full, c.tzz, 1);
+        const C ax = r_sub(n.txx, c.txx), az = r_sub(n.txz, txz_zm);
+        const C bx = r_sub(n.txz, c.txz), bz = r_sub(tzz_zp, c.tzz);
+        C vxn, vzn;
+        if (fast) {
+            vxn = r_fma(n.b, r_add(ax, az), n.vx);
+            vzn = r_fma(c.bm, r_add(bx, bz), c.vz);
+        } else {
+            vxn = (X + 1 < a.NX && zin)
+                      ? e_vx<S, C>(a, sb, X + 1, Z, n.vx, n.b, ax, az, sp.vx, zp, own)
+                      : zero;
+            vzn = zin ? e_vz<S, C>(a, sb, X, Z, c.vz, c.bm, bx, bz, sp.vz, zp, own) : zero;
+        }
+        // ---- stresses of row X (propagate.c:2590-2670, pml.c:684-1403) ----
+        const C vz_zm = __shfl_up_sync(full, vzn, 1);
+        const C vx_zp = __shfl_down_sync(full, vxc, 1);
+        const C sax = r_sub(vxn, vxc), saz = r_sub(vzn, vz_zm);   // txx, tzz
+        const C sbz = r_sub(vx_zp, vxc), sbx = r_sub(vzn, vzp);   // txz
+        C txx, tzz, txz;
+        if (fast || (zin && e_inside(a, X, Z))) {
+            txx = r_add(c.txx, r_fma(c.l2m, sax, r_mul(c.la, saz)));
+            tzz = r_add(c.tzz, r_fma(c.l2m, saz, r_mul(c.la, sax)));
+            txz = r_fma(c.mu, r_add(sbz, sbx), c.txz);
+        } else if (zin) {
+            const C *pr = static_cast<const C *>(a.prof);
+            const EisoProf P{a.NX, a.NZ};
+            const long long cc = sb + e_pml_index(a, X, Z);
+            const C Axh = pr[P.axh() + X], Bxh = pr[P.bxh() + X];
+            txx = e_frame<S, C>(a, F_TXX, cc, Axh, Bxh, zp.An, zp.Bn, sp.t[0], sp.t[1], c.l2m,
+                                c.la, sax, saz, own);
+            tzz = e_frame<S, C>(a, F_TZZ, cc, Axh, Bxh, zp.An, zp.Bn, sp.t[2], sp.t[3], c.la,
+                                c.l2m, sax, saz, own);
+            txz = e_frame<S, C>(a, F_TXZ, cc, pr[P.axn() + X], pr[P.bxn() + X], zp.Ah, zp.Bh,
+                                sp.t[4], sp.t[5], c.mu, c.mu, sbx, sbz, own);
+        } else {
+            txx = tzz = txz = zero;
+        }
+        if (own) {
+            if (X + 1 < a.NX) St::st(vxo + q + a.pitch, vxn, a.sc[F_VX]);
+            St::st(vzo + q, vzn, a.sc[F_VZ]);
+            St::st(txxo + q, txx, a.sc[F_TXX]);
+            St::st(tzzo + q, tzz, a.sc[F_TZZ]);
+            St::st(txzo + q, txz, a.sc[F_TXZ]);
+        }
+        vxc = vxn;
+        vzp = vzn;
+        c = n;
+        n = nn;
+        nn = n3;
+        sp = sn;
+        ++X;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Tiled step kernel: one CTA updates a TX x TZ tile of one shot for a whole
+// time step (e_iso.c:595-636).  The five old wavefields of rows X0-1 ..
+// X0+TX and z cells Z0-HS .. Z0+TZ+HS-1 arrive by TMA (out-of-grid cells read
+// as zero, which is the reference's boundary).  Phase 1 computes vx on
+// [X0, X0+TX] x [Z0, Z0+TZ] and vz on [X0-1, X0+TX-1] x [Z0-1, Z0+TZ-1]
+// into shared memory (the halo is recomputed by the neighbouring CTA
+// bitwise, since the arithmetic is the same); phase 2 computes the stresses
+// of the tile from them.  Only cells of the tile are written (ping-pong
+// sets), and split parts of frame cells likewise.  Materials are read with
+// plain loads, issued before the TMA wait: they are shared by every shot
+// and stay in L2.
+// ---------------------------------------------------------------------------
+struct EisoMaps {
+    CUtensorMap f[5];   // the old set's wavefields: (z, x, shot), box (BZ, TX+2, 1)
+};
+
+template <typename S, int TX, int TZ>
+struct ETile {
+    using C = typename Store<S>::C;
+    static constexpr int HS = 16 / (int)sizeof(S);   // cells per 16 bytes
+    static constexpr int BZ = TZ + 2 * HS;            // box width (z cells)
+    static constexpr int RX = TX + 2;                 // box height (rows)
+    static constexpr int VP = TZ + 1;                 // velocity tile pitch
+    static constexpr int NVP = (TX + 1) * (TZ + 1);   // velocity points
+    static constexpr size_t al(size_t x) { return (x + 127) / 128 * 128; }
+    static constexpr size_t FB = (size_t)RX * BZ * sizeof(S);   // one field's box
+    static constexpr size_t FS = al(FB);                          // its slot (128-aligned)
+    static constexpr size_t oV = 5 * FS;
+    static constexpr size_t oBar = al(oV + 2 * (size_t)NVP * sizeof(C));
+    static constexpr size_t bytes = oBar + 16;
+    static constexpr unsigned tx = (unsigned)(5 * FB);
+};
+
+template <typename S, int TX, int TZ, int NT, int MINB>
+__global__ void __launch_bounds__(NT, MINB) eiso_tile_kernel(const EisoArgs a,
+                                                             const __grid_constant__ EisoMaps mp) {
+    using C = typename Store<S>::C;
+    using St = Store<S>;
+    using L = ETile<S, TX, TZ>;
+    constexpr int NV = (L::NVP + NT - 1) / NT;
+    constexpr int NS = (TX * TZ + NT - 1) / NT;
+    extern __shared__ __align__(128) unsigned char smem[];
+    C *vxs = reinterpret_cast<C *>(smem + L::oV);
+    C *vzs = vxs + L::NVP;
+    uint64_t *bar = reinterpret_cast<uint64_t *>(smem + L::oBar);
+    const int tid = threadIdx.x;
+    const int Z0 = blockIdx.x * TZ, X0 = blockIdx.y * TX, shot = blockIdx.z;
+    const long long fb = (long long)shot * a.fstride;
+    const long long sb = (long long)shot * a.sstride;
+
+    if (tid == 0) {
+        mbar_init(bar, 1);
+        fence_proxy_async();
+        mbar_expect_tx(bar, L::tx);
+#pragma unroll
+        for (int f = 0; f < 5; ++f)
+            tma_load_3d(smem + f * L::FS, &mp.f[f], Z0 - L::HS, X0 - 1, shot, bar);
+    }
+    // materials of this thread's points while the tile is in flight
+    const C *mat_b = static_cast<const C *>(a.mat[M_B]);
+    const C *mat_bm = static_cast<const C *>(a.mat[M_BM]);
+    C mb[NV], mbm[NV];
+#pragma unroll
+    for (int j = 0; j < NV; ++j) {
+        const int i = tid + j * NT;
+        mb[j] = mbm[j] = C(0);
+        if (i < L::NVP) {
+            const int r = i / (TZ + 1), k = i % (TZ + 1);
+            const int X = X0 + r, Z = Z0 + k;          // vx point
+            if (X < a.NX && Z < a.NZ) mb[j] = mat_b[(long long)X * a.pitch + Z];
+            const int Xz = X - 1, Zz = Z - 1;          // vz point
+            if (Xz >= 0 && Xz < a.NX && Zz >= 0 && Zz < a.NZ)
+                mbm[j] = mat_bm[(long long)Xz * a.pitch + Zz];
+        }
+    }
+    C la[NS], l2m[NS], mu[NS];
+#pragma unroll
+    for (int j = 0; j < NS; ++j) {
+        const int i = tid + j * NT;
+        la[j] = l2m[j] = mu[j] = C(0);
+        const int X = X0 + i / TZ, Z = Z0 + i % TZ;
+        if (i < TX * TZ && X < a.NX && Z < a.NZ) {
+            const long long q = (long long)X * a.pitch + Z;
+            la[j] = static_cast<const C *>(a.mat[M_LA])[q];
+            l2m[j] = static_cast<const C *>(a.mat[M_L2M])[q];
+            mu[j] = static_cast<const C *>(a.mat[M_MU])[q];
+        }
+    }
+    __syncthreads();   // barrier initialised before anyone polls it
+    if (!mbar_wait(bar, 0, a.err, 2)) {
+        mbar_wait(bar, 0, a.err, 2);   // give copies in flight a last bounded chance
+        return;
+    }
+    // field f at (X, Z), X in [X0-1, X0+TX], Z in [Z0-HS, Z0+TZ+HS)
+    auto F = [&](int f, int X, int Z) -> C {
+        return St::ld(reinterpret_cast<const S *>(smem + f * L::FS) + (X - X0 + 1) * L::BZ +
+                          (Z - Z0 + L::HS),
+                      a.isc[f]);
+    };
+    // the tile and its halo lie inside the interior update region
+    const bool tint = X0 - 1 >= a.np && X0 + TX <= a.np + a.nx - 1 && Z0 - 1 >= a.np &&
+                      Z0 + TZ <= a.np + a.nz - 1;
+    const EisoProf P{a.NX, a.NZ};
+    const C *pr = static_cast<const C *>(a.prof);
+    S *vxo = static_cast<S *>(a.fo[F_VX]) + fb;
+    S *vzo = static_cast<S *>(a.fo[F_VZ]) + fb;
+
+    // ---- phase 1: velocities (propagate.c:2511-2588, pml.c:39-680) ----
+#pragma unroll
+    for (int j = 0; j < NV; ++j) {
+        const int i = tid + j * NT;
+        if (i >= L::NVP) break;
+        const int r = i / (TZ + 1), k = i % (TZ + 1);
+        {   // vx at (X, Z)
+            const int X = X0 + r, Z = Z0 + k;
+            C v = C(0);
+            if (X < a.NX && Z < a.NZ) {
+                const C ax = r_sub(F(F_TXX, X, Z), F(F_TXX, X - 1, Z));
+                const C az = r_sub(F(F_TXZ, X, Z), F(F_TXZ, X, Z - 1));
+                const C vold = F(F_VX, X, Z);
+                if (tint || e_inside(a, X, Z)) {
+                    v = r_fma(mb[j], r_add(ax, az), vold);
+                } else {
+                    const long long c = sb + e_pml_index(a, X, Z);
+                    const bool own = X < X0 + TX && Z < Z0 + TZ;
+                    v = e_frame<S, C>(a, F_VX, c, pr[P.axn() + X], pr[P.bxn() + X],
+                                      pr[P.azn() + Z], pr[P.bzn() + Z],
+                                      St::ld(static_cast<const S *>(a.fx[F_VX]) + c, a.isc[F_VX]),
+                                      St::ld(static_cast<const S *>(a.fz[F_VX]) + c, a.isc[F_VX]),
+                                      mb[j], mb[j], ax, az, own);
+                }
+                if (X < X0 + TX && Z < Z0 + TZ)
+                    St::st(vxo + (long long)X * a.pitch + Z, v, a.sc[F_VX]);
+            }
+            vxs[r * L::VP + k] = v;
+        }
+        {   // vz at (X + 1/2, Z + 1/2), X = X0 - 1 + r, Z = Z0 - 1 + k
+            const int X = X0 - 1 + r, Z = Z0 - 1 + k;
+            C v = C(0);
+            if (X >= 0 && X < a.NX && Z >= 0 && Z < a.NZ) {
+                const C bx = r_sub(F(F_TXZ, X + 1, Z), F(F_TXZ, X, Z));
+                const C bz = r_sub(F(F_TZZ, X, Z + 1), F(F_TZZ, X, Z));
+                const C vold = F(F_VZ, X, Z);
+                if (tint || e_inside(a, X, Z)) {
+                    v = r_fma(mbm[j], r_add(bx, bz), vold);
+                } else {
+                    const long long c = sb + e_pml_index(a, X, Z);
+                    const bool own = X >= X0 && Z >= Z0;
+                    v = e_frame<S, C>(a, F_VZ, c, pr[P.axh() + X], pr[P.bxh() + X],
+                                      pr[P.azh() + Z], pr[P.bzh() + Z],
+                                      St::ld(static_cast<const S *>(a.fx[F_VZ]) + c, a.isc[F_VZ]),
+                                      St::ld(static_cast<const S *>(a.fz[F_VZ]) + c, a.isc[F_VZ]),
+                                      mbm[j], mbm[j], bx, bz, own);
+                }
+                if (X >= X0 && Z >= Z0) St::st(vzo + (long long)X * a.pitch + Z, v, a.sc[F_VZ]);
+            }
+            vzs[r * L::VP + k] = v;
+        }
+    }
+    __syncthreads();
+
+    // ---- phase 2: stresses of the tile (propagate.c:2590-2670, pml.c:684-1403) ----
+    S *txxo = static_cast<S *>(a.fo[F_TXX]) + fb;
+    S *tzzo = static_cast<S *>(a.fo[F_TZZ]) + fb;
+    S *txzo = static_cast<S *>(a.fo[F_TXZ]) + fb;
+#pragma unroll
+    for (int j = 0; j < NS; ++j) {
+        const int i = tid + j * NT;
+        if (i >= TX * TZ) break;
+        const int r = i / TZ, k = i % TZ;
+        const int X = X0 + r, Z = Z0 + k;
+        if (X >= a.NX || Z >= a.NZ) continue;
+        // vx(X, Z) at vxs[r][k]; vz(X, Z) at vzs[r+1][k+1]
+        const C vxc = vxs[r * L::VP + k];
+        const C vxn = vxs[(r + 1) * L::VP + k];
+        const C vx_zp = vxs[r * L::VP + k + 1];
+        const C vzc = vzs[(r + 1) * L::VP + k + 1];
+        const C vz_zm = vzs[(r + 1) * L::VP + k];
+        const C vzp = vzs[r * L::VP + k + 1];
+        const C sax = r_sub(vxn, vxc), saz = r_sub(vzc, vz_zm);
+        const C sbz = r_sub(vx_zp, vxc), sbx = r_sub(vzc, vzp);
+        const C txx0 = F(F_TXX, X, Z), tzz0 = F(F_TZZ, X, Z), txz0 = F(F_TXZ, X, Z);
+        C txx, tzz, txz;
+        if (tint || e_inside(a, X, Z)) {
+            txx = r_add(txx0, r_fma(l2m[j], sax, r_mul(la[j], saz)));
+            tzz = r_add(tzz0, r_fma(l2m[j], saz, r_mul(la[j], sax)));
+            txz = r_fma(mu[j], r_add(sbz, sbx), txz0);
+        } else {
+            const long long c = sb + e_pml_index(a, X, Z);
+            const C Axh = pr[P.axh() + X], Bxh = pr[P.bxh() + X];
+            const C Azn = pr[P.azn() + Z], Bzn = pr[P.bzn() + Z];
+            auto old = [&](const void *base, int f) {
+                return St::ld(static_cast<const S *>(base) + c, a.isc[f]);
+            };
+            txx = e_frame<S, C>(a, F_TXX, c, Axh, Bxh, Azn, Bzn, old(a.fx[F_TXX], F_TXX),
+                                old(a.fz[F_TXX], F_TXX), l2m[j], la[j], sax, saz, true);
+            tzz = e_frame<S, C>(a, F_TZZ, c, Axh, Bxh, Azn, Bzn, old(a.fx[F_TZZ], F_TZZ),
+                                old(a.fz[F_TZZ], F_TZZ), la[j], l2m[j], sax, saz, true);
+            txz = e_frame<S, C>(a, F_TXZ, c, pr[P.axn() + X], pr[P.bxn() + X], pr[P.azh() + Z],
+                                pr[P.bzh() + Z], old(a.fx[F_TXZ], F_TXZ), old(a.fz[F_TXZ], F_TXZ),
+                                mu[j], mu[j], sbx, sbz, true);
+        }
+        const long long q = (long long)X * a.pitch + Z;
+        St::st(txxo + q, txx, a.sc[F_TXX]);
+        St::st(tzzo + q, tzz, a.sc[F_TZZ]);
+        St::st(txzo + q, txz, a.sc[F_TXZ]);
+    }
 }
 
 // one entry per source, sorted by shot; one thread per shot adds its
@@ -261,7 +691,16 @@ struct sm_eiso {
     size_t it = 0;
     cudaStream_t stream = nullptr;
     EisoArgs args{};
-    DevBuf fields[5], xpart[5], zpart[5], mat[5], prof;
+    // two buffer sets of wavefields and split parts: a step reads set `cur`
+    // and writes the other one
+    DevBuf fields[2][5], xpart[2][5], zpart[2][5], mat[5], prof;
+    int cur = 0;
+    int chunk = 0;   // rows per warp march (0: chosen from the grid size)
+    int config = 4;  // index into kEisoConfigs
+    DevBuf err;      // bounded-wait failure flag of the tiled kernel
+    EisoMaps maps[2];            // TMA maps of each buffer set
+    int maps_key = -1;           // (TX, TZ) the maps were built for
+    int sms = 148;
     // sources
     std::vector<std::vector<SrcEntry>> shot_src;     // per shot (voff local)
     std::vector<std::vector<double>> shot_vals;      // per shot scaled samples
@@ -291,15 +730,125 @@ int eiso_check(sm_eiso_t h) {
     return SM_OK;
 }
 
+// point the kernel arguments at the current (read) and other (write) sets
+void eiso_bind(sm_eiso *h) {
+    const int c = h->cur, o = 1 - h->cur;
+    for (int f = 0; f < 5; ++f) {
+        h->args.f[f] = h->fields[c][f].p;
+        h->args.fx[f] = h->xpart[c][f].p;
+        h->args.fz[f] = h->zpart[c][f].p;
+        h->args.fo[f] = h->fields[o][f].p;
+        h->args.fxo[f] = h->xpart[o][f].p;
+        h->args.fzo[f] = h->zpart[o][f].p;
+    }
+}
+
+// launch configurations of the step kernel.  tile: TX x TZ tiles, NT
+// threads per CTA; march (tx == 0): warps per CTA `nt`, L2 prefetch distance.
+// minb = minimum resident CTAs per SM the register allocation is held to.
+struct EisoConfig {
+    int tx, tz, nt, minb, pfd;
+};
+static const EisoConfig kEisoConfigs[] = {
+    {16, 64, 256, 2, 0}, {8, 64, 256, 3, 0}, {16, 128, 256, 1, 0}, {32, 64, 256, 1, 0},
+    {8, 32, 128, 6, 0},  {16, 32, 128, 4, 0}, {0, 0, 4, 5, 0},     {0, 0, 2, 12, 0}};
+
+template <typename S, int TX, int TZ>
+int eiso_make_maps(sm_eiso *h) {
+    using L = ETile<S, TX, TZ>;
+    const int key = TX * 4096 + TZ;
+    if (h->maps_key == key) return SM_OK;
+    for (int b = 0; b < 2; ++b)
+        for (int f = 0; f < 5; ++f)
+            if (int rc = make_map_3d(&h->maps[b].f[f], h->fields[b][f].p, MapType<S>::v, sizeof(S),
+                                     h->NZ, h->NX, h->nshots, h->pitch, L::BZ, L::RX))
+                return rc;
+    h->maps_key = key;
+    return SM_OK;
+}
+
+template <typename S, int TX, int TZ, int NT, int MINB>
+int launch_tile_cfg(sm_eiso *h) {
+    using L = ETile<S, TX, TZ>;
+    if (int rc = eiso_make_maps<S, TX, TZ>(h)) return rc;
+    static bool attr = false;   // per instantiation
+    if (!attr) {
+        SM_CUDA_TRY(cudaFuncSetAttribute(eiso_tile_kernel<S, TX, TZ, NT, MINB>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L::bytes));
+        attr = true;
+    }
+    dim3 grd((h->NZ + TZ - 1) / TZ, (h->NX + TX - 1) / TX, (unsigned)h->nshots);
+    eiso_tile_kernel<S, TX, TZ, NT, MINB><<<grd, NT, L::bytes, h->stream>>>(h->args,
+                                                                           h->maps[h->cur]);
+    return SM_OK;
+}
+
 template <typename S>
-void launch_step(sm_eiso *h) {
-    dim3 blk(32, 8, 1);
-    dim3 grd((h->NZ + 31) / 32, (h->NX + 7) / 8, (unsigned)h->nshots);
+size_t eiso_config_smem(int config) {
+    const EisoConfig &k = kEisoConfigs[config];
+    if (k.tx == 16 && k.tz == 64) return ETile<S, 16, 64>::bytes;
+    if (k.tx == 8 && k.tz == 64) return ETile<S, 8, 64>::bytes;
+    if (k.tx == 16 && k.tz == 128) return ETile<S, 16, 128>::bytes;
+    if (k.tx == 32 && k.tz == 64) return ETile<S, 32, 64>::bytes;
+    if (k.tx == 8 && k.tz == 32) return ETile<S, 8, 32>::bytes;
+    if (k.tx == 16 && k.tz == 32) return ETile<S, 16, 32>::bytes;
+    return 0;
+}
+
+size_t eiso_config_smem_prec(int precision, int config) {
+    switch (precision) {
+    case SM_FP64: return eiso_config_smem<double>(config);
+    case SM_FP16: return eiso_config_smem<__half>(config);
+    case SM_BF16: return eiso_config_smem<__nv_bfloat16>(config);
+    default: return eiso_config_smem<float>(config);
+    }
+}
+static const int kEisoNumConfigs = sizeof(kEisoConfigs) / sizeof(kEisoConfigs[0]);
+
+// rows per warp march: long enough that the two rows re-read at each chunk
+// start stay cheap, short enough to give every SM about 48 warps
+int eiso_pick_chunk(const sm_eiso *h) {
+    if (h->chunk > 0) return h->chunk;
+    const int sms = h->sms;
+    const long long wz = (h->NZ + 29) / 30;
+    const long long want = (long long)sms * 48;
+    long long per = wz * (long long)h->nshots;                 // warps per row band
+    long long bands = (want + per - 1) / per;                  // row bands wanted
+    long long c = (h->NX + bands - 1) / std::max<long long>(bands, 1);
+    return (int)std::min<long long>(std::max<long long>(c, 16), 256);
+}
+
+template <typename S, int W, int MINB>
+void launch_step_cfg(sm_eiso *h) {
+    const int wz = (h->NZ + 29) / 30;
+    dim3 blk(32 * W, 1, 1);
+    dim3 grd((wz + W - 1) / W, (h->NX + h->args.chunk - 1) / h->args.chunk, (unsigned)h->nshots);
+    eiso_step_kernel<S, W, MINB><<<grd, blk, 0, h->stream>>>(h->args);
+}
+
+template <typename S>
+int launch_step(sm_eiso *h) {
+    h->args.chunk = eiso_pick_chunk(h);
+    const EisoConfig &k = kEisoConfigs[h->config];
+    h->args.pfd = k.pfd;
     cudaEvent_t t0 = h->timer.begin(h->stream);
-    eiso_velocity_kernel<S><<<grd, blk, 0, h->stream>>>(h->args);
-    eiso_stress_kernel<S><<<grd, blk, 0, h->stream>>>(h->args);
+    int rc = SM_OK;
+    switch (h->config) {
+    case 0: rc = launch_tile_cfg<S, 16, 64, 256, 2>(h); break;
+    case 1: rc = launch_tile_cfg<S, 8, 64, 256, 3>(h); break;
+    case 2: rc = launch_tile_cfg<S, 16, 128, 256, 1>(h); break;
+    case 3: rc = launch_tile_cfg<S, 32, 64, 256, 1>(h); break;
+    case 4: rc = launch_tile_cfg<S, 8, 32, 128, 6>(h); break;
+    case 5: rc = launch_tile_cfg<S, 16, 32, 128, 4>(h); break;
+    case 6: launch_step_cfg<S, 4, 5>(h); break;
+    default: launch_step_cfg<S, 2, 12>(h); break;
+    }
+    if (rc) return rc;
     h->timer.end(t0, h->stream);
-    h->timer.launches += 2;
+    h->timer.launches += 1;
+    h->cur = 1 - h->cur;
+    eiso_bind(h);
+    return SM_OK;
 }
 
 template <typename S>
@@ -338,9 +887,9 @@ int eiso_rescale(sm_eiso *h) {
     static const char *names[5] = {"vx", "vz", "txx", "tzz", "txz"};
     const size_t fcells = (size_t)h->NX * h->pitch * h->nshots;
     for (int f = 0; f < 5; ++f) {
-        ptrs[3 * f] = h->fields[f].p; ns[3 * f] = fcells; groups[3 * f] = f;
-        ptrs[3 * f + 1] = h->xpart[f].p; ns[3 * f + 1] = h->npml_cells * h->nshots; groups[3 * f + 1] = f;
-        ptrs[3 * f + 2] = h->zpart[f].p; ns[3 * f + 2] = h->npml_cells * h->nshots; groups[3 * f + 2] = f;
+        ptrs[3 * f] = h->fields[h->cur][f].p; ns[3 * f] = fcells; groups[3 * f] = f;
+        ptrs[3 * f + 1] = h->xpart[h->cur][f].p; ns[3 * f + 1] = h->npml_cells * h->nshots; groups[3 * f + 1] = f;
+        ptrs[3 * f + 2] = h->zpart[h->cur][f].p; ns[3 * f + 2] = h->npml_cells * h->nshots; groups[3 * f + 2] = f;
     }
     int rc = h->precision == SM_FP16
                  ? h->scaler.check<__half>(h->stream, 15, ptrs, ns, groups, names)
@@ -463,6 +1012,13 @@ int field_id(int comp) {
     }
 }
 
+int eiso_check_err(sm_eiso *h) {
+    int e = 0;
+    SM_CUDA_TRY(cudaMemcpy(&e, h->err.p, sizeof(int), cudaMemcpyDeviceToHost));
+    if (e) return sm_fail(SM_ETIMEOUT, "e_iso step kernel: a bounded wait for a TMA load gave up");
+    return SM_OK;
+}
+
 bool in_frame(const sm_eiso *h, size_t X, size_t Z) {
     return X < h->np || X >= h->np + h->nx || Z < h->np || Z >= h->np + h->nz;
 }
@@ -514,18 +1070,23 @@ extern "C" int sm_eiso_create(int device, size_t nx, size_t nz, size_t npml, dou
     h->npml_cells = 4 * npml * npml + 2 * npml * (nx + nz);
     h->elem = storage_bytes(precision);
     SM_CUDA_TRY(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
+    SM_CUDA_TRY(cudaDeviceGetAttribute(&h->sms, cudaDevAttrMultiProcessorCount, device));
 
     const size_t cplx = precision == SM_FP64 ? 8 : 4;    // compute type bytes
     const size_t fcells = NX * (size_t)h->pitch;
     int rc;
     for (int f = 0; f < 5; ++f) {
-        if ((rc = h->fields[f].alloc(fcells * nshots * h->elem))) return rc;
-        if ((rc = h->xpart[f].alloc(h->npml_cells * nshots * h->elem))) return rc;
-        if ((rc = h->zpart[f].alloc(h->npml_cells * nshots * h->elem))) return rc;
+        for (int k = 0; k < 2; ++k) {
+            if ((rc = h->fields[k][f].alloc(fcells * nshots * h->elem))) return rc;
+            if ((rc = h->xpart[k][f].alloc(h->npml_cells * nshots * h->elem))) return rc;
+            if ((rc = h->zpart[k][f].alloc(h->npml_cells * nshots * h->elem))) return rc;
+        }
         if ((rc = h->mat[f].alloc(fcells * cplx))) return rc;
     }
     EisoProf P{(int)NX, (int)NZ};
     if ((rc = h->prof.alloc((size_t)P.size() * cplx))) return rc;
+    if ((rc = h->err.alloc(sizeof(int)))) return rc;
+    if ((rc = h->err.zero(h->stream))) return rc;
 
     // ---- materials on the padded grid: edge replicated, scaled by dt/h ----
     // pml.c reads the interior's edge values in the frame; for lambda and
@@ -586,15 +1147,14 @@ extern "C" int sm_eiso_create(int device, size_t nx, size_t nz, size_t npml, dou
     a.sstride = (long long)h->npml_cells;
     a.mid_off = (int)(npml * NZ);
     a.right_off = (int)(npml * NZ + nx * 2 * npml);
+    eiso_bind(h.get());
     for (int f = 0; f < 5; ++f) {
-        a.f[f] = h->fields[f].p;
-        a.fx[f] = h->xpart[f].p;
-        a.fz[f] = h->zpart[f].p;
         a.mat[f] = h->mat[f].p;
         a.sc[f] = 1.0f;
         a.isc[f] = 1.0f;
     }
     a.prof = h->prof.p;
+    a.err = h->err.as<int>();
     if (precision == SM_FP16 || precision == SM_BF16) {
         if ((rc = h->scaler.init(5, 15))) return rc;
         h->expo0.assign(5, 0);
@@ -620,12 +1180,16 @@ extern "C" int sm_eiso_create(int device, size_t nx, size_t nz, size_t npml, dou
 extern "C" int sm_eiso_reset(sm_eiso_t h) {
     if (int rc = eiso_check(h)) return rc;
     DeviceGuard g(h->device);
-    for (int f = 0; f < 5; ++f) {
-        if (int rc = h->fields[f].zero(h->stream)) return rc;
-        if (int rc = h->xpart[f].zero(h->stream)) return rc;
-        if (int rc = h->zpart[f].zero(h->stream)) return rc;
-    }
+    for (int k = 0; k < 2; ++k)
+        for (int f = 0; f < 5; ++f) {
+            if (int rc = h->fields[k][f].zero(h->stream)) return rc;
+            if (int rc = h->xpart[k][f].zero(h->stream)) return rc;
+            if (int rc = h->zpart[k][f].zero(h->stream)) return rc;
+        }
+    h->cur = 0;
+    eiso_bind(h);
     if (int rc = h->d_traces.zero(h->stream)) return rc;
+    if (int rc = h->err.zero(h->stream)) return rc;
     SM_CUDA_TRY(cudaStreamSynchronize(h->stream));
     h->it = 0;
     if (eiso_is16(h)) {
@@ -734,15 +1298,25 @@ extern "C" int sm_eiso_run(sm_eiso_t h, size_t nsteps) {
     if (h->rec_dirty)
         if (int rc = upload_receivers(h)) return rc;
     for (size_t k = 0; k < nsteps; ++k) {
+        int rc = SM_OK;
         switch (h->precision) {
-        case SM_FP64: launch_step<double>(h); launch_src<double>(h); launch_gather<double>(h); break;
-        case SM_FP16: launch_step<__half>(h); launch_src<__half>(h); launch_gather<__half>(h); break;
-        case SM_BF16:
-            launch_step<__nv_bfloat16>(h); launch_src<__nv_bfloat16>(h);
-            launch_gather<__nv_bfloat16>(h);
+        case SM_FP64:
+            if (!(rc = launch_step<double>(h))) { launch_src<double>(h); launch_gather<double>(h); }
             break;
-        default: launch_step<float>(h); launch_src<float>(h); launch_gather<float>(h); break;
+        case SM_FP16:
+            if (!(rc = launch_step<__half>(h))) { launch_src<__half>(h); launch_gather<__half>(h); }
+            break;
+        case SM_BF16:
+            if (!(rc = launch_step<__nv_bfloat16>(h))) {
+                launch_src<__nv_bfloat16>(h);
+                launch_gather<__nv_bfloat16>(h);
+            }
+            break;
+        default:
+            if (!(rc = launch_step<float>(h))) { launch_src<float>(h); launch_gather<float>(h); }
+            break;
         }
+        if (rc) return rc;
         h->it++;
         if (eiso_is16(h) && h->it % sm_eiso::kScalePeriod == 0)
             if (int rc = eiso_rescale(h)) return rc;
@@ -753,8 +1327,9 @@ extern "C" int sm_eiso_run(sm_eiso_t h, size_t nsteps) {
 
 extern "C" int sm_eiso_sync(sm_eiso_t h) {
     if (int rc = eiso_check(h)) return rc;
+    DeviceGuard g(h->device);
     SM_CUDA_TRY(cudaStreamSynchronize(h->stream));
-    return SM_OK;
+    return eiso_check_err(h);
 }
 
 extern "C" int sm_eiso_step_count(sm_eiso_t h, size_t *it) {
@@ -775,6 +1350,7 @@ extern "C" int sm_eiso_read_traces(sm_eiso_t h, size_t shot, size_t rec0, size_t
     if (rec0 + nrec > sr.entries.size())
         return sm_fail(SM_EINVAL, "sm_eiso_read_traces: receiver range out of bounds");
     SM_CUDA_TRY(cudaStreamSynchronize(h->stream));
+    if (int rc = eiso_check_err(h)) return rc;
     const size_t ms = sr.plan.max_samples;
     std::vector<double> buf(ms);
     for (size_t r = 0; r < nrec; ++r) {
@@ -805,7 +1381,7 @@ extern "C" int sm_eiso_get_field(sm_eiso_t h, size_t shot, int comp, int part, d
     if (part == SM_PART_TOTAL) {
         std::vector<unsigned char> buf(NX * (size_t)h->pitch * e);
         SM_CUDA_TRY(cudaMemcpy(buf.data(),
-                               static_cast<char *>(h->fields[f].p) + shot * h->args.fstride * e,
+                               static_cast<char *>(h->fields[h->cur][f].p) + shot * h->args.fstride * e,
                                buf.size(), cudaMemcpyDeviceToHost));
         for (size_t X = 0; X < NX; ++X)
             for (size_t Z = 0; Z < NZ; ++Z)
@@ -813,7 +1389,7 @@ extern "C" int sm_eiso_get_field(sm_eiso_t h, size_t shot, int comp, int part, d
                                             h->args.isc[f]);
         return SM_OK;
     }
-    const DevBuf &src = part == SM_PART_X ? h->xpart[f] : h->zpart[f];
+    const DevBuf &src = part == SM_PART_X ? h->xpart[h->cur][f] : h->zpart[h->cur][f];
     std::vector<unsigned char> buf(h->npml_cells * e);
     SM_CUDA_TRY(cudaMemcpy(buf.data(), static_cast<char *>(src.p) + shot * h->npml_cells * e,
                            buf.size(), cudaMemcpyDeviceToHost));
@@ -835,9 +1411,9 @@ extern "C" int sm_eiso_set_field(sm_eiso_t h, size_t shot, int comp, int part, c
     const size_t NX = h->NX, NZ = h->NZ, e = h->elem;
     std::vector<unsigned char> tot(NX * (size_t)h->pitch * e), px(h->npml_cells * e),
         pz(h->npml_cells * e);
-    char *dtot = static_cast<char *>(h->fields[f].p) + shot * h->args.fstride * e;
-    char *dpx = static_cast<char *>(h->xpart[f].p) + shot * h->npml_cells * e;
-    char *dpz = static_cast<char *>(h->zpart[f].p) + shot * h->npml_cells * e;
+    char *dtot = static_cast<char *>(h->fields[h->cur][f].p) + shot * h->args.fstride * e;
+    char *dpx = static_cast<char *>(h->xpart[h->cur][f].p) + shot * h->npml_cells * e;
+    char *dpz = static_cast<char *>(h->zpart[h->cur][f].p) + shot * h->npml_cells * e;
     SM_CUDA_TRY(cudaMemcpy(tot.data(), dtot, tot.size(), cudaMemcpyDeviceToHost));
     SM_CUDA_TRY(cudaMemcpy(px.data(), dpx, px.size(), cudaMemcpyDeviceToHost));
     SM_CUDA_TRY(cudaMemcpy(pz.data(), dpz, pz.size(), cudaMemcpyDeviceToHost));
@@ -879,6 +1455,46 @@ extern "C" int sm_eiso_stream(sm_eiso_t h, void **stream) {
     if (int rc = eiso_check(h)) return rc;
     if (!stream) return sm_fail(SM_EINVAL, "sm_eiso_stream: NULL");
     *stream = (void *)h->stream;
+    return SM_OK;
+}
+
+extern "C" int sm_eiso_set_chunk(sm_eiso_t h, int chunk) {
+    if (int rc = eiso_check(h)) return rc;
+    if (chunk < 0 || chunk > (1 << 20))
+        return sm_fail(SM_EINVAL, "sm_eiso_set_chunk: chunk %d out of range", chunk);
+    h->chunk = chunk;
+    return SM_OK;
+}
+
+extern "C" int sm_eiso_set_config(sm_eiso_t h, int config) {
+    if (int rc = eiso_check(h)) return rc;
+    if (config < 0 || config >= kEisoNumConfigs)
+        return sm_fail(SM_EINVAL, "sm_eiso_set_config: config %d not in [0, %d)", config,
+                       kEisoNumConfigs);
+    DeviceGuard g(h->device);
+    int lim = 0;
+    SM_CUDA_TRY(cudaDeviceGetAttribute(&lim, cudaDevAttrMaxSharedMemoryPerBlockOptin, h->device));
+    const size_t need = eiso_config_smem_prec(h->precision, config);
+    if (need > (size_t)lim)
+        return sm_fail(SM_EINVAL,
+                       "sm_eiso_set_config: config %d needs %zu bytes of shared memory per block "
+                       "(device limit %d)",
+                       config, need, lim);
+    h->config = config;
+    return SM_OK;
+}
+
+extern "C" int sm_eiso_get_config(sm_eiso_t h, int *config, int *nconfigs) {
+    if (int rc = eiso_check(h)) return rc;
+    if (config) *config = h->config;
+    if (nconfigs) *nconfigs = kEisoNumConfigs;
+    return SM_OK;
+}
+
+extern "C" int sm_eiso_get_chunk(sm_eiso_t h, int *chunk) {
+    if (int rc = eiso_check(h)) return rc;
+    if (!chunk) return sm_fail(SM_EINVAL, "sm_eiso_get_chunk: NULL");
+    *chunk = eiso_pick_chunk(h);
     return SM_OK;
 }
 

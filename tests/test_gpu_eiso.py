@@ -97,6 +97,43 @@ def test_cfg0_full_size_against_oracle(precision):
     assert H.rel_l2([1e3 * g for g in got], orc) < TOL[precision]
 
 
+def _state_after(nx, nz, P, precision, steps, config=None, chunk=None):
+    orc, dev = _pair(nx, nz, P, 7, precision)
+    if config is not None:
+        dev.set_config(config)
+    if chunk is not None:
+        dev.set_chunk(chunk)
+        if chunk:
+            assert dev.get_chunk() == chunk
+    dev.run(steps)
+    got = {(f, part): dev.get_field(f, part=part) for f in FIELDS for part in ("total", "x", "z")}
+    nconf = dev.get_config()[1]
+    dev.close()
+    return orc, got, nconf
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+def test_every_launch_config_gives_identical_results(precision):
+    """Tile shapes and the row-march variants of the step kernel must not
+    show in the results: halo cells are recomputed bitwise by neighbours."""
+    nx, nz, P = 70, 95, 5       # NZ = 105: ragged against every tile width
+    orc, ref, nconf = _state_after(nx, nz, P, precision, 6)
+    for _ in range(6):
+        orc.velocity()
+        orc.stress()
+    for (f, part), a in ref.items():
+        assert O.rel_l2(a, orc.get(f, part)) < TOL[precision], (f, part)
+    for config in range(nconf):
+        _, got, _ = _state_after(nx, nz, P, precision, 6, config=config)
+        for k, a in got.items():
+            np.testing.assert_array_equal(a, ref[k], err_msg=f"config {config} {k}")
+    # the row march with its chunk lengths
+    for chunk in (1, 2, 5, 17, 200):
+        _, got, _ = _state_after(nx, nz, P, precision, 6, config=nconf - 1, chunk=chunk)
+        for k, a in got.items():
+            np.testing.assert_array_equal(a, ref[k], err_msg=f"chunk {chunk} {k}")
+
+
 def test_batched_shots_equal_single_shots():
     p = W.cfg2(nx=120, nz=80, npml=10, nsteps=250, nshots=5, nrec=12)
     batch = api.run_eiso(p, "fp32")
