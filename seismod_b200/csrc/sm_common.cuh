@@ -298,6 +298,15 @@ __device__ __forceinline__ void tma_load_3d(void *dst, const CUtensorMap *map, i
         "l"(reinterpret_cast<uint64_t>(map)), "r"(c0), "r"(c1), "r"(c2), "r"(smem_u32(bar))
         : "memory");
 }
+__device__ __forceinline__ void tma_load_4d(void *dst, const CUtensorMap *map, int c0, int c1,
+                                            int c2, int c3, uint64_t *bar) {
+    asm volatile(
+        "cp.async.bulk.tensor.4d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
+        " [%0], [%1, {%2, %3, %4, %5}], [%6];\n" ::"r"(smem_u32(dst)),
+        "l"(reinterpret_cast<uint64_t>(map)), "r"(c0), "r"(c1), "r"(c2), "r"(c3),
+        "r"(smem_u32(bar))
+        : "memory");
+}
 __device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, unsigned parity) {
     unsigned ok;
     asm volatile(
@@ -308,12 +317,24 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, unsigned parity) {
         : "memory");
     return ok != 0;
 }
-// Wait for the phase with this parity; gives up after ~2^22 polls (each
-// try_wait may suspend for a while), records `code` in *err and returns
-// false.  A normal load lands within microseconds.
+// try_wait with a suspend-time hint (ns): the thread sleeps until the phase
+// completes or the hint runs out, instead of spinning on the issue slots
+__device__ __forceinline__ bool mbar_try_wait_for(uint64_t *bar, unsigned parity, unsigned ns) {
+    unsigned ok;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n"
+        " selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity), "r"(ns)
+        : "memory");
+    return ok != 0;
+}
+// Wait for the phase with this parity; gives up after 2^18 tries of up to
+// 10 us each (at least ~26 ms even if no try suspends), records `code` in
+// *err and returns false.  A normal load lands within microseconds.
 __device__ __forceinline__ bool mbar_wait(uint64_t *bar, unsigned parity, int *err, int code) {
-    for (int n = 0; n < (1 << 22); ++n)
-        if (mbar_try_wait(bar, parity)) return true;
+    for (int n = 0; n < (1 << 18); ++n)
+        if (mbar_try_wait_for(bar, parity, 10000u)) return true;
     atomicExch(err, code);
     return false;
 }
@@ -378,6 +399,32 @@ inline int make_map_3d(CUtensorMap *m, const void *base, CUtensorMapDataType dt,
     cuuint32_t box[3] = {b0, b1, 1};
     cuuint32_t es[3] = {1, 1, 1};
     CUresult r = enc(m, dt, 3, const_cast<void *>(base), dims, strides, box, es,
+                     CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                     CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) return sm_fail(SM_ECUDA, "cuTensorMapEncodeTiled failed (%d)", (int)r);
+    return SM_OK;
+}
+
+// general tiled map: dims / box innermost first, strides (bytes) of dims 1..
+inline int make_map_nd(CUtensorMap *m, const void *base, CUtensorMapDataType dt, size_t elem,
+                       int rank, const size_t *dims, const size_t *strides, const unsigned *box) {
+    auto enc = tensor_map_encoder();
+    if (!enc) return sm_fail(SM_ECUDA, "cuTensorMapEncodeTiled is not available");
+    if (rank < 1 || rank > 5) return sm_fail(SM_EINVAL, "tensor map: rank %d", rank);
+    if ((box[0] * elem) % 16 || (reinterpret_cast<uintptr_t>(base) % 16))
+        return sm_fail(SM_EINVAL, "tensor map: 16-byte alignment rule violated");
+    cuuint64_t d[5], st[4];
+    cuuint32_t b[5], es[5];
+    for (int i = 0; i < rank; ++i) {
+        d[i] = dims[i];
+        b[i] = box[i];
+        es[i] = 1;
+        if (i > 0) {
+            if (strides[i - 1] % 16) return sm_fail(SM_EINVAL, "tensor map: stride not a multiple of 16");
+            st[i - 1] = strides[i - 1];
+        }
+    }
+    CUresult r = enc(m, dt, (cuuint32_t)rank, const_cast<void *>(base), d, st, b, es,
                      CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
                      CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
     if (r != CUDA_SUCCESS) return sm_fail(SM_ECUDA, "cuTensorMapEncodeTiled failed (%d)", (int)r);

@@ -61,7 +61,6 @@ struct EisoArgs {
     void *fxo[5];
     void *fzo[5];
     int chunk;           // rows (x) each warp marches through
-    int pfd;             // rows ahead the march asks L2 to fetch (0: none)
     int *err;            // set by a bounded wait that gave up
     const void *mat[5];
     const void *prof;
@@ -76,102 +75,6 @@ __device__ __forceinline__ int e_pml_index(const EisoArgs &a, int X, int Z) {
     if (X < a.np) return X * a.NZ + Z;
     if (X >= a.np + a.nx) return a.right_off + (X - a.np - a.nx) * a.NZ + Z;
     return a.mid_off + (X - a.np) * 2 * a.np + (Z < a.np ? Z : Z - a.nz);
-}
-
-// values of one grid row (x = X) at this lane's z: the five wavefields of
-// the old state and the five (scaled) materials
-template <typename C>
-struct ERow {
-    C txx, tzz, txz, vx, vz, b, bm, la, l2m, mu;
-};
-
-template <typename S, typename C = typename Store<S>::C>
-__device__ __forceinline__ ERow<C> e_load_row(const EisoArgs &a, long long fb, int X, int Z) {
-    ERow<C> r;
-    using St = Store<S>;
-    if (X < 0 || X >= a.NX || Z < 0 || Z >= a.NZ) {
-        r.txx = r.tzz = r.txz = r.vx = r.vz = C(0);
-        r.b = r.bm = r.la = r.l2m = r.mu = C(0);
-        return r;
-    }
-    const long long q = (long long)X * a.pitch + Z;
-    r.txx = St::ld(static_cast<const S *>(a.f[F_TXX]) + fb + q, a.isc[F_TXX]);
-    r.tzz = St::ld(static_cast<const S *>(a.f[F_TZZ]) + fb + q, a.isc[F_TZZ]);
-    r.txz = St::ld(static_cast<const S *>(a.f[F_TXZ]) + fb + q, a.isc[F_TXZ]);
-    r.vx = St::ld(static_cast<const S *>(a.f[F_VX]) + fb + q, a.isc[F_VX]);
-    r.vz = St::ld(static_cast<const S *>(a.f[F_VZ]) + fb + q, a.isc[F_VZ]);
-    r.b = static_cast<const C *>(a.mat[M_B])[q];
-    r.bm = static_cast<const C *>(a.mat[M_BM])[q];
-    r.la = static_cast<const C *>(a.mat[M_LA])[q];
-    r.l2m = static_cast<const C *>(a.mat[M_L2M])[q];
-    r.mu = static_cast<const C *>(a.mat[M_MU])[q];
-    return r;
-}
-
-// e_load_row for a row and lane known to lie on the grid
-template <typename S, typename C = typename Store<S>::C>
-__device__ __forceinline__ ERow<C> e_load_row_in(const EisoArgs &a, long long fb, int X, int Z) {
-    ERow<C> r;
-    using St = Store<S>;
-    const long long q = (long long)X * a.pitch + Z;
-    r.txx = St::ld(static_cast<const S *>(a.f[F_TXX]) + fb + q, a.isc[F_TXX]);
-    r.tzz = St::ld(static_cast<const S *>(a.f[F_TZZ]) + fb + q, a.isc[F_TZZ]);
-    r.txz = St::ld(static_cast<const S *>(a.f[F_TXZ]) + fb + q, a.isc[F_TXZ]);
-    r.vx = St::ld(static_cast<const S *>(a.f[F_VX]) + fb + q, a.isc[F_VX]);
-    r.vz = St::ld(static_cast<const S *>(a.f[F_VZ]) + fb + q, a.isc[F_VZ]);
-    r.b = static_cast<const C *>(a.mat[M_B])[q];
-    r.bm = static_cast<const C *>(a.mat[M_BM])[q];
-    r.la = static_cast<const C *>(a.mat[M_LA])[q];
-    r.l2m = static_cast<const C *>(a.mat[M_L2M])[q];
-    r.mu = static_cast<const C *>(a.mat[M_MU])[q];
-    return r;
-}
-
-// ask L2 for row X (fields of the old state and materials) of this lane
-template <typename S, typename C>
-__device__ __forceinline__ void e_prefetch_row(const EisoArgs &a, long long fb, int X, int Z) {
-    const long long q = (long long)X * a.pitch + Z;
-#pragma unroll
-    for (int f = 0; f < 5; ++f) prefetch_l2(static_cast<const S *>(a.f[f]) + fb + q);
-#pragma unroll
-    for (int m = 0; m < 5; ++m) prefetch_l2(static_cast<const C *>(a.mat[m]) + q);
-}
-
-// One march iteration at row X for a warp whose cells and rows X-1 .. X+3
-// all lie inside the interior-update region: no frame test, no bounds test.
-// c, n = rows X, X+1; row X+3 is loaded into `ahead`.  The arithmetic is the
-// general iteration's interior branch, operation for operation.
-template <typename S, typename C>
-__device__ __forceinline__ void e_fast_row(const EisoArgs &a, long long fb, int X, int Z, bool own,
-                                           const ERow<C> &c, const ERow<C> &n, ERow<C> &ahead,
-                                           C &vxc, C &vzp) {
-    using St = Store<S>;
-    const unsigned full = 0xffffffffu;
-    ahead = e_load_row_in<S, C>(a, fb, X + 3, Z);
-    if (a.pfd > 0 && X + a.pfd < a.NX) e_prefetch_row<S, C>(a, fb, X + a.pfd, Z);
-    const C txz_zm = __shfl_up_sync(full, n.txz, 1);
-    const C tzz_zp = __shfl_down_sync(full, c.tzz, 1);
-    const C ax = r_sub(n.txx, c.txx), az = r_sub(n.txz, txz_zm);
-    const C bx = r_sub(n.txz, c.txz), bz = r_sub(tzz_zp, c.tzz);
-    const C vxn = r_fma(n.b, r_add(ax, az), n.vx);
-    const C vzn = r_fma(c.bm, r_add(bx, bz), c.vz);
-    const C vz_zm = __shfl_up_sync(full, vzn, 1);
-    const C vx_zp = __shfl_down_sync(full, vxc, 1);
-    const C sax = r_sub(vxn, vxc), saz = r_sub(vzn, vz_zm);
-    const C sbz = r_sub(vx_zp, vxc), sbx = r_sub(vzn, vzp);
-    const C txx = r_add(c.txx, r_fma(c.l2m, sax, r_mul(c.la, saz)));
-    const C tzz = r_add(c.tzz, r_fma(c.l2m, saz, r_mul(c.la, sax)));
-    const C txz = r_fma(c.mu, r_add(sbz, sbx), c.txz);
-    if (own) {
-        const long long q = fb + (long long)X * a.pitch + Z;
-        St::st(static_cast<S *>(a.fo[F_VX]) + q + a.pitch, vxn, a.sc[F_VX]);
-        St::st(static_cast<S *>(a.fo[F_VZ]) + q, vzn, a.sc[F_VZ]);
-        St::st(static_cast<S *>(a.fo[F_TXX]) + q, txx, a.sc[F_TXX]);
-        St::st(static_cast<S *>(a.fo[F_TZZ]) + q, tzz, a.sc[F_TZZ]);
-        St::st(static_cast<S *>(a.fo[F_TXZ]) + q, txz, a.sc[F_TXZ]);
-    }
-    vxc = vxn;
-    vzp = vzn;
 }
 
 // split-part update in the frame: q' = A q + B (m * delta)  (pml.c, see above)
@@ -258,134 +161,237 @@ __device__ __forceinline__ C e_vz(const EisoArgs &a, long long sb, int X, int Z,
                          zp.Ah, zp.Bh, q[0], q[1], mbm, mbm, bx, bz, store);
 }
 
-// One time step, fused (e_iso.c:595-636).  Each warp owns 30 consecutive z
-// cells of one shot and marches along x over rows [X0, X1); lane l computes
-// z = Z0 - 1 + l, lanes 0 and 31 being the halo cells, so every z neighbour
-// comes from a warp shuffle and warps never wait on one another.
-// Iteration X computes vx of row X+1 and vz of row X (velocity half step),
-// then txx, tzz, txz of row X (stress half step) from them, with vx of row
-// X and vz of row X-1 carried in registers.  Rows are prefetched two ahead,
-// frame split parts one ahead.  Old and new state live in separate buffer
-// sets (ping-pong), so halo reads of neighbouring warps' cells never race
-// with their writes.
-template <typename S, int W, int MINB>
-__global__ void __launch_bounds__(32 * W, MINB) eiso_step_kernel(const EisoArgs a) {
+// ---------------------------------------------------------------------------
+// Band step kernel: one time step (e_iso.c:595-636), fused.  Each warp owns
+// 30 consecutive z cells of one shot and marches along x over rows [X0, X1);
+// lane l computes z = Z0 - 1 + l, lanes 0 and 31 being the halo cells, so
+// every z neighbour comes from a warp shuffle.  Each warp keeps its own ring
+// of D rows in shared memory, filled by TMA (one box spans the five
+// wavefields, one the five materials; out-of-grid cells read as zero, the
+// reference's boundary), so warps never wait on one another.  Iteration X
+// computes vx of row X+1 and vz of row X (velocity half step), then txx,
+// tzz, txz of row X (stress half step), with vx of row X and vz of row X-1
+// carried in registers.  Frame split parts are loaded one row ahead.  Old
+// and new state live in separate buffer sets (ping-pong).
+// ---------------------------------------------------------------------------
+struct EisoBandMaps {
+    CUtensorMap f;   // the old set's wavefields: (z, x, shot, field), box (BW, 1, 1, 5)
+    CUtensorMap m;   // materials: (z, x, material), box (BWC, 1, 5)
+};
+
+template <typename S>
+struct EBand {
+    using C = typename Store<S>::C;
+    static constexpr int HS = 16 / (int)sizeof(S), HC = 16 / (int)sizeof(C);
+    // a warp reads z cells Z0-1 .. Z0+30 from a start rounded down to 16 bytes
+    static constexpr int BW = (32 + HS - 1 + HS - 1) / HS * HS;
+    static constexpr int BWC = (32 + HC - 1 + HC - 1) / HC * HC;
+    static constexpr size_t al(size_t x) { return (x + 127) / 128 * 128; }
+    static constexpr size_t oM = al(5 * (size_t)BW * sizeof(S));   // materials in a stage
+    static constexpr size_t stage = oM + al(5 * (size_t)BWC * sizeof(C));
+    static constexpr unsigned tx = (unsigned)(5 * BW * sizeof(S) + 5 * BWC * sizeof(C));
+    static constexpr size_t warp_bytes(int D) { return D * stage + al(8 * (size_t)D); }
+};
+
+template <typename S, int W, int D, int MINB>
+__global__ void __launch_bounds__(32 * W, MINB) eiso_band_kernel(const EisoArgs a,
+                                                                 const __grid_constant__ EisoBandMaps mp) {
     using C = typename Store<S>::C;
     using St = Store<S>;
-    const int lane = threadIdx.x & 31;
-    const int wcol = blockIdx.x * W + (threadIdx.x >> 5);
-    const int Z0 = wcol * 30;
+    using L = EBand<S>;
+    extern __shared__ __align__(128) unsigned char smem[];
+    const unsigned full = 0xffffffffu;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    unsigned char *ring = smem + (size_t)warp * L::warp_bytes(D);
+    uint64_t *bars = reinterpret_cast<uint64_t *>(ring + (size_t)D * L::stage);
+    const int Z0 = (blockIdx.x * W + warp) * 30;
     if (Z0 >= a.NZ) return;                          // whole warp idle
     const int Z = Z0 - 1 + lane;
     const bool zin = Z >= 0 && Z < a.NZ;
     const bool own = lane >= 1 && lane <= 30 && Z < a.NZ;
     const int X0 = blockIdx.y * a.chunk;
     const int X1 = min(X0 + a.chunk, a.NX);
-    const long long fb = (long long)blockIdx.z * a.fstride;
-    const long long sb = (long long)blockIdx.z * a.sstride;
-    const unsigned full = 0xffffffffu;
+    const int shot = blockIdx.z;
+    const long long fb = (long long)shot * a.fstride;
+    const long long sb = (long long)shot * a.sstride;
     const C zero = C(0);
-    // a warp whose 32 cells all lie inside the frame's interior in z takes
-    // the lean path on rows that are interior in x
+    // box starts: Z0 - 1 rounded down to 16 bytes (Z0 - 1 >= -1)
+    const int zs = (Z0 - 1 + L::HS) / L::HS * L::HS - L::HS;
+    const int zc = (Z0 - 1 + L::HC) / L::HC * L::HC - L::HC;
+    const int of = Z - zs, om = Z - zc;              // this lane's cell in a stage row
+    const int nrows = X1 - X0 + 2;                   // rows X0-1 .. X1
+    if (lane == 0) {
+        for (int d = 0; d < D; ++d) mbar_init(&bars[d], 1);
+        fence_proxy_async();
+    }
+    __syncwarp();
+    // ring: row X0-1+rho lives in slot rho % D, phase (rho / D) & 1
+    auto issue = [&](int rho) {                      // lane 0 only
+        if (rho >= nrows) return;
+        unsigned char *st = ring + (size_t)(rho % D) * L::stage;
+        uint64_t *bar = &bars[rho % D];
+        fence_proxy_async();
+        mbar_expect_tx(bar, L::tx);
+        tma_load_4d(st, &mp.f, zs, X0 - 1 + rho, shot, 0, bar);
+        tma_load_3d(st + L::oM, &mp.m, zc, X0 - 1 + rho, 0, bar);
+    };
+    if (lane == 0)
+        for (int r = 0; r < min(D, nrows); ++r) issue(r);
+    auto wait = [&](int rho) -> bool {
+        return __all_sync(full, mbar_wait(&bars[rho % D], (rho / D) & 1, a.err, 3));
+    };
+    // after a failed wait: give the copies of rows [from, to) a last bounded chance
+    auto drain = [&](int from, int to) {
+        for (int r = from; r < min(to, nrows); ++r) mbar_wait(&bars[r % D], (r / D) & 1, a.err, 3);
+    };
+    auto stage = [&](int rho) { return ring + (size_t)(rho % D) * L::stage; };
+    auto F = [&](const unsigned char *st, int f) -> C {
+        return St::ld(reinterpret_cast<const S *>(st) + f * L::BW + of, a.isc[f]);
+    };
+    auto M = [&](const unsigned char *st, int m) -> C {
+        return reinterpret_cast<const C *>(st + L::oM)[m * L::BWC + om];
+    };
     const bool zint = (Z0 - 1 >= a.np) && (Z0 + 30 <= a.np + a.nz - 1);
-    S *vxo = static_cast<S *>(a.fo[F_VX]) + fb;
-    S *vzo = static_cast<S *>(a.fo[F_VZ]) + fb;
-    S *txxo = static_cast<S *>(a.fo[F_TXX]) + fb;
-    S *tzzo = static_cast<S *>(a.fo[F_TZZ]) + fb;
-    S *txzo = static_cast<S *>(a.fo[F_TXZ]) + fb;
     EZProf<C> zp{C(1), C(1), C(1), C(1)};
     if (zin) {
         const C *pr = static_cast<const C *>(a.prof);
         const EisoProf P{a.NX, a.NZ};
         zp = EZProf<C>{pr[P.azn() + Z], pr[P.bzn() + Z], pr[P.azh() + Z], pr[P.bzh() + Z]};
     }
+    S *vxo = static_cast<S *>(a.fo[F_VX]) + fb;
+    S *vzo = static_cast<S *>(a.fo[F_VZ]) + fb;
+    S *txxo = static_cast<S *>(a.fo[F_TXX]) + fb;
+    S *tzzo = static_cast<S *>(a.fo[F_TZZ]) + fb;
+    S *txzo = static_cast<S *>(a.fo[F_TXZ]) + fb;
 
     // ---- prologue: vx of row X0 and vz of row X0-1 (recomputed; stored
     // only for X0 == 0, the row no other warp's march reaches) ----
-    ERow<C> p = e_load_row<S>(a, fb, X0 - 1, Z);
-    ERow<C> c = e_load_row<S>(a, fb, X0, Z);
-    ERow<C> n = e_load_row<S>(a, fb, X0 + 1, Z);
     ESplit<C> sp;
     e_load_split<S, C>(a, sb, X0 - 1, Z, zin, sp);
+    if (!wait(0) || !wait(1)) { drain(0, D); return; }
     C vxc, vzp;
     {
-        const C txz_zm = __shfl_up_sync(full, c.txz, 1);
-        vxc = zin ? e_vx<S, C>(a, sb, X0, Z, c.vx, c.b, r_sub(c.txx, p.txx),
-                               r_sub(c.txz, txz_zm), sp.vx, zp, X0 == 0 && own)
+        const unsigned char *p = stage(0), *c = stage(1);
+        const C c_txz = F(c, F_TXZ), p_tzz = F(p, F_TZZ);
+        const C txz_zm = __shfl_up_sync(full, c_txz, 1);
+        const C tzz_zp = __shfl_down_sync(full, p_tzz, 1);
+        vxc = zin ? e_vx<S, C>(a, sb, X0, Z, F(c, F_VX), M(c, M_B), r_sub(F(c, F_TXX), F(p, F_TXX)),
+                               r_sub(c_txz, txz_zm), sp.vx, zp, X0 == 0 && own)
                   : zero;
         if (X0 == 0 && own) St::st(vxo + (long long)X0 * a.pitch + Z, vxc, a.sc[F_VX]);
-        const C tzz_zp = __shfl_down_sync(full, p.tzz, 1);
         vzp = zero;
         if (X0 >= 1 && zin)
-            vzp = e_vz<S, C>(a, sb, X0 - 1, Z, p.vz, p.bm, r_sub(c.txz, p.txz),
-                             r_sub(tzz_zp, p.tzz), sp.vz, zp, false);
+            vzp = e_vz<S, C>(a, sb, X0 - 1, Z, F(p, F_VZ), M(p, M_BM), r_sub(c_txz, F(p, F_TXZ)),
+                             r_sub(tzz_zp, p_tzz), sp.vz, zp, false);
     }
-    ERow<C> nn = e_load_row<S>(a, fb, X0 + 2, Z);
-    e_load_split<S, C>(a, sb, X0, Z, zin, sp);
-    // rows [Xf0, Xf1) take e_fast_row, four at a time: X >= np, X + 1 still
-    // interior, X + 3 on the grid
-    const int Xf1 = zint ? min(X1, min(a.np + a.nx - 1, a.NX - 3)) : X1;
+    __syncwarp();
+    if (lane == 0) issue(D);                         // row X0-1 is done with
 
-    for (int X = X0; X < X1;) {
-        if (zint && X >= a.np && X + 4 <= Xf1) {
-            ERow<C> r3;
-            do {
-                e_fast_row<S, C>(a, fb, X, Z, own, c, n, r3, vxc, vzp);
-                e_fast_row<S, C>(a, fb, X + 1, Z, own, n, nn, c, vxc, vzp);
-                e_fast_row<S, C>(a, fb, X + 2, Z, own, nn, r3, n, vxc, vzp);
-                e_fast_row<S, C>(a, fb, X + 3, Z, own, r3, c, nn, vxc, vzp);
-                // rows X+4, X+5, X+6 now sit in c, n, nn
-                X += 4;
-            } while (X + 4 <= Xf1);
-            if (X >= X1) break;
-            e_load_split<S, C>(a, sb, X, Z, zin, sp);
-            continue;
+    // Lean loop: every row of this warp's march, and the next one, lies in
+    // the interior update region, so no frame tests and no split parts; the
+    // arithmetic is the general loop's interior branch, operation for
+    // operation.
+    if (zint && X0 >= a.np && X1 <= a.np + a.nx - 1) {
+        long long q = fb + (long long)X0 * a.pitch + Z;
+        S *const fo0 = static_cast<S *>(a.fo[0]);   // the five arrays of the new set
+        const long long fso = static_cast<S *>(a.fo[1]) - fo0;
+        for (int rc = 1; rc <= X1 - X0; ++rc, q += a.pitch) {
+            if (!wait(rc + 1)) { drain(rc + 1, rc + D); return; }
+            const S *cf = reinterpret_cast<const S *>(stage(rc)) + of;
+            const S *nf = reinterpret_cast<const S *>(stage(rc + 1)) + of;
+            const C *cm = reinterpret_cast<const C *>(stage(rc) + L::oM) + om;
+            const C *nm = reinterpret_cast<const C *>(stage(rc + 1) + L::oM) + om;
+            const C n_txz = St::ld(nf + F_TXZ * L::BW, a.isc[F_TXZ]);
+            const C c_txz = St::ld(cf + F_TXZ * L::BW, a.isc[F_TXZ]);
+            const C c_tzz = St::ld(cf + F_TZZ * L::BW, a.isc[F_TZZ]);
+            const C c_txx = St::ld(cf + F_TXX * L::BW, a.isc[F_TXX]);
+            const C n_txx = St::ld(nf + F_TXX * L::BW, a.isc[F_TXX]);
+            const C n_vx = St::ld(nf + F_VX * L::BW, a.isc[F_VX]);
+            const C c_vz = St::ld(cf + F_VZ * L::BW, a.isc[F_VZ]);
+            const C n_b = nm[M_B * L::BWC], c_bm = cm[M_BM * L::BWC];
+            const C la = cm[M_LA * L::BWC], l2m = cm[M_L2M * L::BWC], mu = cm[M_MU * L::BWC];
+            const C txz_zm = __shfl_up_sync(full, n_txz, 1);
+            const C tzz_zp = __shfl_down_sync(full, c_tzz, 1);
+            const C ax = r_sub(n_txx, c_txx), az = r_sub(n_txz, txz_zm);
+            const C bx = r_sub(n_txz, c_txz), bz = r_sub(tzz_zp, c_tzz);
+            const C vxn = r_fma(n_b, r_add(ax, az), n_vx);
+            const C vzn = r_fma(c_bm, r_add(bx, bz), c_vz);
+            const C vz_zm = __shfl_up_sync(full, vzn, 1);
+            const C vx_zp = __shfl_down_sync(full, vxc, 1);
+            const C sax = r_sub(vxn, vxc), saz = r_sub(vzn, vz_zm);
+            const C sbz = r_sub(vx_zp, vxc), sbx = r_sub(vzn, vzp);
+            const C txx = r_add(c_txx, r_fma(l2m, sax, r_mul(la, saz)));
+            const C tzz = r_add(c_tzz, r_fma(l2m, saz, r_mul(la, sax)));
+            const C txz = r_fma(mu, r_add(sbz, sbx), c_txz);
+            __syncwarp();
+            if (lane == 0) issue(rc + D);            // row X0-1+rc is done with
+            if (own) {
+                S *o = fo0 + q;
+                St::st(o + F_VX * fso + a.pitch, vxn, a.sc[F_VX]);
+                St::st(o + F_VZ * fso, vzn, a.sc[F_VZ]);
+                St::st(o + F_TXX * fso, txx, a.sc[F_TXX]);
+                St::st(o + F_TZZ * fso, tzz, a.sc[F_TZZ]);
+                St::st(o + F_TXZ * fso, txz, a.sc[F_TXZ]);
+            }
+            vxc = vxn;
+            vzp = vzn;
         }
-        ERow<C> n3 = e_load_row<S>(a, fb, X + 3, Z);   // prefetch
-        if (a.pfd > 0 && zin && X + a.pfd < a.NX) e_prefetch_row<S, C>(a, fb, X + a.pfd, Z);
+        return;
+    }
+
+    e_load_split<S, C>(a, sb, X0, Z, zin, sp);
+    for (int X = X0; X < X1; ++X) {
+        const int rc = X - X0 + 1;                   // row X; row X+1 is rc + 1
         ESplit<C> sn;
         e_load_split<S, C>(a, sb, X + 1, Z, zin && X + 1 < X1, sn);
+        if (!wait(rc + 1)) { drain(rc + 1, rc + D); return; }
+        const unsigned char *c = stage(rc), *n = stage(rc + 1);
         const bool fast = zint && X >= a.np && X + 1 <= a.np + a.nx - 1;
         const long long q = (long long)X * a.pitch + Z;
-        // ---- velocities: vx(X+1), vz(X) ----
-        const C txz_zm = __shfl_up_sync(full, n.txz, 1);
-        const C tzz_zp = __shfl_down_sync(full, c.tzz, 1);
-        const C ax = r_sub(n.txx, c.txx), az = r_sub(n.txz, txz_zm);
-        const C bx = r_sub(n.txz, c.txz), bz = r_sub(tzz_zp, c.tzz);
+        // ---- velocities: vx(X+1), vz(X) (propagate.c:2511-2588, pml.c:39-680) ----
+        const C n_txz = F(n, F_TXZ), c_txz = F(c, F_TXZ), c_tzz = F(c, F_TZZ);
+        const C c_txx = F(c, F_TXX);
+        const C txz_zm = __shfl_up_sync(full, n_txz, 1);
+        const C tzz_zp = __shfl_down_sync(full, c_tzz, 1);
+        const C ax = r_sub(F(n, F_TXX), c_txx), az = r_sub(n_txz, txz_zm);
+        const C bx = r_sub(n_txz, c_txz), bz = r_sub(tzz_zp, c_tzz);
         C vxn, vzn;
         if (fast) {
-            vxn = r_fma(n.b, r_add(ax, az), n.vx);
-            vzn = r_fma(c.bm, r_add(bx, bz), c.vz);
+            vxn = r_fma(M(n, M_B), r_add(ax, az), F(n, F_VX));
+            vzn = r_fma(M(c, M_BM), r_add(bx, bz), F(c, F_VZ));
         } else {
             vxn = (X + 1 < a.NX && zin)
-                      ? e_vx<S, C>(a, sb, X + 1, Z, n.vx, n.b, ax, az, sp.vx, zp, own)
+                      ? e_vx<S, C>(a, sb, X + 1, Z, F(n, F_VX), M(n, M_B), ax, az, sp.vx, zp, own)
                       : zero;
-            vzn = zin ? e_vz<S, C>(a, sb, X, Z, c.vz, c.bm, bx, bz, sp.vz, zp, own) : zero;
+            vzn = zin ? e_vz<S, C>(a, sb, X, Z, F(c, F_VZ), M(c, M_BM), bx, bz, sp.vz, zp, own) : zero;
         }
         // ---- stresses of row X (propagate.c:2590-2670, pml.c:684-1403) ----
         const C vz_zm = __shfl_up_sync(full, vzn, 1);
         const C vx_zp = __shfl_down_sync(full, vxc, 1);
         const C sax = r_sub(vxn, vxc), saz = r_sub(vzn, vz_zm);   // txx, tzz
         const C sbz = r_sub(vx_zp, vxc), sbx = r_sub(vzn, vzp);   // txz
+        const C la = M(c, M_LA), l2m = M(c, M_L2M), mu = M(c, M_MU);
         C txx, tzz, txz;
         if (fast || (zin && e_inside(a, X, Z))) {
-            txx = r_add(c.txx, r_fma(c.l2m, sax, r_mul(c.la, saz)));
-            tzz = r_add(c.tzz, r_fma(c.l2m, saz, r_mul(c.la, sax)));
-            txz = r_fma(c.mu, r_add(sbz, sbx), c.txz);
+            txx = r_add(c_txx, r_fma(l2m, sax, r_mul(la, saz)));
+            tzz = r_add(c_tzz, r_fma(l2m, saz, r_mul(la, sax)));
+            txz = r_fma(mu, r_add(sbz, sbx), c_txz);
         } else if (zin) {
             const C *pr = static_cast<const C *>(a.prof);
             const EisoProf P{a.NX, a.NZ};
             const long long cc = sb + e_pml_index(a, X, Z);
             const C Axh = pr[P.axh() + X], Bxh = pr[P.bxh() + X];
-            txx = e_frame<S, C>(a, F_TXX, cc, Axh, Bxh, zp.An, zp.Bn, sp.t[0], sp.t[1], c.l2m,
-                                c.la, sax, saz, own);
-            tzz = e_frame<S, C>(a, F_TZZ, cc, Axh, Bxh, zp.An, zp.Bn, sp.t[2], sp.t[3], c.la,
-                                c.l2m, sax, saz, own);
+            txx = e_frame<S, C>(a, F_TXX, cc, Axh, Bxh, zp.An, zp.Bn, sp.t[0], sp.t[1], l2m, la,
+                                sax, saz, own);
+            tzz = e_frame<S, C>(a, F_TZZ, cc, Axh, Bxh, zp.An, zp.Bn, sp.t[2], sp.t[3], la, l2m,
+                                sax, saz, own);
             txz = e_frame<S, C>(a, F_TXZ, cc, pr[P.axn() + X], pr[P.bxn() + X], zp.Ah, zp.Bh,
-                                sp.t[4], sp.t[5], c.mu, c.mu, sbx, sbz, own);
+                                sp.t[4], sp.t[5], mu, mu, sbx, sbz, own);
         } else {
             txx = tzz = txz = zero;
         }
+        __syncwarp();
+        if (lane == 0) issue(rc + D);                // row X is done with
         if (own) {
             if (X + 1 < a.NX) St::st(vxo + q + a.pitch, vxn, a.sc[F_VX]);
             St::st(vzo + q, vzn, a.sc[F_VZ]);
@@ -395,11 +401,7 @@ __global__ void __launch_bounds__(32 * W, MINB) eiso_step_kernel(const EisoArgs 
         }
         vxc = vxn;
         vzp = vzn;
-        c = n;
-        n = nn;
-        nn = n3;
         sp = sn;
-        ++X;
     }
 }
 
@@ -693,13 +695,23 @@ struct sm_eiso {
     EisoArgs args{};
     // two buffer sets of wavefields and split parts: a step reads set `cur`
     // and writes the other one
-    DevBuf fields[2][5], xpart[2][5], zpart[2][5], mat[5], prof;
+    // the five wavefields of a set are one allocation ([field][shot][x][z],
+    // so one TMA box can span all five), likewise the five materials
+    DevBuf fset[2], xpart[2][5], zpart[2][5], matbuf, prof;
+    void *field(int set, int f) const {
+        return static_cast<char *>(fset[set].p) + (size_t)f * fset_stride;
+    }
+    void *mat(int k) const { return static_cast<char *>(matbuf.p) + (size_t)k * mat_stride; }
+    size_t fset_stride = 0, mat_stride = 0;   // bytes between consecutive arrays
     int cur = 0;
     int chunk = 0;   // rows per warp march (0: chosen from the grid size)
-    int config = 4;  // index into kEisoConfigs
+    int config = 5;  // index into kEisoConfigs (tile 8 x 32: fastest on B200 for
+                     // 64 x 1040 x 540 FP32/FP16 and 440 x 440 single shots)
     DevBuf err;      // bounded-wait failure flag of the tiled kernel
-    EisoMaps maps[2];            // TMA maps of each buffer set
+    EisoMaps maps[2];            // TMA maps of each buffer set (tile kernel)
     int maps_key = -1;           // (TX, TZ) the maps were built for
+    EisoBandMaps band_maps[2];   // TMA maps of each buffer set (band kernel)
+    bool band_maps_ok = false;
     int sms = 148;
     // sources
     std::vector<std::vector<SrcEntry>> shot_src;     // per shot (voff local)
@@ -734,43 +746,70 @@ int eiso_check(sm_eiso_t h) {
 void eiso_bind(sm_eiso *h) {
     const int c = h->cur, o = 1 - h->cur;
     for (int f = 0; f < 5; ++f) {
-        h->args.f[f] = h->fields[c][f].p;
+        h->args.f[f] = h->field(c, f);
         h->args.fx[f] = h->xpart[c][f].p;
         h->args.fz[f] = h->zpart[c][f].p;
-        h->args.fo[f] = h->fields[o][f].p;
+        h->args.fo[f] = h->field(o, f);
         h->args.fxo[f] = h->xpart[o][f].p;
         h->args.fzo[f] = h->zpart[o][f].p;
     }
 }
 
-// launch configurations of the step kernel.  tile: TX x TZ tiles, NT
-// threads per CTA; march (tx == 0): warps per CTA `nt`, L2 prefetch distance.
-// minb = minimum resident CTAs per SM the register allocation is held to.
+// launch configurations of the step kernel.
+//   tile (kind 0): p = {TX, TZ, threads, min CTAs per SM}
+//   band (kind 1): p = {warps per CTA, ring depth D, min CTAs per SM, -}
+// The minimum resident CTAs per SM caps the registers a thread may use.
 struct EisoConfig {
-    int tx, tz, nt, minb, pfd;
+    int kind;
+    int p[4];
 };
 static const EisoConfig kEisoConfigs[] = {
-    {16, 64, 256, 2, 0}, {8, 64, 256, 3, 0}, {16, 128, 256, 1, 0}, {32, 64, 256, 1, 0},
-    {8, 32, 128, 6, 0},  {16, 32, 128, 4, 0}, {0, 0, 4, 5, 0},     {0, 0, 2, 12, 0}};
+    {1, {4, 4, 8, 0}}, {1, {4, 8, 4, 0}}, {1, {2, 8, 8, 0}},     {1, {8, 4, 3, 0}},
+    {1, {2, 4, 16, 0}}, {0, {8, 32, 128, 6}}, {0, {16, 64, 256, 2}}, {0, {8, 64, 256, 3}}};
+static const int kEisoNumConfigs = sizeof(kEisoConfigs) / sizeof(kEisoConfigs[0]);
 
 template <typename S, int TX, int TZ>
-int eiso_make_maps(sm_eiso *h) {
+int eiso_make_tile_maps(sm_eiso *h) {
     using L = ETile<S, TX, TZ>;
     const int key = TX * 4096 + TZ;
     if (h->maps_key == key) return SM_OK;
     for (int b = 0; b < 2; ++b)
         for (int f = 0; f < 5; ++f)
-            if (int rc = make_map_3d(&h->maps[b].f[f], h->fields[b][f].p, MapType<S>::v, sizeof(S),
+            if (int rc = make_map_3d(&h->maps[b].f[f], h->field(b, f), MapType<S>::v, sizeof(S),
                                      h->NZ, h->NX, h->nshots, h->pitch, L::BZ, L::RX))
                 return rc;
     h->maps_key = key;
     return SM_OK;
 }
 
+template <typename S>
+int eiso_make_band_maps(sm_eiso *h) {
+    using L = EBand<S>;
+    using C = typename Store<S>::C;
+    if (h->band_maps_ok) return SM_OK;
+    const size_t e = sizeof(S), c = sizeof(C), row = (size_t)h->pitch;
+    const size_t fdims[4] = {(size_t)h->NZ, (size_t)h->NX, h->nshots, 5};
+    const size_t fstr[3] = {row * e, h->NX * row * e, h->fset_stride};
+    const unsigned fbox[4] = {(unsigned)L::BW, 1, 1, 5};
+    const size_t mdims[3] = {(size_t)h->NZ, (size_t)h->NX, 5};
+    const size_t mstr[2] = {row * c, h->mat_stride};
+    const unsigned mbox[3] = {(unsigned)L::BWC, 1, 5};
+    for (int b = 0; b < 2; ++b) {
+        if (int rc = make_map_nd(&h->band_maps[b].f, h->fset[b].p, MapType<S>::v, e, 4, fdims,
+                                 fstr, fbox))
+            return rc;
+        if (int rc = make_map_nd(&h->band_maps[b].m, h->matbuf.p, MapType<C>::v, c, 3, mdims, mstr,
+                                 mbox))
+            return rc;
+    }
+    h->band_maps_ok = true;
+    return SM_OK;
+}
+
 template <typename S, int TX, int TZ, int NT, int MINB>
 int launch_tile_cfg(sm_eiso *h) {
     using L = ETile<S, TX, TZ>;
-    if (int rc = eiso_make_maps<S, TX, TZ>(h)) return rc;
+    if (int rc = eiso_make_tile_maps<S, TX, TZ>(h)) return rc;
     static bool attr = false;   // per instantiation
     if (!attr) {
         SM_CUDA_TRY(cudaFuncSetAttribute(eiso_tile_kernel<S, TX, TZ, NT, MINB>,
@@ -783,15 +822,31 @@ int launch_tile_cfg(sm_eiso *h) {
     return SM_OK;
 }
 
+template <typename S, int W, int D, int MINB>
+int launch_band_cfg(sm_eiso *h) {
+    using L = EBand<S>;
+    if (int rc = eiso_make_band_maps<S>(h)) return rc;
+    const size_t bytes = W * L::warp_bytes(D);
+    static bool attr = false;   // per instantiation
+    if (!attr) {
+        SM_CUDA_TRY(cudaFuncSetAttribute(eiso_band_kernel<S, W, D, MINB>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
+        attr = true;
+    }
+    const int wz = (h->NZ + 29) / 30;
+    dim3 grd((wz + W - 1) / W, (h->NX + h->args.chunk - 1) / h->args.chunk, (unsigned)h->nshots);
+    eiso_band_kernel<S, W, D, MINB><<<grd, 32 * W, bytes, h->stream>>>(h->args,
+                                                                      h->band_maps[h->cur]);
+    return SM_OK;
+}
+
 template <typename S>
 size_t eiso_config_smem(int config) {
     const EisoConfig &k = kEisoConfigs[config];
-    if (k.tx == 16 && k.tz == 64) return ETile<S, 16, 64>::bytes;
-    if (k.tx == 8 && k.tz == 64) return ETile<S, 8, 64>::bytes;
-    if (k.tx == 16 && k.tz == 128) return ETile<S, 16, 128>::bytes;
-    if (k.tx == 32 && k.tz == 64) return ETile<S, 32, 64>::bytes;
-    if (k.tx == 8 && k.tz == 32) return ETile<S, 8, 32>::bytes;
-    if (k.tx == 16 && k.tz == 32) return ETile<S, 16, 32>::bytes;
+    if (k.kind == 1) return k.p[0] * EBand<S>::warp_bytes(k.p[1]);
+    if (k.p[0] == 8 && k.p[1] == 32) return ETile<S, 8, 32>::bytes;
+    if (k.p[0] == 16 && k.p[1] == 64) return ETile<S, 16, 64>::bytes;
+    if (k.p[0] == 8 && k.p[1] == 64) return ETile<S, 8, 64>::bytes;
     return 0;
 }
 
@@ -803,45 +858,35 @@ size_t eiso_config_smem_prec(int precision, int config) {
     default: return eiso_config_smem<float>(config);
     }
 }
-static const int kEisoNumConfigs = sizeof(kEisoConfigs) / sizeof(kEisoConfigs[0]);
 
-// rows per warp march: long enough that the two rows re-read at each chunk
-// start stay cheap, short enough to give every SM about 48 warps
+// rows per warp march of the band kernel: long enough that the rows
+// re-read at each chunk start stay cheap, short enough for about three
+// waves of 32 warps per SM (the last wave's tail stays small)
 int eiso_pick_chunk(const sm_eiso *h) {
     if (h->chunk > 0) return h->chunk;
     const int sms = h->sms;
     const long long wz = (h->NZ + 29) / 30;
-    const long long want = (long long)sms * 48;
+    const long long want = (long long)sms * 96;
     long long per = wz * (long long)h->nshots;                 // warps per row band
     long long bands = (want + per - 1) / per;                  // row bands wanted
     long long c = (h->NX + bands - 1) / std::max<long long>(bands, 1);
-    return (int)std::min<long long>(std::max<long long>(c, 16), 256);
-}
-
-template <typename S, int W, int MINB>
-void launch_step_cfg(sm_eiso *h) {
-    const int wz = (h->NZ + 29) / 30;
-    dim3 blk(32 * W, 1, 1);
-    dim3 grd((wz + W - 1) / W, (h->NX + h->args.chunk - 1) / h->args.chunk, (unsigned)h->nshots);
-    eiso_step_kernel<S, W, MINB><<<grd, blk, 0, h->stream>>>(h->args);
+    return (int)std::min<long long>(std::max<long long>(c, 8), 512);
 }
 
 template <typename S>
 int launch_step(sm_eiso *h) {
     h->args.chunk = eiso_pick_chunk(h);
-    const EisoConfig &k = kEisoConfigs[h->config];
-    h->args.pfd = k.pfd;
     cudaEvent_t t0 = h->timer.begin(h->stream);
     int rc = SM_OK;
     switch (h->config) {
-    case 0: rc = launch_tile_cfg<S, 16, 64, 256, 2>(h); break;
-    case 1: rc = launch_tile_cfg<S, 8, 64, 256, 3>(h); break;
-    case 2: rc = launch_tile_cfg<S, 16, 128, 256, 1>(h); break;
-    case 3: rc = launch_tile_cfg<S, 32, 64, 256, 1>(h); break;
-    case 4: rc = launch_tile_cfg<S, 8, 32, 128, 6>(h); break;
-    case 5: rc = launch_tile_cfg<S, 16, 32, 128, 4>(h); break;
-    case 6: launch_step_cfg<S, 4, 5>(h); break;
-    default: launch_step_cfg<S, 2, 12>(h); break;
+    case 0: rc = launch_band_cfg<S, 4, 4, 8>(h); break;
+    case 1: rc = launch_band_cfg<S, 4, 8, 4>(h); break;
+    case 2: rc = launch_band_cfg<S, 2, 8, 8>(h); break;
+    case 3: rc = launch_band_cfg<S, 8, 4, 3>(h); break;
+    case 4: rc = launch_band_cfg<S, 2, 4, 16>(h); break;
+    case 5: rc = launch_tile_cfg<S, 8, 32, 128, 6>(h); break;
+    case 6: rc = launch_tile_cfg<S, 16, 64, 256, 2>(h); break;
+    default: rc = launch_tile_cfg<S, 8, 64, 256, 3>(h); break;
     }
     if (rc) return rc;
     h->timer.end(t0, h->stream);
@@ -887,7 +932,7 @@ int eiso_rescale(sm_eiso *h) {
     static const char *names[5] = {"vx", "vz", "txx", "tzz", "txz"};
     const size_t fcells = (size_t)h->NX * h->pitch * h->nshots;
     for (int f = 0; f < 5; ++f) {
-        ptrs[3 * f] = h->fields[h->cur][f].p; ns[3 * f] = fcells; groups[3 * f] = f;
+        ptrs[3 * f] = h->field(h->cur, f); ns[3 * f] = fcells; groups[3 * f] = f;
         ptrs[3 * f + 1] = h->xpart[h->cur][f].p; ns[3 * f + 1] = h->npml_cells * h->nshots; groups[3 * f + 1] = f;
         ptrs[3 * f + 2] = h->zpart[h->cur][f].p; ns[3 * f + 2] = h->npml_cells * h->nshots; groups[3 * f + 2] = f;
     }
@@ -1075,14 +1120,16 @@ extern "C" int sm_eiso_create(int device, size_t nx, size_t nz, size_t npml, dou
     const size_t cplx = precision == SM_FP64 ? 8 : 4;    // compute type bytes
     const size_t fcells = NX * (size_t)h->pitch;
     int rc;
-    for (int f = 0; f < 5; ++f) {
-        for (int k = 0; k < 2; ++k) {
-            if ((rc = h->fields[k][f].alloc(fcells * nshots * h->elem))) return rc;
+    h->fset_stride = fcells * nshots * h->elem;
+    h->mat_stride = fcells * cplx;
+    for (int k = 0; k < 2; ++k) {
+        if ((rc = h->fset[k].alloc(5 * h->fset_stride))) return rc;
+        for (int f = 0; f < 5; ++f) {
             if ((rc = h->xpart[k][f].alloc(h->npml_cells * nshots * h->elem))) return rc;
             if ((rc = h->zpart[k][f].alloc(h->npml_cells * nshots * h->elem))) return rc;
         }
-        if ((rc = h->mat[f].alloc(fcells * cplx))) return rc;
     }
+    if ((rc = h->matbuf.alloc(5 * h->mat_stride))) return rc;
     EisoProf P{(int)NX, (int)NZ};
     if ((rc = h->prof.alloc((size_t)P.size() * cplx))) return rc;
     if ((rc = h->err.alloc(sizeof(int)))) return rc;
@@ -1110,8 +1157,8 @@ extern "C" int sm_eiso_create(int device, size_t nx, size_t nz, size_t npml, dou
                     m[X * h->pitch + Z] = s * src[k][idx];
                 }
             }
-            rc = precision == SM_FP64 ? upload_convert<double>(h->mat[k].p, m.data(), fcells, h->stream)
-                                      : upload_convert<float>(h->mat[k].p, m.data(), fcells, h->stream);
+            rc = precision == SM_FP64 ? upload_convert<double>(h->mat(k), m.data(), fcells, h->stream)
+                                      : upload_convert<float>(h->mat(k), m.data(), fcells, h->stream);
             if (rc) return rc;
         }
     }
@@ -1149,7 +1196,7 @@ extern "C" int sm_eiso_create(int device, size_t nx, size_t nz, size_t npml, dou
     a.right_off = (int)(npml * NZ + nx * 2 * npml);
     eiso_bind(h.get());
     for (int f = 0; f < 5; ++f) {
-        a.mat[f] = h->mat[f].p;
+        a.mat[f] = h->mat(f);
         a.sc[f] = 1.0f;
         a.isc[f] = 1.0f;
     }
@@ -1180,12 +1227,13 @@ extern "C" int sm_eiso_create(int device, size_t nx, size_t nz, size_t npml, dou
 extern "C" int sm_eiso_reset(sm_eiso_t h) {
     if (int rc = eiso_check(h)) return rc;
     DeviceGuard g(h->device);
-    for (int k = 0; k < 2; ++k)
+    for (int k = 0; k < 2; ++k) {
+        if (int rc = h->fset[k].zero(h->stream)) return rc;
         for (int f = 0; f < 5; ++f) {
-            if (int rc = h->fields[k][f].zero(h->stream)) return rc;
             if (int rc = h->xpart[k][f].zero(h->stream)) return rc;
             if (int rc = h->zpart[k][f].zero(h->stream)) return rc;
         }
+    }
     h->cur = 0;
     eiso_bind(h);
     if (int rc = h->d_traces.zero(h->stream)) return rc;
@@ -1381,7 +1429,7 @@ extern "C" int sm_eiso_get_field(sm_eiso_t h, size_t shot, int comp, int part, d
     if (part == SM_PART_TOTAL) {
         std::vector<unsigned char> buf(NX * (size_t)h->pitch * e);
         SM_CUDA_TRY(cudaMemcpy(buf.data(),
-                               static_cast<char *>(h->fields[h->cur][f].p) + shot * h->args.fstride * e,
+                               static_cast<char *>(h->field(h->cur, f)) + shot * h->args.fstride * e,
                                buf.size(), cudaMemcpyDeviceToHost));
         for (size_t X = 0; X < NX; ++X)
             for (size_t Z = 0; Z < NZ; ++Z)
@@ -1411,7 +1459,7 @@ extern "C" int sm_eiso_set_field(sm_eiso_t h, size_t shot, int comp, int part, c
     const size_t NX = h->NX, NZ = h->NZ, e = h->elem;
     std::vector<unsigned char> tot(NX * (size_t)h->pitch * e), px(h->npml_cells * e),
         pz(h->npml_cells * e);
-    char *dtot = static_cast<char *>(h->fields[h->cur][f].p) + shot * h->args.fstride * e;
+    char *dtot = static_cast<char *>(h->field(h->cur, f)) + shot * h->args.fstride * e;
     char *dpx = static_cast<char *>(h->xpart[h->cur][f].p) + shot * h->npml_cells * e;
     char *dpz = static_cast<char *>(h->zpart[h->cur][f].p) + shot * h->npml_cells * e;
     SM_CUDA_TRY(cudaMemcpy(tot.data(), dtot, tot.size(), cudaMemcpyDeviceToHost));
