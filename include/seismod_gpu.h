@@ -186,6 +186,18 @@ int sm_eiso_get_chunk(sm_eiso_t h, int *chunk);
  * an index in [0, *nconfigs); results do not depend on it */
 int sm_eiso_set_config(sm_eiso_t h, int config);
 int sm_eiso_get_config(sm_eiso_t h, int *config, int *nconfigs);
+/* Autotuner: times every launch configuration that fits (and a few march
+ * lengths) for trial_steps steps (<= 0: 20) from a zero state and keeps the
+ * fastest; results are cached per (precision, grid, shots, device) for the
+ * process.  Call at step 0 (or after sm_eiso_reset); the handle is left
+ * reset.  Any output pointer may be NULL. */
+int sm_eiso_autotune(sm_eiso_t h, int trial_steps, int *config, int *chunk, double *ms_per_step);
+/* Replay the time loop as CUDA graphs of `steps` steps (2, 4, 8 or 16; 0
+ * launches every kernel from the host, the default).  Results are the same
+ * either way.  Graphs are captured lazily and again after new sources,
+ * receivers, configurations or 16-bit scales; per-kernel timing
+ * (sm_eiso_set_timing) launches without graphs. */
+int sm_eiso_set_graph(sm_eiso_t h, int steps);
 /* Per-kernel timing.  With timing on, every launch of the wavefield update
  * kernel(s) is bracketed by CUDA events on the handle's stream;
  * sm_eiso_kernel_stats synchronises and returns their summed duration and
@@ -234,6 +246,10 @@ int sm_a3d_set_config(sm_a3d_t h, int config);
 /* x planes each CTA marches through (<= 0: the library's choice) */
 int sm_a3d_set_chunk(sm_a3d_t h, int chunk);
 int sm_a3d_get_config(sm_a3d_t h, int *config, int *nconfigs);
+/* autotuner and CUDA-graph replay, as sm_eiso_autotune / sm_eiso_set_graph
+ * (trial_steps <= 0: 10) */
+int sm_a3d_autotune(sm_a3d_t h, int trial_steps, int *config, int *chunk, double *ms_per_step);
+int sm_a3d_set_graph(sm_a3d_t h, int steps);
 int sm_a3d_set_timing(sm_a3d_t h, int on);
 int sm_a3d_kernel_stats(sm_a3d_t h, int reset, double *update_ms, size_t *update_launches,
                         size_t *all_launches);

@@ -80,11 +80,17 @@ _SIGS = {
     "sm_eiso_get_chunk": (C.c_int, [_vp, C.POINTER(C.c_int)]),
     "sm_eiso_set_config": (C.c_int, [_vp, C.c_int]),
     "sm_eiso_get_config": (C.c_int, [_vp, C.POINTER(C.c_int), C.POINTER(C.c_int)]),
+    "sm_eiso_autotune": (C.c_int, [_vp, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int),
+                                   C.POINTER(C.c_double)]),
+    "sm_eiso_set_graph": (C.c_int, [_vp, C.c_int]),
     "sm_eiso_kernel_stats": (C.c_int, [_vp, C.c_int, _dp, _szp, _szp]),
     "sm_a3d_stream": (C.c_int, [_vp, C.POINTER(_vp)]),
     "sm_a3d_set_timing": (C.c_int, [_vp, C.c_int]),
     "sm_a3d_set_config": (C.c_int, [_vp, C.c_int]),
     "sm_a3d_set_chunk": (C.c_int, [_vp, C.c_int]),
+    "sm_a3d_autotune": (C.c_int, [_vp, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int),
+                                  C.POINTER(C.c_double)]),
+    "sm_a3d_set_graph": (C.c_int, [_vp, C.c_int]),
     "sm_a3d_get_config": (C.c_int, [_vp, _ip, _ip]),
     "sm_a3d_kernel_stats": (C.c_int, [_vp, C.c_int, _dp, _szp, _szp]),
     "sm_e_iso_main": (C.c_int, [C.c_int, C.POINTER(C.c_char_p)]),

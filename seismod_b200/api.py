@@ -147,6 +147,11 @@ class EIsoDevice:
     def sync(self):
         L.check(L.load().sm_eiso_sync(self._h))
 
+    def step_count(self):
+        n = C.c_size_t()
+        L.check(L.load().sm_eiso_step_count(self._h, C.byref(n)))
+        return n.value
+
     def traces(self, shot=0, max_samples=None):
         n = self.nrec[shot]
         counts = np.zeros(n, dtype=np.uintp)
@@ -190,6 +195,17 @@ class EIsoDevice:
 
     def set_config(self, config):
         L.check(L.load().sm_eiso_set_config(self._h, int(config)))
+
+    def autotune(self, trial_steps=20):
+        """Pick the fastest launch configuration (the handle is left reset).
+        Returns (config, chunk, ms per step)."""
+        c, k, ms = C.c_int(), C.c_int(), C.c_double()
+        L.check(L.load().sm_eiso_autotune(self._h, int(trial_steps), C.byref(c), C.byref(k),
+                                          C.byref(ms)))
+        return c.value, k.value, ms.value
+
+    def set_graph(self, steps):
+        L.check(L.load().sm_eiso_set_graph(self._h, int(steps)))
 
     def get_config(self):
         """(current config, number of configs)."""
@@ -254,6 +270,11 @@ class A3DDevice:
     def sync(self):
         L.check(L.load().sm_a3d_sync(self._h))
 
+    def step_count(self):
+        n = C.c_size_t()
+        L.check(L.load().sm_a3d_step_count(self._h, C.byref(n)))
+        return n.value
+
     def traces(self):
         n = self.nrec
         counts = np.zeros(n, dtype=np.uintp)
@@ -280,6 +301,17 @@ class A3DDevice:
 
     def set_chunk(self, chunk):
         L.check(L.load().sm_a3d_set_chunk(self._h, int(chunk)))
+
+    def autotune(self, trial_steps=10):
+        """Pick the fastest launch configuration (the handle is left reset).
+        Returns (config, chunk, ms per step)."""
+        c, k, ms = C.c_int(), C.c_int(), C.c_double()
+        L.check(L.load().sm_a3d_autotune(self._h, int(trial_steps), C.byref(c), C.byref(k),
+                                         C.byref(ms)))
+        return c.value, k.value, ms.value
+
+    def set_graph(self, steps):
+        L.check(L.load().sm_a3d_set_graph(self._h, int(steps)))
 
     def get_config(self):
         c, n = C.c_int(), C.c_int()

@@ -18,8 +18,11 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <map>
 #include <memory>
+#include <mutex>
 #include <new>
+#include <tuple>
 #include <vector>
 
 #include "sm_common.cuh"
@@ -52,6 +55,8 @@ struct A3Args {
     int nx2, ny2, nz2, pitch, np;
     int sx, sy;                // strides of i and j in elements (grids < 2^31 cells)
     int *err;                  // set by a kernel whose bounded wait gave up
+    long long *step;           // steps begun; the step kernel counts, source and
+                               // receiver kernels of step it read it + 1
     void *f[4];                // wavefields read this step
     void *psi[6];              // CPML memory variables read this step
     void *fo[4];               // ... and written this step (the other buffer)
@@ -185,6 +190,7 @@ __global__ void __launch_bounds__(32 * W, MINB)
 
     const int lane = threadIdx.x, w = threadIdx.y;
     const int tid = w * 32 + lane;
+    if ((blockIdx.x | blockIdx.y | blockIdx.z | tid) == 0) ++*a.step;
     const int k0 = blockIdx.x * 32, j0 = blockIdx.y * TY;
     const int k = k0 + lane;
     const int i0 = blockIdx.z * a.chunk;
@@ -494,11 +500,11 @@ struct A3Src {
 };
 
 template <typename S>
-__global__ void a3d_source_kernel(A3Args a, const A3Src *src, int nsrc, const double *vals,
-                                  long long it) {
+__global__ void a3d_source_kernel(A3Args a, const A3Src *src, int nsrc, const double *vals) {
     using St = Store<S>;
     using C = typename Store<S>::C;
     if (blockIdx.x != 0 || threadIdx.x != 0) return;
+    const long long it = *a.step - 1;
     // one thread, in source order, as a_iso_3d.c:689-693
     S *P = static_cast<S *>(a.f[A_P]);
     for (int e = 0; e < nsrc; ++e) {
@@ -517,9 +523,10 @@ struct A3Rec {
 
 template <typename S>
 __global__ void a3d_gather_kernel(A3Args a, const A3Rec *rec, int nrec, const int32_t *table,
-                                  long long nsteps_max, long long it, double *traces) {
+                                  long long nsteps_max, double *traces) {
     using St = Store<S>;
     const int r = blockIdx.x * blockDim.x + threadIdx.x;
+    const long long it = *a.step - 1;
     if (r >= nrec || it >= nsteps_max) return;
     const A3Rec e = rec[r];
     const int32_t slot = table[(long long)e.group * nsteps_max + it];
@@ -559,6 +566,20 @@ struct sm_a3d {
     A3Maps maps[2];                            // TMA maps with set b as input
     int maps_ty = -1;                          // tile rows the maps were made for
     DevBuf err;                                // kernel timeout flag
+    DevBuf d_step;                             // device step counter (A3Args::step)
+    // CUDA graphs of graph_steps steps, one per parity of the starting
+    // buffer set; captured again when graph_epoch moved since
+    int graph_steps = 0;
+    unsigned graph_epoch = 1;
+    struct Graph {
+        cudaGraphExec_t exec = nullptr;
+        unsigned epoch = 0;
+        int steps = 0;
+    } graphs[2];
+    ~sm_a3d() {
+        for (Graph &g : graphs)
+            if (g.exec) cudaGraphExecDestroy(g.exec);
+    }
     // 16-bit storage: exponents of the 4 fields (A_*) and 6 memory
     // variables (4 + PS_*), stored = value * 2^expo
     Scaler16 scaler;
@@ -597,16 +618,24 @@ static const A3Config kA3Configs[] = {
 };
 static const int kA3NumConfigs = sizeof(kA3Configs) / sizeof(kA3Configs[0]);
 
+// dynamic shared memory above 48 KB must be allowed per kernel and device
+template <typename S, int W, int R, int D, int MINB>
+int a3d_ready_cfg(sm_a3d *h) {
+    static bool done[64] = {};   // per instantiation and device
+    if (h->device < 0 || h->device >= 64) return sm_fail(SM_EINVAL, "device %d", h->device);
+    if (!done[h->device]) {
+        SM_CUDA_TRY(cudaFuncSetAttribute(a3d_step_kernel<S, W, R, D, MINB>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)a3d_step_smem<S, W * R, D>()));
+        done[h->device] = true;
+    }
+    return SM_OK;
+}
+
 template <typename S, int W, int R, int D, int MINB>
 void a3d_launch_cfg(sm_a3d *h) {
     constexpr int TY = W * R;
     constexpr size_t smem = a3d_step_smem<S, TY, D>();
-    static bool configured = false;   // once per instantiation and process
-    if (!configured) {
-        cudaFuncSetAttribute(a3d_step_kernel<S, W, R, D, MINB>,
-                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        configured = true;
-    }
     dim3 blk(32, W, 1);
     dim3 grd((unsigned)((h->nz2 + 31) / 32), (unsigned)((h->ny2 + TY - 1) / TY),
              (unsigned)((h->nx2 + h->args.chunk - 1) / h->args.chunk));
@@ -672,10 +701,12 @@ int a3d_rescale(sm_a3d *h) {
     static const int groups[10] = {0, 1, 2, 3, 4, 5, 6, 7, 8, 9};
     for (int f = 0; f < 4; ++f) { ptrs[f] = h->f[h->cur][f].p; ns[f] = ncell; }
     for (int q = 0; q < 6; ++q) { ptrs[4 + q] = h->psi[h->cur][q].p; ns[4 + q] = h->psi_cells[q]; }
+    const std::vector<int> before = h->scaler.expo;
     int rc = h->precision == SM_FP16
                  ? h->scaler.check<__half>(h->stream, 10, ptrs, ns, groups, names)
                  : h->scaler.check<__nv_bfloat16>(h->stream, 10, ptrs, ns, groups, names);
     a3d_apply_scales(h);
+    if (h->scaler.expo != before) h->graph_epoch++;   // scales are baked into graphs
     return rc;
 }
 
@@ -710,6 +741,20 @@ size_t a3d_config_smem_prec(int precision, int config) {
 }
 
 template <typename S>
+int a3d_ready(sm_a3d *h) {
+    switch (h->config) {
+    case 0: return a3d_ready_cfg<S, 8, 2, 5, 2>(h);
+    case 1: return a3d_ready_cfg<S, 4, 4, 5, 3>(h);
+    case 2: return a3d_ready_cfg<S, 8, 4, 4, 1>(h);
+    case 3: return a3d_ready_cfg<S, 8, 1, 6, 3>(h);
+    case 4: return a3d_ready_cfg<S, 16, 2, 4, 1>(h);
+    case 5: return a3d_ready_cfg<S, 4, 2, 6, 4>(h);
+    case 6: return a3d_ready_cfg<S, 8, 2, 4, 3>(h);
+    default: return a3d_ready_cfg<S, 4, 8, 4, 2>(h);
+    }
+}
+
+template <typename S>
 void a3d_launch_step(sm_a3d *h) {
     switch (h->config) {
     case 0: a3d_launch_cfg<S, 8, 2, 5, 2>(h); break;
@@ -735,13 +780,12 @@ void a3d_launch(sm_a3d *h) {
     h->timer.launches += 1 + (h->src.empty() ? 0 : 1) + (h->rec.empty() ? 0 : 1);
     if (!h->src.empty())
         a3d_source_kernel<S><<<1, 32, 0, h->stream>>>(h->args, h->d_src.as<A3Src>(),
-                                                      (int)h->src.size(), h->d_vals.as<double>(),
-                                                      (long long)h->it);
+                                                      (int)h->src.size(), h->d_vals.as<double>());
     if (!h->rec.empty()) {
         int n = (int)h->rec.size();
         a3d_gather_kernel<S><<<(n + 127) / 128, 128, 0, h->stream>>>(
             h->args, h->d_rec.as<A3Rec>(), n, h->d_table.as<int32_t>(),
-            (long long)h->plan.nsteps_max, (long long)h->it, h->d_traces.as<double>());
+            (long long)h->plan.nsteps_max, h->d_traces.as<double>());
     }
 }
 
@@ -912,6 +956,8 @@ extern "C" int sm_a3d_create(int device, size_t nx2, size_t ny2, size_t nz2, siz
     if ((rc = h->err.alloc(sizeof(int)))) return rc;
     if ((rc = h->err.zero(h->stream))) return rc;
     a.err = h->err.as<int>();
+    if ((rc = h->d_step.alloc(sizeof(long long)))) return rc;
+    a.step = h->d_step.as<long long>();
     for (int f = 0; f < 4; ++f) { a.sc[f] = 1.f; a.isc[f] = 1.f; }
     for (int p = 0; p < 6; ++p) { a.psc[p] = 1.f; a.pisc[p] = 1.f; }
     cudaDeviceGetAttribute(&h->sms, cudaDevAttrMultiProcessorCount, device);
@@ -940,10 +986,12 @@ extern "C" int sm_a3d_reset(sm_a3d_t h) {
     }
     h->cur = 0;
     if (a3d_is16(h)) {
+        if (h->scaler.expo != h->expo0) h->graph_epoch++;
         h->scaler.expo = h->expo0;
         a3d_apply_scales(h);
     }
     if (int rc = h->d_traces.zero(h->stream)) return rc;
+    if (int rc = h->d_step.zero(h->stream)) return rc;
     SM_CUDA_TRY(cudaStreamSynchronize(h->stream));
     h->it = 0;
     return SM_OK;
@@ -1024,6 +1072,7 @@ extern "C" int sm_a3d_set_receivers(sm_a3d_t h, size_t nrec, const size_t *index
 namespace {
 int a3d_upload(sm_a3d *h) {
     int rc;
+    h->graph_epoch++;
     if (h->src_dirty) {
         if (!h->src.empty()) {
             if ((rc = h->d_src.alloc(h->src.size() * sizeof(A3Src)))) return rc;
@@ -1058,24 +1107,173 @@ int a3d_upload(sm_a3d *h) {
 }
 }  // namespace
 
+namespace {
+
+// the graph of h->graph_steps steps starting from buffer set h->cur
+template <typename S>
+int a3d_graph(sm_a3d *h, cudaGraphExec_t *out) {
+    sm_a3d::Graph &gr = h->graphs[h->cur];
+    if (gr.exec && gr.epoch == h->graph_epoch && gr.steps == h->graph_steps) {
+        *out = gr.exec;
+        return SM_OK;
+    }
+    if (gr.exec) {
+        cudaGraphExecDestroy(gr.exec);
+        gr.exec = nullptr;
+    }
+    const size_t launches = h->timer.launches;
+    const int cur = h->cur;
+    SM_CUDA_TRY(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
+    for (int k = 0; k < h->graph_steps; ++k) a3d_launch<S>(h);
+    cudaGraph_t graph = nullptr;
+    cudaError_t e = cudaStreamEndCapture(h->stream, &graph);
+    h->timer.launches = launches;
+    h->cur = cur;   // an even number of steps: back to the starting set
+    a3d_bind(h, h->cur);
+    if (e != cudaSuccess) {
+        if (graph) cudaGraphDestroy(graph);
+        return sm_fail(SM_ECUDA, "stream capture: %s", cudaGetErrorString(e));
+    }
+    e = cudaGraphInstantiate(&gr.exec, graph, 0);
+    cudaGraphDestroy(graph);
+    if (e != cudaSuccess) {
+        gr.exec = nullptr;
+        return sm_fail(SM_ECUDA, "cudaGraphInstantiate: %s", cudaGetErrorString(e));
+    }
+    gr.epoch = h->graph_epoch;
+    gr.steps = h->graph_steps;
+    *out = gr.exec;
+    return SM_OK;
+}
+
+template <typename S>
+int a3d_run_t(sm_a3d *h, size_t nsteps) {
+    if (int rc = a3d_ready<S>(h)) return rc;
+    const size_t G = (size_t)h->graph_steps;
+    const size_t per_step = 1 + (h->src.empty() ? 0 : 1) + (h->rec.empty() ? 0 : 1);
+    while (nsteps > 0) {
+        if (G && !h->timer.on && h->it % G == 0 && nsteps >= G) {
+            cudaGraphExec_t ex = nullptr;
+            if (int rc = a3d_graph<S>(h, &ex)) return rc;
+            SM_CUDA_TRY(cudaGraphLaunch(ex, h->stream));
+            h->timer.launches += per_step * G;
+            h->it += G;
+            nsteps -= G;
+        } else {
+            a3d_launch<S>(h);
+            h->it++;
+            nsteps--;
+        }
+        if (a3d_is16(h) && h->it % sm_a3d::kScalePeriod == 0)
+            if (int rc = a3d_rescale(h)) return rc;
+    }
+    return SM_OK;
+}
+
+}  // namespace
+
 extern "C" int sm_a3d_run(sm_a3d_t h, size_t nsteps) {
     if (int rc = a3d_check(h)) return rc;
     DeviceGuard g(h->device);
     if (int rc = a3d_ensure_maps(h)) return rc;
     if (h->src_dirty || h->rec_dirty)
         if (int rc = a3d_upload(h)) return rc;
-    for (size_t s = 0; s < nsteps; ++s) {
-        switch (h->precision) {
-        case SM_FP64: a3d_launch<double>(h); break;
-        case SM_FP16: a3d_launch<__half>(h); break;
-        case SM_BF16: a3d_launch<__nv_bfloat16>(h); break;
-        default: a3d_launch<float>(h); break;
-        }
-        h->it++;
-        if (a3d_is16(h) && h->it % sm_a3d::kScalePeriod == 0)
-            if (int rc = a3d_rescale(h)) return rc;
+    int rc;
+    switch (h->precision) {
+    case SM_FP64: rc = a3d_run_t<double>(h, nsteps); break;
+    case SM_FP16: rc = a3d_run_t<__half>(h, nsteps); break;
+    case SM_BF16: rc = a3d_run_t<__nv_bfloat16>(h, nsteps); break;
+    default: rc = a3d_run_t<float>(h, nsteps); break;
     }
+    if (rc) return rc;
     SM_CUDA_TRY(cudaGetLastError());
+    return SM_OK;
+}
+
+extern "C" int sm_a3d_set_graph(sm_a3d_t h, int steps) {
+    if (int rc = a3d_check(h)) return rc;
+    if (steps != 0 && steps != 2 && steps != 4 && steps != 8 && steps != 16)
+        return sm_fail(SM_EINVAL, "sm_a3d_set_graph: steps must be 0, 2, 4, 8 or 16 (got %d)",
+                       steps);
+    h->graph_steps = steps;
+    h->graph_epoch++;
+    return SM_OK;
+}
+
+// Launch-configuration search, as sm_eiso_autotune: every configuration that
+// fits, with a few x-chunk lengths, timed over trial_steps steps from a zero
+// state; the fastest is kept and cached per (precision, grid, device).
+extern "C" int sm_a3d_autotune(sm_a3d_t h, int trial_steps, int *config, int *chunk,
+                               double *ms_per_step) {
+    if (int rc = a3d_check(h)) return rc;
+    if (h->it != 0)
+        return sm_fail(SM_ESTATE, "sm_a3d_autotune: call before the first step (or after reset)");
+    if (trial_steps <= 0) trial_steps = 10;
+    DeviceGuard g(h->device);
+    struct Key {
+        int prec;
+        size_t nx2, ny2, nz2, np;
+        int dev;
+        bool operator<(const Key &o) const {
+            return std::tie(prec, nx2, ny2, nz2, np, dev) <
+                   std::tie(o.prec, o.nx2, o.ny2, o.nz2, o.np, o.dev);
+        }
+    };
+    struct Val {
+        int config, chunk;
+        double ms;
+    };
+    static std::map<Key, Val> cache;
+    static std::mutex mu;
+    const Key key{h->precision, h->nx2, h->ny2, h->nz2, h->np, h->device};
+    Val best{-1, 0, 0.0};
+    bool cached = false;
+    {
+        std::lock_guard<std::mutex> lk(mu);
+        auto it = cache.find(key);
+        if (it != cache.end()) {
+            best = it->second;
+            cached = true;
+        }
+    }
+    int rc = SM_OK;
+    if (!cached) {
+        int lim = 0;
+        SM_CUDA_TRY(cudaDeviceGetAttribute(&lim, cudaDevAttrMaxSharedMemoryPerBlockOptin, h->device));
+        cudaEvent_t e0, e1;
+        SM_CUDA_TRY(cudaEventCreate(&e0));
+        SM_CUDA_TRY(cudaEventCreate(&e1));
+        const bool timing = h->timer.on;
+        h->timer.on = false;
+        for (int c = 0; c < kA3NumConfigs && rc == SM_OK; ++c) {
+            if (a3d_config_smem_prec(h->precision, c) > (size_t)lim) continue;
+            for (int ch : {0, 16, 32, 64}) {
+                if ((rc = sm_a3d_set_config(h, c)) || (rc = sm_a3d_set_chunk(h, ch))) break;
+                if ((rc = sm_a3d_reset(h)) || (rc = sm_a3d_run(h, 2))) break;
+                cudaEventRecord(e0, h->stream);
+                if ((rc = sm_a3d_run(h, (size_t)trial_steps))) break;
+                cudaEventRecord(e1, h->stream);
+                if ((rc = sm_a3d_sync(h))) break;
+                float t = 0.f;
+                cudaEventElapsedTime(&t, e0, e1);
+                const double ms = t / trial_steps;
+                if (best.config < 0 || ms < best.ms) best = Val{c, ch, ms};
+            }
+        }
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+        h->timer.on = timing;
+        if (rc) return rc;
+        if (best.config < 0) return sm_fail(SM_EINVAL, "sm_a3d_autotune: no configuration fits");
+        std::lock_guard<std::mutex> lk(mu);
+        cache[key] = best;
+    }
+    if ((rc = sm_a3d_set_config(h, best.config)) || (rc = sm_a3d_set_chunk(h, best.chunk)) ||
+        (rc = sm_a3d_reset(h)))
+        return rc;
+    if (config) *config = best.config;
+    if (chunk) *chunk = best.chunk;
+    if (ms_per_step) *ms_per_step = best.ms;
     return SM_OK;
 }
 
@@ -1218,6 +1416,7 @@ extern "C" int sm_a3d_set_config(sm_a3d_t h, int config) {
                        a3d_config_smem_prec(h->precision, config), maxsm);
     h->config = config;
     h->args.chunk = a3d_pick_chunk(h->nx2, h->ny2, h->nz2, h->sms, kA3Configs[config].ty());
+    h->graph_epoch++;
     // maps are rebuilt for the new tile height at the next run
     return SM_OK;
 }
@@ -1228,6 +1427,7 @@ extern "C" int sm_a3d_set_chunk(sm_a3d_t h, int chunk) {
         h->args.chunk = a3d_pick_chunk(h->nx2, h->ny2, h->nz2, h->sms, kA3Configs[h->config].ty());
     else
         h->args.chunk = chunk > A3_CHMAX ? A3_CHMAX : (chunk > (int)h->nx2 ? (int)h->nx2 : chunk);
+    h->graph_epoch++;
     return SM_OK;
 }
 

@@ -23,8 +23,12 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <map>
 #include <memory>
+#include <mutex>
 #include <new>
+#include <set>
+#include <tuple>
 #include <vector>
 
 #include "sm_common.cuh"
@@ -62,6 +66,8 @@ struct EisoArgs {
     void *fzo[5];
     int chunk;           // rows (x) each warp marches through
     int *err;            // set by a bounded wait that gave up
+    long long *step;     // steps begun; the step kernel counts, source and
+                         // receiver kernels of step it read it + 1
     const void *mat[5];
     const void *prof;
     float sc[5], isc[5];
@@ -202,6 +208,7 @@ __global__ void __launch_bounds__(32 * W, MINB) eiso_band_kernel(const EisoArgs 
     extern __shared__ __align__(128) unsigned char smem[];
     const unsigned full = 0xffffffffu;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    if ((blockIdx.x | blockIdx.y | blockIdx.z | threadIdx.x) == 0) ++*a.step;
     unsigned char *ring = smem + (size_t)warp * L::warp_bytes(D);
     uint64_t *bars = reinterpret_cast<uint64_t *>(ring + (size_t)D * L::stage);
     const int Z0 = (blockIdx.x * W + warp) * 30;
@@ -452,6 +459,7 @@ __global__ void __launch_bounds__(NT, MINB) eiso_tile_kernel(const EisoArgs a,
     C *vzs = vxs + L::NVP;
     uint64_t *bar = reinterpret_cast<uint64_t *>(smem + L::oBar);
     const int tid = threadIdx.x;
+    if ((blockIdx.x | blockIdx.y | blockIdx.z | tid) == 0) ++*a.step;
     const int Z0 = blockIdx.x * TZ, X0 = blockIdx.y * TX, shot = blockIdx.z;
     const long long fb = (long long)shot * a.fstride;
     const long long sb = (long long)shot * a.sstride;
@@ -627,7 +635,8 @@ struct SrcEntry {
 
 template <typename S>
 __global__ void eiso_source_kernel(EisoArgs a, const SrcEntry *src, const int *shot_first,
-                                   const double *vals, int nshots, long long it) {
+                                   const double *vals, int nshots) {
+    const long long it = *a.step - 1;
     using St = Store<S>;
     using C = typename Store<S>::C;
     const int shot = blockIdx.x * blockDim.x + threadIdx.x;
@@ -662,10 +671,11 @@ struct RecEntry {
 
 template <typename S>
 __global__ void eiso_gather_kernel(EisoArgs a, const RecEntry *rec, int nrec,
-                                   const int32_t *table, long long nsteps_max, long long it,
+                                   const int32_t *table, long long nsteps_max,
                                    double *traces) {
     using St = Store<S>;
     const int r = blockIdx.x * blockDim.x + threadIdx.x;
+    const long long it = *a.step - 1;
     if (r >= nrec || it >= nsteps_max) return;
     const RecEntry e = rec[r];
     const int32_t slot = table[(long long)e.group * nsteps_max + it];
@@ -712,6 +722,21 @@ struct sm_eiso {
     int maps_key = -1;           // (TX, TZ) the maps were built for
     EisoBandMaps band_maps[2];   // TMA maps of each buffer set (band kernel)
     bool band_maps_ok = false;
+    DevBuf d_step;               // device step counter (EisoArgs::step)
+    // CUDA graphs of graph_steps steps, one per parity of the starting
+    // buffer set; captured again when graph_epoch moved since (new sources,
+    // receivers, launch configuration or 16-bit scales)
+    int graph_steps = 0;
+    unsigned graph_epoch = 1;
+    struct Graph {
+        cudaGraphExec_t exec = nullptr;
+        unsigned epoch = 0;
+        int steps = 0;
+    } graphs[2];
+    ~sm_eiso() {
+        for (Graph &g : graphs)
+            if (g.exec) cudaGraphExecDestroy(g.exec);
+    }
     int sms = 148;
     // sources
     std::vector<std::vector<SrcEntry>> shot_src;     // per shot (voff local)
@@ -806,16 +831,36 @@ int eiso_make_band_maps(sm_eiso *h) {
     return SM_OK;
 }
 
+// dynamic shared memory above 48 KB must be allowed per kernel and device
+template <typename K>
+int allow_smem(K kernel, size_t bytes, int device) {
+    static std::mutex mu;
+    static std::set<std::pair<const void *, int>> done;   // (kernel, device)
+    const std::pair<const void *, int> key(reinterpret_cast<const void *>(kernel), device);
+    std::lock_guard<std::mutex> lk(mu);
+    if (!done.count(key)) {
+        SM_CUDA_TRY(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)bytes));
+        done.insert(key);
+    }
+    return SM_OK;
+}
+
+template <typename S, int TX, int TZ, int NT, int MINB>
+int ready_tile_cfg(sm_eiso *h) {
+    if (int rc = eiso_make_tile_maps<S, TX, TZ>(h)) return rc;
+    return allow_smem(eiso_tile_kernel<S, TX, TZ, NT, MINB>, ETile<S, TX, TZ>::bytes, h->device);
+}
+
+template <typename S, int W, int D, int MINB>
+int ready_band_cfg(sm_eiso *h) {
+    if (int rc = eiso_make_band_maps<S>(h)) return rc;
+    return allow_smem(eiso_band_kernel<S, W, D, MINB>, W * EBand<S>::warp_bytes(D), h->device);
+}
+
 template <typename S, int TX, int TZ, int NT, int MINB>
 int launch_tile_cfg(sm_eiso *h) {
     using L = ETile<S, TX, TZ>;
-    if (int rc = eiso_make_tile_maps<S, TX, TZ>(h)) return rc;
-    static bool attr = false;   // per instantiation
-    if (!attr) {
-        SM_CUDA_TRY(cudaFuncSetAttribute(eiso_tile_kernel<S, TX, TZ, NT, MINB>,
-                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L::bytes));
-        attr = true;
-    }
     dim3 grd((h->NZ + TZ - 1) / TZ, (h->NX + TX - 1) / TX, (unsigned)h->nshots);
     eiso_tile_kernel<S, TX, TZ, NT, MINB><<<grd, NT, L::bytes, h->stream>>>(h->args,
                                                                            h->maps[h->cur]);
@@ -825,14 +870,7 @@ int launch_tile_cfg(sm_eiso *h) {
 template <typename S, int W, int D, int MINB>
 int launch_band_cfg(sm_eiso *h) {
     using L = EBand<S>;
-    if (int rc = eiso_make_band_maps<S>(h)) return rc;
     const size_t bytes = W * L::warp_bytes(D);
-    static bool attr = false;   // per instantiation
-    if (!attr) {
-        SM_CUDA_TRY(cudaFuncSetAttribute(eiso_band_kernel<S, W, D, MINB>,
-                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
-        attr = true;
-    }
     const int wz = (h->NZ + 29) / 30;
     dim3 grd((wz + W - 1) / W, (h->NX + h->args.chunk - 1) / h->args.chunk, (unsigned)h->nshots);
     eiso_band_kernel<S, W, D, MINB><<<grd, 32 * W, bytes, h->stream>>>(h->args,
@@ -873,6 +911,22 @@ int eiso_pick_chunk(const sm_eiso *h) {
     return (int)std::min<long long>(std::max<long long>(c, 8), 512);
 }
 
+// TMA maps and shared-memory limits of the current configuration (kept out
+// of stream capture)
+template <typename S>
+int eiso_ready(sm_eiso *h) {
+    switch (h->config) {
+    case 0: return ready_band_cfg<S, 4, 4, 8>(h);
+    case 1: return ready_band_cfg<S, 4, 8, 4>(h);
+    case 2: return ready_band_cfg<S, 2, 8, 8>(h);
+    case 3: return ready_band_cfg<S, 8, 4, 3>(h);
+    case 4: return ready_band_cfg<S, 2, 4, 16>(h);
+    case 5: return ready_tile_cfg<S, 8, 32, 128, 6>(h);
+    case 6: return ready_tile_cfg<S, 16, 64, 256, 2>(h);
+    default: return ready_tile_cfg<S, 8, 64, 256, 3>(h);
+    }
+}
+
 template <typename S>
 int launch_step(sm_eiso *h) {
     h->args.chunk = eiso_pick_chunk(h);
@@ -902,8 +956,7 @@ void launch_src(sm_eiso *h) {
     int n = (int)h->nshots;
     h->timer.launches += 1;
     eiso_source_kernel<S><<<(n + 127) / 128, 128, 0, h->stream>>>(
-        h->args, h->d_src.as<SrcEntry>(), h->d_src_first.as<int>(), h->d_vals.as<double>(), n,
-        (long long)h->it);
+        h->args, h->d_src.as<SrcEntry>(), h->d_src_first.as<int>(), h->d_vals.as<double>(), n);
 }
 
 template <typename S>
@@ -913,7 +966,7 @@ void launch_gather(sm_eiso *h) {
     h->timer.launches += 1;
     eiso_gather_kernel<S><<<(n + 127) / 128, 128, 0, h->stream>>>(
         h->args, h->d_rec.as<RecEntry>(), n, h->d_table.as<int32_t>(), h->table_steps,
-        (long long)h->it, h->d_traces.as<double>());
+        h->d_traces.as<double>());
 }
 
 bool eiso_is16(const sm_eiso *h) { return h->precision == SM_FP16 || h->precision == SM_BF16; }
@@ -936,14 +989,17 @@ int eiso_rescale(sm_eiso *h) {
         ptrs[3 * f + 1] = h->xpart[h->cur][f].p; ns[3 * f + 1] = h->npml_cells * h->nshots; groups[3 * f + 1] = f;
         ptrs[3 * f + 2] = h->zpart[h->cur][f].p; ns[3 * f + 2] = h->npml_cells * h->nshots; groups[3 * f + 2] = f;
     }
+    const std::vector<int> before = h->scaler.expo;
     int rc = h->precision == SM_FP16
                  ? h->scaler.check<__half>(h->stream, 15, ptrs, ns, groups, names)
                  : h->scaler.check<__nv_bfloat16>(h->stream, 15, ptrs, ns, groups, names);
     eiso_apply_scales(h);
+    if (h->scaler.expo != before) h->graph_epoch++;   // scales are baked into graphs
     return rc;
 }
 
 int upload_sources(sm_eiso *h) {
+    h->graph_epoch++;
     std::vector<SrcEntry> all;
     std::vector<int> first(h->nshots + 1, 0);
     std::vector<double> vals;
@@ -979,6 +1035,7 @@ int upload_sources(sm_eiso *h) {
 }
 
 int upload_receivers(sm_eiso *h) {
+    h->graph_epoch++;
     // flatten every shot's receivers; each shot's sampling groups get a
     // distinct group id range in one combined table with a common step count
     long long steps = 0;
@@ -1134,6 +1191,8 @@ extern "C" int sm_eiso_create(int device, size_t nx, size_t nz, size_t npml, dou
     if ((rc = h->prof.alloc((size_t)P.size() * cplx))) return rc;
     if ((rc = h->err.alloc(sizeof(int)))) return rc;
     if ((rc = h->err.zero(h->stream))) return rc;
+    if ((rc = h->d_step.alloc(sizeof(long long)))) return rc;
+    if ((rc = h->d_step.zero(h->stream))) return rc;
 
     // ---- materials on the padded grid: edge replicated, scaled by dt/h ----
     // pml.c reads the interior's edge values in the frame; for lambda and
@@ -1202,6 +1261,7 @@ extern "C" int sm_eiso_create(int device, size_t nx, size_t nz, size_t npml, dou
     }
     a.prof = h->prof.p;
     a.err = h->err.as<int>();
+    a.step = h->d_step.as<long long>();
     if (precision == SM_FP16 || precision == SM_BF16) {
         if ((rc = h->scaler.init(5, 15))) return rc;
         h->expo0.assign(5, 0);
@@ -1238,9 +1298,11 @@ extern "C" int sm_eiso_reset(sm_eiso_t h) {
     eiso_bind(h);
     if (int rc = h->d_traces.zero(h->stream)) return rc;
     if (int rc = h->err.zero(h->stream)) return rc;
+    if (int rc = h->d_step.zero(h->stream)) return rc;
     SM_CUDA_TRY(cudaStreamSynchronize(h->stream));
     h->it = 0;
     if (eiso_is16(h)) {
+        if (h->scaler.expo != h->expo0) h->graph_epoch++;
         h->scaler.expo = h->expo0;
         eiso_apply_scales(h);
     }
@@ -1338,6 +1400,82 @@ extern "C" int sm_eiso_set_receivers(sm_eiso_t h, size_t shot, size_t nrec, cons
     return SM_OK;
 }
 
+namespace {
+
+// one time step: update, sources, receivers
+template <typename S>
+int eiso_step_once(sm_eiso *h) {
+    if (int rc = launch_step<S>(h)) return rc;
+    launch_src<S>(h);
+    launch_gather<S>(h);
+    return SM_OK;
+}
+
+// the graph of h->graph_steps steps starting from buffer set h->cur
+template <typename S>
+int eiso_graph(sm_eiso *h, cudaGraphExec_t *out) {
+    sm_eiso::Graph &gr = h->graphs[h->cur];
+    if (gr.exec && gr.epoch == h->graph_epoch && gr.steps == h->graph_steps) {
+        *out = gr.exec;
+        return SM_OK;
+    }
+    if (gr.exec) {
+        cudaGraphExecDestroy(gr.exec);
+        gr.exec = nullptr;
+    }
+    const size_t launches = h->timer.launches;
+    const int cur = h->cur;
+    SM_CUDA_TRY(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
+    int rc = SM_OK;
+    for (int k = 0; k < h->graph_steps && rc == SM_OK; ++k) rc = eiso_step_once<S>(h);
+    cudaGraph_t graph = nullptr;
+    cudaError_t e = cudaStreamEndCapture(h->stream, &graph);
+    h->timer.launches = launches;
+    h->cur = cur;   // an even number of steps: back to the starting set
+    eiso_bind(h);
+    if (rc) {
+        if (graph) cudaGraphDestroy(graph);
+        return rc;
+    }
+    if (e != cudaSuccess) return sm_fail(SM_ECUDA, "stream capture: %s", cudaGetErrorString(e));
+    e = cudaGraphInstantiate(&gr.exec, graph, 0);
+    cudaGraphDestroy(graph);
+    if (e != cudaSuccess) {
+        gr.exec = nullptr;
+        return sm_fail(SM_ECUDA, "cudaGraphInstantiate: %s", cudaGetErrorString(e));
+    }
+    gr.epoch = h->graph_epoch;
+    gr.steps = h->graph_steps;
+    *out = gr.exec;
+    return SM_OK;
+}
+
+template <typename S>
+int eiso_run_t(sm_eiso *h, size_t nsteps) {
+    if (int rc = eiso_ready<S>(h)) return rc;
+    const size_t G = (size_t)h->graph_steps;
+    const size_t per_step = 1 + (h->d_src.bytes ? 1 : 0) + (h->n_rec_total ? 1 : 0);
+    while (nsteps > 0) {
+        if (G && !h->timer.on && h->it % G == 0 && nsteps >= G) {
+            cudaGraphExec_t ex = nullptr;
+            if (int rc = eiso_graph<S>(h, &ex)) return rc;
+            SM_CUDA_TRY(cudaGraphLaunch(ex, h->stream));
+            h->timer.launches += per_step * G;
+            h->it += G;
+            nsteps -= G;
+        } else {
+            if (int rc = eiso_step_once<S>(h)) return rc;
+            h->it++;
+            nsteps--;
+        }
+        if (eiso_is16(h) && h->it % sm_eiso::kScalePeriod == 0)
+            if (int rc = eiso_rescale(h)) return rc;
+    }
+    return SM_OK;
+}
+
+}  // namespace
+
 extern "C" int sm_eiso_run(sm_eiso_t h, size_t nsteps) {
     if (int rc = eiso_check(h)) return rc;
     DeviceGuard g(h->device);
@@ -1345,31 +1483,113 @@ extern "C" int sm_eiso_run(sm_eiso_t h, size_t nsteps) {
         if (int rc = upload_sources(h)) return rc;
     if (h->rec_dirty)
         if (int rc = upload_receivers(h)) return rc;
-    for (size_t k = 0; k < nsteps; ++k) {
-        int rc = SM_OK;
-        switch (h->precision) {
-        case SM_FP64:
-            if (!(rc = launch_step<double>(h))) { launch_src<double>(h); launch_gather<double>(h); }
-            break;
-        case SM_FP16:
-            if (!(rc = launch_step<__half>(h))) { launch_src<__half>(h); launch_gather<__half>(h); }
-            break;
-        case SM_BF16:
-            if (!(rc = launch_step<__nv_bfloat16>(h))) {
-                launch_src<__nv_bfloat16>(h);
-                launch_gather<__nv_bfloat16>(h);
-            }
-            break;
-        default:
-            if (!(rc = launch_step<float>(h))) { launch_src<float>(h); launch_gather<float>(h); }
-            break;
-        }
-        if (rc) return rc;
-        h->it++;
-        if (eiso_is16(h) && h->it % sm_eiso::kScalePeriod == 0)
-            if (int rc = eiso_rescale(h)) return rc;
+    int rc;
+    switch (h->precision) {
+    case SM_FP64: rc = eiso_run_t<double>(h, nsteps); break;
+    case SM_FP16: rc = eiso_run_t<__half>(h, nsteps); break;
+    case SM_BF16: rc = eiso_run_t<__nv_bfloat16>(h, nsteps); break;
+    default: rc = eiso_run_t<float>(h, nsteps); break;
     }
+    if (rc) return rc;
     SM_CUDA_TRY(cudaGetLastError());
+    return SM_OK;
+}
+
+// Launch-configuration search: every configuration that fits the device
+// (and, for the band kernel, a few march lengths) runs trial_steps steps from
+// a zero state, timed with CUDA events; the fastest is kept.  Results are
+// cached per (precision, grid, shots) for the life of the process.
+extern "C" int sm_eiso_autotune(sm_eiso_t h, int trial_steps, int *config, int *chunk,
+                                double *ms_per_step) {
+    if (int rc = eiso_check(h)) return rc;
+    if (h->it != 0)
+        return sm_fail(SM_ESTATE, "sm_eiso_autotune: call before the first step (or after reset)");
+    if (trial_steps <= 0) trial_steps = 20;
+    DeviceGuard g(h->device);
+    struct Key {
+        int prec, NX, NZ, np;
+        size_t shots;
+        int dev;
+        bool operator<(const Key &o) const {
+            return std::tie(prec, NX, NZ, np, shots, dev) <
+                   std::tie(o.prec, o.NX, o.NZ, o.np, o.shots, o.dev);
+        }
+    };
+    struct Val {
+        int config, chunk;
+        double ms;
+    };
+    static std::map<Key, Val> cache;
+    static std::mutex mu;
+    const Key key{h->precision, h->NX, h->NZ, (int)h->np, h->nshots, h->device};
+    {
+        std::lock_guard<std::mutex> lk(mu);
+        auto it = cache.find(key);
+        if (it != cache.end()) {
+            h->config = it->second.config;
+            h->chunk = it->second.chunk;
+            h->graph_epoch++;
+            if (config) *config = h->config;
+            if (chunk) *chunk = h->chunk;
+            if (ms_per_step) *ms_per_step = it->second.ms;
+            return SM_OK;
+        }
+    }
+    int lim = 0;
+    SM_CUDA_TRY(cudaDeviceGetAttribute(&lim, cudaDevAttrMaxSharedMemoryPerBlockOptin, h->device));
+    cudaEvent_t e0, e1;
+    SM_CUDA_TRY(cudaEventCreate(&e0));
+    SM_CUDA_TRY(cudaEventCreate(&e1));
+    const bool timing = h->timer.on;
+    h->timer.on = false;
+    Val best{-1, 0, 0.0};
+    int rc = SM_OK;
+    for (int c = 0; c < kEisoNumConfigs && rc == SM_OK; ++c) {
+        if (eiso_config_smem_prec(h->precision, c) > (size_t)lim) continue;
+        std::vector<int> chunks{0};
+        if (kEisoConfigs[c].kind == 1) chunks = {0, 16, 32, 64};
+        for (int ch : chunks) {
+            h->config = c;
+            h->chunk = ch;
+            h->graph_epoch++;
+            if ((rc = sm_eiso_reset(h))) break;
+            if ((rc = sm_eiso_run(h, 2))) break;
+            cudaEventRecord(e0, h->stream);
+            if ((rc = sm_eiso_run(h, (size_t)trial_steps))) break;
+            cudaEventRecord(e1, h->stream);
+            if ((rc = sm_eiso_sync(h))) break;
+            float t = 0.f;
+            cudaEventElapsedTime(&t, e0, e1);
+            const double ms = t / trial_steps;
+            if (best.config < 0 || ms < best.ms) best = Val{c, ch, ms};
+        }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    h->timer.on = timing;
+    if (rc) return rc;
+    if (best.config < 0) return sm_fail(SM_EINVAL, "sm_eiso_autotune: no configuration fits");
+    h->config = best.config;
+    h->chunk = best.chunk;
+    h->graph_epoch++;
+    if ((rc = sm_eiso_reset(h))) return rc;
+    {
+        std::lock_guard<std::mutex> lk(mu);
+        cache[key] = best;
+    }
+    if (config) *config = best.config;
+    if (chunk) *chunk = best.chunk;
+    if (ms_per_step) *ms_per_step = best.ms;
+    return SM_OK;
+}
+
+extern "C" int sm_eiso_set_graph(sm_eiso_t h, int steps) {
+    if (int rc = eiso_check(h)) return rc;
+    if (steps != 0 && steps != 2 && steps != 4 && steps != 8 && steps != 16)
+        return sm_fail(SM_EINVAL, "sm_eiso_set_graph: steps must be 0, 2, 4, 8 or 16 (got %d)",
+                       steps);
+    h->graph_steps = steps;
+    h->graph_epoch++;
     return SM_OK;
 }
 
@@ -1511,6 +1731,7 @@ extern "C" int sm_eiso_set_chunk(sm_eiso_t h, int chunk) {
     if (chunk < 0 || chunk > (1 << 20))
         return sm_fail(SM_EINVAL, "sm_eiso_set_chunk: chunk %d out of range", chunk);
     h->chunk = chunk;
+    h->graph_epoch++;
     return SM_OK;
 }
 
@@ -1529,6 +1750,7 @@ extern "C" int sm_eiso_set_config(sm_eiso_t h, int config) {
                        "(device limit %d)",
                        config, need, lim);
     h->config = config;
+    h->graph_epoch++;
     return SM_OK;
 }
 
