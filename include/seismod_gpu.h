@@ -255,6 +255,117 @@ int sm_a3d_kernel_stats(sm_a3d_t h, int reset, double *update_ms, size_t *update
                         size_t *all_launches);
 
 /* ======================================================================
+ * device memory a handle needs (estimate used for admission; no reference
+ * counterpart).  nrec receivers per shot, nsteps_max samples at most.
+ * ====================================================================== */
+int sm_eiso_device_bytes(size_t nx, size_t nz, size_t npml, int precision, size_t nshots,
+                         size_t nrec, size_t nsteps_max, size_t *bytes);
+int sm_a3d_device_bytes(size_t nx2, size_t ny2, size_t nz2, size_t np, int precision,
+                        size_t nrec, size_t nsteps_max, size_t *bytes);
+
+/* ======================================================================
+ * Serving: a request loop over many shots of different grids (no reference
+ * counterpart; the reference runs one program per shot).
+ *
+ * A request carries everything sm_eiso_create / sm_a3d_create and the
+ * source and receiver set-up take, plus its step count; submit copies it, so
+ * the caller's arrays may be freed on return.  A worker thread admits queued
+ * requests in arrival order while the sum of admitted requests' device
+ * memory (sm_*_device_bytes) stays within the budget and fewer than
+ * max_active run; each admitted request gets its own handle and CUDA stream,
+ * and the worker feeds every running request slices of slice_steps steps
+ * (at most two slices queued per request), so requests that arrive while
+ * others run start as soon as memory and a slot free up, and their kernels
+ * overlap on the device.  A finished request's traces are copied to the host
+ * and its device memory released.  Results do not depend on what else runs:
+ * each request's arithmetic is that of a handle of its own.
+ * ====================================================================== */
+typedef struct {
+    size_t nx, nz, npml;
+    double h, dt;
+    const double *la, *mu, *l2m, *b, *bm;   /* nx*nz, as sm_eiso_create */
+    const double *d, *dh, *dH;              /* npml */
+    int precision;
+    size_t nsrc;                            /* as sm_eiso_set_sources */
+    const size_t *src_index;
+    const int *src_type;
+    const double *src_fct;
+    const size_t *src_length;
+    size_t src_stride;
+    double src_scale;
+    size_t nrec;                            /* as sm_eiso_set_receivers */
+    const size_t *rec_index;
+    const int *rec_comp;
+    const double *rec_t0, *rec_dt;
+    size_t nsteps;
+} sm_eiso_request;
+
+typedef struct {
+    size_t nx2, ny2, nz2, np;
+    double dx, dy, dz, dt;
+    const double *vp, *rho;                 /* padded, as sm_a3d_create */
+    const double *const *coef;              /* 18 arrays, as sm_a3d_cpml */
+    int precision;
+    size_t nsrc;                            /* as sm_a3d_set_sources */
+    const size_t *src_index;
+    const double *src_fct;
+    const size_t *src_length;
+    size_t src_stride;
+    double src_scale;
+    size_t nrec;                            /* as sm_a3d_set_receivers */
+    const size_t *rec_index;
+    const int *rec_comp;
+    const double *rec_t0, *rec_dt;
+    size_t nsteps;
+} sm_a3d_request;
+
+/* request states */
+#define SM_REQ_QUEUED  0
+#define SM_REQ_RUNNING 1
+#define SM_REQ_DONE    2
+#define SM_REQ_FAILED  3
+
+typedef struct {
+    size_t submitted, completed, failed, running, queued;
+    double latency_p50, latency_p99, latency_mean, latency_max;   /* s, submit -> traces on host */
+    double wait_p50, wait_p99;            /* s, submit -> admitted */
+    double busy_s;                        /* first submit -> last completion */
+    double shots_per_s;                   /* completed / busy_s */
+    double gcell_per_s;                   /* completed cell updates / busy_s / 1e9 */
+    size_t hbm_budget, hbm_peak;          /* bytes admitted at most at one time */
+    size_t max_running;                   /* most requests running at one time */
+} sm_server_stats;
+
+typedef struct sm_server *sm_server_t;
+
+/* hbm_budget: bytes requests may hold (0: free device memory at creation
+ * minus 2 GiB); max_active: running requests at most (0: 64); slice_steps:
+ * steps per slice (0: 64); graph_steps: CUDA-graph length for each request
+ * (0 none; else as sm_eiso_set_graph). */
+int sm_server_create(int device, size_t hbm_budget, int max_active, int slice_steps,
+                     int graph_steps, sm_server_t *out);
+/* SM_EBUSY when the request alone exceeds the budget */
+int sm_server_submit_eiso(sm_server_t s, const sm_eiso_request *r, uint64_t *ticket);
+int sm_server_submit_a3d(sm_server_t s, const sm_a3d_request *r, uint64_t *ticket);
+/* block until the request is done (SM_OK), failed (its error), or timeout_s
+ * passed (SM_ETIMEOUT; < 0 waits for good) */
+int sm_server_wait(sm_server_t s, uint64_t ticket, double timeout_s);
+/* wait for every submitted request */
+int sm_server_drain(sm_server_t s, double timeout_s);
+int sm_server_status(sm_server_t s, uint64_t ticket, int *state, double *latency_s);
+/* traces of a finished request, layout as sm_eiso_read_traces */
+int sm_server_traces(sm_server_t s, uint64_t ticket, size_t rec0, size_t nrec, double *out,
+                     size_t ld, size_t *counts);
+/* forget a finished request (its traces) */
+int sm_server_release(sm_server_t s, uint64_t ticket);
+int sm_server_get_stats(sm_server_t s, sm_server_stats *st);
+/* stops the worker after the running requests' queued slices; queued
+ * requests are dropped */
+int sm_server_destroy(sm_server_t s);
+/* sizeof the request and stats structs, for bindings that lay them out */
+int sm_server_struct_sizes(size_t *eiso_request, size_t *a3d_request, size_t *stats);
+
+/* ======================================================================
  * drop-in programs: the whole of e_iso / a_iso_3d main() on the device,
  * reading the reference's .par / model / source / output files and writing
  * its trc/<base>/<base>_<n>.trc files.  argv as the reference takes it

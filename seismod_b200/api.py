@@ -351,30 +351,43 @@ class A3DDevice:
 # whole shots from workload descriptions (seismod_b200.workloads)
 # ----------------------------------------------------------------------------
 
-def eiso_device(p, precision="fp32", shots=None, device=0):
-    """Build an EIsoDevice for problem p with sources of `shots` (default:
-    all shots of p) and p's receivers.  Returns (dev, nsteps)."""
+def eiso_inputs(p, shots=None):
+    """Everything sm_eiso_create and the source / receiver set-up take for
+    problem p (host arrays), as e_iso.c:379-557 prepares it: averaged
+    materials, PML profiles, Ricker series of each shot, node indices."""
     la, mu, l2m, b, bm, vpmax = eiso_materials(p.vp, p.vs, p.rho)
     dt = p.dt
     if dt > p.h / (math.sqrt(2.0) * vpmax):
         raise L.SeismodError(L.SM_ECFL, "time step too large (e_iso.c:476)")
     d, dh, dH = eiso_profiles(p.npml, p.h, p.vp)
     shots = list(range(len(p.shots))) if shots is None else list(shots)
-    dev = EIsoDevice(p.nx, p.nz, p.npml, p.h, dt, la, mu, l2m, b, bm, d, dh, dH, precision,
-                     len(shots), device)
-    n = nsteps(p.duration, dt)
-    for k, s in enumerate(shots):
+    src = []
+    for s in shots:
         srcs = p.shots[s]
         fct, ln = ricker([q[1] for q in srcs], [q[2] for q in srcs], dt)
         idx = [c_round((q[3] - p.x0) / p.h) * p.nz + c_round((q[4] - p.z0) / p.h) for q in srcs]
         typ = [L.SM_SRC[q[0].lower()] for q in srcs]
-        dev.set_sources(k, idx, typ, fct, ln, dt)
+        src.append((idx, typ, fct, ln))
     ridx = [c_round((x - p.x0) / p.h) * p.nz + c_round((z - p.z0) / p.h)
             for (_, x, z, _, _) in p.receivers]
     comps = [L.SM_COMP[c.lower()] for (c, _, _, _, _) in p.receivers]
     t0 = [r[3] for r in p.receivers]
     rdt = [r[4] * 1e-3 for r in p.receivers]
-    dev.set_receivers(None, ridx, comps, t0, rdt, n)
+    return dict(nx=p.nx, nz=p.nz, npml=p.npml, h=p.h, dt=dt, la=la, mu=mu, l2m=l2m, b=b, bm=bm,
+                d=d, dh=dh, dH=dH, src=src, src_scale=dt, rec=(ridx, comps, t0, rdt),
+                nsteps=nsteps(p.duration, dt))
+
+
+def eiso_device(p, precision="fp32", shots=None, device=0):
+    """Build an EIsoDevice for problem p with sources of `shots` (default:
+    all shots of p) and p's receivers.  Returns (dev, nsteps)."""
+    q = eiso_inputs(p, shots)
+    dev = EIsoDevice(q["nx"], q["nz"], q["npml"], q["h"], q["dt"], q["la"], q["mu"], q["l2m"],
+                     q["b"], q["bm"], q["d"], q["dh"], q["dH"], precision, len(q["src"]), device)
+    for k, (idx, typ, fct, ln) in enumerate(q["src"]):
+        dev.set_sources(k, idx, typ, fct, ln, q["src_scale"])
+    n = q["nsteps"]
+    dev.set_receivers(None, *q["rec"], n)
     return dev, n
 
 
@@ -396,7 +409,9 @@ def a3d_index(p, x, y, z):
     return (i * ny2 + j) * nz2 + k
 
 
-def a3d_device(p, precision="fp32", device=0):
+def a3d_inputs(p):
+    """Everything sm_a3d_create and the source / receiver set-up take for
+    problem p (host arrays), as a_iso_3d.c:317-590 prepares it."""
     nx, ny, nz = p.shape
     vpp, rhop = a3d_pad_model(p.vp, p.rho, p.npml)
     dt = p.dt
@@ -406,15 +421,22 @@ def a3d_device(p, precision="fp32", device=0):
         raise L.SeismodError(L.SM_ECFL, "time step too large (a_iso_3d.c:411-417)")
     coef = a3d_cpml(p.npml, vpp.shape, p.d, dt, 2.0, 5000.0, p.Rc, p.kappa_max, p.alpha_max,
                     p.sources[0][2])
-    dev = A3DDevice(vpp, rhop, p.npml, p.d, dt, coef, precision, device)
-    n = nsteps(p.duration, dt)
     fct, ln = ricker([q[1] for q in p.sources], [q[2] for q in p.sources], dt)
     idx = [a3d_index(p, q[3], q[4], q[5]) for q in p.sources]
-    dev.set_sources(idx, fct, ln, dt * 1e6)
     ridx = [a3d_index(p, x, y, z) for (_, x, y, z, _, _) in p.receivers]
     comps = [L.SM_COMP[c.lower()] for (c, _, _, _, _, _) in p.receivers]
-    dev.set_receivers(ridx, comps, [r[4] for r in p.receivers],
-                      [r[5] * 1e-3 for r in p.receivers], n)
+    return dict(vp=vpp, rho=rhop, npml=p.npml, d=p.d, dt=dt, coef=coef,
+                src=(idx, fct, ln), src_scale=dt * 1e6,
+                rec=(ridx, comps, [r[4] for r in p.receivers], [r[5] * 1e-3 for r in p.receivers]),
+                nsteps=nsteps(p.duration, dt))
+
+
+def a3d_device(p, precision="fp32", device=0):
+    q = a3d_inputs(p)
+    dev = A3DDevice(q["vp"], q["rho"], q["npml"], q["d"], q["dt"], q["coef"], precision, device)
+    n = q["nsteps"]
+    dev.set_sources(*q["src"], q["src_scale"])
+    dev.set_receivers(*q["rec"], n)
     return dev, n
 
 

@@ -834,6 +834,26 @@ void a3_from_double(void *p, size_t i, int prec, double v, float sc) {
 
 }  // namespace
 
+static size_t a3d_mb2(size_t b) { return (b + (2u << 20) - 1) / (2u << 20) * (2u << 20); }
+
+extern "C" int sm_a3d_device_bytes(size_t nx2, size_t ny2, size_t nz2, size_t np, int precision,
+                                   size_t nrec, size_t nsteps_max, size_t *bytes) {
+    if (!bytes) return sm_fail(SM_EINVAL, "sm_a3d_device_bytes: NULL");
+    if (precision < SM_FP32 || precision > SM_BF16)
+        return sm_fail(SM_EINVAL, "sm_a3d_device_bytes: unknown precision %d", precision);
+    const size_t pitch = round_up(nz2, 32), ncell = nx2 * ny2 * pitch;
+    const size_t e = storage_bytes(precision), c = precision == SM_FP64 ? 8 : 4;
+    const size_t slabs = 2 * (2 * np * ny2 * pitch + nx2 * 2 * np * pitch + nx2 * ny2 * 2 * np);
+    size_t b = 8 * a3d_mb2(ncell * e);                        // 4 fields, two sets
+    b += 2 * a3d_mb2(slabs * e);                              // CPML memory variables
+    b += 2 * a3d_mb2(ncell * c);                              // rho, K
+    b += a3d_mb2(18 * (nx2 + ny2 + nz2) * c);                 // coefficients
+    b += a3d_mb2(nrec * nsteps_max * (sizeof(double) + sizeof(int32_t)));
+    b += 16u << 20;
+    *bytes = b;
+    return SM_OK;
+}
+
 extern "C" int sm_a3d_create(int device, size_t nx2, size_t ny2, size_t nz2, size_t np,
                              double dx, double dy, double dz, double dt, const double *vp,
                              const double *rho, const double *const *coef, int precision,

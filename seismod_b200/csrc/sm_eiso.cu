@@ -1134,6 +1134,28 @@ size_t pml_index_host(const sm_eiso *h, size_t X, size_t Z) {
 
 }  // namespace
 
+// 2 MB rounding of each large array (the allocation granularity)
+static size_t mb2(size_t b) { return (b + (2u << 20) - 1) / (2u << 20) * (2u << 20); }
+
+extern "C" int sm_eiso_device_bytes(size_t nx, size_t nz, size_t npml, int precision,
+                                    size_t nshots, size_t nrec, size_t nsteps_max,
+                                    size_t *bytes) {
+    if (!bytes) return sm_fail(SM_EINVAL, "sm_eiso_device_bytes: NULL");
+    if (precision < SM_FP32 || precision > SM_BF16)
+        return sm_fail(SM_EINVAL, "sm_eiso_device_bytes: unknown precision %d", precision);
+    const size_t NX = nx + 2 * npml, NZ = nz + 2 * npml, pitch = round_up(NZ, 32);
+    const size_t fcells = NX * pitch, e = storage_bytes(precision);
+    const size_t c = precision == SM_FP64 ? 8 : 4;
+    const size_t pml = 4 * npml * npml + 2 * npml * (nx + nz);
+    size_t b = 2 * mb2(5 * fcells * nshots * e);              // two buffer sets
+    b += 20 * mb2(pml * nshots * e);                          // split parts, both sets
+    b += mb2(5 * fcells * c) + mb2((4 * NX + 4 * NZ) * c);    // materials, profiles
+    b += mb2(nrec * nshots * nsteps_max * (sizeof(double) + sizeof(int32_t)));   // traces, table
+    b += 16u << 20;                                           // small buffers, 16-bit scaler
+    *bytes = b;
+    return SM_OK;
+}
+
 extern "C" int sm_eiso_create(int device, size_t nx, size_t nz, size_t npml, double hh,
                               double dt, const double *la, const double *mu, const double *l2m,
                               const double *b, const double *bm, const double *d,

@@ -118,3 +118,25 @@ def test_a3d_rejects_coefficients_that_are_not_reference_defaults_inside():
 def test_c_round_is_half_away_from_zero():
     assert api.c_round(2.5) == 3 and api.c_round(-2.5) == -3 and api.c_round(1.4999) == 1
     assert math.floor(0.5 + 0.5) == api.c_round(0.5)
+
+
+def test_server_request_structs_match_the_c_layout():
+    from seismod_b200 import serving
+    e, a, s = serving.struct_sizes()
+    assert e == C.sizeof(serving.EisoRequest)
+    assert a == C.sizeof(serving.A3dRequest)
+    assert s == C.sizeof(serving.ServerStats)
+
+
+def test_device_bytes_estimates_grow_with_the_problem():
+    from seismod_b200 import serving
+    lib = serving.lib()
+    b1, b2 = C.c_size_t(), C.c_size_t()
+    assert lib.sm_eiso_device_bytes(400, 400, 20, 0, 1, 64, 1500, C.byref(b1)) == 0
+    assert lib.sm_eiso_device_bytes(400, 400, 20, 0, 64, 64, 1500, C.byref(b2)) == 0
+    # two buffer sets of five FP32 fields per shot at least
+    assert b2.value > b1.value >= 2 * 5 * 440 * 448 * 4
+    assert lib.sm_a3d_device_bytes(288, 288, 288, 16, 2, 0, 0, C.byref(b1)) == 0
+    assert lib.sm_a3d_device_bytes(288, 288, 288, 16, 0, 0, 0, C.byref(b2)) == 0
+    assert b2.value > b1.value >= 8 * 288 * 288 * 288 * 2
+    assert lib.sm_eiso_device_bytes(10, 10, 2, 9, 1, 0, 0, C.byref(b1)) == 1   # bad precision
