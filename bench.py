@@ -2,7 +2,8 @@
 """Benchmark of the seismod FDTD hot path on B200.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--workload a3d|a3d512|eiso|eiso1] [--precision fp32|fp16|bf16|fp64]
+                    [--workload a3d|a3d512|eiso|eiso1|serve]
+                    [--precision fp32|fp16|bf16|fp64]
 
 A "step" is one FDTD time step of the whole workload (velocity + pressure /
 stress update, CPML/PML memory variables, source injection, receiver
@@ -18,6 +19,13 @@ ranks; value = all ranks' cell-updates / that time.
 --impl reference times the reference's own CPU program (oracle/_ref, built
 from its sources) on the host cores for a bounded number of steps of the
 same workload.
+
+Every device handle is autotuned (launch configuration) and replays its time
+loop as CUDA graphs of 16 steps unless --no-tune / --no-graph.  --workload
+eiso adds the batching comparison (plain single-shot FP32 against 64 batched
+shots in FP32, FP16 and BF16, trace errors against FP64); --workload serve
+runs the mixed Poisson request stream through the request loop and reports
+p50/p99 latency beside shots/s and Gcell/s.
 """
 from __future__ import annotations
 
@@ -137,6 +145,10 @@ def make_workload(name, size=None):
                 "e_iso 1000x500 (+2x20 PML), 64 shots batched, 2000-step shots")
     if name == "eiso1":
         return "eiso", W.cfg0(), "e_iso 400x400 (+2x20 PML), single shot, 1500-step shot"
+    if name == "serve":
+        return ("serve", W.cfg4(),
+                "request stream: 64 Poisson arrivals at 4/s, 70% e_iso 200^2..2000^2, "
+                "30% a_iso_3d 128^3..384^3, 500..3000 steps, seeded layered models")
     raise SystemExit(f"unknown workload {name}")
 
 
@@ -150,11 +162,21 @@ def trace_err(a, b):
     return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))
 
 
-def device_for(kind, p, precision, dev_id):
+TUNE = True
+GRAPH = 16
+
+
+def device_for(kind, p, precision, dev_id, shots=None):
     from seismod_b200 import api
     if kind == "a3d":
-        return api.a3d_device(p, precision, dev_id)
-    return api.eiso_device(p, precision, None, dev_id)
+        dev, n = api.a3d_device(p, precision, dev_id)
+    else:
+        dev, n = api.eiso_device(p, precision, shots, dev_id)
+    if TUNE:
+        dev.autotune()
+    if GRAPH:
+        dev.set_graph(GRAPH)
+    return dev, n
 
 
 def time_steps(dev, K, torch):
@@ -251,6 +273,85 @@ def precision_side(kind, p, local_rank, K):
     return res
 
 
+def batching_side(p, local_rank, K, batched_ms):
+    """Shots/s of the plain single-shot FP32 form (one shot per handle) against
+    the batched forms, and each form's trace error against an FP64 run of the
+    same shot."""
+    from seismod_b200 import api
+    import torch
+    nsh = len(p.shots)
+    n = api.nsteps(p.duration, p.dt)
+    ref64 = api.run_eiso(p, "fp64", [0], local_rank)[0]
+    out = {}
+    dev, _ = device_for("eiso", p, "fp32", local_rank, shots=[0])
+    dev.run(10)
+    k1 = min(K, 400)
+    ms1 = time_steps(dev, k1, torch) / k1
+    dev.close()
+    tr = api.run_eiso(p, "fp32", [0], local_rank)[0]
+    out["single_shot_fp32"] = {"ms_per_step": round(ms1, 5),
+                               "shots_per_s": round(1.0 / (ms1 * 1e-3 * n), 3),
+                               "trace_err_vs_fp64": trace_err(tr, ref64)}
+    for prec in ("fp32", "fp16", "bf16"):
+        if prec == "fp32" and batched_ms is not None:
+            ms = batched_ms
+        else:
+            dev, _ = device_for("eiso", p, prec, local_rank)
+            dev.run(10)
+            kb = min(K, 200)
+            ms = time_steps(dev, kb, torch) / kb
+            dev.close()
+        tr = api.run_eiso(p, prec, [0], local_rank)[0]
+        sps = nsh / (ms * 1e-3 * n)
+        out[f"batched_{prec}"] = {"ms_per_step": round(ms, 5), "shots_per_s": round(sps, 3),
+                                  "speedup_vs_single_fp32": round(sps * ms1 * 1e-3 * n, 3),
+                                  "trace_err_vs_fp64": trace_err(tr, ref64)}
+    return out
+
+
+def run_serve(args, local_rank):
+    """The mixed request stream through the request loop: each request is
+    built on the host and submitted at its arrival time; value = cell updates
+    of completed requests / (first submit -> last completion)."""
+    from seismod_b200 import serving
+    _, reqs, desc = make_workload("serve")
+    srv = serving.Server(device=local_rank, max_active=16, slice_steps=64,
+                         graph_steps=GRAPH or 0)
+    t0 = time.perf_counter()
+    lag = []
+    with Clocks(local_rank) as clk:
+        for r in reqs:
+            now = time.perf_counter() - t0
+            if r.arrival > now:
+                time.sleep(r.arrival - now)
+            lag.append(max(0.0, time.perf_counter() - t0 - r.arrival))
+            srv.submit(r.kind, r.problem, args.precision)
+        srv.drain()
+    st = srv.stats()
+    srv.close()
+    out = {
+        "metric": METRIC, "value": round(st["gcell_per_s"], 3), "unit": "Gcell/s",
+        "n_gpus": 1, "steps": len(reqs), "warmup": 0,
+        "ms_per_step": None, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64" if args.precision == "fp64" else "f32",
+        "data": "synthetic (seeded request stream of the named configuration)",
+        "config": {"workload": desc, "precision": f"{args.precision} storage",
+                   "server": "max_active 16, slices of 64 steps, CUDA graphs of %d steps"
+                             % (GRAPH or 0)},
+        "serving": {"shots_per_s": round(st["shots_per_s"], 4),
+                    "latency_p50_s": round(st["latency_p50"], 4),
+                    "latency_p99_s": round(st["latency_p99"], 4),
+                    "wait_p50_s": round(st["wait_p50"], 4), "wait_p99_s": round(st["wait_p99"], 4),
+                    "completed": st["completed"], "failed": st["failed"],
+                    "busy_s": round(st["busy_s"], 3), "max_running": st["max_running"],
+                    "hbm_peak_gb": round(st["hbm_peak"] / 1e9, 2),
+                    "hbm_budget_gb": round(st["hbm_budget"] / 1e9, 2),
+                    "submit_lag_p99_s": round(float(np.percentile(lag, 99)), 3)},
+        "clocks": clk.summary(),
+    }
+    return out
+
+
 def e2e(kind, p, K, local_rank):
     """Whole user call through the public API from host arrays: set-up and
     upload, K steps, traces back to the host, teardown."""
@@ -329,6 +430,11 @@ def run_reference_arm(args, rank, world):
     if rank != 0:
         return None
     kind, p, desc = make_workload(args.workload)
+    if kind == "serve":
+        # the reference serves nothing: one program per shot; its rate on the
+        # stream's first e_iso request stands for the stream
+        p = next(r.problem for r in p if r.kind == "eiso")
+        kind = "eiso"
     steps = max(1, min(args.steps, 12 if kind == "a3d" else 200))
     rate, sample = reference_rate(kind, p, steps)
     if rate is None:
@@ -352,13 +458,19 @@ def main():
     ap.add_argument("--steps", type=int, default=1000)
     ap.add_argument("--warmup", type=int, default=20)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="a3d", choices=["a3d", "a3d512", "eiso", "eiso1"])
+    ap.add_argument("--workload", default="a3d",
+                    choices=["a3d", "a3d512", "eiso", "eiso1", "serve"])
     ap.add_argument("--precision", default="fp32", choices=["fp32", "fp64", "fp16", "bf16"])
     ap.add_argument("--no-side", action="store_true", help="skip precision / CPU side runs")
+    ap.add_argument("--no-tune", action="store_true", help="default launch configuration")
+    ap.add_argument("--no-graph", action="store_true", help="launch every kernel from the host")
     ap.add_argument("--size", type=int, default=None,
                     help="a3d only: interior edge length instead of 256 (profiling captures)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
+    global TUNE, GRAPH
+    TUNE = not args.no_tune
+    GRAPH = 0 if args.no_graph else 16
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -377,7 +489,16 @@ def main():
         import torch.distributed as dist
         torch.cuda.set_device(local_rank)
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    if args.workload == "serve":
+        if rank == 0:
+            print(json.dumps(run_serve(args, local_rank)), flush=True)
+        if world > 1:
+            dist.barrier()
+            dist.destroy_process_group()
+        return 0
     out, kind, p, desc, cells = run_ours(args, rank, world, local_rank, torch, dist)
+    if rank == 0 and not args.no_side and kind == "eiso" and len(p.shots) > 1:
+        out["batching"] = batching_side(p, local_rank, args.steps, out["ms_per_step"])
     if rank == 0 and not args.no_side:
         out["precisions"] = precision_side(kind, p, local_rank, args.steps)
         out["e2e"] = e2e(kind, p, args.steps, local_rank)
