@@ -365,6 +365,29 @@ int sm_server_destroy(sm_server_t s);
 /* sizeof the request and stats structs, for bindings that lay them out */
 int sm_server_struct_sizes(size_t *eiso_request, size_t *a3d_request, size_t *stats);
 
+/* One e_iso shot that allocates no device memory (no counterpart in the
+ * reference).  For callers that cannot call cudaMalloc: programs whose device
+ * memory is all handed out by their own allocator, or code running where a
+ * device allocation is not allowed or would stall the device.  The whole run
+ * (state, materials, tables, traces) lives in one fixed array of 24 MiB
+ * inside this library, which every GPU that loads the library holds until
+ * the process exits; a shot that needs more is rejected with SM_EINVAL and a
+ * message giving the bytes it needs (a 400 x 400 grid with 20 PML cells, 64
+ * receivers and 1500 steps fits).  FP32 storage only; results equal
+ * sm_eiso_create / sm_eiso_run / sm_eiso_read_traces on the same request.
+ *   r:       the shot, as for sm_server_submit_eiso (nshots = 1)
+ *   stream:  cudaStream_t to run on (NULL: the legacy default stream); the
+ *            call returns when the run is done and the traces are copied
+ *   traces:  nrec rows of ld doubles (may be NULL to learn the counts),
+ *            counts: samples per receiver (required when nrec > 0)
+ * The first call on a device looks up the array's device address (once per
+ * device); make that first call before any stream capture.  Every call uses
+ * the same array and clears what must start at zero, so calls on one device
+ * that overlap on the GPU (other threads, other streams) race: run them one
+ * at a time per device. */
+int sm_eiso_run_noalloc(int device, void *stream, const sm_eiso_request *r, double *traces,
+                        size_t ld, size_t *counts);
+
 /* ======================================================================
  * drop-in programs: the whole of e_iso / a_iso_3d main() on the device,
  * reading the reference's .par / model / source / output files and writing

@@ -1802,3 +1802,291 @@ extern "C" int sm_eiso_kernel_stats(sm_eiso_t h, int reset, double *update_ms,
     DeviceGuard g(h->device);
     return h->timer.stats(reset, update_ms, update_launches, all_launches);
 }
+
+// ===========================================================================
+// Allocation-free single-shot run (no counterpart in the reference).
+//
+// Some callers of this library cannot call cudaMalloc: a host program whose
+// device memory is all owned by its own allocator (a solver or a serving
+// framework that hands out every byte itself), or code that runs where a
+// device allocation is not allowed or would stall other work (allocation
+// synchronises the device).  sm_eiso_run_noalloc gives them one e_iso shot
+// without any device allocation: every device-side array of the run (two
+// buffer sets of wavefields, split parts, materials, damping tables, source
+// and receiver tables, traces, the step counter and the wait flag) lives in
+// the file-scope array below, of fixed size, which every GPU that loads this
+// library holds until the process exits.  The kernels are the tiled step
+// kernel and the source / receiver kernels of the handle path, unchanged.
+// ===========================================================================
+namespace {
+
+constexpr size_t kNoallocBytes = (size_t)24 << 20;   // 24 MiB per device
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoallocBytes];
+
+// device address of g_noalloc_scratch on each device, looked up once per
+// device with that device current (the host-side name is only a stand-in)
+std::mutex g_noalloc_mu;
+void *g_noalloc_ptr[64] = {};
+
+int noalloc_scratch(int device, unsigned char **out) {
+    if (device < 0 || device >= 64) return sm_fail(SM_EINVAL, "sm_eiso_run_noalloc: device %d", device);
+    std::lock_guard<std::mutex> lk(g_noalloc_mu);
+    if (!g_noalloc_ptr[device]) {
+        void *p = nullptr;
+        cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+        if (e != cudaSuccess || !p)
+            return sm_fail(SM_ECUDA, "sm_eiso_run_noalloc: cudaGetSymbolAddress: %s",
+                           cudaGetErrorString(e));
+        g_noalloc_ptr[device] = p;
+    }
+    *out = static_cast<unsigned char *>(g_noalloc_ptr[device]);
+    return SM_OK;
+}
+
+// bump allocator over the scratch array (offsets only; nothing is allocated)
+struct NoallocLayout {
+    size_t off = 0;
+    size_t take(size_t bytes) {
+        const size_t o = off;
+        off = round_up(off + bytes, 256);
+        return o;
+    }
+};
+
+}  // namespace
+
+extern "C" int sm_eiso_run_noalloc(int device, void *stream, const sm_eiso_request *r,
+                                   double *traces, size_t ld, size_t *counts) {
+    using S = float;
+    using L = ETile<S, 8, 32>;
+    if (!r) return sm_fail(SM_EINVAL, "sm_eiso_run_noalloc: request is NULL");
+    const sm_eiso_request &q = *r;
+    if (q.precision != SM_FP32)
+        return sm_fail(SM_EINVAL, "sm_eiso_run_noalloc: FP32 storage only (precision %d)",
+                       q.precision);
+    if (q.nx < 2 || q.nz < 2 || q.npml < 1)
+        return sm_fail(SM_EINVAL, "sm_eiso_run_noalloc: nx, nz >= 2 and npml >= 1 required");
+    if (!(q.h > 0.0) || !(q.dt > 0.0)) return sm_fail(SM_EINVAL, "sm_eiso_run_noalloc: h, dt > 0");
+    if (!q.la || !q.mu || !q.l2m || !q.b || !q.bm || !q.d || !q.dh || !q.dH ||
+        (q.nsrc && (!q.src_index || !q.src_type || !q.src_fct || !q.src_length)) ||
+        (q.nrec && (!q.rec_index || !q.rec_comp || !q.rec_t0 || !q.rec_dt)))
+        return sm_fail(SM_EINVAL, "sm_eiso_run_noalloc: NULL array in the request");
+    if (q.nrec && !counts) return sm_fail(SM_EINVAL, "sm_eiso_run_noalloc: counts is NULL");
+    const size_t nx = q.nx, nz = q.nz, np = q.npml;
+    const size_t NX = nx + 2 * np, NZ = nz + 2 * np, pitch = round_up(NZ, 32);
+    if (NX > (1u << 20) || NZ > (1u << 20)) return sm_fail(SM_EINVAL, "sm_eiso_run_noalloc: grid too large");
+    const size_t fcells = NX * pitch;
+    const size_t pml = 4 * np * np + 2 * np * (nx + nz);
+    const EisoProf P{(int)NX, (int)NZ};
+
+    // ---- host-side tables (sources, receiver sampling), as the handle path ----
+    std::vector<SrcEntry> src;
+    std::vector<double> vals;
+    for (size_t s = 0; s < q.nsrc; ++s) {
+        const int t = q.src_type[s];
+        if (q.src_index[s] >= nx * nz)
+            return sm_fail(SM_EINVAL, "sm_eiso_run_noalloc: source %zu outside the grid", s);
+        if (t != SM_SRC_SX && t != SM_SRC_SZ && t != SM_SRC_SXZ && t != SM_SRC_BULK)
+            return sm_fail(SM_EINVAL, "sm_eiso_run_noalloc: source type %d not supported", t);
+        if (q.src_length[s] > q.src_stride)
+            return sm_fail(SM_EINVAL, "sm_eiso_run_noalloc: source length exceeds stride");
+        SrcEntry e{};
+        e.q = (long long)(q.src_index[s] / nz + np) * (long long)pitch +
+              (long long)(q.src_index[s] % nz + np);
+        e.shot = 0;
+        e.type = t;
+        e.voff = (long long)vals.size();
+        e.len = (int)q.src_length[s];
+        for (size_t k = 0; k < q.src_length[s]; ++k)
+            vals.push_back(q.src_scale * q.src_fct[s * q.src_stride + k]);
+        src.push_back(e);
+    }
+    SamplePlan plan;
+    plan.build(q.nrec, q.rec_t0, q.rec_dt, q.dt, q.nsteps);
+    std::vector<RecEntry> rec;
+    for (size_t k = 0; k < q.nrec; ++k) {
+        const int f = field_id(q.rec_comp[k]);
+        if (q.rec_index[k] >= nx * nz || f < 0)
+            return sm_fail(SM_EINVAL, "sm_eiso_run_noalloc: receiver %zu outside the grid or "
+                                      "not an e_iso component", k);
+        RecEntry e{};
+        e.q = (long long)(q.rec_index[k] / nz + np) * (long long)pitch +
+              (long long)(q.rec_index[k] % nz + np);
+        e.shot = 0;
+        e.field = f;
+        e.group = plan.group_of[k];
+        e.out = (long long)k * (long long)plan.max_samples;
+        rec.push_back(e);
+    }
+    if (q.nrec && ld < plan.max_samples && traces)
+        return sm_fail(SM_EINVAL, "sm_eiso_run_noalloc: ld %zu < %zu samples per receiver", ld,
+                       plan.max_samples);
+
+    // ---- layout in the scratch array, and the size check ----
+    NoallocLayout lay;
+    const size_t o_set[2] = {lay.take(5 * fcells * sizeof(S)), lay.take(5 * fcells * sizeof(S))};
+    size_t o_split[2][10];
+    for (int k = 0; k < 2; ++k)
+        for (int a = 0; a < 10; ++a) o_split[k][a] = lay.take(pml * sizeof(S));
+    const size_t o_mat = lay.take(5 * fcells * sizeof(S));
+    const size_t o_prof = lay.take((size_t)P.size() * sizeof(S));
+    const size_t o_err = lay.take(sizeof(int));
+    const size_t o_step = lay.take(sizeof(long long));
+    const size_t o_src = lay.take(std::max<size_t>(src.size(), 1) * sizeof(SrcEntry));
+    const size_t o_first = lay.take(2 * sizeof(int));
+    const size_t o_vals = lay.take(std::max<size_t>(vals.size(), 1) * sizeof(double));
+    const size_t o_rec = lay.take(std::max<size_t>(rec.size(), 1) * sizeof(RecEntry));
+    const size_t o_table = lay.take(std::max<size_t>(plan.table.size(), 1) * sizeof(int32_t));
+    const size_t o_tr = lay.take(std::max<size_t>(q.nrec * plan.max_samples, 1) * sizeof(double));
+    if (lay.off > kNoallocBytes)
+        return sm_fail(SM_EINVAL,
+                       "sm_eiso_run_noalloc: this shot needs %zu bytes of device scratch, the "
+                       "library's fixed scratch holds %zu (use sm_eiso_create for larger shots)",
+                       lay.off, kNoallocBytes);
+
+    int ndev = 0;
+    SM_CUDA_TRY(cudaGetDeviceCount(&ndev));
+    if (device < 0 || device >= ndev)
+        return sm_fail(SM_EINVAL, "sm_eiso_run_noalloc: no CUDA device %d", device);
+    DeviceGuard g(device);
+    unsigned char *base = nullptr;
+    if (int rc = noalloc_scratch(device, &base)) return rc;
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+
+    // ---- inputs into the scratch; what must start at zero is cleared ----
+    SM_CUDA_TRY(cudaMemsetAsync(base, 0, o_mat, st));   // both sets and all split parts
+    SM_CUDA_TRY(cudaMemsetAsync(base + o_err, 0, o_src - o_err, st));
+    SM_CUDA_TRY(cudaMemsetAsync(base + o_tr, 0, lay.off - o_tr, st));
+    {
+        const double *m5[5] = {q.b, q.bm, q.la, q.l2m, q.mu};
+        std::vector<double> m(fcells, 0.0);
+        const double s = q.dt / q.h;
+        size_t lr = nx * nx - 1;   // pml.c:1044-1084, kept while inside the array
+        if (lr >= nx * nz) lr = nx * nz - 1;
+        for (int k = 0; k < 5; ++k) {
+            std::fill(m.begin(), m.end(), 0.0);
+            for (size_t X = 0; X < NX; ++X) {
+                const size_t i = X < np ? 0 : (X - np >= nx ? nx - 1 : X - np);
+                for (size_t Z = 0; Z < NZ; ++Z) {
+                    const size_t j = Z < np ? 0 : (Z - np >= nz ? nz - 1 : Z - np);
+                    size_t idx = i * nz + j;
+                    if ((k == M_LA || k == M_L2M) && X >= np + nx && Z >= np + nz) idx = lr;
+                    m[X * pitch + Z] = s * m5[k][idx];
+                }
+            }
+            if (int rc = upload_convert<S>(base + o_mat + k * fcells * sizeof(S), m.data(), fcells, st))
+                return rc;
+        }
+        std::vector<double> t((size_t)P.size(), 1.0);
+        auto fill = [&](int aoff, int boff, size_t n, size_t ncell, bool half) {
+            for (size_t X = 0; X < n; ++X) {
+                double dd = -1.0;
+                if (X < np) dd = half ? q.dh[X] : q.d[X];
+                else if (X >= np + ncell) {
+                    const size_t i = X - np - ncell;
+                    dd = half ? q.dH[np - 1 - i] : q.d[np - 1 - i];
+                }
+                if (dd >= 0.0) {
+                    t[aoff + X] = (2. - q.dt * dd) / (2. + q.dt * dd);
+                    t[boff + X] = 2. / (2. + q.dt * dd);
+                }
+            }
+        };
+        fill(P.axn(), P.bxn(), NX, nx, false);
+        fill(P.axh(), P.bxh(), NX, nx, true);
+        fill(P.azn(), P.bzn(), NZ, nz, false);
+        fill(P.azh(), P.bzh(), NZ, nz, true);
+        if (int rc = upload_convert<S>(base + o_prof, t.data(), t.size(), st)) return rc;
+    }
+    const int first[2] = {0, (int)src.size()};
+    if (!src.empty()) {
+        SM_CUDA_TRY(cudaMemcpyAsync(base + o_src, src.data(), src.size() * sizeof(SrcEntry),
+                                    cudaMemcpyHostToDevice, st));
+        SM_CUDA_TRY(cudaMemcpyAsync(base + o_first, first, sizeof(first), cudaMemcpyHostToDevice, st));
+        SM_CUDA_TRY(cudaMemcpyAsync(base + o_vals, vals.data(), vals.size() * sizeof(double),
+                                    cudaMemcpyHostToDevice, st));
+    }
+    if (!rec.empty()) {
+        SM_CUDA_TRY(cudaMemcpyAsync(base + o_rec, rec.data(), rec.size() * sizeof(RecEntry),
+                                    cudaMemcpyHostToDevice, st));
+        if (!plan.table.empty())
+            SM_CUDA_TRY(cudaMemcpyAsync(base + o_table, plan.table.data(),
+                                        plan.table.size() * sizeof(int32_t),
+                                        cudaMemcpyHostToDevice, st));
+    }
+    SM_CUDA_TRY(cudaStreamSynchronize(st));   // host staging goes out of scope below
+
+    // ---- kernel arguments and TMA maps over the scratch ----
+    EisoArgs a{};
+    a.NX = (int)NX; a.NZ = (int)NZ; a.pitch = (int)pitch;
+    a.np = (int)np; a.nx = (int)nx; a.nz = (int)nz;
+    a.fstride = (long long)fcells;
+    a.sstride = (long long)pml;
+    a.mid_off = (int)(np * NZ);
+    a.right_off = (int)(np * NZ + nx * 2 * np);
+    a.chunk = 1;
+    for (int f = 0; f < 5; ++f) {
+        a.mat[f] = base + o_mat + f * fcells * sizeof(S);
+        a.sc[f] = a.isc[f] = 1.0f;
+    }
+    a.prof = base + o_prof;
+    a.err = reinterpret_cast<int *>(base + o_err);
+    a.step = reinterpret_cast<long long *>(base + o_step);
+    EisoMaps maps[2];
+    auto field = [&](int set, int f) { return base + o_set[set] + f * fcells * sizeof(S); };
+    for (int b = 0; b < 2; ++b)
+        for (int f = 0; f < 5; ++f)
+            if (int rc = make_map_3d(&maps[b].f[f], field(b, f), MapType<S>::v, sizeof(S), NZ, NX,
+                                     1, pitch, L::BZ, L::RX))
+                return rc;
+    auto bind = [&](int cur) {
+        for (int f = 0; f < 5; ++f) {
+            a.f[f] = field(cur, f);
+            a.fo[f] = field(1 - cur, f);
+            a.fx[f] = base + o_split[cur][f];
+            a.fz[f] = base + o_split[cur][5 + f];
+            a.fxo[f] = base + o_split[1 - cur][f];
+            a.fzo[f] = base + o_split[1 - cur][5 + f];
+        }
+    };
+
+    // ---- the time loop: step, sources, receivers ----
+    const dim3 grd((unsigned)((NZ + 31) / 32), (unsigned)((NX + 7) / 8), 1);
+    int cur = 0;
+    for (size_t it = 0; it < q.nsteps; ++it) {
+        bind(cur);
+        eiso_tile_kernel<S, 8, 32, 128, 6><<<grd, 128, L::bytes, st>>>(a, maps[cur]);
+        cur = 1 - cur;
+        bind(cur);
+        if (!src.empty())
+            eiso_source_kernel<S><<<1, 128, 0, st>>>(
+                a, reinterpret_cast<const SrcEntry *>(base + o_src),
+                reinterpret_cast<const int *>(base + o_first),
+                reinterpret_cast<const double *>(base + o_vals), 1);
+        if (!rec.empty())
+            eiso_gather_kernel<S><<<(unsigned)((rec.size() + 127) / 128), 128, 0, st>>>(
+                a, reinterpret_cast<const RecEntry *>(base + o_rec), (int)rec.size(),
+                reinterpret_cast<const int32_t *>(base + o_table), (long long)plan.nsteps_max,
+                reinterpret_cast<double *>(base + o_tr));
+    }
+    SM_CUDA_TRY(cudaGetLastError());
+
+    // ---- traces back to the caller ----
+    int err = 0;
+    SM_CUDA_TRY(cudaMemcpyAsync(&err, base + o_err, sizeof(int), cudaMemcpyDeviceToHost, st));
+    SM_CUDA_TRY(cudaStreamSynchronize(st));
+    if (err) return sm_fail(SM_ETIMEOUT, "sm_eiso_run_noalloc: a bounded wait for a TMA load gave up");
+    for (size_t k = 0; k < q.nrec; ++k) {
+        size_t c = 0;
+        const size_t lim = std::min(q.nsteps, plan.nsteps_max);
+        for (size_t it = 0; it < lim; ++it)
+            if (plan.table[(size_t)rec[k].group * plan.nsteps_max + it] >= 0) ++c;
+        counts[k] = c;
+        if (traces && c)
+            SM_CUDA_TRY(cudaMemcpyAsync(traces + k * ld,
+                                        base + o_tr + (size_t)rec[k].out * sizeof(double),
+                                        c * sizeof(double), cudaMemcpyDeviceToHost, st));
+    }
+    SM_CUDA_TRY(cudaStreamSynchronize(st));
+    return SM_OK;
+}
