@@ -76,12 +76,9 @@ _SIGS = {
     "sm_a3d_destroy": (C.c_int, [_vp]),
     "sm_eiso_stream": (C.c_int, [_vp, C.POINTER(_vp)]),
     "sm_eiso_set_timing": (C.c_int, [_vp, C.c_int]),
-    "sm_eiso_set_chunk": (C.c_int, [_vp, C.c_int]),
-    "sm_eiso_get_chunk": (C.c_int, [_vp, C.POINTER(C.c_int)]),
     "sm_eiso_set_config": (C.c_int, [_vp, C.c_int]),
     "sm_eiso_get_config": (C.c_int, [_vp, C.POINTER(C.c_int), C.POINTER(C.c_int)]),
-    "sm_eiso_autotune": (C.c_int, [_vp, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int),
-                                   C.POINTER(C.c_double)]),
+    "sm_eiso_autotune": (C.c_int, [_vp, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_double)]),
     "sm_eiso_set_graph": (C.c_int, [_vp, C.c_int]),
     "sm_eiso_kernel_stats": (C.c_int, [_vp, C.c_int, _dp, _szp, _szp]),
     "sm_a3d_stream": (C.c_int, [_vp, C.POINTER(_vp)]),

@@ -185,24 +185,15 @@ class EIsoDevice:
     def set_timing(self, on=True):
         L.check(L.load().sm_eiso_set_timing(self._h, 1 if on else 0))
 
-    def set_chunk(self, chunk):
-        L.check(L.load().sm_eiso_set_chunk(self._h, int(chunk)))
-
-    def get_chunk(self):
-        c = C.c_int()
-        L.check(L.load().sm_eiso_get_chunk(self._h, C.byref(c)))
-        return c.value
-
     def set_config(self, config):
         L.check(L.load().sm_eiso_set_config(self._h, int(config)))
 
     def autotune(self, trial_steps=20):
         """Pick the fastest launch configuration (the handle is left reset).
-        Returns (config, chunk, ms per step)."""
-        c, k, ms = C.c_int(), C.c_int(), C.c_double()
-        L.check(L.load().sm_eiso_autotune(self._h, int(trial_steps), C.byref(c), C.byref(k),
-                                          C.byref(ms)))
-        return c.value, k.value, ms.value
+        Returns (config, ms per step)."""
+        c, ms = C.c_int(), C.c_double()
+        L.check(L.load().sm_eiso_autotune(self._h, int(trial_steps), C.byref(c), C.byref(ms)))
+        return c.value, ms.value
 
     def set_graph(self, steps):
         L.check(L.load().sm_eiso_set_graph(self._h, int(steps)))

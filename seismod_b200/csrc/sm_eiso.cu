@@ -64,10 +64,10 @@ struct EisoArgs {
     void *fo[5];         // written this step (the other buffer set)
     void *fxo[5];
     void *fzo[5];
-    int chunk;           // rows (x) each warp marches through
     int *err;            // set by a bounded wait that gave up
     long long *step;     // steps begun; the step kernel counts, source and
                          // receiver kernels of step it read it + 1
+    int nshots;          // shots in the buffers
     const void *mat[5];
     const void *prof;
     float sc[5], isc[5];
@@ -168,96 +168,78 @@ __device__ __forceinline__ C e_vz(const EisoArgs &a, long long sb, int X, int Z,
 }
 
 // ---------------------------------------------------------------------------
-// Band step kernel: one time step (e_iso.c:595-636), fused.  Each warp owns
-// 30 consecutive z cells of one shot and marches along x over rows [X0, X1);
-// lane l computes z = Z0 - 1 + l, lanes 0 and 31 being the halo cells, so
-// every z neighbour comes from a warp shuffle.  Each warp keeps its own ring
-// of D rows in shared memory, filled by TMA (one box spans the five
-// wavefields, one the five materials; out-of-grid cells read as zero, the
-// reference's boundary), so warps never wait on one another.  Iteration X
-// computes vx of row X+1 and vz of row X (velocity half step), then txx,
-// tzz, txz of row X (stress half step), with vx of row X and vz of row X-1
-// carried in registers.  Frame split parts are loaded one row ahead.  Old
-// and new state live in separate buffer sets (ping-pong).
+// Slab step kernel: one time step (e_iso.c:595-636) over a slab of TX rows and
+// W warp columns of 30 z cells.  One TMA box brings the five old wavefields
+// of rows X0-1 .. X0+TX and z cells Z0-1 .. Z0+30W (start rounded down to 16
+// bytes; out-of-grid cells read as zero, the reference's boundary), one more
+// the five materials; then each warp marches its column down the slab out of
+// shared memory, as the band kernel does (z neighbours by shuffles, vx of
+// row X and vz of row X-1 carried in registers), with no further waits.
 // ---------------------------------------------------------------------------
-struct EisoBandMaps {
-    CUtensorMap f;   // the old set's wavefields: (z, x, shot, field), box (BW, 1, 1, 5)
-    CUtensorMap m;   // materials: (z, x, material), box (BWC, 1, 5)
+struct EisoSlabMaps {
+    CUtensorMap f;   // the old set's wavefields: (z, x, shot, field), box (BW, TX+2, 1, 5)
+    CUtensorMap m;   // materials: (z, x, material), box (BWC, TX+2, 5)
 };
 
-template <typename S>
-struct EBand {
+template <typename S, int W, int TX>
+struct ESlab {
     using C = typename Store<S>::C;
     static constexpr int HS = 16 / (int)sizeof(S), HC = 16 / (int)sizeof(C);
-    // a warp reads z cells Z0-1 .. Z0+30 from a start rounded down to 16 bytes
-    static constexpr int BW = (32 + HS - 1 + HS - 1) / HS * HS;
-    static constexpr int BWC = (32 + HC - 1 + HC - 1) / HC * HC;
+    static constexpr int RX = TX + 2;
+    static constexpr int BW = (30 * W + 2 + HS - 1 + HS - 1) / HS * HS;
+    static constexpr int BWC = (30 * W + 2 + HC - 1 + HC - 1) / HC * HC;
     static constexpr size_t al(size_t x) { return (x + 127) / 128 * 128; }
-    static constexpr size_t oM = al(5 * (size_t)BW * sizeof(S));   // materials in a stage
-    static constexpr size_t stage = oM + al(5 * (size_t)BWC * sizeof(C));
-    static constexpr unsigned tx = (unsigned)(5 * BW * sizeof(S) + 5 * BWC * sizeof(C));
-    static constexpr size_t warp_bytes(int D) { return D * stage + al(8 * (size_t)D); }
+    static constexpr size_t oM = al(5 * (size_t)RX * BW * sizeof(S));
+    static constexpr size_t oBar = al(oM + 5 * (size_t)RX * BWC * sizeof(C));
+    static constexpr size_t bytes = oBar + 16;
+    static constexpr unsigned tx =
+        (unsigned)(5 * RX * BW * sizeof(S) + 5 * RX * BWC * sizeof(C));
 };
 
-template <typename S, int W, int D, int MINB>
-__global__ void __launch_bounds__(32 * W, MINB) eiso_band_kernel(const EisoArgs a,
-                                                                 const __grid_constant__ EisoBandMaps mp) {
+template <typename S, int W, int TX, int MINB>
+__global__ void __launch_bounds__(32 * W, MINB) eiso_slab_kernel(const EisoArgs a,
+                                                                 const __grid_constant__ EisoSlabMaps mp) {
     using C = typename Store<S>::C;
     using St = Store<S>;
-    using L = EBand<S>;
+    using L = ESlab<S, W, TX>;
     extern __shared__ __align__(128) unsigned char smem[];
     const unsigned full = 0xffffffffu;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     if ((blockIdx.x | blockIdx.y | blockIdx.z | threadIdx.x) == 0) ++*a.step;
-    unsigned char *ring = smem + (size_t)warp * L::warp_bytes(D);
-    uint64_t *bars = reinterpret_cast<uint64_t *>(ring + (size_t)D * L::stage);
-    const int Z0 = (blockIdx.x * W + warp) * 30;
-    if (Z0 >= a.NZ) return;                          // whole warp idle
+    const S *fbox = reinterpret_cast<const S *>(smem);
+    const C *mbox = reinterpret_cast<const C *>(smem + L::oM);
+    uint64_t *bar = reinterpret_cast<uint64_t *>(smem + L::oBar);
+    const int Zc = blockIdx.x * W * 30;              // the slab's first column
+    const int X0 = blockIdx.y * TX;
+    const int X1 = min(X0 + TX, a.NX);
+    const int shot = blockIdx.z;
+    // box starts: Zc - 1 rounded down to 16 bytes (Zc - 1 >= -1)
+    const int zs = (Zc - 1 + L::HS) / L::HS * L::HS - L::HS;
+    const int zc = (Zc - 1 + L::HC) / L::HC * L::HC - L::HC;
+    if (threadIdx.x == 0) {
+        mbar_init(bar, 1);
+        fence_proxy_async();
+        mbar_expect_tx(bar, L::tx);
+        tma_load_4d(smem, &mp.f, zs, X0 - 1, shot, 0, bar);
+        tma_load_3d(smem + L::oM, &mp.m, zc, X0 - 1, 0, bar);
+    }
+    __syncthreads();   // the barrier is initialised before anyone polls it
+    const int Z0 = Zc + warp * 30;
+    // warp 0 always has cells (the grid holds no empty slab) and keeps the
+    // CTA alive until the copy has landed; later warps past the grid leave
+    if (Z0 >= a.NZ) return;
     const int Z = Z0 - 1 + lane;
     const bool zin = Z >= 0 && Z < a.NZ;
     const bool own = lane >= 1 && lane <= 30 && Z < a.NZ;
-    const int X0 = blockIdx.y * a.chunk;
-    const int X1 = min(X0 + a.chunk, a.NX);
-    const int shot = blockIdx.z;
     const long long fb = (long long)shot * a.fstride;
     const long long sb = (long long)shot * a.sstride;
     const C zero = C(0);
-    // box starts: Z0 - 1 rounded down to 16 bytes (Z0 - 1 >= -1)
-    const int zs = (Z0 - 1 + L::HS) / L::HS * L::HS - L::HS;
-    const int zc = (Z0 - 1 + L::HC) / L::HC * L::HC - L::HC;
-    const int of = Z - zs, om = Z - zc;              // this lane's cell in a stage row
-    const int nrows = X1 - X0 + 2;                   // rows X0-1 .. X1
-    if (lane == 0) {
-        for (int d = 0; d < D; ++d) mbar_init(&bars[d], 1);
-        fence_proxy_async();
-    }
-    __syncwarp();
-    // ring: row X0-1+rho lives in slot rho % D, phase (rho / D) & 1
-    auto issue = [&](int rho) {                      // lane 0 only
-        if (rho >= nrows) return;
-        unsigned char *st = ring + (size_t)(rho % D) * L::stage;
-        uint64_t *bar = &bars[rho % D];
-        fence_proxy_async();
-        mbar_expect_tx(bar, L::tx);
-        tma_load_4d(st, &mp.f, zs, X0 - 1 + rho, shot, 0, bar);
-        tma_load_3d(st + L::oM, &mp.m, zc, X0 - 1 + rho, 0, bar);
+    const int of = Z - zs, om = Z - zc;              // this lane's cell in a box row
+    // row X0-1+rho of field f / material m at this lane's cell
+    auto F = [&](int rho, int f) -> C {
+        return St::ld(fbox + (f * L::RX + rho) * L::BW + of, a.isc[f]);
     };
-    if (lane == 0)
-        for (int r = 0; r < min(D, nrows); ++r) issue(r);
-    auto wait = [&](int rho) -> bool {
-        return __all_sync(full, mbar_wait(&bars[rho % D], (rho / D) & 1, a.err, 3));
-    };
-    // after a failed wait: give the copies of rows [from, to) a last bounded chance
-    auto drain = [&](int from, int to) {
-        for (int r = from; r < min(to, nrows); ++r) mbar_wait(&bars[r % D], (r / D) & 1, a.err, 3);
-    };
-    auto stage = [&](int rho) { return ring + (size_t)(rho % D) * L::stage; };
-    auto F = [&](const unsigned char *st, int f) -> C {
-        return St::ld(reinterpret_cast<const S *>(st) + f * L::BW + of, a.isc[f]);
-    };
-    auto M = [&](const unsigned char *st, int m) -> C {
-        return reinterpret_cast<const C *>(st + L::oM)[m * L::BWC + om];
-    };
+    auto M = [&](int rho, int m) -> C { return mbox[(m * L::RX + rho) * L::BWC + om]; };
     const bool zint = (Z0 - 1 >= a.np) && (Z0 + 30 <= a.np + a.nz - 1);
     EZProf<C> zp{C(1), C(1), C(1), C(1)};
     if (zin) {
@@ -271,52 +253,44 @@ __global__ void __launch_bounds__(32 * W, MINB) eiso_band_kernel(const EisoArgs 
     S *tzzo = static_cast<S *>(a.fo[F_TZZ]) + fb;
     S *txzo = static_cast<S *>(a.fo[F_TXZ]) + fb;
 
-    // ---- prologue: vx of row X0 and vz of row X0-1 (recomputed; stored
-    // only for X0 == 0, the row no other warp's march reaches) ----
     ESplit<C> sp;
     e_load_split<S, C>(a, sb, X0 - 1, Z, zin, sp);
-    if (!wait(0) || !wait(1)) { drain(0, D); return; }
+    if (!__all_sync(full, mbar_wait(bar, 0, a.err, 4))) {
+        mbar_wait(bar, 0, a.err, 4);   // a last bounded chance for the copy in flight
+        return;
+    }
+
+    // ---- prologue: vx of row X0 and vz of row X0-1 (recomputed; stored
+    // only for X0 == 0, the row no other slab reaches) ----
     C vxc, vzp;
     {
-        const unsigned char *p = stage(0), *c = stage(1);
-        const C c_txz = F(c, F_TXZ), p_tzz = F(p, F_TZZ);
+        const C c_txz = F(1, F_TXZ), p_tzz = F(0, F_TZZ);
         const C txz_zm = __shfl_up_sync(full, c_txz, 1);
         const C tzz_zp = __shfl_down_sync(full, p_tzz, 1);
-        vxc = zin ? e_vx<S, C>(a, sb, X0, Z, F(c, F_VX), M(c, M_B), r_sub(F(c, F_TXX), F(p, F_TXX)),
+        vxc = zin ? e_vx<S, C>(a, sb, X0, Z, F(1, F_VX), M(1, M_B), r_sub(F(1, F_TXX), F(0, F_TXX)),
                                r_sub(c_txz, txz_zm), sp.vx, zp, X0 == 0 && own)
                   : zero;
         if (X0 == 0 && own) St::st(vxo + (long long)X0 * a.pitch + Z, vxc, a.sc[F_VX]);
         vzp = zero;
         if (X0 >= 1 && zin)
-            vzp = e_vz<S, C>(a, sb, X0 - 1, Z, F(p, F_VZ), M(p, M_BM), r_sub(c_txz, F(p, F_TXZ)),
+            vzp = e_vz<S, C>(a, sb, X0 - 1, Z, F(0, F_VZ), M(0, M_BM), r_sub(c_txz, F(0, F_TXZ)),
                              r_sub(tzz_zp, p_tzz), sp.vz, zp, false);
     }
-    __syncwarp();
-    if (lane == 0) issue(D);                         // row X0-1 is done with
 
-    // Lean loop: every row of this warp's march, and the next one, lies in
-    // the interior update region, so no frame tests and no split parts; the
-    // arithmetic is the general loop's interior branch, operation for
-    // operation.
+    // Lean loop: every row of this slab and the one after lie in the interior
+    // update region: no frame tests, no split parts; the arithmetic is the
+    // general loop's interior branch, operation for operation.
     if (zint && X0 >= a.np && X1 <= a.np + a.nx - 1) {
         long long q = fb + (long long)X0 * a.pitch + Z;
         S *const fo0 = static_cast<S *>(a.fo[0]);   // the five arrays of the new set
         const long long fso = static_cast<S *>(a.fo[1]) - fo0;
+#pragma unroll 2
         for (int rc = 1; rc <= X1 - X0; ++rc, q += a.pitch) {
-            if (!wait(rc + 1)) { drain(rc + 1, rc + D); return; }
-            const S *cf = reinterpret_cast<const S *>(stage(rc)) + of;
-            const S *nf = reinterpret_cast<const S *>(stage(rc + 1)) + of;
-            const C *cm = reinterpret_cast<const C *>(stage(rc) + L::oM) + om;
-            const C *nm = reinterpret_cast<const C *>(stage(rc + 1) + L::oM) + om;
-            const C n_txz = St::ld(nf + F_TXZ * L::BW, a.isc[F_TXZ]);
-            const C c_txz = St::ld(cf + F_TXZ * L::BW, a.isc[F_TXZ]);
-            const C c_tzz = St::ld(cf + F_TZZ * L::BW, a.isc[F_TZZ]);
-            const C c_txx = St::ld(cf + F_TXX * L::BW, a.isc[F_TXX]);
-            const C n_txx = St::ld(nf + F_TXX * L::BW, a.isc[F_TXX]);
-            const C n_vx = St::ld(nf + F_VX * L::BW, a.isc[F_VX]);
-            const C c_vz = St::ld(cf + F_VZ * L::BW, a.isc[F_VZ]);
-            const C n_b = nm[M_B * L::BWC], c_bm = cm[M_BM * L::BWC];
-            const C la = cm[M_LA * L::BWC], l2m = cm[M_L2M * L::BWC], mu = cm[M_MU * L::BWC];
+            const C n_txz = F(rc + 1, F_TXZ), c_txz = F(rc, F_TXZ), c_tzz = F(rc, F_TZZ);
+            const C c_txx = F(rc, F_TXX), n_txx = F(rc + 1, F_TXX);
+            const C n_vx = F(rc + 1, F_VX), c_vz = F(rc, F_VZ);
+            const C n_b = M(rc + 1, M_B), c_bm = M(rc, M_BM);
+            const C la = M(rc, M_LA), l2m = M(rc, M_L2M), mu = M(rc, M_MU);
             const C txz_zm = __shfl_up_sync(full, n_txz, 1);
             const C tzz_zp = __shfl_down_sync(full, c_tzz, 1);
             const C ax = r_sub(n_txx, c_txx), az = r_sub(n_txz, txz_zm);
@@ -330,8 +304,6 @@ __global__ void __launch_bounds__(32 * W, MINB) eiso_band_kernel(const EisoArgs 
             const C txx = r_add(c_txx, r_fma(l2m, sax, r_mul(la, saz)));
             const C tzz = r_add(c_tzz, r_fma(l2m, saz, r_mul(la, sax)));
             const C txz = r_fma(mu, r_add(sbz, sbx), c_txz);
-            __syncwarp();
-            if (lane == 0) issue(rc + D);            // row X0-1+rc is done with
             if (own) {
                 S *o = fo0 + q;
                 St::st(o + F_VX * fso + a.pitch, vxn, a.sc[F_VX]);
@@ -351,33 +323,33 @@ __global__ void __launch_bounds__(32 * W, MINB) eiso_band_kernel(const EisoArgs 
         const int rc = X - X0 + 1;                   // row X; row X+1 is rc + 1
         ESplit<C> sn;
         e_load_split<S, C>(a, sb, X + 1, Z, zin && X + 1 < X1, sn);
-        if (!wait(rc + 1)) { drain(rc + 1, rc + D); return; }
-        const unsigned char *c = stage(rc), *n = stage(rc + 1);
         const bool fast = zint && X >= a.np && X + 1 <= a.np + a.nx - 1;
         const long long q = (long long)X * a.pitch + Z;
         // ---- velocities: vx(X+1), vz(X) (propagate.c:2511-2588, pml.c:39-680) ----
-        const C n_txz = F(n, F_TXZ), c_txz = F(c, F_TXZ), c_tzz = F(c, F_TZZ);
-        const C c_txx = F(c, F_TXX);
+        const C n_txz = F(rc + 1, F_TXZ), c_txz = F(rc, F_TXZ), c_tzz = F(rc, F_TZZ);
+        const C c_txx = F(rc, F_TXX);
         const C txz_zm = __shfl_up_sync(full, n_txz, 1);
         const C tzz_zp = __shfl_down_sync(full, c_tzz, 1);
-        const C ax = r_sub(F(n, F_TXX), c_txx), az = r_sub(n_txz, txz_zm);
+        const C ax = r_sub(F(rc + 1, F_TXX), c_txx), az = r_sub(n_txz, txz_zm);
         const C bx = r_sub(n_txz, c_txz), bz = r_sub(tzz_zp, c_tzz);
         C vxn, vzn;
         if (fast) {
-            vxn = r_fma(M(n, M_B), r_add(ax, az), F(n, F_VX));
-            vzn = r_fma(M(c, M_BM), r_add(bx, bz), F(c, F_VZ));
+            vxn = r_fma(M(rc + 1, M_B), r_add(ax, az), F(rc + 1, F_VX));
+            vzn = r_fma(M(rc, M_BM), r_add(bx, bz), F(rc, F_VZ));
         } else {
             vxn = (X + 1 < a.NX && zin)
-                      ? e_vx<S, C>(a, sb, X + 1, Z, F(n, F_VX), M(n, M_B), ax, az, sp.vx, zp, own)
+                      ? e_vx<S, C>(a, sb, X + 1, Z, F(rc + 1, F_VX), M(rc + 1, M_B), ax, az, sp.vx,
+                                   zp, own)
                       : zero;
-            vzn = zin ? e_vz<S, C>(a, sb, X, Z, F(c, F_VZ), M(c, M_BM), bx, bz, sp.vz, zp, own) : zero;
+            vzn = zin ? e_vz<S, C>(a, sb, X, Z, F(rc, F_VZ), M(rc, M_BM), bx, bz, sp.vz, zp, own)
+                      : zero;
         }
         // ---- stresses of row X (propagate.c:2590-2670, pml.c:684-1403) ----
         const C vz_zm = __shfl_up_sync(full, vzn, 1);
         const C vx_zp = __shfl_down_sync(full, vxc, 1);
         const C sax = r_sub(vxn, vxc), saz = r_sub(vzn, vz_zm);   // txx, tzz
         const C sbz = r_sub(vx_zp, vxc), sbx = r_sub(vzn, vzp);   // txz
-        const C la = M(c, M_LA), l2m = M(c, M_L2M), mu = M(c, M_MU);
+        const C la = M(rc, M_LA), l2m = M(rc, M_L2M), mu = M(rc, M_MU);
         C txx, tzz, txz;
         if (fast || (zin && e_inside(a, X, Z))) {
             txx = r_add(c_txx, r_fma(l2m, sax, r_mul(la, saz)));
@@ -397,8 +369,234 @@ __global__ void __launch_bounds__(32 * W, MINB) eiso_band_kernel(const EisoArgs 
         } else {
             txx = tzz = txz = zero;
         }
-        __syncwarp();
-        if (lane == 0) issue(rc + D);                // row X is done with
+        if (own) {
+            if (X + 1 < a.NX) St::st(vxo + q + a.pitch, vxn, a.sc[F_VX]);
+            St::st(vzo + q, vzn, a.sc[F_VZ]);
+            St::st(txxo + q, txx, a.sc[F_TXX]);
+            St::st(tzzo + q, tzz, a.sc[F_TZZ]);
+            St::st(txzo + q, txz, a.sc[F_TXZ]);
+        }
+        vxc = vxn;
+        vzp = vzn;
+        sp = sn;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Slab step kernel with materials from global memory: the slab kernel with
+// only the wavefields in the TMA box (half the shared memory per cell, so
+// twice the slabs in flight per SM).  The materials of a slab's rows are read
+// from L2 (they are shared by every shot) into registers before the TMA wait,
+// so their latency hides behind it.
+// ---------------------------------------------------------------------------
+template <typename S, int W, int TX>
+struct ESlabG {
+    static constexpr int HS = 16 / (int)sizeof(S);
+    static constexpr int RX = TX + 2;
+    static constexpr int BW = (30 * W + 2 + HS - 1 + HS - 1) / HS * HS;
+    static constexpr int BWC = 4;   // unused: no materials box
+    static constexpr size_t al(size_t x) { return (x + 127) / 128 * 128; }
+    static constexpr size_t oBar = al(5 * (size_t)RX * BW * sizeof(S));
+    static constexpr size_t bytes = oBar + 16;
+    static constexpr unsigned tx = (unsigned)(5 * RX * BW * sizeof(S));
+};
+
+template <typename S, int W, int TX, int MINB>
+__global__ void __launch_bounds__(32 * W, MINB) eiso_slabg_kernel(const EisoArgs a,
+                                                                  const __grid_constant__ EisoSlabMaps mp) {
+    using C = typename Store<S>::C;
+    using St = Store<S>;
+    using L = ESlabG<S, W, TX>;
+    extern __shared__ __align__(128) unsigned char smem[];
+    const unsigned full = 0xffffffffu;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    if ((blockIdx.x | blockIdx.y | blockIdx.z | threadIdx.x) == 0) ++*a.step;
+    const S *fbox = reinterpret_cast<const S *>(smem);
+    uint64_t *bar = reinterpret_cast<uint64_t *>(smem + L::oBar);
+    const int Zc = blockIdx.x * W * 30;
+    const int X0 = blockIdx.y * TX;
+    const int X1 = min(X0 + TX, a.NX);
+    const int shot = blockIdx.z;
+    const int zs = (Zc - 1 + L::HS) / L::HS * L::HS - L::HS;
+    if (threadIdx.x == 0) {
+        mbar_init(bar, 1);
+        fence_proxy_async();
+        mbar_expect_tx(bar, L::tx);
+        tma_load_4d(smem, &mp.f, zs, X0 - 1, shot, 0, bar);
+    }
+    __syncthreads();   // the barrier is initialised before anyone polls it
+    const int Z0 = Zc + warp * 30;
+    // warp 0 always has cells and keeps the CTA alive until the copy has
+    // landed; later warps past the grid leave
+    if (Z0 >= a.NZ) return;
+    const int Z = Z0 - 1 + lane;
+    const bool zin = Z >= 0 && Z < a.NZ;
+    const bool own = lane >= 1 && lane <= 30 && Z < a.NZ;
+    const long long fb = (long long)shot * a.fstride;
+    const long long sb = (long long)shot * a.sstride;
+    const C zero = C(0);
+    const int of = Z - zs;
+    auto F = [&](int rho, int f) -> C {
+        return St::ld(fbox + (f * L::RX + rho) * L::BW + of, a.isc[f]);
+    };
+    // material m of row X0-1+rho at this lane's cell, zero off the grid (as
+    // the TMA box would read it)
+    auto M = [&](int rho, int m) -> C {
+        const int x = X0 - 1 + rho;
+        if (!zin || x < 0 || x >= a.NX) return zero;
+        return __ldg(static_cast<const C *>(a.mat[m]) + (long long)x * a.pitch + Z);
+    };
+    const bool zint = (Z0 - 1 >= a.np) && (Z0 + 30 <= a.np + a.nz - 1);
+    const bool lean = zint && X0 >= a.np && X1 <= a.np + a.nx - 1;
+    S *const fo0 = static_cast<S *>(a.fo[0]);
+    const long long fso = static_cast<S *>(a.fo[1]) - fo0;
+    S *vxo = fo0 + F_VX * fso + fb, *vzo = fo0 + F_VZ * fso + fb;
+    S *txxo = fo0 + F_TXX * fso + fb, *tzzo = fo0 + F_TZZ * fso + fb, *txzo = fo0 + F_TXZ * fso + fb;
+
+    if (lean) {
+        // materials of every row of the slab, read while the box is in flight
+        C nb[TX], cbm[TX], cla[TX], cl2m[TX], cmu[TX];
+        const C b1 = M(1, M_B), bm0 = M(0, M_BM);
+#pragma unroll
+        for (int r = 0; r < TX; ++r) {
+            nb[r] = M(r + 2, M_B);
+            cbm[r] = M(r + 1, M_BM);
+            cla[r] = M(r + 1, M_LA);
+            cl2m[r] = M(r + 1, M_L2M);
+            cmu[r] = M(r + 1, M_MU);
+        }
+        if (!__all_sync(full, mbar_wait(bar, 0, a.err, 9))) {
+            mbar_wait(bar, 0, a.err, 9);
+            return;
+        }
+        C vxc, vzp;
+        {
+            const C c_txz = F(1, F_TXZ), p_tzz = F(0, F_TZZ);
+            const C txz_zm = __shfl_up_sync(full, c_txz, 1);
+            const C tzz_zp = __shfl_down_sync(full, p_tzz, 1);
+            // interior cells (lean): e_vx / e_vz reduce to their interior branch
+            vxc = r_fma(b1, r_add(r_sub(F(1, F_TXX), F(0, F_TXX)), r_sub(c_txz, txz_zm)), F(1, F_VX));
+            vzp = zero;
+            if (X0 - 1 >= a.np)
+                vzp = r_fma(bm0, r_add(r_sub(c_txz, F(0, F_TXZ)), r_sub(tzz_zp, p_tzz)), F(0, F_VZ));
+        }
+        if (X0 - 1 < a.np) {
+            // vz of row X0-1 lies in the frame: the general helper with its split parts
+            ESplit<C> sp;
+            const EisoProf P{a.NX, a.NZ};
+            const C *pr = static_cast<const C *>(a.prof);
+            e_load_split<S, C>(a, sb, X0 - 1, Z, zin, sp);
+            const EZProf<C> zp{pr[P.azn() + Z], pr[P.bzn() + Z], pr[P.azh() + Z], pr[P.bzh() + Z]};
+            const C c_txz = F(1, F_TXZ), p_tzz = F(0, F_TZZ);
+            const C tzz_zp = __shfl_down_sync(full, p_tzz, 1);
+            vzp = e_vz<S, C>(a, sb, X0 - 1, Z, F(0, F_VZ), bm0, r_sub(c_txz, F(0, F_TXZ)),
+                             r_sub(tzz_zp, p_tzz), sp.vz, zp, false);
+        }
+        long long q = (long long)X0 * a.pitch + Z;
+#pragma unroll
+        for (int r = 0; r < TX; ++r, q += a.pitch) {
+            if (r >= X1 - X0) break;
+            const int rc = r + 1;
+            const C n_txz = F(rc + 1, F_TXZ), c_txz = F(rc, F_TXZ), c_tzz = F(rc, F_TZZ);
+            const C c_txx = F(rc, F_TXX), n_txx = F(rc + 1, F_TXX);
+            const C n_vx = F(rc + 1, F_VX), c_vz = F(rc, F_VZ);
+            const C txz_zm = __shfl_up_sync(full, n_txz, 1);
+            const C tzz_zp = __shfl_down_sync(full, c_tzz, 1);
+            const C ax = r_sub(n_txx, c_txx), az = r_sub(n_txz, txz_zm);
+            const C bx = r_sub(n_txz, c_txz), bz = r_sub(tzz_zp, c_tzz);
+            const C vxn = r_fma(nb[r], r_add(ax, az), n_vx);
+            const C vzn = r_fma(cbm[r], r_add(bx, bz), c_vz);
+            const C vz_zm = __shfl_up_sync(full, vzn, 1);
+            const C vx_zp = __shfl_down_sync(full, vxc, 1);
+            const C sax = r_sub(vxn, vxc), saz = r_sub(vzn, vz_zm);
+            const C sbz = r_sub(vx_zp, vxc), sbx = r_sub(vzn, vzp);
+            const C txx = r_add(c_txx, r_fma(cl2m[r], sax, r_mul(cla[r], saz)));
+            const C tzz = r_add(c_tzz, r_fma(cl2m[r], saz, r_mul(cla[r], sax)));
+            const C txz = r_fma(cmu[r], r_add(sbz, sbx), c_txz);
+            if (own) {
+                St::st(vxo + q + a.pitch, vxn, a.sc[F_VX]);
+                St::st(vzo + q, vzn, a.sc[F_VZ]);
+                St::st(txxo + q, txx, a.sc[F_TXX]);
+                St::st(tzzo + q, tzz, a.sc[F_TZZ]);
+                St::st(txzo + q, txz, a.sc[F_TXZ]);
+            }
+            vxc = vxn;
+            vzp = vzn;
+        }
+        return;
+    }
+
+    // general march (frame): materials straight from L2
+    const C *pr = static_cast<const C *>(a.prof);
+    const EisoProf P{a.NX, a.NZ};
+    EZProf<C> zp{C(1), C(1), C(1), C(1)};
+    if (zin) zp = EZProf<C>{pr[P.azn() + Z], pr[P.bzn() + Z], pr[P.azh() + Z], pr[P.bzh() + Z]};
+    ESplit<C> sp;
+    e_load_split<S, C>(a, sb, X0 - 1, Z, zin, sp);
+    if (!__all_sync(full, mbar_wait(bar, 0, a.err, 9))) {
+        mbar_wait(bar, 0, a.err, 9);
+        return;
+    }
+    C vxc, vzp;
+    {
+        const C c_txz = F(1, F_TXZ), p_tzz = F(0, F_TZZ);
+        const C txz_zm = __shfl_up_sync(full, c_txz, 1);
+        const C tzz_zp = __shfl_down_sync(full, p_tzz, 1);
+        vxc = zin ? e_vx<S, C>(a, sb, X0, Z, F(1, F_VX), M(1, M_B), r_sub(F(1, F_TXX), F(0, F_TXX)),
+                               r_sub(c_txz, txz_zm), sp.vx, zp, X0 == 0 && own)
+                  : zero;
+        if (X0 == 0 && own) St::st(vxo + (long long)X0 * a.pitch + Z, vxc, a.sc[F_VX]);
+        vzp = zero;
+        if (X0 >= 1 && zin)
+            vzp = e_vz<S, C>(a, sb, X0 - 1, Z, F(0, F_VZ), M(0, M_BM), r_sub(c_txz, F(0, F_TXZ)),
+                             r_sub(tzz_zp, p_tzz), sp.vz, zp, false);
+    }
+    e_load_split<S, C>(a, sb, X0, Z, zin, sp);
+    for (int X = X0; X < X1; ++X) {
+        const int rc = X - X0 + 1;
+        ESplit<C> sn;
+        e_load_split<S, C>(a, sb, X + 1, Z, zin && X + 1 < X1, sn);
+        const bool fast = zint && X >= a.np && X + 1 <= a.np + a.nx - 1;
+        const long long q = (long long)X * a.pitch + Z;
+        const C n_b = M(rc + 1, M_B), c_bm = M(rc, M_BM);
+        const C la = M(rc, M_LA), l2m = M(rc, M_L2M), mu = M(rc, M_MU);
+        const C n_txz = F(rc + 1, F_TXZ), c_txz = F(rc, F_TXZ), c_tzz = F(rc, F_TZZ);
+        const C c_txx = F(rc, F_TXX);
+        const C txz_zm = __shfl_up_sync(full, n_txz, 1);
+        const C tzz_zp = __shfl_down_sync(full, c_tzz, 1);
+        const C ax = r_sub(F(rc + 1, F_TXX), c_txx), az = r_sub(n_txz, txz_zm);
+        const C bx = r_sub(n_txz, c_txz), bz = r_sub(tzz_zp, c_tzz);
+        C vxn, vzn;
+        if (fast) {
+            vxn = r_fma(n_b, r_add(ax, az), F(rc + 1, F_VX));
+            vzn = r_fma(c_bm, r_add(bx, bz), F(rc, F_VZ));
+        } else {
+            vxn = (X + 1 < a.NX && zin)
+                      ? e_vx<S, C>(a, sb, X + 1, Z, F(rc + 1, F_VX), n_b, ax, az, sp.vx, zp, own)
+                      : zero;
+            vzn = zin ? e_vz<S, C>(a, sb, X, Z, F(rc, F_VZ), c_bm, bx, bz, sp.vz, zp, own) : zero;
+        }
+        const C vz_zm = __shfl_up_sync(full, vzn, 1);
+        const C vx_zp = __shfl_down_sync(full, vxc, 1);
+        const C sax = r_sub(vxn, vxc), saz = r_sub(vzn, vz_zm);
+        const C sbz = r_sub(vx_zp, vxc), sbx = r_sub(vzn, vzp);
+        C txx, tzz, txz;
+        if (fast || (zin && e_inside(a, X, Z))) {
+            txx = r_add(c_txx, r_fma(l2m, sax, r_mul(la, saz)));
+            tzz = r_add(c_tzz, r_fma(l2m, saz, r_mul(la, sax)));
+            txz = r_fma(mu, r_add(sbz, sbx), c_txz);
+        } else if (zin) {
+            const long long cc = sb + e_pml_index(a, X, Z);
+            const C Axh = pr[P.axh() + X], Bxh = pr[P.bxh() + X];
+            txx = e_frame<S, C>(a, F_TXX, cc, Axh, Bxh, zp.An, zp.Bn, sp.t[0], sp.t[1], l2m, la,
+                                sax, saz, own);
+            tzz = e_frame<S, C>(a, F_TZZ, cc, Axh, Bxh, zp.An, zp.Bn, sp.t[2], sp.t[3], la, l2m,
+                                sax, saz, own);
+            txz = e_frame<S, C>(a, F_TXZ, cc, pr[P.axn() + X], pr[P.bxn() + X], zp.Ah, zp.Bh,
+                                sp.t[4], sp.t[5], mu, mu, sbx, sbz, own);
+        } else {
+            txx = tzz = txz = zero;
+        }
         if (own) {
             if (X + 1 < a.NX) St::st(vxo + q + a.pitch, vxn, a.sc[F_VX]);
             St::st(vzo + q, vzn, a.sc[F_VZ]);
@@ -714,14 +912,13 @@ struct sm_eiso {
     void *mat(int k) const { return static_cast<char *>(matbuf.p) + (size_t)k * mat_stride; }
     size_t fset_stride = 0, mat_stride = 0;   // bytes between consecutive arrays
     int cur = 0;
-    int chunk = 0;   // rows per warp march (0: chosen from the grid size)
-    int config = 5;  // index into kEisoConfigs (tile 8 x 32: fastest on B200 for
-                     // 64 x 1040 x 540 FP32/FP16 and 440 x 440 single shots)
-    DevBuf err;      // bounded-wait failure flag of the tiled kernel
+    int config = 0;  // index into kEisoConfigs (slab 2 x 8 with materials from L2:
+                     // the fastest on B200 for batches of 1040 x 540 shots)
+    DevBuf err;      // bounded-wait failure flag of the step kernels
     EisoMaps maps[2];            // TMA maps of each buffer set (tile kernel)
     int maps_key = -1;           // (TX, TZ) the maps were built for
-    EisoBandMaps band_maps[2];   // TMA maps of each buffer set (band kernel)
-    bool band_maps_ok = false;
+    EisoSlabMaps slab_maps[2];   // TMA maps of each buffer set (slab kernels)
+    int slab_key = -1;           // box shape the slab maps were built for
     DevBuf d_step;               // device step counter (EisoArgs::step)
     // CUDA graphs of graph_steps steps, one per parity of the starting
     // buffer set; captured again when graph_epoch moved since (new sources,
@@ -780,17 +977,19 @@ void eiso_bind(sm_eiso *h) {
     }
 }
 
-// launch configurations of the step kernel.
-//   tile (kind 0): p = {TX, TZ, threads, min CTAs per SM}
-//   band (kind 1): p = {warps per CTA, ring depth D, min CTAs per SM, -}
+// launch configurations of the step kernel (an index into this table):
+//   slab, materials from global (kind 0): p = {warps per CTA, rows TX, min CTAs per SM}
+//   tile (kind 1): p = {TX, TZ, threads, min CTAs per SM}
+//   slab, materials by TMA (kind 2): p = {warps per CTA, rows TX, min CTAs per SM}
 // The minimum resident CTAs per SM caps the registers a thread may use.
 struct EisoConfig {
     int kind;
     int p[4];
 };
 static const EisoConfig kEisoConfigs[] = {
-    {1, {4, 4, 8, 0}}, {1, {4, 8, 4, 0}}, {1, {2, 8, 8, 0}},     {1, {8, 4, 3, 0}},
-    {1, {2, 4, 16, 0}}, {0, {8, 32, 128, 6}}, {0, {16, 64, 256, 2}}, {0, {8, 64, 256, 3}}};
+    {0, {2, 8, 8, 0}},  {0, {2, 4, 12, 0}},   {0, {4, 4, 6, 0}},    {0, {1, 8, 16, 0}},
+    {0, {4, 8, 4, 0}},  {0, {2, 16, 4, 0}},   {1, {8, 32, 128, 6}}, {1, {16, 64, 256, 2}},
+    {1, {8, 64, 256, 3}}, {2, {2, 8, 8, 0}},  {2, {4, 8, 4, 0}},    {2, {1, 16, 12, 0}}};
 static const int kEisoNumConfigs = sizeof(kEisoConfigs) / sizeof(kEisoConfigs[0]);
 
 template <typename S, int TX, int TZ>
@@ -807,27 +1006,29 @@ int eiso_make_tile_maps(sm_eiso *h) {
     return SM_OK;
 }
 
-template <typename S>
-int eiso_make_band_maps(sm_eiso *h) {
-    using L = EBand<S>;
+// TMA maps of the slab kernels: the five wavefields of a set as one 4-D
+// tensor (z, x, shot, field) and the materials as one 3-D tensor (z, x,
+// material), boxes of L's shape
+template <typename S, typename L, int KEY>
+int eiso_make_slab_maps(sm_eiso *h) {
     using C = typename Store<S>::C;
-    if (h->band_maps_ok) return SM_OK;
+    if (h->slab_key == KEY) return SM_OK;
     const size_t e = sizeof(S), c = sizeof(C), row = (size_t)h->pitch;
     const size_t fdims[4] = {(size_t)h->NZ, (size_t)h->NX, h->nshots, 5};
     const size_t fstr[3] = {row * e, h->NX * row * e, h->fset_stride};
-    const unsigned fbox[4] = {(unsigned)L::BW, 1, 1, 5};
+    const unsigned fbox[4] = {(unsigned)L::BW, (unsigned)L::RX, 1, 5};
     const size_t mdims[3] = {(size_t)h->NZ, (size_t)h->NX, 5};
     const size_t mstr[2] = {row * c, h->mat_stride};
-    const unsigned mbox[3] = {(unsigned)L::BWC, 1, 5};
+    const unsigned mbox[3] = {(unsigned)L::BWC, (unsigned)L::RX, 5};
     for (int b = 0; b < 2; ++b) {
-        if (int rc = make_map_nd(&h->band_maps[b].f, h->fset[b].p, MapType<S>::v, e, 4, fdims,
+        if (int rc = make_map_nd(&h->slab_maps[b].f, h->fset[b].p, MapType<S>::v, e, 4, fdims,
                                  fstr, fbox))
             return rc;
-        if (int rc = make_map_nd(&h->band_maps[b].m, h->matbuf.p, MapType<C>::v, c, 3, mdims, mstr,
+        if (int rc = make_map_nd(&h->slab_maps[b].m, h->matbuf.p, MapType<C>::v, c, 3, mdims, mstr,
                                  mbox))
             return rc;
     }
-    h->band_maps_ok = true;
+    h->slab_key = KEY;
     return SM_OK;
 }
 
@@ -852,12 +1053,6 @@ int ready_tile_cfg(sm_eiso *h) {
     return allow_smem(eiso_tile_kernel<S, TX, TZ, NT, MINB>, ETile<S, TX, TZ>::bytes, h->device);
 }
 
-template <typename S, int W, int D, int MINB>
-int ready_band_cfg(sm_eiso *h) {
-    if (int rc = eiso_make_band_maps<S>(h)) return rc;
-    return allow_smem(eiso_band_kernel<S, W, D, MINB>, W * EBand<S>::warp_bytes(D), h->device);
-}
-
 template <typename S, int TX, int TZ, int NT, int MINB>
 int launch_tile_cfg(sm_eiso *h) {
     using L = ETile<S, TX, TZ>;
@@ -867,25 +1062,53 @@ int launch_tile_cfg(sm_eiso *h) {
     return SM_OK;
 }
 
-template <typename S, int W, int D, int MINB>
-int launch_band_cfg(sm_eiso *h) {
-    using L = EBand<S>;
-    const size_t bytes = W * L::warp_bytes(D);
+template <typename S, int W, int TX, int MINB>
+int ready_slab_cfg(sm_eiso *h) {
+    if (int rc = eiso_make_slab_maps<S, ESlab<S, W, TX>, W * 4096 + TX>(h)) return rc;
+    return allow_smem(eiso_slab_kernel<S, W, TX, MINB>, ESlab<S, W, TX>::bytes, h->device);
+}
+
+template <typename S, int W, int TX, int MINB>
+int launch_slab_cfg(sm_eiso *h) {
+    using L = ESlab<S, W, TX>;
     const int wz = (h->NZ + 29) / 30;
-    dim3 grd((wz + W - 1) / W, (h->NX + h->args.chunk - 1) / h->args.chunk, (unsigned)h->nshots);
-    eiso_band_kernel<S, W, D, MINB><<<grd, 32 * W, bytes, h->stream>>>(h->args,
-                                                                      h->band_maps[h->cur]);
+    dim3 grd((wz + W - 1) / W, (h->NX + TX - 1) / TX, (unsigned)h->nshots);
+    eiso_slab_kernel<S, W, TX, MINB><<<grd, 32 * W, L::bytes, h->stream>>>(h->args,
+                                                                          h->slab_maps[h->cur]);
+    return SM_OK;
+}
+
+template <typename S, int W, int TX, int MINB>
+int ready_slabg_cfg(sm_eiso *h) {
+    if (int rc = eiso_make_slab_maps<S, ESlabG<S, W, TX>, (1 << 20) + W * 4096 + TX>(h)) return rc;
+    return allow_smem(eiso_slabg_kernel<S, W, TX, MINB>, ESlabG<S, W, TX>::bytes, h->device);
+}
+
+template <typename S, int W, int TX, int MINB>
+int launch_slabg_cfg(sm_eiso *h) {
+    const int wz = (h->NZ + 29) / 30;
+    dim3 grd((wz + W - 1) / W, (h->NX + TX - 1) / TX, (unsigned)h->nshots);
+    eiso_slabg_kernel<S, W, TX, MINB><<<grd, 32 * W, ESlabG<S, W, TX>::bytes, h->stream>>>(
+        h->args, h->slab_maps[h->cur]);
     return SM_OK;
 }
 
 template <typename S>
 size_t eiso_config_smem(int config) {
-    const EisoConfig &k = kEisoConfigs[config];
-    if (k.kind == 1) return k.p[0] * EBand<S>::warp_bytes(k.p[1]);
-    if (k.p[0] == 8 && k.p[1] == 32) return ETile<S, 8, 32>::bytes;
-    if (k.p[0] == 16 && k.p[1] == 64) return ETile<S, 16, 64>::bytes;
-    if (k.p[0] == 8 && k.p[1] == 64) return ETile<S, 8, 64>::bytes;
-    return 0;
+    switch (config) {
+    case 0: return ESlabG<S, 2, 8>::bytes;
+    case 1: return ESlabG<S, 2, 4>::bytes;
+    case 2: return ESlabG<S, 4, 4>::bytes;
+    case 3: return ESlabG<S, 1, 8>::bytes;
+    case 4: return ESlabG<S, 4, 8>::bytes;
+    case 5: return ESlabG<S, 2, 16>::bytes;
+    case 6: return ETile<S, 8, 32>::bytes;
+    case 7: return ETile<S, 16, 64>::bytes;
+    case 8: return ETile<S, 8, 64>::bytes;
+    case 9: return ESlab<S, 2, 8>::bytes;
+    case 10: return ESlab<S, 4, 8>::bytes;
+    default: return ESlab<S, 1, 16>::bytes;
+    }
 }
 
 size_t eiso_config_smem_prec(int precision, int config) {
@@ -897,50 +1120,43 @@ size_t eiso_config_smem_prec(int precision, int config) {
     }
 }
 
-// rows per warp march of the band kernel: long enough that the rows
-// re-read at each chunk start stay cheap, short enough for about three
-// waves of 32 warps per SM (the last wave's tail stays small)
-int eiso_pick_chunk(const sm_eiso *h) {
-    if (h->chunk > 0) return h->chunk;
-    const int sms = h->sms;
-    const long long wz = (h->NZ + 29) / 30;
-    const long long want = (long long)sms * 96;
-    long long per = wz * (long long)h->nshots;                 // warps per row band
-    long long bands = (want + per - 1) / per;                  // row bands wanted
-    long long c = (h->NX + bands - 1) / std::max<long long>(bands, 1);
-    return (int)std::min<long long>(std::max<long long>(c, 8), 512);
-}
-
 // TMA maps and shared-memory limits of the current configuration (kept out
 // of stream capture)
 template <typename S>
 int eiso_ready(sm_eiso *h) {
     switch (h->config) {
-    case 0: return ready_band_cfg<S, 4, 4, 8>(h);
-    case 1: return ready_band_cfg<S, 4, 8, 4>(h);
-    case 2: return ready_band_cfg<S, 2, 8, 8>(h);
-    case 3: return ready_band_cfg<S, 8, 4, 3>(h);
-    case 4: return ready_band_cfg<S, 2, 4, 16>(h);
-    case 5: return ready_tile_cfg<S, 8, 32, 128, 6>(h);
-    case 6: return ready_tile_cfg<S, 16, 64, 256, 2>(h);
-    default: return ready_tile_cfg<S, 8, 64, 256, 3>(h);
+    case 0: return ready_slabg_cfg<S, 2, 8, 8>(h);
+    case 1: return ready_slabg_cfg<S, 2, 4, 12>(h);
+    case 2: return ready_slabg_cfg<S, 4, 4, 6>(h);
+    case 3: return ready_slabg_cfg<S, 1, 8, 16>(h);
+    case 4: return ready_slabg_cfg<S, 4, 8, 4>(h);
+    case 5: return ready_slabg_cfg<S, 2, 16, 4>(h);
+    case 6: return ready_tile_cfg<S, 8, 32, 128, 6>(h);
+    case 7: return ready_tile_cfg<S, 16, 64, 256, 2>(h);
+    case 8: return ready_tile_cfg<S, 8, 64, 256, 3>(h);
+    case 9: return ready_slab_cfg<S, 2, 8, 8>(h);
+    case 10: return ready_slab_cfg<S, 4, 8, 4>(h);
+    default: return ready_slab_cfg<S, 1, 16, 12>(h);
     }
 }
 
 template <typename S>
 int launch_step(sm_eiso *h) {
-    h->args.chunk = eiso_pick_chunk(h);
     cudaEvent_t t0 = h->timer.begin(h->stream);
     int rc = SM_OK;
     switch (h->config) {
-    case 0: rc = launch_band_cfg<S, 4, 4, 8>(h); break;
-    case 1: rc = launch_band_cfg<S, 4, 8, 4>(h); break;
-    case 2: rc = launch_band_cfg<S, 2, 8, 8>(h); break;
-    case 3: rc = launch_band_cfg<S, 8, 4, 3>(h); break;
-    case 4: rc = launch_band_cfg<S, 2, 4, 16>(h); break;
-    case 5: rc = launch_tile_cfg<S, 8, 32, 128, 6>(h); break;
-    case 6: rc = launch_tile_cfg<S, 16, 64, 256, 2>(h); break;
-    default: rc = launch_tile_cfg<S, 8, 64, 256, 3>(h); break;
+    case 0: rc = launch_slabg_cfg<S, 2, 8, 8>(h); break;
+    case 1: rc = launch_slabg_cfg<S, 2, 4, 12>(h); break;
+    case 2: rc = launch_slabg_cfg<S, 4, 4, 6>(h); break;
+    case 3: rc = launch_slabg_cfg<S, 1, 8, 16>(h); break;
+    case 4: rc = launch_slabg_cfg<S, 4, 8, 4>(h); break;
+    case 5: rc = launch_slabg_cfg<S, 2, 16, 4>(h); break;
+    case 6: rc = launch_tile_cfg<S, 8, 32, 128, 6>(h); break;
+    case 7: rc = launch_tile_cfg<S, 16, 64, 256, 2>(h); break;
+    case 8: rc = launch_tile_cfg<S, 8, 64, 256, 3>(h); break;
+    case 9: rc = launch_slab_cfg<S, 2, 8, 8>(h); break;
+    case 10: rc = launch_slab_cfg<S, 4, 8, 4>(h); break;
+    default: rc = launch_slab_cfg<S, 1, 16, 12>(h); break;
     }
     if (rc) return rc;
     h->timer.end(t0, h->stream);
@@ -1271,6 +1487,7 @@ extern "C" int sm_eiso_create(int device, size_t nx, size_t nz, size_t npml, dou
     EisoArgs &a = h->args;
     a.NX = (int)NX; a.NZ = (int)NZ; a.pitch = h->pitch;
     a.np = (int)npml; a.nx = (int)nx; a.nz = (int)nz;
+    a.nshots = (int)nshots;
     a.fstride = (long long)fcells;
     a.sstride = (long long)h->npml_cells;
     a.mid_off = (int)(npml * NZ);
@@ -1518,10 +1735,10 @@ extern "C" int sm_eiso_run(sm_eiso_t h, size_t nsteps) {
 }
 
 // Launch-configuration search: every configuration that fits the device
-// (and, for the band kernel, a few march lengths) runs trial_steps steps from
+// runs trial_steps steps from
 // a zero state, timed with CUDA events; the fastest is kept.  Results are
 // cached per (precision, grid, shots) for the life of the process.
-extern "C" int sm_eiso_autotune(sm_eiso_t h, int trial_steps, int *config, int *chunk,
+extern "C" int sm_eiso_autotune(sm_eiso_t h, int trial_steps, int *config,
                                 double *ms_per_step) {
     if (int rc = eiso_check(h)) return rc;
     if (h->it != 0)
@@ -1538,7 +1755,7 @@ extern "C" int sm_eiso_autotune(sm_eiso_t h, int trial_steps, int *config, int *
         }
     };
     struct Val {
-        int config, chunk;
+        int config;
         double ms;
     };
     static std::map<Key, Val> cache;
@@ -1549,10 +1766,8 @@ extern "C" int sm_eiso_autotune(sm_eiso_t h, int trial_steps, int *config, int *
         auto it = cache.find(key);
         if (it != cache.end()) {
             h->config = it->second.config;
-            h->chunk = it->second.chunk;
             h->graph_epoch++;
             if (config) *config = h->config;
-            if (chunk) *chunk = h->chunk;
             if (ms_per_step) *ms_per_step = it->second.ms;
             return SM_OK;
         }
@@ -1564,27 +1779,22 @@ extern "C" int sm_eiso_autotune(sm_eiso_t h, int trial_steps, int *config, int *
     SM_CUDA_TRY(cudaEventCreate(&e1));
     const bool timing = h->timer.on;
     h->timer.on = false;
-    Val best{-1, 0, 0.0};
+    Val best{-1, 0.0};
     int rc = SM_OK;
     for (int c = 0; c < kEisoNumConfigs && rc == SM_OK; ++c) {
         if (eiso_config_smem_prec(h->precision, c) > (size_t)lim) continue;
-        std::vector<int> chunks{0};
-        if (kEisoConfigs[c].kind == 1) chunks = {0, 16, 32, 64};
-        for (int ch : chunks) {
-            h->config = c;
-            h->chunk = ch;
-            h->graph_epoch++;
-            if ((rc = sm_eiso_reset(h))) break;
-            if ((rc = sm_eiso_run(h, 2))) break;
-            cudaEventRecord(e0, h->stream);
-            if ((rc = sm_eiso_run(h, (size_t)trial_steps))) break;
-            cudaEventRecord(e1, h->stream);
-            if ((rc = sm_eiso_sync(h))) break;
-            float t = 0.f;
-            cudaEventElapsedTime(&t, e0, e1);
-            const double ms = t / trial_steps;
-            if (best.config < 0 || ms < best.ms) best = Val{c, ch, ms};
-        }
+        h->config = c;
+        h->graph_epoch++;
+        if ((rc = sm_eiso_reset(h))) break;
+        if ((rc = sm_eiso_run(h, 2))) break;
+        cudaEventRecord(e0, h->stream);
+        if ((rc = sm_eiso_run(h, (size_t)trial_steps))) break;
+        cudaEventRecord(e1, h->stream);
+        if ((rc = sm_eiso_sync(h))) break;
+        float t = 0.f;
+        cudaEventElapsedTime(&t, e0, e1);
+        const double ms = t / trial_steps;
+        if (best.config < 0 || ms < best.ms) best = Val{c, ms};
     }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
@@ -1592,7 +1802,6 @@ extern "C" int sm_eiso_autotune(sm_eiso_t h, int trial_steps, int *config, int *
     if (rc) return rc;
     if (best.config < 0) return sm_fail(SM_EINVAL, "sm_eiso_autotune: no configuration fits");
     h->config = best.config;
-    h->chunk = best.chunk;
     h->graph_epoch++;
     if ((rc = sm_eiso_reset(h))) return rc;
     {
@@ -1600,7 +1809,6 @@ extern "C" int sm_eiso_autotune(sm_eiso_t h, int trial_steps, int *config, int *
         cache[key] = best;
     }
     if (config) *config = best.config;
-    if (chunk) *chunk = best.chunk;
     if (ms_per_step) *ms_per_step = best.ms;
     return SM_OK;
 }
@@ -1748,15 +1956,6 @@ extern "C" int sm_eiso_stream(sm_eiso_t h, void **stream) {
     return SM_OK;
 }
 
-extern "C" int sm_eiso_set_chunk(sm_eiso_t h, int chunk) {
-    if (int rc = eiso_check(h)) return rc;
-    if (chunk < 0 || chunk > (1 << 20))
-        return sm_fail(SM_EINVAL, "sm_eiso_set_chunk: chunk %d out of range", chunk);
-    h->chunk = chunk;
-    h->graph_epoch++;
-    return SM_OK;
-}
-
 extern "C" int sm_eiso_set_config(sm_eiso_t h, int config) {
     if (int rc = eiso_check(h)) return rc;
     if (config < 0 || config >= kEisoNumConfigs)
@@ -1780,13 +1979,6 @@ extern "C" int sm_eiso_get_config(sm_eiso_t h, int *config, int *nconfigs) {
     if (int rc = eiso_check(h)) return rc;
     if (config) *config = h->config;
     if (nconfigs) *nconfigs = kEisoNumConfigs;
-    return SM_OK;
-}
-
-extern "C" int sm_eiso_get_chunk(sm_eiso_t h, int *chunk) {
-    if (int rc = eiso_check(h)) return rc;
-    if (!chunk) return sm_fail(SM_EINVAL, "sm_eiso_get_chunk: NULL");
-    *chunk = eiso_pick_chunk(h);
     return SM_OK;
 }
 
@@ -2024,7 +2216,6 @@ extern "C" int sm_eiso_run_noalloc(int device, void *stream, const sm_eiso_reque
     a.sstride = (long long)pml;
     a.mid_off = (int)(np * NZ);
     a.right_off = (int)(np * NZ + nx * 2 * np);
-    a.chunk = 1;
     for (int f = 0; f < 5; ++f) {
         a.mat[f] = base + o_mat + f * fcells * sizeof(S);
         a.sc[f] = a.isc[f] = 1.0f;

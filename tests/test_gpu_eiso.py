@@ -97,14 +97,10 @@ def test_cfg0_full_size_against_oracle(precision):
     assert H.rel_l2([1e3 * g for g in got], orc) < TOL[precision]
 
 
-def _state_after(nx, nz, P, precision, steps, config=None, chunk=None):
+def _state_after(nx, nz, P, precision, steps, config=None):
     orc, dev = _pair(nx, nz, P, 7, precision)
     if config is not None:
         dev.set_config(config)
-    if chunk is not None:
-        dev.set_chunk(chunk)
-        if chunk:
-            assert dev.get_chunk() == chunk
     dev.run(steps)
     got = {(f, part): dev.get_field(f, part=part) for f in FIELDS for part in ("total", "x", "z")}
     nconf = dev.get_config()[1]
@@ -114,8 +110,9 @@ def _state_after(nx, nz, P, precision, steps, config=None, chunk=None):
 
 @pytest.mark.parametrize("precision", ["fp64", "fp32"])
 def test_every_launch_config_gives_identical_results(precision):
-    """Band and tile variants of the step kernel and the band kernel's chunk
-    length must not show in the results: halo cells are recomputed bitwise."""
+    """The step kernel's variants (tiles, slabs with materials from L2 or in
+    the TMA box, every shape) must not show in the results: halo cells are
+    recomputed bitwise by neighbours."""
     nx, nz, P = 70, 95, 5       # NZ = 105: ragged against every tile width
     orc, ref, nconf = _state_after(nx, nz, P, precision, 6)
     for _ in range(6):
@@ -127,11 +124,25 @@ def test_every_launch_config_gives_identical_results(precision):
         _, got, _ = _state_after(nx, nz, P, precision, 6, config=config)
         for k, a in got.items():
             np.testing.assert_array_equal(a, ref[k], err_msg=f"config {config} {k}")
-    # the band kernel (config 0) with its chunk lengths
-    for chunk in (1, 2, 5, 17, 200):
-        _, got, _ = _state_after(nx, nz, P, precision, 6, config=0, chunk=chunk)
-        for k, a in got.items():
-            np.testing.assert_array_equal(a, ref[k], err_msg=f"chunk {chunk} {k}")
+
+
+def test_every_launch_config_batched_shots_identical():
+    """Kernels that take several shots per CTA (and every other variant)
+    must give each shot of a batch the same bits, including a last group
+    with fewer shots than the CTA holds."""
+    p = W.cfg2(nx=150, nz=130, npml=9, nsteps=90, nshots=5, nrec=12)
+    dev, n = api.eiso_device(p, "fp32")
+    nconf = dev.get_config()[1]
+    dev.run(n)
+    ref = [dev.traces(s) for s in range(5)]
+    for config in range(nconf):
+        dev.reset()
+        dev.set_config(config)
+        dev.run(n)
+        for s in range(5):
+            for x, y in zip(dev.traces(s), ref[s]):
+                np.testing.assert_array_equal(x, y, err_msg=f"config {config} shot {s}")
+    dev.close()
 
 
 def test_batched_shots_equal_single_shots():
