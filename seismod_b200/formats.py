@@ -16,6 +16,8 @@ The formats are the ones the reference programs read and write:
                    t0 (s) / dt (ms)`` (io_utils.c:1592-1741).
 * trace file       ``trc/<base>/<base>_<n>.trc``: ``"%le    %le"`` of time
                    and 1e3 * velocity (io_utils.c:1744-1768).
+* binary model     this package's own: the same model values without text
+                   parsing (write_model_bin); the drop-in programs read either.
 """
 from __future__ import annotations
 
@@ -126,3 +128,25 @@ def read_traces(workdir, basename, nrec):
         ts.append(t)
         vs.append(v)
     return ts, vs
+
+
+def write_model_bin(path, fields, d, origin):
+    """Binary model file read by the drop-in programs in place of the ASCII
+    model: "SEISMODB", uint32 version 1, ndim, nfields, 0; uint64 nx ny nz;
+    float64 dx dy dz x0 y0 z0; the fields' float64 values, index
+    (i*ny + j)*nz + k (host byte order).  fields: [vp, vs, rho] of shape
+    (nx, nz) for e_iso, [vp, rho] of shape (nx, ny, nz) for a_iso_3d; d and
+    origin have 2 or 3 entries to match."""
+    arrs = [np.ascontiguousarray(f, dtype=np.float64) for f in fields]
+    shape = arrs[0].shape
+    ndim = len(shape)
+    n3 = (shape[0], 1, shape[1]) if ndim == 2 else shape
+    d3 = (d[0], 1.0, d[1]) if ndim == 2 else tuple(d)
+    o3 = (origin[0], 0.0, origin[1]) if ndim == 2 else tuple(origin)
+    with open(path, "wb") as f:
+        f.write(b"SEISMODB")
+        f.write(np.array([1, ndim, len(arrs), 0], dtype=np.uint32).tobytes())
+        f.write(np.array(n3, dtype=np.uint64).tobytes())
+        f.write(np.array(d3 + o3, dtype=np.float64).tobytes())
+        for a in arrs:
+            f.write(a.tobytes())

@@ -216,7 +216,6 @@ int sm_a_iso_3d_main(int argc, char **argv)
     if (p.verbose) fprintf(stdout, "\n *** a_iso_3d - Acoustic wave propagation in 3D isotropic media (GPU) ***\n\n");
     if ((rc = sm_read_model_a(p.modelfile, &g, &vp, &rho))) goto out;
     if (g.dx != g.dz) { rc = sm_fail(SM_EINVAL, "grid cell size must be equal in X and Z"); goto out; }
-    if (p.segy) { rc = sm_fail(SM_EINVAL, "SEG-Y output (segy 1) is not supported; use segy 0"); goto out; }
     const size_t np = p.np, nx2 = g.nx + 2 * np, ny2 = g.ny + 2 * np, nz2 = g.nz + 2 * np;
     const size_t n3 = nx2 * ny2 * nz2;
     const double dt = p.dt;
@@ -290,7 +289,22 @@ int sm_a_iso_3d_main(int argc, char **argv)
     for (size_t r = 0; r < rp.n; ++r) ld = counts[r] > ld ? counts[r] : ld;
     vals = malloc(rp.n * ld * sizeof(double) + 1);
     if ((rc = sm_a3d_read_traces(h, 0, rp.n, vals, ld, counts))) goto out;
-    rc = write_traces(p.basename, &rp, vals, ld, counts, dt, nsteps);
+    if (p.segy) {   /* save_segy, io_utils.c:3269-3559 */
+        sm_record *tr = malloc((rp.n ? rp.n : 1) * sizeof(sm_record));
+        double *tt = malloc(rp.n * ld * sizeof(double) + 1);
+        if (!tr || !tt) { free(tr); free(tt); rc = sm_fail(SM_ENOMEM, "out of host memory"); goto out; }
+        for (size_t r = 0; r < rp.n; ++r) {   /* sample times: t = dt (it + 1), a_iso_3d.c:595 */
+            tr[r] = rec[rp.recno[r]];
+            size_t s = 0;
+            for (size_t it = 0; it < nsteps && s < counts[r]; ++it)
+                if (sm_sample_predicate(it, dt, rp.t0[r], rp.rdt[r])) tt[r * ld + s++] = dt * (it + 1);
+        }
+        rc = sm_write_segy(p.basename, &p, tr, rp.n, nsrc ? &src[0] : NULL, vals, tt, ld, counts);
+        free(tr);
+        free(tt);
+    } else {
+        rc = write_traces(p.basename, &rp, vals, ld, counts, dt, nsteps);
+    }
     if (p.verbose) fprintf(stdout, "\nEnd of computation\n");
 out:
     sm_a3d_destroy(h);

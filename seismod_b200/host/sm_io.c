@@ -16,6 +16,8 @@
 #include <string.h>
 #include <sys/stat.h>
 #include <sys/types.h>
+#include <stdint.h>
+#include <time.h>
 
 void sm_params_defaults(sm_params *p)
 {
@@ -28,6 +30,7 @@ void sm_params_defaults(sm_params *p)
     p->np = 20;
     p->segy = 0;
     p->shotpt_no = 1;
+    p->simulate_cmp = 0;
     p->Rc = 1.e-5;
     p->kappa_max = 1.;
     p->alpha_max = 1;
@@ -103,19 +106,91 @@ int sm_read_par(const char *path, sm_params *p)
         else if (!strcmp(keyword, "nl")) p->np = (size_t)atoi(value);
         else if (!strcmp(keyword, "segy")) p->segy = (short)atoi(value);
         else if (!strcmp(keyword, "shotpoint")) p->shotpt_no = atoi(value);
+        else if (!strcmp(keyword, "simulateCMP")) p->simulate_cmp = atoi(value);
         else if (!strcmp(keyword, "Rc")) p->Rc = strtod(value, NULL);
         else if (!strcmp(keyword, "kappa_max")) p->kappa_max = strtod(value, NULL);
         else if (!strcmp(keyword, "alpha_max")) p->alpha_max = (short)atoi(value);
         /* plstr, check_model, chkpt_inc, pml_median, saveEnergy, EnergyROI,
-         * simulateCMP, azimuthal_mode: accepted, unused by these programs */
+         * azimuthal_mode: accepted, unused by these programs */
     }
     fclose(fid);
     if (p->iwipe == 0) p->np = 0;   /* io_utils.c:293 */
     return SM_OK;
 }
 
+/* Binary model files (no counterpart in the reference, whose ASCII models
+ * take minutes to parse at 512^3): the 8 bytes "SEISMODB", then uint32
+ * version (1), ndim (2 or 3), nfields (3: vp vs rho for e_iso, 2: vp rho for
+ * a_iso_3d), reserved (0); uint64 nx ny nz (ny = 1 in 2-D); float64 dx dy dz
+ * x0 y0 z0; then each field's nx*ny*nz float64 values in the ASCII files'
+ * order (index (i*ny + j)*nz + k).  All in the host's byte order. */
+static const char kModelMagic[8] = {'S', 'E', 'I', 'S', 'M', 'O', 'D', 'B'};
+
+static int model_is_binary(const char *path)
+{
+    FILE *f = fopen(path, "rb");
+    if (!f) return 0;
+    char m[8];
+    const int yes = fread(m, 1, 8, f) == 8 && memcmp(m, kModelMagic, 8) == 0;
+    fclose(f);
+    return yes;
+}
+
+static int read_model_bin(const char *path, unsigned ndim, unsigned nfields, sm_grid *g,
+                          double **out)
+{
+    FILE *f = fopen(path, "rb");
+    if (!f) return sm_fail(SM_EIO, "cannot open %s for reading", path);
+    char m[8];
+    uint32_t hdr[4];
+    uint64_t n[3];
+    double d[6];
+    if (fread(m, 1, 8, f) != 8 || fread(hdr, 4, 4, f) != 4 || fread(n, 8, 3, f) != 3 ||
+        fread(d, 8, 6, f) != 6) {
+        fclose(f);
+        return sm_fail(SM_EIO, "%s: short binary model header", path);
+    }
+    if (hdr[0] != 1 || hdr[1] != ndim || hdr[2] != nfields) {
+        fclose(f);
+        return sm_fail(SM_EIO, "%s: binary model version %u, %u-D, %u fields; expected 1, %u-D, %u",
+                       path, hdr[0], hdr[1], hdr[2], ndim, nfields);
+    }
+    memset(g, 0, sizeof *g);
+    g->nx = n[0]; g->ny = n[1]; g->nz = n[2];
+    g->dx = d[0]; g->dy = d[1]; g->dz = d[2];
+    g->x0 = d[3]; g->y0 = d[4]; g->z0 = d[5];
+    if (!g->nx || !g->ny || !g->nz || (ndim == 2 && g->ny != 1)) {
+        fclose(f);
+        return sm_fail(SM_EIO, "%s: bad binary model dimensions", path);
+    }
+    const size_t cells = g->nx * g->ny * g->nz;
+    for (unsigned k = 0; k < nfields; ++k) out[k] = NULL;
+    for (unsigned k = 0; k < nfields; ++k) {
+        out[k] = malloc(cells * sizeof(double));
+        if (!out[k] || fread(out[k], sizeof(double), cells, f) != cells) {
+            for (unsigned j = 0; j <= k; ++j) { free(out[j]); out[j] = NULL; }
+            fclose(f);
+            return sm_fail(SM_EIO, "%s: binary model data too short", path);
+        }
+    }
+    fclose(f);
+    return SM_OK;
+}
+
 int sm_read_model_e(const char *path, sm_grid *g, double **pvp, double **pvs, double **prho)
 {
+    if (model_is_binary(path)) {
+        double *a[3];
+        int rc = read_model_bin(path, 2, 3, g, a);
+        if (rc) return rc;
+        if (g->nx < 2 || g->nz < 2) {
+            free(a[0]); free(a[1]); free(a[2]);
+            return sm_fail(SM_EIO, "%s: grid must be at least 2 x 2", path);
+        }
+        g->dy = 1.0;
+        *pvp = a[0]; *pvs = a[1]; *prho = a[2];
+        return SM_OK;
+    }
     /* io_utils.c:296-328 (grid) and 892-947 (values; one column = 1-D profile) */
     FILE *fid = fopen(path, "r");
     if (!fid) return sm_fail(SM_EIO, "cannot open %s for reading", path);
@@ -172,6 +247,13 @@ bad:
 
 int sm_read_model_a(const char *path, sm_grid *g, double **pvp, double **prho)
 {
+    if (model_is_binary(path)) {
+        double *a[2];
+        int rc = read_model_bin(path, 3, 2, g, a);
+        if (rc) return rc;
+        *pvp = a[0]; *prho = a[1];
+        return SM_OK;
+    }
     /* io_utils.c:384-401 (grid) and 1029-1094 (values; one (x,y) column is
      * a 1-D profile).  Returns the nx*ny*nz interior. */
     FILE *fid = fopen(path, "r");
@@ -399,5 +481,118 @@ int sm_write_trace_file(const char *base, size_t n, const double *t, const doubl
     if (!f) return sm_fail(SM_EIO, "cannot open %s for output (%s)", path, strerror(errno));
     for (size_t s = 0; s < ns; ++s) fprintf(f, "%le    %le\n", t[s], 1.e3 * v[s]);
     if (fclose(f) != 0) return sm_fail(SM_EIO, "write error on %s", path);
+    return SM_OK;
+}
+
+/* ---- SEG-Y (io_utils.c:3269-3559 layout) ---- */
+
+static int put(FILE *f, const void *p, size_t n) { return fwrite(p, 1, n, f) == n; }
+static int put16(FILE *f, int16_t v) { return put(f, &v, 2); }
+static int put32(FILE *f, int32_t v) { return put(f, &v, 4); }
+static int pad_to(FILE *f, long pos) {
+    long cur = ftell(f);
+    while (cur < pos) {
+        if (fputc(0, f) == EOF) return 0;
+        ++cur;
+    }
+    return 1;
+}
+
+static size_t segy_samples(const sm_params *p, double rdt)
+{
+    return (size_t)llround(p->duration / rdt) + 1;
+}
+
+int sm_write_segy(const char *base, const sm_params *p, const sm_record *rec, size_t ntr,
+                  const sm_source *src0, const double *v, const double *t, size_t ld,
+                  const size_t *count)
+{
+    char fname[600];
+    struct stat sb;
+    if (stat("segy", &sb) < 0 && errno == ENOENT) mkdir("segy", S_IRWXU);
+    snprintf(fname, sizeof fname, "segy/%s.sgy", base);
+    FILE *f = fopen(fname, "wb");
+    if (!f) return sm_fail(SM_EIO, "cannot open %s for output (%s)", fname, strerror(errno));
+    int ok = 1;
+    /* textual file header: blanks with 'C' in columns 1 of the first two cards */
+    char text[3200];
+    memset(text, ' ', sizeof text);
+    text[0] = 'C';
+    text[80] = 'C';
+    ok = ok && put(f, text, sizeof text);
+    /* binary file header (fields 1-26, then the revision block at 3500) */
+    int16_t dt_us = 0, ns0 = 0, fold = 0;
+    if (ntr) {
+        dt_us = (int16_t)(1000000 * rec[0].dt);
+        ns0 = (int16_t)segy_samples(p, rec[0].dt);
+    }
+    for (size_t r = 0; r < ntr; ++r) fold += rec[r].comp == SM_VZ;
+    if (fold == 0)
+        for (size_t r = 0; r < ntr; ++r) fold += rec[r].comp == SM_VY;
+    ok = ok && put32(f, 1) && put32(f, 1) && put32(f, 1);     /* job, line, reel */
+    ok = ok && put16(f, (int16_t)ntr) && put16(f, 0);          /* traces, aux traces */
+    ok = ok && put16(f, dt_us) && put16(f, dt_us);             /* sample interval (us) */
+    ok = ok && put16(f, ns0) && put16(f, ns0);                 /* samples per trace */
+    ok = ok && put16(f, 5);                                    /* IEEE float32 */
+    ok = ok && put16(f, fold) && put16(f, 1) && put16(f, 1);   /* fold, sorting, vertical sum */
+    for (int k = 14; k <= 23; ++k) ok = ok && put16(f, 0);
+    ok = ok && put16(f, 1) && put16(f, 1) && put16(f, 1);      /* amp. recovery, units, polarity */
+    ok = ok && pad_to(f, 3500);
+    ok = ok && put16(f, 1) && put16(f, 0) && put16(f, 0);      /* rev. 1, fixed-length flag, ext. hdrs */
+    ok = ok && pad_to(f, 3600);
+    time_t now = time(NULL);
+    struct tm *tm_now = gmtime(&now);
+    int32_t src_no = p->shotpt_no;
+    const double sx = src0 ? src0->x : 0.0, sz = src0 ? src0->z : 0.0;
+    for (size_t r = 0; r < ntr && ok; ++r) {
+        const sm_record *q = &rec[r];
+        const int32_t tr_no = (int32_t)(r + 1);
+        const long start = ftell(f);
+        ok = ok && put32(f, tr_no) && put32(f, tr_no) && put32(f, tr_no) && put32(f, tr_no);
+        ok = ok && put32(f, src_no) && put32(f, 1) && put32(f, tr_no);
+        if (p->simulate_cmp) src_no++;
+        int16_t code = 1;
+        if (q->comp == SM_VZ) code = 12;
+        else if (q->comp == SM_VY) code = 13;
+        else if (q->comp == SM_VX) code = 14;
+        else if (q->comp == SM_P) code = 11;
+        ok = ok && put16(f, code) && put16(f, 1) && put16(f, 1) && put16(f, 1);
+        const int32_t offset = (int32_t)(q->x - sx);
+        ok = ok && put32(f, offset) && put32(f, (int32_t)(-q->z)) && put32(f, 0) &&
+             put32(f, (int32_t)(sz - 0));
+        for (int k = 0; k < 4; ++k) ok = ok && put32(f, 0);
+        ok = ok && put16(f, 1) && put16(f, 1);
+        ok = ok && put32(f, p->simulate_cmp ? -offset / 2 : (int32_t)sx) && put32(f, 0);
+        ok = ok && put32(f, p->simulate_cmp ? offset / 2 : (int32_t)q->x) && put32(f, 0);
+        ok = ok && put16(f, 1) && put16(f, 500) && put16(f, 500);
+        for (int k = 0; k < 10; ++k) ok = ok && put16(f, 0);
+        const size_t ns = segy_samples(p, q->dt);
+        ok = ok && put16(f, (int16_t)ns) && put16(f, (int16_t)(1000000 * q->dt));
+        ok = ok && put16(f, 1) && put16(f, 1) && put16(f, 1);
+        for (int k = 0; k < 16; ++k) ok = ok && put16(f, 0);
+        ok = ok && put16(f, (int16_t)(1900 + tm_now->tm_year)) && put16(f, (int16_t)tm_now->tm_yday) &&
+             put16(f, (int16_t)tm_now->tm_hour) && put16(f, (int16_t)tm_now->tm_min) &&
+             put16(f, (int16_t)tm_now->tm_sec) && put16(f, 2);
+        for (int k = 0; k < 5; ++k) ok = ok && put16(f, 0);
+        ok = ok && put16(f, 2);
+        ok = ok && put32(f, offset);
+        for (int k = 0; k < 4; ++k) ok = ok && put32(f, 0);
+        ok = ok && put16(f, 1) && put16(f, 6) && put32(f, 1) && put16(f, 0) && put16(f, 6) &&
+             put16(f, 0) && put16(f, 1) && put16(f, 4);
+        ok = ok && pad_to(f, start + 240);
+        float *data = calloc(ns, sizeof(float));
+        if (!data) {
+            fclose(f);
+            return sm_fail(SM_ENOMEM, "out of host memory");
+        }
+        for (size_t k = 0; k < count[r]; ++k) {
+            const size_t i = (size_t)llround(t[r * ld + k] / q->dt);
+            if (i < ns) data[i] = (float)v[r * ld + k];
+        }
+        ok = ok && put(f, data, ns * sizeof(float));
+        free(data);
+    }
+    if (fclose(f) != 0) ok = 0;
+    if (!ok) return sm_fail(SM_EIO, "write error on %s", fname);
     return SM_OK;
 }

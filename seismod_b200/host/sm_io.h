@@ -22,7 +22,7 @@ typedef struct {
     char modelfile[256], sourcefile[256], outputfile[256], basename[256];
     int iwipe;           /* "abs" */
     size_t np;           /* "nl" */
-    int segy, shotpt_no;
+    int segy, shotpt_no, simulate_cmp;
     double Rc, kappa_max, vmax, pml_order;
     int alpha_max;
     int verbose;
@@ -54,7 +54,9 @@ int sm_parse_args(int argc, char **argv, sm_params *p, const char *prog);
 int sm_read_par(const char *path, sm_params *p);
 /* model files: e_iso (io_utils.c:296-328, 892-947) and a_iso_3d
  * (io_utils.c:384-401, 1029-1153, interior values only: padding is done by
- * sm_a3d_pad_model).  Arrays are malloc'ed; the caller frees them. */
+ * sm_a3d_pad_model).  A file that starts with "SEISMODB" is read as a binary
+ * model instead (layout in sm_io.c).  Arrays are malloc'ed; the caller frees
+ * them. */
 int sm_read_model_e(const char *path, sm_grid *g, double **vp, double **vs, double **rho);
 int sm_read_model_a(const char *path, sm_grid *g, double **vp, double **rho);
 /* source and output files (io_utils.c:1432-1741); *src / *rec malloc'ed */
@@ -65,6 +67,22 @@ int sm_read_records(const char *path, const sm_grid *g, int three_d, sm_record *
 /* trc/<base>/<base>_<n>.trc, "%le    %le" of t and 1e3 * v (io_utils.c:1744-1768) */
 int sm_write_trace_file(const char *base, size_t n, const double *t, const double *v,
                         size_t ns);
+/* segy/<base>.sgy with the layout save_segy writes (io_utils.c:3269-3559):
+ * 3200-byte textual header, 400-byte binary header, per trace a 240-byte
+ * header and its samples as IEEE float32, all in the host's byte order as the
+ * reference writes them.  Sample i of a trace is the value at time i*dt_r
+ * (dt_r the record's interval), as fill_data_segy (io_utils.c:1770-1773)
+ * places it; but where that routine keeps round(duration/dt_r) samples, so
+ * that the last one lands one past its array and sample 0 (t = 0, never
+ * recorded) is left uninitialised, each trace here holds
+ * round(duration/dt_r) + 1 samples and every sample not recorded is zero.
+ * Pressure traces are written too (trace code 11, the SEG-Y code of a
+ * pressure sensor); the reference leaves them out.
+ * rec[r]: the record of trace r; v, t: ntr rows of ld recorded values and
+ * their times; count[r] of them. */
+int sm_write_segy(const char *base, const sm_params *p, const sm_record *rec, size_t ntr,
+                  const sm_source *src0, const double *v, const double *t, size_t ld,
+                  const size_t *count);
 
 #ifdef __cplusplus
 }

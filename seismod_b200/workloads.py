@@ -106,7 +106,9 @@ class A3DProblem:
     def cells(self):
         return int(np.prod([n + 2 * self.npml for n in self.shape]))
 
-    def write(self, workdir, basename=None, profile_1d=False):
+    def write(self, workdir, basename=None, profile_1d=False, **par_extra):
+        """Write run.par, model.dat, src.dat, rcv.dat; par_extra adds .par
+        keywords (e.g. segy=1)."""
         os.makedirs(workdir, exist_ok=True)
         base = basename or self.name
         if profile_1d:
@@ -122,7 +124,7 @@ class A3DProblem:
         formats.write_par(par, "model.dat", "src.dat", "rcv.dat", base, self.duration,
                           self.dt_ms, abs_=1 if self.npml > 0 else 0, nl=self.npml,
                           Rc=repr(self.Rc), kappa_max=repr(self.kappa_max),
-                          alpha_max=int(self.alpha_max))
+                          alpha_max=int(self.alpha_max), **par_extra)
         return par
 
 

@@ -99,9 +99,31 @@ def _save(path, p, kind, program, t, v):
     np.savez_compressed(path, meta=json.dumps(meta), **arrays)
 
 
+def segy_case():
+    """a_iso_3d with SEG-Y output (segy 1): the reference's .sgy bytes."""
+    p = W.cfg1(n=20, npml=5, nsteps=120, seed=13)
+    p.sources = [("Bulk", 1.0, 40.0, 50.0, 45.0, 40.0)]
+    p.receivers = [("Vz", 5.0, 10.0, 0.0, 0.0, p.dt_ms), ("Vx", 70.0, 35.0, 15.0, 0.0, p.dt_ms),
+                   ("Vy", 60.0, 15.0, 50.0, 0.0, p.dt_ms), ("Vz", 45.0, 60.0, 35.0, 0.0, p.dt_ms)]
+    p.name = "a3d_segy"
+    return p
+
+
+def make_segy_fixture():
+    p = segy_case()
+    d = tempfile.mkdtemp(prefix="golden_")
+    par = p.write(d, segy=1, shotpoint=7)
+    O.run_reference("a_iso_3d", par, d)
+    with open(os.path.join(d, "segy", f"{p.name}.sgy"), "rb") as f:
+        sgy = np.frombuffer(f.read(), dtype=np.uint8)
+    np.savez_compressed(os.path.join(HERE, "segy_a3d.npz"), sgy=sgy)
+    print(f"{p.name}: a_iso_3d segy -> {sgy.size} bytes")
+
+
 def main():
     if not O.ref_available():
         O.build()
+    make_segy_fixture()
     for name, (p, prog) in {**eiso_cases(), **a3d_cases()}.items():
         d = tempfile.mkdtemp(prefix="golden_")
         if prog.startswith("a_iso_3d"):

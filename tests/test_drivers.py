@@ -16,7 +16,8 @@ from seismod_b200 import workloads as W
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 BIN = os.path.join(ROOT, "seismod_b200", "bin")
-GOLDEN = sorted(glob.glob(os.path.join(os.path.dirname(__file__), "golden", "*.npz")))
+GOLDEN = sorted(p for p in glob.glob(os.path.join(os.path.dirname(__file__), "golden", "*.npz"))
+                if not os.path.basename(p).startswith("segy_"))
 
 
 def run(prog, args, cwd):
@@ -80,3 +81,90 @@ def test_drop_in_programs_write_the_reference_traces(path, tmp_path):
     # the same "%le    %le" text layout
     line = open(F.trace_path(str(tmp_path), p.name, 1)).readline()
     assert len(line.split("    ")) == 2 and "e" in line.split()[0]
+
+
+SEGY = os.path.join(os.path.dirname(__file__), "golden", "segy_a3d.npz")
+
+
+def _segy_traces(b, ns_key=114):
+    """(headers, samples) of each trace of a SEG-Y byte string laid out as
+    save_segy writes it (host byte order)."""
+    out, pos = [], 3600
+    while pos < len(b):
+        hdr = b[pos:pos + 240]
+        ns = int(np.frombuffer(hdr[ns_key:ns_key + 2].tobytes(), dtype=np.int16)[0])
+        out.append((hdr, np.frombuffer(b[pos + 240:pos + 240 + 4 * ns].tobytes(), dtype=np.float32)))
+        pos += 240 + 4 * ns
+    return out
+
+
+@pytest.mark.gpu
+def test_segy_output_matches_the_reference_layout(tmp_path):
+    """segy 1: same file, headers field for field (clock fields and sample
+    counts aside), the reference's samples.  Sample i is the value at
+    i * dt; the reference keeps one sample too few (its last recorded one is
+    written past its array) and leaves sample 0 (t = 0) uninitialised, so
+    samples 1 .. n-1 are compared and ours holds one more, and zero at t = 0."""
+    ref = np.load(SEGY)["sgy"]
+    p = G.segy_case()
+    par = p.write(str(tmp_path), segy=1, shotpoint=7)
+    r = run("a_iso_3d_gpu", ["-p", os.path.basename(par)], tmp_path)
+    assert r.returncode == 0, r.stderr
+    got = np.fromfile(os.path.join(str(tmp_path), "segy", f"{p.name}.sgy"), dtype=np.uint8)
+    # textual and binary file headers: equal except the sample counts (bytes 3221-3224)
+    keep = np.ones(3600, bool)
+    keep[3220:3224] = False
+    np.testing.assert_array_equal(got[:3600][keep], ref[:3600][keep])
+    rt, gt = _segy_traces(ref), _segy_traces(got)
+    assert len(rt) == len(gt) == len(p.receivers)
+    hkeep = np.ones(240, bool)
+    hkeep[114:116] = False      # samples in this trace
+    hkeep[156:166] = False      # year, day, hour, minute, second of writing
+    a, b = [], []
+    for (rh, rs), (gh, gs) in zip(rt, gt):
+        np.testing.assert_array_equal(gh[hkeep], rh[hkeep])
+        assert len(gs) == len(rs) + 1 and gs[0] == 0.0
+        a.append(gs[1:len(rs)].astype(np.float64))
+        b.append(rs[1:].astype(np.float64))
+    assert H.rel_l2(a, b) < 1e-5
+    # the samples are the raw velocities the trace files would hold (x 1e-3)
+    r = run("a_iso_3d_gpu", ["-p", os.path.basename(p.write(str(tmp_path / "trc")))], tmp_path / "trc")
+    assert r.returncode == 0, r.stderr
+    t, v = F.read_traces(str(tmp_path / "trc"), p.name, len(p.receivers))
+    assert H.rel_l2([1e-3 * x for x in v], [g[1][1:].astype(np.float64) for g in gt]) < 1e-6
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name", ["eiso_square", "a3d_cube"])
+def test_binary_model_gives_the_same_traces_as_ascii(name, tmp_path):
+    """A model given as a binary file (no text parsing) runs exactly as the
+    same values in the reference's ASCII format: identical trace files."""
+    p, kind, program, _, _ = G.load(os.path.join(os.path.dirname(__file__), "golden", f"{name}.npz"))
+    out = {}
+    for fmt in ("ascii", "bin"):
+        d = tmp_path / fmt
+        if kind == "eiso":
+            par = p.write(str(d), shot=0, basename=p.name)
+            if fmt == "bin":
+                F.write_model_bin(os.path.join(str(d), "model.dat"), [p.vp, p.vs, p.rho],
+                                  (p.h, p.h), (p.x0, p.z0))
+            r = run("e_iso_gpu", ["-p", os.path.basename(par)], d)
+        else:
+            par = p.write(str(d))
+            if fmt == "bin":
+                F.write_model_bin(os.path.join(str(d), "model.dat"), [p.vp, p.rho], p.d, p.origin)
+            r = run("a_iso_3d_gpu", ["-p", os.path.basename(par)], d)
+        assert r.returncode == 0, r.stderr
+        out[fmt] = [open(F.trace_path(str(d), p.name, n + 1)).read()
+                    for n in range(len(p.receivers))]
+    assert out["ascii"] == out["bin"]
+
+
+def test_binary_model_header_errors_are_reported(tmp_path):
+    """A truncated binary model is an input error, not a crash (CPU path)."""
+    p = W.cfg0(nx=20, nz=20, npml=3, nsteps=10, nrec=2)
+    par = p.write(str(tmp_path), shot=0, basename="b")
+    with open(os.path.join(str(tmp_path), "model.dat"), "wb") as f:
+        f.write(b"SEISMODB" + bytes(10))
+    r = run("e_iso_gpu", ["-p", os.path.basename(par)], tmp_path)
+    assert r.returncode != 0 and "binary model" in r.stderr
