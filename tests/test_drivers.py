@@ -168,3 +168,22 @@ def test_binary_model_header_errors_are_reported(tmp_path):
         f.write(b"SEISMODB" + bytes(10))
     r = run("e_iso_gpu", ["-p", os.path.basename(par)], tmp_path)
     assert r.returncode != 0 and "binary model" in r.stderr
+
+
+@pytest.mark.gpu
+def test_pressure_traces_from_the_drop_in_program(tmp_path):
+    """a_iso_3d accepts P records but its loop leaves them undefined
+    (a_iso_3d.c:703-715); here they are the pressure at the node, written like
+    the velocity traces (1e3 * value), and equal what the library records."""
+    from seismod_b200 import api
+    p = W.cfg1(n=24, npml=5, nsteps=140, seed=17)
+    p.receivers = [("P", 40.0, 45.0, 30.0, 0.0, p.dt_ms), ("Vz", 40.0, 45.0, 30.0, 0.0, p.dt_ms),
+                   ("P", 10.0, 70.0, 80.0, 0.0, 2 * p.dt_ms)]
+    par = p.write(str(tmp_path))
+    r = run("a_iso_3d_gpu", ["-p", os.path.basename(par)], tmp_path)
+    assert r.returncode == 0, r.stderr
+    t, v = F.read_traces(str(tmp_path), p.name, len(p.receivers))
+    ref = api.run_a3d(p, "fp32")
+    assert [len(a) for a in v] == [len(a) for a in ref]
+    assert H.rel_l2(v, [1e3 * a for a in ref]) < 1e-6
+    assert np.abs(v[0]).max() > 0
