@@ -102,11 +102,21 @@ def write_src(path, sources, ntemplate=1):
 
 
 def write_rcv(path, records):
-    """records: list of (comp, coords tuple, t0_s, dt_ms)."""
+    """records: list of (comp, coords tuple, t0_s, dt_ms[, "Trace" | "Snapshot"]).
+    A Snapshot record has no coordinates in the file (io_utils.c:1668-1672):
+    its coords entry is ignored."""
     with open(path, "w") as f:
         f.write(f"{len(records)}\n")
-        for comp, xyz, t0, dtms in records:
-            f.write(f"\n{comp}\nTrace\n{' '.join(_num(c) for c in xyz)}\n{_num(t0)}\n{_num(dtms)}\n")
+        for comp, xyz, t0, dtms, *kind in records:
+            typ = kind[0] if kind else "Trace"
+            where = "" if typ.lower() == "snapshot" else " ".join(_num(c) for c in xyz) + "\n"
+            f.write(f"\n{comp}\n{typ}\n{where}{_num(t0)}\n{_num(dtms)}\n")
+
+
+def read_snapshot(path):
+    """(x, z, value) columns of a text snapshot (write_snapshot layout)."""
+    a = np.loadtxt(path, ndmin=2)
+    return a[:, 0], a[:, 1], a[:, 2]
 
 
 def trace_path(workdir, basename, n):

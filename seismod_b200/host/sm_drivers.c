@@ -6,9 +6,10 @@
  * a_iso_3d/a_iso_3d.c:240-591) in FP64 through the library's host
  * functions; the loop (e_iso.c:589-670, a_iso_3d.c:593-741) runs through
  * the C ABI.  Differences: errors return a non-zero status with a message
- * instead of abort()/exit(); snapshot records (netCDF) are skipped with a
- * warning; the 8 outer points of a 9-point source template take the
- * centre's type (io_utils.c:1494-1535 leaves them unset).
+ * instead of abort()/exit(); snapshot records are written in the reference's
+ * text snapshot format (write_snapshot, io_utils.c:1775-1820) since netCDF
+ * is not available here; the 8 outer points of a 9-point source template
+ * take the centre's type (io_utils.c:1494-1535 leaves them unset).
  */
 #include <math.h>
 #include <stdio.h>
@@ -49,6 +50,43 @@ static int write_traces(const char *base, const rec_plan *rp, const double *vals
         if (rc) { free(t); return rc; }
     }
     free(t);
+    return SM_OK;
+}
+
+/* Snapshot records: the steps at which each is taken, by the traces'
+ * sampling test (e_iso.c:641-669, a_iso_3d.c:698-741), in step order. */
+typedef struct {
+    size_t it, rec;
+} snap_ev;
+
+static int snap_cmp(const void *a, const void *b)
+{
+    const snap_ev *x = a, *y = b;
+    if (x->it != y->it) return x->it < y->it ? -1 : 1;
+    return x->rec < y->rec ? -1 : (x->rec > y->rec);
+}
+
+static int snap_events(const sm_record *rec, size_t nrec, double dt, size_t nsteps, snap_ev **out,
+                       size_t *n)
+{
+    size_t cap = 16;
+    *n = 0;
+    *out = malloc(cap * sizeof(snap_ev));
+    if (!*out) return sm_fail(SM_ENOMEM, "out of host memory");
+    for (size_t r = 0; r < nrec; ++r) {
+        if (rec[r].is_trace) continue;
+        for (size_t it = 0; it < nsteps; ++it) {
+            if (!sm_sample_predicate(it, dt, rec[r].t0, rec[r].dt)) continue;
+            if (*n == cap) {
+                snap_ev *m = realloc(*out, 2 * cap * sizeof(snap_ev));
+                if (!m) return sm_fail(SM_ENOMEM, "out of host memory");
+                *out = m;
+                cap *= 2;
+            }
+            (*out)[(*n)++] = (snap_ev){it, r};
+        }
+    }
+    qsort(*out, *n, sizeof(snap_ev), snap_cmp);
     return SM_OK;
 }
 
@@ -162,10 +200,7 @@ int sm_e_iso_main(int argc, char **argv)
     rp.comp = malloc((nrec ? nrec : 1) * sizeof(int));
     rp.t0 = malloc((nrec ? nrec : 1) * sizeof(double)); rp.rdt = malloc((nrec ? nrec : 1) * sizeof(double));
     for (size_t n = 0; n < nrec; ++n) {
-        if (!rec[n].is_trace) {
-            fprintf(stderr, "%s: record %zu is a snapshot (netCDF); skipped\n", prog, n + 1);
-            continue;
-        }
+        if (!rec[n].is_trace) continue;   /* snapshots: written as the loop passes them */
         if (rec[n].i < 0 || rec[n].k < 0 || (size_t)rec[n].i >= nx || (size_t)rec[n].k >= nz) {
             rc = sm_fail(SM_EINVAL, "record %zu lies outside the grid", n + 1);
             goto out;
@@ -179,7 +214,31 @@ int sm_e_iso_main(int argc, char **argv)
     }
     if ((rc = sm_eiso_set_receivers(h, 0, rp.n, rp.index, rp.comp, rp.t0, rp.rdt, nsteps))) goto out;
     if (p.verbose) fprintf(stdout, "Starting main loop (%zu iterations)\n", nsteps);
-    if ((rc = sm_eiso_run(h, nsteps))) goto out;
+    {   /* the loop, stopping after each snapshot step (write_snapshot, io_utils.c:1775) */
+        snap_ev *ev = NULL;
+        size_t nev = 0, done = 0;
+        const size_t NX = nx + 2 * npml, NZ = nz + 2 * npml;
+        double *field = NULL;
+        if ((rc = snap_events(rec, nrec, dt, nsteps, &ev, &nev))) { free(ev); goto out; }
+        if (nev && !(field = malloc(NX * NZ * sizeof(double)))) {
+            free(ev);
+            rc = sm_fail(SM_ENOMEM, "out of host memory");
+            goto out;
+        }
+        for (size_t e = 0; e < nev && !rc; ++e) {
+            const size_t upto = ev[e].it + 1;
+            if (upto > done) rc = sm_eiso_run(h, upto - done);
+            done = upto;
+            if (!rc) rc = sm_eiso_get_field(h, 0, rec[ev[e].rec].comp, SM_PART_TOTAL, field);
+            if (!rc)
+                rc = sm_write_snapshot(p.basename, ev[e].rec + 1, dt * (double)upto, field, NX, NZ,
+                                       npml, g.dx, g.dz, g.x0, g.z0, p.plot_strips);
+        }
+        if (!rc && done < nsteps) rc = sm_eiso_run(h, nsteps - done);
+        free(ev);
+        free(field);
+        if (rc) goto out;
+    }
     counts = calloc(rp.n ? rp.n : 1, sizeof(size_t));
     if ((rc = sm_eiso_read_traces(h, 0, 0, rp.n, NULL, 0, counts))) goto out;
     size_t ld = 1;
@@ -264,10 +323,7 @@ int sm_a_iso_3d_main(int argc, char **argv)
     rp.comp = malloc((nrec ? nrec : 1) * sizeof(int));
     rp.t0 = malloc((nrec ? nrec : 1) * sizeof(double)); rp.rdt = malloc((nrec ? nrec : 1) * sizeof(double));
     for (size_t n = 0; n < nrec; ++n) {
-        if (!rec[n].is_trace) {
-            fprintf(stderr, "%s: record %zu is a snapshot (netCDF); skipped\n", prog, n + 1);
-            continue;
-        }
+        if (!rec[n].is_trace) continue;   /* snapshots: written as the loop passes them */
         long i = rec[n].i + (long)np, j = rec[n].j + (long)np, k = rec[n].k + (long)np;
         if (i < 0 || j < 0 || k < 0 || (size_t)i >= nx2 || (size_t)j >= ny2 || (size_t)k >= nz2) {
             rc = sm_fail(SM_EINVAL, "record %zu lies outside the grid", n + 1);
@@ -282,7 +338,39 @@ int sm_a_iso_3d_main(int argc, char **argv)
     }
     if ((rc = sm_a3d_set_receivers(h, rp.n, rp.index, rp.comp, rp.t0, rp.rdt, nsteps))) goto out;
     if (p.verbose) fprintf(stdout, "Starting main loop (%zu iterations)\n", nsteps);
-    if ((rc = sm_a3d_run(h, nsteps))) goto out;
+    {   /* the loop, stopping after each snapshot step: the x-z plane through the
+         * first source, at y index (y_src - y0) / dy of the padded grid as
+         * a_iso_3d.c:722-730 takes it */
+        snap_ev *ev = NULL;
+        size_t nev = 0, done = 0;
+        double *vol = NULL, *plane = NULL;
+        if ((rc = snap_events(rec, nrec, dt, nsteps, &ev, &nev))) { free(ev); goto out; }
+        const size_t iy = nsrc ? (size_t)((src[0].y - g.y0) / g.dy) : 0;
+        if (nev && iy >= ny2) {
+            free(ev);
+            rc = sm_fail(SM_EINVAL, "snapshot plane y index %zu outside the grid", iy);
+            goto out;
+        }
+        if (nev && (!(vol = malloc(n3 * sizeof(double))) || !(plane = malloc(nx2 * nz2 * sizeof(double))))) {
+            free(ev); free(vol);
+            rc = sm_fail(SM_ENOMEM, "out of host memory");
+            goto out;
+        }
+        for (size_t e = 0; e < nev && !rc; ++e) {
+            const size_t upto = ev[e].it + 1;
+            if (upto > done) rc = sm_a3d_run(h, upto - done);
+            done = upto;
+            if (!rc) rc = sm_a3d_get_field(h, rec[ev[e].rec].comp, vol);
+            if (rc) break;
+            for (size_t i = 0; i < nx2; ++i)
+                for (size_t k = 0; k < nz2; ++k) plane[i * nz2 + k] = vol[(i * ny2 + iy) * nz2 + k];
+            rc = sm_write_snapshot(p.basename, ev[e].rec + 1, dt * (double)upto, plane, nx2, nz2,
+                                   np, g.dx, g.dz, g.x0, g.z0, p.plot_strips);
+        }
+        if (!rc && done < nsteps) rc = sm_a3d_run(h, nsteps - done);
+        free(ev); free(vol); free(plane);
+        if (rc) goto out;
+    }
     counts = calloc(rp.n ? rp.n : 1, sizeof(size_t));
     if ((rc = sm_a3d_read_traces(h, 0, rp.n, NULL, 0, counts))) goto out;
     size_t ld = 1;

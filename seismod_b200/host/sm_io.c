@@ -31,6 +31,7 @@ void sm_params_defaults(sm_params *p)
     p->segy = 0;
     p->shotpt_no = 1;
     p->simulate_cmp = 0;
+    p->plot_strips = 0;
     p->Rc = 1.e-5;
     p->kappa_max = 1.;
     p->alpha_max = 1;
@@ -105,12 +106,13 @@ int sm_read_par(const char *path, sm_params *p)
         else if (!strcmp(keyword, "abs")) p->iwipe = (short)atoi(value);
         else if (!strcmp(keyword, "nl")) p->np = (size_t)atoi(value);
         else if (!strcmp(keyword, "segy")) p->segy = (short)atoi(value);
+        else if (!strcmp(keyword, "plstr")) p->plot_strips = atoi(value);
         else if (!strcmp(keyword, "shotpoint")) p->shotpt_no = atoi(value);
         else if (!strcmp(keyword, "simulateCMP")) p->simulate_cmp = atoi(value);
         else if (!strcmp(keyword, "Rc")) p->Rc = strtod(value, NULL);
         else if (!strcmp(keyword, "kappa_max")) p->kappa_max = strtod(value, NULL);
         else if (!strcmp(keyword, "alpha_max")) p->alpha_max = (short)atoi(value);
-        /* plstr, check_model, chkpt_inc, pml_median, saveEnergy, EnergyROI,
+        /* check_model, chkpt_inc, pml_median, saveEnergy, EnergyROI,
          * azimuthal_mode: accepted, unused by these programs */
     }
     fclose(fid);
@@ -595,4 +597,38 @@ int sm_write_segy(const char *base, const sm_params *p, const sm_record *rec, si
     if (fclose(f) != 0) ok = 0;
     if (!ok) return sm_fail(SM_EIO, "write error on %s", fname);
     return SM_OK;
+}
+
+int sm_write_snapshot(const char *base, size_t n, double t, const double *data, size_t nx2,
+                      size_t nz2, size_t np, double dx, double dz, double x0, double z0,
+                      int plot_strips)
+{
+    char name[700];
+    struct stat sb;
+    if (stat("ssh", &sb) < 0 && errno == ENOENT) mkdir("ssh", S_IRWXU);
+    snprintf(name, sizeof name, "ssh/%s", base);
+    if (stat(name, &sb) < 0 && errno == ENOENT) mkdir(name, S_IRWXU);
+    snprintf(name, sizeof name, "ssh/%s/%s_%zu_%lf.ssh", base, base, n, t);
+    FILE *f = fopen(name, "w");
+    if (!f) return sm_fail(SM_EIO, "cannot open %s for output (%s)", name, strerror(errno));
+    int ok = 1;
+    if (plot_strips) {
+        for (size_t i = 0; i < nx2 && ok; ++i) {
+            const double x = x0 + ((double)i - (double)np) * dx;
+            for (size_t k = 0; k < nz2 && ok; ++k) {
+                const double z = z0 + ((double)k - (double)np) * dz;
+                ok = fprintf(f, "%le  %le  %le\n", x, z, 1.e3 * data[i * nz2 + k]) > 0;
+            }
+        }
+    } else {
+        for (size_t i = 0; i + 2 * np < nx2 && ok; ++i) {
+            const double x = x0 + i * dx;
+            for (size_t k = 0; k + 2 * np < nz2 && ok; ++k) {
+                const double z = z0 + k * dz;
+                ok = fprintf(f, "%le  %le  %le\n", x, z, 1.e3 * data[(i + np) * nz2 + k + np]) > 0;
+            }
+        }
+    }
+    if (fclose(f) != 0) ok = 0;
+    return ok ? SM_OK : sm_fail(SM_EIO, "write error on %s", name);
 }

@@ -26,6 +26,7 @@ typedef struct {
     double Rc, kappa_max, vmax, pml_order;
     int alpha_max;
     int verbose;
+    int plot_strips;     /* "plstr": snapshots include the absorbing frame */
     int precision;       /* SM_FP32 by default; "-P" */
 } sm_params;
 
@@ -80,6 +81,13 @@ int sm_write_trace_file(const char *base, size_t n, const double *t, const doubl
  * pressure sensor); the reference leaves them out.
  * rec[r]: the record of trace r; v, t: ntr rows of ld recorded values and
  * their times; count[r] of them. */
+/* ssh/<base>/<base>_<n>_<t>.ssh, the text snapshot of write_snapshot
+ * (io_utils.c:1775-1820): "%le  %le  %le" of x, z and 1e3 * value per node,
+ * x slow; the interior nodes, or every node of the padded nx2 x nz2 plane
+ * when plot_strips.  data: the padded plane, index i*nz2 + k. */
+int sm_write_snapshot(const char *base, size_t n, double t, const double *data, size_t nx2,
+                      size_t nz2, size_t np, double dx, double dz, double x0, double z0,
+                      int plot_strips);
 int sm_write_segy(const char *base, const sm_params *p, const sm_record *rec, size_t ntr,
                   const sm_source *src0, const double *v, const double *t, size_t ld,
                   const size_t *count);

@@ -59,8 +59,9 @@ class EIsoProblem:
     def cells(self):
         return (self.nx + 2 * self.npml) * (self.nz + 2 * self.npml)
 
-    def write(self, workdir, shot=0, basename=None, profile_1d=False):
-        """Write the reference's input files for one shot; returns the .par path."""
+    def write(self, workdir, shot=0, basename=None, profile_1d=False, **par_extra):
+        """Write the reference's input files for one shot; returns the .par path.
+        par_extra adds .par keywords (e.g. plstr=1)."""
         os.makedirs(workdir, exist_ok=True)
         base = basename or f"{self.name}_s{shot}"
         if profile_1d:
@@ -74,7 +75,7 @@ class EIsoProblem:
                           [(c, (x, z), t0, r) for (c, x, z, t0, r) in self.receivers])
         par = os.path.join(workdir, "run.par")
         formats.write_par(par, "model.dat", "src.dat", "rcv.dat", base, self.duration,
-                          self.dt_ms, abs_=1 if self.npml > 0 else 0, nl=self.npml)
+                          self.dt_ms, abs_=1 if self.npml > 0 else 0, nl=self.npml, **par_extra)
         return par
 
 

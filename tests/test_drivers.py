@@ -187,3 +187,63 @@ def test_pressure_traces_from_the_drop_in_program(tmp_path):
     assert [len(a) for a in v] == [len(a) for a in ref]
     assert H.rel_l2(v, [1e3 * a for a in ref]) < 1e-6
     assert np.abs(v[0]).max() > 0
+
+
+def _snapshot_file(d, base, n):
+    files = glob.glob(os.path.join(str(d), "ssh", base, f"{base}_{n}_*.ssh"))
+    assert len(files) == 1, files
+    return files[0]
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("strips", [0, 1])
+def test_eiso_snapshots_in_the_reference_text_format(strips, tmp_path):
+    """Snapshot records are written as write_snapshot writes them (netCDF is
+    not available): one file per snapshot time, x, z and 1e3 * value per
+    node, the interior or, with plstr 1, the whole padded grid."""
+    from seismod_b200 import api
+    p = W.cfg0(nx=48, nz=40, npml=6, nsteps=120, nrec=2)
+    k = 60
+    par = p.write(str(tmp_path), shot=0, basename="snap", plstr=strips)
+    recs = [(c, (x, z), t0, r) for (c, x, z, t0, r) in p.receivers]
+    recs.append(("Vz", (0.0, 0.0), k * p.dt, 1e6, "Snapshot"))
+    F.write_rcv(os.path.join(str(tmp_path), "rcv.dat"), recs)
+    r = run("e_iso_gpu", ["-p", os.path.basename(par)], tmp_path)
+    assert r.returncode == 0, r.stderr
+    x, z, val = F.read_snapshot(_snapshot_file(tmp_path, "snap", len(recs)))
+    dev, _ = api.eiso_device(p, "fp32")
+    dev.run(k)
+    vz = dev.get_field("vz")
+    dev.close()
+    np_ = p.npml
+    ref = vz if strips else vz[np_:np_ + p.nx, np_:np_ + p.nz]
+    assert val.size == ref.size
+    np.testing.assert_allclose(val.reshape(ref.shape), 1e3 * ref, rtol=1e-5,
+                               atol=1e-5 * np.abs(1e3 * ref).max())
+    assert x[0] == (-np_ * p.h if strips else 0.0)
+    # the trace records are unchanged by the stops for the snapshot
+    t, v = F.read_traces(str(tmp_path), "snap", len(p.receivers))
+    assert H.rel_l2(v, [1e3 * a for a in api.run_eiso(p, "fp32")[0]]) < 1e-6
+
+
+@pytest.mark.gpu
+def test_a3d_snapshot_plane(tmp_path):
+    from seismod_b200 import api
+    p = W.cfg1(n=20, npml=4, nsteps=90, seed=19, rec_stride=10)
+    k = 40
+    par = p.write(str(tmp_path))
+    recs = [(c, (x, y, z), t0, r) for (c, x, y, z, t0, r) in p.receivers]
+    recs.append(("Vz", (0.0, 0.0, 0.0), k * p.dt, 1e6, "Snapshot"))
+    F.write_rcv(os.path.join(str(tmp_path), "rcv.dat"), recs)
+    r = run("a_iso_3d_gpu", ["-p", os.path.basename(par)], tmp_path)
+    assert r.returncode == 0, r.stderr
+    _, _, val = F.read_snapshot(_snapshot_file(tmp_path, p.name, len(recs)))
+    dev, _ = api.a3d_device(p, "fp32")
+    dev.run(k)
+    vol = dev.get_field("vz")
+    dev.close()
+    iy = int((p.sources[0][4] - p.origin[1]) / p.d[1])   # a_iso_3d.c: plane index as it takes it
+    n = p.npml
+    ref = vol[n:-n, iy, n:-n]
+    np.testing.assert_allclose(val.reshape(ref.shape), 1e3 * ref, rtol=1e-5,
+                               atol=1e-5 * np.abs(1e3 * ref).max())
