@@ -156,6 +156,16 @@ int sm_eiso_set_receivers(sm_eiso_t h, size_t shot, size_t nrec, const size_t *i
 /* Advance every shot by nsteps time steps (the body of e_iso.c:589-670).
  * Asynchronous: returns once the work is queued. */
 int sm_eiso_run(sm_eiso_t h, size_t nsteps);
+/* Advance n handles of possibly different grid sizes, shot counts and
+ * sources together by nsteps steps each (the same loop, e_iso.c:589-670,
+ * for several models at once): each step is one launch over the slabs of
+ * all of them (up to 32 handles per launch), one for all their sources and
+ * one for all their receivers.  Every handle ends bit for bit where
+ * sm_eiso_run(handles[k], nsteps) would leave it.  Same device and
+ * precision for all; the work is queued on handles[0]'s stream after the
+ * work already queued on every handle's stream, and every handle's stream
+ * waits for it.  Asynchronous like sm_eiso_run. */
+int sm_eiso_group_run(sm_eiso_t const *handles, int n, size_t nsteps);
 int sm_eiso_sync(sm_eiso_t h);
 /* steps taken so far */
 int sm_eiso_step_count(sm_eiso_t h, size_t *it);
@@ -339,6 +349,11 @@ typedef struct sm_server *sm_server_t;
  * (0 none; else as sm_eiso_set_graph). */
 int sm_server_create(int device, size_t hbm_budget, int max_active, int slice_steps,
                      int graph_steps, sm_server_t *out);
+/* on != 0: running e_iso requests of one precision take their slices
+ * together, one sm_eiso_group_run call (one launch per step over all of
+ * their grids) instead of one sm_eiso_run each; results are the same bits.
+ * Call before the first submission. */
+int sm_server_set_group(sm_server_t s, int on);
 /* SM_EBUSY when the request alone exceeds the budget */
 int sm_server_submit_eiso(sm_server_t s, const sm_eiso_request *r, uint64_t *ticket);
 int sm_server_submit_a3d(sm_server_t s, const sm_a3d_request *r, uint64_t *ticket);

@@ -21,6 +21,7 @@
 //   B = 2/(2 + dt d); d = 0 along a strip gives A = B = 1.
 // The reference's c1/c2 form (q*c2 + m*delta/h)*c1 is the same expression.
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstring>
 #include <map>
@@ -401,28 +402,28 @@ struct ESlabG {
     static constexpr unsigned tx = (unsigned)(5 * RX * BW * sizeof(S));
 };
 
-template <typename S, int W, int TX, int MINB>
-__global__ void __launch_bounds__(32 * W, MINB) eiso_slabg_kernel(const EisoArgs a,
-                                                                  const __grid_constant__ EisoSlabMaps mp) {
+// the slab step of block (bx, by, shot) of one problem; fmap is the TMA map
+// of its old set (box (BW, TX+2, 1, 5)); smem holds ESlabG's layout
+template <typename S, int W, int TX>
+__device__ __forceinline__ void eiso_slabg_body(const EisoArgs &a, const CUtensorMap *fmap,
+                                                int bx, int by, int shot, unsigned char *smem) {
     using C = typename Store<S>::C;
     using St = Store<S>;
     using L = ESlabG<S, W, TX>;
-    extern __shared__ __align__(128) unsigned char smem[];
     const unsigned full = 0xffffffffu;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    if ((blockIdx.x | blockIdx.y | blockIdx.z | threadIdx.x) == 0) ++*a.step;
+    if ((bx | by | shot | threadIdx.x) == 0) ++*a.step;
     const S *fbox = reinterpret_cast<const S *>(smem);
     uint64_t *bar = reinterpret_cast<uint64_t *>(smem + L::oBar);
-    const int Zc = blockIdx.x * W * 30;
-    const int X0 = blockIdx.y * TX;
+    const int Zc = bx * W * 30;
+    const int X0 = by * TX;
     const int X1 = min(X0 + TX, a.NX);
-    const int shot = blockIdx.z;
     const int zs = (Zc - 1 + L::HS) / L::HS * L::HS - L::HS;
     if (threadIdx.x == 0) {
         mbar_init(bar, 1);
         fence_proxy_async();
         mbar_expect_tx(bar, L::tx);
-        tma_load_4d(smem, &mp.f, zs, X0 - 1, shot, 0, bar);
+        tma_load_4d(smem, fmap, zs, X0 - 1, shot, 0, bar);
     }
     __syncthreads();   // the barrier is initialised before anyone polls it
     const int Z0 = Zc + warp * 30;
@@ -608,6 +609,13 @@ __global__ void __launch_bounds__(32 * W, MINB) eiso_slabg_kernel(const EisoArgs
         vzp = vzn;
         sp = sn;
     }
+}
+
+template <typename S, int W, int TX, int MINB>
+__global__ void __launch_bounds__(32 * W, MINB) eiso_slabg_kernel(const EisoArgs a,
+                                                                  const __grid_constant__ EisoSlabMaps mp) {
+    extern __shared__ __align__(128) unsigned char smem[];
+    eiso_slabg_body<S, W, TX>(a, &mp.f, blockIdx.x, blockIdx.y, blockIdx.z, smem);
 }
 
 // ---------------------------------------------------------------------------
@@ -831,32 +839,40 @@ struct SrcEntry {
     int len;
 };
 
+// add_src (src.c:170-184) for one shot, into the wavefields f just written
 template <typename S>
-__global__ void eiso_source_kernel(EisoArgs a, const SrcEntry *src, const int *shot_first,
-                                   const double *vals, int nshots) {
-    const long long it = *a.step - 1;
+__device__ __forceinline__ void eiso_inject(void *const *f, long long fstride, const float *sc,
+                                            const float *isc, long long it, const SrcEntry *src,
+                                            const int *shot_first, const double *vals, int shot) {
     using St = Store<S>;
     using C = typename Store<S>::C;
-    const int shot = blockIdx.x * blockDim.x + threadIdx.x;
-    if (shot >= nshots) return;
     for (int e = shot_first[shot]; e < shot_first[shot + 1]; ++e) {
         const SrcEntry s = src[e];
         if (it >= s.len) continue;
         const C v = static_cast<C>(vals[s.voff + it]);
-        const long long base = (long long)shot * a.fstride + s.q;
+        const long long base = (long long)shot * fstride + s.q;
         if (s.type == SM_SRC_SX || s.type == SM_SRC_BULK) {
-            S *p = static_cast<S *>(a.f[F_TXX]) + base;
-            St::st(p, St::ld(p, a.isc[F_TXX]) + v, a.sc[F_TXX]);
+            S *p = static_cast<S *>(f[F_TXX]) + base;
+            St::st(p, St::ld(p, isc[F_TXX]) + v, sc[F_TXX]);
         }
         if (s.type == SM_SRC_SZ || s.type == SM_SRC_BULK) {
-            S *p = static_cast<S *>(a.f[F_TZZ]) + base;
-            St::st(p, St::ld(p, a.isc[F_TZZ]) + v, a.sc[F_TZZ]);
+            S *p = static_cast<S *>(f[F_TZZ]) + base;
+            St::st(p, St::ld(p, isc[F_TZZ]) + v, sc[F_TZZ]);
         }
         if (s.type == SM_SRC_SXZ) {
-            S *p = static_cast<S *>(a.f[F_TXZ]) + base;
-            St::st(p, St::ld(p, a.isc[F_TXZ]) + v, a.sc[F_TXZ]);
+            S *p = static_cast<S *>(f[F_TXZ]) + base;
+            St::st(p, St::ld(p, isc[F_TXZ]) + v, sc[F_TXZ]);
         }
     }
+}
+
+template <typename S>
+__global__ void eiso_source_kernel(EisoArgs a, const SrcEntry *src, const int *shot_first,
+                                   const double *vals, int nshots) {
+    const long long it = *a.step - 1;
+    const int shot = blockIdx.x * blockDim.x + threadIdx.x;
+    if (shot >= nshots) return;
+    eiso_inject<S>(a.f, a.fstride, a.sc, a.isc, it, src, shot_first, vals, shot);
 }
 
 struct RecEntry {
@@ -867,19 +883,115 @@ struct RecEntry {
     long long out;     // offset of its first sample in the trace buffer
 };
 
+// one receiver's sample of step it, if the record's predicate takes it
+// (e_iso.c:641-669, resolved into the slot table on the host)
+template <typename S>
+__device__ __forceinline__ void eiso_sample(void *const *f, long long fstride, const float *isc,
+                                            long long it, const RecEntry &e, const int32_t *table,
+                                            long long nsteps_max, double *traces) {
+    using St = Store<S>;
+    if (it >= nsteps_max) return;
+    const int32_t slot = table[(long long)e.group * nsteps_max + it];
+    if (slot < 0) return;
+    const S *p = static_cast<const S *>(f[e.field]) + (long long)e.shot * fstride + e.q;
+    traces[e.out + slot] = static_cast<double>(St::ld(p, isc[e.field]));
+}
+
 template <typename S>
 __global__ void eiso_gather_kernel(EisoArgs a, const RecEntry *rec, int nrec,
                                    const int32_t *table, long long nsteps_max,
                                    double *traces) {
-    using St = Store<S>;
     const int r = blockIdx.x * blockDim.x + threadIdx.x;
-    const long long it = *a.step - 1;
-    if (r >= nrec || it >= nsteps_max) return;
-    const RecEntry e = rec[r];
-    const int32_t slot = table[(long long)e.group * nsteps_max + it];
-    if (slot < 0) return;
-    const S *p = static_cast<const S *>(a.f[e.field]) + (long long)e.shot * a.fstride + e.q;
-    traces[e.out + slot] = static_cast<double>(St::ld(p, a.isc[e.field]));
+    if (r >= nrec) return;
+    eiso_sample<S>(a.f, a.fstride, a.isc, *a.step - 1, rec[r], table, nsteps_max, traces);
+}
+
+// ---------------------------------------------------------------------------
+// Grouped step: one launch advances up to kGroupMax e_iso problems of
+// different grid sizes and shot counts by one time step.  Linear CTA b
+// belongs to the problem p with first[p] <= b < first[p+1]; inside it the
+// block is (bx, by, shot) of that problem's own slab grid and the update is
+// the slab step above, so each problem gets the bits its own launch gives.
+// Each problem's TMA map is a kernel parameter (read from parameter space
+// like the single-problem launch's); its other arguments are copied into
+// shared memory once per CTA.  Sources and receivers of all problems follow
+// in one launch each.
+// ---------------------------------------------------------------------------
+constexpr int kGroupMax = 32;
+
+struct EisoGroupStepParams {
+    CUtensorMap f[kGroupMax];     // each problem's old-set slab map
+    EisoArgs a[kGroupMax];        // its arguments for this step
+    int first[kGroupMax + 1];     // first linear CTA of each problem
+    int gx[kGroupMax], gy[kGroupMax];
+    int n;
+};
+static_assert(sizeof(EisoGroupStepParams) <= 32000, "kernel parameters are limited to 32 KB");
+static_assert(sizeof(EisoArgs) % 4 == 0, "EisoArgs is copied as 32-bit words");
+
+template <typename S, int W, int TX, int MINB>
+__global__ void __launch_bounds__(32 * W, MINB) eiso_group_step_kernel(
+    const __grid_constant__ EisoGroupStepParams P) {
+    extern __shared__ __align__(128) unsigned char smem[];
+    __shared__ EisoArgs sa;
+    const int b = blockIdx.x;
+    int p = 0;
+    while (p + 1 < P.n && P.first[p + 1] <= b) ++p;
+    const int local = b - P.first[p];
+    const int bx = local % P.gx[p], rest = local / P.gx[p];
+    const int by = rest % P.gy[p], shot = rest / P.gy[p];
+    {
+        const int *src = reinterpret_cast<const int *>(&P.a[p]);
+        int *dst = reinterpret_cast<int *>(&sa);
+        for (int i = threadIdx.x; i < (int)(sizeof(EisoArgs) / 4); i += blockDim.x) dst[i] = src[i];
+    }
+    __syncthreads();
+    eiso_slabg_body<S, W, TX>(sa, &P.f[p], bx, by, shot, smem);
+}
+
+// what the source and receiver kernels of one problem need after its step
+struct EisoPost {
+    void *f[5];                  // the wavefields just written
+    long long fstride;
+    const long long *step;
+    float sc[5], isc[5];
+    const SrcEntry *src;
+    const int *src_first;
+    const double *vals;
+    const RecEntry *rec;
+    const int32_t *table;
+    long long nsteps_max;
+    double *traces;
+};
+
+struct EisoGroupPostParams {
+    EisoPost q[kGroupMax];
+    int first_src[kGroupMax + 1];   // prefix sums of the problems' source threads (shots)
+    int first_rec[kGroupMax + 1];   // ... and receiver threads
+    int n;
+};
+static_assert(sizeof(EisoGroupPostParams) <= 32000, "kernel parameters are limited to 32 KB");
+
+template <typename S>
+__global__ void eiso_group_source_kernel(const __grid_constant__ EisoGroupPostParams P) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= P.first_src[P.n]) return;
+    int p = 0;
+    while (p + 1 < P.n && P.first_src[p + 1] <= t) ++p;
+    const EisoPost &q = P.q[p];
+    eiso_inject<S>(q.f, q.fstride, q.sc, q.isc, *q.step - 1, q.src, q.src_first, q.vals,
+                   t - P.first_src[p]);
+}
+
+template <typename S>
+__global__ void eiso_group_gather_kernel(const __grid_constant__ EisoGroupPostParams P) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= P.first_rec[P.n]) return;
+    int p = 0;
+    while (p + 1 < P.n && P.first_rec[p + 1] <= t) ++p;
+    const EisoPost &q = P.q[p];
+    eiso_sample<S>(q.f, q.fstride, q.isc, *q.step - 1, q.rec[t - P.first_rec[p]], q.table,
+                   q.nsteps_max, q.traces);
 }
 
 }  // namespace sm
@@ -935,6 +1047,7 @@ struct sm_eiso {
             if (g.exec) cudaGraphExecDestroy(g.exec);
     }
     int sms = 148;
+    uint64_t serial = 0;   // unique per handle in the process (grouped graphs' keys)
     // sources
     std::vector<std::vector<SrcEntry>> shot_src;     // per shot (voff local)
     std::vector<std::vector<double>> shot_vals;      // per shot scaled samples
@@ -1400,6 +1513,8 @@ extern "C" int sm_eiso_create(int device, size_t nx, size_t nz, size_t npml, dou
     DeviceGuard g(device);
 
     std::unique_ptr<sm_eiso> h(new (std::nothrow) sm_eiso());
+    static std::atomic<uint64_t> serials{1};
+    if (h) h->serial = serials.fetch_add(1);
     if (!h) return sm_fail(SM_ENOMEM, "sm_eiso_create: out of host memory");
     h->device = device;
     h->precision = precision;
@@ -1729,6 +1844,240 @@ extern "C" int sm_eiso_run(sm_eiso_t h, size_t nsteps) {
     case SM_BF16: rc = eiso_run_t<__nv_bfloat16>(h, nsteps); break;
     default: rc = eiso_run_t<float>(h, nsteps); break;
     }
+    if (rc) return rc;
+    SM_CUDA_TRY(cudaGetLastError());
+    return SM_OK;
+}
+
+namespace {
+
+// one grouped step of the problems hs[0..n) (n <= kGroupMax), all on stream st
+template <typename S>
+int eiso_group_step(sm_eiso *const *hs, int n, cudaStream_t st) {
+    using L = ESlabG<S, 2, 8>;
+    static EisoGroupStepParams P;   // large: built in place, one caller at a time
+    static EisoGroupPostParams Q;
+    static std::mutex mu;
+    std::lock_guard<std::mutex> lk(mu);
+    int total = 0;
+    for (int k = 0; k < n; ++k) {
+        sm_eiso *h = hs[k];
+        P.f[k] = h->slab_maps[h->cur].f;
+        P.a[k] = h->args;
+        P.gx[k] = ((h->NZ + 29) / 30 + 1) / 2;
+        P.gy[k] = (h->NX + 7) / 8;
+        P.first[k] = total;
+        total += P.gx[k] * P.gy[k] * (int)h->nshots;
+    }
+    P.first[n] = total;
+    P.n = n;
+    eiso_group_step_kernel<S, 2, 8, 8><<<total, 64, L::bytes, st>>>(P);
+    int nsrc = 0, nrec = 0;
+    for (int k = 0; k < n; ++k) {
+        sm_eiso *h = hs[k];
+        h->cur = 1 - h->cur;
+        eiso_bind(h);
+        EisoPost &q = Q.q[k];
+        for (int f = 0; f < 5; ++f) {
+            q.f[f] = h->args.f[f];
+            q.sc[f] = h->args.sc[f];
+            q.isc[f] = h->args.isc[f];
+        }
+        q.fstride = h->args.fstride;
+        q.step = h->args.step;
+        q.src = h->d_src.as<SrcEntry>();
+        q.src_first = h->d_src_first.as<int>();
+        q.vals = h->d_vals.as<double>();
+        q.rec = h->d_rec.as<RecEntry>();
+        q.table = h->d_table.as<int32_t>();
+        q.nsteps_max = h->table_steps;
+        q.traces = h->d_traces.as<double>();
+        Q.first_src[k] = nsrc;
+        Q.first_rec[k] = nrec;
+        nsrc += h->d_src.bytes ? (int)h->nshots : 0;
+        nrec += h->n_rec_total;
+    }
+    Q.first_src[n] = nsrc;
+    Q.first_rec[n] = nrec;
+    Q.n = n;
+    if (nsrc) eiso_group_source_kernel<S><<<(nsrc + 127) / 128, 128, 0, st>>>(Q);
+    if (nrec) eiso_group_gather_kernel<S><<<(nrec + 127) / 128, 128, 0, st>>>(Q);
+    hs[0]->timer.launches += 1 + (nsrc ? 1 : 0) + (nrec ? 1 : 0);
+    SM_CUDA_TRY(cudaGetLastError());
+    return SM_OK;
+}
+
+// CUDA graphs of kGroupGraphSteps grouped steps, cached per group: the key
+// holds each handle's serial, starting buffer set and graph epoch (sources,
+// receivers, scales), so a graph is only replayed on the state it was
+// captured for.  A few are kept, the least recently used dropped.
+constexpr int kGroupGraphSteps = 16;
+constexpr size_t kGroupGraphCache = 8;
+
+struct GroupGraphKey {
+    int device;
+    std::vector<std::tuple<uint64_t, int, unsigned>> members;
+    bool operator<(const GroupGraphKey &o) const {
+        return std::tie(device, members) < std::tie(o.device, o.members);
+    }
+};
+struct GroupGraph {
+    cudaGraphExec_t exec = nullptr;
+    uint64_t used = 0;
+};
+std::mutex g_group_mu;
+std::map<GroupGraphKey, GroupGraph> g_group_graphs;
+uint64_t g_group_clock = 0;
+
+template <typename S>
+int eiso_group_steps(sm_eiso *const *hs, int n, int steps) {
+    for (int s = 0; s < steps; ++s)
+        for (int k0 = 0; k0 < n; k0 += kGroupMax)
+            if (int rc = eiso_group_step<S>(hs + k0, std::min(kGroupMax, n - k0), hs[0]->stream))
+                return rc;
+    return SM_OK;
+}
+
+template <typename S>
+int eiso_group_graph(sm_eiso *const *hs, int n, cudaGraphExec_t *out) {
+    GroupGraphKey key{hs[0]->device, {}};
+    for (int k = 0; k < n; ++k) key.members.emplace_back(hs[k]->serial, hs[k]->cur, hs[k]->graph_epoch);
+    std::lock_guard<std::mutex> lk(g_group_mu);
+    auto it = g_group_graphs.find(key);
+    if (it != g_group_graphs.end()) {
+        it->second.used = ++g_group_clock;
+        *out = it->second.exec;
+        return SM_OK;
+    }
+    const size_t launches = hs[0]->timer.launches;
+    SM_CUDA_TRY(cudaStreamBeginCapture(hs[0]->stream, cudaStreamCaptureModeThreadLocal));
+    const int rc = eiso_group_steps<S>(hs, n, kGroupGraphSteps);
+    cudaGraph_t graph = nullptr;
+    cudaError_t e = cudaStreamEndCapture(hs[0]->stream, &graph);
+    hs[0]->timer.launches = launches;
+    for (int k = 0; k < n; ++k) eiso_bind(hs[k]);   // an even number of steps: sets as before
+    if (rc) {
+        if (graph) cudaGraphDestroy(graph);
+        return rc;
+    }
+    if (e != cudaSuccess) return sm_fail(SM_ECUDA, "stream capture: %s", cudaGetErrorString(e));
+    cudaGraphExec_t exec = nullptr;
+    e = cudaGraphInstantiate(&exec, graph, 0);
+    cudaGraphDestroy(graph);
+    if (e != cudaSuccess) return sm_fail(SM_ECUDA, "cudaGraphInstantiate: %s", cudaGetErrorString(e));
+    if (g_group_graphs.size() >= kGroupGraphCache) {
+        auto old = g_group_graphs.begin();
+        for (auto i = g_group_graphs.begin(); i != g_group_graphs.end(); ++i)
+            if (i->second.used < old->second.used) old = i;
+        // some stream may still run it: wait before the executable goes
+        cudaDeviceSynchronize();
+        cudaGraphExecDestroy(old->second.exec);
+        g_group_graphs.erase(old);
+    }
+    g_group_graphs[key] = GroupGraph{exec, ++g_group_clock};
+    *out = exec;
+    return SM_OK;
+}
+
+template <typename S>
+int eiso_group_run_t(sm_eiso *const *hs, int n, size_t nsteps) {
+    using L = ESlabG<S, 2, 8>;
+    for (int k = 0; k < n; ++k)
+        if (int rc = eiso_make_slab_maps<S, L, (1 << 20) + 2 * 4096 + 8>(hs[k])) return rc;
+    if (int rc = allow_smem(eiso_group_step_kernel<S, 2, 8, 8>, L::bytes, hs[0]->device))
+        return rc;
+    const bool is16 = eiso_is16(hs[0]);
+    const size_t G = kGroupGraphSteps;
+    int per_step = 1;
+    for (int k0 = 0; k0 < n; k0 += kGroupMax) {
+        bool src = false, rec = false;
+        for (int k = k0; k < std::min(n, k0 + kGroupMax); ++k) {
+            src = src || hs[k]->d_src.bytes;
+            rec = rec || hs[k]->n_rec_total;
+        }
+        per_step += (k0 ? 1 : 0) + (src ? 1 : 0) + (rec ? 1 : 0);
+    }
+    while (nsteps > 0) {
+        // a graph of G steps when no handle rescales inside it
+        bool aligned = true;
+        for (int k = 0; k < n && is16; ++k) aligned = aligned && hs[k]->it % G == 0;
+        size_t done;
+        if (nsteps >= G && aligned) {
+            cudaGraphExec_t ex = nullptr;
+            if (int rc = eiso_group_graph<S>(hs, n, &ex)) return rc;
+            SM_CUDA_TRY(cudaGraphLaunch(ex, hs[0]->stream));
+            hs[0]->timer.launches += per_step * G;
+            done = G;
+        } else {
+            if (int rc = eiso_group_steps<S>(hs, n, 1)) return rc;
+            done = 1;
+        }
+        nsteps -= done;
+        for (int k = 0; k < n; ++k) {
+            sm_eiso *h = hs[k];
+            const size_t before = h->it;
+            h->it += done;
+            if (is16 && h->it / sm_eiso::kScalePeriod != before / sm_eiso::kScalePeriod)
+                if (int rc = eiso_rescale(h)) return rc;
+        }
+    }
+    return SM_OK;
+}
+
+}  // namespace
+
+// Several e_iso handles of different grid sizes advanced together: every step
+// is one launch over all their slabs (up to 32 handles per launch), one for
+// all their sources and one for all their receivers.  Each handle ends where
+// sm_eiso_run(h, nsteps) would have left it, bit for bit.  The work runs on
+// the first handle's stream, ordered after the work already queued on every
+// handle's stream; every handle's stream waits for it to finish.
+extern "C" int sm_eiso_group_run(sm_eiso_t const *handles, int n, size_t nsteps) {
+    if (!handles || n <= 0) return sm_fail(SM_EINVAL, "sm_eiso_group_run: no handles");
+    for (int k = 0; k < n; ++k) {
+        if (int rc = eiso_check(handles[k])) return rc;
+        if (handles[k]->device != handles[0]->device ||
+            handles[k]->precision != handles[0]->precision)
+            return sm_fail(SM_EINVAL,
+                           "sm_eiso_group_run: handle %d differs in device or precision from "
+                           "handle 0", k);
+        for (int j = 0; j < k; ++j)
+            if (handles[j] == handles[k])
+                return sm_fail(SM_EINVAL, "sm_eiso_group_run: handle %d appears twice", k);
+    }
+    if (nsteps == 0) return SM_OK;
+    sm_eiso *const *hs = handles;
+    DeviceGuard g(hs[0]->device);
+    for (int k = 0; k < n; ++k) {
+        if (hs[k]->src_dirty)
+            if (int rc = upload_sources(hs[k])) return rc;
+        if (hs[k]->rec_dirty)
+            if (int rc = upload_receivers(hs[k])) return rc;
+    }
+    // run every handle on the first handle's stream for the duration
+    const cudaStream_t st = hs[0]->stream;
+    std::vector<cudaStream_t> own(n);
+    cudaEvent_t ev = nullptr;
+    SM_CUDA_TRY(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+    for (int k = 1; k < n; ++k) {
+        cudaEventRecord(ev, hs[k]->stream);
+        cudaStreamWaitEvent(st, ev, 0);
+    }
+    for (int k = 0; k < n; ++k) {
+        own[k] = hs[k]->stream;
+        hs[k]->stream = st;
+    }
+    int rc;
+    switch (hs[0]->precision) {
+    case SM_FP64: rc = eiso_group_run_t<double>(hs, n, nsteps); break;
+    case SM_FP16: rc = eiso_group_run_t<__half>(hs, n, nsteps); break;
+    case SM_BF16: rc = eiso_group_run_t<__nv_bfloat16>(hs, n, nsteps); break;
+    default: rc = eiso_group_run_t<float>(hs, n, nsteps); break;
+    }
+    for (int k = 0; k < n; ++k) hs[k]->stream = own[k];
+    cudaEventRecord(ev, st);
+    for (int k = 1; k < n; ++k) cudaStreamWaitEvent(hs[k]->stream, ev, 0);
+    cudaEventDestroy(ev);
     if (rc) return rc;
     SM_CUDA_TRY(cudaGetLastError());
     return SM_OK;

@@ -70,6 +70,7 @@ struct sm_server {
     int device = 0;
     size_t budget = 0, used = 0, peak = 0;
     int max_active = 64, slice = 64, graph = 0;
+    bool group = false;   // e_iso requests stepped together (sm_eiso_group_run)
     std::mutex mu;
     std::condition_variable cv;        // request finished / new request
     std::deque<std::shared_ptr<Req>> queue;
@@ -164,6 +165,28 @@ int feed(sm_server *s, Req &r) {
     return SM_OK;
 }
 
+// grouped mode: every running e_iso request of one precision that wants a
+// slice gets it from one sm_eiso_group_run call (one launch per step over
+// all of their grids); the slice is as long as the shortest remainder
+int feed_group(sm_server *s, std::vector<Req *> &grp) {
+    size_t k = (size_t)s->slice;
+    for (Req *r : grp) k = std::min(k, r->nsteps - r->enqueued);
+    std::vector<sm_eiso_t> hs;
+    for (Req *r : grp) hs.push_back(r->he);
+    if (int rc = sm_eiso_group_run(hs.data(), (int)hs.size(), k)) return rc;
+    for (Req *r : grp) {
+        cudaEvent_t ev = nullptr;
+        if (cudaEventCreateWithFlags(&ev, cudaEventDisableTiming) != cudaSuccess ||
+            cudaEventRecord(ev, r->stream) != cudaSuccess) {
+            if (ev) cudaEventDestroy(ev);
+            return sm_fail(SM_ECUDA, "server: event record failed");
+        }
+        r->slices.push_back(ev);
+        r->enqueued += k;
+    }
+    return SM_OK;
+}
+
 // copy a finished request's traces to the host
 int collect(Req &r) {
     std::vector<size_t> cnt(r.nrec, 0);
@@ -220,14 +243,36 @@ void work(sm_server *s) {
             std::lock_guard<std::mutex> lk(s->mu);
             run = s->running;
         }
+        std::map<Req *, int> grc;   // grouped feed failures
+        if (s->group) {
+            std::map<int, std::vector<Req *>> need;   // by precision
+            for (auto &r : run) {
+                while (!r->slices.empty() && cudaEventQuery(r->slices.front()) == cudaSuccess) {
+                    cudaEventDestroy(r->slices.front());
+                    r->slices.pop_front();
+                    progress = true;
+                }
+                if (r->kind == 0 && r->enqueued < r->nsteps && r->slices.size() < 2)
+                    need[r->e.precision].push_back(r.get());
+            }
+            for (auto &g : need) {
+                const int rc = feed_group(s, g.second);
+                if (rc)
+                    for (Req *r : g.second) grc[r] = rc;
+                progress = true;
+            }
+        }
         for (auto &r : run) {
             int rc = SM_OK;
+            auto gf = grc.find(r.get());
+            if (gf != grc.end()) rc = gf->second;
             while (!r->slices.empty() && cudaEventQuery(r->slices.front()) == cudaSuccess) {
                 cudaEventDestroy(r->slices.front());
                 r->slices.pop_front();
                 progress = true;
             }
-            while (rc == SM_OK && r->enqueued < r->nsteps && r->slices.size() < 2) {
+            while (rc == SM_OK && !(s->group && r->kind == 0) && r->enqueued < r->nsteps &&
+                   r->slices.size() < 2) {
                 rc = feed(s, *r);
                 progress = true;
             }
@@ -514,6 +559,14 @@ extern "C" int sm_server_get_stats(sm_server_t s, sm_server_stats *st) {
     st->hbm_budget = s->budget;
     st->hbm_peak = s->peak;
     st->max_running = s->max_running;
+    return SM_OK;
+}
+
+extern "C" int sm_server_set_group(sm_server_t s, int on) {
+    if (!s) return sm_fail(SM_EINVAL, "sm_server_set_group: null server");
+    std::lock_guard<std::mutex> lk(s->mu);
+    if (s->submitted) return sm_fail(SM_ESTATE, "sm_server_set_group: requests already submitted");
+    s->group = on != 0;
     return SM_OK;
 }
 

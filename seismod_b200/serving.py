@@ -62,6 +62,7 @@ _SIGS = {
     "sm_server_release": (C.c_int, [C.c_void_p, C.c_uint64]),
     "sm_server_get_stats": (C.c_int, [C.c_void_p, C.POINTER(ServerStats)]),
     "sm_server_destroy": (C.c_int, [C.c_void_p]),
+    "sm_server_set_group": (C.c_int, [C.c_void_p, C.c_int]),
     "sm_server_struct_sizes": (C.c_int, [_szp, _szp, _szp]),
     "sm_eiso_device_bytes": (C.c_int, [_sz, _sz, _sz, C.c_int, _sz, _sz, _sz, _szp]),
     "sm_a3d_device_bytes": (C.c_int, [_sz, _sz, _sz, _sz, C.c_int, _sz, _sz, _szp]),
@@ -142,12 +143,15 @@ def a3d_request(p, precision="fp32"):
 class Server:
     """A request loop on one GPU (sm_server_*)."""
 
-    def __init__(self, device=0, hbm_budget=0, max_active=0, slice_steps=0, graph_steps=0):
+    def __init__(self, device=0, hbm_budget=0, max_active=0, slice_steps=0, graph_steps=0,
+                 group=False):
         h = C.c_void_p()
         L.check(lib().sm_server_create(device, hbm_budget, max_active, slice_steps, graph_steps,
                                        C.byref(h)))
         self._h = h
         self._nrec = {}
+        if group:
+            L.check(lib().sm_server_set_group(h, 1))
 
     def close(self):
         if getattr(self, "_h", None) and self._h.value:

@@ -145,6 +145,24 @@ def test_every_launch_config_batched_shots_identical():
     dev.close()
 
 
+def test_every_launch_config_16bit_storage_identical():
+    """16-bit storage: every launch configuration gives the same bits,
+    through the power-of-two rescales (every 16 steps) and the source."""
+    p = W.cfg2(nx=150, nz=130, npml=9, nsteps=90, nshots=3, nrec=12)
+    dev, n = api.eiso_device(p, "fp16")
+    nconf = dev.get_config()[1]
+    dev.run(n)
+    ref = [dev.traces(s) for s in range(3)]
+    for config in range(nconf):
+        dev.reset()
+        dev.set_config(config)
+        dev.run(n)
+        for s in range(3):
+            for x, y in zip(dev.traces(s), ref[s]):
+                np.testing.assert_array_equal(x, y, err_msg=f"config {config} shot {s}")
+    dev.close()
+
+
 def test_batched_shots_equal_single_shots():
     p = W.cfg2(nx=120, nz=80, npml=10, nsteps=250, nshots=5, nrec=12)
     batch = api.run_eiso(p, "fp32")

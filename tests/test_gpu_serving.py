@@ -30,10 +30,15 @@ def _same(a, b):
         np.testing.assert_array_equal(x, y)
 
 
-@pytest.mark.parametrize("precision,graph", [("fp32", 0), ("fp32", 16), ("fp16", 16)])
-def test_results_in_the_mix_equal_results_alone(precision, graph):
+@pytest.mark.parametrize("precision,graph,group", [("fp32", 0, False), ("fp32", 16, False),
+                                                   ("fp16", 16, False), ("fp32", 16, True),
+                                                   ("fp16", 0, True)])
+def test_results_in_the_mix_equal_results_alone(precision, graph, group):
+    """With group=True the running e_iso requests are stepped together, one
+    launch per step over their uneven grids; results stay those of each shot
+    alone."""
     mix = _mix()
-    srv = serving.Server(max_active=4, slice_steps=32, graph_steps=graph)
+    srv = serving.Server(max_active=4, slice_steps=32, graph_steps=graph, group=group)
     tickets = [srv.submit(k, p, precision) for k, p in mix]
     srv.drain(timeout=300)
     st = srv.stats()
