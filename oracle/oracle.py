@@ -83,6 +83,26 @@ def _load():
     return lib
 
 
+def _load_ecyl(lib):
+    lib.orc_ecyl_materials.restype = C.c_double
+    lib.orc_ecyl_materials.argtypes = [_sz, _sz] + [_dp] * 11
+    lib.orc_ecyl_cpml.argtypes = [_sz] + [C.c_double] * 8 + [C.c_int, C.POINTER(_dp)]
+    lib.orc_ecyl_kurkjian.restype = _sz
+    lib.orc_ecyl_kurkjian.argtypes = [C.c_double] * 7 + [C.c_int, _sz, _dp]
+    lib.orc_ecyl_new.restype = C.c_void_p
+    lib.orc_ecyl_new.argtypes = [_sz, _sz, _sz, C.c_int, C.c_double, C.c_double, C.c_double,
+                                 C.POINTER(_dp), C.POINTER(_dp)]
+    lib.orc_ecyl_free.argtypes = [C.c_void_p]
+    lib.orc_ecyl_velocity.argtypes = [C.c_void_p]
+    lib.orc_ecyl_stress.argtypes = [C.c_void_p]
+    lib.orc_ecyl_force.argtypes = [C.c_void_p, _sz, C.c_int, C.c_double]
+    lib.orc_ecyl_kurkjian_add.argtypes = [C.c_void_p, _sz, C.c_double]
+    lib.orc_ecyl_get.argtypes = [C.c_void_p, C.c_int, _dp]
+    lib.orc_ecyl_set.argtypes = [C.c_void_p, C.c_int, _dp]
+    lib.orc_ecyl_probe.restype = C.c_double
+    lib.orc_ecyl_probe.argtypes = [C.c_void_p, C.c_int, _sz]
+
+
 _LIB = None
 
 
@@ -90,6 +110,7 @@ def lib():
     global _LIB
     if _LIB is None:
         _LIB = _load()
+        _load_ecyl(_LIB)
     return _LIB
 
 
@@ -249,6 +270,83 @@ class A3D:
 
     def probe(self, field, index):
         return lib().orc_a3d_probe(self.h_, FIELDS_A[field], int(index))
+
+
+# ----------------------------------------------------------------------------
+# e_cyl_iso
+# ----------------------------------------------------------------------------
+
+FIELDS_C = {"vr": 0, "vt": 1, "vz": 2, "trr": 3, "ttt": 4, "tzz": 5, "trz": 6, "trt": 7,
+            "ttz": 8, "div": 9, "curl": 10}
+ECYL_MATS = ("lij", "l2mij", "mu", "mui", "muj", "bi", "bj", "bij")
+ECYL_SRC = {"Bulk": 6, "Fr": 9, "Ftheta": 10, "Fz": 11, "Kurkjian": 12}
+
+
+def ecyl_materials(vp, vs, rho):
+    """Padded (nx2, nz2) models -> (dict of the 8 averaged materials, vpmax)."""
+    vp, vs, rho = (np.ascontiguousarray(a, dtype=np.float64) for a in (vp, vs, rho))
+    out = {k: np.zeros(vp.shape) for k in ECYL_MATS}
+    vmax = lib().orc_ecyl_materials(vp.shape[0], vp.shape[1], _ptr(vp), _ptr(vs), _ptr(rho),
+                                    *[_ptr(out[k]) for k in ECYL_MATS])
+    return out, vmax
+
+
+def ecyl_cpml(npml, dx, dz, dt, order=2.0, vmax=5000.0, Rc=1e-5, kappa_max=1.0,
+              alpha_max=0.0, absorb=1):
+    """The 15 coefficient arrays of pml.c:2107-2185 (9 of npml, 6 of npml+1)."""
+    arrs = [np.zeros(npml if k < 9 else npml + 1) for k in range(15)]
+    ptrs = (_dp * 15)(*[_ptr(a) for a in arrs])
+    lib().orc_ecyl_cpml(npml, dx, dz, dt, order, vmax, Rc, kappa_max, alpha_max, int(absorb),
+                        ptrs)
+    return arrs
+
+
+def ecyl_kurkjian(A, f, dt, lij_at_src, x_src, dx, dz, n):
+    maxlen = int(np.ceil(2.0 / f / dt)) + 2
+    out = np.zeros(maxlen)
+    k = lib().orc_ecyl_kurkjian(A, f, dt, lij_at_src, x_src, dx, dz, int(n), maxlen, _ptr(out))
+    return out[:k].copy()
+
+
+class ECyl:
+    """FP64 e_cyl_iso state: padded nx2 = nx + npml by nz2 = nz + 2 npml."""
+
+    def __init__(self, nx, nz, npml, n, dx, dz, dt, mats, coef):
+        self.shape = (nx + npml, nz + 2 * npml)
+        self._mats = [np.ascontiguousarray(mats[k], dtype=np.float64) for k in ECYL_MATS]
+        self._coef = [np.ascontiguousarray(c, dtype=np.float64) for c in coef]
+        mp = (_dp * 8)(*[_ptr(a) for a in self._mats])
+        cp = (_dp * 15)(*[_ptr(a) for a in self._coef])
+        self.h_ = lib().orc_ecyl_new(nx, nz, npml, int(n), dx, dz, dt, mp, cp)
+
+    def __del__(self):
+        if getattr(self, "h_", None):
+            lib().orc_ecyl_free(self.h_)
+            self.h_ = None
+
+    def velocity(self):
+        lib().orc_ecyl_velocity(self.h_)
+
+    def stress(self):
+        lib().orc_ecyl_stress(self.h_)
+
+    def force(self, index, typ, value):
+        lib().orc_ecyl_force(self.h_, int(index), int(typ), float(value))
+
+    def kurkjian(self, index, value):
+        lib().orc_ecyl_kurkjian_add(self.h_, int(index), float(value))
+
+    def get(self, field):
+        out = np.zeros(self.shape)
+        lib().orc_ecyl_get(self.h_, FIELDS_C[field], _ptr(out))
+        return out
+
+    def set(self, field, arr):
+        a = np.ascontiguousarray(arr, dtype=np.float64)
+        lib().orc_ecyl_set(self.h_, FIELDS_C[field], _ptr(a))
+
+    def probe(self, comp, index):
+        return lib().orc_ecyl_probe(self.h_, FIELDS_C[comp], int(index))
 
 
 # ----------------------------------------------------------------------------

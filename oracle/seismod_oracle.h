@@ -10,6 +10,9 @@
  *              PML; e_iso.c:423-670, propagate.c:2511-2670, pml.c:39-1403)
  *   a_iso_3d  (3D acoustic, velocity-pressure staggered grid, CPML;
  *              a_iso_3d/a_iso_3d.c:368-693)
+ *   e_cyl_iso (2.5-D elastic in r, z with azimuthal mode n, CPML;
+ *              e_cyl_iso.c:363-790, propagate.c:2706-4118, pml.c:2107-2185;
+ *              oracle_ecyl.c)
  * plus the host-side set-up they share (src.c:43-65,170-184;
  * io_utils.c:892-947,1029-1153,1744-1768).
  *
@@ -108,6 +111,40 @@ void orc_a3d_add_source(orc_a3d *o, size_t index, double value); /* :689-693 */
 void orc_a3d_get(const orc_a3d *o, int field, double *out);
 void orc_a3d_set(orc_a3d *o, int field, const double *in);
 double orc_a3d_probe(const orc_a3d *o, int field, size_t index);
+
+/* ---------------- e_cyl_iso (oracle_ecyl.c) ---------------- */
+
+/* padded grid nx2 = nx + np (PML at the outer radius only) by
+ * nz2 = nz + 2 np, index i*nz2 + j.  Fields: */
+enum { ORC_C_VR = 0, ORC_C_VT, ORC_C_VZ, ORC_C_TRR, ORC_C_TTT, ORC_C_TZZ, ORC_C_TRZ,
+       ORC_C_TRT, ORC_C_TTZ, ORC_C_DIV, ORC_C_CURL };
+/* source types, numbered as enum sourceType (structs.h:44) */
+enum { ORC_C_SRC_BULK = 6, ORC_C_SRC_FR = 9, ORC_C_SRC_FT = 10, ORC_C_SRC_FZ = 11,
+       ORC_C_SRC_KURKJIAN = 12 };
+typedef struct orc_ecyl orc_ecyl;
+/* e_cyl_iso.c:363-441 on the padded model; returns max vp */
+double orc_ecyl_materials(size_t nx2, size_t nz2, const double *vp, const double *vs,
+                          const double *rho, double *lij, double *l2mij, double *mu,
+                          double *mui, double *muj, double *bi, double *bj, double *bij);
+/* pml.c:2107-2185; c: 15 arrays ik_r ik_z ikh_z b_r c_r b_z c_z bh_z ch_z
+ * (np values) then ikH_r ikH_z bH_r cH_r bH_z cH_z (np + 1 values) */
+void orc_ecyl_cpml(size_t np, double dx, double dz, double dt, double order, double vmax,
+                   double Rc, double kappa_max, double alpha_max, int absorb,
+                   double *const *c);
+/* src.c:202-228 compute_kurkjian; returns the sample count */
+size_t orc_ecyl_kurkjian(double A, double f, double dt, double lij_at_src, double x_src,
+                         double dx, double dz, int n, size_t maxlen, double *fct);
+/* mat: lij l2mij mu mui muj bi bj bij (padded); coef as orc_ecyl_cpml */
+orc_ecyl *orc_ecyl_new(size_t nx, size_t nz, size_t np, int n, double dx, double dz, double dt,
+                       const double *const *mat, const double *const *coef);
+void orc_ecyl_free(orc_ecyl *o);
+void orc_ecyl_velocity(orc_ecyl *o);       /* vr, vt, vz */
+void orc_ecyl_stress(orc_ecyl *o);         /* trr ttt tzz, trz, trt, ttz */
+void orc_ecyl_force(orc_ecyl *o, size_t index, int type, double value);   /* src.c:186-199 */
+void orc_ecyl_kurkjian_add(orc_ecyl *o, size_t index, double value);     /* src.c:231-236 */
+void orc_ecyl_get(const orc_ecyl *o, int field, double *out);
+void orc_ecyl_set(orc_ecyl *o, int field, const double *in);
+double orc_ecyl_probe(const orc_ecyl *o, int comp, size_t index);         /* with div, curl */
 
 #ifdef __cplusplus
 }

@@ -14,6 +14,9 @@ The formats are the ones the reference programs read and write:
                    coordinates`` (io_utils.c:1432-1589).
 * output file      ``nrec`` then per record ``comp / Trace / coordinates /
                    t0 (s) / dt (ms)`` (io_utils.c:1592-1741).
+* e_cyl_iso model  ``nr nz / dr dz / r0 z0 / isotropic_elastic_cyl`` then
+                   ``vp vs rho`` per node, r fast within each z row; a single
+                   row is a radial profile (io_utils.c:949-1027).
 * trace file       ``trc/<base>/<base>_<n>.trc``: ``"%le    %le"`` of time
                    and 1e3 * velocity (io_utils.c:1744-1768).
 * binary model     this package's own: the same model values without text
@@ -68,6 +71,19 @@ def write_model_e_1d(path, nx, vp, vs, rho, dx, x0=0.0, z0=0.0):
     with open(path, "w") as f:
         f.write(f"{nx} {nz}\n{_num(dx)} {_num(dx)}\n{_num(x0)} {_num(z0)}\nisotropic_elastic\n")
         _write_rows(f, (vp, vs, rho))
+
+
+def write_model_ecyl(path, vp, vs, rho, dx, dz, x0=0.0, z0=0.0, profile_1d=False):
+    """e_cyl_iso model (io_utils.c:949-1027): ``nr nz / dr dz / r0 z0 /
+    isotropic_elastic_cyl`` then ``vp vs rho`` per node, r fastest within
+    each z row; with profile_1d only the first row (a radial profile, copied
+    down every row by the reader)."""
+    nx, nz = vp.shape
+    with open(path, "w") as f:
+        f.write(f"{nx} {nz}\n{_num(dx)} {_num(dz)}\n{_num(x0)} {_num(z0)}\nisotropic_elastic_cyl\n")
+        rows = 1 if profile_1d else nz
+        for j in range(rows):
+            _write_rows(f, (vp[:, j], vs[:, j], rho[:, j]))
 
 
 def write_model_a(path, vp, rho, d, origin=(0.0, 0.0, 0.0)):

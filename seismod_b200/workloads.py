@@ -80,6 +80,89 @@ class EIsoProblem:
 
 
 @dataclasses.dataclass
+class ECylProblem:
+    """One e_cyl_iso run: radial (r) by vertical (z) model, azimuthal mode n."""
+    vp: np.ndarray                 # (nx, nz) m/s, r slow, z fast
+    vs: np.ndarray
+    rho: np.ndarray
+    dx: float                      # radial step, m
+    dz: float
+    npml: int
+    dt_ms: float
+    duration: float
+    sources: list                  # (type, A, f, r, z); type Fr Fz Ftheta Bulk Kurkjian
+    receivers: list                # (comp, r, z, t0_s, rdt_ms)
+    n: int = 0                     # azimuthal mode
+    absorb: int = 1                # the .par "abs" flag
+    Rc: float = 1e-5
+    kappa_max: float = 1.0
+    alpha_max: int = 1
+    x0: float = 0.0
+    z0: float = 0.0
+    name: str = "ecyl"
+
+    @property
+    def nx(self):
+        return self.vp.shape[0]
+
+    @property
+    def nz(self):
+        return self.vp.shape[1]
+
+    @property
+    def dt(self):
+        return self.dt_ms * 0.001
+
+    @property
+    def np_used(self):
+        """PML width the programs use: abs 0 sets it to zero (io_utils.c:293)."""
+        return self.npml if self.absorb else 0
+
+    @property
+    def cells(self):
+        return (self.nx + self.np_used) * (self.nz + 2 * self.np_used)
+
+    def write(self, workdir, basename=None, profile_1d=False, **par_extra):
+        """The reference's input files; returns the .par path."""
+        os.makedirs(workdir, exist_ok=True)
+        base = basename or self.name
+        formats.write_model_ecyl(os.path.join(workdir, "model.dat"), self.vp, self.vs, self.rho,
+                                 self.dx, self.dz, self.x0, self.z0, profile_1d=profile_1d)
+        formats.write_src(os.path.join(workdir, "src.dat"), self.sources)
+        formats.write_rcv(os.path.join(workdir, "rcv.dat"),
+                          [(c, (x, z), t0, r) for (c, x, z, t0, r) in self.receivers])
+        par = os.path.join(workdir, "run.par")
+        extra = dict(Rc=self.Rc, kappa_max=self.kappa_max, alpha_max=self.alpha_max,
+                     azimuthal_mode=self.n)
+        extra.update(par_extra)
+        formats.write_par(par, "model.dat", "src.dat", "rcv.dat", base, self.duration,
+                          self.dt_ms, abs_=self.absorb, nl=self.npml, **extra)
+        return par
+
+
+def ecyl_case(nx=120, nz=160, npml=12, nsteps=300, n=0, src="Fz", seed=5, nrec=12,
+              dx=1.0, dz=1.0, comps=("Vr", "Vz"), absorb=1):
+    """A seeded layered cylindrical model (vp per layer, vs = vp/1.73,
+    Gardner density), one source at r = 0.3 nx dr, z = 0.45 nz dz, receivers
+    along the radius three cells below the source, components cycling
+    through `comps`."""
+    vp1 = random_layers_1d(nz, seed, vmin=1800.0, vmax=4200.0, min_thick=8)
+    vp = vp1[None, :].repeat(nx, 0)
+    vs = vp / 1.73
+    rho = gardner(vp)
+    dt_ms = 0.5 * 0.5 * (dx + dz) / (math.sqrt(2.0) * float(vp.max())) * 1e3
+    A = 1.0e-6 if src == "Kurkjian" else 1.0
+    sources = [(src, A, 60.0, round(0.3 * nx) * dx, round(0.45 * nz) * dz)]
+    recs = []
+    for k in range(nrec):
+        comp = comps[k % len(comps)]
+        recs.append((comp, (2 + k * (nx - 4) // max(nrec - 1, 1)) * dx,
+                     (round(0.45 * nz) + 3) * dz, 0.0, dt_ms))
+    return ECylProblem(vp, vs, rho, dx, dz, npml, dt_ms, steps_duration(nsteps, dt_ms),
+                       sources, recs, n=n, absorb=absorb, name="ecyl")
+
+
+@dataclasses.dataclass
 class A3DProblem:
     vp: np.ndarray                 # (nx, ny, nz) m/s
     rho: np.ndarray

@@ -3,10 +3,11 @@
 Run in a container where the reference sources are present, after
 ``make -C oracle`` has built oracle/_ref/:
 
-    python tests/golden/make_golden.py
+    python tests/golden/make_golden.py          # every fixture
+    python tests/golden/make_golden.py ecyl     # the e_cyl_iso ones only
 
 Each case is a small seeded problem.  The reference program (e_iso,
-e_iso_lrfix for nx > nz, or a_iso_3d) runs it from its own input files and
+e_iso_lrfix for nx > nz, a_iso_3d, or e_cyl_iso_serial) runs it from its own input files and
 the traces it writes are stored, together with the complete problem, in
 tests/golden/<case>.npz.  The tests rebuild the problem from the fixture, so
 nothing at test time needs the reference.
@@ -83,6 +84,36 @@ def a3d_cases():
     return cases
 
 
+ECYL_COMPS = ("Vr", "Vz", "Vtheta", "trr", "tzz", "trz", "trtheta", "tthetatheta", "tthetaz",
+              "div", "curl")
+
+
+def ecyl_cases():
+    """e_cyl_iso, run by the reference built without OpenMP (its force
+    sources are added once per thread under OpenMP, see oracle/Makefile)."""
+    cases = {}
+    p = W.ecyl_case(nx=48, nz=56, npml=8, nsteps=220, n=0, src="Fz", nrec=22, comps=ECYL_COMPS,
+                    seed=21)
+    p.name = "ecyl_m0"
+    cases[p.name] = p
+    q = W.ecyl_case(nx=44, nz=60, npml=7, nsteps=200, n=1, src="Kurkjian", nrec=22,
+                    comps=ECYL_COMPS, seed=22)
+    q.name = "ecyl_m1_kurkjian"
+    cases[q.name] = q
+    r = W.ecyl_case(nx=40, nz=50, npml=6, nsteps=200, n=2, src="Bulk", nrec=11,
+                    comps=ECYL_COMPS, seed=23, dx=1.5, dz=1.0)
+    r.alpha_max, r.kappa_max, r.Rc = 0, 1.5, 1e-4
+    r.receivers = [(c, x, z, 0.002 if k % 3 == 0 else 0.0, (2 if k % 2 else 1) * rdt)
+                   for k, (c, x, z, t0, rdt) in enumerate(r.receivers)]
+    r.name = "ecyl_m2_bulk"
+    cases[r.name] = r
+    u = W.ecyl_case(nx=36, nz=40, npml=6, nsteps=160, n=0, src="Fr", nrec=11, comps=ECYL_COMPS,
+                    seed=24, absorb=0)
+    u.name = "ecyl_noabs"
+    cases[u.name] = u
+    return cases
+
+
 def _save(path, p, kind, program, t, v):
     meta = dict(kind=kind, program=program, name=p.name, npml=p.npml, dt_ms=p.dt_ms,
                 duration=p.duration)
@@ -90,6 +121,11 @@ def _save(path, p, kind, program, t, v):
                   ref_n=np.array([len(a) for a in v], dtype=np.int64))
     if kind == "eiso":
         meta.update(h=p.h, x0=p.x0, z0=p.z0, shots=p.shots[:1], receivers=p.receivers)
+        arrays.update(vp=p.vp, vs=p.vs, rho=p.rho)
+    elif kind == "ecyl":
+        meta.update(dx=p.dx, dz=p.dz, x0=p.x0, z0=p.z0, sources=p.sources,
+                    receivers=p.receivers, n=p.n, absorb=p.absorb, Rc=p.Rc,
+                    kappa_max=p.kappa_max, alpha_max=p.alpha_max)
         arrays.update(vp=p.vp, vs=p.vs, rho=p.rho)
     else:
         meta.update(d=list(p.d), origin=list(p.origin), sources=p.sources,
@@ -120,10 +156,24 @@ def make_segy_fixture():
     print(f"{p.name}: a_iso_3d segy -> {sgy.size} bytes")
 
 
+def make_ecyl_fixtures():
+    for name, p in ecyl_cases().items():
+        d = tempfile.mkdtemp(prefix="golden_")
+        par = p.write(d)
+        O.run_reference("e_cyl_iso_serial", par, d)
+        t, v = F.read_traces(d, p.name, len(p.receivers))
+        _save(os.path.join(HERE, f"{name}.npz"), p, "ecyl", "e_cyl_iso_serial", t, v)
+        print(f"{name}: e_cyl_iso_serial -> {[len(a) for a in v]}")
+
+
 def main():
     if not O.ref_available():
         O.build()
+    if sys.argv[1:] == ["ecyl"]:   # only the e_cyl_iso fixtures
+        make_ecyl_fixtures()
+        return
     make_segy_fixture()
+    make_ecyl_fixtures()
     for name, (p, prog) in {**eiso_cases(), **a3d_cases()}.items():
         d = tempfile.mkdtemp(prefix="golden_")
         if prog.startswith("a_iso_3d"):
@@ -148,6 +198,13 @@ def load(path):
         p = W.EIsoProblem(z["vp"], z["vs"], z["rho"], meta["h"], meta["npml"], meta["dt_ms"],
                           meta["duration"], [[tuple(s) for s in meta["shots"][0]]],
                           [tuple(r) for r in meta["receivers"]], meta["x0"], meta["z0"],
+                          name=meta["name"])
+    elif meta["kind"] == "ecyl":
+        p = W.ECylProblem(z["vp"], z["vs"], z["rho"], meta["dx"], meta["dz"], meta["npml"],
+                          meta["dt_ms"], meta["duration"], [tuple(s) for s in meta["sources"]],
+                          [tuple(r) for r in meta["receivers"]], n=meta["n"],
+                          absorb=meta["absorb"], Rc=meta["Rc"], kappa_max=meta["kappa_max"],
+                          alpha_max=meta["alpha_max"], x0=meta["x0"], z0=meta["z0"],
                           name=meta["name"])
     else:
         p = W.A3DProblem(z["vp"], z["rho"], tuple(meta["d"]), meta["npml"], meta["dt_ms"],

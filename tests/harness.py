@@ -145,3 +145,87 @@ def run_a3d_oracle(p, nsteps=None, fields_at=None):
 def rel_l2(a, b):
     return O.rel_l2(np.concatenate([np.ravel(x) for x in a]),
                     np.concatenate([np.ravel(x) for x in b]))
+
+
+# ----------------------------------------------------------------------------
+# e_cyl_iso (e_cyl_iso.c:277-790)
+# ----------------------------------------------------------------------------
+
+ECYL_COMPS = {"vr": "vr", "vtheta": "vt", "vz": "vz", "trr": "trr", "trtheta": "trt",
+              "trz": "trz", "tthetatheta": "ttt", "tthetaz": "ttz", "tzz": "tzz",
+              "div": "div", "curl": "curl"}
+
+
+def ecyl_pad(p, a):
+    """read_model_e_cyl's padding (io_utils.c:993-1026): z rows copied into
+    the top and bottom PML, the last radial column into the outer PML."""
+    n = p.np_used
+    out = np.zeros((p.nx + n, p.nz + 2 * n))
+    out[:p.nx, n:n + p.nz] = a
+    out[:p.nx, :n] = a[:, :1]
+    out[:p.nx, n + p.nz:] = a[:, -1:]
+    out[p.nx:, :] = out[p.nx - 1:p.nx, :]
+    return out
+
+
+def ecyl_setup(p):
+    vp, vs, rho = (ecyl_pad(p, a) for a in (p.vp, p.vs, p.rho))
+    mats, vpmax = O.ecyl_materials(vp, vs, rho)
+    dt = p.dt
+    if dt > 0.5 * (p.dx + p.dz) / (math.sqrt(2.0) * vpmax):
+        raise ValueError("CFL")
+    f0 = p.sources[0][2]
+    alpha = math.pi * f0 if p.alpha_max else 0.0
+    coef = O.ecyl_cpml(p.np_used, p.dx, p.dz, dt, 2.0, 5000.0, p.Rc, p.kappa_max, alpha,
+                       p.absorb)
+    return dict(mats=mats, coef=coef, dt=dt, nsteps=O.nsteps(p.duration, dt), vp=vp)
+
+
+def ecyl_index(p, x, z):
+    i = c_round((x - p.x0) / p.dx)          # no PML before r = 0
+    j = c_round((z - p.z0) / p.dz) + p.np_used
+    return i * (p.nz + 2 * p.np_used) + j
+
+
+def ecyl_sources(p, s):
+    """[(index, type id, samples)], Kurkjian wavelet for a Kurkjian first
+    source (e_cyl_iso.c:497-502), Ricker otherwise."""
+    idx = [ecyl_index(p, q[3], q[4]) for q in p.sources]
+    if p.sources[0][0] == "Kurkjian":
+        q = p.sources[0]
+        w = O.ecyl_kurkjian(q[1], q[2], p.dt, s["mats"]["lij"].reshape(-1)[idx[0]], q[3],
+                            p.dx, p.dz, p.n)
+        return [(idx[0], O.ECYL_SRC["Kurkjian"], w)]
+    fct = O.src_fct([q[1] for q in p.sources], [q[2] for q in p.sources], p.dt, 1.0)
+    return [(k, O.ECYL_SRC[q[0]], w) for k, q, w in zip(idx, p.sources, fct)]
+
+
+def run_ecyl_oracle(p, nsteps=None, fields_at=None):
+    """FP64 oracle run of a whole e_cyl_iso shot: traces (1e3 * value, as
+    write_trace writes them), times, optional final fields."""
+    s = ecyl_setup(p)
+    n = s["nsteps"] if nsteps is None else nsteps
+    o = O.ECyl(p.nx, p.nz, p.np_used, p.n, p.dx, p.dz, s["dt"], s["mats"], s["coef"])
+    srcs = ecyl_sources(p, s)
+    recs = [(ecyl_index(p, x, z), ECYL_COMPS[c.lower()], t0, r * 1e-3)
+            for (c, x, z, t0, r) in p.receivers]
+    dt = s["dt"]
+    tr = [[] for _ in recs]
+    tt = [[] for _ in recs]
+    kurk = srcs[0][1] == O.ECYL_SRC["Kurkjian"]
+    for it in range(n):
+        o.velocity()
+        if not kurk:
+            for (idx, typ, w) in srcs:
+                if it < len(w):
+                    o.force(idx, typ, w[it])
+        o.stress()
+        if kurk and it < len(srcs[0][2]):
+            o.kurkjian(srcs[0][0], srcs[0][2][it])
+        t = dt * (it + 1)
+        for r, (idx, comp, t0, rdt) in enumerate(recs):
+            if O.sample(it, dt, t0, rdt):
+                tr[r].append(1e3 * o.probe(comp, idx))
+                tt[r].append(t)
+    fields = {f: o.get(f) for f in fields_at} if fields_at else None
+    return [np.array(a) for a in tr], [np.array(a) for a in tt], fields

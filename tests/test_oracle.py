@@ -21,11 +21,26 @@ def test_oracle_matches_reference_traces(path):
     p, kind, program, ref_t, ref_v = G.load(path)
     if kind == "eiso":
         tr, tt, _ = H.run_eiso_oracle(p)
+    elif kind == "ecyl":
+        tr, tt, _ = H.run_ecyl_oracle(p)
     else:
         tr, tt, _ = H.run_a3d_oracle(p)
     assert [len(a) for a in tr] == [len(a) for a in ref_v]
     for a, b in zip(tt, ref_t):
         np.testing.assert_allclose(a, b, rtol=1e-6)
+    if kind == "ecyl":
+        # components differ by orders of magnitude (stresses, velocities,
+        # div, curl) and some traces hold only round-off before the wave
+        # arrives: compare each component over all of its records
+        for comp in sorted({r[0] for r in p.receivers}):
+            ks = [k for k, r in enumerate(p.receivers) if r[0] == comp]
+            a = np.concatenate([tr[k] for k in ks])
+            b = np.concatenate([ref_v[k] for k in ks])
+            if np.abs(b).max() == 0.0:
+                assert np.abs(a).max() == 0.0, comp
+            else:
+                assert O.rel_l2(a, b) < 2e-6, comp
+        return
     # the reference prints 7 significant digits ("%le"), so agreement is
     # bounded by text precision, not by arithmetic
     for a, b in zip(tr, ref_v):
