@@ -57,15 +57,28 @@ extern "C" {
 #define SM_SRC_SZ   2
 #define SM_SRC_SXZ  4
 #define SM_SRC_BULK 6
+#define SM_SRC_FR   9    /* e_cyl_iso force sources */
+#define SM_SRC_FT   10
+#define SM_SRC_FZ   11
+#define SM_SRC_KURKJIAN 12
 
 /* record components, numbered as enum component (structs.h:45) */
-#define SM_VX  0
-#define SM_VY  1
-#define SM_VZ  2
-#define SM_TXX 5
-#define SM_TZZ 6
-#define SM_TXZ 7
-#define SM_P   8
+#define SM_VX   0
+#define SM_VY   1
+#define SM_VZ   2
+#define SM_TXX  5
+#define SM_TZZ  6
+#define SM_TXZ  7
+#define SM_P    8
+#define SM_DIV  11   /* e_cyl_iso: divergence of particle velocity */
+#define SM_CURL 12   /* e_cyl_iso: curl of particle velocity */
+#define SM_VR   13
+#define SM_VT   14   /* v_theta */
+#define SM_TRR  15
+#define SM_TRT  16   /* tau_r theta */
+#define SM_TRZ  17
+#define SM_TTT  18   /* tau_theta theta */
+#define SM_TTZ  19   /* tau_theta z */
 
 /* which part of an e_iso field: the total, or the x / z split part that the
  * PML frame carries (pml.c keeps q_x and q_z, q = q_x + q_z) */
@@ -260,6 +273,76 @@ int sm_a3d_kernel_stats(sm_a3d_t h, int reset, double *update_ms, size_t *update
                         size_t *all_launches);
 
 /* ======================================================================
+ * e_cyl_iso on the device: 2.5-D elastic FDTD in cylindrical coordinates
+ * (r, z) for azimuthal mode n, CPML at the outer radius and at both z ends
+ * (e_cyl_iso.c, propagate.c:2706-4118, pml.c:1811-2185).  Padded arrays are
+ * nx2*nz2 with nx2 = nx + np (no layer before the axis r = 0) and
+ * nz2 = nz + 2*np, index i*nz2 + j.  With the .par "abs 0" the reference
+ * uses np = 0 (io_utils.c:293).  FP32 or FP64 storage.
+ * ====================================================================== */
+
+typedef struct sm_ecyl *sm_ecyl_t;
+
+/* model padding of read_model_e_cyl (io_utils.c:993-1026): interior nx*nz
+ * (index i*nz + j) into nx2*nz2 */
+int sm_ecyl_pad_model(size_t nx, size_t nz, size_t np, const double *vp, const double *vs,
+                      const double *rho, double *vp_pad, double *vs_pad, double *rho_pad);
+/* material averaging e_cyl_iso.c:363-441 on the padded model; mat: 8 arrays
+ * lij l2mij mu mui muj bi bj bij (nx2*nz2 each); vpmax for the CFL test
+ * dt <= (dx+dz)/2 / (sqrt(2) vpmax) (e_cyl_iso.c:484-488) */
+int sm_ecyl_materials(size_t nx2, size_t nz2, const double *vp, const double *vs,
+                      const double *rho, double *const *mat, double *vpmax);
+/* CPML coefficients, pml.c:2107-2185 (compute_cpml_cyl): 15 arrays ik_r
+ * ik_z ikh_z b_r c_r b_z c_z bh_z ch_z (np values) then ikH_r ikH_z bH_r cH_r
+ * bH_z cH_z (np + 1 values); absorb = the .par "abs" flag; alpha_max =
+ * pi f0, or 0 when the .par alpha_max is 0 (e_cyl_iso.c:532-535) */
+int sm_ecyl_cpml(size_t np, double dx, double dz, double dt, double order, double vmax,
+                 double Rc, double kappa_max, double alpha_max, int absorb, double *const *c);
+/* Kurkjian source wavelet, src.c:202-228 (lij_at_src: lij at the source
+ * node, r_src its radius); returns the sample count (fct may be NULL) */
+size_t sm_ecyl_kurkjian(double A, double f, double dt, double lij_at_src, double r_src,
+                        double dx, double dz, int n, size_t maxlen, double *fct);
+
+/* Replaces the allocations of e_cyl_iso.c:341-360 and the state of its time
+ * loop e_cyl_iso.c:605-790.  mat and coef as produced above. */
+int sm_ecyl_create(int device, size_t nx, size_t nz, size_t np, int n, double dx, double dz,
+                   double dt, const double *const *mat, const double *const *coef,
+                   int precision, sm_ecyl_t *out);
+/* Sources at padded index[s]: SM_SRC_FR / SM_SRC_FT / SM_SRC_FZ / SM_SRC_BULK
+ * add dt*b*fct[s*stride + it] after the velocity update (add_force_src_cyl,
+ * src.c:186-199; fct from sm_ricker); one SM_SRC_KURKJIAN adds
+ * dt*fct[it] to trr and tzz after the stress update (add_kurkjian_src,
+ * src.c:231-236; fct from sm_ecyl_kurkjian).  Other types add nothing, as in
+ * the reference's cylindrical loop. */
+int sm_ecyl_set_sources(sm_ecyl_t h, size_t nsrc, const size_t *index, const int *type,
+                        const double *fct, const size_t *length, size_t stride);
+/* Records at padded index[r] (e_cyl_iso.c:668-790): components SM_VR SM_VT
+ * SM_VZ SM_TRR SM_TTT SM_TZZ SM_TRZ SM_TRT SM_TTZ, or SM_DIV / SM_CURL
+ * (compute_div_cyl / compute_curl_cyl, propagate.c:4090-4118, evaluated at
+ * the record's node), sampled by sm_sample_predicate for it < nsteps_max */
+int sm_ecyl_set_receivers(sm_ecyl_t h, size_t nrec, const size_t *index, const int *comp,
+                          const double *t0, const double *rdt, size_t nsteps_max);
+/* nsteps steps of the loop e_cyl_iso.c:605-790 (mode 0 or n > 0 forms) */
+int sm_ecyl_run(sm_ecyl_t h, size_t nsteps);
+int sm_ecyl_sync(sm_ecyl_t h);
+int sm_ecyl_reset(sm_ecyl_t h);
+/* samples so far of records [rec0, rec0+nrec) into out[r*ld + s] (raw
+ * values; the reference writes 1e3 * value); counts[r] gets their number */
+int sm_ecyl_read_traces(sm_ecyl_t h, size_t rec0, size_t nrec, double *out, size_t ld,
+                        size_t *counts);
+/* a whole padded field (nx2*nz2) of component SM_VR ... SM_TTZ */
+int sm_ecyl_get_field(sm_ecyl_t h, int comp, double *out);
+int sm_ecyl_set_field(sm_ecyl_t h, int comp, const double *in);
+int sm_ecyl_stream(sm_ecyl_t h, void **stream);
+int sm_ecyl_set_timing(sm_ecyl_t h, int on);
+/* update_ms: device time of the velocity + source + stress launches */
+int sm_ecyl_kernel_stats(sm_ecyl_t h, int reset, double *update_ms, size_t *update_launches,
+                         size_t *all_launches);
+int sm_ecyl_destroy(sm_ecyl_t h);
+/* device memory of a handle, bytes */
+size_t sm_ecyl_device_bytes(size_t nx, size_t nz, size_t np, int precision);
+
+/* ======================================================================
  * device memory a handle needs (estimate used for admission; no reference
  * counterpart).  nrec receivers per shot, nsteps_max samples at most.
  * ====================================================================== */
@@ -407,6 +490,7 @@ int sm_eiso_run_noalloc(int device, void *stream, const sm_eiso_request *r, doub
  * ====================================================================== */
 int sm_e_iso_main(int argc, char **argv);
 int sm_a_iso_3d_main(int argc, char **argv);
+int sm_e_cyl_iso_main(int argc, char **argv);
 
 #ifdef __cplusplus
 }

@@ -21,6 +21,9 @@ PRECISIONS = {"fp32": SM_FP32, "fp64": SM_FP64, "fp16": SM_FP16, "bf16": SM_BF16
 SM_SRC = {"sx": 0, "sz": 2, "sxz": 4, "bulk": 6}
 SM_COMP = {"vx": 0, "vy": 1, "vz": 2, "txx": 5, "tzz": 6, "txz": 7, "p": 8}
 SM_PART = {"total": 0, "x": 1, "z": 2}
+# e_cyl_iso components (enum component, structs.h:45)
+SM_VZ, SM_TZZ, SM_DIV, SM_CURL = 2, 6, 11, 12
+SM_VR, SM_VT, SM_TRR, SM_TRT, SM_TRZ, SM_TTT, SM_TTZ = 13, 14, 15, 16, 17, 18, 19
 SM_ALL_SHOTS = C.c_size_t(-1).value
 
 
@@ -50,6 +53,26 @@ _SIGS = {
     "sm_a3d_cfl_vpmax": (C.c_double, [_sz, _sz, _dp]),
     "sm_a3d_cpml": (C.c_int, [_sz, _sz, _sz, _sz] + [C.c_double] * 8 +
                     [C.c_int, C.c_double, C.POINTER(_dp)]),
+    "sm_ecyl_pad_model": (C.c_int, [_sz, _sz, _sz] + [_dp] * 6),
+    "sm_ecyl_materials": (C.c_int, [_sz, _sz, _dp, _dp, _dp, C.POINTER(_dp), _dp]),
+    "sm_ecyl_cpml": (C.c_int, [_sz] + [C.c_double] * 8 + [C.c_int, C.POINTER(_dp)]),
+    "sm_ecyl_kurkjian": (_sz, [C.c_double] * 7 + [C.c_int, _sz, _dp]),
+    "sm_ecyl_create": (C.c_int, [C.c_int, _sz, _sz, _sz, C.c_int, C.c_double, C.c_double,
+                                 C.c_double, C.POINTER(_dp), C.POINTER(_dp), C.c_int,
+                                 C.POINTER(_vp)]),
+    "sm_ecyl_set_sources": (C.c_int, [_vp, _sz, _szp, _ip, _dp, _szp, _sz]),
+    "sm_ecyl_set_receivers": (C.c_int, [_vp, _sz, _szp, _ip, _dp, _dp, _sz]),
+    "sm_ecyl_run": (C.c_int, [_vp, _sz]),
+    "sm_ecyl_sync": (C.c_int, [_vp]),
+    "sm_ecyl_reset": (C.c_int, [_vp]),
+    "sm_ecyl_read_traces": (C.c_int, [_vp, _sz, _sz, _dp, _sz, _szp]),
+    "sm_ecyl_get_field": (C.c_int, [_vp, C.c_int, _dp]),
+    "sm_ecyl_set_field": (C.c_int, [_vp, C.c_int, _dp]),
+    "sm_ecyl_stream": (C.c_int, [_vp, C.POINTER(_vp)]),
+    "sm_ecyl_set_timing": (C.c_int, [_vp, C.c_int]),
+    "sm_ecyl_kernel_stats": (C.c_int, [_vp, C.c_int, _dp, _szp, _szp]),
+    "sm_ecyl_destroy": (C.c_int, [_vp]),
+    "sm_ecyl_device_bytes": (_sz, [_sz, _sz, _sz, C.c_int]),
     "sm_eiso_create": (C.c_int, [C.c_int, _sz, _sz, _sz, C.c_double, C.c_double] + [_dp] * 8 +
                        [C.c_int, _sz, C.POINTER(_vp)]),
     "sm_eiso_set_sources": (C.c_int, [_vp, _sz, _sz, _szp, _ip, _dp, _szp, _sz, C.c_double]),

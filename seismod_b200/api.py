@@ -1,4 +1,5 @@
-"""Python front end of the C ABI: device handles for e_iso and a_iso_3d and
+"""Python front end of the C ABI: device handles for e_iso, a_iso_3d and
+e_cyl_iso and
 helpers that take a whole shot from a workload description to traces.
 
 Everything here calls libseismod_gpu.so; the arithmetic of the set-up
@@ -440,6 +441,158 @@ def a3d_device(p, precision="fp32", device=0):
 
 def run_a3d(p, precision="fp32", device=0, nsteps_override=None):
     dev, n = a3d_device(p, precision, device)
+    dev.run(n if nsteps_override is None else nsteps_override)
+    out = dev.traces()
+    dev.close()
+    return out
+
+
+# ----------------------------------------------------------------------------
+# e_cyl_iso
+# ----------------------------------------------------------------------------
+
+ECYL_COMP = {"vr": L.SM_VR, "vtheta": L.SM_VT, "vz": L.SM_VZ, "trr": L.SM_TRR,
+             "trtheta": L.SM_TRT, "trz": L.SM_TRZ, "tthetatheta": L.SM_TTT,
+             "tthetaz": L.SM_TTZ, "tzz": L.SM_TZZ, "div": L.SM_DIV, "curl": L.SM_CURL}
+ECYL_FIELD = {"vr": L.SM_VR, "vt": L.SM_VT, "vz": L.SM_VZ, "trr": L.SM_TRR, "ttt": L.SM_TTT,
+              "tzz": L.SM_TZZ, "trz": L.SM_TRZ, "trt": L.SM_TRT, "ttz": L.SM_TTZ}
+ECYL_SRC = {"fr": 9, "ftheta": 10, "fz": 11, "bulk": 6, "kurkjian": 12}
+
+
+def ecyl_inputs(p):
+    """Everything sm_ecyl_create and the source / receiver set-up take for an
+    ECylProblem, as e_cyl_iso.c:277-600 prepares it (library host code)."""
+    lib = L.load()
+    npml = p.np_used
+    nx2, nz2 = p.nx + npml, p.nz + 2 * npml
+    pads = [np.zeros((nx2, nz2)) for _ in range(3)]
+    vp, vs, rho = _f64(p.vp), _f64(p.vs), _f64(p.rho)
+    L.check(lib.sm_ecyl_pad_model(p.nx, p.nz, npml, L.dptr(vp), L.dptr(vs), L.dptr(rho),
+                                  *[L.dptr(a) for a in pads]))
+    mats = [np.zeros((nx2, nz2)) for _ in range(8)]
+    vmax = C.c_double()
+    mp = (L._dp * 8)(*[L.dptr(a) for a in mats])
+    L.check(lib.sm_ecyl_materials(nx2, nz2, *[L.dptr(a) for a in pads], mp, C.byref(vmax)))
+    dt = p.dt
+    if dt > 0.5 * (p.dx + p.dz) / (math.sqrt(2.0) * vmax.value):
+        raise L.SeismodError(L.SM_ECFL, "time step too large (e_cyl_iso.c:484-488)")
+    alpha = math.pi * p.sources[0][2] if p.alpha_max else 0.0
+    coef = [np.zeros(npml if k < 9 else npml + 1) for k in range(15)]
+    cp = (L._dp * 15)(*[L.dptr(a) for a in coef])
+    L.check(lib.sm_ecyl_cpml(npml, p.dx, p.dz, dt, 2.0, 5000.0, p.Rc, p.kappa_max, alpha,
+                             int(p.absorb), cp))
+
+    def index(x, z):
+        return c_round((x - p.x0) / p.dx) * nz2 + c_round((z - p.z0) / p.dz) + npml
+
+    sidx = [index(q[3], q[4]) for q in p.sources]
+    if p.sources[0][0].lower() == "kurkjian":
+        q = p.sources[0]
+        n = int(lib.sm_ecyl_kurkjian(q[1], q[2], dt, 0.0, q[3], p.dx, p.dz, p.n, 0, None))
+        fct = np.zeros((1, max(n, 1)))
+        lij = mats[0].reshape(-1)[sidx[0]]
+        n = int(lib.sm_ecyl_kurkjian(q[1], q[2], dt, lij, q[3], p.dx, p.dz, p.n, n,
+                                     L.dptr(fct)))
+        src = ([sidx[0]], [ECYL_SRC["kurkjian"]], fct, [n])
+    else:
+        fct, ln = ricker([q[1] for q in p.sources], [q[2] for q in p.sources], dt)
+        src = (sidx, [ECYL_SRC[q[0].lower()] for q in p.sources], fct, ln)
+    rec = ([index(x, z) for (_, x, z, _, _) in p.receivers],
+           [ECYL_COMP[c.lower()] for (c, _, _, _, _) in p.receivers],
+           [t0 for (_, _, _, t0, _) in p.receivers],
+           [r * 1e-3 for (_, _, _, _, r) in p.receivers])
+    return dict(npml=npml, mats=mats, coef=coef, dt=dt, src=src, rec=rec,
+                nsteps=nsteps(p.duration, dt))
+
+
+class ECylDevice:
+    """An e_cyl_iso state on the GPU."""
+
+    def __init__(self, nx, nz, npml, n, dx, dz, dt, mats, coef, precision="fp32", device=0):
+        lib = L.load()
+        self.shape = (nx + npml, nz + 2 * npml)
+        self._keep = [_f64(a) for a in mats] + [_f64(c) for c in coef]
+        mp = (L._dp * 8)(*[L.dptr(a) for a in self._keep[:8]])
+        cp = (L._dp * 15)(*[L.dptr(a) for a in self._keep[8:]])
+        hnd = C.c_void_p()
+        L.check(lib.sm_ecyl_create(device, nx, nz, npml, int(n), dx, dz, dt, mp, cp,
+                                   L.PRECISIONS[precision], C.byref(hnd)))
+        self._h = hnd
+        self.nrec = 0
+
+    def close(self):
+        if getattr(self, "_h", None) and self._h.value:
+            L.load().sm_ecyl_destroy(self._h)
+            self._h = None
+
+    __del__ = close
+
+    def set_sources(self, index, types, fct, lengths):
+        index = np.ascontiguousarray(index, dtype=np.uintp)
+        types = np.ascontiguousarray(types, dtype=np.int32)
+        fct = _f64(np.atleast_2d(fct))
+        lengths = np.ascontiguousarray(lengths, dtype=np.uintp)
+        L.check(L.load().sm_ecyl_set_sources(self._h, len(index), L.szptr(index),
+                                             types.ctypes.data_as(L._ip), L.dptr(fct),
+                                             L.szptr(lengths), fct.shape[1]))
+
+    def set_receivers(self, index, comp, t0, rdt, nsteps_max):
+        index = np.ascontiguousarray(index, dtype=np.uintp)
+        comp = np.ascontiguousarray(comp, dtype=np.int32)
+        t0, rdt = _f64(t0), _f64(rdt)
+        L.check(L.load().sm_ecyl_set_receivers(self._h, len(index), L.szptr(index),
+                                               comp.ctypes.data_as(L._ip), L.dptr(t0),
+                                               L.dptr(rdt), nsteps_max))
+        self.nrec = len(index)
+
+    def run(self, n):
+        L.check(L.load().sm_ecyl_run(self._h, n))
+
+    def sync(self):
+        L.check(L.load().sm_ecyl_sync(self._h))
+
+    def reset(self):
+        L.check(L.load().sm_ecyl_reset(self._h))
+
+    def stream(self):
+        s = C.c_void_p()
+        L.check(L.load().sm_ecyl_stream(self._h, C.byref(s)))
+        return s.value
+
+    def traces(self):
+        n = self.nrec
+        counts = np.zeros(n, dtype=np.uintp)
+        L.check(L.load().sm_ecyl_read_traces(self._h, 0, n, None, 0, L.szptr(counts)))
+        ld = int(counts.max()) if n else 0
+        out = np.zeros((n, max(ld, 1)))
+        if n and ld:
+            L.check(L.load().sm_ecyl_read_traces(self._h, 0, n, L.dptr(out), ld,
+                                                 L.szptr(counts)))
+        return [out[k, :counts[k]].copy() for k in range(n)]
+
+    def get_field(self, name):
+        out = np.zeros(self.shape)
+        L.check(L.load().sm_ecyl_get_field(self._h, ECYL_FIELD[name], L.dptr(out)))
+        return out
+
+    def set_field(self, name, arr):
+        a = _f64(arr)
+        L.check(L.load().sm_ecyl_set_field(self._h, ECYL_FIELD[name], L.dptr(a)))
+
+
+def ecyl_device(p, precision="fp32", device=0):
+    q = ecyl_inputs(p)
+    dev = ECylDevice(p.nx, p.nz, q["npml"], p.n, p.dx, p.dz, q["dt"], q["mats"], q["coef"],
+                     precision, device)
+    dev.set_sources(*q["src"])
+    dev.set_receivers(*q["rec"], q["nsteps"])
+    return dev, q["nsteps"]
+
+
+def run_ecyl(p, precision="fp32", device=0, nsteps_override=None):
+    """A whole e_cyl_iso shot -> list of trace arrays (raw values; the
+    reference's .trc files hold 1e3 * value)."""
+    dev, n = ecyl_device(p, precision, device)
     dev.run(n if nsteps_override is None else nsteps_override)
     out = dev.traces()
     dev.close()

@@ -402,3 +402,133 @@ out:
     rec_plan_free(&rp);
     return report(rc, prog);
 }
+
+int sm_e_cyl_iso_main(int argc, char **argv)
+{
+    /* e_cyl_iso.c:277-790: set-up in FP64 through the library's host
+     * functions, the loop through the C ABI.  Differences from the
+     * reference: force sources are added once per step (the OpenMP build of
+     * the reference adds them once per thread, e_cyl_iso.c:612-637); the
+     * 9-point source template is refused (io_utils.c:1513-1534 offsets its
+     * radial indices by np, which the cylindrical grid does not have);
+     * snapshot records are skipped (netCDF) with a warning. */
+    const char *prog = "e_cyl_iso_gpu";
+    sm_params p;
+    sm_grid g;
+    double *vp = NULL, *vs = NULL, *rho = NULL, *pad[3] = {0}, *mat[8] = {0}, *coef[15] = {0};
+    double *fct = NULL, *vals = NULL;
+    size_t *len = NULL, *counts = NULL, *sidx = NULL;
+    int *stype = NULL;
+    sm_source *src = NULL;
+    sm_record *rec = NULL;
+    rec_plan rp = {0};
+    sm_ecyl_t h = NULL;
+    size_t nsrc = 0, ntpl = 1, nrec = 0, stride = 0;
+    int rc;
+
+    sm_params_defaults(&p);
+    if ((rc = sm_parse_args(argc, argv, &p, prog))) return report(rc, prog);
+    const size_t np = p.np;   /* 0 with abs 0 (io_utils.c:293) */
+    const int n = p.azimuthal_mode;
+    if (p.verbose)
+        fprintf(stdout, "\n *** e_cyl_iso - Elastic wave propagation in 2.5D isotropic media in "
+                        "cylindrical coordinates (GPU) ***\n\n");
+    if (n < 0) { rc = sm_fail(SM_EINVAL, "azimuthal_mode must be >= 0"); goto out; }
+    if ((rc = sm_read_model_ecyl(p.modelfile, &g, &vp, &vs, &rho))) goto out;
+    const size_t nx = g.nx, nz = g.nz, nx2 = nx + np, nz2 = nz + 2 * np, N = nx2 * nz2;
+    const double dt = p.dt;
+    for (int k = 0; k < 3; ++k)
+        if (!(pad[k] = malloc(N * sizeof(double)))) { rc = sm_fail(SM_ENOMEM, "out of host memory"); goto out; }
+    for (int k = 0; k < 8; ++k)
+        if (!(mat[k] = malloc(N * sizeof(double)))) { rc = sm_fail(SM_ENOMEM, "out of host memory"); goto out; }
+    for (int k = 0; k < 15; ++k)
+        if (!(coef[k] = malloc((np + 1) * sizeof(double)))) { rc = sm_fail(SM_ENOMEM, "out of host memory"); goto out; }
+    if ((rc = sm_ecyl_pad_model(nx, nz, np, vp, vs, rho, pad[0], pad[1], pad[2]))) goto out;
+    double vpmax = 0.0;
+    if ((rc = sm_ecyl_materials(nx2, nz2, pad[0], pad[1], pad[2], mat, &vpmax))) goto out;
+    if (dt > 0.5 * (g.dx + g.dz) / (sqrt(2.0) * vpmax)) {   /* e_cyl_iso.c:484-488 */
+        rc = sm_fail(SM_ECFL, "Time step too large");
+        goto out;
+    }
+    if ((rc = sm_read_sources(p.sourcefile, &g, 0, &src, &nsrc, &ntpl))) goto out;
+    if (ntpl != 1) {
+        rc = sm_fail(SM_EINVAL, "e_cyl_iso takes 1-point sources (the 9-point template of "
+                                "io_utils.c:1513-1534 does not fit the cylindrical grid)");
+        goto out;
+    }
+    sidx = malloc(nsrc * sizeof(size_t));
+    stype = malloc(nsrc * sizeof(int));
+    if (!sidx || !stype) { rc = sm_fail(SM_ENOMEM, "out of host memory"); goto out; }
+    for (size_t q = 0; q < nsrc; ++q) {
+        if (src[q].i < 0 || src[q].k < 0 || (size_t)src[q].i >= nx2 || (size_t)src[q].k + np >= nz2) {
+            rc = sm_fail(SM_EINVAL, "source %zu lies outside the grid", q + 1);
+            goto out;
+        }
+        sidx[q] = (size_t)src[q].i * nz2 + (size_t)src[q].k + np;   /* io_utils.c:1487-1492 */
+        stype[q] = src[q].type;
+    }
+    if (src[0].type == SM_SRC_KURKJIAN) {   /* e_cyl_iso.c:497-502: the first source alone */
+        stride = sm_ecyl_kurkjian(src[0].A, src[0].f, dt, 0.0, src[0].x, g.dx, g.dz, n, 0, NULL);
+        fct = calloc(stride ? stride : 1, sizeof(double));
+        len = calloc(1, sizeof(size_t));
+        if (!fct || !len) { rc = sm_fail(SM_ENOMEM, "out of host memory"); goto out; }
+        len[0] = sm_ecyl_kurkjian(src[0].A, src[0].f, dt, mat[0][sidx[0]], src[0].x, g.dx, g.dz,
+                                  n, stride, fct);
+        nsrc = 1;
+    } else if ((rc = make_wavelets(src, nsrc, dt, &fct, &len, &stride))) {
+        goto out;
+    }
+    {   /* CPML, e_cyl_iso.c:529-535 */
+        const double pi = 4.0 * atan(1.0);
+        const double alpha = p.alpha_max ? pi * src[0].f : 0.0;
+        if ((rc = sm_ecyl_cpml(np, g.dx, g.dz, dt, p.pml_order, p.vmax, p.Rc, p.kappa_max, alpha,
+                               p.iwipe, coef)))
+            goto out;
+    }
+    if ((rc = sm_read_records(p.outputfile, &g, 0, &rec, &nrec))) goto out;
+    check_dt_trc(rec, nrec, dt);
+    const size_t nsteps = sm_nsteps(p.duration, dt);
+    if ((rc = sm_ecyl_create(0, nx, nz, np, n, g.dx, g.dz, dt, (const double *const *)mat,
+                             (const double *const *)coef, p.precision, &h)))
+        goto out;
+    if ((rc = sm_ecyl_set_sources(h, nsrc, sidx, stype, fct, len, stride))) goto out;
+    rp.index = malloc((nrec ? nrec : 1) * sizeof(size_t)); rp.recno = malloc((nrec ? nrec : 1) * sizeof(size_t));
+    rp.comp = malloc((nrec ? nrec : 1) * sizeof(int));
+    rp.t0 = malloc((nrec ? nrec : 1) * sizeof(double)); rp.rdt = malloc((nrec ? nrec : 1) * sizeof(double));
+    for (size_t r = 0; r < nrec; ++r) {
+        if (!rec[r].is_trace) {
+            fprintf(stderr, "%s: record %zu is a snapshot (netCDF in the reference); skipped\n", prog, r + 1);
+            continue;
+        }
+        if (rec[r].i < 0 || rec[r].k < 0 || (size_t)rec[r].i >= nx2 || (size_t)rec[r].k + np >= nz2) {
+            rc = sm_fail(SM_EINVAL, "record %zu lies outside the grid", r + 1);
+            goto out;
+        }
+        rp.index[rp.n] = (size_t)rec[r].i * nz2 + (size_t)rec[r].k + np;   /* io_utils.c:1661-1666 */
+        rp.comp[rp.n] = rec[r].comp;
+        rp.t0[rp.n] = rec[r].t0;
+        rp.rdt[rp.n] = rec[r].dt;
+        rp.recno[rp.n] = r;
+        rp.n++;
+    }
+    if ((rc = sm_ecyl_set_receivers(h, rp.n, rp.index, rp.comp, rp.t0, rp.rdt, nsteps))) goto out;
+    if (p.verbose) fprintf(stdout, "Starting main loop (%zu iterations)\n", nsteps);
+    if ((rc = sm_ecyl_run(h, nsteps))) goto out;
+    counts = calloc(rp.n ? rp.n : 1, sizeof(size_t));
+    if ((rc = sm_ecyl_read_traces(h, 0, rp.n, NULL, 0, counts))) goto out;
+    size_t ld = 1;
+    for (size_t r = 0; r < rp.n; ++r) ld = counts[r] > ld ? counts[r] : ld;
+    vals = malloc(rp.n * ld * sizeof(double) + 1);
+    if ((rc = sm_ecyl_read_traces(h, 0, rp.n, vals, ld, counts))) goto out;
+    rc = write_traces(p.basename, &rp, vals, ld, counts, dt, nsteps);
+    if (p.verbose) fprintf(stdout, "\nEnd of computation\n");
+out:
+    sm_ecyl_destroy(h);
+    free(vp); free(vs); free(rho);
+    for (int k = 0; k < 3; ++k) free(pad[k]);
+    for (int k = 0; k < 8; ++k) free(mat[k]);
+    for (int k = 0; k < 15; ++k) free(coef[k]);
+    free(fct); free(len); free(sidx); free(stype); free(src); free(rec); free(vals); free(counts);
+    rec_plan_free(&rp);
+    return report(rc, prog);
+}

@@ -32,6 +32,7 @@ void sm_params_defaults(sm_params *p)
     p->shotpt_no = 1;
     p->simulate_cmp = 0;
     p->plot_strips = 0;
+    p->azimuthal_mode = 0;
     p->Rc = 1.e-5;
     p->kappa_max = 1.;
     p->alpha_max = 1;
@@ -112,8 +113,9 @@ int sm_read_par(const char *path, sm_params *p)
         else if (!strcmp(keyword, "Rc")) p->Rc = strtod(value, NULL);
         else if (!strcmp(keyword, "kappa_max")) p->kappa_max = strtod(value, NULL);
         else if (!strcmp(keyword, "alpha_max")) p->alpha_max = (short)atoi(value);
-        /* check_model, chkpt_inc, pml_median, saveEnergy, EnergyROI,
-         * azimuthal_mode: accepted, unused by these programs */
+        else if (!strcmp(keyword, "azimuthal_mode")) p->azimuthal_mode = atoi(value);
+        /* check_model, chkpt_inc, pml_median, saveEnergy, EnergyROI:
+         * accepted, unused by these programs */
     }
     fclose(fid);
     if (p->iwipe == 0) p->np = 0;   /* io_utils.c:293 */
@@ -176,6 +178,62 @@ static int read_model_bin(const char *path, unsigned ndim, unsigned nfields, sm_
         }
     }
     fclose(f);
+    return SM_OK;
+}
+
+int sm_read_model_ecyl(const char *path, sm_grid *g, double **pvp, double **pvs, double **prho)
+{
+    if (model_is_binary(path)) return sm_read_model_e(path, g, pvp, pvs, prho);
+    /* io_utils.c:296-328 (grid) and 949-991 (values): the rows are z, r fast
+     * within each; a file holding only the first row is a radial profile
+     * copied down every row */
+    FILE *fid = fopen(path, "r");
+    if (!fid) return sm_fail(SM_EIO, "cannot open %s for reading", path);
+    char type[64];
+    memset(g, 0, sizeof *g);
+    g->ny = 1;
+    g->dy = 1.0;
+    if (fscanf(fid, "%zu %zu", &g->nx, &g->nz) != 2 || fscanf(fid, "%lf %lf", &g->dx, &g->dz) != 2 ||
+        fscanf(fid, "%lf %lf", &g->x0, &g->z0) != 2 || fscanf(fid, "%63s", type) != 1) {
+        fclose(fid);
+        return sm_fail(SM_EIO, "%s: bad header", path);
+    }
+    if (strcmp(type, "isotropic_elastic_cyl") != 0) {
+        fclose(fid);
+        return sm_fail(SM_EIO, "model in %s not isotropic_elastic_cyl", path);
+    }
+    const size_t nx = g->nx, nz = g->nz;
+    if (nx < 2 || nz < 2) {
+        fclose(fid);
+        return sm_fail(SM_EIO, "%s: grid must be at least 2 x 2", path);
+    }
+    double *vp = malloc(nx * nz * sizeof(double)), *vs = malloc(nx * nz * sizeof(double));
+    double *rho = malloc(nx * nz * sizeof(double));
+    if (!vp || !vs || !rho) {
+        free(vp); free(vs); free(rho); fclose(fid);
+        return sm_fail(SM_ENOMEM, "out of host memory");
+    }
+    int profile = 0;
+    for (size_t j = 0; j < nz && !profile; ++j) {
+        for (size_t i = 0; i < nx; ++i) {
+            const size_t q = i * nz + j;
+            const int nread = fscanf(fid, "%lf %lf %lf", &vp[q], &vs[q], &rho[q]);
+            if (nread <= 0 && j == 1 && i == 0) { profile = 1; break; }
+            if (nread != 3) {
+                fclose(fid); free(vp); free(vs); free(rho);
+                return sm_fail(SM_EIO, "something wrong with file %s", path);
+            }
+        }
+    }
+    fclose(fid);
+    if (profile)
+        for (size_t i = 0; i < nx; ++i)
+            for (size_t j = 1; j < nz; ++j) {
+                vp[i * nz + j] = vp[i * nz];
+                vs[i * nz + j] = vs[i * nz];
+                rho[i * nz + j] = rho[i * nz];
+            }
+    *pvp = vp; *pvs = vs; *prho = rho;
     return SM_OK;
 }
 
@@ -401,7 +459,11 @@ static int record_comp(const char *t, int three_d)
         {"Qx", "qx", "QX", 3, 0}, {"Qz", "qz", "QZ", 4, 0}, {"txx", "TXX", "TXX", 5, 0},
         {"tzz", "TZZ", "TZZ", 6, 0}, {"txy", "TXY", "TXY", 9, 0}, {"tyz", "TYZ", "TYZ", 10, 0},
         {"txz", "TXZ", "TXZ", 7, 0}, {"p", "P", "P", 8, 1}, {"div", "Div", "DIV", 11, 0},
-        {"curl", "Curl", "CURL", 12, 0},
+        {"curl", "Curl", "CURL", 12, 0}, {"Vr", "vr", "VR", 13, 0},
+        {"Vtheta", "vtheta", "VTHETA", 14, 0}, {"trr", "TRR", "TRR", 15, 0},
+        {"trtheta", "TRTHETA", "TRTHETA", 16, 0}, {"trz", "TRZ", "TRZ", 17, 0},
+        {"tthetatheta", "TTHETATHETA", "TTHETATHETA", 18, 0},
+        {"tthetaz", "TTHETAZ", "TTHETAZ", 19, 0},
     };
     for (size_t q = 0; q < sizeof tab / sizeof tab[0]; ++q)
         if ((!three_d || tab[q].in3d) &&

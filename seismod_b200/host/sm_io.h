@@ -27,6 +27,7 @@ typedef struct {
     int alpha_max;
     int verbose;
     int plot_strips;     /* "plstr": snapshots include the absorbing frame */
+    int azimuthal_mode;  /* e_cyl_iso: "azimuthal_mode" n */
     int precision;       /* SM_FP32 by default; "-P" */
 } sm_params;
 
@@ -60,6 +61,10 @@ int sm_read_par(const char *path, sm_params *p);
  * them. */
 int sm_read_model_e(const char *path, sm_grid *g, double **vp, double **vs, double **rho);
 int sm_read_model_a(const char *path, sm_grid *g, double **vp, double **rho);
+/* e_cyl_iso model (io_utils.c:949-991, keyword isotropic_elastic_cyl; rows
+ * are z, r fastest, one row = a radial profile); interior nx*nz values,
+ * index i*nz + j, padding by sm_ecyl_pad_model.  Binary files as e_iso. */
+int sm_read_model_ecyl(const char *path, sm_grid *g, double **vp, double **vs, double **rho);
 /* source and output files (io_utils.c:1432-1741); *src / *rec malloc'ed */
 int sm_read_sources(const char *path, const sm_grid *g, int three_d, sm_source **src,
                     size_t *nsrc, size_t *ntemplate);

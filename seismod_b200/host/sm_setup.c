@@ -227,3 +227,173 @@ int sm_a3d_cpml(size_t np, size_t nx2, size_t ny2, size_t nz2,
     }
     return SM_OK;
 }
+
+/* ======================================================================
+ * e_cyl_iso (padded grid nx2 = nx + np radial columns, PML at the outer
+ * radius only; nz2 = nz + 2 np rows; index i*nz2 + j)
+ * ====================================================================== */
+
+int sm_ecyl_pad_model(size_t nx, size_t nz, size_t np, const double *vp, const double *vs,
+                      const double *rho, double *vp_pad, double *vs_pad, double *rho_pad)
+{
+    /* io_utils.c:993-1026: interior at rows np..np+nz-1; the PML rows copy
+     * the first / last interior row of their column; the outer PML columns
+     * copy column nx-1 */
+    if (!vp || !vs || !rho || !vp_pad || !vs_pad || !rho_pad || nx == 0 || nz == 0)
+        return sm_fail(SM_EINVAL, "sm_ecyl_pad_model: bad argument");
+    const size_t nz2 = nz + 2 * np, nx2 = nx + np;
+    const double *src[3] = {vp, vs, rho};
+    double *dst[3] = {vp_pad, vs_pad, rho_pad};
+    for (int k = 0; k < 3; ++k) {
+        for (size_t i = 0; i < nx; ++i) {
+            double *col = dst[k] + i * nz2;
+            memcpy(col + np, src[k] + i * nz, nz * sizeof(double));
+            for (size_t j = 0; j < np; ++j) {
+                col[j] = col[np];
+                col[np + nz + j] = col[np + nz - 1];
+            }
+        }
+        for (size_t i = nx; i < nx2; ++i)
+            memcpy(dst[k] + i * nz2, dst[k] + (nx - 1) * nz2, nz2 * sizeof(double));
+    }
+    return SM_OK;
+}
+
+static double ecyl_harm(double a, double b)
+{
+    return (a == 0.0 && b == 0.0) ? 0.0 : 2. * a * b / (a + b);
+}
+
+int sm_ecyl_materials(size_t nx2, size_t nz2, const double *vp, const double *vs,
+                      const double *rho, double *const *mat, double *vpmax)
+{
+    /* e_cyl_iso.c:363-441; mat: lij l2mij mu mui muj bi bj bij */
+    if (!vp || !vs || !rho || !mat || nx2 == 0 || nz2 == 0)
+        return sm_fail(SM_EINVAL, "sm_ecyl_materials: bad argument");
+    for (int k = 0; k < 8; ++k)
+        if (!mat[k]) return sm_fail(SM_EINVAL, "sm_ecyl_materials: material %d is NULL", k);
+    double *lij = mat[0], *l2m = mat[1], *mu = mat[2], *mui = mat[3], *muj = mat[4],
+           *bi = mat[5], *bj = mat[6], *bij = mat[7];
+    const size_t N = nx2 * nz2;
+    double *m = malloc(N * sizeof *m);
+    if (!m) return sm_fail(SM_ENOMEM, "sm_ecyl_materials: out of host memory");
+    double vmax = 0.0;
+    for (size_t k = 0; k < N; ++k) {
+        if (vp[k] > vmax) vmax = vp[k];
+        lij[k] = rho[k] * (vp[k] * vp[k] - 2. * vs[k] * vs[k]);
+        m[k] = rho[k] * vs[k] * vs[k];
+        l2m[k] = lij[k] + 2.0 * m[k];
+        bij[k] = 1. / rho[k];
+    }
+    for (size_t i = 0; i < nx2; ++i) {   /* z averages */
+        const size_t c = i * nz2;
+        muj[c] = m[c];
+        bj[c] = bij[c];
+        for (size_t j = 1; j < nz2; ++j) {
+            muj[c + j] = ecyl_harm(m[c + j], m[c + j - 1]);
+            bj[c + j] = 1. / ((rho[c + j] + rho[c + j - 1]) / 2.0);
+        }
+    }
+    for (size_t j = 0; j < nz2; ++j) {   /* r averages */
+        mui[j] = m[j];
+        bi[j] = 1. / rho[j];
+        for (size_t i = 1; i < nx2; ++i) {
+            const size_t q = i * nz2 + j;
+            mui[q] = ecyl_harm(m[q], m[q - nz2]);
+            bi[q] = 1. / ((rho[q] + rho[q - nz2]) / 2.0);
+        }
+    }
+    mu[0] = m[0];
+    for (size_t j = 1; j < nz2; ++j) mu[j] = ecyl_harm(m[j], m[j - 1]);
+    for (size_t i = 1; i < nx2; ++i) {   /* four-point average */
+        const size_t c = i * nz2;
+        mu[c] = ecyl_harm(m[c], m[c - nz2]);
+        for (size_t j = 1; j < nz2; ++j) {
+            const double a = m[c + j], b = m[c + j - 1], e = m[c - nz2 + j], d = m[c - nz2 + j - 1];
+            const int none = b * e * d == 0.0 && a * e * d == 0.0 && a * b * d == 0.0 &&
+                             a * b * e == 0.0;
+            mu[c + j] = none ? 0.0 : 4. * a * b * e * d / (b * e * d + a * e * d + a * b * d + a * b * e);
+        }
+    }
+    free(m);
+    if (vpmax) *vpmax = vmax;
+    return SM_OK;
+}
+
+int sm_ecyl_cpml(size_t np, double dx, double dz, double dt, double order, double vmax,
+                 double Rc, double kappa_max, double alpha_max, int absorb, double *const *c)
+{
+    /* pml.c:2107-2185 (compute_cpml_cyl); c: ik_r ik_z ikh_z b_r c_r b_z c_z
+     * bh_z ch_z (np) then ikH_r ikH_z bH_r cH_r bH_z cH_z (np + 1) */
+    if (!c) return sm_fail(SM_EINVAL, "sm_ecyl_cpml: NULL");
+    for (int k = 0; k < 15; ++k)
+        if (!c[k]) return sm_fail(SM_EINVAL, "sm_ecyl_cpml: array %d is NULL", k);
+    const double Lx = np * dx, Lz = np * dz;
+    const double d0x = -(order + 1.) * vmax * log(Rc) / (2. * Lx);
+    const double d0z = -(order + 1.) * vmax * log(Rc) / (2. * Lz);
+    const double da = alpha_max / np, da2 = alpha_max / (np + 1);
+    for (size_t n = 0; n < np; ++n) {
+        if (!absorb) {
+            c[0][n] = c[1][n] = c[2][n] = 1.;
+            c[3][n] = c[4][n] = c[5][n] = c[6][n] = c[7][n] = c[8][n] = 0.;
+            continue;
+        }
+        const double kr = 1. + (kappa_max - 1.) * pow(((np - n) * dx / Lx), order);
+        const double kz = 1. + (kappa_max - 1.) * pow(((np - n) * dz / Lz), order);
+        /* the half-node z kappa uses dx / Lx, as pml.c:2126 does */
+        const double khz = 1. + (kappa_max - 1.) * pow(((np - n - 0.5) * dx / Lx), order);
+        c[0][n] = 1. / kr;
+        c[1][n] = 1. / kz;
+        c[2][n] = 1. / khz;
+        const double dxn = d0x * pow(((np - n) * dx / Lx), order), axn = n * da;
+        c[3][n] = exp(-(dxn / kr + axn) * dt);
+        c[4][n] = dxn * (c[3][n] - 1.) / (kr * (dxn + kr * axn));
+        const double dzn = d0z * pow(((np - n) * dz / Lz), order), azn = n * da;
+        const double dzh = d0z * pow(((np - n - 0.5) * dz / Lz), order), azh = (n + 0.5) * da;
+        c[5][n] = exp(-(dzn / kz + azn) * dt);
+        c[6][n] = dzn * (c[5][n] - 1.) / (kz * (dzn + kz * azn));
+        c[7][n] = exp(-(dzh / khz + azh) * dt);
+        c[8][n] = dzh * (c[7][n] - 1.) / (khz * (dzh + khz * azh));
+    }
+    for (size_t n = 0; n <= np; ++n) {
+        if (!absorb) {
+            c[9][n] = c[10][n] = 1.;
+            c[11][n] = c[12][n] = c[13][n] = c[14][n] = 0.;
+            continue;
+        }
+        const double kr = 1. + (kappa_max - 1.) * pow(((n + 0.5) * dx / Lx), order);
+        const double kz = 1. + (kappa_max - 1.) * pow(((n + 0.5) * dz / Lz), order);
+        c[9][n] = 1. / kr;
+        c[10][n] = 1. / kz;
+        const double dxe = d0x * pow(((n + 0.5) * dx / Lx), order), axe = (np - n - 0.5) * da2;
+        c[11][n] = exp(-(dxe / kr + axe) * dt);
+        c[12][n] = dxe * (c[11][n] - 1.) / (kr * (dxe + kr * axe));
+        const double dze = d0z * pow(((n + 0.5) * dz / Lz), order), aze = (np - n - 0.5) * da2;
+        c[13][n] = exp(-(dze / kz + aze) * dt);
+        c[14][n] = dze * (c[13][n] - 1.) / (kz * (dze + kz * aze));
+    }
+    return SM_OK;
+}
+
+size_t sm_ecyl_kurkjian(double A, double f, double dt, double lij_at_src, double r_src,
+                        double dx, double dz, int n, size_t maxlen, double *fct)
+{
+    /* src.c:202-228: peak-1 Ricker times A lambda/(2 pi) eps 2/(dx^2 dz)
+     * (r/dx)^n, eps = 2 for n > 0 */
+    const double pi = 4.0 * atan(1.0), pi2 = pi * pi;
+    const double eps = n > 0 ? 2.0 : 1.0;
+    const double term = lij_at_src / (2. * pi) * eps * 2. / (dx * dx * dz) * pow(r_src / dx, n);
+    const double tcut = 1.0 / f;
+    size_t len = (size_t)ceil(tcut * 2.0 / dt);
+    if (!fct) return len;
+    if (len > maxlen) len = maxlen;
+    double amax = 0.0;
+    for (size_t i = 0; i < len; ++i) {
+        const double t = i * dt - tcut;
+        const double K = pi2 * f * f * t * t;
+        fct[i] = 2. * pi2 * f * f * (1.0 - 2.0 * K) * exp(-K);
+        if (fabs(fct[i]) > amax) amax = fabs(fct[i]);
+    }
+    for (size_t i = 0; i < len; ++i) fct[i] *= A / amax * term;
+    return len;
+}

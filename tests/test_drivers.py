@@ -1,4 +1,4 @@
-"""The drop-in programs e_iso_gpu / a_iso_3d_gpu: argument and input errors
+"""The drop-in programs e_iso_gpu / a_iso_3d_gpu / e_cyl_iso_gpu: argument and input errors
 come back as a non-zero exit with the reference's message (CPU: these paths
 return before the device is used); on the GPU the trace files they write
 match the reference's (golden fixtures) in format and values."""
@@ -66,6 +66,9 @@ def test_unequal_spacing_is_refused(tmp_path):
 @pytest.mark.parametrize("path", GOLDEN, ids=[os.path.basename(p)[:-4] for p in GOLDEN])
 def test_drop_in_programs_write_the_reference_traces(path, tmp_path):
     p, kind, program, ref_t, ref_v = G.load(path)
+    if kind == "ecyl":
+        _check_ecyl_drop_in(p, ref_t, ref_v, tmp_path, "fp32")
+        return
     if kind == "eiso":
         par = p.write(str(tmp_path), shot=0, basename=p.name)
         r = run("e_iso_gpu", ["-p", os.path.basename(par)], tmp_path)
@@ -247,3 +250,52 @@ def test_a3d_snapshot_plane(tmp_path):
     ref = vol[n:-n, iy, n:-n]
     np.testing.assert_allclose(val.reshape(ref.shape), 1e3 * ref, rtol=1e-5,
                                atol=1e-5 * np.abs(1e3 * ref).max())
+
+
+def _check_ecyl_drop_in(p, ref_t, ref_v, tmp_path, precision):
+    """e_cyl_iso_gpu against the reference's traces, per record component:
+    1e-5 in FP32 (1e-4 for div and curl, differences of neighbouring
+    velocities), text precision (2e-6) in FP64."""
+    par = p.write(str(tmp_path))
+    r = run("e_cyl_iso_gpu", ["-p", os.path.basename(par), "-P", precision], tmp_path)
+    assert r.returncode == 0, r.stderr
+    t, v = F.read_traces(str(tmp_path), p.name, len(p.receivers))
+    assert [len(a) for a in v] == [len(a) for a in ref_v]
+    for a, b in zip(t, ref_t):
+        np.testing.assert_allclose(a, b, rtol=1e-6)
+    for comp in sorted({q[0] for q in p.receivers}):
+        ks = [k for k, q in enumerate(p.receivers) if q[0] == comp]
+        a = np.concatenate([v[k] for k in ks])
+        b = np.concatenate([ref_v[k] for k in ks])
+        if np.abs(b).max() < 1e-300:
+            assert np.abs(a).max() < 1e-300, comp
+            continue
+        tol = 2e-6 if precision == "fp64" else (1e-4 if comp in ("div", "curl") else 1e-5)
+        assert H.rel_l2([a], [b]) < tol, (comp, H.rel_l2([a], [b]))
+
+
+ECYL_GOLDEN = [q for q in GOLDEN if os.path.basename(q).startswith("ecyl_")]
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("path", ECYL_GOLDEN, ids=[os.path.basename(q)[:-4] for q in ECYL_GOLDEN])
+def test_ecyl_drop_in_fp64_matches_the_reference_to_text_precision(path, tmp_path):
+    p, kind, program, ref_t, ref_v = G.load(path)
+    _check_ecyl_drop_in(p, ref_t, ref_v, tmp_path, "fp64")
+
+
+def test_ecyl_drop_in_refuses_what_it_cannot_run(tmp_path):
+    p = W.ecyl_case(nx=20, nz=24, npml=4, nsteps=10, nrec=2)
+    par = p.write(str(tmp_path))
+    F.write_src(os.path.join(str(tmp_path), "src.dat"), p.sources, ntemplate=9)
+    r = run("e_cyl_iso_gpu", ["-p", os.path.basename(par)], tmp_path)
+    assert r.returncode != 0 and "1-point sources" in r.stderr
+    (tmp_path / "model.dat").write_text("4 4\n1.0 1.0\n0 0\nisotropic_elastic\n" +
+                                        "3000 1700 2000\n" * 16)
+    r = run("e_cyl_iso_gpu", ["-p", os.path.basename(par)], tmp_path)
+    assert r.returncode != 0 and "not isotropic_elastic_cyl" in r.stderr
+    q = W.ecyl_case(nx=20, nz=24, npml=4, nsteps=10, nrec=2)
+    q.dt_ms *= 3.0
+    par = q.write(str(tmp_path / "cfl"))
+    r = run("e_cyl_iso_gpu", ["-p", "run.par"], tmp_path / "cfl")
+    assert r.returncode != 0 and "Time step too large" in r.stderr

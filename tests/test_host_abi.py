@@ -140,3 +140,27 @@ def test_device_bytes_estimates_grow_with_the_problem():
     assert lib.sm_a3d_device_bytes(288, 288, 288, 16, 0, 0, 0, C.byref(b2)) == 0
     assert b2.value > b1.value >= 8 * 288 * 288 * 288 * 2
     assert lib.sm_eiso_device_bytes(10, 10, 2, 9, 1, 0, 0, C.byref(b1)) == 1   # bad precision
+
+
+def test_ecyl_host_setup_equals_the_oracle_bit_for_bit():
+    """Materials, CPML coefficients and the Kurkjian wavelet of the library's
+    C host code against the oracle's restatement, with and without the
+    absorbing layer."""
+    from oracle import oracle as O
+    import harness as H
+    from seismod_b200 import api
+    from seismod_b200 import workloads as W
+    for kw in (dict(n=1, src="Kurkjian"), dict(n=0, src="Fz", absorb=0),
+               dict(n=2, src="Bulk", dx=1.5, dz=1.0)):
+        p = W.ecyl_case(nx=34, nz=41, npml=6, nsteps=40, **kw)
+        q = api.ecyl_inputs(p)
+        s = H.ecyl_setup(p)
+        for k, nm in enumerate(O.ECYL_MATS):
+            np.testing.assert_array_equal(q["mats"][k], s["mats"][nm], err_msg=nm)
+        for k in range(15):
+            np.testing.assert_array_equal(q["coef"][k], s["coef"][k])
+        srcs = H.ecyl_sources(p, s)
+        for k, (idx, typ, w) in enumerate(srcs):
+            assert q["src"][0][k] == idx
+            np.testing.assert_array_equal(q["src"][2][k][:q["src"][3][k]], w)
+        assert q["nsteps"] == s["nsteps"]
