@@ -131,8 +131,22 @@ def eiso_bytes_per_step(p, nshots, s, m=4):
     return nshots * (nint * 10 * s + (nall - nint) * 20 * s) + nall * 3 * m
 
 
+def ecyl_bytes_per_step(p, s, m=4):
+    """cells (9 fields read and written, 8 materials read) + the CPML memory
+    variables of the z strips (6) and the outer radial strip (12 for mode 0,
+    18 for n > 0), each read and written."""
+    npml = p.np_used
+    nx2, nz2 = p.nx + npml, p.nz + 2 * npml
+    nr = 18 if p.n > 0 else 12
+    return nx2 * nz2 * (18 * s + 8 * m) + 2 * s * (6 * nx2 * 2 * npml + nr * npml * nz2)
+
+
 def make_workload(name, size=None):
     from seismod_b200 import workloads as W
+    if name == "ecyl":
+        p = W.ecyl_case(nx=2000, nz=4000, npml=20, nsteps=1000, n=1, src="Fz", nrec=64, seed=7)
+        return ("ecyl", p, "e_cyl_iso 2000 x 4000 (r x z, +20 CPML), dr = dz = 1 m, azimuthal "
+                           "mode 1, Fz source, 1000-step shot")
     if name == "a3d" and size:
         return ("a3d", W.cfg1(n=size),
                 f"a_iso_3d {size}^3 (+2x16 CPML), dx 5 m, cfg1 model family, 1000-step shot")
@@ -171,6 +185,8 @@ GRAPH = 16
 
 def device_for(kind, p, precision, dev_id, shots=None):
     from seismod_b200 import api
+    if kind == "ecyl":
+        return api.ecyl_device(p, precision, dev_id)   # one launch shape, no graphs
     if kind == "a3d":
         dev, n = api.a3d_device(p, precision, dev_id)
     else:
@@ -203,6 +219,9 @@ def run_ours(args, rank, world, local_rank, torch, dist):
     nshots = len(p.shots) if kind == "eiso" else 1
     if kind == "a3d":
         bps = a3d_bytes_per_step(p, sbytes, mbytes)
+        cells = p.cells
+    elif kind == "ecyl":
+        bps = ecyl_bytes_per_step(p, sbytes, mbytes)
         cells = p.cells
     else:
         bps = eiso_bytes_per_step(p, nshots, sbytes, mbytes)
@@ -260,9 +279,11 @@ def precision_side(kind, p, local_rank, K):
     from seismod_b200 import api
     import torch
     run = api.run_a3d if kind == "a3d" else (lambda q, pr, d: api.run_eiso(q, pr, [0], d)[0])
+    if kind == "ecyl":
+        run = api.run_ecyl
     ref64 = run(p, "fp64", local_rank)
     res = {}
-    for prec in ("fp32", "fp16", "bf16"):
+    for prec in (("fp32",) if kind == "ecyl" else ("fp32", "fp16", "bf16")):
         try:
             tr = run(p, prec, local_rank)
             err = trace_err(tr, ref64)
@@ -366,6 +387,9 @@ def e2e(kind, p, K, local_rank):
     if kind == "a3d":
         tr = dev.traces_array()
         d2h = tr.size * 8
+    elif kind == "ecyl":
+        tr = dev.traces()
+        d2h = sum(len(x) for x in tr) * 8
     else:
         tr = [dev.traces(s) for s in range(dev.nshots)]
         d2h = sum(sum(len(x) for x in t) for t in tr) * 8
@@ -375,6 +399,10 @@ def e2e(kind, p, K, local_rank):
         n2 = [n + 2 * p.npml for n in p.shape]
         pitch = math.ceil(n2[2] / 32) * 32
         h2d = 2 * n2[0] * n2[1] * pitch * 4
+        cells = p.cells
+    elif kind == "ecyl":
+        pitch = math.ceil((p.nz + 2 * p.np_used) / 32) * 32
+        h2d = 8 * (p.nx + p.np_used) * pitch * 4   # the eight materials
         cells = p.cells
     else:
         pitch = math.ceil((p.nz + 2 * p.npml) / 32) * 32
@@ -414,17 +442,20 @@ def reference_rate(kind, p, steps):
     if nrec + 64 > nofile:  # the reference keeps one open file per trace
         q = dataclasses.replace(p, receivers=p.receivers[: max(nofile - 64, 1)])
     prog = "a_iso_3d" if kind == "a3d" else ("e_iso" if p.nx <= p.nz else "e_iso_lrfix")
+    if kind == "ecyl":
+        prog = "e_cyl_iso"
     times = []
     for n in (2, 2 + steps):
         r = dataclasses.replace(q, duration=W.steps_duration(n, q.dt_ms))
-        if kind == "a3d":
+        if kind in ("a3d", "ecyl"):
             par = r.write(os.path.join(d, f"n{n}"), profile_1d=True)
         else:
             par = r.write(os.path.join(d, f"n{n}"), shot=0, profile_1d=True)
         times.append(O.run_reference(prog, par, os.path.dirname(par), timeout=3600))
     dt = (times[1] - times[0]) / steps
     cells = p.cells
-    sample = (f"{prog} (oracle/_ref, gcc -O3, OpenMP, 3 threads as hard-coded), "
+    threads = 4 if kind == "ecyl" else 3
+    sample = (f"{prog} (oracle/_ref, gcc -O3, OpenMP, {threads} threads as hard-coded), "
               f"{steps} steps of the full grid, {len(q.receivers)} receivers, "
               f"1-D profile model file; time(2+{steps} steps) - time(2 steps)")
     return cells / dt / 1e9, sample
@@ -439,7 +470,7 @@ def run_reference_arm(args, rank, world):
         # stream's first e_iso request stands for the stream
         p = next(r.problem for r in p if r.kind == "eiso")
         kind = "eiso"
-    steps = max(1, min(args.steps, 12 if kind == "a3d" else 200))
+    steps = max(1, min(args.steps, 12 if kind == "a3d" else (20 if kind == "ecyl" else 200)))
     rate, sample = reference_rate(kind, p, steps)
     if rate is None:
         return {"impl": "reference", "unavailable": sample}
@@ -448,7 +479,8 @@ def run_reference_arm(args, rank, world):
             "ms_per_step": round(p.cells / (rate * 1e9) * 1e3, 3),
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic", "config": {"workload": desc},
-            "cpu_baseline": {"value": round(rate, 4), "unit": "Gcell/s", "cores": 3,
+            "cpu_baseline": {"value": round(rate, 4), "unit": "Gcell/s",
+                             "cores": 4 if kind == "ecyl" else 3,
                              "kind": "reference", "sample": sample},
             "e2e": {"value": round(rate, 4), "unit": "Gcell/s", "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": 0}}
@@ -463,7 +495,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=20)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="a3d",
-                    choices=["a3d", "a3d512", "eiso", "eiso1", "serve", "serve_overload"])
+                    choices=["a3d", "a3d512", "eiso", "eiso1", "ecyl", "serve", "serve_overload"])
     ap.add_argument("--precision", default="fp32", choices=["fp32", "fp64", "fp16", "bf16"])
     ap.add_argument("--no-side", action="store_true", help="skip precision / CPU side runs")
     ap.add_argument("--no-tune", action="store_true", help="default launch configuration")
@@ -509,10 +541,11 @@ def main():
     if rank == 0 and not args.no_side:
         out["precisions"] = precision_side(kind, p, local_rank, args.steps)
         out["e2e"] = e2e(kind, p, args.steps, local_rank)
-        steps = 12 if kind == "a3d" else 200
+        steps = 12 if kind == "a3d" else (20 if kind == "ecyl" else 200)
         rate, sample = reference_rate(kind, p, steps)
         if rate is not None:
-            out["cpu_baseline"] = {"value": round(rate, 4), "unit": "Gcell/s", "cores": 3,
+            out["cpu_baseline"] = {"value": round(rate, 4), "unit": "Gcell/s",
+                                   "cores": 4 if kind == "ecyl" else 3,
                                    "kind": "reference", "sample": sample}
         else:
             out["cpu_baseline"] = {"value": None, "unit": "Gcell/s", "cores": 0,

@@ -570,6 +570,18 @@ class ECylDevice:
                                                  L.szptr(counts)))
         return [out[k, :counts[k]].copy() for k in range(n)]
 
+    def set_timing(self, on=True):
+        L.check(L.load().sm_ecyl_set_timing(self._h, 1 if on else 0))
+
+    def kernel_stats(self, reset=False):
+        """(summed velocity + source + stress ms, timed steps, all kernel launches)."""
+        ms = C.c_double()
+        n = C.c_size_t()
+        a = C.c_size_t()
+        L.check(L.load().sm_ecyl_kernel_stats(self._h, 1 if reset else 0, C.byref(ms),
+                                              C.byref(n), C.byref(a)))
+        return ms.value, n.value, a.value
+
     def get_field(self, name):
         out = np.zeros(self.shape)
         L.check(L.load().sm_ecyl_get_field(self._h, ECYL_FIELD[name], L.dptr(out)))

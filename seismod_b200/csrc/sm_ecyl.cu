@@ -16,6 +16,8 @@
 // operations (propagate.c:2706-3309 for mode 0, :3312-4088 for n > 0); this
 // file is compiled without FMA contraction, so the FP64 build follows the
 // FP64 reference to the last bit where the reference is built the same way.
+// The FP32 build multiplies by reciprocals of the grid lengths instead of
+// dividing (ECylQ).
 // Materials arrive multiplied by dt on the host in FP64 (the reference's
 // dt*b*(...) evaluates dt*b first).
 //
@@ -46,7 +48,8 @@ enum { RV_DTRR, RV_TRR1, RV_TRT1, RV_TTT1, RV_TRT2, RV_DTRT, RV_TTT2, RV_DTRZ, R
 template <typename C>
 struct ECylArgs {
     int nx, nz, np, nx2, nz2, pitch, n;
-    C dx, dz;
+    C dx, dz, idx, idz;   // and 1/dx, 1/dz (FP32 path)
+    const C *inv;         // FP32 path: per column 1/(2 i dx), 1/(i dx), 1/((i+1/2) dx), 1/(2 (i+1/2) dx)
     C *f[9];
     const C *m[8];    // dt * (lij l2mij mu mui muj bi bj bij)
     const C *k;       // the 15 coefficient arrays, back to back
@@ -59,7 +62,9 @@ struct ECylDev {
     const ECylArgs<C> &a;
     int i, j;
     __device__ C F(int k, int ii, int jj) const { return a.f[k][(long long)ii * a.pitch + jj]; }
-    __device__ C M(int k) const { return a.m[k][(long long)i * a.pitch + j]; }
+    // a field this launch only reads, through the read-only cache path
+    __device__ C G(int k, int ii, int jj) const { return __ldg(a.f[k] + (long long)ii * a.pitch + jj); }
+    __device__ C M(int k) const { return __ldg(a.m[k] + (long long)i * a.pitch + j); }
     __device__ C K(int arr, int idx) const {
         const int np = a.np;
         const int off = arr < 9 ? arr * np : 9 * np + (arr - 9) * (np + 1);
@@ -69,8 +74,8 @@ struct ECylDev {
     // row -1 of column i is row nz2-1 of column i-1, and before the array
     // (i = 0) it is taken as zero
     __device__ C below(int k) const {
-        if (j > 0) return F(k, i, j - 1);
-        return i > 0 ? F(k, i - 1, a.nz2 - 1) : C(0);
+        if (j > 0) return G(k, i, j - 1);
+        return i > 0 ? G(k, i - 1, a.nz2 - 1) : C(0);
     }
     __device__ C cpml(C *psi, C b, C c, C ik, C d) const {
         const C p = b * *psi + c * d;
@@ -119,6 +124,37 @@ struct ECylDev {
     }
 };
 
+// Quotients by the grid's lengths: dx, dz, 2 i dx, i dx, (i + 1/2) dx and
+// 2 (i + 1/2) dx.  FP64 divides, as the reference does; FP32 multiplies by
+// reciprocals formed in FP64 on the host (per column), which keeps the FP32
+// path far from its own error bound and avoids the division routine.
+template <typename C>
+struct ECylQ {
+    static constexpr bool exact = sizeof(C) == 8;
+    C dx, dz, idx, idz;
+    C r2i, ri, r5, r25;       // denominators of column i (exact path)
+    C i2i, ii, i5, i25;       // their reciprocals (FP32 path)
+    __device__ ECylQ(const ECylArgs<C> &a, int i) : dx(a.dx), dz(a.dz), idx(a.idx), idz(a.idz) {
+        r2i = C(2.) * C(i) * dx;
+        ri = C(i) * dx;
+        r5 = (C(i) + C(0.5)) * dx;
+        r25 = C(2.) * (C(i) + C(0.5)) * dx;
+        if (!exact) {
+            const long long s = a.nx2;
+            i2i = a.inv[i];
+            ii = a.inv[s + i];
+            i5 = a.inv[2 * s + i];
+            i25 = a.inv[3 * s + i];
+        }
+    }
+    __device__ C x(C v) const { return exact ? v / dx : v * idx; }
+    __device__ C z(C v) const { return exact ? v / dz : v * idz; }
+    __device__ C twoi(C v) const { return exact ? v / r2i : v * i2i; }
+    __device__ C i1(C v) const { return exact ? v / ri : v * ii; }
+    __device__ C half(C v) const { return exact ? v / r5 : v * i5; }
+    __device__ C twohalf(C v) const { return exact ? v / r25 : v * i25; }
+};
+
 // vr, vt, vz of cell (i, j): update_vr/vt/vz_cyl (mode 0) or *_cyl_n (n > 0)
 template <typename C, bool NPOS>
 __global__ void __launch_bounds__(256) ecyl_velocity_kernel(const ECylArgs<C> a) {
@@ -126,32 +162,30 @@ __global__ void __launch_bounds__(256) ecyl_velocity_kernel(const ECylArgs<C> a)
     const int i = blockIdx.y;
     if (j >= a.nz2) return;
     const ECylDev<C> d{a, i, j};
-    const C dx = a.dx, dz = a.dz;
+    const ECylQ<C> Q(a, i);
     const int n = a.n;
     const long long q = (long long)i * a.pitch + j;
     // vr: rows [0, nz2-1), columns from 1 (from 0 for odd n: the axis)
     if (j + 1 < a.nz2 && (i >= 1 || (NPOS && (n % 2)))) {
-        C ddz = (d.F(C_TRZ, i, j + 1) - d.F(C_TRZ, i, j)) / dz;
+        C ddz = Q.z(d.G(C_TRZ, i, j + 1) - d.G(C_TRZ, i, j));
         if (d.zhalf()) ddz = d.zf_half(ZV_TRZ, ddz);
         C s;
         if (i == 0) {
-            s = (d.F(C_TRR, i, j) - -d.F(C_TRR, i, j)) / dx + ddz;
+            s = Q.x(d.G(C_TRR, i, j) - -d.G(C_TRR, i, j)) + ddz;
         } else if (i < a.nx) {
-            const C A = (d.F(C_TRR, i, j) - d.F(C_TRR, i - 1, j)) / dx;
-            const C B = (d.F(C_TRR, i, j) + d.F(C_TRR, i - 1, j)) / (C(2.) * C(i) * dx);
-            const C D = (d.F(C_TTT, i, j) + d.F(C_TTT, i - 1, j)) / (C(2.) * C(i) * dx);
+            const C A = Q.x(d.G(C_TRR, i, j) - d.G(C_TRR, i - 1, j));
+            const C B = Q.twoi(d.G(C_TRR, i, j) + d.G(C_TRR, i - 1, j));
+            const C D = Q.twoi(d.G(C_TTT, i, j) + d.G(C_TTT, i - 1, j));
             if (NPOS)
-                s = A + B + C(n) * d.F(C_TRT, i, j) / (C(i) * dx) - D + ddz;
+                s = A + B + Q.i1(C(n) * d.G(C_TRT, i, j)) - D + ddz;
             else
                 s = A + B - D + ddz;
         } else {
-            const C A = d.rf_node(RV_DTRR, (d.F(C_TRR, i, j) - d.F(C_TRR, i - 1, j)) / dx);
-            const C B = d.rf_node(RV_TRR1, (d.F(C_TRR, i, j) + d.F(C_TRR, i - 1, j)) /
-                                               (C(2.) * C(i) * dx));
-            const C D = d.rf_node(RV_TTT1, (d.F(C_TTT, i, j) + d.F(C_TTT, i - 1, j)) /
-                                               (C(2.) * C(i) * dx));
+            const C A = d.rf_node(RV_DTRR, Q.x(d.G(C_TRR, i, j) - d.G(C_TRR, i - 1, j)));
+            const C B = d.rf_node(RV_TRR1, Q.twoi(d.G(C_TRR, i, j) + d.G(C_TRR, i - 1, j)));
+            const C D = d.rf_node(RV_TTT1, Q.twoi(d.G(C_TTT, i, j) + d.G(C_TTT, i - 1, j)));
             if (NPOS) {
-                const C E = d.rf_node(RV_TRT1, d.F(C_TRT, i, j) / (C(i) * dx));
+                const C E = d.rf_node(RV_TRT1, Q.i1(d.G(C_TRT, i, j)));
                 s = A + B + C(n) * E - D + ddz;
             } else {
                 s = A + B - D + ddz;
@@ -160,23 +194,22 @@ __global__ void __launch_bounds__(256) ecyl_velocity_kernel(const ECylArgs<C> a)
         a.f[C_VR][q] += d.M(CM_BJ) * s;
     }
     if (i + 1 < a.nx2) {
-        const C r5 = (C(i) + C(0.5)) * dx;
         // vt: rows [0, nz2-1)
         if (j + 1 < a.nz2) {
-            C ddz = (d.F(C_TTZ, i, j + 1) - d.F(C_TTZ, i, j)) / dz;
+            C ddz = Q.z(d.G(C_TTZ, i, j + 1) - d.G(C_TTZ, i, j));
             if (d.zhalf()) ddz = d.zf_half(ZV_TTZ, ddz);
-            const C A = (d.F(C_TRT, i + 1, j) + d.F(C_TRT, i, j)) / r5;
-            const C B = (d.F(C_TRT, i + 1, j) - d.F(C_TRT, i, j)) / dx;
+            const C A = Q.half(d.G(C_TRT, i + 1, j) + d.G(C_TRT, i, j));
+            const C B = Q.x(d.G(C_TRT, i + 1, j) - d.G(C_TRT, i, j));
             C s;
             if (i + 1 < a.nx) {
                 if (NPOS)
-                    s = A + B - C(n) * d.F(C_TTT, i, j) / r5 + ddz;
+                    s = A + B - Q.half(C(n) * d.G(C_TTT, i, j)) + ddz;
                 else
                     s = A + B + ddz;
             } else {
                 const C fa = d.rf_half(RV_TRT2, A), fb = d.rf_half(RV_DTRT, B);
                 if (NPOS) {
-                    const C E = d.rf_half(RV_TTT2, d.F(C_TTT, i, j) / r5);
+                    const C E = d.rf_half(RV_TTT2, Q.half(d.G(C_TTT, i, j)));
                     s = fa + fb - C(n) * E + ddz;
                 } else {
                     s = fa + fb + ddz;
@@ -186,20 +219,20 @@ __global__ void __launch_bounds__(256) ecyl_velocity_kernel(const ECylArgs<C> a)
         }
         // vz: rows from 1 (from 0 without a PML)
         if (j >= 1 || a.np == 0) {
-            C ddz = (d.F(C_TZZ, i, j) - d.below(C_TZZ)) / dz;
+            C ddz = Q.z(d.G(C_TZZ, i, j) - d.below(C_TZZ));
             if (d.znode()) ddz = d.zf_node(ZV_TZZ, ddz);
-            const C A = (d.F(C_TRZ, i + 1, j) - d.F(C_TRZ, i, j)) / dx;
-            const C B = (d.F(C_TRZ, i + 1, j) + d.F(C_TRZ, i, j)) / (C(2.) * (C(i) + C(0.5)) * dx);
+            const C A = Q.x(d.G(C_TRZ, i + 1, j) - d.G(C_TRZ, i, j));
+            const C B = Q.twohalf(d.G(C_TRZ, i + 1, j) + d.G(C_TRZ, i, j));
             C s;
             if (i + 1 < a.nx) {
                 if (NPOS)
-                    s = ddz + A + B + C(n) * d.F(C_TTZ, i, j) / r5;
+                    s = ddz + A + B + Q.half(C(n) * d.G(C_TTZ, i, j));
                 else
                     s = ddz + A + B;
             } else {
                 const C fa = d.rf_half(RV_DTRZ, A), fb = d.rf_half(RV_TRZ, B);
                 if (NPOS) {
-                    const C E = d.rf_half(RV_TTZ, d.F(C_TTZ, i, j) / r5);
+                    const C E = d.rf_half(RV_TTZ, Q.half(d.G(C_TTZ, i, j)));
                     s = ddz + fa + fb + C(n) * E;
                 } else {
                     s = ddz + fa + fb;
@@ -217,15 +250,15 @@ __global__ void __launch_bounds__(256) ecyl_stress_kernel(const ECylArgs<C> a) {
     const int i = blockIdx.y;
     if (j >= a.nz2) return;
     const ECylDev<C> d{a, i, j};
-    const C dx = a.dx, dz = a.dz;
+    const ECylQ<C> Q(a, i);
     const int n = a.n;
     const long long q = (long long)i * a.pitch + j;
     // trr, ttt, tzz: columns [0, nx2-1), rows [0, nz2-1)
     if (i + 1 < a.nx2 && j + 1 < a.nz2) {
-        C dvrdr = (d.F(C_VR, i + 1, j) - d.F(C_VR, i, j)) / dx;
-        C vrr = (d.F(C_VR, i + 1, j) + d.F(C_VR, i, j)) / (C(2.) * (C(i) + C(0.5)) * dx);
-        C vtr = NPOS ? d.F(C_VT, i, j) / ((C(i) + C(0.5)) * dx) : C(0);
-        C dvzdz = (d.F(C_VZ, i, j + 1) - d.F(C_VZ, i, j)) / dz;
+        C dvrdr = Q.x(d.G(C_VR, i + 1, j) - d.G(C_VR, i, j));
+        C vrr = Q.twohalf(d.G(C_VR, i + 1, j) + d.G(C_VR, i, j));
+        C vtr = NPOS ? Q.half(d.G(C_VT, i, j)) : C(0);
+        C dvzdz = Q.z(d.G(C_VZ, i, j + 1) - d.G(C_VZ, i, j));
         if (i + 1 >= a.nx) {
             dvrdr = d.rf_half(RV_DVR, dvrdr);
             vrr = d.rf_half(RV_VR1, vrr);
@@ -245,9 +278,9 @@ __global__ void __launch_bounds__(256) ecyl_stress_kernel(const ECylArgs<C> a) {
     }
     // trz (update_trz_cyl for every n): columns from 1, rows from 1
     if (i >= 1 && (j >= 1 || a.np == 0)) {
-        C ddz = (d.F(C_VR, i, j) - d.below(C_VR)) / dz;
+        C ddz = Q.z(d.G(C_VR, i, j) - d.below(C_VR));
         if (d.znode()) ddz = d.zf_trz(ddz);
-        C ddr = (d.F(C_VZ, i, j) - d.F(C_VZ, i - 1, j)) / dx;
+        C ddr = Q.x(d.G(C_VZ, i, j) - d.G(C_VZ, i - 1, j));
         if (i >= a.nx) {
             const int ii = i - a.nx;
             ddr = d.cpml(d.rvar(RV_DVZ, ii), d.K(K_BHR_E, ii), d.K(K_CHR_E, ii),
@@ -259,20 +292,19 @@ __global__ void __launch_bounds__(256) ecyl_stress_kernel(const ECylArgs<C> a) {
     if (i >= 1 || (NPOS && (n % 2))) {
         C s;
         if (i == 0) {
-            s = (d.F(C_VT, i, j) - -d.F(C_VT, i, j)) / dx;
+            s = Q.x(d.G(C_VT, i, j) - -d.G(C_VT, i, j));
         } else if (i < a.nx) {
-            const C A = (d.F(C_VT, i, j) - d.F(C_VT, i - 1, j)) / dx;
-            const C D = (d.F(C_VT, i, j) + d.F(C_VT, i - 1, j)) / (C(2.) * C(i) * dx);
+            const C A = Q.x(d.G(C_VT, i, j) - d.G(C_VT, i - 1, j));
+            const C D = Q.twoi(d.G(C_VT, i, j) + d.G(C_VT, i - 1, j));
             if (NPOS)
-                s = A - C(n) * d.F(C_VR, i, j) / (C(i) * dx) - D;
+                s = A - Q.i1(C(n) * d.G(C_VR, i, j)) - D;
             else
                 s = A - D;
         } else {
-            const C A = d.rf_node(RV_DVT, (d.F(C_VT, i, j) - d.F(C_VT, i - 1, j)) / dx);
-            const C D = d.rf_node(RV_VT2, (d.F(C_VT, i, j) + d.F(C_VT, i - 1, j)) /
-                                              (C(2.) * C(i) * dx));
+            const C A = d.rf_node(RV_DVT, Q.x(d.G(C_VT, i, j) - d.G(C_VT, i - 1, j)));
+            const C D = d.rf_node(RV_VT2, Q.twoi(d.G(C_VT, i, j) + d.G(C_VT, i - 1, j)));
             if (NPOS) {
-                const C B = d.rf_node(RV_VR2, d.F(C_VR, i, j) / (C(i) * dx));
+                const C B = d.rf_node(RV_VR2, Q.i1(d.G(C_VR, i, j)));
                 s = A - C(n) * B - D;
             } else {
                 s = A - D;
@@ -282,23 +314,22 @@ __global__ void __launch_bounds__(256) ecyl_stress_kernel(const ECylArgs<C> a) {
     }
     // ttz: columns [0, nx2-1), rows from 1 (from 0 without a PML)
     if (i + 1 < a.nx2 && (j >= 1 || a.np == 0)) {
-        const C diff = d.F(C_VT, i, j) - d.below(C_VT);
+        const C diff = d.G(C_VT, i, j) - d.below(C_VT);
         const C mui = d.M(CM_MUI);
         const bool zp = d.znode();
         if (!NPOS) {
             // interior rows: dt mui (vt_j - vt_j-1) / dz, the division last
             if (zp)
-                a.f[C_TTZ][q] += mui * d.zf_node(ZV_VT, diff / dz);
+                a.f[C_TTZ][q] += mui * d.zf_node(ZV_VT, Q.z(diff));
             else
-                a.f[C_TTZ][q] += mui * diff / dz;
+                a.f[C_TTZ][q] += Q.z(mui * diff);
         } else {
-            const C ddz = zp ? d.zf_node(ZV_VT, diff / dz) : diff / dz;
-            const C r5 = (C(i) + C(0.5)) * dx;
+            const C ddz = zp ? d.zf_node(ZV_VT, Q.z(diff)) : Q.z(diff);
             C s;
             if (i + 1 < a.nx)
-                s = ddz - C(n) * d.F(C_VZ, i, j) / r5;
+                s = ddz - Q.half(C(n) * d.G(C_VZ, i, j));
             else
-                s = ddz - C(n) * d.rf_half(RV_VZ, d.F(C_VZ, i, j) / r5);
+                s = ddz - C(n) * d.rf_half(RV_VZ, Q.half(d.G(C_VZ, i, j)));
             a.f[C_TTZ][q] += mui * s;
         }
     }
@@ -406,7 +437,7 @@ struct sm_ecyl {
     size_t it = 0;
     size_t elem = 4;
     cudaStream_t stream = nullptr;
-    DevBuf fields, mats, coef, zm, rm;
+    DevBuf fields, mats, coef, zm, rm, inv;
     size_t fstride = 0;   // elements between fields
     // sources
     std::vector<ECylSrc> src;
@@ -440,6 +471,9 @@ ECylArgs<C> ecyl_args(sm_ecyl *h) {
     a.n = h->n;
     a.dx = static_cast<C>(h->dx);
     a.dz = static_cast<C>(h->dz);
+    a.idx = static_cast<C>(1.0 / h->dx);
+    a.idz = static_cast<C>(1.0 / h->dz);
+    a.inv = h->inv.as<C>();
     C *f = h->fields.as<C>();
     for (int k = 0; k < 9; ++k) a.f[k] = f + (size_t)k * h->fstride;
     const C *m = h->mats.as<C>();
@@ -580,6 +614,20 @@ extern "C" int sm_ecyl_create(int device, size_t nx, size_t nz, size_t np, int n
                  : upload_pitched<float>(h->mats, k, h->fstride, tmp.data(), h->nx2, h->nz2, h->pitch, h->stream);
         if (rc) return rc;
     }
+    {   // per-column reciprocals of the radial lengths (FP32 path)
+        const size_t nx2 = (size_t)h->nx2;
+        std::vector<double> r(4 * nx2, 0.0);
+        for (size_t i = 0; i < nx2; ++i) {
+            r[i] = i ? 1.0 / (2. * i * dx) : 0.0;
+            r[nx2 + i] = i ? 1.0 / (i * dx) : 0.0;
+            r[2 * nx2 + i] = 1.0 / ((i + 0.5) * dx);
+            r[3 * nx2 + i] = 1.0 / (2. * (i + 0.5) * dx);
+        }
+        if ((rc = h->inv.alloc(r.size() * h->elem))) return rc;
+        rc = precision == SM_FP64 ? upload_convert<double>(h->inv.p, r.data(), r.size(), h->stream)
+                                  : upload_convert<float>(h->inv.p, r.data(), r.size(), h->stream);
+        if (rc) return rc;
+    }
     std::vector<double> kt;
     for (int k = 0; k < 15; ++k) kt.insert(kt.end(), coef[k], coef[k] + (k < 9 ? np : np + 1));
     kt.push_back(0.0);
@@ -601,6 +649,7 @@ extern "C" int sm_ecyl_destroy(sm_ecyl_t h) {
         h->coef.release();
         h->zm.release();
         h->rm.release();
+        h->inv.release();
         h->d_src.release();
         h->d_vals.release();
         h->d_kurk.release();
