@@ -73,7 +73,7 @@ def a3d_pad_model(vp, rho, npml):
     nx, ny, nz = vp.shape
     vp, rho = _f64(vp), _f64(rho)
     shp = (nx + 2 * npml, ny + 2 * npml, nz + 2 * npml)
-    vpp, rhop = np.zeros(shp), np.zeros(shp)
+    vpp, rhop = np.empty(shp), np.empty(shp)   # every cell is written
     L.check(L.load().sm_a3d_pad_model(nx, ny, nz, npml, L.dptr(vp), L.dptr(rho), L.dptr(vpp),
                                       L.dptr(rhop)))
     return vpp, rhop
@@ -408,6 +408,19 @@ def a3d_index(p, x, y, z):
     return (i * ny2 + j) * nz2 + k
 
 
+def _c_round_many(v):
+    """c_round over an array: half away from zero."""
+    return (np.sign(v) * np.floor(np.abs(v) + 0.5)).astype(np.int64)
+
+
+def _a3d_index_many(p, xyz):
+    nx2, ny2, nz2 = (n + 2 * p.npml for n in p.shape)
+    i = _c_round_many((xyz[:, 0] - p.origin[0]) / p.d[0]) + p.npml
+    j = _c_round_many((xyz[:, 1] - p.origin[1]) / p.d[1]) + p.npml
+    k = _c_round_many((xyz[:, 2] - p.origin[2]) / p.d[2]) + p.npml
+    return ((i * ny2 + j) * nz2 + k).tolist()
+
+
 def a3d_inputs(p):
     """Everything sm_a3d_create and the source / receiver set-up take for
     problem p (host arrays), as a_iso_3d.c:317-590 prepares it."""
@@ -422,7 +435,8 @@ def a3d_inputs(p):
                     p.sources[0][2])
     fct, ln = ricker([q[1] for q in p.sources], [q[2] for q in p.sources], dt)
     idx = [a3d_index(p, q[3], q[4], q[5]) for q in p.sources]
-    ridx = [a3d_index(p, x, y, z) for (_, x, y, z, _, _) in p.receivers]
+    rxyz = np.array([r[1:4] for r in p.receivers], dtype=np.float64).reshape(-1, 3)
+    ridx = _a3d_index_many(p, rxyz)
     comps = [L.SM_COMP[c.lower()] for (c, _, _, _, _, _) in p.receivers]
     return dict(vp=vpp, rho=rhop, npml=p.npml, d=p.d, dt=dt, coef=coef,
                 src=(idx, fct, ln), src_scale=dt * 1e6,

@@ -23,6 +23,7 @@
 #include <mutex>
 #include <new>
 #include <tuple>
+#include <thread>
 #include <vector>
 
 #include "sm_common.cuh"
@@ -854,6 +855,43 @@ extern "C" int sm_a3d_device_bytes(size_t nx2, size_t ny2, size_t nz2, size_t np
     return SM_OK;
 }
 
+// pitched rho and K = rho vp^2 dt (a_iso_3d.c:407-409) in the compute type,
+// filled by a few host threads straight into the upload buffers (the model
+// of a large grid is hundreds of MB).  Pitch padding: rho repeats the last
+// real value so the on-the-fly buoyancy never divides by zero there (those
+// cells are not updated), K is zero.
+template <typename C>
+int a3d_upload_materials(sm_a3d *h, const double *rho, const double *vp, double dt, size_t nx2,
+                         size_t ny2, size_t nz2) {
+    const size_t pitch = (size_t)h->pitch, ncell = nx2 * ny2 * pitch;
+    std::unique_ptr<C[]> r(new (std::nothrow) C[ncell]), kk(new (std::nothrow) C[ncell]);
+    if (!r || !kk) return sm_fail(SM_ENOMEM, "sm_a3d_create: out of host memory");
+    auto fill = [&](size_t ib, size_t ie) {
+        for (size_t i = ib; i < ie; ++i)
+            for (size_t j = 0; j < ny2; ++j) {
+                const size_t s0 = (i * ny2 + j) * nz2, d0 = (i * ny2 + j) * pitch;
+                for (size_t k = 0; k < nz2; ++k) {
+                    r[d0 + k] = static_cast<C>(rho[s0 + k]);
+                    kk[d0 + k] = static_cast<C>(rho[s0 + k] * vp[s0 + k] * vp[s0 + k] * dt);
+                }
+                for (size_t k = nz2; k < pitch; ++k) {
+                    r[d0 + k] = r[d0 + nz2 - 1];
+                    kk[d0 + k] = C(0);
+                }
+            }
+    };
+    const size_t nt = std::min<size_t>(std::max(1u, std::thread::hardware_concurrency()), 16);
+    std::vector<std::thread> pool;
+    for (size_t t = 0; t < nt; ++t) {
+        const size_t ib = nx2 * t / nt, ie = nx2 * (t + 1) / nt;
+        if (ib < ie) pool.emplace_back(fill, ib, ie);
+    }
+    for (auto &th : pool) th.join();
+    SM_CUDA_TRY(cudaMemcpy(h->rho.p, r.get(), ncell * sizeof(C), cudaMemcpyHostToDevice));
+    SM_CUDA_TRY(cudaMemcpy(h->K.p, kk.get(), ncell * sizeof(C), cudaMemcpyHostToDevice));
+    return SM_OK;
+}
+
 extern "C" int sm_a3d_create(int device, size_t nx2, size_t ny2, size_t nz2, size_t np,
                              double dx, double dy, double dz, double dt, const double *vp,
                              const double *rho, const double *const *coef, int precision,
@@ -913,30 +951,9 @@ extern "C" int sm_a3d_create(int device, size_t nx2, size_t ny2, size_t nz2, siz
             if ((rc = h->psi[b][p].alloc(h->psi_cells[p] * h->elem))) return rc;
     if ((rc = h->rho.alloc(ncell * cb))) return rc;
     if ((rc = h->K.alloc(ncell * cb))) return rc;
-    {
-        // pitched copies of rho and K = rho vp^2 dt (a_iso_3d.c:407-409)
-        std::vector<double> r(ncell, 0.0), kk(ncell, 0.0);
-        for (size_t i = 0; i < nx2; ++i)
-            for (size_t j = 0; j < ny2; ++j)
-                for (size_t k = 0; k < nz2; ++k) {
-                    size_t s = (i * ny2 + j) * nz2 + k;
-                    size_t d = (i * ny2 + j) * h->pitch + k;
-                    r[d] = rho[s];
-                    kk[d] = rho[s] * vp[s] * vp[s] * dt;
-                }
-        // pitch padding: repeat the last real value so the on-the-fly
-        // buoyancy never divides by zero there (those cells are not updated)
-        for (size_t i = 0; i < nx2; ++i)
-            for (size_t j = 0; j < ny2; ++j)
-                for (size_t k = nz2; k < (size_t)h->pitch; ++k)
-                    r[(i * ny2 + j) * h->pitch + k] = r[(i * ny2 + j) * h->pitch + nz2 - 1];
-        rc = precision == SM_FP64 ? upload_convert<double>(h->rho.p, r.data(), ncell, h->stream)
-                                  : upload_convert<float>(h->rho.p, r.data(), ncell, h->stream);
-        if (rc) return rc;
-        rc = precision == SM_FP64 ? upload_convert<double>(h->K.p, kk.data(), ncell, h->stream)
-                                  : upload_convert<float>(h->K.p, kk.data(), ncell, h->stream);
-        if (rc) return rc;
-    }
+    rc = precision == SM_FP64 ? a3d_upload_materials<double>(h.get(), rho, vp, dt, nx2, ny2, nz2)
+                              : a3d_upload_materials<float>(h.get(), rho, vp, dt, nx2, ny2, nz2);
+    if (rc) return rc;
     A3Coef cf{{(int)nx2, (int)ny2, (int)nz2}};
     {
         std::vector<double> t((size_t)cf.size(), 0.0);
@@ -1327,14 +1344,29 @@ extern "C" int sm_a3d_read_traces(sm_a3d_t h, size_t rec0, size_t nrec, double *
             if (h->plan.table[gi * h->plan.nsteps_max + it] >= 0) ++gcount[gi];
     const size_t ms = h->plan.max_samples;
     if (out && nrec && ms) {
-        // one bulk copy, then scatter into the caller's layout
-        std::vector<double> buf(nrec * ms);
-        SM_CUDA_TRY(cudaMemcpy(buf.data(), h->d_traces.as<double>() + rec0 * ms,
-                               buf.size() * sizeof(double), cudaMemcpyDeviceToHost));
+        size_t cmax = 0;
+        bool same = true;
         for (size_t r = 0; r < nrec; ++r) {
-            size_t c = gcount[h->rec[rec0 + r].group];
+            const size_t c = gcount[h->rec[rec0 + r].group];
             if (ld < c) return sm_fail(SM_EINVAL, "sm_a3d_read_traces: ld too small");
-            std::memcpy(out + r * ld, buf.data() + r * ms, c * sizeof(double));
+            same = same && (r == 0 || c == cmax);
+            cmax = std::max(cmax, c);
+        }
+        const double *src = h->d_traces.as<double>() + rec0 * ms;
+        if (same) {
+            // every record has cmax samples: one strided copy into the caller's rows
+            if (cmax)
+                SM_CUDA_TRY(cudaMemcpy2D(out, ld * sizeof(double), src, ms * sizeof(double),
+                                         cmax * sizeof(double), nrec, cudaMemcpyDeviceToHost));
+        } else {
+            // one bulk copy, then scatter into the caller's layout
+            std::unique_ptr<double[]> buf(new (std::nothrow) double[nrec * ms]);
+            if (!buf) return sm_fail(SM_ENOMEM, "sm_a3d_read_traces: out of host memory");
+            SM_CUDA_TRY(cudaMemcpy(buf.get(), src, nrec * ms * sizeof(double),
+                                   cudaMemcpyDeviceToHost));
+            for (size_t r = 0; r < nrec; ++r)
+                std::memcpy(out + r * ld, buf.get() + r * ms,
+                            gcount[h->rec[rec0 + r].group] * sizeof(double));
         }
     }
     if (counts)
