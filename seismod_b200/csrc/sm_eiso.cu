@@ -2199,20 +2199,34 @@ extern "C" int sm_eiso_read_traces(sm_eiso_t h, size_t shot, size_t rec0, size_t
     SM_CUDA_TRY(cudaStreamSynchronize(h->stream));
     if (int rc = eiso_check_err(h)) return rc;
     const size_t ms = sr.plan.max_samples;
-    std::vector<double> buf(ms);
-    for (size_t r = 0; r < nrec; ++r) {
-        const RecEntry &e = sr.entries[rec0 + r];
-        // samples taken so far by this receiver's group
-        size_t c = 0;
-        const size_t lim = std::min(h->it, sr.plan.nsteps_max);
+    // samples taken so far, per sampling group of the shot
+    const size_t lim = std::min(h->it, sr.plan.nsteps_max);
+    std::vector<size_t> gcount(sr.plan.count_total.size(), 0);
+    for (size_t gi = 0; gi < gcount.size(); ++gi)
         for (size_t it = 0; it < lim; ++it)
-            if (sr.plan.table[(size_t)e.group * sr.plan.nsteps_max + it] >= 0) ++c;
+            if (sr.plan.table[gi * sr.plan.nsteps_max + it] >= 0) ++gcount[gi];
+    size_t cmax = 0;
+    bool same = true;
+    for (size_t r = 0; r < nrec; ++r) {
+        const size_t c = gcount[sr.entries[rec0 + r].group];
         if (counts) counts[r] = c;
-        if (!out || c == 0) continue;
-        if (ld < c) return sm_fail(SM_EINVAL, "sm_eiso_read_traces: ld smaller than sample count");
-        const long long off = h->rec_out_base[shot] + (long long)(rec0 + r) * (long long)ms;
-        SM_CUDA_TRY(cudaMemcpy(out + r * ld, h->d_traces.as<double>() + off, c * sizeof(double),
-                               cudaMemcpyDeviceToHost));
+        if (out && ld < c) return sm_fail(SM_EINVAL, "sm_eiso_read_traces: ld smaller than sample count");
+        same = same && (r == 0 || c == cmax);
+        cmax = std::max(cmax, c);
+    }
+    if (!out || !nrec || !cmax) return SM_OK;
+    // the shot's receivers are consecutive rows of ms samples on the device
+    const double *src = h->d_traces.as<double>() + h->rec_out_base[shot] + (long long)rec0 * (long long)ms;
+    if (same) {
+        SM_CUDA_TRY(cudaMemcpy2D(out, ld * sizeof(double), src, ms * sizeof(double),
+                                 cmax * sizeof(double), nrec, cudaMemcpyDeviceToHost));
+    } else {
+        for (size_t r = 0; r < nrec; ++r) {
+            const size_t c = gcount[sr.entries[rec0 + r].group];
+            if (c)
+                SM_CUDA_TRY(cudaMemcpy(out + r * ld, src + r * ms, c * sizeof(double),
+                                       cudaMemcpyDeviceToHost));
+        }
     }
     return SM_OK;
 }

@@ -403,6 +403,31 @@ out:
     return report(rc, prog);
 }
 
+/* div or curl of particle velocity over the grid (compute_div_cyl,
+ * compute_curl_cyl, propagate.c:4090-4118), cells it does not reach left zero */
+static void ecyl_div_curl(int comp, int n, size_t nx2, size_t nz2, double dx, double dz,
+                          const double *vr, const double *vt, const double *vz, double *out)
+{
+    for (size_t q = 0; q < nx2 * nz2; ++q) out[q] = 0.0;
+    if (comp == SM_DIV) {
+        for (size_t i = 0; i + 1 < nx2; ++i)
+            for (size_t j = 0; j + 1 < nz2; ++j) {
+                const size_t q = i * nz2 + j;
+                out[q] = ((i + 1) * vr[q + nz2] - i * vr[q]) / (i + 0.5) +
+                         n * vt[q] / ((i + 0.5) * dx) + (vz[q + 1] - vz[q]) / dz;
+            }
+        return;
+    }
+    if (n % 2)
+        for (size_t j = 1; j < nz2; ++j)
+            out[j] = (vr[j] - vr[j - 1]) / dz - (vz[j] - -vz[j]) / dx;
+    for (size_t i = 1; i < nx2; ++i)
+        for (size_t j = 1; j < nz2; ++j) {
+            const size_t q = i * nz2 + j;
+            out[q] = (vr[q] - vr[q - 1]) / dz - (vz[q] - vz[q - nz2]) / dx;
+        }
+}
+
 int sm_e_cyl_iso_main(int argc, char **argv)
 {
     /* e_cyl_iso.c:277-790: set-up in FP64 through the library's host
@@ -411,7 +436,9 @@ int sm_e_cyl_iso_main(int argc, char **argv)
      * the reference adds them once per thread, e_cyl_iso.c:612-637); the
      * 9-point source template is refused (io_utils.c:1513-1534 offsets its
      * radial indices by np, which the cylindrical grid does not have);
-     * snapshot records are skipped (netCDF) with a warning. */
+     * snapshot records are written in the text format of write_snapshot
+     * (io_utils.c:1775-1820) with the cylindrical grid's radii, where the
+     * reference writes netCDF (write_snapshot_nc, e_cyl_iso.c:781). */
     const char *prog = "e_cyl_iso_gpu";
     sm_params p;
     sm_grid g;
@@ -496,10 +523,7 @@ int sm_e_cyl_iso_main(int argc, char **argv)
     rp.comp = malloc((nrec ? nrec : 1) * sizeof(int));
     rp.t0 = malloc((nrec ? nrec : 1) * sizeof(double)); rp.rdt = malloc((nrec ? nrec : 1) * sizeof(double));
     for (size_t r = 0; r < nrec; ++r) {
-        if (!rec[r].is_trace) {
-            fprintf(stderr, "%s: record %zu is a snapshot (netCDF in the reference); skipped\n", prog, r + 1);
-            continue;
-        }
+        if (!rec[r].is_trace) continue;   /* snapshots: written as the loop passes them */
         if (rec[r].i < 0 || rec[r].k < 0 || (size_t)rec[r].i >= nx2 || (size_t)rec[r].k + np >= nz2) {
             rc = sm_fail(SM_EINVAL, "record %zu lies outside the grid", r + 1);
             goto out;
@@ -513,7 +537,36 @@ int sm_e_cyl_iso_main(int argc, char **argv)
     }
     if ((rc = sm_ecyl_set_receivers(h, rp.n, rp.index, rp.comp, rp.t0, rp.rdt, nsteps))) goto out;
     if (p.verbose) fprintf(stdout, "Starting main loop (%zu iterations)\n", nsteps);
-    if ((rc = sm_ecyl_run(h, nsteps))) goto out;
+    {   /* the loop, stopping after each snapshot step (e_cyl_iso.c:768-785) */
+        snap_ev *ev = NULL;
+        size_t nev = 0, done = 0;
+        double *field = NULL, *vr = NULL, *vt = NULL, *vz = NULL;
+        if ((rc = snap_events(rec, nrec, dt, nsteps, &ev, &nev))) { free(ev); goto out; }
+        if (nev && (!(field = calloc(N, sizeof(double))) || !(vr = malloc(N * sizeof(double))) ||
+                    !(vt = malloc(N * sizeof(double))) || !(vz = malloc(N * sizeof(double))))) {
+            free(ev); free(field); free(vr); free(vt);
+            rc = sm_fail(SM_ENOMEM, "out of host memory");
+            goto out;
+        }
+        for (size_t e = 0; e < nev && !rc; ++e) {
+            const size_t upto = ev[e].it + 1;
+            if (upto > done) rc = sm_ecyl_run(h, upto - done);
+            done = upto;
+            const int comp = rec[ev[e].rec].comp;
+            if (!rc && comp != SM_DIV && comp != SM_CURL) rc = sm_ecyl_get_field(h, comp, field);
+            if (!rc && (comp == SM_DIV || comp == SM_CURL)) {
+                if (!(rc = sm_ecyl_get_field(h, SM_VR, vr)) && !(rc = sm_ecyl_get_field(h, SM_VT, vt)))
+                    rc = sm_ecyl_get_field(h, SM_VZ, vz);
+                if (!rc) ecyl_div_curl(comp, n, nx2, nz2, g.dx, g.dz, vr, vt, vz, field);
+            }
+            if (!rc)
+                rc = sm_write_snapshot_cyl(p.basename, ev[e].rec + 1, dt * (double)upto, field, nx2,
+                                           nz2, np, g.dx, g.dz, g.x0, g.z0, p.plot_strips);
+        }
+        if (!rc && done < nsteps) rc = sm_ecyl_run(h, nsteps - done);
+        free(ev); free(field); free(vr); free(vt); free(vz);
+        if (rc) goto out;
+    }
     counts = calloc(rp.n ? rp.n : 1, sizeof(size_t));
     if ((rc = sm_ecyl_read_traces(h, 0, rp.n, NULL, 0, counts))) goto out;
     size_t ld = 1;

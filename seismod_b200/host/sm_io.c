@@ -661,9 +661,12 @@ int sm_write_segy(const char *base, const sm_params *p, const sm_record *rec, si
     return SM_OK;
 }
 
-int sm_write_snapshot(const char *base, size_t n, double t, const double *data, size_t nx2,
-                      size_t nz2, size_t np, double dx, double dz, double x0, double z0,
-                      int plot_strips)
+/* the snapshot file of write_snapshot; npl: absorbing columns before column
+ * 0 of the model (np on the Cartesian grids, 0 on the cylindrical one, whose
+ * axis has none), npr: after its last column */
+static int write_snapshot_grid(const char *base, size_t n, double t, const double *data,
+                               size_t nx2, size_t nz2, size_t npl, size_t npr, size_t np,
+                               double dx, double dz, double x0, double z0, int plot_strips)
 {
     char name[700];
     struct stat sb;
@@ -676,21 +679,37 @@ int sm_write_snapshot(const char *base, size_t n, double t, const double *data, 
     int ok = 1;
     if (plot_strips) {
         for (size_t i = 0; i < nx2 && ok; ++i) {
-            const double x = x0 + ((double)i - (double)np) * dx;
+            const double x = x0 + ((double)i - (double)npl) * dx;
             for (size_t k = 0; k < nz2 && ok; ++k) {
                 const double z = z0 + ((double)k - (double)np) * dz;
                 ok = fprintf(f, "%le  %le  %le\n", x, z, 1.e3 * data[i * nz2 + k]) > 0;
             }
         }
     } else {
-        for (size_t i = 0; i + 2 * np < nx2 && ok; ++i) {
+        for (size_t i = 0; i + npl + npr < nx2 && ok; ++i) {
             const double x = x0 + i * dx;
             for (size_t k = 0; k + 2 * np < nz2 && ok; ++k) {
                 const double z = z0 + k * dz;
-                ok = fprintf(f, "%le  %le  %le\n", x, z, 1.e3 * data[(i + np) * nz2 + k + np]) > 0;
+                ok = fprintf(f, "%le  %le  %le\n", x, z, 1.e3 * data[(i + npl) * nz2 + k + np]) > 0;
             }
         }
     }
     if (fclose(f) != 0) ok = 0;
     return ok ? SM_OK : sm_fail(SM_EIO, "write error on %s", name);
+}
+
+int sm_write_snapshot(const char *base, size_t n, double t, const double *data, size_t nx2,
+                      size_t nz2, size_t np, double dx, double dz, double x0, double z0,
+                      int plot_strips)
+{
+    return write_snapshot_grid(base, n, t, data, nx2, nz2, np, np, np, dx, dz, x0, z0,
+                               plot_strips);
+}
+
+int sm_write_snapshot_cyl(const char *base, size_t n, double t, const double *data, size_t nx2,
+                          size_t nz2, size_t np, double dx, double dz, double x0, double z0,
+                          int plot_strips)
+{
+    return write_snapshot_grid(base, n, t, data, nx2, nz2, 0, np, np, dx, dz, x0, z0,
+                               plot_strips);
 }

@@ -93,6 +93,11 @@ int sm_write_trace_file(const char *base, size_t n, const double *t, const doubl
 int sm_write_snapshot(const char *base, size_t n, double t, const double *data, size_t nx2,
                       size_t nz2, size_t np, double dx, double dz, double x0, double z0,
                       int plot_strips);
+/* the same for the cylindrical grid of e_cyl_iso (nx2 = nx + np: no
+ * absorbing columns before the axis) */
+int sm_write_snapshot_cyl(const char *base, size_t n, double t, const double *data, size_t nx2,
+                          size_t nz2, size_t np, double dx, double dz, double x0, double z0,
+                          int plot_strips);
 int sm_write_segy(const char *base, const sm_params *p, const sm_record *rec, size_t ntr,
                   const sm_source *src0, const double *v, const double *t, size_t ld,
                   const size_t *count);

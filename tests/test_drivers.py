@@ -299,3 +299,40 @@ def test_ecyl_drop_in_refuses_what_it_cannot_run(tmp_path):
     par = q.write(str(tmp_path / "cfl"))
     r = run("e_cyl_iso_gpu", ["-p", "run.par"], tmp_path / "cfl")
     assert r.returncode != 0 and "Time step too large" in r.stderr
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("strips", [0, 1])
+def test_ecyl_snapshots(strips, tmp_path):
+    """e_cyl_iso_gpu writes snapshot records as text snapshots on the
+    cylindrical grid (radii from the axis, no columns before it): a field
+    (Vz) and a derived one (div), against the device state after the same
+    number of steps."""
+    from seismod_b200 import api
+    p = W.ecyl_case(nx=36, nz=44, npml=6, nsteps=90, nrec=2, n=1, src="Fz")
+    k = 50
+    par = p.write(str(tmp_path), plstr=strips)
+    recs = [(c, (x, z), t0, r) for (c, x, z, t0, r) in p.receivers]
+    recs.append(("Vz", (0.0, 0.0), k * p.dt, 1e6, "Snapshot"))
+    recs.append(("div", (0.0, 0.0), k * p.dt, 1e6, "Snapshot"))
+    F.write_rcv(os.path.join(str(tmp_path), "rcv.dat"), recs)
+    r = run("e_cyl_iso_gpu", ["-p", os.path.basename(par)], tmp_path)
+    assert r.returncode == 0, r.stderr
+    dev, _ = api.ecyl_device(p, "fp32")
+    dev.run(k)
+    vr, vt, vz = dev.get_field("vr"), dev.get_field("vt"), dev.get_field("vz")
+    dev.close()
+    n, np_ = p.n, p.np_used
+    nx2, nz2 = vz.shape
+    div = np.zeros_like(vz)
+    i = np.arange(nx2 - 1)[:, None].astype(float)
+    div[:-1, :-1] = (((i + 1) * vr[1:, :-1] - i * vr[:-1, :-1]) / (i + 0.5) +
+                     n * vt[:-1, :-1] / ((i + 0.5) * p.dx) + (vz[:-1, 1:] - vz[:-1, :-1]) / p.dz)
+    for rec_no, ref in ((len(recs) - 1, vz), (len(recs), div)):
+        x, z, val = F.read_snapshot(_snapshot_file(tmp_path, p.name, rec_no))
+        want = ref if strips else ref[:p.nx, np_:np_ + p.nz]
+        assert val.size == want.size
+        np.testing.assert_allclose(val.reshape(want.shape), 1e3 * want, rtol=1e-5,
+                                   atol=1e-5 * np.abs(1e3 * want).max())
+        assert x[0] == 0.0   # the axis: no absorbing columns before r = 0
+        assert z[0] == (-np_ * p.dz if strips else 0.0)
