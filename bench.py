@@ -173,6 +173,23 @@ def make_workload(name, size=None):
 # our arm
 # ----------------------------------------------------------------------------
 
+def max_over_ranks(x, dist, device):
+    """The largest x over all ranks: the job's time is its slowest rank's.
+    dist is torch.distributed (initialised, any backend) or None."""
+    if dist is None or not dist.is_initialized() or dist.get_world_size() == 1:
+        return x
+    import torch
+    t = torch.tensor([float(x)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def job_gcells(cells, K, world, ms):
+    """Whole-job throughput of replicas: every rank updates `cells` cells per
+    step for K steps; ms is the slowest rank's time."""
+    return cells * K * world / (ms * 1e-3) / 1e9
+
+
 def trace_err(a, b):
     a = np.concatenate([np.ravel(x) for x in a])
     b = np.concatenate([np.ravel(x) for x in b])
@@ -237,10 +254,7 @@ def run_ours(args, rank, world, local_rank, torch, dist):
     with Clocks(local_rank) as clk:
         ms = time_steps(dev, K, torch)
     _, _, launches = dev.kernel_stats(reset=True)
-    if world > 1:
-        t = torch.tensor([ms], device=f"cuda:{local_rank}")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
+    ms = max_over_ranks(ms, dist, f"cuda:{local_rank}")
     # dominant-kernel duration: separate pass with per-launch events
     dev.set_timing(True)
     Kr = min(K, 400)
@@ -248,8 +262,7 @@ def run_ours(args, rank, world, local_rank, torch, dist):
     upd_ms, upd_n, _ = dev.kernel_stats(reset=True)
     dev.set_timing(False)
     dev.close()
-    total_cells = cells * K * world
-    value = total_cells / (ms * 1e-3) / 1e9
+    value = job_gcells(cells, K, world, ms)
     hbm, how = peaks()
     achieved = bps / (upd_ms / upd_n * 1e-3) / 1e9
     out = {
