@@ -23,6 +23,7 @@
 #include <mutex>
 #include <new>
 #include <tuple>
+#include <type_traits>
 #include <thread>
 #include <vector>
 
@@ -63,6 +64,11 @@ struct A3Args {
     void *fo[4];               // ... and written this step (the other buffer)
     void *pso[6];
     int chunk;                 // x planes per CTA
+    // tiles (32 k x TY j): nkt x njt in all; the interior class is the
+    // rectangle [kt0, kt1) x [jt0, jt1) of tiles clear of the CPML frame and
+    // the grid edge in y and z, the edge class every other tile
+    int nkt, njt, kt0, kt1, jt0, jt1;
+    int step_cls;              // the class whose first CTA counts the step
     const void *rho;           // compute type, padded layout
     const void *K;
     const void *coef;
@@ -146,6 +152,9 @@ __device__ __forceinline__ C a3_dv(C g, C ca, C cb, C cik, C psi_old, C &psi_new
     return r_fma(g, cik, psi_new);
 }
 
+template <bool B>
+using BoolT = std::integral_constant<bool, B>;
+
 struct A3Maps {
     CUtensorMap P, vx, vy, vz, rho, K;
 };
@@ -167,10 +176,35 @@ struct A3Maps {
 //   * inside the CPML frame the memory variables of the next plane are
 //     loaded one iteration ahead, and the coefficients of the tile's planes,
 //     rows and columns sit in shared memory, so no global load waits in the
-//     loop; tiles and planes clear of the frame take a lean path.
+//     loop; each axis on which a tile (y, z) or a plane (x) is clear of the
+//     frame and of the grid edge takes the plain update, so a tile on one
+//     face of the frame pays the CPML only for that face's component.
 // Old and new wavefields and CPML memory variables live in separate buffers
 // (ping-pong): every stored value is read once and written once per step.
-template <typename S, int W, int R, int D, int MINB>
+// Tile classes, one launch each: A3_INNER runs the interior rectangle with
+// y and z fast at compile time (only the x frame planes take a general
+// update, one component), A3_EDGE the ring of tiles around it with the flags
+// read at run time; blockIdx.x numbers the ring's tiles.
+enum { A3_INNER = 0, A3_EDGE = 1 };
+
+// tile (kt, jt) of ring index e: rows below the rectangle, rows above it,
+// then the tiles left and right of it in its rows
+__device__ __forceinline__ void a3_edge_tile(const A3Args &a, int e, int &kt, int &jt) {
+    const int below = a.jt0 * a.nkt, above = (a.njt - a.jt1) * a.nkt;
+    if (e < below) {
+        jt = e / a.nkt; kt = e % a.nkt;
+    } else if (e < below + above) {
+        e -= below; jt = a.jt1 + e / a.nkt; kt = e % a.nkt;
+    } else {
+        e -= below + above;
+        const int m = a.nkt - (a.kt1 - a.kt0);
+        jt = a.jt0 + e / m;
+        const int c = e % m;
+        kt = c < a.kt0 ? c : a.kt1 + (c - a.kt0);
+    }
+}
+
+template <typename S, int W, int R, int D, int MINB, int CLS>
 __global__ void __launch_bounds__(32 * W, MINB)
     a3d_step_kernel(const A3Args a, const __grid_constant__ A3Maps m) {
     constexpr int TY = W * R;
@@ -191,8 +225,23 @@ __global__ void __launch_bounds__(32 * W, MINB)
 
     const int lane = threadIdx.x, w = threadIdx.y;
     const int tid = w * 32 + lane;
-    if ((blockIdx.x | blockIdx.y | blockIdx.z | tid) == 0) ++*a.step;
-    const int k0 = blockIdx.x * 32, j0 = blockIdx.y * TY;
+    if (CLS == a.step_cls && (blockIdx.x | blockIdx.y | blockIdx.z | tid) == 0) ++*a.step;
+    int kt, jt;
+    if (CLS == A3_INNER) {
+        kt = a.kt0 + blockIdx.x; jt = a.jt0 + blockIdx.y;
+    } else {
+        a3_edge_tile(a, blockIdx.x, kt, jt);
+    }
+    const int k0 = kt * 32, j0 = jt * TY;
+    const int lo = a.np > 1 ? a.np : 1;
+    const bool ytile = j0 >= lo && j0 + TY - 1 <= a.ny2 - 2 - a.np;
+    const bool ztile = k0 >= lo && k0 + 31 <= a.nz2 - 2 - a.np;
+    // checked before any barrier or copy: an interior tile that is not
+    // clear means the host's rectangle is wrong
+    if (CLS == A3_INNER && !(ytile && ztile)) {
+        if (tid == 0) atomicExch(a.err, 3);
+        return;
+    }
     const int k = k0 + lane;
     const int i0 = blockIdx.z * a.chunk;
     const int i1 = min(i0 + a.chunk, a.nx2);
@@ -285,31 +334,67 @@ __global__ void __launch_bounds__(32 * W, MINB)
     const int hrow = w * R + lane;                 // halo-column row of lanes 0..R-1
     const bool hcol = lane < R && km >= 0 && j0 + hrow < ny2;
     const int kmh = (km >= 0) ? half_slab(km, nz2, np) : -1;
-    const bool tile_fast = (j0 - 1 >= np) && (j0 + TY - 1 <= ny2 - 2 - np) &&
-                           (k0 - 1 >= np) && (k0 + 31 <= nz2 - 2 - np);
+    // Per-axis fast flags.  An axis is "fast" for a cell when neither its CPML
+    // frame nor the grid edge touches it: the velocity component along the
+    // axis is then the plain update (a3_vel0) and the pressure needs no
+    // memory variable and no edge test for it.  y and z are decided per tile
+    // (uniform over the CTA), x per plane.  Velocity: half nodes
+    // np .. n2-2-np; pressure: nodes max(np,1) .. n2-1-np (the reference
+    // updates the pressure from index 1).  The velocity and pressure bodies
+    // are compiled twice: with every axis fast (interior tiles on planes
+    // clear of the x frame: straight-line code) and with the flags read at
+    // run time.  The halo row and column always take the general update.
+    const bool yfast = CLS == A3_INNER || ytile;
+    const bool zfast = CLS == A3_INNER || ztile;
 
-    // memory variables prefetched one plane ahead
+    // memory variables prefetched one plane ahead (loaded only for the
+    // axes and planes that use them)
     C fPx[R], fPy[R], fPz[R], fVx[R], fVy[R], fVz[R], fHy = C(0), fHz = C(0);
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+        fPx[r] = C(0); fPy[r] = C(0); fPz[r] = C(0);
+        fVx[r] = C(0); fVy[r] = C(0); fVz[r] = C(0);
+    }
     auto load_vpsi = [&](int ip) {   // for the velocities of plane ip
         const int s = (ip < nx2 - 1) ? half_slab(ip, nx2, np) : -1;
+        if (s >= 0) {
 #pragma unroll
-        for (int r = 0; r < R; ++r) {
-            const int j = j0 + w * R + r;
-            fPx[r] = (rin[r] && s >= 0) ? St::ld(psPx + s * sx + joff[r], a.pisc[PS_PX]) : C(0);
-            fPy[r] = (rin[r] && jh[r] >= 0) ? St::ld(psPy + (ip * 2 * np + jh[r]) * pitch + k, a.pisc[PS_PY]) : C(0);
-            fPz[r] = (rin[r] && kh >= 0) ? St::ld(psPz + (ip * ny2 + j) * 2 * np + kh, a.pisc[PS_PZ]) : C(0);
+            for (int r = 0; r < R; ++r)
+                fPx[r] = rin[r] ? St::ld(psPx + s * sx + joff[r], a.pisc[PS_PX]) : C(0);
         }
-        fHy = (w == 0 && kin && jmh >= 0) ? St::ld(psPy + (ip * 2 * np + jmh) * pitch + k, a.pisc[PS_PY]) : C(0);
-        fHz = (hcol && kmh >= 0) ? St::ld(psPz + (ip * ny2 + j0 + hrow) * 2 * np + kmh, a.pisc[PS_PZ]) : C(0);
+        if (!yfast) {
+#pragma unroll
+            for (int r = 0; r < R; ++r)
+                fPy[r] = (rin[r] && jh[r] >= 0) ? St::ld(psPy + (ip * 2 * np + jh[r]) * pitch + k, a.pisc[PS_PY]) : C(0);
+        }
+        if (!zfast) {
+#pragma unroll
+            for (int r = 0; r < R; ++r) {
+                const int j = j0 + w * R + r;
+                fPz[r] = (rin[r] && kh >= 0) ? St::ld(psPz + (ip * ny2 + j) * 2 * np + kh, a.pisc[PS_PZ]) : C(0);
+            }
+        }
+        if (w == 0 && kin && jmh >= 0) fHy = St::ld(psPy + (ip * 2 * np + jmh) * pitch + k, a.pisc[PS_PY]);
+        if (hcol && kmh >= 0) fHz = St::ld(psPz + (ip * ny2 + j0 + hrow) * 2 * np + kmh, a.pisc[PS_PZ]);
     };
     auto load_ppsi = [&](int ip) {   // for the pressure of plane ip
         const int s = node_slab(ip, nx2, np);
+        if (s >= 0) {
 #pragma unroll
-        for (int r = 0; r < R; ++r) {
-            const int j = j0 + w * R + r;
-            fVx[r] = (rin[r] && s >= 0) ? St::ld(psVx + s * sx + joff[r], a.pisc[PS_VX]) : C(0);
-            fVy[r] = (rin[r] && jn[r] >= 0) ? St::ld(psVy + (ip * 2 * np + jn[r]) * pitch + k, a.pisc[PS_VY]) : C(0);
-            fVz[r] = (rin[r] && kn >= 0) ? St::ld(psVz + (ip * ny2 + j) * 2 * np + kn, a.pisc[PS_VZ]) : C(0);
+            for (int r = 0; r < R; ++r)
+                fVx[r] = rin[r] ? St::ld(psVx + s * sx + joff[r], a.pisc[PS_VX]) : C(0);
+        }
+        if (!yfast) {
+#pragma unroll
+            for (int r = 0; r < R; ++r)
+                fVy[r] = (rin[r] && jn[r] >= 0) ? St::ld(psVy + (ip * 2 * np + jn[r]) * pitch + k, a.pisc[PS_VY]) : C(0);
+        }
+        if (!zfast) {
+#pragma unroll
+            for (int r = 0; r < R; ++r) {
+                const int j = j0 + w * R + r;
+                fVz[r] = (rin[r] && kn >= 0) ? St::ld(psVz + (ip * ny2 + j) * 2 * np + kn, a.pisc[PS_VZ]) : C(0);
+            }
         }
     };
 
@@ -334,12 +419,15 @@ __global__ void __launch_bounds__(32 * W, MINB)
     load_vpsi(i0);
 
     // ---- the lagged pressure half step of plane ip (a_iso_3d.c:659-683) ----
-    auto pressure = [&](int ip, int lp, bool fast) {
+    auto pressure = [&](int ip, int lp, auto AFt) {
+        constexpr bool AF = decltype(AFt)::value;
+        const bool fx = AF || (ip >= lo && ip <= nx2 - 1 - np);
+        const bool fy = AF || yfast, fz = AF || zfast;
         const unsigned char *pb = ring + (size_t)(lp % D) * L::stage;
         const S *pP = reinterpret_cast<const S *>(pb + L::oP);
         const C *pK = reinterpret_cast<const C *>(pb + L::oK);
         const C(*vy)[32] = VYs[ip & 1];
-        const int sxn = node_slab(ip, nx2, np);
+        const int sxn = fx ? -1 : node_slab(ip, nx2, np);
         const int e = ip - (i0 - 1);
         S *po = Pout + ip * sx;
 #pragma unroll
@@ -351,24 +439,27 @@ __global__ void __launch_bounds__(32 * W, MINB)
             if (!rin[r]) continue;
             const C p_c = St::ld(pP + (row + 1) * WS + HS + lane, isP);
             C pn = p_c;
-            if (fast || (ip >= 1 && j >= 1 && k >= 1)) {
+            // the reference leaves index 0 of every axis untouched
+            bool upd = true;
+            if (!fx) upd = ip >= 1;
+            if (!fy) upd = upd && j >= 1;
+            if (!fz) upd = upd && k >= 1;
+            if (upd) {
                 C gx = r_mul(r_sub(vxa[r], vxb[r]), idx);
                 C gy = r_mul(r_sub(vy[row + 1][lane], vy[row][lane]), idy);
                 C gz = r_mul(r_sub(vzp[r], vzm), idz);
-                if (!fast) {
-                    C psi_new;
-                    if (sxn >= 0) {
-                        gx = a3_dv<C>(gx, CX[3][e], CX[4][e], CX[5][e], fVx[r], psi_new);
-                        St::st(poVx + sxn * sx + joff[r], psi_new, a.psc[PS_VX]);
-                    }
-                    if (jn[r] >= 0) {
-                        gy = a3_dv<C>(gy, CY[3][row + 1], CY[4][row + 1], CY[5][row + 1], fVy[r], psi_new);
-                        St::st(poVy + (ip * 2 * np + jn[r]) * pitch + k, psi_new, a.psc[PS_VY]);
-                    }
-                    if (kn >= 0) {
-                        gz = a3_dv<C>(gz, CZ[3][lane + 1], CZ[4][lane + 1], CZ[5][lane + 1], fVz[r], psi_new);
-                        St::st(poVz + (ip * ny2 + j) * 2 * np + kn, psi_new, a.psc[PS_VZ]);
-                    }
+                C psi_new;
+                if (sxn >= 0) {
+                    gx = a3_dv<C>(gx, CX[3][e], CX[4][e], CX[5][e], fVx[r], psi_new);
+                    St::st(poVx + sxn * sx + joff[r], psi_new, a.psc[PS_VX]);
+                }
+                if (!fy && jn[r] >= 0) {
+                    gy = a3_dv<C>(gy, CY[3][row + 1], CY[4][row + 1], CY[5][row + 1], fVy[r], psi_new);
+                    St::st(poVy + (ip * 2 * np + jn[r]) * pitch + k, psi_new, a.psc[PS_VY]);
+                }
+                if (!fz && kn >= 0) {
+                    gz = a3_dv<C>(gz, CZ[3][lane + 1], CZ[4][lane + 1], CZ[5][lane + 1], fVz[r], psi_new);
+                    St::st(poVz + (ip * ny2 + j) * 2 * np + kn, psi_new, a.psc[PS_VZ]);
                 }
                 pn = r_fma(-pK[row * 32 + lane], r_add(r_add(gx, gy), gz), p_c);
             }
@@ -393,14 +484,20 @@ __global__ void __launch_bounds__(32 * W, MINB)
         const S *nP = reinterpret_cast<const S *>(nbuf + L::oP);
         const C *nR = reinterpret_cast<const C *>(nbuf + L::oR);
         C(*vyw)[32] = VYs[i & 1];
-        const bool fast = tile_fast && i >= np && i <= nx2 - 2 - np;
+        const bool xf = i >= np && i <= nx2 - 2 - np;
         const int sxh = (i < nx2 - 1) ? half_slab(i, nx2, np) : -1;
         const int e = i - (i0 - 1);
         S *ox = Vxout + i * sx, *oy = Vyout + i * sx, *oz = Vzout + i * sx;
 
         // ---- velocity half step at plane i (a_iso_3d.c:605-651) ----
+        // A component on a fast axis is updated even in cells outside the
+        // grid (from the zero fill): such values are neither stored nor
+        // read by a cell inside the grid.
         C vxn[R], vzn[R];
         C vzh = C(0);
+        auto velocity = [&](auto AFt) {
+        constexpr bool AF = decltype(AFt)::value;
+        const bool fx = AF || xf, fy = AF || yfast, fz = AF || zfast;
 #pragma unroll
         for (int r = 0; r < R; ++r) {
             const int row = w * R + r, j = j0 + row;
@@ -411,30 +508,30 @@ __global__ void __launch_bounds__(32 * W, MINB)
             C vx = St::ld(cX + row * 32 + lane, isX);
             C vy = St::ld(cY + (row + 1) * 32 + lane, isY);
             C vz = St::ld(cZ + row * WZ + HS + lane, isZ);
-            if (fast) {
+            C psi_new;
+            if (fx) {
                 vx = a3_vel0<C>(vx, p_c, St::ld(nP + cc, isP), r_c, nR[rc], idx, two_dt);
+            } else if (rin[r] && i < nx2 - 1) {
+                vx = a3_vel<C>(vx, p_c, St::ld(nP + cc, isP), r_c, nR[rc], idx, two_dt, sxh >= 0,
+                               CX[0][e], CX[1][e], CX[2][e], fPx[r], psi_new);
+                if (sxh >= 0) St::st(poPx + sxh * sx + joff[r], psi_new, a.psc[PS_PX]);
+            }
+            if (fy) {
                 vy = a3_vel0<C>(vy, p_c, St::ld(cP + cc + WS, isP), r_c, cR[rc + WC], idy, two_dt);
+            } else if (rin[r] && j < ny2 - 1) {
+                vy = a3_vel<C>(vy, p_c, St::ld(cP + cc + WS, isP), r_c, cR[rc + WC], idy, two_dt,
+                               jh[r] >= 0, CY[0][row + 1], CY[1][row + 1], CY[2][row + 1], fPy[r],
+                               psi_new);
+                if (jh[r] >= 0)
+                    St::st(poPy + (i * 2 * np + jh[r]) * pitch + k, psi_new, a.psc[PS_PY]);
+            }
+            if (fz) {
                 vz = a3_vel0<C>(vz, p_c, St::ld(cP + cc + 1, isP), r_c, cR[rc + 1], idz, two_dt);
-            } else if (rin[r]) {
-                C psi_new;
-                if (i < nx2 - 1) {
-                    vx = a3_vel<C>(vx, p_c, St::ld(nP + cc, isP), r_c, nR[rc], idx, two_dt, sxh >= 0,
-                                   CX[0][e], CX[1][e], CX[2][e], fPx[r], psi_new);
-                    if (sxh >= 0) St::st(poPx + sxh * sx + joff[r], psi_new, a.psc[PS_PX]);
-                }
-                if (j < ny2 - 1) {
-                    vy = a3_vel<C>(vy, p_c, St::ld(cP + cc + WS, isP), r_c, cR[rc + WC], idy, two_dt,
-                                   jh[r] >= 0, CY[0][row + 1], CY[1][row + 1], CY[2][row + 1], fPy[r],
-                                   psi_new);
-                    if (jh[r] >= 0)
-                        St::st(poPy + (i * 2 * np + jh[r]) * pitch + k, psi_new, a.psc[PS_PY]);
-                }
-                if (k < nz2 - 1) {
-                    vz = a3_vel<C>(vz, p_c, St::ld(cP + cc + 1, isP), r_c, cR[rc + 1], idz, two_dt,
-                                   kh >= 0, CZ[0][lane + 1], CZ[1][lane + 1], CZ[2][lane + 1], fPz[r],
-                                   psi_new);
-                    if (kh >= 0) St::st(poPz + (i * ny2 + j) * 2 * np + kh, psi_new, a.psc[PS_PZ]);
-                }
+            } else if (rin[r] && k < nz2 - 1) {
+                vz = a3_vel<C>(vz, p_c, St::ld(cP + cc + 1, isP), r_c, cR[rc + 1], idz, two_dt,
+                               kh >= 0, CZ[0][lane + 1], CZ[1][lane + 1], CZ[2][lane + 1], fPz[r],
+                               psi_new);
+                if (kh >= 0) St::st(poPz + (i * ny2 + j) * 2 * np + kh, psi_new, a.psc[PS_PZ]);
             }
             vyw[row + 1][lane] = vy;
             vxn[r] = vx;
@@ -445,6 +542,9 @@ __global__ void __launch_bounds__(32 * W, MINB)
                 St::st(oz + joff[r], vz, a.sc[A_VZ]);
             }
         }
+        };
+        if (CLS == A3_INNER && xf) velocity(BoolT<true>{});
+        else velocity(BoolT<false>{});
         // halo row: vy(i, j0-1, k), by warp 0
         if (w == 0) {
             C vyh = C(0);
@@ -465,13 +565,14 @@ __global__ void __launch_bounds__(32 * W, MINB)
                             CZ[1][0], CZ[2][0], fHz, psi_new);
         }
         // memory variables for the next plane's velocities
-        if (i + 1 < i1 && (!tile_fast || i + 1 < np || i + 1 > nx2 - 2 - np)) load_vpsi(i + 1);
+        if (i + 1 < i1) load_vpsi(i + 1);
         // the pressure of the previous plane (its velocities are complete)
         if (i > i0) {
             const int ip = i - 1;
-            pressure(ip, l - 1, tile_fast && ip >= np && ip <= nx2 - 1 - np);
+            if (CLS == A3_INNER && ip >= lo && ip <= nx2 - 1 - np) pressure(ip, l - 1, BoolT<true>{});
+            else pressure(ip, l - 1, BoolT<false>{});
         }
-        if (!tile_fast || i < np || i > nx2 - 1 - np) load_ppsi(i);
+        load_ppsi(i);
 #pragma unroll
         for (int r = 0; r < R; ++r) {
             vxb[r] = vxa[r];
@@ -485,7 +586,8 @@ __global__ void __launch_bounds__(32 * W, MINB)
     // the last plane's pressure
     if (i1 > i0) {
         const int ip = i1 - 1;
-        pressure(ip, ip - i0, tile_fast && ip >= np && ip <= nx2 - 1 - np);
+        if (CLS == A3_INNER && ip >= lo && ip <= nx2 - 1 - np) pressure(ip, ip - i0, BoolT<true>{});
+        else pressure(ip, ip - i0, BoolT<false>{});
     }
 }
 
@@ -548,6 +650,10 @@ struct sm_a3d {
     int pitch = 0;
     size_t it = 0;
     cudaStream_t stream = nullptr;
+    // the edge-tile launch runs on `side`, forked from and joined back to
+    // `stream` by the two events, so it overlaps the interior launch
+    cudaStream_t side = nullptr;
+    cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
     A3Args args{};
     DevBuf f[2][4], psi[2][6], rho, K, coef;   // two buffer sets (ping-pong)
     int cur = 0;                               // set holding the current state
@@ -619,13 +725,49 @@ static const A3Config kA3Configs[] = {
 };
 static const int kA3NumConfigs = sizeof(kA3Configs) / sizeof(kA3Configs[0]);
 
+// The interior rectangle of tiles for tile rows ty: tiles (32 k x ty j)
+// whose every cell is clear in y and z of the CPML frame and of the grid
+// edge (velocity half nodes np .. n2-2-np, pressure nodes max(np,1) ..
+// n2-1-np), the same test the step kernel makes per tile.  Empty when no
+// tile qualifies; the edge class is then every tile.
+void a3d_tile_classes(sm_a3d *h, int ty) {
+    A3Args &a = h->args;
+    const long long np = (long long)h->np, lo = np > 1 ? np : 1;
+    a.nkt = (int)((h->nz2 + 31) / 32);
+    a.njt = (int)((h->ny2 + ty - 1) / ty);
+    auto range = [&](long long n2, int w, int nt, int &t0, int &t1) {
+        t0 = (int)((lo + w - 1) / w);                      // first t with t*w >= lo
+        const long long last = (long long)n2 - 2 - np - (w - 1);
+        t1 = last < 0 ? 0 : (int)(last / w) + 1;           // t*w + w-1 <= n2-2-np
+        if (t1 > nt) t1 = nt;
+        if (t1 < t0) t1 = t0;
+    };
+    range((long long)h->nz2, 32, a.nkt, a.kt0, a.kt1);
+    range((long long)h->ny2, ty, a.njt, a.jt0, a.jt1);
+    if (a.kt1 == a.kt0 || a.jt1 == a.jt0) {
+        a.kt0 = a.kt1 = 0;
+        a.jt0 = a.jt1 = a.njt;
+    }
+}
+
+// step kernels one step launches: one per non-empty tile class
+int a3d_step_kernels(sm_a3d *h) {
+    a3d_tile_classes(h, kA3Configs[h->config].ty());
+    const A3Args &a = h->args;
+    const int ninner = (a.kt1 - a.kt0) * (a.jt1 - a.jt0);
+    return (ninner > 0) + (a.nkt * a.njt - ninner > 0);
+}
+
 // dynamic shared memory above 48 KB must be allowed per kernel and device
 template <typename S, int W, int R, int D, int MINB>
 int a3d_ready_cfg(sm_a3d *h) {
     static bool done[64] = {};   // per instantiation and device
     if (h->device < 0 || h->device >= 64) return sm_fail(SM_EINVAL, "device %d", h->device);
     if (!done[h->device]) {
-        SM_CUDA_TRY(cudaFuncSetAttribute(a3d_step_kernel<S, W, R, D, MINB>,
+        SM_CUDA_TRY(cudaFuncSetAttribute(a3d_step_kernel<S, W, R, D, MINB, A3_INNER>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)a3d_step_smem<S, W * R, D>()));
+        SM_CUDA_TRY(cudaFuncSetAttribute(a3d_step_kernel<S, W, R, D, MINB, A3_EDGE>,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          (int)a3d_step_smem<S, W * R, D>()));
         done[h->device] = true;
@@ -634,13 +776,33 @@ int a3d_ready_cfg(sm_a3d *h) {
 }
 
 template <typename S, int W, int R, int D, int MINB>
-void a3d_launch_cfg(sm_a3d *h) {
+int a3d_launch_cfg(sm_a3d *h) {
     constexpr int TY = W * R;
     constexpr size_t smem = a3d_step_smem<S, TY, D>();
+    A3Args &a = h->args;
+    a3d_tile_classes(h, TY);
+    const unsigned nch = (unsigned)((h->nx2 + a.chunk - 1) / a.chunk);
+    const int ninner = (a.kt1 - a.kt0) * (a.jt1 - a.jt0);
+    const int nedge = a.nkt * a.njt - ninner;
+    a.step_cls = ninner > 0 ? A3_INNER : A3_EDGE;
     dim3 blk(32, W, 1);
-    dim3 grd((unsigned)((h->nz2 + 31) / 32), (unsigned)((h->ny2 + TY - 1) / TY),
-             (unsigned)((h->nx2 + h->args.chunk - 1) / h->args.chunk));
-    a3d_step_kernel<S, W, R, D, MINB><<<grd, blk, smem, h->stream>>>(h->args, h->maps[h->cur]);
+    if (nedge > 0 && ninner > 0) {   // fork: the edge ring first, on the side stream
+        cudaEventRecord(h->ev_fork, h->stream);
+        cudaStreamWaitEvent(h->side, h->ev_fork, 0);
+    }
+    if (nedge > 0)
+        a3d_step_kernel<S, W, R, D, MINB, A3_EDGE>
+            <<<dim3((unsigned)nedge, 1, nch), blk, smem, ninner > 0 ? h->side : h->stream>>>(
+                a, h->maps[h->cur]);
+    if (ninner > 0)
+        a3d_step_kernel<S, W, R, D, MINB, A3_INNER>
+            <<<dim3((unsigned)(a.kt1 - a.kt0), (unsigned)(a.jt1 - a.jt0), nch), blk, smem,
+               h->stream>>>(a, h->maps[h->cur]);
+    if (nedge > 0 && ninner > 0) {   // join
+        cudaEventRecord(h->ev_join, h->side);
+        cudaStreamWaitEvent(h->stream, h->ev_join, 0);
+    }
+    return (nedge > 0) + (ninner > 0);
 }
 
 // TMA maps of one buffer set (as the step's input) for tile rows ty; box
@@ -755,17 +917,18 @@ int a3d_ready(sm_a3d *h) {
     }
 }
 
+// the step's kernels (one per non-empty tile class); returns how many
 template <typename S>
-void a3d_launch_step(sm_a3d *h) {
+int a3d_launch_step(sm_a3d *h) {
     switch (h->config) {
-    case 0: a3d_launch_cfg<S, 8, 2, 5, 2>(h); break;
-    case 1: a3d_launch_cfg<S, 4, 4, 5, 3>(h); break;
-    case 2: a3d_launch_cfg<S, 8, 4, 4, 1>(h); break;
-    case 3: a3d_launch_cfg<S, 8, 1, 6, 3>(h); break;
-    case 4: a3d_launch_cfg<S, 16, 2, 4, 1>(h); break;
-    case 5: a3d_launch_cfg<S, 4, 2, 6, 4>(h); break;
-    case 6: a3d_launch_cfg<S, 8, 2, 4, 3>(h); break;
-    default: a3d_launch_cfg<S, 4, 8, 4, 2>(h); break;
+    case 0: return a3d_launch_cfg<S, 8, 2, 5, 2>(h);
+    case 1: return a3d_launch_cfg<S, 4, 4, 5, 3>(h);
+    case 2: return a3d_launch_cfg<S, 8, 4, 4, 1>(h);
+    case 3: return a3d_launch_cfg<S, 8, 1, 6, 3>(h);
+    case 4: return a3d_launch_cfg<S, 16, 2, 4, 1>(h);
+    case 5: return a3d_launch_cfg<S, 4, 2, 6, 4>(h);
+    case 6: return a3d_launch_cfg<S, 8, 2, 4, 3>(h);
+    default: return a3d_launch_cfg<S, 4, 8, 4, 2>(h);
     }
 }
 
@@ -773,12 +936,12 @@ template <typename S>
 void a3d_launch(sm_a3d *h) {
     a3d_bind(h, h->cur);
     cudaEvent_t t0 = h->timer.begin(h->stream);
-    a3d_launch_step<S>(h);
+    const int nstep = a3d_launch_step<S>(h);
     h->timer.end(t0, h->stream);
     h->cur = 1 - h->cur;
     // sources and receivers act on the state just written
     a3d_bind(h, h->cur);
-    h->timer.launches += 1 + (h->src.empty() ? 0 : 1) + (h->rec.empty() ? 0 : 1);
+    h->timer.launches += nstep + (h->src.empty() ? 0 : 1) + (h->rec.empty() ? 0 : 1);
     if (!h->src.empty())
         a3d_source_kernel<S><<<1, 32, 0, h->stream>>>(h->args, h->d_src.as<A3Src>(),
                                                       (int)h->src.size(), h->d_vals.as<double>());
@@ -937,6 +1100,9 @@ extern "C" int sm_a3d_create(int device, size_t nx2, size_t ny2, size_t nz2, siz
     h->pitch = (int)round_up(nz2, 32);
     h->elem = storage_bytes(precision);
     SM_CUDA_TRY(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
+    SM_CUDA_TRY(cudaStreamCreateWithFlags(&h->side, cudaStreamNonBlocking));
+    SM_CUDA_TRY(cudaEventCreateWithFlags(&h->ev_fork, cudaEventDisableTiming));
+    SM_CUDA_TRY(cudaEventCreateWithFlags(&h->ev_join, cudaEventDisableTiming));
     const size_t cb = precision == SM_FP64 ? 8 : 4;
     const size_t ncell = nx2 * ny2 * (size_t)h->pitch;
     int rc;
@@ -1187,7 +1353,8 @@ template <typename S>
 int a3d_run_t(sm_a3d *h, size_t nsteps) {
     if (int rc = a3d_ready<S>(h)) return rc;
     const size_t G = (size_t)h->graph_steps;
-    const size_t per_step = 1 + (h->src.empty() ? 0 : 1) + (h->rec.empty() ? 0 : 1);
+    const size_t per_step =
+        (size_t)a3d_step_kernels(h) + (h->src.empty() ? 0 : 1) + (h->rec.empty() ? 0 : 1);
     while (nsteps > 0) {
         if (G && !h->timer.on && h->it % G == 0 && nsteps >= G) {
             cudaGraphExec_t ex = nullptr;
@@ -1416,6 +1583,12 @@ extern "C" int sm_a3d_destroy(sm_a3d_t h) {
         cudaStreamSynchronize(h->stream);
         cudaStreamDestroy(h->stream);
     }
+    if (h->side) {
+        cudaStreamSynchronize(h->side);
+        cudaStreamDestroy(h->side);
+    }
+    if (h->ev_fork) cudaEventDestroy(h->ev_fork);
+    if (h->ev_join) cudaEventDestroy(h->ev_join);
     delete h;
     return SM_OK;
 }

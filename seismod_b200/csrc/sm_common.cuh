@@ -258,8 +258,14 @@ __device__ __forceinline__ float r_add(float a, float b) { return __fadd_rn(a, b
 __device__ __forceinline__ float r_sub(float a, float b) { return __fsub_rn(a, b); }
 __device__ __forceinline__ float r_mul(float a, float b) { return __fmul_rn(a, b); }
 __device__ __forceinline__ float r_fma(float a, float b, float c) { return __fmaf_rn(a, b, c); }
-// 2 dt / (a + b): fast reciprocal in FP32 (within 2 ulp), exact in FP64
-__device__ __forceinline__ float r_quot(float num, float den) { return __fdividef(num, den); }
+// 2 dt / (a + b): in FP32 the numerator times the hardware's approximate
+// reciprocal (PTX rcp.approx.ftz.f32, within 1 ulp; the denominators here are
+// sums of densities, far from the denormal and overflow ranges), exact in FP64
+__device__ __forceinline__ float r_quot(float num, float den) {
+    float r;
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(den));
+    return __fmul_rn(num, r);
+}
 __device__ __forceinline__ double r_add(double a, double b) { return __dadd_rn(a, b); }
 __device__ __forceinline__ double r_sub(double a, double b) { return __dsub_rn(a, b); }
 __device__ __forceinline__ double r_mul(double a, double b) { return __dmul_rn(a, b); }

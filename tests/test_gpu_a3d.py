@@ -19,7 +19,12 @@ GOLDEN = sorted(glob.glob(os.path.join(os.path.dirname(__file__), "golden", "a3d
 
 
 @pytest.mark.parametrize("precision", ["fp64", "fp32"])
-@pytest.mark.parametrize("shape", [((12, 10, 14), 2), ((20, 20, 20), 5), ((9, 17, 33), 3)])
+@pytest.mark.parametrize("shape", [((12, 10, 14), 2), ((20, 20, 20), 5), ((9, 17, 33), 3),
+                                   # 48 x 58 x 98 padded: tiles clear of the frame, on one
+                                   # face (y or z), on two, and planes inside the x frame
+                                   ((40, 50, 90), 4),
+                                   # abs 0: no frame, the edges alone (index 0 never updated)
+                                   ((40, 50, 90), 0)])
 def test_steps_from_random_state(shape, precision):
     (nx, ny, nz), npml = shape
     rng = np.random.default_rng(nx * ny + nz)
