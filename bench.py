@@ -175,11 +175,12 @@ def make_workload(name, size=None):
 
 # DRAM bytes (read + written) per step of the dominant kernel(s), measured
 # with ncu on B200 for exactly these workloads (profiles/ holds the
-# summaries and the commands): a_iso_3d 288^3 FP32 (a 224^3 capture scaled by
-# the cell count, which traffic follows), e_iso 64 x 1040 x 540 FP32, and the
-# velocity + stress launches of e_cyl_iso 2020 x 4040 FP32.
+# summaries and the commands): the interior + ring launches of a_iso_3d
+# 288^3 FP32 (a 224^3 capture scaled by the cell count, which traffic
+# follows), e_iso 64 x 1040 x 540 FP32, and the velocity + stress launches of
+# e_cyl_iso 2020 x 4040 FP32.
 MEASURED_TRAFFIC = {
-    ("a3d", 256, "fp32"): 1.085e9,
+    ("a3d", 256, "fp32"): 1.129e9,
     ("eiso", 1000, "fp32"): 1.8375e9,
     ("ecyl", 2000, "fp32"): 1.1106e9,
 }
