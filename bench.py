@@ -413,9 +413,26 @@ def e2e(kind, p, K, local_rank):
     """Whole user call through the public API from host arrays: set-up and
     upload, K steps, traces back to the host, teardown."""
     from seismod_b200 import api
-    t0 = time.perf_counter()
-    dev, _ = device_for(kind, p, "fp32", local_rank)
+    marks = [("start", time.perf_counter())]
+    if kind == "a3d":   # the steps of api.a3d_device, timed one by one
+        q = api.a3d_inputs(p)
+        marks.append(("host_inputs", time.perf_counter()))
+        dev = api.A3DDevice(q["vp"], q["rho"], q["npml"], q["d"], q["dt"], q["coef"], "fp32",
+                            local_rank)
+        dev.set_sources(*q["src"], q["src_scale"])
+        dev.set_receivers(*q["rec"], q["nsteps"])
+        marks.append(("create_upload", time.perf_counter()))
+        if TUNE:
+            dev.autotune()
+        if GRAPH:
+            dev.set_graph(GRAPH)
+        marks.append(("tune_graph", time.perf_counter()))
+    else:
+        dev, _ = device_for(kind, p, "fp32", local_rank)
+        marks.append(("setup", time.perf_counter()))
     dev.run(K)
+    dev.sync()
+    marks.append(("steps", time.perf_counter()))
     if kind == "a3d":
         tr = dev.traces_array()
         d2h = tr.size * 8
@@ -425,8 +442,11 @@ def e2e(kind, p, K, local_rank):
     else:
         tr = [dev.traces(s) for s in range(dev.nshots)]
         d2h = sum(sum(len(x) for x in t) for t in tr) * 8
+    marks.append(("traces_back", time.perf_counter()))
     dev.close()
-    wall = time.perf_counter() - t0
+    marks.append(("teardown", time.perf_counter()))
+    wall = marks[-1][1] - marks[0][1]
+    phases = {marks[k][0]: round(marks[k][1] - marks[k - 1][1], 4) for k in range(1, len(marks))}
     if kind == "a3d":
         n2 = [n + 2 * p.npml for n in p.shape]
         pitch = math.ceil(n2[2] / 32) * 32
@@ -442,7 +462,7 @@ def e2e(kind, p, K, local_rank):
         cells = p.cells * len(p.shots)
     return {"value": round(cells * K / wall / 1e9, 3), "unit": "Gcell/s",
             "h2d_bytes_per_step": int(h2d / K), "d2h_bytes_per_step": int(d2h / K),
-            "wall_s": round(wall, 3)}
+            "wall_s": round(wall, 3), "phases_s": phases}
 
 
 # ----------------------------------------------------------------------------

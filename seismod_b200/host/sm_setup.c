@@ -8,8 +8,10 @@
 #include "sm_host.h"
 
 #include <math.h>
+#include <pthread.h>
 #include <stdlib.h>
 #include <string.h>
+#include <unistd.h>
 
 size_t sm_ricker_length(double f, double dt, double fac)
 {
@@ -139,28 +141,69 @@ int sm_eiso_profiles(size_t np, double h, size_t ncell, const double *vp,
     return SM_OK;
 }
 
+/* one thread's share of sm_a3d_pad_model: padded x planes [i0, i1) */
+struct a3d_pad_part {
+    size_t nx, ny, nz, np, i0, i1;
+    const double *vp, *rho;
+    double *vp_pad, *rho_pad;
+};
+
+static void *a3d_pad_planes(void *arg)
+{
+    const struct a3d_pad_part *t = (const struct a3d_pad_part *)arg;
+    const size_t nx = t->nx, ny = t->ny, nz = t->nz, np = t->np;
+    const size_t ny2 = ny + 2 * np, nz2 = nz + 2 * np;
+    for (size_t i = t->i0; i < t->i1; ++i) {
+        size_t ii = i < np ? 0 : (i - np >= nx ? nx - 1 : i - np);
+        for (size_t j = 0; j < ny2; ++j) {
+            size_t jj = j < np ? 0 : (j - np >= ny ? ny - 1 : j - np);
+            const double *sv = t->vp + (ii * ny + jj) * nz;
+            const double *sr = t->rho + (ii * ny + jj) * nz;
+            double *dv = t->vp_pad + (i * ny2 + j) * nz2;
+            double *dr = t->rho_pad + (i * ny2 + j) * nz2;
+            for (size_t k = 0; k < np; ++k) {
+                dv[k] = sv[0];
+                dr[k] = sr[0];
+            }
+            memcpy(dv + np, sv, nz * sizeof(double));
+            memcpy(dr + np, sr, nz * sizeof(double));
+            for (size_t k = np + nz; k < nz2; ++k) {
+                dv[k] = sv[nz - 1];
+                dr[k] = sr[nz - 1];
+            }
+        }
+    }
+    return NULL;
+}
+
 int sm_a3d_pad_model(size_t nx, size_t ny, size_t nz, size_t np,
                      const double *vp, const double *rho, double *vp_pad, double *rho_pad)
 {
     if (!nx || !ny || !nz || !vp || !rho || !vp_pad || !rho_pad)
         return sm_fail(SM_EINVAL, "sm_a3d_pad_model: bad argument");
     /* io_utils.c:1096-1143: every padded node takes the value of the nearest
-     * interior node (replication along z, then y, then x) */
+     * interior node (replication along z, then y, then x).  A pure copy, so
+     * the x planes are split over host threads (the two padded volumes of a
+     * 544^3 grid are 2.5 GB; one thread spends most of a second on them,
+     * first-touch page faults included). */
     const size_t nx2 = nx + 2 * np, ny2 = ny + 2 * np, nz2 = nz + 2 * np;
-    for (size_t i = 0; i < nx2; ++i) {
-        size_t ii = i < np ? 0 : (i - np >= nx ? nx - 1 : i - np);
-        for (size_t j = 0; j < ny2; ++j) {
-            size_t jj = j < np ? 0 : (j - np >= ny ? ny - 1 : j - np);
-            const double *sv = vp + (ii * ny + jj) * nz;
-            const double *sr = rho + (ii * ny + jj) * nz;
-            double *dv = vp_pad + (i * ny2 + j) * nz2;
-            double *dr = rho_pad + (i * ny2 + j) * nz2;
-            for (size_t k = 0; k < nz2; ++k) {
-                size_t kk = k < np ? 0 : (k - np >= nz ? nz - 1 : k - np);
-                dv[k] = sv[kk];
-                dr[k] = sr[kk];
-            }
-        }
+    const size_t cells = nx2 * ny2 * nz2;
+    long ncpu = sysconf(_SC_NPROCESSORS_ONLN);
+    size_t nt = cells < ((size_t)1 << 20) || ncpu < 2 ? 1 : (size_t)ncpu;
+    if (nt > 16) nt = 16;
+    if (nt > nx2) nt = nx2;
+    struct a3d_pad_part part[16];
+    pthread_t tid[16];
+    int started[16] = {0};
+    for (size_t t = 0; t < nt; ++t) {
+        part[t] = (struct a3d_pad_part){nx, ny, nz, np, nx2 * t / nt, nx2 * (t + 1) / nt,
+                                        vp, rho, vp_pad, rho_pad};
+        if (t > 0) started[t] = pthread_create(&tid[t], NULL, a3d_pad_planes, &part[t]) == 0;
+    }
+    a3d_pad_planes(&part[0]);
+    for (size_t t = 1; t < nt; ++t) {
+        if (started[t]) pthread_join(tid[t], NULL);
+        else a3d_pad_planes(&part[t]);   /* no thread: do its share here */
     }
     return SM_OK;
 }

@@ -66,6 +66,21 @@ def test_a3d_setup_matches_oracle_bitwise():
                 np.testing.assert_array_equal(u, v)
 
 
+def test_a3d_pad_model_split_over_threads_equals_the_oracle():
+    # above 2^20 padded cells the padding runs on several host threads, each
+    # owning a range of x planes: edge planes, rows and columns must come out
+    # as the single-threaded oracle pads them
+    rng = np.random.default_rng(5)
+    for shape, npml in [((61, 70, 83), 16), ((100, 9, 1100), 5), ((3, 400, 900), 1)]:
+        vp = 1500 + 3000 * rng.random(shape)
+        rho = 1800 + 500 * rng.random(shape)
+        a = api.a3d_pad_model(vp, rho, npml)
+        b = O.a3d_pad_model(vp, rho, npml)
+        assert a[0].size >= 1 << 20
+        np.testing.assert_array_equal(a[0], b[0])
+        np.testing.assert_array_equal(a[1], b[1])
+
+
 def test_sampling_and_nsteps_match_oracle():
     for dt in (8.838834764831844e-05, 1e-4, 1.7e-4):
         for (t0, rdt) in [(0.0, dt), (0.0, 3 * dt), (2e-3, dt), (5 * dt, 0.0), (0.0, 2.5 * dt)]:
