@@ -758,11 +758,15 @@ int a3d_step_kernels(sm_a3d *h) {
     return (ninner > 0) + (a.nkt * a.njt - ninner > 0);
 }
 
-// dynamic shared memory above 48 KB must be allowed per kernel and device
+// dynamic shared memory above 48 KB must be allowed per kernel and device;
+// handles are created from several threads (the request loop's worker and
+// its callers), so the per-device flags are read and set under a lock
 template <typename S, int W, int R, int D, int MINB>
 int a3d_ready_cfg(sm_a3d *h) {
+    static std::mutex mu;
     static bool done[64] = {};   // per instantiation and device
     if (h->device < 0 || h->device >= 64) return sm_fail(SM_EINVAL, "device %d", h->device);
+    std::lock_guard<std::mutex> lk(mu);
     if (!done[h->device]) {
         SM_CUDA_TRY(cudaFuncSetAttribute(a3d_step_kernel<S, W, R, D, MINB, A3_INNER>,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize,
