@@ -16,6 +16,8 @@
 #include <string.h>
 #include <sys/stat.h>
 #include <sys/types.h>
+#include <pthread.h>
+#include <unistd.h>
 #include <stdint.h>
 #include <time.h>
 
@@ -305,6 +307,143 @@ bad:
     return sm_fail(SM_EIO, "something wrong with file %s", path);
 }
 
+/* ---------------------------------------------------------------------------
+ * Whitespace-separated numbers of a text model, parsed on host threads.  The
+ * reference reads one value per fscanf("%lf") call (io_utils.c:1068-1094),
+ * minutes for a 512^3 model.  Here the rest of the file is read into memory
+ * and cut into chunks at whitespace; pass 1 counts each chunk's tokens, pass 2
+ * converts each token with strtod (the conversion fscanf's %lf makes, so the
+ * values are the same bits) into its place: token t is field t % 2 of cell
+ * t / 2, the file's order.
+ * ------------------------------------------------------------------------- */
+typedef struct {
+    const char *b, *e;   /* [b, e): starts and ends on a token boundary */
+    size_t ntok;         /* pass 1: tokens in the chunk */
+    size_t first, need;  /* pass 2: index of the chunk's first token; tokens to convert */
+    double *v[2];        /* even tokens -> v[0][t / 2], odd -> v[1][t / 2] */
+    size_t bad;          /* first token that is not a whole number, or (size_t)-1 */
+} num_chunk;
+
+static void *num_count(void *arg)
+{
+    num_chunk *c = (num_chunk *)arg;
+    size_t n = 0;
+    int in = 0;
+    for (const char *p = c->b; p < c->e; ++p) {
+        const int sp = isspace((unsigned char)*p);
+        if (!sp && !in) ++n;
+        in = !sp;
+    }
+    c->ntok = n;
+    return NULL;
+}
+
+static void *num_convert(void *arg)
+{
+    num_chunk *c = (num_chunk *)arg;
+    size_t t = c->first;
+    const char *p = c->b;
+    c->bad = (size_t)-1;
+    while (p < c->e && t < c->need) {
+        while (p < c->e && isspace((unsigned char)*p)) ++p;
+        if (p >= c->e) break;
+        const char *q = p;
+        while (q < c->e && !isspace((unsigned char)*q)) ++q;
+        char *end;
+        const double x = strtod(p, &end);   /* stops at the whitespace after the token */
+        if (end != q) {
+            c->bad = t;
+            return NULL;
+        }
+        c->v[t & 1][t >> 1] = x;
+        ++t;
+        p = q;
+    }
+    return NULL;
+}
+
+/* run fn over the chunks, one thread each (the first on the caller) */
+static void num_run(void *(*fn)(void *), num_chunk *c, size_t nc)
+{
+    pthread_t tid[16];
+    int started[16] = {0};
+    for (size_t k = 1; k < nc; ++k) started[k] = pthread_create(&tid[k], NULL, fn, &c[k]) == 0;
+    fn(&c[0]);
+    for (size_t k = 1; k < nc; ++k) {
+        if (started[k]) pthread_join(tid[k], NULL);
+        else fn(&c[k]);
+    }
+}
+
+/* The values after a model header: 2*nz numbers (one column, the 1-D profile
+ * shortcut) when no number follows them, else 2*n.  *is1d tells which.
+ * Returns 0, or -1 when the file holds fewer numbers than needed or a token
+ * that is not a number where one is needed (the reference's "something
+ * wrong" cases). */
+static int read_pairs(FILE *fid, size_t nz, size_t n, double *v0, double *v1, int *is1d)
+{
+    struct stat st;
+    const long off = ftell(fid);
+    if (off < 0 || fstat(fileno(fid), &st) != 0 || (long long)st.st_size < off) return -1;
+    const size_t rem = (size_t)st.st_size - (size_t)off;
+    char *buf = malloc(rem + 1);
+    if (!buf) return -1;
+    const size_t len = fread(buf, 1, rem, fid);
+    buf[len] = 0;
+    long ncpu = sysconf(_SC_NPROCESSORS_ONLN);
+    size_t nc = len < ((size_t)1 << 20) || ncpu < 2 ? 1 : (size_t)ncpu;
+    if (nc > 16) nc = 16;
+    num_chunk c[16];
+    const char *start = buf;
+    for (size_t k = 0; k < nc; ++k) {
+        const char *e = k + 1 == nc ? buf + len : buf + len * (k + 1) / nc;
+        if (e < start) e = start;
+        while (e < buf + len && !isspace((unsigned char)*e)) ++e;   /* end at whitespace */
+        c[k].b = start;
+        c[k].e = e;
+        start = e;
+    }
+    num_run(num_count, c, nc);
+    size_t ntok = 0;
+    for (size_t k = 0; k < nc; ++k) {
+        c[k].first = ntok;
+        ntok += c[k].ntok;
+    }
+    int rc = -1;
+    if (ntok < 2 * nz) goto done;
+    /* io_utils.c:1074-1080: the read of the second column returning nothing
+     * (end of file, or no number at all) means a 1-D profile */
+    *is1d = 1;
+    if (ntok > 2 * nz) {
+        size_t t = 0, k = 0;   /* the token at index 2*nz */
+        while (k < nc && t + c[k].ntok <= 2 * nz) t += c[k++].ntok;
+        const char *p = c[k].b;
+        for (;;) {
+            while (isspace((unsigned char)*p)) ++p;
+            if (t == 2 * nz) break;
+            while (*p && !isspace((unsigned char)*p)) ++p;
+            ++t;
+        }
+        char *end;
+        (void)strtod(p, &end);
+        if (end != p) *is1d = 0;
+    }
+    const size_t need = *is1d ? 2 * nz : 2 * n;
+    if (ntok < need) goto done;
+    for (size_t k = 0; k < nc; ++k) {
+        c[k].need = need;
+        c[k].v[0] = v0;
+        c[k].v[1] = v1;
+    }
+    num_run(num_convert, c, nc);
+    rc = 0;
+    for (size_t k = 0; k < nc; ++k)
+        if (c[k].bad != (size_t)-1) rc = -1;
+done:
+    free(buf);
+    return rc;
+}
+
 int sm_read_model_a(const char *path, sm_grid *g, double **pvp, double **prho)
 {
     if (model_is_binary(path)) {
@@ -341,15 +480,7 @@ int sm_read_model_a(const char *path, sm_grid *g, double **pvp, double **prho)
         return sm_fail(SM_ENOMEM, "out of host memory");
     }
     int flag1d = 0;
-    for (size_t i = 0; i < nx && !flag1d; ++i)
-        for (size_t j = 0; j < ny; ++j) {
-            size_t q = (i * ny + j) * nz;
-            int nread = fscanf(fid, "%lf %lf", &vp[q], &rho[q]);
-            if (nread <= 0 && j == 1) { flag1d = 1; break; }
-            if (nread != 2) goto bad;
-            for (size_t k = 1; k < nz; ++k)
-                if (fscanf(fid, "%lf %lf", &vp[q + k], &rho[q + k]) != 2) goto bad;
-        }
+    if (read_pairs(fid, nz, n, vp, rho, &flag1d)) goto bad;
     fclose(fid);
     if (flag1d)
         for (size_t q = nz; q < n; ++q) {
