@@ -183,6 +183,10 @@ static int read_model_bin(const char *path, unsigned ndim, unsigned nfields, sm_
     return SM_OK;
 }
 
+/* the values of a text model, on host threads (below) */
+static int read_values(FILE *fid, size_t ncol, size_t n, int nf, double *const *v, size_t tnx,
+                       size_t tnz, int *is1d);
+
 int sm_read_model_ecyl(const char *path, sm_grid *g, double **pvp, double **pvs, double **prho)
 {
     if (model_is_binary(path)) return sm_read_model_e(path, g, pvp, pvs, prho);
@@ -216,16 +220,10 @@ int sm_read_model_ecyl(const char *path, sm_grid *g, double **pvp, double **pvs,
         return sm_fail(SM_ENOMEM, "out of host memory");
     }
     int profile = 0;
-    for (size_t j = 0; j < nz && !profile; ++j) {
-        for (size_t i = 0; i < nx; ++i) {
-            const size_t q = i * nz + j;
-            const int nread = fscanf(fid, "%lf %lf %lf", &vp[q], &vs[q], &rho[q]);
-            if (nread <= 0 && j == 1 && i == 0) { profile = 1; break; }
-            if (nread != 3) {
-                fclose(fid); free(vp); free(vs); free(rho);
-                return sm_fail(SM_EIO, "something wrong with file %s", path);
-            }
-        }
+    double *const va[3] = {vp, vs, rho};
+    if (read_values(fid, nx, nx * nz, 3, va, nx, nz, &profile)) {
+        fclose(fid); free(vp); free(vs); free(rho);
+        return sm_fail(SM_EIO, "something wrong with file %s", path);
     }
     fclose(fid);
     if (profile)
@@ -281,16 +279,8 @@ int sm_read_model_e(const char *path, sm_grid *g, double **pvp, double **pvs, do
         return sm_fail(SM_ENOMEM, "out of host memory");
     }
     int flag1d = 0;
-    for (size_t i = 0; i < nx && !flag1d; ++i) {
-        size_t q = i * nz;
-        int nread = fscanf(fid, "%lf %lf %lf", &vp[q], &vs[q], &rho[q]);
-        if (nread <= 0 && i == 1) { flag1d = 1; break; }
-        if (nread != 3) goto bad;
-        for (size_t j = 1; j < nz; ++j) {
-            q = i * nz + j;
-            if (fscanf(fid, "%lf %lf %lf", &vp[q], &vs[q], &rho[q]) != 3) goto bad;
-        }
-    }
+    double *const va[3] = {vp, vs, rho};
+    if (read_values(fid, nz, nx * nz, 3, va, 0, 0, &flag1d)) goto bad;
     fclose(fid);
     if (flag1d)
         for (size_t i = 1; i < nx; ++i)
@@ -313,14 +303,17 @@ bad:
  * minutes for a 512^3 model.  Here the rest of the file is read into memory
  * and cut into chunks at whitespace; pass 1 counts each chunk's tokens, pass 2
  * converts each token with strtod (the conversion fscanf's %lf makes, so the
- * values are the same bits) into its place: token t is field t % 2 of cell
- * t / 2, the file's order.
+ * values are the same bits) into its place: token t is field t % nf of the
+ * file's cell t / nf, stored at that cell's index (the file's order, or for
+ * the cylindrical models, whose rows are z, the transposed one).
  * ------------------------------------------------------------------------- */
 typedef struct {
     const char *b, *e;   /* [b, e): starts and ends on a token boundary */
     size_t ntok;         /* pass 1: tokens in the chunk */
     size_t first, need;  /* pass 2: index of the chunk's first token; tokens to convert */
-    double *v[2];        /* even tokens -> v[0][t / 2], odd -> v[1][t / 2] */
+    int nf;              /* fields per cell */
+    size_t tnx, tnz;     /* tnx > 0: file cell c is stored at (c % tnx) * tnz + c / tnx */
+    double *v[3];        /* field f of the cell -> v[f][cell] */
     size_t bad;          /* first token that is not a whole number, or (size_t)-1 */
 } num_chunk;
 
@@ -355,7 +348,9 @@ static void *num_convert(void *arg)
             c->bad = t;
             return NULL;
         }
-        c->v[t & 1][t >> 1] = x;
+        const size_t cell = t / (size_t)c->nf;
+        const size_t at = c->tnx ? (cell % c->tnx) * c->tnz + cell / c->tnx : cell;
+        c->v[t % (size_t)c->nf][at] = x;
         ++t;
         p = q;
     }
@@ -375,13 +370,15 @@ static void num_run(void *(*fn)(void *), num_chunk *c, size_t nc)
     }
 }
 
-/* The values after a model header: 2*nz numbers (one column, the 1-D profile
- * shortcut) when no number follows them, else 2*n.  *is1d tells which.
- * Returns 0, or -1 when the file holds fewer numbers than needed or a token
- * that is not a number where one is needed (the reference's "something
- * wrong" cases). */
-static int read_pairs(FILE *fid, size_t nz, size_t n, double *v0, double *v1, int *is1d)
+/* The values after a model header, nf per cell: ncol cells (the first
+ * column or row: the profile shortcut) when no number follows them, else all
+ * n cells.  *is1d tells which.  Returns 0, or -1 when the file holds fewer
+ * numbers than needed or a token that is not a number where one is needed
+ * (the reference's "something wrong" cases). */
+static int read_values(FILE *fid, size_t ncol, size_t n, int nf, double *const *v, size_t tnx,
+                       size_t tnz, int *is1d)
 {
+    const size_t nfz = (size_t)nf;
     struct stat st;
     const long off = ftell(fid);
     if (off < 0 || fstat(fileno(fid), &st) != 0 || (long long)st.st_size < off) return -1;
@@ -410,17 +407,18 @@ static int read_pairs(FILE *fid, size_t nz, size_t n, double *v0, double *v1, in
         ntok += c[k].ntok;
     }
     int rc = -1;
-    if (ntok < 2 * nz) goto done;
-    /* io_utils.c:1074-1080: the read of the second column returning nothing
-     * (end of file, or no number at all) means a 1-D profile */
+    if (ntok < nfz * ncol) goto done;
+    /* the read of the second column (row) returning nothing -- end of file,
+     * or no number at all -- means a profile (io_utils.c:918-946, 970-990,
+     * 1074-1080) */
     *is1d = 1;
-    if (ntok > 2 * nz) {
-        size_t t = 0, k = 0;   /* the token at index 2*nz */
-        while (k < nc && t + c[k].ntok <= 2 * nz) t += c[k++].ntok;
+    if (ntok > nfz * ncol) {
+        size_t t = 0, k = 0;   /* the token at index nf*ncol */
+        while (k < nc && t + c[k].ntok <= nfz * ncol) t += c[k++].ntok;
         const char *p = c[k].b;
         for (;;) {
             while (isspace((unsigned char)*p)) ++p;
-            if (t == 2 * nz) break;
+            if (t == nfz * ncol) break;
             while (*p && !isspace((unsigned char)*p)) ++p;
             ++t;
         }
@@ -428,12 +426,14 @@ static int read_pairs(FILE *fid, size_t nz, size_t n, double *v0, double *v1, in
         (void)strtod(p, &end);
         if (end != p) *is1d = 0;
     }
-    const size_t need = *is1d ? 2 * nz : 2 * n;
+    const size_t need = *is1d ? nfz * ncol : nfz * n;
     if (ntok < need) goto done;
     for (size_t k = 0; k < nc; ++k) {
         c[k].need = need;
-        c[k].v[0] = v0;
-        c[k].v[1] = v1;
+        c[k].nf = nf;
+        c[k].tnx = tnx;
+        c[k].tnz = tnz;
+        for (int fl = 0; fl < 3; ++fl) c[k].v[fl] = fl < nf ? v[fl] : NULL;
     }
     num_run(num_convert, c, nc);
     rc = 0;
@@ -480,7 +480,8 @@ int sm_read_model_a(const char *path, sm_grid *g, double **pvp, double **prho)
         return sm_fail(SM_ENOMEM, "out of host memory");
     }
     int flag1d = 0;
-    if (read_pairs(fid, nz, n, vp, rho, &flag1d)) goto bad;
+    double *const va[2] = {vp, rho};
+    if (read_values(fid, nz, n, 2, va, 0, 0, &flag1d)) goto bad;
     fclose(fid);
     if (flag1d)
         for (size_t q = nz; q < n; ++q) {
