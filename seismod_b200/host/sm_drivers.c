@@ -40,17 +40,8 @@ static void rec_plan_free(rec_plan *r)
 static int write_traces(const char *base, const rec_plan *rp, const double *vals, size_t ld,
                         const size_t *counts, double dt, size_t nsteps)
 {
-    double *t = malloc((ld ? ld : 1) * sizeof(double));
-    if (!t) return sm_fail(SM_ENOMEM, "out of host memory");
-    for (size_t r = 0; r < rp->n; ++r) {
-        size_t s = 0;
-        for (size_t it = 0; it < nsteps && s < counts[r]; ++it)
-            if (sm_sample_predicate(it, dt, rp->t0[r], rp->rdt[r])) t[s++] = dt * (it + 1);
-        int rc = sm_write_trace_file(base, rp->recno[r] + 1, t, vals + r * ld, counts[r]);
-        if (rc) { free(t); return rc; }
-    }
-    free(t);
-    return SM_OK;
+    return sm_write_trace_set(base, rp->n, rp->recno, rp->t0, rp->rdt, dt, nsteps, vals, ld,
+                              counts);
 }
 
 /* Snapshot records: the steps at which each is taken, by the traces'

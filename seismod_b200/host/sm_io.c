@@ -680,6 +680,78 @@ int sm_write_trace_file(const char *base, size_t n, const double *t, const doubl
     return SM_OK;
 }
 
+/* ---- the trace files of a run, written on host threads ---- */
+typedef struct {
+    const char *base;
+    const size_t *recno, *counts;
+    const double *t0, *rdt, *vals;
+    double dt;
+    size_t nsteps, ld, r0, r1;
+    int rc;
+    char msg[512];   /* the failing thread's message (messages are per thread) */
+} trace_part;
+
+static void *trace_files(void *arg)
+{
+    trace_part *w = (trace_part *)arg;
+    w->rc = SM_OK;
+    double *t = malloc((w->ld ? w->ld : 1) * sizeof(double));
+    if (!t) {
+        w->rc = SM_ENOMEM;
+        snprintf(w->msg, sizeof w->msg, "out of host memory");
+        return NULL;
+    }
+    for (size_t r = w->r0; r < w->r1; ++r) {
+        /* the sample times: the steps the sampling test keeps (e_iso.c:641-669) */
+        size_t s = 0;
+        for (size_t it = 0; it < w->nsteps && s < w->counts[r]; ++it)
+            if (sm_sample_predicate(it, w->dt, w->t0[r], w->rdt[r])) t[s++] = w->dt * (double)(it + 1);
+        const int rc = sm_write_trace_file(w->base, w->recno[r] + 1, t, w->vals + r * w->ld,
+                                           w->counts[r]);
+        if (rc) {
+            w->rc = rc;
+            snprintf(w->msg, sizeof w->msg, "%s", sm_last_error());
+            break;
+        }
+    }
+    free(t);
+    return NULL;
+}
+
+int sm_write_trace_set(const char *base, size_t nrec, const size_t *recno, const double *t0,
+                       const double *rdt, double dt, size_t nsteps, const double *vals, size_t ld,
+                       const size_t *counts)
+{
+    if (!nrec) return SM_OK;
+    if (!base || !recno || !t0 || !rdt || !vals || !counts)
+        return sm_fail(SM_EINVAL, "sm_write_trace_set: NULL argument");
+    /* the directories first, so the threads only find them */
+    char path[512];
+    int rc;
+    if ((rc = ensure_dir("trc"))) return rc;
+    snprintf(path, sizeof path, "trc/%s", base);
+    if ((rc = ensure_dir(path))) return rc;
+    long ncpu = sysconf(_SC_NPROCESSORS_ONLN);
+    size_t nt = nrec < 64 || ncpu < 2 ? 1 : (size_t)ncpu;
+    if (nt > 16) nt = 16;
+    trace_part w[16];
+    pthread_t tid[16];
+    int started[16] = {0};
+    for (size_t k = 0; k < nt; ++k) {
+        w[k] = (trace_part){base, recno, counts, t0, rdt, vals, dt, nsteps, ld,
+                            nrec * k / nt, nrec * (k + 1) / nt, SM_OK, {0}};
+        if (k > 0) started[k] = pthread_create(&tid[k], NULL, trace_files, &w[k]) == 0;
+    }
+    trace_files(&w[0]);
+    for (size_t k = 1; k < nt; ++k) {
+        if (started[k]) pthread_join(tid[k], NULL);
+        else trace_files(&w[k]);
+    }
+    for (size_t k = 0; k < nt; ++k)   /* the first failure in receiver order */
+        if (w[k].rc) return sm_fail(w[k].rc, "%s", w[k].msg);
+    return SM_OK;
+}
+
 /* ---- SEG-Y (io_utils.c:3269-3559 layout) ---- */
 
 static int put(FILE *f, const void *p, size_t n) { return fwrite(p, 1, n, f) == n; }

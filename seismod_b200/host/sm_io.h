@@ -73,6 +73,14 @@ int sm_read_records(const char *path, const sm_grid *g, int three_d, sm_record *
 /* trc/<base>/<base>_<n>.trc, "%le    %le" of t and 1e3 * v (io_utils.c:1744-1768) */
 int sm_write_trace_file(const char *base, size_t n, const double *t, const double *v,
                         size_t ns);
+/* every receiver's trace file of a run (receiver r: file recno[r] + 1, its
+ * counts[r] samples vals[r * ld ...] at the times dt * (it + 1) of the steps
+ * it < nsteps that sm_sample_predicate(it, dt, t0[r], rdt[r]) keeps), the
+ * files split over host threads; the first failure in receiver order is
+ * returned */
+int sm_write_trace_set(const char *base, size_t nrec, const size_t *recno, const double *t0,
+                       const double *rdt, double dt, size_t nsteps, const double *vals, size_t ld,
+                       const size_t *counts);
 /* segy/<base>.sgy with the layout save_segy writes (io_utils.c:3269-3559):
  * 3200-byte textual header, 400-byte binary header, per trace a 240-byte
  * header and its samples as IEEE float32, all in the host's byte order as the
