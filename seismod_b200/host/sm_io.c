@@ -379,13 +379,28 @@ static int read_values(FILE *fid, size_t ncol, size_t n, int nf, double *const *
                        size_t tnz, int *is1d)
 {
     const size_t nfz = (size_t)nf;
+    /* the rest of the file, to its end: the buffer is sized from the file's
+     * size and grows if more comes (a file still being written) */
     struct stat st;
     const long off = ftell(fid);
-    if (off < 0 || fstat(fileno(fid), &st) != 0 || (long long)st.st_size < off) return -1;
-    const size_t rem = (size_t)st.st_size - (size_t)off;
-    char *buf = malloc(rem + 1);
+    size_t cap = (size_t)1 << 20;
+    if (off >= 0 && fstat(fileno(fid), &st) == 0 && S_ISREG(st.st_mode) &&
+        (long long)st.st_size >= off)
+        cap = (size_t)st.st_size - (size_t)off + 2;   /* + a byte to meet the end, + NUL */
+    char *buf = malloc(cap);
     if (!buf) return -1;
-    const size_t len = fread(buf, 1, rem, fid);
+    size_t len = 0;
+    for (;;) {
+        len += fread(buf + len, 1, cap - 1 - len, fid);
+        if (len < cap - 1 || feof(fid)) break;
+        char *nb = realloc(buf, 2 * cap);   /* full: the input goes on */
+        if (!nb) {
+            free(buf);
+            return -1;
+        }
+        buf = nb;
+        cap *= 2;
+    }
     buf[len] = 0;
     long ncpu = sysconf(_SC_NPROCESSORS_ONLN);
     size_t nc = len < ((size_t)1 << 20) || ncpu < 2 ? 1 : (size_t)ncpu;

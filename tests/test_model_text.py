@@ -184,3 +184,4 @@ def test_2d_models_equal_a_correctly_rounded_parse(tmp_path, fn, kw, rows_are_z,
             f.write(f"{nx} {nz}\n1.0 1.0\n0.0 0.0\n{kw}\n" + " ".join(body.split()[:-1]) + "\n")
         rc, _, _ = _read3(fn, path)
         assert rc == L.SM_EIO
+
