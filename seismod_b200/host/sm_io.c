@@ -883,6 +883,54 @@ int sm_write_segy(const char *base, const sm_params *p, const sm_record *rec, si
 /* the snapshot file of write_snapshot; npl: absorbing columns before column
  * 0 of the model (np on the Cartesian grids, 0 on the cylindrical one, whose
  * axis has none), npr: after its last column */
+/* one thread's share of a text snapshot: the lines of columns [i0, i1),
+ * formatted into its own buffer (the bytes fprintf would write) */
+typedef struct {
+    const double *data;
+    size_t nx2, nz2, npl, npr, np, i0, i1;
+    double dx, dz, x0, z0;
+    int plot_strips;
+    char *buf;
+    size_t len, cap;
+    int bad;
+} snap_part;
+
+static void snap_put(snap_part *w, double x, double z, double v)
+{
+    if (w->bad) return;
+    if (w->cap - w->len < 128) {
+        size_t cap = w->cap ? 2 * w->cap : (size_t)1 << 16;
+        char *nb = realloc(w->buf, cap);
+        if (!nb) { w->bad = 1; return; }
+        w->buf = nb;
+        w->cap = cap;
+    }
+    const int k = snprintf(w->buf + w->len, w->cap - w->len, "%le  %le  %le\n", x, z, v);
+    if (k < 0 || (size_t)k >= w->cap - w->len) { w->bad = 1; return; }
+    w->len += (size_t)k;
+}
+
+static void *snap_format(void *arg)
+{
+    snap_part *w = (snap_part *)arg;
+    for (size_t i = w->i0; i < w->i1; ++i) {
+        if (w->plot_strips) {
+            const double x = w->x0 + ((double)i - (double)w->npl) * w->dx;
+            for (size_t k = 0; k < w->nz2; ++k)
+                snap_put(w, x, w->z0 + ((double)k - (double)w->np) * w->dz,
+                         1.e3 * w->data[i * w->nz2 + k]);
+        } else {
+            const double x = w->x0 + i * w->dx;
+            for (size_t k = 0; k + 2 * w->np < w->nz2; ++k)
+                snap_put(w, x, w->z0 + k * w->dz, 1.e3 * w->data[(i + w->npl) * w->nz2 + k + w->np]);
+        }
+    }
+    return NULL;
+}
+
+/* write_snapshot (io_utils.c:1775-1820): "x  z  1e3*v" per node, the
+ * interior or with plot_strips the whole padded grid; the columns are
+ * formatted on host threads and written in order */
 static int write_snapshot_grid(const char *base, size_t n, double t, const double *data,
                                size_t nx2, size_t nz2, size_t npl, size_t npr, size_t np,
                                double dx, double dz, double x0, double z0, int plot_strips)
@@ -895,23 +943,29 @@ static int write_snapshot_grid(const char *base, size_t n, double t, const doubl
     snprintf(name, sizeof name, "ssh/%s/%s_%zu_%lf.ssh", base, base, n, t);
     FILE *f = fopen(name, "w");
     if (!f) return sm_fail(SM_EIO, "cannot open %s for output (%s)", name, strerror(errno));
+    const size_t ncol = plot_strips ? nx2 : (nx2 > npl + npr ? nx2 - npl - npr : 0);
+    long ncpu = sysconf(_SC_NPROCESSORS_ONLN);
+    size_t nt = ncol * nz2 < ((size_t)1 << 16) || ncpu < 2 ? 1 : (size_t)ncpu;
+    if (nt > 16) nt = 16;
+    if (nt > ncol) nt = ncol ? ncol : 1;
+    snap_part w[16];
+    pthread_t tid[16];
+    int started[16] = {0};
+    for (size_t k = 0; k < nt; ++k) {
+        w[k] = (snap_part){data, nx2, nz2, npl, npr, np, ncol * k / nt, ncol * (k + 1) / nt,
+                           dx, dz, x0, z0, plot_strips, NULL, 0, 0, 0};
+        if (k > 0) started[k] = pthread_create(&tid[k], NULL, snap_format, &w[k]) == 0;
+    }
+    snap_format(&w[0]);
+    for (size_t k = 1; k < nt; ++k) {
+        if (started[k]) pthread_join(tid[k], NULL);
+        else snap_format(&w[k]);
+    }
     int ok = 1;
-    if (plot_strips) {
-        for (size_t i = 0; i < nx2 && ok; ++i) {
-            const double x = x0 + ((double)i - (double)npl) * dx;
-            for (size_t k = 0; k < nz2 && ok; ++k) {
-                const double z = z0 + ((double)k - (double)np) * dz;
-                ok = fprintf(f, "%le  %le  %le\n", x, z, 1.e3 * data[i * nz2 + k]) > 0;
-            }
-        }
-    } else {
-        for (size_t i = 0; i + npl + npr < nx2 && ok; ++i) {
-            const double x = x0 + i * dx;
-            for (size_t k = 0; k + 2 * np < nz2 && ok; ++k) {
-                const double z = z0 + k * dz;
-                ok = fprintf(f, "%le  %le  %le\n", x, z, 1.e3 * data[(i + npl) * nz2 + k + np]) > 0;
-            }
-        }
+    for (size_t k = 0; k < nt; ++k) {
+        if (w[k].bad) ok = 0;
+        if (ok && w[k].len && fwrite(w[k].buf, 1, w[k].len, f) != w[k].len) ok = 0;
+        free(w[k].buf);
     }
     if (fclose(f) != 0) ok = 0;
     return ok ? SM_OK : sm_fail(SM_EIO, "write error on %s", name);
