@@ -16,8 +16,6 @@
 #include <string.h>
 #include <sys/stat.h>
 #include <sys/types.h>
-#include <pthread.h>
-#include <unistd.h>
 #include <stdint.h>
 #include <time.h>
 
@@ -357,19 +355,6 @@ static void *num_convert(void *arg)
     return NULL;
 }
 
-/* run fn over the chunks, one thread each (the first on the caller) */
-static void num_run(void *(*fn)(void *), num_chunk *c, size_t nc)
-{
-    pthread_t tid[16];
-    int started[16] = {0};
-    for (size_t k = 1; k < nc; ++k) started[k] = pthread_create(&tid[k], NULL, fn, &c[k]) == 0;
-    fn(&c[0]);
-    for (size_t k = 1; k < nc; ++k) {
-        if (started[k]) pthread_join(tid[k], NULL);
-        else fn(&c[k]);
-    }
-}
-
 /* The values after a model header, nf per cell: ncol cells (the first
  * column or row: the profile shortcut) when no number follows them, else all
  * n cells.  *is1d tells which.  Returns 0, or -1 when the file holds fewer
@@ -402,10 +387,8 @@ static int read_values(FILE *fid, size_t ncol, size_t n, int nf, double *const *
         cap *= 2;
     }
     buf[len] = 0;
-    long ncpu = sysconf(_SC_NPROCESSORS_ONLN);
-    size_t nc = len < ((size_t)1 << 20) || ncpu < 2 ? 1 : (size_t)ncpu;
-    if (nc > 16) nc = 16;
-    num_chunk c[16];
+    const size_t nc = sm_host_threads(len, (size_t)1 << 20);
+    num_chunk c[SM_MAX_HOST_THREADS];
     const char *start = buf;
     for (size_t k = 0; k < nc; ++k) {
         const char *e = k + 1 == nc ? buf + len : buf + len * (k + 1) / nc;
@@ -415,7 +398,7 @@ static int read_values(FILE *fid, size_t ncol, size_t n, int nf, double *const *
         c[k].e = e;
         start = e;
     }
-    num_run(num_count, c, nc);
+    sm_parallel(num_count, c, sizeof c[0], nc);
     size_t ntok = 0;
     for (size_t k = 0; k < nc; ++k) {
         c[k].first = ntok;
@@ -450,7 +433,7 @@ static int read_values(FILE *fid, size_t ncol, size_t n, int nf, double *const *
         c[k].tnz = tnz;
         for (int fl = 0; fl < 3; ++fl) c[k].v[fl] = fl < nf ? v[fl] : NULL;
     }
-    num_run(num_convert, c, nc);
+    sm_parallel(num_convert, c, sizeof c[0], nc);
     rc = 0;
     for (size_t k = 0; k < nc; ++k)
         if (c[k].bad != (size_t)-1) rc = -1;
@@ -746,22 +729,12 @@ int sm_write_trace_set(const char *base, size_t nrec, const size_t *recno, const
     if ((rc = ensure_dir("trc"))) return rc;
     snprintf(path, sizeof path, "trc/%s", base);
     if ((rc = ensure_dir(path))) return rc;
-    long ncpu = sysconf(_SC_NPROCESSORS_ONLN);
-    size_t nt = nrec < 64 || ncpu < 2 ? 1 : (size_t)ncpu;
-    if (nt > 16) nt = 16;
-    trace_part w[16];
-    pthread_t tid[16];
-    int started[16] = {0};
-    for (size_t k = 0; k < nt; ++k) {
+    const size_t nt = sm_host_threads(nrec, 64);
+    trace_part w[SM_MAX_HOST_THREADS];
+    for (size_t k = 0; k < nt; ++k)
         w[k] = (trace_part){base, recno, counts, t0, rdt, vals, dt, nsteps, ld,
                             nrec * k / nt, nrec * (k + 1) / nt, SM_OK, {0}};
-        if (k > 0) started[k] = pthread_create(&tid[k], NULL, trace_files, &w[k]) == 0;
-    }
-    trace_files(&w[0]);
-    for (size_t k = 1; k < nt; ++k) {
-        if (started[k]) pthread_join(tid[k], NULL);
-        else trace_files(&w[k]);
-    }
+    sm_parallel(trace_files, w, sizeof w[0], nt);
     for (size_t k = 0; k < nt; ++k)   /* the first failure in receiver order */
         if (w[k].rc) return sm_fail(w[k].rc, "%s", w[k].msg);
     return SM_OK;
@@ -944,23 +917,13 @@ static int write_snapshot_grid(const char *base, size_t n, double t, const doubl
     FILE *f = fopen(name, "w");
     if (!f) return sm_fail(SM_EIO, "cannot open %s for output (%s)", name, strerror(errno));
     const size_t ncol = plot_strips ? nx2 : (nx2 > npl + npr ? nx2 - npl - npr : 0);
-    long ncpu = sysconf(_SC_NPROCESSORS_ONLN);
-    size_t nt = ncol * nz2 < ((size_t)1 << 16) || ncpu < 2 ? 1 : (size_t)ncpu;
-    if (nt > 16) nt = 16;
+    size_t nt = sm_host_threads(ncol * nz2, (size_t)1 << 16);
     if (nt > ncol) nt = ncol ? ncol : 1;
-    snap_part w[16];
-    pthread_t tid[16];
-    int started[16] = {0};
-    for (size_t k = 0; k < nt; ++k) {
+    snap_part w[SM_MAX_HOST_THREADS];
+    for (size_t k = 0; k < nt; ++k)
         w[k] = (snap_part){data, nx2, nz2, npl, npr, np, ncol * k / nt, ncol * (k + 1) / nt,
                            dx, dz, x0, z0, plot_strips, NULL, 0, 0, 0};
-        if (k > 0) started[k] = pthread_create(&tid[k], NULL, snap_format, &w[k]) == 0;
-    }
-    snap_format(&w[0]);
-    for (size_t k = 1; k < nt; ++k) {
-        if (started[k]) pthread_join(tid[k], NULL);
-        else snap_format(&w[k]);
-    }
+    sm_parallel(snap_format, w, sizeof w[0], nt);
     int ok = 1;
     for (size_t k = 0; k < nt; ++k) {
         if (w[k].bad) ok = 0;

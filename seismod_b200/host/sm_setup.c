@@ -8,10 +8,8 @@
 #include "sm_host.h"
 
 #include <math.h>
-#include <pthread.h>
 #include <stdlib.h>
 #include <string.h>
-#include <unistd.h>
 
 size_t sm_ricker_length(double f, double dt, double fac)
 {
@@ -188,23 +186,13 @@ int sm_a3d_pad_model(size_t nx, size_t ny, size_t nz, size_t np,
      * first-touch page faults included). */
     const size_t nx2 = nx + 2 * np, ny2 = ny + 2 * np, nz2 = nz + 2 * np;
     const size_t cells = nx2 * ny2 * nz2;
-    long ncpu = sysconf(_SC_NPROCESSORS_ONLN);
-    size_t nt = cells < ((size_t)1 << 20) || ncpu < 2 ? 1 : (size_t)ncpu;
-    if (nt > 16) nt = 16;
+    size_t nt = sm_host_threads(cells, (size_t)1 << 20);
     if (nt > nx2) nt = nx2;
-    struct a3d_pad_part part[16];
-    pthread_t tid[16];
-    int started[16] = {0};
-    for (size_t t = 0; t < nt; ++t) {
+    struct a3d_pad_part part[SM_MAX_HOST_THREADS];
+    for (size_t t = 0; t < nt; ++t)
         part[t] = (struct a3d_pad_part){nx, ny, nz, np, nx2 * t / nt, nx2 * (t + 1) / nt,
                                         vp, rho, vp_pad, rho_pad};
-        if (t > 0) started[t] = pthread_create(&tid[t], NULL, a3d_pad_planes, &part[t]) == 0;
-    }
-    a3d_pad_planes(&part[0]);
-    for (size_t t = 1; t < nt; ++t) {
-        if (started[t]) pthread_join(tid[t], NULL);
-        else a3d_pad_planes(&part[t]);   /* no thread: do its share here */
-    }
+    sm_parallel(a3d_pad_planes, part, sizeof part[0], nt);
     return SM_OK;
 }
 
