@@ -470,7 +470,9 @@ int sm_server_struct_sizes(size_t *eiso_request, size_t *a3d_request, size_t *st
  * sm_eiso_create / sm_eiso_run / sm_eiso_read_traces on the same request.
  *   r:       the shot, as for sm_server_submit_eiso (nshots = 1)
  *   stream:  cudaStream_t to run on (NULL: the legacy default stream); the
- *            call returns when the run is done and the traces are copied
+ *            call synchronizes this stream (after the uploads and again at
+ *            the end) and returns when the run is done and the traces are
+ *            copied
  *   traces:  nrec rows of ld doubles (may be NULL to learn the counts),
  *            counts: samples per receiver (required when nrec > 0)
  * The first call on a device looks up the array's device address (once per

@@ -1461,6 +1461,96 @@ size_t pml_index_host(const sm_eiso *h, size_t X, size_t Z) {
     return (size_t)h->args.mid_off + (X - np) * 2 * np + (Z < np ? Z : Z - h->nz);
 }
 
+// ---- host set-up shared by sm_eiso_create and sm_eiso_run_noalloc ----
+
+// Material k (M_B, M_BM, M_LA, M_L2M, M_MU; src is the reference's [nx][nz]
+// array of it) on the padded grid of (nx + 2 np) rows of `pitch` values,
+// edge replicated and multiplied by `scale` (dt/h); the pitch padding is 0.
+// pml.c reads the interior's edge values in the frame; for lambda and
+// lambda+2mu in the lower-right corner it reads [nx*nx-1]
+// (pml.c:1044-1084).  That index is kept while it lies inside the array
+// (nx <= nz) and replaced by the intended [nx*nz-1] otherwise.
+void eiso_pad_material(size_t nx, size_t nz, size_t np, size_t pitch, double scale,
+                       const double *src, int k, double *m) {
+    const size_t NX = nx + 2 * np, NZ = nz + 2 * np;
+    size_t lr = nx * nx - 1;
+    if (lr >= nx * nz) lr = nx * nz - 1;
+    for (size_t X = 0; X < NX; ++X) {
+        const size_t i = X < np ? 0 : (X - np >= nx ? nx - 1 : X - np);
+        double *row = m + X * pitch;
+        for (size_t Z = 0; Z < NZ; ++Z) {
+            const size_t j = Z < np ? 0 : (Z - np >= nz ? nz - 1 : Z - np);
+            size_t idx = i * nz + j;
+            if ((k == M_LA || k == M_L2M) && X >= np + nx && Z >= np + nz) idx = lr;
+            row[Z] = scale * src[idx];
+        }
+        for (size_t Z = NZ; Z < pitch; ++Z) row[Z] = 0.0;
+    }
+}
+
+// The damping tables of the split-field PML in the EisoProf layout:
+// A = (2 - dt d)/(2 + dt d), B = 2/(2 + dt d) per node and half node of each
+// axis, from the reference's profiles d (nodes), dh (half nodes, start side)
+// and dH (half nodes, end side) read reversed on the far side; A = B = 1
+// outside the frame (e_iso.c:482-500, pml.c:39-1403).
+std::vector<double> eiso_damping_tables(size_t nx, size_t nz, size_t np, double dt,
+                                        const double *d, const double *dh, const double *dH) {
+    const size_t NX = nx + 2 * np, NZ = nz + 2 * np;
+    const EisoProf P{(int)NX, (int)NZ};
+    std::vector<double> t((size_t)P.size(), 1.0);
+    auto fill = [&](int aoff, int boff, size_t n, size_t ncell, bool half) {
+        for (size_t X = 0; X < n; ++X) {
+            double dd = -1.0;
+            if (X < np) dd = half ? dh[X] : d[X];
+            else if (X >= np + ncell) {
+                const size_t i = X - np - ncell;
+                dd = half ? dH[np - 1 - i] : d[np - 1 - i];
+            }
+            if (dd >= 0.0) {
+                t[aoff + X] = (2. - dt * dd) / (2. + dt * dd);
+                t[boff + X] = 2. / (2. + dt * dd);
+            }
+        }
+    };
+    fill(P.axn(), P.bxn(), NX, nx, false);
+    fill(P.axh(), P.bxh(), NX, nx, true);
+    fill(P.azn(), P.bzn(), NZ, nz, false);
+    fill(P.azh(), P.bzh(), NZ, nz, true);
+    return t;
+}
+
+// One source at the reference's cell index (i*nz + j) as a padded-grid entry
+// with its samples (scale * fct) appended to vals; `who` names the caller in
+// the error message.
+int eiso_source_entry(size_t nx, size_t nz, size_t np, size_t pitch, size_t index, int type,
+                      const double *fct, size_t length, size_t stride, double scale,
+                      const char *who, SrcEntry *e, std::vector<double> &vals) {
+    if (index >= nx * nz) return sm_fail(SM_EINVAL, "%s: source outside the grid", who);
+    if (type != SM_SRC_SX && type != SM_SRC_SZ && type != SM_SRC_SXZ && type != SM_SRC_BULK)
+        return sm_fail(SM_EINVAL, "%s: source type %d not supported", who, type);
+    if (length > stride) return sm_fail(SM_EINVAL, "%s: source length exceeds stride", who);
+    *e = SrcEntry{};
+    e->q = (long long)(index / nz + np) * (long long)pitch + (long long)(index % nz + np);
+    e->type = type;
+    e->voff = (long long)vals.size();
+    e->len = (int)length;
+    for (size_t k = 0; k < length; ++k) vals.push_back(scale * fct[k]);
+    return SM_OK;
+}
+
+// One receiver at the reference's cell index as a padded-grid entry.
+int eiso_receiver_entry(size_t nx, size_t nz, size_t np, size_t pitch, size_t index, int comp,
+                        int group, const char *who, RecEntry *e) {
+    if (index >= nx * nz) return sm_fail(SM_EINVAL, "%s: receiver outside the grid", who);
+    const int f = field_id(comp);
+    if (f < 0) return sm_fail(SM_EINVAL, "%s: component %d not recorded by e_iso", who, comp);
+    *e = RecEntry{};
+    e->q = (long long)(index / nz + np) * (long long)pitch + (long long)(index % nz + np);
+    e->field = f;
+    e->group = group;
+    return SM_OK;
+}
+
 }  // namespace
 
 // 2 MB rounding of each large array (the allocation granularity)
@@ -1548,27 +1638,11 @@ extern "C" int sm_eiso_create(int device, size_t nx, size_t nz, size_t npml, dou
     if ((rc = h->d_step.zero(h->stream))) return rc;
 
     // ---- materials on the padded grid: edge replicated, scaled by dt/h ----
-    // pml.c reads the interior's edge values in the frame; for lambda and
-    // lambda+2mu in the lower-right corner it reads [nx*nx-1]
-    // (pml.c:1044-1084).  That index is kept while it lies inside the array
-    // (nx <= nz) and replaced by the intended [nx*nz-1] otherwise.
     {
         const double *src[5] = {b, bm, la, l2m, mu};
         std::vector<double> m(fcells, 0.0);
-        const double s = dt / hh;
-        size_t lr = nx * nx - 1;
-        if (lr >= nx * nz) lr = nx * nz - 1;
         for (int k = 0; k < 5; ++k) {
-            std::fill(m.begin(), m.end(), 0.0);
-            for (size_t X = 0; X < NX; ++X) {
-                size_t i = X < npml ? 0 : (X - npml >= nx ? nx - 1 : X - npml);
-                for (size_t Z = 0; Z < NZ; ++Z) {
-                    size_t j = Z < npml ? 0 : (Z - npml >= nz ? nz - 1 : Z - npml);
-                    size_t idx = i * nz + j;
-                    if ((k == M_LA || k == M_L2M) && X >= npml + nx && Z >= npml + nz) idx = lr;
-                    m[X * h->pitch + Z] = s * src[k][idx];
-                }
-            }
+            eiso_pad_material(nx, nz, npml, (size_t)h->pitch, dt / hh, src[k], k, m.data());
             rc = precision == SM_FP64 ? upload_convert<double>(h->mat(k), m.data(), fcells, h->stream)
                                       : upload_convert<float>(h->mat(k), m.data(), fcells, h->stream);
             if (rc) return rc;
@@ -1576,25 +1650,7 @@ extern "C" int sm_eiso_create(int device, size_t nx, size_t nz, size_t npml, dou
     }
     // ---- damping tables: A = (2 - dt d)/(2 + dt d), B = 2/(2 + dt d) ----
     {
-        std::vector<double> t((size_t)P.size(), 1.0);
-        auto fill = [&](int aoff, int boff, size_t n, size_t ncell, bool half) {
-            for (size_t X = 0; X < n; ++X) {
-                double dd = -1.0;
-                if (X < npml) dd = half ? dh[X] : d[X];
-                else if (X >= npml + ncell) {
-                    size_t i = X - npml - ncell;
-                    dd = half ? dH[npml - 1 - i] : d[npml - 1 - i];
-                }
-                if (dd >= 0.0) {
-                    t[aoff + X] = (2. - dt * dd) / (2. + dt * dd);
-                    t[boff + X] = 2. / (2. + dt * dd);
-                }
-            }
-        };
-        fill(P.axn(), P.bxn(), NX, nx, false);
-        fill(P.axh(), P.bxh(), NX, nx, true);
-        fill(P.azn(), P.bzn(), NZ, nz, false);
-        fill(P.azh(), P.bzh(), NZ, nz, true);
+        const std::vector<double> t = eiso_damping_tables(nx, nz, npml, dt, d, dh, dH);
         rc = precision == SM_FP64 ? upload_convert<double>(h->prof.p, t.data(), t.size(), h->stream)
                                   : upload_convert<float>(h->prof.p, t.data(), t.size(), h->stream);
         if (rc) return rc;
@@ -1674,20 +1730,11 @@ extern "C" int sm_eiso_set_sources(sm_eiso_t h, size_t shot, size_t nsrc, const 
     std::vector<SrcEntry> e;
     std::vector<double> vals;
     for (size_t s = 0; s < nsrc; ++s) {
-        if (index[s] >= h->nx * h->nz)
-            return sm_fail(SM_EINVAL, "sm_eiso_set_sources: source %zu outside the grid", s);
-        int t = type[s];
-        if (t != SM_SRC_SX && t != SM_SRC_SZ && t != SM_SRC_SXZ && t != SM_SRC_BULK)
-            return sm_fail(SM_EINVAL, "sm_eiso_set_sources: source type %d not supported", t);
-        if (length[s] > stride)
-            return sm_fail(SM_EINVAL, "sm_eiso_set_sources: length exceeds stride");
-        size_t i = index[s] / h->nz, j = index[s] % h->nz;
-        SrcEntry se{};
-        se.q = (long long)(i + h->np) * h->pitch + (long long)(j + h->np);
-        se.type = t;
-        se.voff = (long long)vals.size();
-        se.len = (int)length[s];
-        for (size_t k = 0; k < length[s]; ++k) vals.push_back(scale * fct[s * stride + k]);
+        SrcEntry se;
+        if (int rc = eiso_source_entry(h->nx, h->nz, h->np, (size_t)h->pitch, index[s], type[s],
+                                       fct + s * stride, length[s], stride, scale,
+                                       "sm_eiso_set_sources", &se, vals))
+            return rc;
         e.push_back(se);
     }
     for (size_t s = 0; s < h->nshots; ++s) {
@@ -1732,17 +1779,10 @@ extern "C" int sm_eiso_set_receivers(sm_eiso_t h, size_t shot, size_t nrec, cons
     ShotRecs sr;
     sr.plan.build(nrec, t0, rdt, h->dt, nsteps_max);
     for (size_t r = 0; r < nrec; ++r) {
-        if (index[r] >= h->nx * h->nz)
-            return sm_fail(SM_EINVAL, "sm_eiso_set_receivers: receiver %zu outside the grid", r);
-        int f = field_id(comp[r]);
-        if (f < 0)
-            return sm_fail(SM_EINVAL, "sm_eiso_set_receivers: component %d not recorded by e_iso",
-                           comp[r]);
-        size_t i = index[r] / h->nz, j = index[r] % h->nz;
-        RecEntry e{};
-        e.q = (long long)(i + h->np) * h->pitch + (long long)(j + h->np);
-        e.field = f;
-        e.group = sr.plan.group_of[r];
+        RecEntry e;
+        if (int rc = eiso_receiver_entry(h->nx, h->nz, h->np, (size_t)h->pitch, index[r], comp[r],
+                                         sr.plan.group_of[r], "sm_eiso_set_receivers", &e))
+            return rc;
         sr.entries.push_back(e);
     }
     for (size_t s = 0; s < h->nshots; ++s) {
@@ -2414,6 +2454,9 @@ extern "C" int sm_eiso_run_noalloc(int device, void *stream, const sm_eiso_reque
                                    double *traces, size_t ld, size_t *counts) {
     using S = float;
     using L = ETile<S, 8, 32>;
+    // launched without raising the kernel's dynamic shared-memory limit, so
+    // its tile must stay within the default 48 KB
+    static_assert(L::bytes <= 48 * 1024, "noalloc tile needs an opt-in shared-memory size");
     if (!r) return sm_fail(SM_EINVAL, "sm_eiso_run_noalloc: request is NULL");
     const sm_eiso_request &q = *r;
     if (q.precision != SM_FP32)
@@ -2438,38 +2481,23 @@ extern "C" int sm_eiso_run_noalloc(int device, void *stream, const sm_eiso_reque
     std::vector<SrcEntry> src;
     std::vector<double> vals;
     for (size_t s = 0; s < q.nsrc; ++s) {
-        const int t = q.src_type[s];
-        if (q.src_index[s] >= nx * nz)
-            return sm_fail(SM_EINVAL, "sm_eiso_run_noalloc: source %zu outside the grid", s);
-        if (t != SM_SRC_SX && t != SM_SRC_SZ && t != SM_SRC_SXZ && t != SM_SRC_BULK)
-            return sm_fail(SM_EINVAL, "sm_eiso_run_noalloc: source type %d not supported", t);
-        if (q.src_length[s] > q.src_stride)
-            return sm_fail(SM_EINVAL, "sm_eiso_run_noalloc: source length exceeds stride");
-        SrcEntry e{};
-        e.q = (long long)(q.src_index[s] / nz + np) * (long long)pitch +
-              (long long)(q.src_index[s] % nz + np);
+        SrcEntry e;
+        if (int rc = eiso_source_entry(nx, nz, np, pitch, q.src_index[s], q.src_type[s],
+                                       q.src_fct + s * q.src_stride, q.src_length[s],
+                                       q.src_stride, q.src_scale, "sm_eiso_run_noalloc", &e, vals))
+            return rc;
         e.shot = 0;
-        e.type = t;
-        e.voff = (long long)vals.size();
-        e.len = (int)q.src_length[s];
-        for (size_t k = 0; k < q.src_length[s]; ++k)
-            vals.push_back(q.src_scale * q.src_fct[s * q.src_stride + k]);
         src.push_back(e);
     }
     SamplePlan plan;
     plan.build(q.nrec, q.rec_t0, q.rec_dt, q.dt, q.nsteps);
     std::vector<RecEntry> rec;
     for (size_t k = 0; k < q.nrec; ++k) {
-        const int f = field_id(q.rec_comp[k]);
-        if (q.rec_index[k] >= nx * nz || f < 0)
-            return sm_fail(SM_EINVAL, "sm_eiso_run_noalloc: receiver %zu outside the grid or "
-                                      "not an e_iso component", k);
-        RecEntry e{};
-        e.q = (long long)(q.rec_index[k] / nz + np) * (long long)pitch +
-              (long long)(q.rec_index[k] % nz + np);
+        RecEntry e;
+        if (int rc = eiso_receiver_entry(nx, nz, np, pitch, q.rec_index[k], q.rec_comp[k],
+                                         plan.group_of[k], "sm_eiso_run_noalloc", &e))
+            return rc;
         e.shot = 0;
-        e.field = f;
-        e.group = plan.group_of[k];
         e.out = (long long)k * (long long)plan.max_samples;
         rec.push_back(e);
     }
@@ -2515,42 +2543,12 @@ extern "C" int sm_eiso_run_noalloc(int device, void *stream, const sm_eiso_reque
     {
         const double *m5[5] = {q.b, q.bm, q.la, q.l2m, q.mu};
         std::vector<double> m(fcells, 0.0);
-        const double s = q.dt / q.h;
-        size_t lr = nx * nx - 1;   // pml.c:1044-1084, kept while inside the array
-        if (lr >= nx * nz) lr = nx * nz - 1;
         for (int k = 0; k < 5; ++k) {
-            std::fill(m.begin(), m.end(), 0.0);
-            for (size_t X = 0; X < NX; ++X) {
-                const size_t i = X < np ? 0 : (X - np >= nx ? nx - 1 : X - np);
-                for (size_t Z = 0; Z < NZ; ++Z) {
-                    const size_t j = Z < np ? 0 : (Z - np >= nz ? nz - 1 : Z - np);
-                    size_t idx = i * nz + j;
-                    if ((k == M_LA || k == M_L2M) && X >= np + nx && Z >= np + nz) idx = lr;
-                    m[X * pitch + Z] = s * m5[k][idx];
-                }
-            }
+            eiso_pad_material(nx, nz, np, pitch, q.dt / q.h, m5[k], k, m.data());
             if (int rc = upload_convert<S>(base + o_mat + k * fcells * sizeof(S), m.data(), fcells, st))
                 return rc;
         }
-        std::vector<double> t((size_t)P.size(), 1.0);
-        auto fill = [&](int aoff, int boff, size_t n, size_t ncell, bool half) {
-            for (size_t X = 0; X < n; ++X) {
-                double dd = -1.0;
-                if (X < np) dd = half ? q.dh[X] : q.d[X];
-                else if (X >= np + ncell) {
-                    const size_t i = X - np - ncell;
-                    dd = half ? q.dH[np - 1 - i] : q.d[np - 1 - i];
-                }
-                if (dd >= 0.0) {
-                    t[aoff + X] = (2. - q.dt * dd) / (2. + q.dt * dd);
-                    t[boff + X] = 2. / (2. + q.dt * dd);
-                }
-            }
-        };
-        fill(P.axn(), P.bxn(), NX, nx, false);
-        fill(P.axh(), P.bxh(), NX, nx, true);
-        fill(P.azn(), P.bzn(), NZ, nz, false);
-        fill(P.azh(), P.bzh(), NZ, nz, true);
+        const std::vector<double> t = eiso_damping_tables(nx, nz, np, q.dt, q.d, q.dh, q.dH);
         if (int rc = upload_convert<S>(base + o_prof, t.data(), t.size(), st)) return rc;
     }
     const int first[2] = {0, (int)src.size()};

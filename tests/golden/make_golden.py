@@ -1,7 +1,7 @@
 """Generate the golden trace fixtures from the reference programs.
 
 Run in a container where the reference sources are present, after
-``make -C oracle`` has built oracle/_ref/:
+``make -C oracle REF=<reference source tree>`` has built oracle/_ref/:
 
     python tests/golden/make_golden.py          # every fixture
     python tests/golden/make_golden.py ecyl     # the e_cyl_iso ones only
