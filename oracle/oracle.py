@@ -77,6 +77,8 @@ def _load():
     lib.orc_a3d_pressure.argtypes = [C.c_void_p]
     lib.orc_a3d_add_source.argtypes = [C.c_void_p, _sz, C.c_double]
     lib.orc_a3d_get.argtypes = [C.c_void_p, C.c_int, _dp]
+    lib.orc_a3d_gather.argtypes = [C.c_void_p, _sz, C.POINTER(C.c_int), C.POINTER(_sz), _dp]
+    lib.orc_a3d_set_bfp.argtypes = [C.c_void_p, C.c_int]
     lib.orc_a3d_set.argtypes = [C.c_void_p, C.c_int, _dp]
     lib.orc_a3d_probe.restype = C.c_double
     lib.orc_a3d_probe.argtypes = [C.c_void_p, C.c_int, _sz]
@@ -270,6 +272,20 @@ class A3D:
 
     def probe(self, field, index):
         return lib().orc_a3d_probe(self.h_, FIELDS_A[field], int(index))
+
+    def gather(self, fields, index):
+        """values of fields[r] at index[r] (arrays of field ids and indices)"""
+        f = np.ascontiguousarray(fields, dtype=np.int32)
+        q = np.ascontiguousarray(index, dtype=np.uintp)
+        out = np.zeros(len(q))
+        lib().orc_a3d_gather(self.h_, len(q), f.ctypes.data_as(C.POINTER(C.c_int)),
+                             q.ctypes.data_as(C.POINTER(_sz)), _ptr(out))
+        return out
+
+    def set_bfp(self, block):
+        """checker mode: round every stored value to 16-bit block floating
+        point with blocks of `block` z cells (0: FP64 storage)"""
+        lib().orc_a3d_set_bfp(self.h_, int(block))
 
 
 # ----------------------------------------------------------------------------

@@ -9,8 +9,65 @@
 #include "seismod_oracle.h"
 
 #include <math.h>
+#include <pthread.h>
 #include <stdlib.h>
 #include <string.h>
+#include <unistd.h>
+
+/* ======================================================================
+ * loops over independent planes split across host threads (the a_iso_3d
+ * sweeps at full grid sizes).  Every cell is still computed by the same
+ * expression in the same order, so the results do not depend on the
+ * thread count.  ORC_THREADS sets the count (default: online cores, <= 64).
+ * ====================================================================== */
+
+typedef void (*orc_range_fn)(void *ctx, size_t lo, size_t hi);
+
+struct orc_job {
+    orc_range_fn fn;
+    void *ctx;
+    size_t lo, hi;
+};
+
+static void *orc_job_run(void *p)
+{
+    struct orc_job *j = p;
+    j->fn(j->ctx, j->lo, j->hi);
+    return NULL;
+}
+
+static int orc_threads(void)
+{
+    const char *e = getenv("ORC_THREADS");
+    long n = e ? atol(e) : sysconf(_SC_NPROCESSORS_ONLN);
+    if (n < 1) n = 1;
+    if (n > 64) n = 64;
+    return (int)n;
+}
+
+static void orc_parallel(size_t n, orc_range_fn fn, void *ctx)
+{
+    int nt = orc_threads();
+    if ((size_t)nt > n) nt = (int)n;
+    if (nt <= 1) {
+        fn(ctx, 0, n);
+        return;
+    }
+    pthread_t th[64];
+    struct orc_job jobs[64];
+    int started[64];
+    for (int t = 0; t < nt; ++t) {
+        jobs[t].fn = fn;
+        jobs[t].ctx = ctx;
+        jobs[t].lo = n * (size_t)t / (size_t)nt;
+        jobs[t].hi = n * (size_t)(t + 1) / (size_t)nt;
+        started[t] = t > 0 && pthread_create(&th[t], NULL, orc_job_run, &jobs[t]) == 0;
+        if (t > 0 && !started[t]) fn(ctx, jobs[t].lo, jobs[t].hi);
+    }
+    fn(ctx, jobs[0].lo, jobs[0].hi);
+    for (int t = 1; t < nt; ++t)
+        if (started[t]) pthread_join(th[t], NULL);
+}
 
 /* ======================================================================
  * shared set-up
@@ -449,6 +506,7 @@ struct orc_a3d {
     double *mPx, *mPy, *mPz, *mvx, *mvy, *mvz;
     double *irx, *iry, *irz, *K;
     double *coef[18];
+    int bfp_block;   /* 0: FP64 storage; else block floating point, see below */
 };
 
 orc_a3d *orc_a3d_new(size_t nx2, size_t ny2, size_t nz2, double dx, double dy, double dz,
@@ -501,14 +559,13 @@ void orc_a3d_free(orc_a3d *o)
     free(o);
 }
 
-void orc_a3d_velocity(orc_a3d *o)
+/* a_iso_3d.c:605-617: vx on i < nx2-1 */
+static void a3d_vx(void *ctx, size_t i0, size_t i1)
 {
-    size_t nx2 = o->nx2, ny2 = o->ny2, nz2 = o->nz2;
+    orc_a3d *o = ctx;
+    size_t ny2 = o->ny2, nz2 = o->nz2;
     const double *ax_h = o->coef[9], *bx_h = o->coef[10], *kx_h = o->coef[11];
-    const double *ay_h = o->coef[12], *by_h = o->coef[13], *ky_h = o->coef[14];
-    const double *az_h = o->coef[15], *bz_h = o->coef[16], *kz_h = o->coef[17];
-    /* a_iso_3d.c:605-617: vx on i < nx2-1 */
-    for (size_t i = 0; i + 1 < nx2; ++i)
+    for (size_t i = i0; i < i1; ++i)
         for (size_t j = 0; j < ny2; ++j)
             for (size_t k = 0; k < nz2; ++k) {
                 size_t a = (i * ny2 + j) * nz2 + k, b = ((i + 1) * ny2 + j) * nz2 + k;
@@ -517,8 +574,15 @@ void orc_a3d_velocity(orc_a3d *o)
                 g = g / kx_h[i] + o->mPx[a];
                 o->vx[a] -= o->irx[a] * g;
             }
-    /* a_iso_3d.c:620-634: vy on j < ny2-1 */
-    for (size_t i = 0; i < nx2; ++i)
+}
+
+/* a_iso_3d.c:620-634: vy on j < ny2-1 */
+static void a3d_vy(void *ctx, size_t i0, size_t i1)
+{
+    orc_a3d *o = ctx;
+    size_t ny2 = o->ny2, nz2 = o->nz2;
+    const double *ay_h = o->coef[12], *by_h = o->coef[13], *ky_h = o->coef[14];
+    for (size_t i = i0; i < i1; ++i)
         for (size_t j = 0; j + 1 < ny2; ++j)
             for (size_t k = 0; k < nz2; ++k) {
                 size_t a = (i * ny2 + j) * nz2 + k, b = (i * ny2 + j + 1) * nz2 + k;
@@ -527,8 +591,15 @@ void orc_a3d_velocity(orc_a3d *o)
                 g = g / ky_h[j] + o->mPy[a];
                 o->vy[a] -= o->iry[a] * g;
             }
-    /* a_iso_3d.c:637-651: vz on k < nz2-1 */
-    for (size_t i = 0; i < nx2; ++i)
+}
+
+/* a_iso_3d.c:637-651: vz on k < nz2-1 */
+static void a3d_vz(void *ctx, size_t i0, size_t i1)
+{
+    orc_a3d *o = ctx;
+    size_t ny2 = o->ny2, nz2 = o->nz2;
+    const double *az_h = o->coef[15], *bz_h = o->coef[16], *kz_h = o->coef[17];
+    for (size_t i = i0; i < i1; ++i)
         for (size_t j = 0; j < ny2; ++j)
             for (size_t k = 0; k + 1 < nz2; ++k) {
                 size_t a = (i * ny2 + j) * nz2 + k;
@@ -539,14 +610,15 @@ void orc_a3d_velocity(orc_a3d *o)
             }
 }
 
-void orc_a3d_pressure(orc_a3d *o)
+/* a_iso_3d.c:659-683: i, j, k >= 1 (plane 0 is never updated) */
+static void a3d_p(void *ctx, size_t i0, size_t i1)
 {
-    /* a_iso_3d.c:659-683: i, j, k >= 1 (plane 0 is never updated) */
-    size_t nx2 = o->nx2, ny2 = o->ny2, nz2 = o->nz2;
+    orc_a3d *o = ctx;
+    size_t ny2 = o->ny2, nz2 = o->nz2;
     const double *ax = o->coef[0], *bx = o->coef[1], *kx = o->coef[2];
     const double *ay = o->coef[3], *by = o->coef[4], *ky = o->coef[5];
     const double *az = o->coef[6], *bz = o->coef[7], *kz = o->coef[8];
-    for (size_t i = 1; i < nx2; ++i)
+    for (size_t i = i0 > 1 ? i0 : 1; i < i1; ++i)
         for (size_t j = 1; j < ny2; ++j)
             for (size_t k = 1; k < nz2; ++k) {
                 size_t a = (i * ny2 + j) * nz2 + k;
@@ -565,9 +637,98 @@ void orc_a3d_pressure(orc_a3d *o)
             }
 }
 
+/* ----------------------------------------------------------------------
+ * Storage rounding (a checker mode with no counterpart in the reference):
+ * the state a step leaves behind (P and the three velocities) is replaced
+ * by the values 16-bit block floating point storage keeps, as the device's
+ * block storage does: the pressure update of a step reads the velocities
+ * that step computed, unrounded, and the state is rounded once when the
+ * step stores it; a source added afterwards re-rounds the block of its cell.
+ * A block is B consecutive z cells of one (i, j) row starting at a multiple
+ * of B; its values share the exponent E of the block's largest magnitude M
+ * (M in [2^(E-1), 2^E)), and each is kept as the integer
+ * m = round_half_even(x 2^(15-E)), at most 32767 (15 bits and a sign),
+ * i.e. x ~ m 2^(E-15); E is held in [-111, 114] as the device's 8-bit
+ * exponent holds it.  The step arithmetic stays FP64, so the difference
+ * from the plain oracle is the storage format's own error.  The CPML memory
+ * variables keep FP64 (the device keeps them in FP32).
+ * ---------------------------------------------------------------------- */
+static void bfp_round_block(double *row, size_t k0, size_t k1)
+{
+    double mx = 0.0;
+    for (size_t k = k0; k < k1; ++k) mx = fabs(row[k]) > mx ? fabs(row[k]) : mx;
+    if (mx == 0.0 || !isfinite(mx)) return;
+    int E;
+    frexp(mx, &E);   /* mx in [2^(E-1), 2^E) */
+    /* the exponent range of the device format (an FP32 biased exponent of
+     * the block maximum in [15, 240]): tiny blocks keep the scale 2^126 */
+    if (E < -111) E = -111;
+    if (E > 114) E = 114;
+    double sc = ldexp(1.0, 15 - E), isc = ldexp(1.0, E - 15);
+    for (size_t k = k0; k < k1; ++k) {
+        double m = nearbyint(row[k] * sc);
+        if (m > 32767.0) m = 32767.0;
+        row[k] = m * isc;
+    }
+}
+
+static void bfp_round_rows(double *f, size_t nrows, size_t n, int B)
+{
+    for (size_t r = 0; r < nrows; ++r)
+        for (size_t k0 = 0; k0 < n; k0 += (size_t)B)
+            bfp_round_block(f + r * n, k0, k0 + (size_t)B < n ? k0 + (size_t)B : n);
+}
+
+struct bfp_job {
+    double *f[3];
+    size_t plane;    /* values per x plane */
+    size_t nz2;
+    int B;
+};
+
+static void bfp_planes(void *ctx, size_t i0, size_t i1)
+{
+    struct bfp_job *j = ctx;
+    for (int a = 0; a < 3; ++a)
+        if (j->f[a])
+            bfp_round_rows(j->f[a] + i0 * j->plane, (i1 - i0) * (j->plane / j->nz2), j->nz2, j->B);
+}
+
+static void a3d_round(orc_a3d *o, double *f0, double *f1, double *f2)
+{
+    struct bfp_job j = {{f0, f1, f2}, o->ny2 * o->nz2, o->nz2, o->bfp_block};
+    orc_parallel(o->nx2, bfp_planes, &j);
+}
+
+void orc_a3d_set_bfp(orc_a3d *o, int block)
+{
+    o->bfp_block = block > 0 ? block : 0;
+}
+
+void orc_a3d_velocity(orc_a3d *o)
+{
+    orc_parallel(o->nx2 - 1, a3d_vx, o);
+    orc_parallel(o->nx2, a3d_vy, o);
+    orc_parallel(o->nx2, a3d_vz, o);
+}
+
+void orc_a3d_pressure(orc_a3d *o)
+{
+    orc_parallel(o->nx2, a3d_p, o);
+    if (o->bfp_block) {
+        a3d_round(o, o->vx, o->vy, o->vz);
+        a3d_round(o, o->P, NULL, NULL);
+    }
+}
+
 void orc_a3d_add_source(orc_a3d *o, size_t index, double value)
 {
     o->P[index] += value;
+    if (o->bfp_block) {
+        size_t B = (size_t)o->bfp_block, k = index % o->nz2, k0 = k / B * B;
+        double *row = o->P + (index - k);
+        bfp_round_block(row, k0, k0 + B < o->nz2 ? k0 + B : o->nz2);
+    }
 }
 
 static double *a3d_field(const orc_a3d *o, int field)
@@ -593,4 +754,10 @@ void orc_a3d_set(orc_a3d *o, int field, const double *in)
 double orc_a3d_probe(const orc_a3d *o, int field, size_t index)
 {
     return a3d_field(o, field)[index];
+}
+
+void orc_a3d_gather(const orc_a3d *o, size_t n, const int *field, const size_t *index,
+                    double *out)
+{
+    for (size_t r = 0; r < n; ++r) out[r] = a3d_field(o, field[r])[index[r]];
 }

@@ -111,6 +111,13 @@ void orc_a3d_add_source(orc_a3d *o, size_t index, double value); /* :689-693 */
 void orc_a3d_get(const orc_a3d *o, int field, double *out);
 void orc_a3d_set(orc_a3d *o, int field, const double *in);
 double orc_a3d_probe(const orc_a3d *o, int field, size_t index);
+/* out[r] = field[r] at index[r], r < n */
+void orc_a3d_gather(const orc_a3d *o, size_t n, const int *field, const size_t *index,
+                    double *out);
+/* storage-rounding checker mode: 0 = FP64 storage (default); B > 0 = every
+ * stored value rounded to 16-bit block floating point with blocks of B z
+ * cells (no counterpart in the reference) */
+void orc_a3d_set_bfp(orc_a3d *o, int block);
 
 /* ---------------- e_cyl_iso (oracle_ecyl.c) ---------------- */
 

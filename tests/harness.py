@@ -112,10 +112,15 @@ def a3d_index(p, x, y, z):
     return (i * ny2 + j) * nz2 + k
 
 
-def run_a3d_oracle(p, nsteps=None, fields_at=None):
+def run_a3d_oracle(p, nsteps=None, fields_at=None, bfp_block=0):
+    """FP64 oracle run of an a_iso_3d shot; bfp_block > 0 rounds every stored
+    value to 16-bit block floating point with blocks of that many z cells
+    (the storage-rounding checker mode)."""
     s = a3d_setup(p)
     n = s["nsteps"] if nsteps is None else nsteps
     o = O.A3D(s["vpp"], s["rhop"], *p.d, s["dt"], s["coef"])
+    if bfp_block:
+        o.set_bfp(bfp_block)
     A = [q[1] for q in p.sources]
     f = [q[2] for q in p.sources]
     fct = O.src_fct(A, f, p.dt, 1.0)
@@ -125,6 +130,13 @@ def run_a3d_oracle(p, nsteps=None, fields_at=None):
     tr = [[] for _ in recs]
     tt = [[] for _ in recs]
     dt = s["dt"]
+    # receivers sharing (t0, rdt) are sampled on the same steps: one gather
+    # per group and step
+    groups = {}
+    for r, (idx, comp, t0, rdt) in enumerate(recs):
+        groups.setdefault((t0, rdt), []).append(r)
+    gsel = {key: (np.array(rs), np.array([O.FIELDS_A[recs[r][1]] for r in rs]),
+                  np.array([recs[r][0] for r in rs])) for key, rs in groups.items()}
     for it in range(n):
         o.velocity()
         o.pressure()
@@ -132,10 +144,12 @@ def run_a3d_oracle(p, nsteps=None, fields_at=None):
             if it < len(w):
                 o.add_source(idx, dt * w[it] * 1.e6)
         t = dt * (it + 1)
-        for r, (idx, comp, t0, rdt) in enumerate(recs):
+        for (t0, rdt), (rs, fl, qs) in gsel.items():
             if O.sample(it, dt, t0, rdt):
-                tr[r].append(1e3 * o.probe(comp, idx))
-                tt[r].append(t)
+                vals = o.gather(fl, qs)
+                for r, v in zip(rs, vals):
+                    tr[r].append(1e3 * v)
+                    tt[r].append(t)
     fields = None
     if fields_at:
         fields = {f: o.get(f) for f in fields_at}

@@ -1,0 +1,139 @@
+"""Parity at the full sizes of the benchmark configurations.
+
+The small-grid tests pin the kernels against the FP64 oracle; these run the
+same comparisons on the grids that are benchmarked, so that the tile classes,
+the x chunking of the a_iso_3d march, the slab shapes of the e_iso step and
+the 32-bit index arithmetic are covered at scale:
+
+  a_iso_3d 256^3 (+2x16 CPML = 288^3)   random state, every field after 6 steps;
+                                        a shot of 300 steps, 16,384 receivers
+  a_iso_3d 512^3 (+2x16 CPML = 544^3)   random state, every field after 4 steps
+  e_iso 1000 x 500 (+2x20 PML), 64 shots in one batched handle: random state
+                                        of shots 0 and 63, every field and
+                                        split part after 4 steps; the shots'
+                                        traces over 400 steps
+
+FP32 storage against the FP64 oracle, relative L2 <= 1e-5 (the FP32 bound of
+the path).  The oracle sweeps run on host threads (ORC_THREADS).
+"""
+import numpy as np
+import pytest
+
+import harness as H
+from oracle import oracle as O
+from seismod_b200 import api
+from seismod_b200 import workloads as W
+
+pytestmark = pytest.mark.gpu
+
+TOL_FP32 = 1e-5
+
+
+def _a3d_random_state(p, steps, seed):
+    s = H.a3d_setup(p)
+    orc = O.A3D(s["vpp"], s["rhop"], *p.d, s["dt"], s["coef"])
+    dev = api.A3DDevice(s["vpp"], s["rhop"], p.npml, p.d, s["dt"], s["coef"], "fp32")
+    rng = np.random.default_rng(seed)
+    shp = s["vpp"].shape
+    for f, sc in (("p", 1e5), ("vx", 1e-2), ("vy", 1e-2), ("vz", 1e-2)):
+        a = (sc * rng.standard_normal(shp, dtype=np.float32)).astype(np.float64)
+        orc.set(f, a)
+        dev.set_field(f, a)
+        del a
+    for _ in range(steps):
+        orc.velocity()
+        orc.pressure()
+    dev.run(steps)
+    errs = {}
+    for f in ("p", "vx", "vy", "vz"):
+        errs[f] = O.rel_l2(dev.get_field(f), orc.get(f))
+    dev.close()
+    del orc
+    return errs
+
+
+def test_a3d_288cube_random_state_every_field():
+    p = W.cfg1()
+    errs = _a3d_random_state(p, 6, 11)
+    assert all(e < TOL_FP32 for e in errs.values()), errs
+
+
+def test_a3d_288cube_shot_surface_receivers():
+    p = W.cfg1(nsteps=300)
+    assert len(p.receivers) == 16384
+    got = [1e3 * t for t in api.run_a3d(p, "fp32")]
+    orc, _, _ = H.run_a3d_oracle(p)
+    assert [len(a) for a in got] == [len(a) for a in orc]
+    assert max(np.abs(a).max() for a in orc) > 0.0
+    assert H.rel_l2(got, orc) < TOL_FP32
+
+
+def _host_gb_available():
+    import psutil
+    return psutil.virtual_memory().available / 1e9
+
+
+def test_a3d_544cube_random_state_every_field():
+    # the FP64 oracle holds 14 full volumes of 544^3 (18 GB) next to the
+    # model, the padded model and the compared fields (about 28 GB at peak)
+    if _host_gb_available() < 48:
+        pytest.skip("fewer than 48 GB of host memory available for the 544^3 oracle")
+    p = W.cfg3()
+    errs = _a3d_random_state(p, 4, 13)
+    assert all(e < TOL_FP32 for e in errs.values()), errs
+
+
+FIELDS = ("vx", "vz", "txx", "tzz", "txz")
+
+
+def test_eiso_1040x540_batched_64_shots_random_state():
+    p = W.cfg2()
+    s = H.eiso_setup(p)
+    args = (p.nx, p.nz, p.npml, p.h, s["dt"], s["la"], s["mu"], s["l2m"], s["b"], s["bm"],
+            s["d"], s["dh"], s["dH"])
+    dev = api.EIsoDevice(*args, "fp32", nshots=64)
+    NX, NZ = p.nx + 2 * p.npml, p.nz + 2 * p.npml
+    inter = np.zeros((NX, NZ), bool)
+    inter[p.npml:p.npml + p.nx, p.npml:p.npml + p.nz] = True
+    rng = np.random.default_rng(17)
+    orcs = {}
+    for shot in (0, 63):
+        orc = O.EIso(*args)
+        for f in FIELDS:
+            scale = 1e-3 if f.startswith("v") else 1e4
+            tot, xp, zp = (scale * rng.standard_normal((NX, NZ)) for _ in range(3))
+            xp[inter] = 0
+            zp[inter] = 0
+            tot = np.where(inter, tot, 0)
+            orc.set(f, "x", xp)
+            orc.set(f, "z", zp)
+            orc.set(f, "total", tot)
+            dev.set_field(f, xp, shot=shot, part="x")
+            dev.set_field(f, zp, shot=shot, part="z")
+            dev.set_field(f, tot, shot=shot, part="total")
+        for _ in range(4):
+            orc.velocity()
+            orc.stress()
+        orcs[shot] = orc
+    dev.run(4)
+    for shot, orc in orcs.items():
+        for f in FIELDS:
+            for part in ("total", "x", "z"):
+                e = O.rel_l2(dev.get_field(f, shot=shot, part=part), orc.get(f, part))
+                assert e < TOL_FP32, (shot, f, part, e)
+    dev.close()
+
+
+def test_eiso_1040x540_batched_64_shots_traces():
+    p = W.cfg2(nsteps=400)
+    assert len(p.shots) == 64
+    dev, n = api.eiso_device(p, "fp32")
+    assert dev.nshots == 64
+    dev.run(n)
+    for shot in (0, 63):
+        got = [1e3 * t for t in dev.traces(shot)]
+        orc, _, _ = H.run_eiso_oracle(p, shot=shot)
+        assert [len(a) for a in got] == [len(a) for a in orc]
+        assert max(np.abs(a).max() for a in orc) > 0.0
+        assert H.rel_l2(got, orc) < TOL_FP32, shot
+    dev.close()
