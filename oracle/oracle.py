@@ -61,6 +61,7 @@ def _load():
     lib.orc_eiso_add_source.argtypes = [C.c_void_p, _sz, C.c_int, C.c_double]
     lib.orc_eiso_get.argtypes = [C.c_void_p, C.c_int, C.c_int, _dp]
     lib.orc_eiso_set.argtypes = [C.c_void_p, C.c_int, C.c_int, _dp]
+    lib.orc_eiso_set_bfp.argtypes = [C.c_void_p, C.c_int, C.c_int]
     lib.orc_eiso_probe.restype = C.c_double
     lib.orc_eiso_probe.argtypes = [C.c_void_p, C.c_int, _sz]
     lib.orc_a3d_pad_model.argtypes = [_sz, _sz, _sz, _sz, _dp, _dp, _dp, _dp]
@@ -78,7 +79,7 @@ def _load():
     lib.orc_a3d_add_source.argtypes = [C.c_void_p, _sz, C.c_double]
     lib.orc_a3d_get.argtypes = [C.c_void_p, C.c_int, _dp]
     lib.orc_a3d_gather.argtypes = [C.c_void_p, _sz, C.POINTER(C.c_int), C.POINTER(_sz), _dp]
-    lib.orc_a3d_set_bfp.argtypes = [C.c_void_p, C.c_int]
+    lib.orc_a3d_set_bfp.argtypes = [C.c_void_p, C.c_int, C.c_int]
     lib.orc_a3d_set.argtypes = [C.c_void_p, C.c_int, _dp]
     lib.orc_a3d_probe.restype = C.c_double
     lib.orc_a3d_probe.argtypes = [C.c_void_p, C.c_int, _sz]
@@ -198,6 +199,11 @@ class EIso:
         a = np.ascontiguousarray(arr, dtype=np.float64).reshape(self.NX, self.NZ)
         lib().orc_eiso_set(self.h_, FIELDS_E[field], PARTS[part], _ptr(a))
 
+    def set_bfp(self, block, axis="x"):
+        """checker mode: the state a step stores is rounded to 16-bit block
+        floating point with blocks of `block` cells along x or z (0: FP64)"""
+        lib().orc_eiso_set_bfp(self.h_, int(block), 0 if axis == "x" else 1)
+
     def probe(self, field, index):
         return lib().orc_eiso_probe(self.h_, FIELDS_E[field], int(index))
 
@@ -282,10 +288,10 @@ class A3D:
                              q.ctypes.data_as(C.POINTER(_sz)), _ptr(out))
         return out
 
-    def set_bfp(self, block):
-        """checker mode: round every stored value to 16-bit block floating
-        point with blocks of `block` z cells (0: FP64 storage)"""
-        lib().orc_a3d_set_bfp(self.h_, int(block))
+    def set_bfp(self, block, axis="y"):
+        """checker mode: round the stored state to 16-bit block floating
+        point with blocks of `block` cells along y or z (0: FP64 storage)"""
+        lib().orc_a3d_set_bfp(self.h_, int(block), 1 if axis == "y" else 2)
 
 
 # ----------------------------------------------------------------------------

@@ -196,12 +196,18 @@ void orc_eiso_profiles(size_t np, double h, size_t ncell, const double *vp,
         dH[n] = d0 * pow((((np - n) * h + h / 2.) / delta), 2);
 }
 
+static void bfp_round_rows(double *f, size_t nrows, size_t n, int B);
+static void bfp_round_cols(double *f, size_t nrows, size_t n, int B);
+static void bfp_round_strided(double *v, size_t stride, size_t n);
+
 struct orc_eiso {
     size_t nx, nz, np, NX, NZ;
     double h, dt;
     const double *mat[5];      /* b, bm, la, l2m, mu: interior, i*nz+j */
     double *d, *dh, *dH;
     double *f[5], *fx[5], *fz[5];
+    int bfp_block;             /* 0: FP64 storage; else block floating point */
+    int bfp_axis;              /* blocks along X (0) or Z (1) */
 };
 
 enum { M_B = 0, M_BM = 1, M_LA = 2, M_L2M = 3, M_MU = 4 };
@@ -260,7 +266,8 @@ static double e_val(const orc_eiso *o, int k, long X, long Z)
 {
     if (X < 0 || Z < 0 || X >= (long)o->NX || Z >= (long)o->NZ) return 0.0;
     size_t q = (size_t)X * o->NZ + (size_t)Z;
-    if (e_interior(o, X, Z)) return o->f[k][q];
+    /* block storage keeps the frame's totals as stored (rounded) values */
+    if (e_interior(o, X, Z) || o->bfp_block) return o->f[k][q];
     return o->fx[k][q] + o->fz[k][q];
 }
 
@@ -381,6 +388,21 @@ void orc_eiso_stress(orc_eiso *o)
             }
         }
     }
+    /* block storage: the step stores its state rounded (velocities and
+     * stresses, totals on the padded grid in blocks of B cells along Z;
+     * the frame's split parts keep their precision, as the device keeps
+     * them in FP32); the stress update above read the unrounded velocities */
+    if (o->bfp_block)
+        for (int k = 0; k < 5; ++k) {
+            if (o->bfp_axis == 0) bfp_round_cols(o->f[k], o->NX, o->NZ, o->bfp_block);
+            else bfp_round_rows(o->f[k], o->NX, o->NZ, o->bfp_block);
+        }
+}
+
+void orc_eiso_set_bfp(orc_eiso *o, int block, int axis)
+{
+    o->bfp_block = block > 0 ? block : 0;
+    o->bfp_axis = axis == 1 ? 1 : 0;
 }
 
 void orc_eiso_add_source(orc_eiso *o, size_t index, int type, double value)
@@ -391,6 +413,18 @@ void orc_eiso_add_source(orc_eiso *o, size_t index, int type, double value)
     if (type == 0 || type == 6) o->f[ORC_TXX][q] += value;
     if (type == 2 || type == 6) o->f[ORC_TZZ][q] += value;
     if (type == 4) o->f[ORC_TXZ][q] += value;
+    if (o->bfp_block) {   /* the block of the source cell is stored again */
+        size_t B = (size_t)o->bfp_block, Z = q % o->NZ, X = q / o->NZ;
+        for (int k = ORC_TXX; k <= ORC_TXZ; ++k) {
+            if (o->bfp_axis == 0) {
+                size_t x0 = X / B * B, nb = x0 + B < o->NX ? B : o->NX - x0;
+                bfp_round_strided(o->f[k] + x0 * o->NZ + Z, o->NZ, nb);
+            } else {
+                size_t z0 = Z / B * B;
+                bfp_round_strided(o->f[k] + q - Z + z0, 1, z0 + B < o->NZ ? B : o->NZ - z0);
+            }
+        }
+    }
 }
 
 void orc_eiso_get(const orc_eiso *o, int field, int part, double *out)
@@ -399,7 +433,8 @@ void orc_eiso_get(const orc_eiso *o, int field, int part, double *out)
     for (size_t q = 0; q < N; ++q) {
         long X = (long)(q / o->NZ), Z = (long)(q % o->NZ);
         int in = e_interior(o, X, Z);
-        if (part == ORC_TOTAL) out[q] = in ? o->f[field][q] : o->fx[field][q] + o->fz[field][q];
+        if (part == ORC_TOTAL)
+            out[q] = (in || o->bfp_block) ? o->f[field][q] : o->fx[field][q] + o->fz[field][q];
         else if (part == ORC_XPART) out[q] = in ? 0.0 : o->fx[field][q];
         else out[q] = in ? 0.0 : o->fz[field][q];
     }
@@ -507,6 +542,7 @@ struct orc_a3d {
     double *irx, *iry, *irz, *K;
     double *coef[18];
     int bfp_block;   /* 0: FP64 storage; else block floating point, see below */
+    int bfp_axis;    /* blocks along z (2) or y (1) */
 };
 
 orc_a3d *orc_a3d_new(size_t nx2, size_t ny2, size_t nz2, double dx, double dy, double dz,
@@ -653,25 +689,35 @@ static void a3d_p(void *ctx, size_t i0, size_t i1)
  * from the plain oracle is the storage format's own error.  The CPML memory
  * variables keep FP64 (the device keeps them in FP32).
  * ---------------------------------------------------------------------- */
-static void bfp_round_block(double *row, size_t k0, size_t k1)
+/* one block of n values at v[0], v[stride], ... */
+static void bfp_round_strided(double *v, size_t stride, size_t n)
 {
     double mx = 0.0;
-    for (size_t k = k0; k < k1; ++k) mx = fabs(row[k]) > mx ? fabs(row[k]) : mx;
+    for (size_t k = 0; k < n; ++k) mx = fabs(v[k * stride]) > mx ? fabs(v[k * stride]) : mx;
     if (mx == 0.0 || !isfinite(mx)) return;
     int E;
     frexp(mx, &E);   /* mx in [2^(E-1), 2^E) */
-    /* the exponent range of the device format (an FP32 biased exponent of
-     * the block maximum in [15, 240]): tiny blocks keep the scale 2^126 */
+    /* a block whose largest value would round up to 2^15 takes the next
+     * exponent (the device compares the FP32 maximum with
+     * 2^E (1 - 2^-16)); E is held in [-111, 114], the range of the
+     * device's 8-bit exponent: tiny blocks keep the scale 2^126 */
+    if (mx >= ldexp(1.0 - ldexp(1.0, -16), E)) E += 1;
     if (E < -111) E = -111;
     if (E > 114) E = 114;
     double sc = ldexp(1.0, 15 - E), isc = ldexp(1.0, E - 15);
-    for (size_t k = k0; k < k1; ++k) {
-        double m = nearbyint(row[k] * sc);
+    for (size_t k = 0; k < n; ++k) {
+        double m = nearbyint(v[k * stride] * sc);
         if (m > 32767.0) m = 32767.0;
-        row[k] = m * isc;
+        v[k * stride] = m * isc;
     }
 }
 
+static void bfp_round_block(double *row, size_t k0, size_t k1)
+{
+    bfp_round_strided(row + k0, 1, k1 - k0);
+}
+
+/* blocks of B consecutive values along the fastest axis of rows of n */
 static void bfp_round_rows(double *f, size_t nrows, size_t n, int B)
 {
     for (size_t r = 0; r < nrows; ++r)
@@ -679,30 +725,45 @@ static void bfp_round_rows(double *f, size_t nrows, size_t n, int B)
             bfp_round_block(f + r * n, k0, k0 + (size_t)B < n ? k0 + (size_t)B : n);
 }
 
+/* blocks of B consecutive rows (stride n) at each position of the fastest
+ * axis, in a plane of nrows rows of n */
+static void bfp_round_cols(double *f, size_t nrows, size_t n, int B)
+{
+    for (size_t r0 = 0; r0 < nrows; r0 += (size_t)B) {
+        size_t nb = r0 + (size_t)B < nrows ? (size_t)B : nrows - r0;
+        for (size_t k = 0; k < n; ++k) bfp_round_strided(f + r0 * n + k, n, nb);
+    }
+}
+
 struct bfp_job {
     double *f[3];
-    size_t plane;    /* values per x plane */
-    size_t nz2;
-    int B;
+    size_t ny2, nz2;
+    int B, axis;
 };
 
 static void bfp_planes(void *ctx, size_t i0, size_t i1)
 {
     struct bfp_job *j = ctx;
-    for (int a = 0; a < 3; ++a)
-        if (j->f[a])
-            bfp_round_rows(j->f[a] + i0 * j->plane, (i1 - i0) * (j->plane / j->nz2), j->nz2, j->B);
+    size_t plane = j->ny2 * j->nz2;
+    for (int a = 0; a < 3; ++a) {
+        if (!j->f[a]) continue;
+        for (size_t i = i0; i < i1; ++i) {
+            if (j->axis == 2) bfp_round_rows(j->f[a] + i * plane, j->ny2, j->nz2, j->B);
+            else bfp_round_cols(j->f[a] + i * plane, j->ny2, j->nz2, j->B);
+        }
+    }
 }
 
 static void a3d_round(orc_a3d *o, double *f0, double *f1, double *f2)
 {
-    struct bfp_job j = {{f0, f1, f2}, o->ny2 * o->nz2, o->nz2, o->bfp_block};
+    struct bfp_job j = {{f0, f1, f2}, o->ny2, o->nz2, o->bfp_block, o->bfp_axis};
     orc_parallel(o->nx2, bfp_planes, &j);
 }
 
-void orc_a3d_set_bfp(orc_a3d *o, int block)
+void orc_a3d_set_bfp(orc_a3d *o, int block, int axis)
 {
     o->bfp_block = block > 0 ? block : 0;
+    o->bfp_axis = axis == 1 ? 1 : 2;
 }
 
 void orc_a3d_velocity(orc_a3d *o)
@@ -724,10 +785,15 @@ void orc_a3d_pressure(orc_a3d *o)
 void orc_a3d_add_source(orc_a3d *o, size_t index, double value)
 {
     o->P[index] += value;
-    if (o->bfp_block) {
-        size_t B = (size_t)o->bfp_block, k = index % o->nz2, k0 = k / B * B;
-        double *row = o->P + (index - k);
-        bfp_round_block(row, k0, k0 + B < o->nz2 ? k0 + B : o->nz2);
+    if (o->bfp_block) {   /* the block of the source cell is stored again */
+        size_t B = (size_t)o->bfp_block, k = index % o->nz2, ij = index / o->nz2;
+        if (o->bfp_axis == 2) {
+            size_t k0 = k / B * B;
+            bfp_round_block(o->P + (index - k), k0, k0 + B < o->nz2 ? k0 + B : o->nz2);
+        } else {
+            size_t j = ij % o->ny2, j0 = j / B * B, nb = j0 + B < o->ny2 ? B : o->ny2 - j0;
+            bfp_round_strided(o->P + (ij - j + j0) * o->nz2 + k, o->nz2, nb);
+        }
     }
 }
 

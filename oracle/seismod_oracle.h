@@ -80,6 +80,11 @@ void orc_eiso_add_source(orc_eiso *o, size_t index, int type, double value);
 void orc_eiso_get(const orc_eiso *o, int field, int part, double *out);
 void orc_eiso_set(orc_eiso *o, int field, int part, const double *in);
 /* interior value at i*nz+j (what a receiver reads), e_iso.c:646-661 */
+/* storage-rounding checker mode: 0 = FP64 storage (default); B > 0 = the
+ * state is rounded to 16-bit block floating point (blocks of B cells along
+ * X or Z of the padded grid) when a step stores it (no counterpart in the
+ * reference) */
+void orc_eiso_set_bfp(orc_eiso *o, int block, int axis);   /* axis 0: X, 1: Z */
 double orc_eiso_probe(const orc_eiso *o, int field, size_t index);
 
 /* ---------------- a_iso_3d ---------------- */
@@ -115,9 +120,9 @@ double orc_a3d_probe(const orc_a3d *o, int field, size_t index);
 void orc_a3d_gather(const orc_a3d *o, size_t n, const int *field, const size_t *index,
                     double *out);
 /* storage-rounding checker mode: 0 = FP64 storage (default); B > 0 = every
- * stored value rounded to 16-bit block floating point with blocks of B z
- * cells (no counterpart in the reference) */
-void orc_a3d_set_bfp(orc_a3d *o, int block);
+ * stored value rounded to 16-bit block floating point with blocks of B
+ * cells along y or z (no counterpart in the reference) */
+void orc_a3d_set_bfp(orc_a3d *o, int block, int axis);     /* axis 1: y, 2: z */
 
 /* ---------------- e_cyl_iso (oracle_ecyl.c) ---------------- */
 

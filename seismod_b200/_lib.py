@@ -16,8 +16,9 @@ HEADER = os.path.join(os.path.dirname(HERE), "include", "seismod_gpu.h")
 
 SM_OK, SM_EINVAL, SM_ENOMEM, SM_ECUDA, SM_ECFL, SM_EIO, SM_ETIMEOUT, SM_EBUSY, SM_ESTATE, \
     SM_ENOTFOUND = range(10)
-SM_FP32, SM_FP64, SM_FP16, SM_BF16 = 0, 1, 2, 3
-PRECISIONS = {"fp32": SM_FP32, "fp64": SM_FP64, "fp16": SM_FP16, "bf16": SM_BF16}
+SM_FP32, SM_FP64, SM_FP16, SM_BF16, SM_BFP16 = 0, 1, 2, 3, 4
+PRECISIONS = {"fp32": SM_FP32, "fp64": SM_FP64, "fp16": SM_FP16, "bf16": SM_BF16,
+              "bfp16": SM_BFP16}
 SM_SRC = {"sx": 0, "sz": 2, "sxz": 4, "bulk": 6}
 SM_COMP = {"vx": 0, "vy": 1, "vz": 2, "txx": 5, "tzz": 6, "txz": 7, "p": 8}
 SM_PART = {"total": 0, "x": 1, "z": 2}

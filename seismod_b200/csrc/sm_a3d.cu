@@ -77,6 +77,11 @@ struct A3Args {
     double idx, idy, idz;      // 1/dx, 1/dy, 1/dz
     float sc[4], isc[4];
     float psc[6], pisc[6];
+    // block-floating-point storage: exponent bytes of the fields read and
+    // written this step, [nx2][nyb][pitch] (nyb blocks of A3_BJ y rows)
+    void *fe[4];
+    void *feo[4];
+    int nyb;
 };
 
 // slab plane of node/half-node index n along an axis of n2 nodes, or -1
@@ -596,10 +601,497 @@ constexpr size_t a3d_step_smem() {
     return A3Lay<S, TY>::head + (size_t)D * A3Lay<S, TY>::stage;
 }
 
+// ===========================================================================
+// Block-floating-point step (SM_BFP16).  The fused step of a3d_step_kernel
+// with P, vx, vy, vz stored as 16-bit mantissas and one exponent byte per
+// block of A3_BJ consecutive y rows of one z column ([nx2][nyb][pitch]
+// bytes); the CPML memory variables, rho and K stay FP32, and the
+// arithmetic is the FP32 path's, operation for operation.  Each thread owns
+// exactly one block (its A3_BJ rows), so the exponent of a block it stores
+// is the maximum over its own registers: no exchange between threads.  The
+// velocities the lagged pressure reads are the unrounded values of this
+// step (vx and vz in registers, vy in the shared row buffer): only the state
+// a step leaves behind is rounded.  Decoded pressures are carried across
+// planes in registers: P(i+1) is decoded once, for vx at plane i, and then
+// serves as P(i) at plane i+1 and in the pressure update of plane i+1.
+// ===========================================================================
+#define A3_BJ 4
+
+template <int TY>
+struct A3BLay {
+    static constexpr int NB = TY / A3_BJ;   // blocks (thread rows) of the tile
+    // row widths (elements): P k0-8 .. k0+39, rho k0-4 .. k0+35, vz k0-8 .. k0+31;
+    // exponent rows (bytes): P k0-16 .. k0+47, vz k0-16 .. k0+31
+    static constexpr int WP = 48, WR = 40, WZ = 40, WEP = 64, WEZ = 48;
+    __host__ __device__ static constexpr size_t al(size_t x) { return (x + 127) / 128 * 128; }
+    static constexpr size_t bP = (size_t)(TY + 2) * WP * 2;
+    static constexpr size_t bEP = (size_t)(NB + 2) * WEP;
+    static constexpr size_t bR = (size_t)(TY + 2) * WR * 4;
+    static constexpr size_t bX = (size_t)TY * 32 * 2;
+    static constexpr size_t bEX = (size_t)NB * 32;
+    static constexpr size_t bY = (size_t)(TY + 1) * 32 * 2;
+    static constexpr size_t bEY = (size_t)(NB + 1) * 32;
+    static constexpr size_t bZ = (size_t)TY * WZ * 2;
+    static constexpr size_t bEZ = (size_t)NB * WEZ;
+    static constexpr size_t bK = (size_t)TY * 32 * 4;
+    static constexpr size_t oP = 0, oEP = al(bP), oR = oEP + al(bEP), oX = oR + al(bR);
+    static constexpr size_t oEX = oX + al(bX), oY = oEX + al(bEX), oEY = oY + al(bY);
+    static constexpr size_t oZ = oEY + al(bEY), oEZ = oZ + al(bZ), oK = oEZ + al(bEZ);
+    static constexpr size_t stage = oK + al(bK);
+    static constexpr unsigned tx =
+        (unsigned)(bP + bEP + bR + bX + bEX + bY + bEY + bZ + bEZ + bK);
+    // head as the FP32 step's: barriers, vy row buffers, coefficient tables
+    static constexpr size_t head = A3Lay<float, TY>::head;
+};
+
+struct A3BMaps {
+    CUtensorMap P, eP, vx, eX, vy, eY, vz, eZ, rho, K;
+};
+
+template <int W, int D, int MINB, int CLS>
+__global__ void __launch_bounds__(32 * W, MINB)
+    a3d_bstep_kernel(const A3Args a, const __grid_constant__ A3BMaps m) {
+    constexpr int R = A3_BJ, TY = W * R;
+    using C = float;
+    using PSt = Store<float>;
+    using L = A3BLay<TY>;
+    using HL = A3Lay<float, TY>;
+    static_assert(D >= 4 && D <= D_HEAD_BARS, "ring depth");
+    constexpr int NXT = A3_CHMAX + 2;
+    constexpr int WP = L::WP, WR = L::WR, WZ = L::WZ, WEP = L::WEP, WEZ = L::WEZ;
+    extern __shared__ __align__(128) unsigned char smem[];
+    uint64_t *bars = reinterpret_cast<uint64_t *>(smem);
+    C(*VYs)[TY + 1][32] = reinterpret_cast<C(*)[TY + 1][32]>(smem + HL::oVY);
+    C(*CX)[NXT] = reinterpret_cast<C(*)[NXT]>(smem + HL::oCX);
+    C(*CY)[TY + 1] = reinterpret_cast<C(*)[TY + 1]>(smem + HL::oCY);
+    C(*CZ)[33] = reinterpret_cast<C(*)[33]>(smem + HL::oCZ);
+    unsigned char *ring = smem + L::head;
+
+    const int lane = threadIdx.x, w = threadIdx.y;
+    const int tid = w * 32 + lane;
+    if (CLS == a.step_cls && (blockIdx.x | blockIdx.y | blockIdx.z | tid) == 0) ++*a.step;
+    int kt, jt;
+    if (CLS == A3_INNER) {
+        kt = a.kt0 + blockIdx.x; jt = a.jt0 + blockIdx.y;
+    } else {
+        a3_edge_tile(a, blockIdx.x, kt, jt);
+    }
+    const int k0 = kt * 32, j0 = jt * TY, jb0 = jt * (TY / R);
+    const int lo = a.np > 1 ? a.np : 1;
+    const bool ytile = j0 >= lo && j0 + TY - 1 <= a.ny2 - 2 - a.np;
+    const bool ztile = k0 >= lo && k0 + 31 <= a.nz2 - 2 - a.np;
+    if (CLS == A3_INNER && !(ytile && ztile)) {
+        if (tid == 0) atomicExch(a.err, 3);
+        return;
+    }
+    const int k = k0 + lane;
+    const int i0 = blockIdx.z * a.chunk;
+    const int i1 = min(i0 + a.chunk, a.nx2);
+    const int nx2 = a.nx2, ny2 = a.ny2, nz2 = a.nz2, np = a.np, pitch = a.pitch;
+    const int sx = a.sx, sy = a.sy;
+    const int ex = a.nyb * pitch;   // exponent bytes per x plane
+    const bool kin = k < nz2;
+    const int16_t *Pin = static_cast<const int16_t *>(a.f[A_P]);
+    const int16_t *Vxin = static_cast<const int16_t *>(a.f[A_VX]);
+    const uint8_t *EPin = static_cast<const uint8_t *>(a.fe[A_P]);
+    const uint8_t *EXin = static_cast<const uint8_t *>(a.fe[A_VX]);
+    int16_t *Pout = static_cast<int16_t *>(a.fo[A_P]);
+    int16_t *Vxout = static_cast<int16_t *>(a.fo[A_VX]);
+    int16_t *Vyout = static_cast<int16_t *>(a.fo[A_VY]);
+    int16_t *Vzout = static_cast<int16_t *>(a.fo[A_VZ]);
+    uint8_t *EPout = static_cast<uint8_t *>(a.feo[A_P]);
+    uint8_t *EXout = static_cast<uint8_t *>(a.feo[A_VX]);
+    uint8_t *EYout = static_cast<uint8_t *>(a.feo[A_VY]);
+    uint8_t *EZout = static_cast<uint8_t *>(a.feo[A_VZ]);
+    const C *rho = static_cast<const C *>(a.rho);
+    const C *cf = static_cast<const C *>(a.coef);
+    const C two_dt = static_cast<C>(a.two_dt);
+    const C idx = static_cast<C>(a.idx), idy = static_cast<C>(a.idy), idz = static_cast<C>(a.idz);
+    const C *psPx = static_cast<const C *>(a.psi[PS_PX]);
+    const C *psPy = static_cast<const C *>(a.psi[PS_PY]);
+    const C *psPz = static_cast<const C *>(a.psi[PS_PZ]);
+    const C *psVx = static_cast<const C *>(a.psi[PS_VX]);
+    const C *psVy = static_cast<const C *>(a.psi[PS_VY]);
+    const C *psVz = static_cast<const C *>(a.psi[PS_VZ]);
+    C *poPx = static_cast<C *>(a.pso[PS_PX]);
+    C *poPy = static_cast<C *>(a.pso[PS_PY]);
+    C *poPz = static_cast<C *>(a.pso[PS_PZ]);
+    C *poVx = static_cast<C *>(a.pso[PS_VX]);
+    C *poVy = static_cast<C *>(a.pso[PS_VY]);
+    C *poVz = static_cast<C *>(a.pso[PS_VZ]);
+
+    // coefficient tables: rows 0..2 half node (a, b, 1/k), 3..5 node
+    for (int t = tid; t < 6 * NXT; t += 32 * W) {
+        const int wch = t / NXT, e = t % NXT, p = i0 - 1 + e;
+        const bool half = wch < 3;
+        const bool ok = p >= 0 && p < (half ? nx2 - 1 : nx2);
+        CX[wch][e] = ok ? cf[a.cf.at(0, half ? 3 + wch : wch - 3) + p] : C(wch % 3 == 0 ? 0 : 1);
+    }
+    for (int t = tid; t < 6 * (TY + 1); t += 32 * W) {
+        const int wch = t / (TY + 1), e = t % (TY + 1), p = j0 - 1 + e;
+        const bool half = wch < 3;
+        const bool ok = p >= 0 && p < (half ? ny2 - 1 : ny2);
+        CY[wch][e] = ok ? cf[a.cf.at(1, half ? 3 + wch : wch - 3) + p] : C(wch % 3 == 0 ? 0 : 1);
+    }
+    for (int t = tid; t < 6 * 33; t += 32 * W) {
+        const int wch = t / 33, e = t % 33, p = k0 - 1 + e;
+        const bool half = wch < 3;
+        const bool ok = p >= 0 && p < (half ? nz2 - 1 : nz2);
+        CZ[wch][e] = ok ? cf[a.cf.at(2, half ? 3 + wch : wch - 3) + p] : C(wch % 3 == 0 ? 0 : 1);
+    }
+    if (tid == 0) {
+        for (int d = 0; d < D; ++d) mbar_init(&bars[d], 1);
+        fence_proxy_async();
+    }
+
+    const int nload = min(i1 + 1, nx2) - i0;
+    auto issue = [&](int l) {   // thread 0 only
+        if (l >= nload) return;
+        unsigned char *b = ring + (size_t)(l % D) * L::stage;
+        uint64_t *bar = &bars[l % D];
+        const int ip = i0 + l;
+        fence_proxy_async();
+        mbar_expect_tx(bar, L::tx);
+        tma_load_3d(b + L::oP, &m.P, k0 - 8, j0 - 1, ip, bar);
+        tma_load_3d(b + L::oEP, &m.eP, k0 - 16, jb0 - 1, ip, bar);
+        tma_load_3d(b + L::oR, &m.rho, k0 - 4, j0 - 1, ip, bar);
+        tma_load_3d(b + L::oX, &m.vx, k0, j0, ip, bar);
+        tma_load_3d(b + L::oEX, &m.eX, k0, jb0, ip, bar);
+        tma_load_3d(b + L::oY, &m.vy, k0, j0 - 1, ip, bar);
+        tma_load_3d(b + L::oEY, &m.eY, k0, jb0 - 1, ip, bar);
+        tma_load_3d(b + L::oZ, &m.vz, k0 - 8, j0, ip, bar);
+        tma_load_3d(b + L::oEZ, &m.eZ, k0 - 16, jb0, ip, bar);
+        tma_load_3d(b + L::oK, &m.K, k0, j0, ip, bar);
+    };
+    __syncthreads();   // barriers initialised, tables filled
+    if (tid == 0)
+        for (int l = 0; l < D - 2; ++l) issue(l);
+
+    // rows of this thread: one block, rows j0 + w*R + r
+    int jh[R], jn[R], joff[R];
+    bool rin[R];
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+        const int j = j0 + w * R + r;
+        rin[r] = kin && j < ny2;
+        jh[r] = j < ny2 ? half_slab(j, ny2, np) : -1;
+        jn[r] = j < ny2 ? node_slab(j, ny2, np) : -1;
+        joff[r] = j * sy + k;
+    }
+    const bool bin = rin[0];                       // the block has a cell in the grid
+    const int eoff = (jb0 + w) * pitch + k;         // this thread's exponent, plane 0
+    const int kh = kin ? half_slab(k, nz2, np) : -1;
+    const int kn = kin ? node_slab(k, nz2, np) : -1;
+    const int jm = j0 - 1, km = k0 - 1;
+    const int jmh = (jm >= 0) ? half_slab(jm, ny2, np) : -1;
+    const int hrow = w * R + lane;
+    const bool hcol = lane < R && km >= 0 && j0 + hrow < ny2;
+    const int kmh = (km >= 0) ? half_slab(km, nz2, np) : -1;
+    const bool yfast = CLS == A3_INNER || ytile;
+    const bool zfast = CLS == A3_INNER || ztile;
+
+    // exponent byte of stage sb: P block b (0: rows above the tile), column
+    // x = k - (k0 - 16); vx block w; vy block b (0: above); vz column x
+    auto eP_ = [&](const unsigned char *sb, int b, int x) -> unsigned { return sb[L::oEP + b * WEP + x]; };
+    auto eX_ = [&](const unsigned char *sb) -> unsigned { return sb[L::oEX + w * 32 + lane]; };
+    auto eY_ = [&](const unsigned char *sb, int b) -> unsigned { return sb[L::oEY + b * 32 + lane]; };
+    auto eZ_ = [&](const unsigned char *sb, int x) -> unsigned { return sb[L::oEZ + w * WEZ + x]; };
+    auto mP = [&](const unsigned char *sb, int row, int x) -> int {   // row of the box, x = k - (k0-8)
+        return reinterpret_cast<const int16_t *>(sb + L::oP)[row * WP + x];
+    };
+
+    C fPx[R], fPy[R], fPz[R], fVx[R], fVy[R], fVz[R], fHy = C(0), fHz = C(0);
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+        fPx[r] = C(0); fPy[r] = C(0); fPz[r] = C(0);
+        fVx[r] = C(0); fVy[r] = C(0); fVz[r] = C(0);
+    }
+    auto load_vpsi = [&](int ip) {
+        const int s = (ip < nx2 - 1) ? half_slab(ip, nx2, np) : -1;
+        if (s >= 0) {
+#pragma unroll
+            for (int r = 0; r < R; ++r) fPx[r] = rin[r] ? psPx[s * sx + joff[r]] : C(0);
+        }
+        if (!yfast) {
+#pragma unroll
+            for (int r = 0; r < R; ++r)
+                fPy[r] = (rin[r] && jh[r] >= 0) ? psPy[(ip * 2 * np + jh[r]) * pitch + k] : C(0);
+        }
+        if (!zfast) {
+#pragma unroll
+            for (int r = 0; r < R; ++r) {
+                const int j = j0 + w * R + r;
+                fPz[r] = (rin[r] && kh >= 0) ? psPz[(ip * ny2 + j) * 2 * np + kh] : C(0);
+            }
+        }
+        if (w == 0 && kin && jmh >= 0) fHy = psPy[(ip * 2 * np + jmh) * pitch + k];
+        if (hcol && kmh >= 0) fHz = psPz[(ip * ny2 + j0 + hrow) * 2 * np + kmh];
+    };
+    auto load_ppsi = [&](int ip) {
+        const int s = node_slab(ip, nx2, np);
+        if (s >= 0) {
+#pragma unroll
+            for (int r = 0; r < R; ++r) fVx[r] = rin[r] ? psVx[s * sx + joff[r]] : C(0);
+        }
+        if (!yfast) {
+#pragma unroll
+            for (int r = 0; r < R; ++r)
+                fVy[r] = (rin[r] && jn[r] >= 0) ? psVy[(ip * 2 * np + jn[r]) * pitch + k] : C(0);
+        }
+        if (!zfast) {
+#pragma unroll
+            for (int r = 0; r < R; ++r) {
+                const int j = j0 + w * R + r;
+                fVz[r] = (rin[r] && kn >= 0) ? psVz[(ip * ny2 + j) * 2 * np + kn] : C(0);
+            }
+        }
+    };
+
+    C vxa[R], vxb[R], vzp[R];
+    C vzhp = C(0);    // lane r < R: the halo-column vz of row w*R + r, previous plane
+    C pc[R], pp[R];   // decoded P of plane i (own cells) and of plane i-1
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+        vxa[r] = C(0); vxb[r] = C(0); vzp[r] = C(0); pc[r] = C(0); pp[r] = C(0);
+    }
+    // vx(i0-1) (direct loads, once per CTA): the pressure of plane i0 needs it
+    if (i0 >= 1 && bin) {
+        const int s = half_slab(i0 - 1, nx2, np);
+        const int eo = (i0 - 1) * ex + eoff;
+        const BDec dX = bfp_dec(EXin[eo]), dP0 = bfp_dec(EPin[eo]), dP1 = bfp_dec(EPin[eo + ex]);
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+            if (!rin[r]) continue;
+            const int qm = (i0 - 1) * sx + joff[r], q0 = qm + sx;
+            C psi_old = C(0), psi_new;
+            if (s >= 0) psi_old = psPx[s * sx + joff[r]];
+            vxa[r] = a3_vel<C>(bfp_val(Vxin[qm], dX), bfp_val(Pin[qm], dP0), bfp_val(Pin[q0], dP1),
+                               rho[qm], rho[q0], idx, two_dt, s >= 0, CX[0][0], CX[1][0], CX[2][0],
+                               psi_old, psi_new);
+        }
+    }
+    load_vpsi(i0);
+    // P of the first plane, decoded once
+    if (!mbar_wait(&bars[0], 0, a.err, 1)) return;
+    {
+        const BDec d = bfp_dec(eP_(ring, w + 1, lane + 16));
+#pragma unroll
+        for (int r = 0; r < R; ++r) pc[r] = bfp_val(mP(ring, w * R + r + 1, lane + 8), d);
+    }
+
+    // encode and store one block (rows of this thread) of a field at plane
+    // ip: mantissas where the row is in the grid, the exponent once
+    auto store_block = [&](int16_t *out, uint8_t *eout, int ip, const C *v) {
+        unsigned mx = 0;
+#pragma unroll
+        for (int r = 0; r < R; ++r) mx = rin[r] ? max(mx, bfp_absbits(v[r])) : mx;
+        bool over;
+        const unsigned e8 = bfp_e8(mx, &over);
+        const float esc = bfp_escale(e8);
+        int16_t *o = out + ip * sx;
+#pragma unroll
+        for (int r = 0; r < R; ++r)
+            if (rin[r]) o[joff[r]] = bfp_man(v[r], esc);
+        if (bin) {
+            eout[ip * ex + eoff] = (uint8_t)e8;
+            if (over) atomicExch(a.err, 4);
+        }
+    };
+
+    // ---- the lagged pressure half step of plane ip (a_iso_3d.c:659-683) ----
+    auto pressure = [&](int ip, int lp, auto AFt) {
+        constexpr bool AF = decltype(AFt)::value;
+        const bool fx = AF || (ip >= lo && ip <= nx2 - 1 - np);
+        const bool fy = AF || yfast, fz = AF || zfast;
+        const unsigned char *pb = ring + (size_t)(lp % D) * L::stage;
+        const C *pK = reinterpret_cast<const C *>(pb + L::oK);
+        const C(*vy)[32] = VYs[ip & 1];
+        const int sxn = fx ? -1 : node_slab(ip, nx2, np);
+        const int e = ip - (i0 - 1);
+        C pn[R];
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+            const int row = w * R + r, j = j0 + row;
+            C vzm = __shfl_up_sync(0xffffffffu, vzp[r], 1);
+            const C hal = __shfl_sync(0xffffffffu, vzhp, r);
+            if (lane == 0) vzm = hal;
+            const C p_c = pp[r];
+            pn[r] = p_c;
+            if (!rin[r]) continue;
+            bool upd = true;
+            if (!fx) upd = ip >= 1;
+            if (!fy) upd = upd && j >= 1;
+            if (!fz) upd = upd && k >= 1;
+            if (upd) {
+                C gx = r_mul(r_sub(vxa[r], vxb[r]), idx);
+                C gy = r_mul(r_sub(vy[row + 1][lane], vy[row][lane]), idy);
+                C gz = r_mul(r_sub(vzp[r], vzm), idz);
+                C psi_new;
+                if (sxn >= 0) {
+                    gx = a3_dv<C>(gx, CX[3][e], CX[4][e], CX[5][e], fVx[r], psi_new);
+                    poVx[sxn * sx + joff[r]] = psi_new;
+                }
+                if (!fy && jn[r] >= 0) {
+                    gy = a3_dv<C>(gy, CY[3][row + 1], CY[4][row + 1], CY[5][row + 1], fVy[r], psi_new);
+                    poVy[(ip * 2 * np + jn[r]) * pitch + k] = psi_new;
+                }
+                if (!fz && kn >= 0) {
+                    gz = a3_dv<C>(gz, CZ[3][lane + 1], CZ[4][lane + 1], CZ[5][lane + 1], fVz[r], psi_new);
+                    poVz[(ip * ny2 + j) * 2 * np + kn] = psi_new;
+                }
+                pn[r] = r_fma(-pK[row * 32 + lane], r_add(r_add(gx, gy), gz), p_c);
+            }
+        }
+        // written whether updated or not: both buffers always hold a
+        // complete state
+        store_block(Pout, EPout, ip, pn);
+    };
+
+    for (int i = i0; i < i1; ++i) {
+        const int l = i - i0;
+        if (tid == 0) issue(l + D - 2);
+        if (!mbar_wait(&bars[l % D], (l / D) & 1, a.err, 1)) return;
+        if (i + 1 < nx2 && !mbar_wait(&bars[(l + 1) % D], ((l + 1) / D) & 1, a.err, 1)) return;
+        const unsigned char *cbuf = ring + (size_t)(l % D) * L::stage;
+        const unsigned char *nbuf = ring + (size_t)((l + 1) % D) * L::stage;
+        const C *cR = reinterpret_cast<const C *>(cbuf + L::oR);
+        const C *nR = reinterpret_cast<const C *>(nbuf + L::oR);
+        const int16_t *cX = reinterpret_cast<const int16_t *>(cbuf + L::oX);
+        const int16_t *cY = reinterpret_cast<const int16_t *>(cbuf + L::oY);
+        const int16_t *cZ = reinterpret_cast<const int16_t *>(cbuf + L::oZ);
+        C(*vyw)[32] = VYs[i & 1];
+        const bool xf = i >= np && i <= nx2 - 2 - np;
+        const int sxh = (i < nx2 - 1) ? half_slab(i, nx2, np) : -1;
+        const int e = i - (i0 - 1);
+        // decoders of this plane's blocks (the next plane's P: its pressures
+        // are decoded here once and carried)
+        const BDec dPz = bfp_dec(eP_(cbuf, w + 1, lane + 17));
+        const BDec dPy = bfp_dec(eP_(cbuf, w + 2, lane + 16));
+        const BDec dX = bfp_dec(eX_(cbuf)), dY = bfp_dec(eY_(cbuf, w + 1));
+        const BDec dZ = bfp_dec(eZ_(cbuf, lane + 16));
+        C pnx[R];
+        if (i + 1 < nx2) {
+            const BDec dPn = bfp_dec(eP_(nbuf, w + 1, lane + 16));
+#pragma unroll
+            for (int r = 0; r < R; ++r) pnx[r] = bfp_val(mP(nbuf, w * R + r + 1, lane + 8), dPn);
+        } else {
+#pragma unroll
+            for (int r = 0; r < R; ++r) pnx[r] = C(0);
+        }
+
+        // ---- velocity half step at plane i (a_iso_3d.c:605-651) ----
+        C vxn[R], vyn[R], vzn[R];
+        C vzh = C(0);
+        auto velocity = [&](auto AFt) {
+        constexpr bool AF = decltype(AFt)::value;
+        const bool fx = AF || xf, fy = AF || yfast, fz = AF || zfast;
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+            const int row = w * R + r, j = j0 + row;
+            const int rc = (row + 1) * WR + 4 + lane;
+            const C p_c = pc[r];
+            const C p_n = pnx[r];
+            const C p_y = r + 1 < R ? pc[r + 1] : bfp_val(mP(cbuf, row + 2, lane + 8), dPy);
+            const C p_z = bfp_val(mP(cbuf, row + 1, lane + 9), dPz);
+            const C r_c = cR[rc];
+            C vx = bfp_val(cX[row * 32 + lane], dX);
+            C vy = bfp_val(cY[(row + 1) * 32 + lane], dY);
+            C vz = bfp_val(cZ[row * WZ + 8 + lane], dZ);
+            C psi_new;
+            if (fx) {
+                vx = a3_vel0<C>(vx, p_c, p_n, r_c, nR[rc], idx, two_dt);
+            } else if (rin[r] && i < nx2 - 1) {
+                vx = a3_vel<C>(vx, p_c, p_n, r_c, nR[rc], idx, two_dt, sxh >= 0,
+                               CX[0][e], CX[1][e], CX[2][e], fPx[r], psi_new);
+                if (sxh >= 0) poPx[sxh * sx + joff[r]] = psi_new;
+            }
+            if (fy) {
+                vy = a3_vel0<C>(vy, p_c, p_y, r_c, cR[rc + WR], idy, two_dt);
+            } else if (rin[r] && j < ny2 - 1) {
+                vy = a3_vel<C>(vy, p_c, p_y, r_c, cR[rc + WR], idy, two_dt, jh[r] >= 0,
+                               CY[0][row + 1], CY[1][row + 1], CY[2][row + 1], fPy[r], psi_new);
+                if (jh[r] >= 0) poPy[(i * 2 * np + jh[r]) * pitch + k] = psi_new;
+            }
+            if (fz) {
+                vz = a3_vel0<C>(vz, p_c, p_z, r_c, cR[rc + 1], idz, two_dt);
+            } else if (rin[r] && k < nz2 - 1) {
+                vz = a3_vel<C>(vz, p_c, p_z, r_c, cR[rc + 1], idz, two_dt, kh >= 0,
+                               CZ[0][lane + 1], CZ[1][lane + 1], CZ[2][lane + 1], fPz[r], psi_new);
+                if (kh >= 0) poPz[(i * ny2 + j) * 2 * np + kh] = psi_new;
+            }
+            vyw[row + 1][lane] = vy;
+            vxn[r] = vx;
+            vyn[r] = vy;
+            vzn[r] = vz;
+        }
+        };
+        if (CLS == A3_INNER && xf) velocity(BoolT<true>{});
+        else velocity(BoolT<false>{});
+        store_block(Vxout, EXout, i, vxn);
+        store_block(Vyout, EYout, i, vyn);
+        store_block(Vzout, EZout, i, vzn);
+        // halo row: vy(i, j0-1, k), by warp 0
+        if (w == 0) {
+            C vyh = C(0);
+            if (jm >= 0 && kin) {
+                C psi_new;
+                vyh = a3_vel<C>(bfp_val(cY[lane], bfp_dec(eY_(cbuf, 0))),
+                                bfp_val(mP(cbuf, 0, lane + 8), bfp_dec(eP_(cbuf, 0, lane + 16))),
+                                bfp_val(mP(cbuf, 1, lane + 8), bfp_dec(eP_(cbuf, 1, lane + 16))),
+                                cR[4 + lane], cR[WR + 4 + lane], idy, two_dt, jmh >= 0, CY[0][0],
+                                CY[1][0], CY[2][0], fHy, psi_new);
+            }
+            vyw[0][lane] = vyh;
+        }
+        // halo column: vz(i, j, k0-1) of row w*R + lane, by lanes 0..R-1
+        if (hcol) {
+            const int rc = (hrow + 1) * WR + 4;
+            const BDec dP0 = bfp_dec(eP_(cbuf, w + 1, 15)), dP1 = bfp_dec(eP_(cbuf, w + 1, 16));
+            C psi_new;
+            vzh = a3_vel<C>(bfp_val(cZ[hrow * WZ + 7], bfp_dec(eZ_(cbuf, 15))),
+                            bfp_val(mP(cbuf, hrow + 1, 7), dP0), bfp_val(mP(cbuf, hrow + 1, 8), dP1),
+                            cR[rc - 1], cR[rc], idz, two_dt, kmh >= 0, CZ[0][0], CZ[1][0], CZ[2][0],
+                            fHz, psi_new);
+        }
+        if (i + 1 < i1) load_vpsi(i + 1);
+        if (i > i0) {
+            const int ip = i - 1;
+            if (CLS == A3_INNER && ip >= lo && ip <= nx2 - 1 - np) pressure(ip, l - 1, BoolT<true>{});
+            else pressure(ip, l - 1, BoolT<false>{});
+        }
+        load_ppsi(i);
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+            vxb[r] = vxa[r];
+            vxa[r] = vxn[r];
+            vzp[r] = vzn[r];
+            pp[r] = pc[r];
+            pc[r] = pnx[r];
+        }
+        vzhp = vzh;
+        __syncthreads();
+    }
+    if (i1 > i0) {
+        const int ip = i1 - 1;
+        if (CLS == A3_INNER && ip >= lo && ip <= nx2 - 1 - np) pressure(ip, ip - i0, BoolT<true>{});
+        else pressure(ip, ip - i0, BoolT<false>{});
+    }
+}
+
+template <int TY, int D>
+constexpr size_t a3d_bstep_smem() {
+    return A3BLay<TY>::head + (size_t)D * A3BLay<TY>::stage;
+}
+
 struct A3Src {
     long long q;
     long long voff;
     int len;
+    // block storage: the exponent index of the cell's block, the first
+    // cell of the block (A3_BJ rows apart), its rows inside the grid and the
+    // source's row in it
+    long long qe, qb;
+    int nb, rs;
 };
 
 template <typename S>
@@ -622,7 +1114,49 @@ struct A3Rec {
     int field;
     int group;
     long long out;
+    long long qe;   // block storage: the exponent index of the cell's block
 };
+
+// block storage: one thread adds the sources in order; each addition
+// decodes the source cell's block, adds, and stores the block again with
+// the exponent its new maximum takes (a_iso_3d.c:689-693)
+__global__ void a3d_bsource_kernel(A3Args a, const A3Src *src, int nsrc, const double *vals) {
+    if (blockIdx.x != 0 || threadIdx.x != 0) return;
+    const long long it = *a.step - 1;
+    int16_t *P = static_cast<int16_t *>(a.f[A_P]);
+    uint8_t *E = static_cast<uint8_t *>(a.fe[A_P]);
+    for (int e = 0; e < nsrc; ++e) {
+        const A3Src s = src[e];
+        if (it >= s.len) continue;
+        const BDec d = bfp_dec(E[s.qe]);
+        float v[A3_BJ];
+        unsigned mx = 0;
+        for (int r = 0; r < s.nb; ++r) {
+            v[r] = bfp_val(P[s.qb + (long long)r * a.sy], d);
+            if (r == s.rs) v[r] = v[r] + static_cast<float>(vals[s.voff + it]);
+            mx = max(mx, bfp_absbits(v[r]));
+        }
+        bool over;
+        const unsigned e8 = bfp_e8(mx, &over);
+        const float esc = bfp_escale(e8);
+        for (int r = 0; r < s.nb; ++r) P[s.qb + (long long)r * a.sy] = bfp_man(v[r], esc);
+        E[s.qe] = (uint8_t)e8;
+        if (over) atomicExch(a.err, 4);
+    }
+}
+
+__global__ void a3d_bgather_kernel(A3Args a, const A3Rec *rec, int nrec, const int32_t *table,
+                                   long long nsteps_max, double *traces) {
+    const int r = blockIdx.x * blockDim.x + threadIdx.x;
+    const long long it = *a.step - 1;
+    if (r >= nrec || it >= nsteps_max) return;
+    const A3Rec e = rec[r];
+    const int32_t slot = table[(long long)e.group * nsteps_max + it];
+    if (slot < 0) return;
+    const int16_t m = static_cast<const int16_t *>(a.f[e.field])[e.q];
+    const unsigned e8 = static_cast<const uint8_t *>(a.fe[e.field])[e.qe];
+    traces[e.out + slot] = static_cast<double>(bfp_val(m, bfp_dec(e8)));
+}
 
 template <typename S>
 __global__ void a3d_gather_kernel(A3Args a, const A3Rec *rec, int nrec, const int32_t *table,
@@ -671,7 +1205,12 @@ struct sm_a3d {
     size_t psi_cells[6] = {0, 0, 0, 0, 0, 0};
     KernelTimer timer;
     A3Maps maps[2];                            // TMA maps with set b as input
+    A3BMaps bmaps[2];                          // ... for block storage (SM_BFP16)
     int maps_ty = -1;                          // tile rows the maps were made for
+    // block storage: exponent bytes of the four fields per buffer set,
+    // [nx2][nyb][pitch], nyb = ceil(ny2 / A3_BJ)
+    DevBuf fe[2][4];
+    size_t nyb = 0;
     DevBuf err;                                // kernel timeout flag
     DevBuf d_step;                             // device step counter (A3Args::step)
     // CUDA graphs of graph_steps steps, one per parity of the starting
@@ -706,6 +1245,8 @@ void a3d_bind(sm_a3d *h, int in) {
     for (int f = 0; f < 4; ++f) {
         h->args.f[f] = h->f[in][f].p;
         h->args.fo[f] = h->f[1 - in][f].p;
+        h->args.fe[f] = h->fe[in][f].p;
+        h->args.feo[f] = h->fe[1 - in][f].p;
     }
     for (int p = 0; p < 6; ++p) {
         h->args.psi[p] = h->psi[in][p].p;
@@ -724,6 +1265,17 @@ static const A3Config kA3Configs[] = {
     {16, 2, 4, 1}, {4, 2, 6, 4}, {8, 2, 4, 3}, {4, 8, 4, 2},
 };
 static const int kA3NumConfigs = sizeof(kA3Configs) / sizeof(kA3Configs[0]);
+// block storage: every thread holds one block of A3_BJ rows
+static const A3Config kA3BConfigs[] = {
+    {8, A3_BJ, 4, 2}, {4, A3_BJ, 4, 3}, {8, A3_BJ, 5, 1}, {4, A3_BJ, 6, 3}, {16, A3_BJ, 4, 1},
+};
+static const int kA3BNumConfigs = sizeof(kA3BConfigs) / sizeof(kA3BConfigs[0]);
+
+bool a3d_isb(const sm_a3d *h) { return h->precision == SM_BFP16; }
+const A3Config &a3d_cfg(const sm_a3d *h, int c) {
+    return a3d_isb(h) ? kA3BConfigs[c] : kA3Configs[c];
+}
+int a3d_ncfg(const sm_a3d *h) { return a3d_isb(h) ? kA3BNumConfigs : kA3NumConfigs; }
 
 // The interior rectangle of tiles for tile rows ty: tiles (32 k x ty j)
 // whose every cell is clear in y and z of the CPML frame and of the grid
@@ -752,7 +1304,7 @@ void a3d_tile_classes(sm_a3d *h, int ty) {
 
 // step kernels one step launches: one per non-empty tile class
 int a3d_step_kernels(sm_a3d *h) {
-    a3d_tile_classes(h, kA3Configs[h->config].ty());
+    a3d_tile_classes(h, a3d_cfg(h, h->config).ty());
     const A3Args &a = h->args;
     const int ninner = (a.kt1 - a.kt0) * (a.jt1 - a.jt0);
     return (ninner > 0) + (a.nkt * a.njt - ninner > 0);
@@ -777,6 +1329,55 @@ int a3d_ready_cfg(sm_a3d *h) {
         done[h->device] = true;
     }
     return SM_OK;
+}
+
+template <int W, int D, int MINB>
+int a3d_bready_cfg(sm_a3d *h) {
+    static std::mutex mu;
+    static bool done[64] = {};
+    if (h->device < 0 || h->device >= 64) return sm_fail(SM_EINVAL, "device %d", h->device);
+    std::lock_guard<std::mutex> lk(mu);
+    if (!done[h->device]) {
+        SM_CUDA_TRY(cudaFuncSetAttribute(a3d_bstep_kernel<W, D, MINB, A3_INNER>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)a3d_bstep_smem<W * A3_BJ, D>()));
+        SM_CUDA_TRY(cudaFuncSetAttribute(a3d_bstep_kernel<W, D, MINB, A3_EDGE>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)a3d_bstep_smem<W * A3_BJ, D>()));
+        done[h->device] = true;
+    }
+    return SM_OK;
+}
+
+// the block-storage step: the same two tile classes as the FP32 step
+template <int W, int D, int MINB>
+int a3d_blaunch_cfg(sm_a3d *h) {
+    constexpr int TY = W * A3_BJ;
+    constexpr size_t smem = a3d_bstep_smem<TY, D>();
+    A3Args &a = h->args;
+    a3d_tile_classes(h, TY);
+    const unsigned nch = (unsigned)((h->nx2 + a.chunk - 1) / a.chunk);
+    const int ninner = (a.kt1 - a.kt0) * (a.jt1 - a.jt0);
+    const int nedge = a.nkt * a.njt - ninner;
+    a.step_cls = ninner > 0 ? A3_INNER : A3_EDGE;
+    dim3 blk(32, W, 1);
+    if (nedge > 0 && ninner > 0) {
+        cudaEventRecord(h->ev_fork, h->stream);
+        cudaStreamWaitEvent(h->side, h->ev_fork, 0);
+    }
+    if (nedge > 0)
+        a3d_bstep_kernel<W, D, MINB, A3_EDGE>
+            <<<dim3((unsigned)nedge, 1, nch), blk, smem, ninner > 0 ? h->side : h->stream>>>(
+                a, h->bmaps[h->cur]);
+    if (ninner > 0)
+        a3d_bstep_kernel<W, D, MINB, A3_INNER>
+            <<<dim3((unsigned)(a.kt1 - a.kt0), (unsigned)(a.jt1 - a.jt0), nch), blk, smem,
+               h->stream>>>(a, h->bmaps[h->cur]);
+    if (nedge > 0 && ninner > 0) {
+        cudaEventRecord(h->ev_join, h->side);
+        cudaStreamWaitEvent(h->stream, h->ev_join, 0);
+    }
+    return (nedge > 0) + (ninner > 0);
 }
 
 template <typename S, int W, int R, int D, int MINB>
@@ -835,10 +1436,36 @@ int a3d_make_maps(sm_a3d *h, int ty) {
     return SM_OK;
 }
 
+// TMA maps of block storage: int16 mantissas and exponent bytes, boxes as
+// A3BLay
+int a3d_make_bmaps(sm_a3d *h, int ty) {
+    const size_t n0 = h->nz2, n1 = h->ny2, n2 = h->nx2, pt = h->pitch, nb = h->nyb;
+    const CUtensorMapDataType i16 = CU_TENSOR_MAP_DATA_TYPE_UINT16, u8 = CU_TENSOR_MAP_DATA_TYPE_UINT8;
+    const CUtensorMapDataType f32 = CU_TENSOR_MAP_DATA_TYPE_FLOAT32;
+    const unsigned nbt = (unsigned)(ty / A3_BJ);
+    int rc;
+    for (int b = 0; b < 2; ++b) {
+        A3BMaps &m = h->bmaps[b];
+        if ((rc = make_map_3d(&m.P, h->f[b][A_P].p, i16, 2, n0, n1, n2, pt, 48, ty + 2))) return rc;
+        if ((rc = make_map_3d(&m.eP, h->fe[b][A_P].p, u8, 1, n0, nb, n2, pt, 64, nbt + 2))) return rc;
+        if ((rc = make_map_3d(&m.vx, h->f[b][A_VX].p, i16, 2, n0, n1, n2, pt, 32, ty))) return rc;
+        if ((rc = make_map_3d(&m.eX, h->fe[b][A_VX].p, u8, 1, n0, nb, n2, pt, 32, nbt))) return rc;
+        if ((rc = make_map_3d(&m.vy, h->f[b][A_VY].p, i16, 2, n0, n1, n2, pt, 32, ty + 1))) return rc;
+        if ((rc = make_map_3d(&m.eY, h->fe[b][A_VY].p, u8, 1, n0, nb, n2, pt, 32, nbt + 1))) return rc;
+        if ((rc = make_map_3d(&m.vz, h->f[b][A_VZ].p, i16, 2, n0, n1, n2, pt, 40, ty))) return rc;
+        if ((rc = make_map_3d(&m.eZ, h->fe[b][A_VZ].p, u8, 1, n0, nb, n2, pt, 48, nbt))) return rc;
+        if ((rc = make_map_3d(&m.rho, h->rho.p, f32, 4, n0, n1, n2, pt, 40, ty + 2))) return rc;
+        if ((rc = make_map_3d(&m.K, h->K.p, f32, 4, n0, n1, n2, pt, 32, ty))) return rc;
+    }
+    h->maps_ty = ty;
+    return SM_OK;
+}
+
 int a3d_ensure_maps(sm_a3d *h) {
-    const int ty = kA3Configs[h->config].ty();
+    const int ty = a3d_cfg(h, h->config).ty();
     if (h->maps_ty == ty) return SM_OK;
     switch (h->precision) {
+    case SM_BFP16: return a3d_make_bmaps(h, ty);
     case SM_FP64: return a3d_make_maps<double>(h, ty);
     case SM_FP16: return a3d_make_maps<__half>(h, ty);
     case SM_BF16: return a3d_make_maps<__nv_bfloat16>(h, ty);
@@ -880,6 +1507,9 @@ int a3d_rescale(sm_a3d *h) {
 int a3d_check_err(sm_a3d *h) {
     int e = 0;
     SM_CUDA_TRY(cudaMemcpy(&e, h->err.p, sizeof(int), cudaMemcpyDeviceToHost));
+    if (e == 4)
+        return sm_fail(SM_ESTATE, "a_iso_3d: a block of the 16-bit block storage exceeded its "
+                                  "range (|value| >= 2^114)");
     if (e) return sm_fail(SM_ETIMEOUT, "a_iso_3d step kernel: a bounded wait for a TMA load gave up");
     return SM_OK;
 }
@@ -898,8 +1528,39 @@ size_t a3d_config_smem(int config) {
     }
 }
 
+size_t a3d_bconfig_smem(int config) {
+    switch (config) {
+    case 0: return a3d_bstep_smem<8 * A3_BJ, 4>();
+    case 1: return a3d_bstep_smem<4 * A3_BJ, 4>();
+    case 2: return a3d_bstep_smem<8 * A3_BJ, 5>();
+    case 3: return a3d_bstep_smem<4 * A3_BJ, 6>();
+    default: return a3d_bstep_smem<16 * A3_BJ, 4>();
+    }
+}
+
+int a3d_bready(sm_a3d *h) {
+    switch (h->config) {
+    case 0: return a3d_bready_cfg<8, 4, 2>(h);
+    case 1: return a3d_bready_cfg<4, 4, 3>(h);
+    case 2: return a3d_bready_cfg<8, 5, 1>(h);
+    case 3: return a3d_bready_cfg<4, 6, 3>(h);
+    default: return a3d_bready_cfg<16, 4, 1>(h);
+    }
+}
+
+int a3d_blaunch_step(sm_a3d *h) {
+    switch (h->config) {
+    case 0: return a3d_blaunch_cfg<8, 4, 2>(h);
+    case 1: return a3d_blaunch_cfg<4, 4, 3>(h);
+    case 2: return a3d_blaunch_cfg<8, 5, 1>(h);
+    case 3: return a3d_blaunch_cfg<4, 6, 3>(h);
+    default: return a3d_blaunch_cfg<16, 4, 1>(h);
+    }
+}
+
 size_t a3d_config_smem_prec(int precision, int config) {
     switch (precision) {
+    case SM_BFP16: return a3d_bconfig_smem(config);
     case SM_FP64: return a3d_config_smem<double>(config);
     case SM_FP16: return a3d_config_smem<__half>(config);
     case SM_BF16: return a3d_config_smem<__nv_bfloat16>(config);
@@ -938,22 +1599,35 @@ int a3d_launch_step(sm_a3d *h) {
 
 template <typename S>
 void a3d_launch(sm_a3d *h) {
+    constexpr bool B = std::is_same<S, Bfp16>::value;
     a3d_bind(h, h->cur);
     cudaEvent_t t0 = h->timer.begin(h->stream);
-    const int nstep = a3d_launch_step<S>(h);
+    int nstep;
+    if constexpr (B) nstep = a3d_blaunch_step(h);
+    else nstep = a3d_launch_step<S>(h);
     h->timer.end(t0, h->stream);
     h->cur = 1 - h->cur;
     // sources and receivers act on the state just written
     a3d_bind(h, h->cur);
     h->timer.launches += nstep + (h->src.empty() ? 0 : 1) + (h->rec.empty() ? 0 : 1);
-    if (!h->src.empty())
-        a3d_source_kernel<S><<<1, 32, 0, h->stream>>>(h->args, h->d_src.as<A3Src>(),
-                                                      (int)h->src.size(), h->d_vals.as<double>());
+    if (!h->src.empty()) {
+        if constexpr (B)
+            a3d_bsource_kernel<<<1, 32, 0, h->stream>>>(h->args, h->d_src.as<A3Src>(),
+                                                        (int)h->src.size(), h->d_vals.as<double>());
+        else
+            a3d_source_kernel<S><<<1, 32, 0, h->stream>>>(h->args, h->d_src.as<A3Src>(),
+                                                          (int)h->src.size(), h->d_vals.as<double>());
+    }
     if (!h->rec.empty()) {
         int n = (int)h->rec.size();
-        a3d_gather_kernel<S><<<(n + 127) / 128, 128, 0, h->stream>>>(
-            h->args, h->d_rec.as<A3Rec>(), n, h->d_table.as<int32_t>(),
-            (long long)h->plan.nsteps_max, h->d_traces.as<double>());
+        if constexpr (B)
+            a3d_bgather_kernel<<<(n + 127) / 128, 128, 0, h->stream>>>(
+                h->args, h->d_rec.as<A3Rec>(), n, h->d_table.as<int32_t>(),
+                (long long)h->plan.nsteps_max, h->d_traces.as<double>());
+        else
+            a3d_gather_kernel<S><<<(n + 127) / 128, 128, 0, h->stream>>>(
+                h->args, h->d_rec.as<A3Rec>(), n, h->d_table.as<int32_t>(),
+                (long long)h->plan.nsteps_max, h->d_traces.as<double>());
     }
 }
 
@@ -1007,13 +1681,16 @@ static size_t a3d_mb2(size_t b) { return (b + (2u << 20) - 1) / (2u << 20) * (2u
 extern "C" int sm_a3d_device_bytes(size_t nx2, size_t ny2, size_t nz2, size_t np, int precision,
                                    size_t nrec, size_t nsteps_max, size_t *bytes) {
     if (!bytes) return sm_fail(SM_EINVAL, "sm_a3d_device_bytes: NULL");
-    if (precision < SM_FP32 || precision > SM_BF16)
+    if (precision < SM_FP32 || precision > SM_BFP16)
         return sm_fail(SM_EINVAL, "sm_a3d_device_bytes: unknown precision %d", precision);
     const size_t pitch = round_up(nz2, 32), ncell = nx2 * ny2 * pitch;
     const size_t e = storage_bytes(precision), c = precision == SM_FP64 ? 8 : 4;
+    const size_t pe = precision == SM_BFP16 ? 4 : e;          // CPML memory variables
     const size_t slabs = 2 * (2 * np * ny2 * pitch + nx2 * 2 * np * pitch + nx2 * ny2 * 2 * np);
     size_t b = 8 * a3d_mb2(ncell * e);                        // 4 fields, two sets
-    b += 2 * a3d_mb2(slabs * e);                              // CPML memory variables
+    if (precision == SM_BFP16)                                // their exponents
+        b += 8 * a3d_mb2(nx2 * ((ny2 + A3_BJ - 1) / A3_BJ) * pitch);
+    b += 2 * a3d_mb2(slabs * pe);                             // CPML memory variables
     b += 2 * a3d_mb2(ncell * c);                              // rho, K
     b += a3d_mb2(18 * (nx2 + ny2 + nz2) * c);                 // coefficients
     b += a3d_mb2(nrec * nsteps_max * (sizeof(double) + sizeof(int32_t)));
@@ -1072,7 +1749,7 @@ extern "C" int sm_a3d_create(int device, size_t nx2, size_t ny2, size_t nz2, siz
         if (!coef[c]) return sm_fail(SM_EINVAL, "sm_a3d_create: NULL coefficient array");
     if (!(dx > 0) || !(dy > 0) || !(dz > 0) || !(dt > 0))
         return sm_fail(SM_EINVAL, "sm_a3d_create: spacings and dt must be > 0");
-    if (precision < SM_FP32 || precision > SM_BF16)
+    if (precision < SM_FP32 || precision > SM_BFP16)
         return sm_fail(SM_EINVAL, "sm_a3d_create: unknown precision %d", precision);
     if (ny2 > 65535 * 4 || nx2 > 65535 || (double)nx2 * ny2 * (nz2 + 31) >= 2147483647.0)
         return sm_fail(SM_EINVAL, "sm_a3d_create: grid too large (cells must stay below 2^31)");
@@ -1103,6 +1780,7 @@ extern "C" int sm_a3d_create(int device, size_t nx2, size_t ny2, size_t nz2, siz
     h->dx = dx; h->dy = dy; h->dz = dz; h->dt = dt;
     h->pitch = (int)round_up(nz2, 32);
     h->elem = storage_bytes(precision);
+    if (precision == SM_BFP16) h->config = 0;   // index into the block-storage table
     SM_CUDA_TRY(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
     SM_CUDA_TRY(cudaStreamCreateWithFlags(&h->side, cudaStreamNonBlocking));
     SM_CUDA_TRY(cudaEventCreateWithFlags(&h->ev_fork, cudaEventDisableTiming));
@@ -1116,9 +1794,17 @@ extern "C" int sm_a3d_create(int device, size_t nx2, size_t ny2, size_t nz2, siz
     h->psi_cells[PS_PX] = h->psi_cells[PS_VX] = 2 * np * ny2 * (size_t)h->pitch;
     h->psi_cells[PS_PY] = h->psi_cells[PS_VY] = nx2 * 2 * np * (size_t)h->pitch;
     h->psi_cells[PS_PZ] = h->psi_cells[PS_VZ] = nx2 * ny2 * 2 * np;
+    // block storage keeps the CPML memory variables in FP32
+    const size_t pelem = precision == SM_BFP16 ? 4 : h->elem;
     for (int b = 0; b < 2; ++b)
         for (int p = 0; p < 6; ++p)
-            if ((rc = h->psi[b][p].alloc(h->psi_cells[p] * h->elem))) return rc;
+            if ((rc = h->psi[b][p].alloc(h->psi_cells[p] * pelem))) return rc;
+    if (precision == SM_BFP16) {
+        h->nyb = (ny2 + A3_BJ - 1) / A3_BJ;
+        for (int b = 0; b < 2; ++b)
+            for (int f = 0; f < 4; ++f)
+                if ((rc = h->fe[b][f].alloc(nx2 * h->nyb * (size_t)h->pitch))) return rc;
+    }
     if ((rc = h->rho.alloc(ncell * cb))) return rc;
     if ((rc = h->K.alloc(ncell * cb))) return rc;
     rc = precision == SM_FP64 ? a3d_upload_materials<double>(h.get(), rho, vp, dt, nx2, ny2, nz2)
@@ -1148,6 +1834,7 @@ extern "C" int sm_a3d_create(int device, size_t nx2, size_t ny2, size_t nz2, siz
     a.nx2 = (int)nx2; a.ny2 = (int)ny2; a.nz2 = (int)nz2; a.pitch = h->pitch; a.np = (int)np;
     a.sy = h->pitch;
     a.sx = (int)(ny2 * h->pitch);
+    a.nyb = (int)h->nyb;
     if (precision == SM_FP16 || precision == SM_BF16) {
         if ((rc = h->scaler.init(10, 10))) return rc;
         const size_t N = nx2 * ny2 * nz2;
@@ -1168,7 +1855,7 @@ extern "C" int sm_a3d_create(int device, size_t nx2, size_t ny2, size_t nz2, siz
     for (int f = 0; f < 4; ++f) { a.sc[f] = 1.f; a.isc[f] = 1.f; }
     for (int p = 0; p < 6; ++p) { a.psc[p] = 1.f; a.pisc[p] = 1.f; }
     cudaDeviceGetAttribute(&h->sms, cudaDevAttrMultiProcessorCount, device);
-    a.chunk = a3d_pick_chunk(nx2, ny2, nz2, h->sms, kA3Configs[h->config].ty());
+    a.chunk = a3d_pick_chunk(nx2, ny2, nz2, h->sms, a3d_cfg(h.get(), h->config).ty());
     a3d_bind(h.get(), 0);
     a.rho = h->rho.p;
     a.K = h->K.p;
@@ -1186,8 +1873,10 @@ extern "C" int sm_a3d_reset(sm_a3d_t h) {
     if (int rc = a3d_check(h)) return rc;
     DeviceGuard g(h->device);
     for (int b = 0; b < 2; ++b) {
-        for (int f = 0; f < 4; ++f)
+        for (int f = 0; f < 4; ++f) {
             if (int rc = h->f[b][f].zero(h->stream)) return rc;
+            if (int rc = h->fe[b][f].zero(h->stream)) return rc;
+        }
         for (int p = 0; p < 6; ++p)
             if (int rc = h->psi[b][p].zero(h->stream)) return rc;
     }
@@ -1220,6 +1909,11 @@ extern "C" int sm_a3d_set_sources(sm_a3d_t h, size_t nsrc, const size_t *index, 
         e.q = (long long)((i * h->ny2 + j) * h->pitch + k);
         e.voff = (long long)h->vals.size();
         e.len = (int)length[s];
+        const size_t jb = j / A3_BJ;
+        e.qe = (long long)((i * h->nyb + jb) * h->pitch + k);
+        e.qb = (long long)((i * h->ny2 + jb * A3_BJ) * h->pitch + k);
+        e.nb = (int)std::min<size_t>(A3_BJ, h->ny2 - jb * A3_BJ);
+        e.rs = (int)(j - jb * A3_BJ);
         for (size_t t = 0; t < length[s]; ++t) h->vals.push_back(scale * fct[s * stride + t]);
         h->src.push_back(e);
     }
@@ -1267,6 +1961,7 @@ extern "C" int sm_a3d_set_receivers(sm_a3d_t h, size_t nrec, const size_t *index
         size_t j = ij % h->ny2, i = ij / h->ny2;
         A3Rec e{};
         e.q = (long long)((i * h->ny2 + j) * h->pitch + k);
+        e.qe = (long long)((i * h->nyb + j / A3_BJ) * h->pitch + k);
         e.field = f;
         e.group = h->plan.group_of[r];
         e.out = (long long)r * (long long)h->plan.max_samples;
@@ -1355,7 +2050,11 @@ int a3d_graph(sm_a3d *h, cudaGraphExec_t *out) {
 
 template <typename S>
 int a3d_run_t(sm_a3d *h, size_t nsteps) {
-    if (int rc = a3d_ready<S>(h)) return rc;
+    if constexpr (std::is_same<S, Bfp16>::value) {
+        if (int rc = a3d_bready(h)) return rc;
+    } else {
+        if (int rc = a3d_ready<S>(h)) return rc;
+    }
     const size_t G = (size_t)h->graph_steps;
     const size_t per_step =
         (size_t)a3d_step_kernels(h) + (h->src.empty() ? 0 : 1) + (h->rec.empty() ? 0 : 1);
@@ -1391,6 +2090,7 @@ extern "C" int sm_a3d_run(sm_a3d_t h, size_t nsteps) {
     case SM_FP64: rc = a3d_run_t<double>(h, nsteps); break;
     case SM_FP16: rc = a3d_run_t<__half>(h, nsteps); break;
     case SM_BF16: rc = a3d_run_t<__nv_bfloat16>(h, nsteps); break;
+    case SM_BFP16: rc = a3d_run_t<Bfp16>(h, nsteps); break;
     default: rc = a3d_run_t<float>(h, nsteps); break;
     }
     if (rc) return rc;
@@ -1453,7 +2153,7 @@ extern "C" int sm_a3d_autotune(sm_a3d_t h, int trial_steps, int *config, int *ch
         SM_CUDA_TRY(cudaEventCreate(&e1));
         const bool timing = h->timer.on;
         h->timer.on = false;
-        for (int c = 0; c < kA3NumConfigs && rc == SM_OK; ++c) {
+        for (int c = 0; c < a3d_ncfg(h) && rc == SM_OK; ++c) {
             if (a3d_config_smem_prec(h->precision, c) > (size_t)lim) continue;
             for (int ch : {0, 16, 32, 64}) {
                 if ((rc = sm_a3d_set_config(h, c)) || (rc = sm_a3d_set_chunk(h, ch))) break;
@@ -1554,6 +2254,18 @@ extern "C" int sm_a3d_get_field(sm_a3d_t h, int comp, double *out) {
     const size_t ncell = h->nx2 * h->ny2 * (size_t)h->pitch;
     std::vector<unsigned char> buf(ncell * h->elem);
     SM_CUDA_TRY(cudaMemcpy(buf.data(), h->f[h->cur][f].p, buf.size(), cudaMemcpyDeviceToHost));
+    if (a3d_isb(h)) {   // mantissa times 2^(e8 - 126) of the cell's block
+        std::vector<uint8_t> ex(h->fe[h->cur][f].bytes);
+        SM_CUDA_TRY(cudaMemcpy(ex.data(), h->fe[h->cur][f].p, ex.size(), cudaMemcpyDeviceToHost));
+        const int16_t *mm = reinterpret_cast<const int16_t *>(buf.data());
+        for (size_t i = 0; i < h->nx2; ++i)
+            for (size_t j = 0; j < h->ny2; ++j)
+                for (size_t k = 0; k < h->nz2; ++k)
+                    out[(i * h->ny2 + j) * h->nz2 + k] = bfp_value_host(
+                        mm[(i * h->ny2 + j) * h->pitch + k],
+                        ex[(i * h->nyb + j / A3_BJ) * h->pitch + k]);
+        return SM_OK;
+    }
     for (size_t i = 0; i < h->nx2; ++i)
         for (size_t j = 0; j < h->ny2; ++j)
             for (size_t k = 0; k < h->nz2; ++k)
@@ -1571,6 +2283,26 @@ extern "C" int sm_a3d_set_field(sm_a3d_t h, int comp, const double *in) {
     SM_CUDA_TRY(cudaStreamSynchronize(h->stream));
     const size_t ncell = h->nx2 * h->ny2 * (size_t)h->pitch;
     std::vector<unsigned char> buf(ncell * h->elem, 0);
+    if (a3d_isb(h)) {   // each block of A3_BJ rows encoded as the kernels encode it
+        std::vector<uint8_t> ex(h->fe[h->cur][f].bytes, 0);
+        int16_t *mm = reinterpret_cast<int16_t *>(buf.data());
+        for (size_t i = 0; i < h->nx2; ++i)
+            for (size_t jb = 0; jb < h->nyb; ++jb)
+                for (size_t k = 0; k < h->nz2; ++k) {
+                    const size_t ja = jb * A3_BJ, je = std::min(ja + A3_BJ, h->ny2);
+                    float mx = 0.f;
+                    for (size_t j = ja; j < je; ++j)
+                        mx = std::max(mx, std::fabs((float)in[(i * h->ny2 + j) * h->nz2 + k]));
+                    const unsigned e8 = bfp_e8_host(mx);
+                    ex[(i * h->nyb + jb) * h->pitch + k] = (uint8_t)e8;
+                    for (size_t j = ja; j < je; ++j)
+                        mm[(i * h->ny2 + j) * h->pitch + k] =
+                            bfp_man_host((float)in[(i * h->ny2 + j) * h->nz2 + k], e8);
+                }
+        SM_CUDA_TRY(cudaMemcpy(h->fe[h->cur][f].p, ex.data(), ex.size(), cudaMemcpyHostToDevice));
+        SM_CUDA_TRY(cudaMemcpy(h->f[h->cur][f].p, buf.data(), buf.size(), cudaMemcpyHostToDevice));
+        return SM_OK;
+    }
     for (size_t i = 0; i < h->nx2; ++i)
         for (size_t j = 0; j < h->ny2; ++j)
             for (size_t k = 0; k < h->nz2; ++k)
@@ -1634,9 +2366,9 @@ extern "C" int sm_a3d_kernel_stats(sm_a3d_t h, int reset, double *update_ms,
 
 extern "C" int sm_a3d_set_config(sm_a3d_t h, int config) {
     if (int rc = a3d_check(h)) return rc;
-    if (config < 0 || config >= kA3NumConfigs)
+    if (config < 0 || config >= a3d_ncfg(h))
         return sm_fail(SM_EINVAL, "sm_a3d_set_config: config %d not in [0, %d)", config,
-                       kA3NumConfigs);
+                       a3d_ncfg(h));
     int maxsm = 0;
     cudaDeviceGetAttribute(&maxsm, cudaDevAttrMaxSharedMemoryPerBlockOptin, h->device);
     if (a3d_config_smem_prec(h->precision, config) > (size_t)maxsm)
@@ -1644,7 +2376,7 @@ extern "C" int sm_a3d_set_config(sm_a3d_t h, int config) {
                                   "in this precision (device limit %d)", config,
                        a3d_config_smem_prec(h->precision, config), maxsm);
     h->config = config;
-    h->args.chunk = a3d_pick_chunk(h->nx2, h->ny2, h->nz2, h->sms, kA3Configs[config].ty());
+    h->args.chunk = a3d_pick_chunk(h->nx2, h->ny2, h->nz2, h->sms, a3d_cfg(h, config).ty());
     h->graph_epoch++;
     // maps are rebuilt for the new tile height at the next run
     return SM_OK;
@@ -1653,7 +2385,7 @@ extern "C" int sm_a3d_set_config(sm_a3d_t h, int config) {
 extern "C" int sm_a3d_set_chunk(sm_a3d_t h, int chunk) {
     if (int rc = a3d_check(h)) return rc;
     if (chunk <= 0)
-        h->args.chunk = a3d_pick_chunk(h->nx2, h->ny2, h->nz2, h->sms, kA3Configs[h->config].ty());
+        h->args.chunk = a3d_pick_chunk(h->nx2, h->ny2, h->nz2, h->sms, a3d_cfg(h, h->config).ty());
     else
         h->args.chunk = chunk > A3_CHMAX ? A3_CHMAX : (chunk > (int)h->nx2 ? (int)h->nx2 : chunk);
     h->graph_epoch++;
@@ -1663,6 +2395,6 @@ extern "C" int sm_a3d_set_chunk(sm_a3d_t h, int chunk) {
 extern "C" int sm_a3d_get_config(sm_a3d_t h, int *config, int *nconfigs) {
     if (int rc = a3d_check(h)) return rc;
     if (config) *config = h->config;
-    if (nconfigs) *nconfigs = kA3NumConfigs;
+    if (nconfigs) *nconfigs = a3d_ncfg(h);
     return SM_OK;
 }

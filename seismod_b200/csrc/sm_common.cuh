@@ -84,9 +84,71 @@ inline size_t storage_bytes(int precision) {
     switch (precision) {
     case SM_FP64: return 8;
     case SM_FP16:
-    case SM_BF16: return 2;
+    case SM_BF16:
+    case SM_BFP16: return 2;
     default: return 4;
     }
+}
+
+// ---------------------------------------------------------------------------
+// 16-bit block floating point (SM_BFP16; no counterpart in the reference).
+// A block of values shares one 8-bit exponent byte e8; each value is a
+// 16-bit two's-complement mantissa m with value m * 2^(e8 - 126).  The
+// encoder takes e8 from the FP32 bits of the block's largest magnitude M,
+// so that M maps into [2^14, 2^15) (15 significant bits and a sign for the
+// largest value; a block whose M would round up to 2^15 takes the next
+// exponent); e8 = 0 is the finest scale, 2^-126, which also stands for a
+// block of zeros (the zero fill of an out-of-grid TMA read decodes to 0).
+// Arithmetic stays FP32.  Decoding and encoding use the float magic
+// constant 1.5 * 2^23, whose ulp is 1: adding it to an integer or rounding
+// a product onto it is exact, so no conversion instruction is needed.
+// ---------------------------------------------------------------------------
+struct Bfp16 {};     // storage tag of the block-floating-point kernels
+struct BDec {
+    float sc, off;   // value = (1.5 * 2^23 + m) * sc + off
+};
+__device__ __forceinline__ BDec bfp_dec(unsigned e8) {
+    const float sc = __int_as_float((int)((e8 + 1u) << 23));   // 2^(e8 - 126)
+    return BDec{sc, __fmul_rn(-12582912.0f, sc)};
+}
+// m: the mantissa, sign-extended
+__device__ __forceinline__ float bfp_val(int m, BDec d) {
+    return __fmaf_rn(__int_as_float(m + 0x4B400000), d.sc, d.off);
+}
+// e8 of a block from the largest |value|'s bits (sign cleared); *over is set
+// when the block exceeds the format's range (|value| >= 2^114)
+__device__ __forceinline__ unsigned bfp_e8(unsigned mxbits, bool *over) {
+    int eb = (int)((mxbits + 0x100u) >> 23);   // the next exponent from M >= 2^E (1 - 2^-16)
+    *over = eb > 240;
+    eb = eb < 15 ? 15 : (eb > 240 ? 240 : eb);
+    return (unsigned)(eb - 15);
+}
+// 2^(126 - e8): value * scale lies in (-32767.5, 32767.5)
+__device__ __forceinline__ float bfp_escale(unsigned e8) {
+    return __int_as_float((int)((253u - e8) << 23));
+}
+// round-half-even mantissa of value * scale (the low 16 bits of the sum)
+__device__ __forceinline__ short bfp_man(float v, float esc) {
+    return (short)__float_as_int(__fmaf_rn(v, esc, 12582912.0f));
+}
+__device__ __forceinline__ unsigned bfp_absbits(float v) { return __float_as_uint(v) & 0x7fffffffu; }
+
+// host-side counterparts (the same rules, for field reads and writes)
+inline unsigned bfp_e8_host(float mx) {
+    unsigned b;
+    std::memcpy(&b, &mx, 4);
+    b &= 0x7fffffffu;
+    int eb = (int)((b + 0x100u) >> 23);
+    eb = eb < 15 ? 15 : (eb > 240 ? 240 : eb);
+    return (unsigned)(eb - 15);
+}
+inline double bfp_value_host(int16_t m, unsigned e8) { return std::ldexp((double)m, (int)e8 - 126); }
+inline int16_t bfp_man_host(float v, unsigned e8) {
+    const float x = std::ldexp(v, 126 - (int)e8);   // exact (power-of-two scale)
+    float r = std::nearbyint(x);                     // round half even
+    if (r > 32767.f) r = 32767.f;
+    if (r < -32768.f) r = -32768.f;
+    return (int16_t)r;
 }
 
 // ---------------------------------------------------------------------------

@@ -61,13 +61,16 @@ def eiso_receivers(p):
     return out
 
 
-def run_eiso_oracle(p, shot=0, nsteps=None, fields_at=None):
+def run_eiso_oracle(p, shot=0, nsteps=None, fields_at=None, bfp_block=0, bfp_axis="x"):
     """FP64 oracle run.  Returns (traces list of np arrays, times list,
-    optional dict of padded fields after the last step)."""
+    optional dict of padded fields after the last step).  bfp_block > 0
+    rounds the stored state to 16-bit block floating point (checker mode)."""
     s = eiso_setup(p)
     n = s["nsteps"] if nsteps is None else nsteps
     o = O.EIso(p.nx, p.nz, p.npml, p.h, s["dt"], s["la"], s["mu"], s["l2m"], s["b"],
                s["bm"], s["d"], s["dh"], s["dH"])
+    if bfp_block:
+        o.set_bfp(bfp_block, bfp_axis)
     srcs = eiso_sources(p, shot)
     recs = eiso_receivers(p)
     tr = [[] for _ in recs]
@@ -112,15 +115,15 @@ def a3d_index(p, x, y, z):
     return (i * ny2 + j) * nz2 + k
 
 
-def run_a3d_oracle(p, nsteps=None, fields_at=None, bfp_block=0):
+def run_a3d_oracle(p, nsteps=None, fields_at=None, bfp_block=0, bfp_axis="y"):
     """FP64 oracle run of an a_iso_3d shot; bfp_block > 0 rounds every stored
-    value to 16-bit block floating point with blocks of that many z cells
-    (the storage-rounding checker mode)."""
+    value to 16-bit block floating point with blocks of that many cells along
+    bfp_axis ("y" or "z"; the storage-rounding checker mode)."""
     s = a3d_setup(p)
     n = s["nsteps"] if nsteps is None else nsteps
     o = O.A3D(s["vpp"], s["rhop"], *p.d, s["dt"], s["coef"])
     if bfp_block:
-        o.set_bfp(bfp_block)
+        o.set_bfp(bfp_block, bfp_axis)
     A = [q[1] for q in p.sources]
     f = [q[2] for q in p.sources]
     fct = O.src_fct(A, f, p.dt, 1.0)

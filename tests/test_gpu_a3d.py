@@ -134,3 +134,92 @@ def test_16bit_storage_stays_in_range_and_close_to_fp64(precision):
     again = api.run_a3d(p, precision)
     for a, b in zip(got, again):
         np.testing.assert_array_equal(a, b)
+
+
+# ---------------------------------------------------------------------------
+# Block floating point (SM_BFP16): 16-bit mantissas sharing one exponent per
+# 4 consecutive y rows of a z column, FP32 arithmetic.  The oracle's
+# storage-rounding mode applies the same rounding to its FP64 state, so it
+# predicts what the storage alone costs.  Bounds: each stored value is
+# rounded to 2^-16 of its block's largest magnitude once per step, so 4 steps
+# from a random state stay within 1e-4 of the FP64 oracle; the device and
+# the rounding oracle differ only where FP32 and FP64 arithmetic fall on
+# opposite sides of a rounding boundary (2e-5).  Traces of whole shots:
+# the 1e-3 gate against FP64.
+# ---------------------------------------------------------------------------
+BFP_BLOCK = 4
+
+
+@pytest.mark.parametrize("shape", [((12, 10, 14), 2), ((9, 17, 33), 3), ((40, 50, 90), 4),
+                                   ((40, 50, 90), 0)])
+def test_bfp16_steps_from_random_state(shape):
+    (nx, ny, nz), npml = shape
+    rng = np.random.default_rng(nx * ny + nz + 1)
+    vp = 1500 + 3000 * rng.random((nx, ny, nz))
+    rho = 1800 + 600 * rng.random((nx, ny, nz))
+    p = W.A3DProblem(vp, rho, (4.0, 5.0, 3.0), npml, 0.2, 1.0, [("Bulk", 1.0, 30.0, 0, 0, 0)],
+                     [], Rc=1e-3, kappa_max=2.0, alpha_max=1)
+    p.dt_ms = 0.5 / (vp.max() * np.sqrt(1 / 16 + 1 / 25 + 1 / 9)) * 1e3
+    s = H.a3d_setup(p)
+    plain = O.A3D(s["vpp"], s["rhop"], *p.d, s["dt"], s["coef"])
+    rounded = O.A3D(s["vpp"], s["rhop"], *p.d, s["dt"], s["coef"])
+    rounded.set_bfp(BFP_BLOCK, "y")
+    dev = api.A3DDevice(s["vpp"], s["rhop"], npml, p.d, s["dt"], s["coef"], "bfp16")
+    shp = s["vpp"].shape
+    for f, sc in (("p", 1e5), ("vx", 1e-2), ("vy", 1e-2), ("vz", 1e-2)):
+        dev.set_field(f, sc * rng.standard_normal(shp))
+        a = dev.get_field(f)           # the stored (rounded) start state
+        plain.set(f, a)
+        rounded.set(f, a)
+    for _ in range(4):
+        for o in (plain, rounded):
+            o.velocity()
+            o.pressure()
+    dev.run(4)
+    for f in ("p", "vx", "vy", "vz"):
+        got = dev.get_field(f)
+        assert O.rel_l2(got, rounded.get(f)) < 2e-5, (f, O.rel_l2(got, rounded.get(f)))
+        assert O.rel_l2(got, plain.get(f)) < 1e-4, (f, O.rel_l2(got, plain.get(f)))
+    dev.close()
+
+
+def test_bfp16_every_launch_configuration_gives_identical_results():
+    p = W.cfg1(n=120, npml=6, nsteps=90, seed=8, rec_stride=10, nrec_side=12)
+    dev, n = api.a3d_device(p, "bfp16")
+    _, ncfg = dev.get_config()
+    base = None
+    for c in range(ncfg):
+        dev.reset()
+        try:
+            dev.set_config(c)
+        except Exception:
+            continue
+        dev.run(n)
+        tr = dev.traces_array()
+        f = dev.get_field("p")
+        if base is None:
+            base = (tr, f)
+        else:
+            np.testing.assert_array_equal(tr, base[0])
+            np.testing.assert_array_equal(f, base[1])
+    dev.close()
+
+
+def test_bfp16_shot_within_gate_and_as_the_rounding_oracle_predicts():
+    # the cfg1 model family at 48^3 (+2x8 CPML), 300 steps, 16x16 surface
+    # receivers, Vz and a pressure record
+    p = W.cfg1(n=48, npml=8, nsteps=300, seed=21, rec_stride=3, nrec_side=16)
+    p.receivers = p.receivers + [("P", 60.0, 60.0, 60.0, 0.0, p.dt_ms)]
+    got = api.run_a3d(p, "bfp16")
+    assert all(np.isfinite(t).all() for t in got)
+    ref = api.run_a3d(p, "fp64")
+    err = H.rel_l2(got, ref)
+    assert err < 1e-3, err
+    plain, _, _ = H.run_a3d_oracle(p)
+    pred, _, _ = H.run_a3d_oracle(p, bfp_block=BFP_BLOCK, bfp_axis="y")
+    predicted = H.rel_l2(pred, plain)
+    assert 0.5 * predicted < err < 2.0 * predicted, (err, predicted)
+    # deterministic: a second run reproduces the first bit for bit
+    again = api.run_a3d(p, "bfp16")
+    for a, b in zip(got, again):
+        np.testing.assert_array_equal(a, b)

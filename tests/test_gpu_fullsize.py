@@ -8,6 +8,8 @@ the 32-bit index arithmetic are covered at scale:
   a_iso_3d 256^3 (+2x16 CPML = 288^3)   random state, every field after 6 steps;
                                         a shot of 300 steps, 16,384 receivers
   a_iso_3d 512^3 (+2x16 CPML = 544^3)   random state, every field after 4 steps
+  both a_iso_3d shots whole (1000 / 2000 steps) in 16-bit block storage,
+                                        traces within 1e-3 of FP64
   e_iso 1000 x 500 (+2x20 PML), 64 shots in one batched handle: random state
                                         of shots 0 and 63, every field and
                                         split part after 4 steps; the shots'
@@ -137,3 +139,21 @@ def test_eiso_1040x540_batched_64_shots_traces():
         assert max(np.abs(a).max() for a in orc) > 0.0
         assert H.rel_l2(got, orc) < TOL_FP32, shot
     dev.close()
+
+
+# 16-bit block storage on the benchmarked shots: the whole 1000-step 288^3
+# shot and the 2000-step 544^3 shot, traces against an FP64 run of the same
+# shot on the device (which the tests above pin to the oracle at 1e-10 on
+# small grids), at the 1e-3 gate
+def test_a3d_288cube_bfp16_whole_shot_within_1e_3():
+    p = W.cfg1()
+    got = api.run_a3d(p, "bfp16")
+    ref = api.run_a3d(p, "fp64")
+    assert H.rel_l2(got, ref) < 1e-3
+
+
+def test_a3d_544cube_bfp16_whole_shot_within_1e_3():
+    p = W.cfg3()
+    got = api.run_a3d(p, "bfp16")
+    ref = api.run_a3d(p, "fp64")
+    assert H.rel_l2(got, ref) < 1e-3
