@@ -116,19 +116,23 @@ class Clocks:
 
 def a3d_bytes_per_step(p, s, m=4, psi=None):
     """Ncell (8 s + 2 m) + sum over axes of N_slab 4 p (state R+W, rho & K read
-    once, both CPML memory variables R+W on their slabs)."""
+    once, both CPML memory variables R+W on their slabs).  Block storage:
+    s = 2 + 1/4 (a mantissa and a quarter of an exponent byte per value),
+    p = 4 (FP32 memory variables)."""
     psi = s if psi is None else psi
     n2 = [n + 2 * p.npml for n in p.shape]
     ncell = n2[0] * n2[1] * n2[2]
     slab = sum(2 * p.npml * (ncell // n2[a]) for a in range(3))
-    return ncell * (8 * s + 2 * m) + slab * 4 * psi
+    return int(ncell * (8 * s + 2 * m) + slab * 4 * psi)
 
 
-def eiso_bytes_per_step(p, nshots, s, m=4):
-    """shots (N_int 10 s + N_pml 20 s) + N_all 3 m."""
+def eiso_bytes_per_step(p, nshots, s, m=4, split=None):
+    """shots (N_int 10 s + N_pml 20 p) + N_all 3 m, p the split parts' width
+    (= s, or 4 for block storage, whose split parts stay FP32)."""
+    split = s if split is None else split
     nall = p.cells
     nint = p.nx * p.nz
-    return nshots * (nint * 10 * s + (nall - nint) * 20 * s) + nall * 3 * m
+    return int(nshots * (nint * 10 * s + (nall - nint) * 20 * split) + nall * 3 * m)
 
 
 def ecyl_bytes_per_step(p, s, m=4):
@@ -249,11 +253,11 @@ def run_ours(args, rank, world, local_rank, torch, dist):
     from seismod_b200 import api
     kind, p, desc = make_workload(args.workload, args.size)
     prec = args.precision
-    sbytes = {"fp32": 4, "fp64": 8, "fp16": 2, "bf16": 2}[prec]
+    sbytes = {"fp32": 4, "fp64": 8, "fp16": 2, "bf16": 2, "bfp16": 2.25}[prec]
     mbytes = 8 if prec == "fp64" else 4
     nshots = len(p.shots) if kind == "eiso" else 1
     if kind == "a3d":
-        bps = a3d_bytes_per_step(p, sbytes, mbytes)
+        bps = a3d_bytes_per_step(p, sbytes, mbytes, 4 if prec == "bfp16" else None)
         cells = p.cells
     elif kind == "ecyl":
         bps = ecyl_bytes_per_step(p, sbytes, mbytes)
@@ -315,18 +319,110 @@ def precision_side(kind, p, local_rank, K):
         run = api.run_ecyl
     ref64 = run(p, "fp64", local_rank)
     res = {}
-    for prec in (("fp32",) if kind == "ecyl" else ("fp32", "fp16", "bf16")):
+    for prec in (("fp32",) if kind == "ecyl" else ("fp32", "bfp16", "fp16", "bf16")):
         try:
             tr = run(p, prec, local_rank)
             err = trace_err(tr, ref64)
             dev, _ = device_for(kind, p, prec, local_rank)
             dev.run(10)
-            ms = time_steps(dev, min(K, 500), torch)
+            ms = time_steps(dev, 200, torch)
             dev.close()
-            res[prec] = {"trace_err_vs_fp64": err, "ms_per_step": round(ms / min(K, 500), 5)}
+            res[prec] = {"trace_err_vs_fp64": err, "ms_per_step": round(ms / 200, 5)}
         except Exception as e:  # report, do not hide
             res[prec] = {"error": str(e)[:200]}
     return res
+
+
+def timed_rate(kind, p, prec, dev_id, steps, shots=None):
+    """(ms per step of the whole step, mean step-kernel ms per step) of an
+    autotuned, graph-replayed handle: 5 warm-up steps, then `steps` steps
+    timed with CUDA events on the handle's stream, then the same number with
+    per-launch events around the step kernel."""
+    import torch
+    dev, _ = device_for(kind, p, prec, dev_id, shots)
+    dev.run(5)
+    dev.sync()
+    ms = time_steps(dev, steps, torch) / steps
+    dev.set_timing(True)
+    dev.run(steps)
+    kms, kn, _ = dev.kernel_stats(reset=True)
+    dev.set_timing(False)
+    dev.close()
+    return ms, kms / max(kn, 1)
+
+
+def headline(local_rank, cfg1_precisions):
+    """The metric's comparison, measured in the default run: the plain
+    single-shot FP32 form against the batched forms (64 shots of the 1040 x
+    540 e_iso model in one handle, FP32 and 16-bit block storage) in shots/s,
+    each form's trace error against an FP64 run of the same shot, and the
+    roofline fraction of the batched step kernels; the a_iso_3d shots in FP32
+    and block storage (256^3 from the main run, 512^3 here); the 400 x 400
+    e_iso shot.  Step counts are fixed (not --steps) so every entry is a
+    stable rate; whole shots (2000 / 1500 steps) give the trace errors."""
+    from seismod_b200 import api
+    from seismod_b200 import workloads as W
+    hbm, how = peaks()
+    out = {"peak_gbs": hbm, "peak_source": how}
+    # ---- e_iso 1000 x 500 (+2x20 PML), 64 shots, 2000 steps ----
+    p = W.cfg2()
+    n = api.nsteps(p.duration, p.dt)
+    nsh = len(p.shots)
+    ref = {s: api.run_eiso(p, "fp64", [s], local_rank)[0] for s in (0, nsh - 1)}
+    e = {}
+    ms1, _ = timed_rate("eiso", p, "fp32", local_rank, 400, shots=[0])
+    err1 = trace_err(api.run_eiso(p, "fp32", [0], local_rank)[0], ref[0])
+    sps1 = 1.0 / (ms1 * 1e-3 * n)
+    e["single_shot_fp32"] = {"ms_per_step": round(ms1, 5), "shots_per_s": round(sps1, 3),
+                             "trace_err_vs_fp64": err1,
+                             "l2": "state of one shot fits in L2 (no flush): favours this "
+                                   "baseline, so the batched ratios are lower bounds"}
+    for prec in ("fp32", "bfp16"):
+        ms, kms = timed_rate("eiso", p, prec, local_rank, 200)
+        batch = api.run_eiso(p, prec, None, local_rank)
+        err = max(trace_err(batch[s], ref[s]) for s in ref)
+        bps = eiso_bytes_per_step(p, nsh, 2.25 if prec == "bfp16" else 4.0, 4,
+                                  4.0 if prec == "bfp16" else None)
+        sps = nsh / (ms * 1e-3 * n)
+        e[f"batched_{prec}"] = {
+            "ms_per_step": round(ms, 5), "shots_per_s": round(sps, 3),
+            "speedup_vs_single_fp32": round(sps / sps1, 3), "trace_err_vs_fp64": err,
+            "kernel_ms_per_step": round(kms, 5), "algorithmic_bytes_per_step": bps,
+            "roofline_frac": round(bps / (kms * 1e-3) / 1e9 / hbm, 4),
+            "l2": "inputs larger than L2"}
+    out["eiso_1040x540_64shots"] = e
+    b = e["batched_bfp16"]
+    out["batched_bfp16_vs_single_fp32"] = {
+        "shots_per_s_ratio": b["speedup_vs_single_fp32"],
+        "trace_err_vs_fp64": b["trace_err_vs_fp64"],
+        "meets_2x_at_1e-3": bool(b["speedup_vs_single_fp32"] >= 2.0 and b["trace_err_vs_fp64"] <= 1e-3)}
+    # ---- a_iso_3d 256^3 (the main run's shot) ----
+    if cfg1_precisions:
+        out["a3d_288cube"] = {k: cfg1_precisions[k] for k in ("fp32", "bfp16") if k in cfg1_precisions}
+    # ---- a_iso_3d 512^3 (+2x16 CPML = 544^3), 2000 steps ----
+    q = W.cfg3()
+    ref3 = api.run_a3d(q, "fp64", local_rank)
+    a = {}
+    for prec in ("fp32", "bfp16"):
+        ms, kms = timed_rate("a3d", q, prec, local_rank, 100)
+        err = trace_err(api.run_a3d(q, prec, local_rank), ref3)
+        sb = 2.25 if prec == "bfp16" else 4.0
+        bps = a3d_bytes_per_step(q, sb, 4, 4 if prec == "bfp16" else None)
+        a[prec] = {"ms_per_step": round(ms, 5), "gcell_per_s": round(q.cells / (ms * 1e-3) / 1e9, 3),
+                   "shots_per_s": round(1.0 / (ms * 1e-3 * 2000), 4),
+                   "trace_err_vs_fp64": err, "kernel_ms_per_step": round(kms, 5),
+                   "algorithmic_bytes_per_step": bps,
+                   "roofline_frac": round(bps / (kms * 1e-3) / 1e9 / hbm, 4),
+                   "l2": "inputs larger than L2"}
+    out["a3d_544cube_2000steps"] = a
+    del q, ref3
+    # ---- e_iso 400 x 400 (+2x20 PML), one shot, 1500 steps ----
+    c0 = W.cfg0()
+    ms0, _ = timed_rate("eiso", c0, "fp32", local_rank, 1500)
+    out["eiso_440sq_single_fp32"] = {
+        "ms_per_step": round(ms0, 5), "gcell_per_s": round(c0.cells / (ms0 * 1e-3) / 1e9, 3),
+        "l2": "state fits in L2 (launch-bound shot; no flush)"}
+    return out
 
 
 def batching_side(p, local_rank, K, batched_ms):
@@ -558,8 +654,11 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="a3d",
                     choices=["a3d", "a3d512", "eiso", "eiso1", "ecyl", "serve", "serve_overload"])
-    ap.add_argument("--precision", default="fp32", choices=["fp32", "fp64", "fp16", "bf16"])
+    ap.add_argument("--precision", default="fp32",
+                    choices=["fp32", "fp64", "fp16", "bf16", "bfp16"])
     ap.add_argument("--no-side", action="store_true", help="skip precision / CPU side runs")
+    ap.add_argument("--no-headline", action="store_true",
+                    help="skip the batched / 512^3 / 400^2 comparison of the default run")
     ap.add_argument("--no-tune", action="store_true", help="default launch configuration")
     ap.add_argument("--group", action="store_true",
                     help="serve workloads: running e_iso requests take their slices together "
@@ -602,6 +701,11 @@ def main():
         out["batching"] = batching_side(p, local_rank, args.steps, out["ms_per_step"])
     if rank == 0 and not args.no_side:
         out["precisions"] = precision_side(kind, p, local_rank, args.steps)
+        if args.workload == "a3d" and args.size is None and not args.no_headline:
+            try:
+                out["headline"] = headline(local_rank, out["precisions"])
+            except Exception as e:  # report, do not hide
+                out["headline"] = {"error": str(e)[:300]}
         out["e2e"] = e2e(kind, p, args.steps, local_rank)
         steps = 12 if kind == "a3d" else (20 if kind == "ecyl" else 200)
         rate, sample = reference_rate(kind, p, steps)

@@ -445,6 +445,8 @@ void orc_eiso_set(orc_eiso *o, int field, int part, const double *in)
     size_t N = o->NX * o->NZ;
     double *dst = part == ORC_TOTAL ? o->f[field] : (part == ORC_XPART ? o->fx[field] : o->fz[field]);
     memcpy(dst, in, N * sizeof(double));
+    /* block storage holds the frame's totals as stored values of their own */
+    if (o->bfp_block && part == ORC_TOTAL) return;
     for (size_t q = 0; q < N; ++q) {
         long X = (long)(q / o->NZ), Z = (long)(q % o->NZ);
         if (!e_interior(o, X, Z)) o->f[field][q] = o->fx[field][q] + o->fz[field][q];

@@ -72,6 +72,12 @@ struct EisoArgs {
     const void *mat[5];
     const void *prof;
     float sc[5], isc[5];
+    // block-floating-point storage: exponent bytes of the set read and the
+    // set written, [field][shot][nxb][pitch]; estride bytes per field
+    void *fe;
+    void *feo;
+    long long estride;
+    int nxb;
 };
 
 __device__ __forceinline__ bool e_inside(const EisoArgs &a, int X, int Z) {
@@ -619,6 +625,304 @@ __global__ void __launch_bounds__(32 * W, MINB) eiso_slabg_kernel(const EisoArgs
 }
 
 // ---------------------------------------------------------------------------
+// Block-floating-point slab step (SM_BFP16).  The slab step above with the
+// five wavefields stored as 16-bit mantissas sharing one exponent byte per
+// block of EB consecutive x rows of one z column ([field][shot][nxb][pitch]
+// bytes, nxb = ceil(NX / EB)); the frame's split parts and the materials
+// stay FP32 and the arithmetic is the FP32 path's.  A warp's lane marches
+// one z column down the slab, so each block is held by one thread: its
+// exponent is the maximum over that thread's registers, no exchange across
+// lanes.  The slab owns the rows [X0, X0 + TX) of every field, vx included
+// (the FP32 slab step stores vx one row down, X0+1 .. X0+TX: a vx block
+// would then straddle two CTAs); vx(X0) is the value the neighbouring slab
+// computes too, bit for bit.  The stress update reads the unrounded
+// velocities of the step; only the state the step stores is rounded.
+// ---------------------------------------------------------------------------
+#define EISO_EB 4
+
+struct EisoBMaps {
+    CUtensorMap f;   // mantissas of the old set: (z, x, shot, field), box (BW, TX+2, 1, 5)
+    CUtensorMap e;   // exponents of the old set: (z, xblock, shot, field), box (BWE, TX/EB+2, 1, 5)
+};
+
+template <int W, int TX>
+struct ESlabB {
+    static_assert(TX % EISO_EB == 0, "slab rows must be whole blocks");
+    static constexpr int HS = 8;                 // 16 bytes of int16
+    static constexpr int RX = TX + 2;
+    static constexpr int NB = TX / EISO_EB + 2;  // blocks in the box: above, own, below
+    static constexpr int BW = (30 * W + 2 + HS - 1 + HS - 1) / HS * HS;
+    static constexpr int BWE = (30 * W + 17 + 15) / 16 * 16;   // bytes, start rounded to 16
+    static_assert(BW <= 256 && BWE <= 256, "TMA box dimension");
+    static constexpr size_t al(size_t x) { return (x + 127) / 128 * 128; }
+    static constexpr size_t oE = al(5 * (size_t)RX * BW * 2);
+    static constexpr size_t oBar = oE + al(5 * (size_t)NB * BWE);
+    static constexpr size_t bytes = oBar + 16;
+    static constexpr unsigned tx = (unsigned)(5 * RX * BW * 2 + 5 * NB * BWE);
+};
+
+template <int W, int TX>
+__device__ __forceinline__ void eiso_bslab_body(const EisoArgs &a, const CUtensorMap *fmap,
+                                                const CUtensorMap *emap, int bx, int by, int shot,
+                                                unsigned char *smem) {
+    using C = float;
+    using L = ESlabB<W, TX>;
+    constexpr int EB = EISO_EB;
+    const unsigned full = 0xffffffffu;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    if ((bx | by | shot | threadIdx.x) == 0) ++*a.step;
+    const int16_t *fbox = reinterpret_cast<const int16_t *>(smem);
+    const uint8_t *ebox = smem + L::oE;
+    uint64_t *bar = reinterpret_cast<uint64_t *>(smem + L::oBar);
+    const int Zc = bx * W * 30;
+    const int X0 = by * TX;
+    const int X1 = min(X0 + TX, a.NX);
+    const int zs = (Zc - 1 + L::HS) / L::HS * L::HS - L::HS;
+    const int zse = (Zc - 1 + 16) / 16 * 16 - 16;
+    const int xb0 = X0 / EB;
+    if (threadIdx.x == 0) {
+        mbar_init(bar, 1);
+        fence_proxy_async();
+        mbar_expect_tx(bar, L::tx);
+        tma_load_4d(smem, fmap, zs, X0 - 1, shot, 0, bar);
+        tma_load_4d(smem + L::oE, emap, zse, xb0 - 1, shot, 0, bar);
+    }
+    __syncthreads();
+    const int Z0 = Zc + warp * 30;
+    if (Z0 >= a.NZ) return;
+    const int Z = Z0 - 1 + lane;
+    const bool zin = Z >= 0 && Z < a.NZ;
+    const bool own = lane >= 1 && lane <= 30 && Z < a.NZ;
+    const long long fb = (long long)shot * a.fstride;
+    const long long sb = (long long)shot * a.sstride;
+    const C zero = C(0);
+    const int of = Z - zs, oe = Z - zse;
+    // decoder of field f's block b of the box (0: the block holding row
+    // X0-1; 1 .. TX/EB: the slab's own; TX/EB+1: the block holding X0+TX)
+    auto DE = [&](int f, int b) -> BDec { return bfp_dec(ebox[(f * L::NB + b) * L::BWE + oe]); };
+    auto blk = [&](int rho) { return rho == 0 ? 0 : (rho > TX ? L::NB - 1 : (rho - 1) / EB + 1); };
+    auto F = [&](int rho, int f) -> C {
+        return bfp_val(fbox[(f * L::RX + rho) * L::BW + of], DE(f, blk(rho)));
+    };
+    auto M = [&](int rho, int m) -> C {
+        const int x = X0 - 1 + rho;
+        if (!zin || x < 0 || x >= a.NX) return zero;
+        return __ldg(static_cast<const C *>(a.mat[m]) + (long long)x * a.pitch + Z);
+    };
+    const bool zint = (Z0 - 1 >= a.np) && (Z0 + 30 <= a.np + a.nz - 1);
+    const bool lean = zint && X0 >= a.np && X1 <= a.np + a.nx - 1;
+    int16_t *const fo0 = static_cast<int16_t *>(a.fo[0]);
+    const long long fso = static_cast<int16_t *>(a.fo[1]) - fo0;
+    uint8_t *const eo0 = static_cast<uint8_t *>(a.feo) + (long long)shot * a.nxb * a.pitch + Z;
+    // store block q (rows X0 + EB q ..) of field f from v[EB]; rows past the
+    // grid's end (vmask false) are left out of the exponent and not stored
+    auto store_block = [&](int f, int q, const C *v, const bool *vm) {
+        unsigned mx = 0;
+#pragma unroll
+        for (int t = 0; t < EB; ++t) mx = vm[t] ? max(mx, bfp_absbits(v[t])) : mx;
+        bool over;
+        const unsigned e8 = bfp_e8(mx, &over);
+        const float esc = bfp_escale(e8);
+        int16_t *o = fo0 + f * fso + fb + (long long)(X0 + EB * q) * a.pitch + Z;
+#pragma unroll
+        for (int t = 0; t < EB; ++t)
+            if (vm[t]) o[(long long)t * a.pitch] = bfp_man(v[t], esc);
+        if (vm[0]) {   // a lane that owns the column and a block inside the grid
+            eo0[(long long)f * a.estride + (long long)(xb0 + q) * a.pitch] = (uint8_t)e8;
+            if (over) atomicExch(a.err, 4);
+        }
+    };
+
+    if (lean) {
+        C nb[TX], cbm[TX], cla[TX], cl2m[TX], cmu[TX];
+        const C b1 = M(1, M_B), bm0 = M(0, M_BM);
+#pragma unroll
+        for (int r = 0; r < TX; ++r) {
+            nb[r] = M(r + 2, M_B);
+            cbm[r] = M(r + 1, M_BM);
+            cla[r] = M(r + 1, M_LA);
+            cl2m[r] = M(r + 1, M_L2M);
+            cmu[r] = M(r + 1, M_MU);
+        }
+        if (!__all_sync(full, mbar_wait(bar, 0, a.err, 9))) {
+            mbar_wait(bar, 0, a.err, 9);
+            return;
+        }
+        C vxc, vzp;
+        {
+            const C c_txz = F(1, F_TXZ), p_tzz = F(0, F_TZZ);
+            const C txz_zm = __shfl_up_sync(full, c_txz, 1);
+            const C tzz_zp = __shfl_down_sync(full, p_tzz, 1);
+            vxc = r_fma(b1, r_add(r_sub(F(1, F_TXX), F(0, F_TXX)), r_sub(c_txz, txz_zm)), F(1, F_VX));
+            vzp = zero;
+            if (X0 - 1 >= a.np)
+                vzp = r_fma(bm0, r_add(r_sub(c_txz, F(0, F_TXZ)), r_sub(tzz_zp, p_tzz)), F(0, F_VZ));
+        }
+        if (X0 - 1 < a.np) {
+            ESplit<C> sp;
+            const EisoProf P{a.NX, a.NZ};
+            const C *pr = static_cast<const C *>(a.prof);
+            e_load_split<float, C>(a, sb, X0 - 1, Z, zin, sp);
+            const EZProf<C> zp{pr[P.azn() + Z], pr[P.bzn() + Z], pr[P.azh() + Z], pr[P.bzh() + Z]};
+            const C c_txz = F(1, F_TXZ), p_tzz = F(0, F_TZZ);
+            const C tzz_zp = __shfl_down_sync(full, p_tzz, 1);
+            vzp = e_vz<float, C>(a, sb, X0 - 1, Z, F(0, F_VZ), bm0, r_sub(c_txz, F(0, F_TXZ)),
+                                 r_sub(tzz_zp, p_tzz), sp.vz, zp, false);
+        }
+        const bool vm[EB] = {own, own, own, own};
+        C bvx[EB], bvz[EB], btxx[EB], btzz[EB], btxz[EB];
+        bvx[0] = vxc;
+#pragma unroll
+        for (int r = 0; r < TX; ++r) {
+            const int rc = r + 1;
+            const C n_txz = F(rc + 1, F_TXZ), c_txz = F(rc, F_TXZ), c_tzz = F(rc, F_TZZ);
+            const C c_txx = F(rc, F_TXX), n_txx = F(rc + 1, F_TXX);
+            const C n_vx = F(rc + 1, F_VX), c_vz = F(rc, F_VZ);
+            const C txz_zm = __shfl_up_sync(full, n_txz, 1);
+            const C tzz_zp = __shfl_down_sync(full, c_tzz, 1);
+            const C ax = r_sub(n_txx, c_txx), az = r_sub(n_txz, txz_zm);
+            const C bx_ = r_sub(n_txz, c_txz), bz = r_sub(tzz_zp, c_tzz);
+            const C vxn = r_fma(nb[r], r_add(ax, az), n_vx);
+            const C vzn = r_fma(cbm[r], r_add(bx_, bz), c_vz);
+            const C vz_zm = __shfl_up_sync(full, vzn, 1);
+            const C vx_zp = __shfl_down_sync(full, vxc, 1);
+            const C sax = r_sub(vxn, vxc), saz = r_sub(vzn, vz_zm);
+            const C sbz = r_sub(vx_zp, vxc), sbx = r_sub(vzn, vzp);
+            const int t = r % EB;
+            bvz[t] = vzn;
+            btxx[t] = r_add(c_txx, r_fma(cl2m[r], sax, r_mul(cla[r], saz)));
+            btzz[t] = r_add(c_tzz, r_fma(cl2m[r], saz, r_mul(cla[r], sax)));
+            btxz[t] = r_fma(cmu[r], r_add(sbz, sbx), c_txz);
+            if (t == EB - 1) {
+                const int q = r / EB;
+                store_block(F_VX, q, bvx, vm);
+                store_block(F_VZ, q, bvz, vm);
+                store_block(F_TXX, q, btxx, vm);
+                store_block(F_TZZ, q, btzz, vm);
+                store_block(F_TXZ, q, btxz, vm);
+            } else {
+                bvx[t + 1] = vxn;
+            }
+            if (t == EB - 1 && r + 1 < TX) bvx[0] = vxn;
+            vxc = vxn;
+            vzp = vzn;
+        }
+        return;
+    }
+
+    // general march (frame): unrolled over the slab's rows, rows past the
+    // grid's end masked; split parts FP32 as in the other precisions
+    const C *pr = static_cast<const C *>(a.prof);
+    const EisoProf P{a.NX, a.NZ};
+    EZProf<C> zp{C(1), C(1), C(1), C(1)};
+    if (zin) zp = EZProf<C>{pr[P.azn() + Z], pr[P.bzn() + Z], pr[P.azh() + Z], pr[P.bzh() + Z]};
+    ESplit<C> sp;
+    e_load_split<float, C>(a, sb, X0 - 1, Z, zin, sp);
+    if (!__all_sync(full, mbar_wait(bar, 0, a.err, 9))) {
+        mbar_wait(bar, 0, a.err, 9);
+        return;
+    }
+    C vxc, vzp;
+    {
+        const C c_txz = F(1, F_TXZ), p_tzz = F(0, F_TZZ);
+        const C txz_zm = __shfl_up_sync(full, c_txz, 1);
+        const C tzz_zp = __shfl_down_sync(full, p_tzz, 1);
+        // vx(X0) is this slab's row: its split parts are stored here
+        vxc = zin ? e_vx<float, C>(a, sb, X0, Z, F(1, F_VX), M(1, M_B), r_sub(F(1, F_TXX), F(0, F_TXX)),
+                                   r_sub(c_txz, txz_zm), sp.vx, zp, own)
+                  : zero;
+        vzp = zero;
+        if (X0 >= 1 && zin)
+            vzp = e_vz<float, C>(a, sb, X0 - 1, Z, F(0, F_VZ), M(0, M_BM), r_sub(c_txz, F(0, F_TXZ)),
+                                 r_sub(tzz_zp, p_tzz), sp.vz, zp, false);
+    }
+    e_load_split<float, C>(a, sb, X0, Z, zin, sp);
+    C bvx[EB], bvz[EB], btxx[EB], btzz[EB], btxz[EB];
+    bool vm[EB];
+    bvx[0] = vxc;
+#pragma unroll
+    for (int r = 0; r < TX; ++r) {
+        const int X = X0 + r;
+        const bool valid = X < X1;
+        const int rc = r + 1;
+        const int t = r % EB;
+        vm[t] = own && valid;
+        C vxn = zero, vzn = zero, txx = zero, tzz = zero, txz = zero;
+        if (valid) {   // uniform across the CTA
+            ESplit<C> sn;
+            e_load_split<float, C>(a, sb, X + 1, Z, zin && X + 1 < X1, sn);
+            const bool fast = zint && X >= a.np && X + 1 <= a.np + a.nx - 1;
+            const C n_b = M(rc + 1, M_B), c_bm = M(rc, M_BM);
+            const C la = M(rc, M_LA), l2m = M(rc, M_L2M), mu = M(rc, M_MU);
+            const C n_txz = F(rc + 1, F_TXZ), c_txz = F(rc, F_TXZ), c_tzz = F(rc, F_TZZ);
+            const C c_txx = F(rc, F_TXX);
+            const C txz_zm = __shfl_up_sync(full, n_txz, 1);
+            const C tzz_zp = __shfl_down_sync(full, c_tzz, 1);
+            const C ax = r_sub(F(rc + 1, F_TXX), c_txx), az = r_sub(n_txz, txz_zm);
+            const C bx_ = r_sub(n_txz, c_txz), bz = r_sub(tzz_zp, c_tzz);
+            if (fast) {
+                vxn = r_fma(n_b, r_add(ax, az), F(rc + 1, F_VX));
+                vzn = r_fma(c_bm, r_add(bx_, bz), F(rc, F_VZ));
+            } else {
+                // vx(X+1) belongs to this slab when X+1 < X1 (its split
+                // parts are stored then); the last row's is the next slab's
+                vxn = (X + 1 < a.NX && zin)
+                          ? e_vx<float, C>(a, sb, X + 1, Z, F(rc + 1, F_VX), n_b, ax, az, sp.vx, zp,
+                                           own && X + 1 < X1)
+                          : zero;
+                vzn = zin ? e_vz<float, C>(a, sb, X, Z, F(rc, F_VZ), c_bm, bx_, bz, sp.vz, zp, own)
+                          : zero;
+            }
+            const C vz_zm = __shfl_up_sync(full, vzn, 1);
+            const C vx_zp = __shfl_down_sync(full, vxc, 1);
+            const C sax = r_sub(vxn, vxc), saz = r_sub(vzn, vz_zm);
+            const C sbz = r_sub(vx_zp, vxc), sbx = r_sub(vzn, vzp);
+            if (fast || (zin && e_inside(a, X, Z))) {
+                txx = r_add(c_txx, r_fma(l2m, sax, r_mul(la, saz)));
+                tzz = r_add(c_tzz, r_fma(l2m, saz, r_mul(la, sax)));
+                txz = r_fma(mu, r_add(sbz, sbx), c_txz);
+            } else if (zin) {
+                const long long cc = sb + e_pml_index(a, X, Z);
+                const C Axh = pr[P.axh() + X], Bxh = pr[P.bxh() + X];
+                txx = e_frame<float, C>(a, F_TXX, cc, Axh, Bxh, zp.An, zp.Bn, sp.t[0], sp.t[1], l2m,
+                                        la, sax, saz, own);
+                tzz = e_frame<float, C>(a, F_TZZ, cc, Axh, Bxh, zp.An, zp.Bn, sp.t[2], sp.t[3], la,
+                                        l2m, sax, saz, own);
+                txz = e_frame<float, C>(a, F_TXZ, cc, pr[P.axn() + X], pr[P.bxn() + X], zp.Ah, zp.Bh,
+                                        sp.t[4], sp.t[5], mu, mu, sbx, sbz, own);
+            }
+            sp = sn;
+        }
+        bvz[t] = vzn;
+        btxx[t] = txx;
+        btzz[t] = tzz;
+        btxz[t] = txz;
+        if (t == EB - 1) {
+            const int q = r / EB;
+            if (X0 + EB * q < X1) {   // uniform across the CTA
+                store_block(F_VX, q, bvx, vm);
+                store_block(F_VZ, q, bvz, vm);
+                store_block(F_TXX, q, btxx, vm);
+                store_block(F_TZZ, q, btzz, vm);
+                store_block(F_TXZ, q, btxz, vm);
+            }
+            if (r + 1 < TX) bvx[0] = vxn;
+        } else {
+            bvx[t + 1] = vxn;
+        }
+        vxc = vxn;
+        vzp = vzn;
+    }
+}
+
+template <int W, int TX, int MINB>
+__global__ void __launch_bounds__(32 * W, MINB) eiso_bslab_kernel(const EisoArgs a,
+                                                                  const __grid_constant__ EisoBMaps mp) {
+    extern __shared__ __align__(128) unsigned char smem[];
+    eiso_bslab_body<W, TX>(a, &mp.f, &mp.e, blockIdx.x, blockIdx.y, blockIdx.z, smem);
+}
+
+// ---------------------------------------------------------------------------
 // Tiled step kernel: one CTA updates a TX x TZ tile of one shot for a whole
 // time step (e_iso.c:595-636).  The five old wavefields of rows X0-1 ..
 // X0+TX and z cells Z0-HS .. Z0+TZ+HS-1 arrive by TMA (out-of-grid cells read
@@ -837,6 +1141,10 @@ struct SrcEntry {
     int type;         // SM_SRC_*
     long long voff;   // offset of its scaled samples in vals
     int len;
+    // block storage: the cell's block (first cell qb, nb rows inside the
+    // grid, the source's row rs in it) and its exponent index qe, per shot
+    long long qb, qe;
+    int nb, rs;
 };
 
 // add_src (src.c:170-184) for one shot, into the wavefields f just written
@@ -881,6 +1189,7 @@ struct RecEntry {
     int field;         // F_*
     int group;         // sampling group
     long long out;     // offset of its first sample in the trace buffer
+    long long qe;      // block storage: the exponent index of its block, per shot
 };
 
 // one receiver's sample of step it, if the record's predicate takes it
@@ -906,6 +1215,78 @@ __global__ void eiso_gather_kernel(EisoArgs a, const RecEntry *rec, int nrec,
     eiso_sample<S>(a.f, a.fstride, a.isc, *a.step - 1, rec[r], table, nsteps_max, traces);
 }
 
+// block storage: add_src (src.c:170-184) for one shot; each addition decodes
+// the block of the source cell, adds, and stores the block again with the
+// exponent its new maximum takes
+__device__ __forceinline__ void eiso_badd(int16_t *m, uint8_t *e, const SrcEntry &s,
+                                          long long pitch, float add, int *err) {
+    const BDec d = bfp_dec(e[s.qe]);
+    float v[EISO_EB];
+    unsigned mx = 0;
+    for (int r = 0; r < s.nb; ++r) {
+        v[r] = bfp_val(m[s.qb + r * pitch], d);
+        if (r == s.rs) v[r] = v[r] + add;
+        mx = max(mx, bfp_absbits(v[r]));
+    }
+    bool over;
+    const unsigned e8 = bfp_e8(mx, &over);
+    const float esc = bfp_escale(e8);
+    for (int r = 0; r < s.nb; ++r) m[s.qb + r * pitch] = bfp_man(v[r], esc);
+    e[s.qe] = (uint8_t)e8;
+    if (over) atomicExch(err, 4);
+}
+
+__device__ __forceinline__ void eiso_binject(void *const *f, long long fstride, void *fe,
+                                             long long estride, long long eshot, int pitch,
+                                             long long it, const SrcEntry *src,
+                                             const int *shot_first, const double *vals, int shot,
+                                             int *err) {
+    for (int e = shot_first[shot]; e < shot_first[shot + 1]; ++e) {
+        const SrcEntry s = src[e];
+        if (it >= s.len) continue;
+        const float v = static_cast<float>(vals[s.voff + it]);
+        int fs[2] = {-1, -1};
+        if (s.type == SM_SRC_SX || s.type == SM_SRC_BULK) fs[0] = F_TXX;
+        if (s.type == SM_SRC_SZ || s.type == SM_SRC_BULK) fs[1] = F_TZZ;
+        if (s.type == SM_SRC_SXZ) fs[0] = F_TXZ;
+        for (int k = 0; k < 2; ++k) {
+            if (fs[k] < 0) continue;
+            eiso_badd(static_cast<int16_t *>(f[fs[k]]) + (long long)shot * fstride,
+                      static_cast<uint8_t *>(fe) + fs[k] * estride + shot * eshot, s, pitch, v, err);
+        }
+    }
+}
+
+__global__ void eiso_bsource_kernel(EisoArgs a, const SrcEntry *src, const int *shot_first,
+                                    const double *vals, int nshots) {
+    const long long it = *a.step - 1;
+    const int shot = blockIdx.x * blockDim.x + threadIdx.x;
+    if (shot >= nshots) return;
+    eiso_binject(a.f, a.fstride, a.fe, a.estride, (long long)a.nxb * a.pitch, a.pitch, it, src,
+                 shot_first, vals, shot, a.err);
+}
+
+__device__ __forceinline__ void eiso_bsample(void *const *f, long long fstride, const void *fe,
+                                             long long estride, long long eshot, long long it,
+                                             const RecEntry &e, const int32_t *table,
+                                             long long nsteps_max, double *traces) {
+    if (it >= nsteps_max) return;
+    const int32_t slot = table[(long long)e.group * nsteps_max + it];
+    if (slot < 0) return;
+    const int16_t m = static_cast<const int16_t *>(f[e.field])[(long long)e.shot * fstride + e.q];
+    const unsigned e8 =
+        static_cast<const uint8_t *>(fe)[e.field * estride + e.shot * eshot + e.qe];
+    traces[e.out + slot] = static_cast<double>(bfp_val(m, bfp_dec(e8)));
+}
+
+__global__ void eiso_bgather_kernel(EisoArgs a, const RecEntry *rec, int nrec,
+                                    const int32_t *table, long long nsteps_max, double *traces) {
+    const int r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= nrec) return;
+    eiso_bsample(a.f, a.fstride, a.fe, a.estride, (long long)a.nxb * a.pitch, *a.step - 1, rec[r],
+                 table, nsteps_max, traces);
+}
+
 // ---------------------------------------------------------------------------
 // Grouped step: one launch advances up to kGroupMax e_iso problems of
 // different grid sizes and shot counts by one time step.  Linear CTA b
@@ -921,6 +1302,7 @@ constexpr int kGroupMax = 32;
 
 struct EisoGroupStepParams {
     CUtensorMap f[kGroupMax];     // each problem's old-set slab map
+    CUtensorMap e[kGroupMax];     // ... and exponent map (block storage)
     EisoArgs a[kGroupMax];        // its arguments for this step
     int first[kGroupMax + 1];     // first linear CTA of each problem
     int gx[kGroupMax], gy[kGroupMax];
@@ -949,6 +1331,26 @@ __global__ void __launch_bounds__(32 * W, MINB) eiso_group_step_kernel(
     eiso_slabg_body<S, W, TX>(sa, &P.f[p], bx, by, shot, smem);
 }
 
+template <int W, int TX, int MINB>
+__global__ void __launch_bounds__(32 * W, MINB) eiso_bgroup_step_kernel(
+    const __grid_constant__ EisoGroupStepParams P) {
+    extern __shared__ __align__(128) unsigned char smem[];
+    __shared__ EisoArgs sa;
+    const int b = blockIdx.x;
+    int p = 0;
+    while (p + 1 < P.n && P.first[p + 1] <= b) ++p;
+    const int local = b - P.first[p];
+    const int bx = local % P.gx[p], rest = local / P.gx[p];
+    const int by = rest % P.gy[p], shot = rest / P.gy[p];
+    {
+        const int *src = reinterpret_cast<const int *>(&P.a[p]);
+        int *dst = reinterpret_cast<int *>(&sa);
+        for (int i = threadIdx.x; i < (int)(sizeof(EisoArgs) / 4); i += blockDim.x) dst[i] = src[i];
+    }
+    __syncthreads();
+    eiso_bslab_body<W, TX>(sa, &P.f[p], &P.e[p], bx, by, shot, smem);
+}
+
 // what the source and receiver kernels of one problem need after its step
 struct EisoPost {
     void *f[5];                  // the wavefields just written
@@ -962,6 +1364,11 @@ struct EisoPost {
     const int32_t *table;
     long long nsteps_max;
     double *traces;
+    // block storage
+    void *fe;
+    long long estride, eshot;
+    int pitch;
+    int *err;
 };
 
 struct EisoGroupPostParams {
@@ -979,8 +1386,12 @@ __global__ void eiso_group_source_kernel(const __grid_constant__ EisoGroupPostPa
     int p = 0;
     while (p + 1 < P.n && P.first_src[p + 1] <= t) ++p;
     const EisoPost &q = P.q[p];
-    eiso_inject<S>(q.f, q.fstride, q.sc, q.isc, *q.step - 1, q.src, q.src_first, q.vals,
-                   t - P.first_src[p]);
+    if constexpr (std::is_same<S, Bfp16>::value)
+        eiso_binject(q.f, q.fstride, q.fe, q.estride, q.eshot, q.pitch, *q.step - 1, q.src,
+                     q.src_first, q.vals, t - P.first_src[p], q.err);
+    else
+        eiso_inject<S>(q.f, q.fstride, q.sc, q.isc, *q.step - 1, q.src, q.src_first, q.vals,
+                       t - P.first_src[p]);
 }
 
 template <typename S>
@@ -990,8 +1401,12 @@ __global__ void eiso_group_gather_kernel(const __grid_constant__ EisoGroupPostPa
     int p = 0;
     while (p + 1 < P.n && P.first_rec[p + 1] <= t) ++p;
     const EisoPost &q = P.q[p];
-    eiso_sample<S>(q.f, q.fstride, q.isc, *q.step - 1, q.rec[t - P.first_rec[p]], q.table,
-                   q.nsteps_max, q.traces);
+    if constexpr (std::is_same<S, Bfp16>::value)
+        eiso_bsample(q.f, q.fstride, q.fe, q.estride, q.eshot, *q.step - 1,
+                     q.rec[t - P.first_rec[p]], q.table, q.nsteps_max, q.traces);
+    else
+        eiso_sample<S>(q.f, q.fstride, q.isc, *q.step - 1, q.rec[t - P.first_rec[p]], q.table,
+                       q.nsteps_max, q.traces);
 }
 
 }  // namespace sm
@@ -1031,6 +1446,12 @@ struct sm_eiso {
     int maps_key = -1;           // (TX, TZ) the maps were built for
     EisoSlabMaps slab_maps[2];   // TMA maps of each buffer set (slab kernels)
     int slab_key = -1;           // box shape the slab maps were built for
+    // block storage (SM_BFP16): exponent bytes of each set,
+    // [field][shot][nxb][pitch], and the slab kernel's maps
+    DevBuf fexp[2];
+    size_t nxb = 0;
+    EisoBMaps bmaps[2];
+    int bmap_key = -1;
     DevBuf d_step;               // device step counter (EisoArgs::step)
     // CUDA graphs of graph_steps steps, one per parity of the starting
     // buffer set; captured again when graph_epoch moved since (new sources,
@@ -1080,6 +1501,8 @@ int eiso_check(sm_eiso_t h) {
 // point the kernel arguments at the current (read) and other (write) sets
 void eiso_bind(sm_eiso *h) {
     const int c = h->cur, o = 1 - h->cur;
+    h->args.fe = h->fexp[c].p;
+    h->args.feo = h->fexp[o].p;
     for (int f = 0; f < 5; ++f) {
         h->args.f[f] = h->field(c, f);
         h->args.fx[f] = h->xpart[c][f].p;
@@ -1104,6 +1527,42 @@ static const EisoConfig kEisoConfigs[] = {
     {0, {4, 8, 4, 0}},  {0, {2, 16, 4, 0}},   {1, {8, 32, 128, 6}}, {1, {16, 64, 256, 2}},
     {1, {8, 64, 256, 3}}, {2, {2, 8, 8, 0}},  {2, {4, 8, 4, 0}},    {2, {1, 16, 12, 0}}};
 static const int kEisoNumConfigs = sizeof(kEisoConfigs) / sizeof(kEisoConfigs[0]);
+// block storage: the slab step only, {warps per CTA, rows TX (whole blocks),
+// min CTAs per SM}
+struct EisoBConfig {
+    int w, tx, minb;
+};
+static const EisoBConfig kEisoBConfigs[] = {{2, 8, 8}, {4, 8, 4}, {2, 4, 12}, {4, 4, 6}, {1, 8, 16}};
+static const int kEisoBNumConfigs = sizeof(kEisoBConfigs) / sizeof(kEisoBConfigs[0]);
+
+bool eiso_isb(const sm_eiso *h) { return h->precision == SM_BFP16; }
+int eiso_ncfg(const sm_eiso *h) { return eiso_isb(h) ? kEisoBNumConfigs : kEisoNumConfigs; }
+
+// TMA maps of the block-storage slab step: mantissas as the other slab
+// maps (z, x, shot, field), exponents (z, x block, shot, field)
+template <int W, int TX>
+int eiso_make_bmaps(sm_eiso *h) {
+    using L = ESlabB<W, TX>;
+    const int key = W * 4096 + TX;
+    if (h->bmap_key == key) return SM_OK;
+    const size_t row = (size_t)h->pitch;
+    const size_t fdims[4] = {(size_t)h->NZ, (size_t)h->NX, h->nshots, 5};
+    const size_t fstr[3] = {row * 2, h->NX * row * 2, h->fset_stride};
+    const unsigned fbox[4] = {(unsigned)L::BW, (unsigned)L::RX, 1, 5};
+    const size_t edims[4] = {(size_t)h->NZ, h->nxb, h->nshots, 5};
+    const size_t estr[3] = {row, h->nxb * row, (size_t)h->args.estride};
+    const unsigned ebox[4] = {(unsigned)L::BWE, (unsigned)L::NB, 1, 5};
+    for (int b = 0; b < 2; ++b) {
+        if (int rc = make_map_nd(&h->bmaps[b].f, h->fset[b].p, CU_TENSOR_MAP_DATA_TYPE_UINT16, 2,
+                                 4, fdims, fstr, fbox))
+            return rc;
+        if (int rc = make_map_nd(&h->bmaps[b].e, h->fexp[b].p, CU_TENSOR_MAP_DATA_TYPE_UINT8, 1, 4,
+                                 edims, estr, ebox))
+            return rc;
+    }
+    h->bmap_key = key;
+    return SM_OK;
+}
 
 template <typename S, int TX, int TZ>
 int eiso_make_tile_maps(sm_eiso *h) {
@@ -1206,6 +1665,51 @@ int launch_slabg_cfg(sm_eiso *h) {
     return SM_OK;
 }
 
+template <int W, int TX, int MINB>
+int ready_bslab_cfg(sm_eiso *h) {
+    if (int rc = eiso_make_bmaps<W, TX>(h)) return rc;
+    return allow_smem(eiso_bslab_kernel<W, TX, MINB>, ESlabB<W, TX>::bytes, h->device);
+}
+
+template <int W, int TX, int MINB>
+int launch_bslab_cfg(sm_eiso *h) {
+    const int wz = (h->NZ + 29) / 30;
+    dim3 grd((wz + W - 1) / W, (h->NX + TX - 1) / TX, (unsigned)h->nshots);
+    eiso_bslab_kernel<W, TX, MINB><<<grd, 32 * W, ESlabB<W, TX>::bytes, h->stream>>>(
+        h->args, h->bmaps[h->cur]);
+    return SM_OK;
+}
+
+size_t eiso_bconfig_smem(int config) {
+    switch (config) {
+    case 0: return ESlabB<2, 8>::bytes;
+    case 1: return ESlabB<4, 8>::bytes;
+    case 2: return ESlabB<2, 4>::bytes;
+    case 3: return ESlabB<4, 4>::bytes;
+    default: return ESlabB<1, 8>::bytes;
+    }
+}
+
+int eiso_bready(sm_eiso *h) {
+    switch (h->config) {
+    case 0: return ready_bslab_cfg<2, 8, 8>(h);
+    case 1: return ready_bslab_cfg<4, 8, 4>(h);
+    case 2: return ready_bslab_cfg<2, 4, 12>(h);
+    case 3: return ready_bslab_cfg<4, 4, 6>(h);
+    default: return ready_bslab_cfg<1, 8, 16>(h);
+    }
+}
+
+int eiso_blaunch(sm_eiso *h) {
+    switch (h->config) {
+    case 0: return launch_bslab_cfg<2, 8, 8>(h);
+    case 1: return launch_bslab_cfg<4, 8, 4>(h);
+    case 2: return launch_bslab_cfg<2, 4, 12>(h);
+    case 3: return launch_bslab_cfg<4, 4, 6>(h);
+    default: return launch_bslab_cfg<1, 8, 16>(h);
+    }
+}
+
 template <typename S>
 size_t eiso_config_smem(int config) {
     switch (config) {
@@ -1226,6 +1730,7 @@ size_t eiso_config_smem(int config) {
 
 size_t eiso_config_smem_prec(int precision, int config) {
     switch (precision) {
+    case SM_BFP16: return eiso_bconfig_smem(config);
     case SM_FP64: return eiso_config_smem<double>(config);
     case SM_FP16: return eiso_config_smem<__half>(config);
     case SM_BF16: return eiso_config_smem<__nv_bfloat16>(config);
@@ -1237,7 +1742,8 @@ size_t eiso_config_smem_prec(int precision, int config) {
 // of stream capture)
 template <typename S>
 int eiso_ready(sm_eiso *h) {
-    switch (h->config) {
+    if constexpr (std::is_same<S, Bfp16>::value) return eiso_bready(h);
+    else switch (h->config) {
     case 0: return ready_slabg_cfg<S, 2, 8, 8>(h);
     case 1: return ready_slabg_cfg<S, 2, 4, 12>(h);
     case 2: return ready_slabg_cfg<S, 4, 4, 6>(h);
@@ -1257,7 +1763,8 @@ template <typename S>
 int launch_step(sm_eiso *h) {
     cudaEvent_t t0 = h->timer.begin(h->stream);
     int rc = SM_OK;
-    switch (h->config) {
+    if constexpr (std::is_same<S, Bfp16>::value) rc = eiso_blaunch(h);
+    else switch (h->config) {
     case 0: rc = launch_slabg_cfg<S, 2, 8, 8>(h); break;
     case 1: rc = launch_slabg_cfg<S, 2, 4, 12>(h); break;
     case 2: rc = launch_slabg_cfg<S, 4, 4, 6>(h); break;
@@ -1284,8 +1791,12 @@ void launch_src(sm_eiso *h) {
     if (h->d_src.bytes == 0) return;
     int n = (int)h->nshots;
     h->timer.launches += 1;
-    eiso_source_kernel<S><<<(n + 127) / 128, 128, 0, h->stream>>>(
-        h->args, h->d_src.as<SrcEntry>(), h->d_src_first.as<int>(), h->d_vals.as<double>(), n);
+    if constexpr (std::is_same<S, Bfp16>::value)
+        eiso_bsource_kernel<<<(n + 127) / 128, 128, 0, h->stream>>>(
+            h->args, h->d_src.as<SrcEntry>(), h->d_src_first.as<int>(), h->d_vals.as<double>(), n);
+    else
+        eiso_source_kernel<S><<<(n + 127) / 128, 128, 0, h->stream>>>(
+            h->args, h->d_src.as<SrcEntry>(), h->d_src_first.as<int>(), h->d_vals.as<double>(), n);
 }
 
 template <typename S>
@@ -1293,9 +1804,14 @@ void launch_gather(sm_eiso *h) {
     if (h->n_rec_total == 0) return;
     int n = h->n_rec_total;
     h->timer.launches += 1;
-    eiso_gather_kernel<S><<<(n + 127) / 128, 128, 0, h->stream>>>(
-        h->args, h->d_rec.as<RecEntry>(), n, h->d_table.as<int32_t>(), h->table_steps,
-        h->d_traces.as<double>());
+    if constexpr (std::is_same<S, Bfp16>::value)
+        eiso_bgather_kernel<<<(n + 127) / 128, 128, 0, h->stream>>>(
+            h->args, h->d_rec.as<RecEntry>(), n, h->d_table.as<int32_t>(), h->table_steps,
+            h->d_traces.as<double>());
+    else
+        eiso_gather_kernel<S><<<(n + 127) / 128, 128, 0, h->stream>>>(
+            h->args, h->d_rec.as<RecEntry>(), n, h->d_table.as<int32_t>(), h->table_steps,
+            h->d_traces.as<double>());
 }
 
 bool eiso_is16(const sm_eiso *h) { return h->precision == SM_FP16 || h->precision == SM_BF16; }
@@ -1446,6 +1962,9 @@ int field_id(int comp) {
 int eiso_check_err(sm_eiso *h) {
     int e = 0;
     SM_CUDA_TRY(cudaMemcpy(&e, h->err.p, sizeof(int), cudaMemcpyDeviceToHost));
+    if (e == 4)
+        return sm_fail(SM_ESTATE, "e_iso: a block of the 16-bit block storage exceeded its range "
+                                  "(|value| >= 2^114)");
     if (e) return sm_fail(SM_ETIMEOUT, "e_iso step kernel: a bounded wait for a TMA load gave up");
     return SM_OK;
 }
@@ -1531,6 +2050,14 @@ int eiso_source_entry(size_t nx, size_t nz, size_t np, size_t pitch, size_t inde
     if (length > stride) return sm_fail(SM_EINVAL, "%s: source length exceeds stride", who);
     *e = SrcEntry{};
     e->q = (long long)(index / nz + np) * (long long)pitch + (long long)(index % nz + np);
+    {   // its block of EISO_EB rows along x (block storage)
+        const size_t X = index / nz + np, Z = index % nz + np, NX = nx + 2 * np;
+        const size_t xb = X / EISO_EB;
+        e->qb = (long long)(xb * EISO_EB) * (long long)pitch + (long long)Z;
+        e->qe = (long long)xb * (long long)pitch + (long long)Z;
+        e->nb = (int)std::min<size_t>(EISO_EB, NX - xb * EISO_EB);
+        e->rs = (int)(X - xb * EISO_EB);
+    }
     e->type = type;
     e->voff = (long long)vals.size();
     e->len = (int)length;
@@ -1546,6 +2073,7 @@ int eiso_receiver_entry(size_t nx, size_t nz, size_t np, size_t pitch, size_t in
     if (f < 0) return sm_fail(SM_EINVAL, "%s: component %d not recorded by e_iso", who, comp);
     *e = RecEntry{};
     e->q = (long long)(index / nz + np) * (long long)pitch + (long long)(index % nz + np);
+    e->qe = (long long)((index / nz + np) / EISO_EB) * (long long)pitch + (long long)(index % nz + np);
     e->field = f;
     e->group = group;
     return SM_OK;
@@ -1560,14 +2088,17 @@ extern "C" int sm_eiso_device_bytes(size_t nx, size_t nz, size_t npml, int preci
                                     size_t nshots, size_t nrec, size_t nsteps_max,
                                     size_t *bytes) {
     if (!bytes) return sm_fail(SM_EINVAL, "sm_eiso_device_bytes: NULL");
-    if (precision < SM_FP32 || precision > SM_BF16)
+    if (precision < SM_FP32 || precision > SM_BFP16)
         return sm_fail(SM_EINVAL, "sm_eiso_device_bytes: unknown precision %d", precision);
     const size_t NX = nx + 2 * npml, NZ = nz + 2 * npml, pitch = round_up(NZ, 32);
     const size_t fcells = NX * pitch, e = storage_bytes(precision);
     const size_t c = precision == SM_FP64 ? 8 : 4;
+    const size_t pe = precision == SM_BFP16 ? 4 : e;          // split parts
     const size_t pml = 4 * npml * npml + 2 * npml * (nx + nz);
     size_t b = 2 * mb2(5 * fcells * nshots * e);              // two buffer sets
-    b += 20 * mb2(pml * nshots * e);                          // split parts, both sets
+    if (precision == SM_BFP16)                                // their exponents
+        b += 2 * mb2(5 * nshots * ((NX + EISO_EB - 1) / EISO_EB) * pitch);
+    b += 20 * mb2(pml * nshots * pe);                         // split parts, both sets
     b += mb2(5 * fcells * c) + mb2((4 * NX + 4 * NZ) * c);    // materials, profiles
     b += mb2(nrec * nshots * nsteps_max * (sizeof(double) + sizeof(int32_t)));   // traces, table
     b += 16u << 20;                                           // small buffers, 16-bit scaler
@@ -1591,7 +2122,7 @@ extern "C" int sm_eiso_create(int device, size_t nx, size_t nz, size_t npml, dou
     if (!(hh > 0.0) || !(dt > 0.0)) return sm_fail(SM_EINVAL, "sm_eiso_create: h, dt must be > 0");
     if (nshots < 1 || nshots > 65535)
         return sm_fail(SM_EINVAL, "sm_eiso_create: nshots must be in [1, 65535]");
-    if (precision < SM_FP32 || precision > SM_BF16)
+    if (precision < SM_FP32 || precision > SM_BFP16)
         return sm_fail(SM_EINVAL, "sm_eiso_create: unknown precision %d", precision);
     const size_t NX = nx + 2 * npml, NZ = nz + 2 * npml;
     if (NX > (1u << 30) / 4 || NZ > (1u << 30) / 4 || NX * NZ > (size_t)1 << 31)
@@ -1622,12 +2153,21 @@ extern "C" int sm_eiso_create(int device, size_t nx, size_t nz, size_t npml, dou
     int rc;
     h->fset_stride = fcells * nshots * h->elem;
     h->mat_stride = fcells * cplx;
+    // block storage keeps the split parts in FP32
+    const size_t pelem = precision == SM_BFP16 ? 4 : h->elem;
+    if (precision == SM_BFP16) {
+        h->nxb = (NX + EISO_EB - 1) / EISO_EB;
+        h->args.nxb = (int)h->nxb;
+        h->args.estride = (long long)(nshots * h->nxb * (size_t)h->pitch);
+    }
     for (int k = 0; k < 2; ++k) {
         if ((rc = h->fset[k].alloc(5 * h->fset_stride))) return rc;
         for (int f = 0; f < 5; ++f) {
-            if ((rc = h->xpart[k][f].alloc(h->npml_cells * nshots * h->elem))) return rc;
-            if ((rc = h->zpart[k][f].alloc(h->npml_cells * nshots * h->elem))) return rc;
+            if ((rc = h->xpart[k][f].alloc(h->npml_cells * nshots * pelem))) return rc;
+            if ((rc = h->zpart[k][f].alloc(h->npml_cells * nshots * pelem))) return rc;
         }
+        if (precision == SM_BFP16 && (rc = h->fexp[k].alloc(5 * (size_t)h->args.estride)))
+            return rc;
     }
     if ((rc = h->matbuf.alloc(5 * h->mat_stride))) return rc;
     EisoProf P{(int)NX, (int)NZ};
@@ -1699,6 +2239,7 @@ extern "C" int sm_eiso_reset(sm_eiso_t h) {
     DeviceGuard g(h->device);
     for (int k = 0; k < 2; ++k) {
         if (int rc = h->fset[k].zero(h->stream)) return rc;
+        if (int rc = h->fexp[k].zero(h->stream)) return rc;
         for (int f = 0; f < 5; ++f) {
             if (int rc = h->xpart[k][f].zero(h->stream)) return rc;
             if (int rc = h->zpart[k][f].zero(h->stream)) return rc;
@@ -1882,6 +2423,7 @@ extern "C" int sm_eiso_run(sm_eiso_t h, size_t nsteps) {
     case SM_FP64: rc = eiso_run_t<double>(h, nsteps); break;
     case SM_FP16: rc = eiso_run_t<__half>(h, nsteps); break;
     case SM_BF16: rc = eiso_run_t<__nv_bfloat16>(h, nsteps); break;
+    case SM_BFP16: rc = eiso_run_t<Bfp16>(h, nsteps); break;
     default: rc = eiso_run_t<float>(h, nsteps); break;
     }
     if (rc) return rc;
@@ -1894,7 +2436,9 @@ namespace {
 // one grouped step of the problems hs[0..n) (n <= kGroupMax), all on stream st
 template <typename S>
 int eiso_group_step(sm_eiso *const *hs, int n, cudaStream_t st) {
-    using L = ESlabG<S, 2, 8>;
+    constexpr bool B = std::is_same<S, Bfp16>::value;
+    using T = std::conditional_t<B, int16_t, S>;
+    using L = ESlabG<T, 2, 8>;
     static EisoGroupStepParams P;   // large: built in place, one caller at a time
     static EisoGroupPostParams Q;
     static std::mutex mu;
@@ -1902,7 +2446,12 @@ int eiso_group_step(sm_eiso *const *hs, int n, cudaStream_t st) {
     int total = 0;
     for (int k = 0; k < n; ++k) {
         sm_eiso *h = hs[k];
-        P.f[k] = h->slab_maps[h->cur].f;
+        if constexpr (B) {
+            P.f[k] = h->bmaps[h->cur].f;
+            P.e[k] = h->bmaps[h->cur].e;
+        } else {
+            P.f[k] = h->slab_maps[h->cur].f;
+        }
         P.a[k] = h->args;
         P.gx[k] = ((h->NZ + 29) / 30 + 1) / 2;
         P.gy[k] = (h->NX + 7) / 8;
@@ -1911,7 +2460,10 @@ int eiso_group_step(sm_eiso *const *hs, int n, cudaStream_t st) {
     }
     P.first[n] = total;
     P.n = n;
-    eiso_group_step_kernel<S, 2, 8, 8><<<total, 64, L::bytes, st>>>(P);
+    if constexpr (B)
+        eiso_bgroup_step_kernel<2, 8, 8><<<total, 64, ESlabB<2, 8>::bytes, st>>>(P);
+    else
+        eiso_group_step_kernel<S, 2, 8, 8><<<total, 64, L::bytes, st>>>(P);
     int nsrc = 0, nrec = 0;
     for (int k = 0; k < n; ++k) {
         sm_eiso *h = hs[k];
@@ -1932,6 +2484,11 @@ int eiso_group_step(sm_eiso *const *hs, int n, cudaStream_t st) {
         q.table = h->d_table.as<int32_t>();
         q.nsteps_max = h->table_steps;
         q.traces = h->d_traces.as<double>();
+        q.fe = h->args.fe;
+        q.estride = h->args.estride;
+        q.eshot = (long long)h->nxb * h->pitch;
+        q.pitch = h->pitch;
+        q.err = h->args.err;
         Q.first_src[k] = nsrc;
         Q.first_rec[k] = nrec;
         nsrc += h->d_src.bytes ? (int)h->nshots : 0;
@@ -2021,11 +2578,19 @@ int eiso_group_graph(sm_eiso *const *hs, int n, cudaGraphExec_t *out) {
 
 template <typename S>
 int eiso_group_run_t(sm_eiso *const *hs, int n, size_t nsteps) {
-    using L = ESlabG<S, 2, 8>;
-    for (int k = 0; k < n; ++k)
-        if (int rc = eiso_make_slab_maps<S, L, (1 << 20) + 2 * 4096 + 8>(hs[k])) return rc;
-    if (int rc = allow_smem(eiso_group_step_kernel<S, 2, 8, 8>, L::bytes, hs[0]->device))
-        return rc;
+    if constexpr (std::is_same<S, Bfp16>::value) {
+        for (int k = 0; k < n; ++k)
+            if (int rc = eiso_make_bmaps<2, 8>(hs[k])) return rc;
+        if (int rc = allow_smem(eiso_bgroup_step_kernel<2, 8, 8>, ESlabB<2, 8>::bytes,
+                                hs[0]->device))
+            return rc;
+    } else {
+        using L = ESlabG<S, 2, 8>;
+        for (int k = 0; k < n; ++k)
+            if (int rc = eiso_make_slab_maps<S, L, (1 << 20) + 2 * 4096 + 8>(hs[k])) return rc;
+        if (int rc = allow_smem(eiso_group_step_kernel<S, 2, 8, 8>, L::bytes, hs[0]->device))
+            return rc;
+    }
     const bool is16 = eiso_is16(hs[0]);
     const size_t G = kGroupGraphSteps;
     int per_step = 1;
@@ -2112,6 +2677,7 @@ extern "C" int sm_eiso_group_run(sm_eiso_t const *handles, int n, size_t nsteps)
     case SM_FP64: rc = eiso_group_run_t<double>(hs, n, nsteps); break;
     case SM_FP16: rc = eiso_group_run_t<__half>(hs, n, nsteps); break;
     case SM_BF16: rc = eiso_group_run_t<__nv_bfloat16>(hs, n, nsteps); break;
+    case SM_BFP16: rc = eiso_group_run_t<Bfp16>(hs, n, nsteps); break;
     default: rc = eiso_group_run_t<float>(hs, n, nsteps); break;
     }
     for (int k = 0; k < n; ++k) hs[k]->stream = own[k];
@@ -2170,7 +2736,7 @@ extern "C" int sm_eiso_autotune(sm_eiso_t h, int trial_steps, int *config,
     h->timer.on = false;
     Val best{-1, 0.0};
     int rc = SM_OK;
-    for (int c = 0; c < kEisoNumConfigs && rc == SM_OK; ++c) {
+    for (int c = 0; c < eiso_ncfg(h) && rc == SM_OK; ++c) {
         if (eiso_config_smem_prec(h->precision, c) > (size_t)lim) continue;
         h->config = c;
         h->graph_epoch++;
@@ -2279,6 +2845,31 @@ extern "C" int sm_eiso_get_field(sm_eiso_t h, size_t shot, int comp, int part, d
     DeviceGuard g(h->device);
     SM_CUDA_TRY(cudaStreamSynchronize(h->stream));
     const size_t NX = h->NX, NZ = h->NZ, e = h->elem;
+    if (eiso_isb(h)) {   // totals: mantissa times 2^(e8 - 126); split parts FP32
+        if (part == SM_PART_TOTAL) {
+            std::vector<int16_t> m(NX * (size_t)h->pitch);
+            std::vector<uint8_t> ex(h->nxb * (size_t)h->pitch);
+            SM_CUDA_TRY(cudaMemcpy(m.data(), static_cast<char *>(h->field(h->cur, f)) +
+                                                 shot * h->args.fstride * 2,
+                                   m.size() * 2, cudaMemcpyDeviceToHost));
+            SM_CUDA_TRY(cudaMemcpy(ex.data(), static_cast<char *>(h->fexp[h->cur].p) +
+                                                  f * h->args.estride + shot * ex.size(),
+                                   ex.size(), cudaMemcpyDeviceToHost));
+            for (size_t X = 0; X < NX; ++X)
+                for (size_t Z = 0; Z < NZ; ++Z)
+                    out[X * NZ + Z] = bfp_value_host(m[X * h->pitch + Z],
+                                                     ex[(X / EISO_EB) * h->pitch + Z]);
+            return SM_OK;
+        }
+        const DevBuf &src = part == SM_PART_X ? h->xpart[h->cur][f] : h->zpart[h->cur][f];
+        std::vector<float> buf(h->npml_cells);
+        SM_CUDA_TRY(cudaMemcpy(buf.data(), static_cast<char *>(src.p) + shot * h->npml_cells * 4,
+                               buf.size() * 4, cudaMemcpyDeviceToHost));
+        for (size_t X = 0; X < NX; ++X)
+            for (size_t Z = 0; Z < NZ; ++Z)
+                out[X * NZ + Z] = in_frame(h, X, Z) ? (double)buf[pml_index_host(h, X, Z)] : 0.0;
+        return SM_OK;
+    }
     if (part == SM_PART_TOTAL) {
         std::vector<unsigned char> buf(NX * (size_t)h->pitch * e);
         SM_CUDA_TRY(cudaMemcpy(buf.data(),
@@ -2310,6 +2901,50 @@ extern "C" int sm_eiso_set_field(sm_eiso_t h, size_t shot, int comp, int part, c
     DeviceGuard g(h->device);
     SM_CUDA_TRY(cudaStreamSynchronize(h->stream));
     const size_t NX = h->NX, NZ = h->NZ, e = h->elem;
+    if (eiso_isb(h)) {
+        // split parts FP32; the totals (the interior value, or the sum of
+        // the parts in the frame) encoded block by block as the step does
+        std::vector<double> cur(NX * NZ);
+        if (part != SM_PART_TOTAL)
+            if (int rc = sm_eiso_get_field(h, shot, comp, SM_PART_TOTAL, cur.data())) return rc;
+        std::vector<float> px(h->npml_cells), pz(h->npml_cells);
+        char *dpx = static_cast<char *>(h->xpart[h->cur][f].p) + shot * h->npml_cells * 4;
+        char *dpz = static_cast<char *>(h->zpart[h->cur][f].p) + shot * h->npml_cells * 4;
+        SM_CUDA_TRY(cudaMemcpy(px.data(), dpx, px.size() * 4, cudaMemcpyDeviceToHost));
+        SM_CUDA_TRY(cudaMemcpy(pz.data(), dpz, pz.size() * 4, cudaMemcpyDeviceToHost));
+        std::vector<float> tot(NX * NZ);
+        for (size_t X = 0; X < NX; ++X)
+            for (size_t Z = 0; Z < NZ; ++Z) {
+                const double v = in[X * NZ + Z];
+                if (!in_frame(h, X, Z)) {
+                    tot[X * NZ + Z] = (float)(part == SM_PART_TOTAL ? v : cur[X * NZ + Z]);
+                    continue;
+                }
+                const size_t c = pml_index_host(h, X, Z);
+                if (part == SM_PART_X) px[c] = (float)v;
+                if (part == SM_PART_Z) pz[c] = (float)v;
+                tot[X * NZ + Z] = px[c] + pz[c];
+            }
+        std::vector<int16_t> m(NX * (size_t)h->pitch, 0);
+        std::vector<uint8_t> ex(h->nxb * (size_t)h->pitch, 0);
+        for (size_t xb = 0; xb < h->nxb; ++xb)
+            for (size_t Z = 0; Z < NZ; ++Z) {
+                const size_t xa = xb * EISO_EB, xe = std::min(xa + EISO_EB, NX);
+                float mx = 0.f;
+                for (size_t X = xa; X < xe; ++X) mx = std::max(mx, std::fabs(tot[X * NZ + Z]));
+                const unsigned e8 = bfp_e8_host(mx);
+                ex[xb * h->pitch + Z] = (uint8_t)e8;
+                for (size_t X = xa; X < xe; ++X) m[X * h->pitch + Z] = bfp_man_host(tot[X * NZ + Z], e8);
+            }
+        SM_CUDA_TRY(cudaMemcpy(static_cast<char *>(h->field(h->cur, f)) + shot * h->args.fstride * 2,
+                               m.data(), m.size() * 2, cudaMemcpyHostToDevice));
+        SM_CUDA_TRY(cudaMemcpy(static_cast<char *>(h->fexp[h->cur].p) + f * h->args.estride +
+                                   shot * ex.size(),
+                               ex.data(), ex.size(), cudaMemcpyHostToDevice));
+        SM_CUDA_TRY(cudaMemcpy(dpx, px.data(), px.size() * 4, cudaMemcpyHostToDevice));
+        SM_CUDA_TRY(cudaMemcpy(dpz, pz.data(), pz.size() * 4, cudaMemcpyHostToDevice));
+        return SM_OK;
+    }
     std::vector<unsigned char> tot(NX * (size_t)h->pitch * e), px(h->npml_cells * e),
         pz(h->npml_cells * e);
     char *dtot = static_cast<char *>(h->field(h->cur, f)) + shot * h->args.fstride * e;
@@ -2361,9 +2996,9 @@ extern "C" int sm_eiso_stream(sm_eiso_t h, void **stream) {
 
 extern "C" int sm_eiso_set_config(sm_eiso_t h, int config) {
     if (int rc = eiso_check(h)) return rc;
-    if (config < 0 || config >= kEisoNumConfigs)
+    if (config < 0 || config >= eiso_ncfg(h))
         return sm_fail(SM_EINVAL, "sm_eiso_set_config: config %d not in [0, %d)", config,
-                       kEisoNumConfigs);
+                       eiso_ncfg(h));
     DeviceGuard g(h->device);
     int lim = 0;
     SM_CUDA_TRY(cudaDeviceGetAttribute(&lim, cudaDevAttrMaxSharedMemoryPerBlockOptin, h->device));
@@ -2381,7 +3016,7 @@ extern "C" int sm_eiso_set_config(sm_eiso_t h, int config) {
 extern "C" int sm_eiso_get_config(sm_eiso_t h, int *config, int *nconfigs) {
     if (int rc = eiso_check(h)) return rc;
     if (config) *config = h->config;
-    if (nconfigs) *nconfigs = kEisoNumConfigs;
+    if (nconfigs) *nconfigs = eiso_ncfg(h);
     return SM_OK;
 }
 

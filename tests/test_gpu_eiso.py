@@ -216,3 +216,100 @@ def test_16bit_storage_stays_in_range_and_close_to_fp64(precision):
     ref = api.run_eiso(p, "fp64")[0]
     err = H.rel_l2(got, ref)
     assert err < TOL16[precision], err
+
+
+# ---------------------------------------------------------------------------
+# Block floating point (SM_BFP16): the five wavefields as 16-bit mantissas
+# sharing one exponent per 4 consecutive x rows of a z column, split parts
+# FP32, FP32 arithmetic.  The oracle's storage-rounding mode applies the same
+# rounding to its FP64 state.  Bounds as for a_iso_3d: 4 steps from a random
+# state within 1e-4 of the plain FP64 oracle and 2e-5 of the rounding oracle
+# (the device's FP32 arithmetic lands on the other side of a rounding
+# boundary now and then); whole shots within the 1e-3 gate.
+# ---------------------------------------------------------------------------
+BFP_BLOCK = 4
+
+
+def _bfp_pair(nx, nz, P, seed):
+    rng = np.random.default_rng(seed)
+    vp = 3000 + 1000 * rng.random((nx, nz))
+    vs = vp / (1.6 + 0.3 * rng.random((nx, nz)))
+    rho = 2000 + 400 * rng.random((nx, nz))
+    la, mu, l2m, b, bm, vpmax = O.eiso_materials(vp, vs, rho)
+    h = 1.0
+    dt = 0.5 * h / (math.sqrt(2) * vpmax)
+    d, dh, dH = O.eiso_profiles(P, h, vp)
+    args = (nx, nz, P, h, dt, la, mu, l2m, b, bm, d, dh, dH)
+    plain, rounded = O.EIso(*args), O.EIso(*args)
+    rounded.set_bfp(BFP_BLOCK, "x")
+    dev = api.EIsoDevice(*args, "bfp16")
+    NX, NZ = nx + 2 * P, nz + 2 * P
+    inter = np.zeros((NX, NZ), bool)
+    inter[P:P + nx, P:P + nz] = True
+    for f in FIELDS:
+        scale = 1e-3 if f.startswith("v") else 1e4
+        tot, xp, zp = (scale * rng.standard_normal((NX, NZ)) for _ in range(3))
+        xp[inter] = 0
+        zp[inter] = 0
+        dev.set_field(f, xp, part="x")
+        dev.set_field(f, zp, part="z")
+        dev.set_field(f, np.where(inter, tot, 0), part="total")
+        # the oracles start from the stored (rounded) state
+        for o in (plain, rounded):
+            o.set(f, "x", dev.get_field(f, part="x"))
+            o.set(f, "z", dev.get_field(f, part="z"))
+            o.set(f, "total", dev.get_field(f, part="total"))
+    return plain, rounded, dev
+
+
+@pytest.mark.parametrize("shape", [(13, 9, 3), (9, 14, 4), (33, 40, 8), (40, 12, 2), (37, 29, 5)])
+def test_bfp16_steps_from_random_state(shape):
+    nx, nz, P = shape
+    plain, rounded, dev = _bfp_pair(nx, nz, P, sum(shape) + 3)
+    for _ in range(4):
+        for o in (plain, rounded):
+            o.velocity()
+            o.stress()
+    dev.run(4)
+    for f in FIELDS:
+        got = dev.get_field(f, part="total")
+        e_r = O.rel_l2(got, rounded.get(f, "total"))
+        e_p = O.rel_l2(got, plain.get(f, "total"))
+        assert e_r < 2e-5 and e_p < 1e-4, (f, e_r, e_p)
+        for part in ("x", "z"):
+            e = O.rel_l2(dev.get_field(f, part=part), rounded.get(f, part))
+            assert e < 2e-5, (f, part, e)
+    dev.close()
+
+
+def test_bfp16_every_launch_config_and_batch_identical():
+    p = W.cfg2(nx=150, nz=130, npml=9, nsteps=90, nshots=3, nrec=12)
+    dev, n = api.eiso_device(p, "bfp16")
+    nconf = dev.get_config()[1]
+    dev.run(n)
+    ref = [dev.traces(s) for s in range(3)]
+    for config in range(nconf):
+        dev.reset()
+        dev.set_config(config)
+        dev.run(n)
+        for s in range(3):
+            for x, y in zip(dev.traces(s), ref[s]):
+                np.testing.assert_array_equal(x, y, err_msg=f"config {config} shot {s}")
+    dev.close()
+    alone = api.run_eiso(p, "bfp16", shots=[2])[0]
+    for a, b in zip(ref[2], alone):
+        np.testing.assert_array_equal(a, b)
+
+
+def test_bfp16_shot_within_gate_and_as_the_rounding_oracle_predicts():
+    p = W.cfg2(nx=300, nz=160, npml=12, nsteps=800, nshots=1, nrec=24)
+    p.shots = [[("Bulk", 1.0, 50.0, 150.0, 5.0), ("Sxz", 0.5, 40.0, 40.0, 100.0)]]
+    got = api.run_eiso(p, "bfp16")[0]
+    assert all(np.isfinite(t).all() for t in got)
+    ref = api.run_eiso(p, "fp64")[0]
+    err = H.rel_l2(got, ref)
+    assert err < 1e-3, err
+    plain, _, _ = H.run_eiso_oracle(p)
+    pred, _, _ = H.run_eiso_oracle(p, bfp_block=BFP_BLOCK, bfp_axis="x")
+    predicted = H.rel_l2(pred, plain)
+    assert 0.5 * predicted < err < 2.0 * predicted, (err, predicted)

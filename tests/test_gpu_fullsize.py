@@ -157,3 +157,11 @@ def test_a3d_544cube_bfp16_whole_shot_within_1e_3():
     got = api.run_a3d(p, "bfp16")
     ref = api.run_a3d(p, "fp64")
     assert H.rel_l2(got, ref) < 1e-3
+
+
+def test_eiso_1040x540_bfp16_64_shots_whole_shots_within_1e_3():
+    p = W.cfg2()
+    batch = api.run_eiso(p, "bfp16")
+    for shot in (0, 63):
+        ref = api.run_eiso(p, "fp64", shots=[shot])[0]
+        assert H.rel_l2(batch[shot], ref) < 1e-3, shot

@@ -20,7 +20,7 @@ def _problems():
             W.cfg0(nx=210, nz=180, npml=12, nsteps=120, nrec=9)]
 
 
-@pytest.mark.parametrize("precision", ["fp32", "fp64", "fp16"])
+@pytest.mark.parametrize("precision", ["fp32", "fp64", "fp16", "bfp16"])
 def test_group_equals_separate_runs(precision):
     probs = _problems()
     devs, ns = zip(*[api.eiso_device(p, precision) for p in probs])
