@@ -102,6 +102,19 @@ int sm_abi_version(void);
 /* device count and the SM count / HBM size of one device */
 int sm_device_info(int device, int *sm_count, size_t *hbm_bytes, size_t *hbm_free);
 
+/* Cache of the handles' large device arrays (no counterpart in the
+ * reference, whose programs allocate once per run).  Destroying an e_iso or
+ * a_iso_3d handle gives its wavefield, memory-variable and material arrays
+ * to a per-device cache, and creating a handle takes blocks of the same size
+ * (rounded to 2 MiB) from it, so shot after shot runs without cudaMalloc /
+ * cudaFree of the state.  At most `bytes` per device stay cached (32 GiB by
+ * default); sm_pool_trim frees every cached block, and an allocation that
+ * fails trims the cache and tries once more.  sm_pool_cached reports the
+ * bytes held. */
+int sm_pool_trim(int device, size_t *freed);
+int sm_pool_set_limit(int device, size_t bytes);
+int sm_pool_cached(int device, size_t *bytes);
+
 /* ======================================================================
  * host-side set-up, FP64, identical in arithmetic to the reference
  * ====================================================================== */

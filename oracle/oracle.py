@@ -62,6 +62,7 @@ def _load():
     lib.orc_eiso_get.argtypes = [C.c_void_p, C.c_int, C.c_int, _dp]
     lib.orc_eiso_set.argtypes = [C.c_void_p, C.c_int, C.c_int, _dp]
     lib.orc_eiso_set_bfp.argtypes = [C.c_void_p, C.c_int, C.c_int]
+    lib.orc_eiso_add_patch.argtypes = [C.c_void_p, C.c_long, C.c_long, C.c_long, C.c_long]
     lib.orc_eiso_probe.restype = C.c_double
     lib.orc_eiso_probe.argtypes = [C.c_void_p, C.c_int, _sz]
     lib.orc_a3d_pad_model.argtypes = [_sz, _sz, _sz, _sz, _dp, _dp, _dp, _dp]
@@ -203,6 +204,10 @@ class EIso:
         """checker mode: the state a step stores is rounded to 16-bit block
         floating point with blocks of `block` cells along x or z (0: FP64)"""
         lib().orc_eiso_set_bfp(self.h_, int(block), 0 if axis == "x" else 1)
+
+    def add_patch(self, X0, Z0, rows, cols):
+        """checker mode: padded cells the block storage keeps exact"""
+        lib().orc_eiso_add_patch(self.h_, int(X0), int(Z0), int(rows), int(cols))
 
     def probe(self, field, index):
         return lib().orc_eiso_probe(self.h_, FIELDS_E[field], int(index))

@@ -208,6 +208,9 @@ struct orc_eiso {
     double *f[5], *fx[5], *fz[5];
     int bfp_block;             /* 0: FP64 storage; else block floating point */
     int bfp_axis;              /* blocks along X (0) or Z (1) */
+    /* rectangles of cells the block storage keeps exact (source patches) */
+    int npatch;
+    long patch[16][4];         /* first X, first Z, rows, columns */
 };
 
 enum { M_B = 0, M_BM = 1, M_LA = 2, M_L2M = 3, M_MU = 4 };
@@ -251,6 +254,16 @@ void orc_eiso_free(orc_eiso *o)
     free(o->d);
     for (int k = 0; k < 5; ++k) { free(o->f[k]); free(o->fx[k]); free(o->fz[k]); }
     free(o);
+}
+
+/* a cell of a rectangle the block storage keeps exact */
+static int e_in_patch(const orc_eiso *o, long X, long Z)
+{
+    for (int q = 0; q < o->npatch; ++q) {
+        const long *p = o->patch[q];
+        if (X >= p[0] && X < p[0] + p[2] && Z >= p[1] && Z < p[1] + p[3]) return 1;
+    }
+    return 0;
 }
 
 static int e_interior(const orc_eiso *o, long X, long Z)
@@ -392,11 +405,28 @@ void orc_eiso_stress(orc_eiso *o)
      * stresses, totals on the padded grid in blocks of B cells along Z;
      * the frame's split parts keep their precision, as the device keeps
      * them in FP32); the stress update above read the unrounded velocities */
-    if (o->bfp_block)
+    if (o->bfp_block && o->npatch == 0)
         for (int k = 0; k < 5; ++k) {
             if (o->bfp_axis == 0) bfp_round_cols(o->f[k], o->NX, o->NZ, o->bfp_block);
             else bfp_round_rows(o->f[k], o->NX, o->NZ, o->bfp_block);
         }
+    if (o->bfp_block && o->npatch > 0) {   /* blocks along X, patches kept exact */
+        size_t B = (size_t)o->bfp_block;
+        for (int k = 0; k < 5; ++k)
+            for (size_t x0 = 0; x0 < o->NX; x0 += B) {
+                size_t nb = x0 + B < o->NX ? B : o->NX - x0;
+                for (size_t Z = 0; Z < o->NZ; ++Z)
+                    if (!e_in_patch(o, (long)x0, (long)Z))
+                        bfp_round_strided(o->f[k] + x0 * o->NZ + Z, o->NZ, nb);
+            }
+    }
+}
+
+void orc_eiso_add_patch(orc_eiso *o, long X0, long Z0, long rows, long cols)
+{
+    if (o->npatch >= 16) return;
+    long *p = o->patch[o->npatch++];
+    p[0] = X0; p[1] = Z0; p[2] = rows; p[3] = cols;
 }
 
 void orc_eiso_set_bfp(orc_eiso *o, int block, int axis)
@@ -413,7 +443,8 @@ void orc_eiso_add_source(orc_eiso *o, size_t index, int type, double value)
     if (type == 0 || type == 6) o->f[ORC_TXX][q] += value;
     if (type == 2 || type == 6) o->f[ORC_TZZ][q] += value;
     if (type == 4) o->f[ORC_TXZ][q] += value;
-    if (o->bfp_block) {   /* the block of the source cell is stored again */
+    if (o->bfp_block && !e_in_patch(o, (long)(q / o->NZ), (long)(q % o->NZ))) {
+        /* the block of the source cell is stored again */
         size_t B = (size_t)o->bfp_block, Z = q % o->NZ, X = q / o->NZ;
         for (int k = ORC_TXX; k <= ORC_TXZ; ++k) {
             if (o->bfp_axis == 0) {

@@ -85,6 +85,9 @@ void orc_eiso_set(orc_eiso *o, int field, int part, const double *in);
  * X or Z of the padded grid) when a step stores it (no counterpart in the
  * reference) */
 void orc_eiso_set_bfp(orc_eiso *o, int block, int axis);   /* axis 0: X, 1: Z */
+/* a rectangle of padded cells (first X, first Z, rows, columns) the block
+ * storage keeps exact: the source patches of the device's block storage */
+void orc_eiso_add_patch(orc_eiso *o, long X0, long Z0, long rows, long cols);
 double orc_eiso_probe(const orc_eiso *o, int field, size_t index);
 
 /* ---------------- a_iso_3d ---------------- */

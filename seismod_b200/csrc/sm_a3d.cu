@@ -1708,8 +1708,11 @@ template <typename C>
 int a3d_upload_materials(sm_a3d *h, const double *rho, const double *vp, double dt, size_t nx2,
                          size_t ny2, size_t nz2) {
     const size_t pitch = (size_t)h->pitch, ncell = nx2 * ny2 * pitch;
-    std::unique_ptr<C[]> r(new (std::nothrow) C[ncell]), kk(new (std::nothrow) C[ncell]);
-    if (!r || !kk) return sm_fail(SM_ENOMEM, "sm_a3d_create: out of host memory");
+    // pinned staging (cached across handles): the copies run at full link speed
+    PinnedBuf rb, kb;
+    if (int rc = rb.get(ncell * sizeof(C))) return rc;
+    if (int rc = kb.get(ncell * sizeof(C))) return rc;
+    C *r = rb.as<C>(), *kk = kb.as<C>();
     auto fill = [&](size_t ib, size_t ie) {
         for (size_t i = ib; i < ie; ++i)
             for (size_t j = 0; j < ny2; ++j) {
@@ -1731,8 +1734,9 @@ int a3d_upload_materials(sm_a3d *h, const double *rho, const double *vp, double 
         if (ib < ie) pool.emplace_back(fill, ib, ie);
     }
     for (auto &th : pool) th.join();
-    SM_CUDA_TRY(cudaMemcpy(h->rho.p, r.get(), ncell * sizeof(C), cudaMemcpyHostToDevice));
-    SM_CUDA_TRY(cudaMemcpy(h->K.p, kk.get(), ncell * sizeof(C), cudaMemcpyHostToDevice));
+    SM_CUDA_TRY(cudaMemcpyAsync(h->rho.p, r, ncell * sizeof(C), cudaMemcpyHostToDevice, h->stream));
+    SM_CUDA_TRY(cudaMemcpyAsync(h->K.p, kk, ncell * sizeof(C), cudaMemcpyHostToDevice, h->stream));
+    SM_CUDA_TRY(cudaStreamSynchronize(h->stream));   // the staging goes back to the cache
     return SM_OK;
 }
 
@@ -1790,7 +1794,7 @@ extern "C" int sm_a3d_create(int device, size_t nx2, size_t ny2, size_t nz2, siz
     int rc;
     for (int b = 0; b < 2; ++b)
         for (int f = 0; f < 4; ++f)
-            if ((rc = h->f[b][f].alloc(ncell * h->elem))) return rc;
+            if ((rc = h->f[b][f].alloc_pooled(ncell * h->elem, device))) return rc;
     h->psi_cells[PS_PX] = h->psi_cells[PS_VX] = 2 * np * ny2 * (size_t)h->pitch;
     h->psi_cells[PS_PY] = h->psi_cells[PS_VY] = nx2 * 2 * np * (size_t)h->pitch;
     h->psi_cells[PS_PZ] = h->psi_cells[PS_VZ] = nx2 * ny2 * 2 * np;
@@ -1798,15 +1802,15 @@ extern "C" int sm_a3d_create(int device, size_t nx2, size_t ny2, size_t nz2, siz
     const size_t pelem = precision == SM_BFP16 ? 4 : h->elem;
     for (int b = 0; b < 2; ++b)
         for (int p = 0; p < 6; ++p)
-            if ((rc = h->psi[b][p].alloc(h->psi_cells[p] * pelem))) return rc;
+            if ((rc = h->psi[b][p].alloc_pooled(h->psi_cells[p] * pelem, device))) return rc;
     if (precision == SM_BFP16) {
         h->nyb = (ny2 + A3_BJ - 1) / A3_BJ;
         for (int b = 0; b < 2; ++b)
             for (int f = 0; f < 4; ++f)
-                if ((rc = h->fe[b][f].alloc(nx2 * h->nyb * (size_t)h->pitch))) return rc;
+                if ((rc = h->fe[b][f].alloc_pooled(nx2 * h->nyb * (size_t)h->pitch, device))) return rc;
     }
-    if ((rc = h->rho.alloc(ncell * cb))) return rc;
-    if ((rc = h->K.alloc(ncell * cb))) return rc;
+    if ((rc = h->rho.alloc_pooled(ncell * cb, device))) return rc;
+    if ((rc = h->K.alloc_pooled(ncell * cb, device))) return rc;
     rc = precision == SM_FP64 ? a3d_upload_materials<double>(h.get(), rho, vp, dt, nx2, ny2, nz2)
                               : a3d_upload_materials<float>(h.get(), rho, vp, dt, nx2, ny2, nz2);
     if (rc) return rc;

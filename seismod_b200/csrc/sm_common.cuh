@@ -153,19 +153,58 @@ inline int16_t bfp_man_host(float v, unsigned e8) {
 }
 
 // ---------------------------------------------------------------------------
-// owning device buffer
+// cache of large device blocks and pinned host blocks (sm_pool.cu)
+// ---------------------------------------------------------------------------
+int pool_get(int device, size_t bytes, void **out);
+void pool_put(int device, void *ptr, size_t bytes);
+int pinned_get(size_t bytes, void **out);
+void pinned_put(void *ptr, size_t bytes);
+
+// pinned host staging block, given back to the cache on scope exit
+struct PinnedBuf {
+    void *p = nullptr;
+    size_t bytes = 0;
+    PinnedBuf() = default;
+    PinnedBuf(const PinnedBuf &) = delete;
+    PinnedBuf &operator=(const PinnedBuf &) = delete;
+    ~PinnedBuf() { pinned_put(p, bytes); }
+    int get(size_t n) {
+        bytes = n;
+        return pinned_get(n, &p);
+    }
+    template <typename T>
+    T *as() const { return static_cast<T *>(p); }
+};
+
+// ---------------------------------------------------------------------------
+// owning device buffer.  alloc: cudaMalloc / cudaFree.  alloc_pooled: a block
+// of the device cache, given back on release, which the owner may only do
+// when no work in flight uses it (handle teardown after its streams finished)
 // ---------------------------------------------------------------------------
 struct DevBuf {
     void *p = nullptr;
     size_t bytes = 0;
+    int pool_dev = -1;
     DevBuf() = default;
     DevBuf(const DevBuf &) = delete;
     DevBuf &operator=(const DevBuf &) = delete;
     ~DevBuf() { release(); }
     void release() {
-        if (p) cudaFree(p);
+        if (p) {
+            if (pool_dev >= 0) pool_put(pool_dev, p, bytes);
+            else cudaFree(p);
+        }
         p = nullptr;
         bytes = 0;
+        pool_dev = -1;
+    }
+    int alloc_pooled(size_t n, int device) {
+        release();
+        if (n == 0) return SM_OK;
+        if (int rc = pool_get(device, n, &p)) return rc;
+        bytes = n;
+        pool_dev = device;
+        return SM_OK;
     }
     int alloc(size_t n) {
         release();

@@ -78,6 +78,13 @@ struct EisoArgs {
     void *feo;
     long long estride;
     int nxb;
+    // ... and its source patches: per shot the first patch (pfirst[nshots]
+    // = total), per patch its first row and column, and their FP32 values
+    // [patch][field][EISO_PR][EISO_PC] in the set read and the set written
+    const int *pfirst;
+    const int *pxz;
+    float *pv;
+    float *pvo;
 };
 
 __device__ __forceinline__ bool e_inside(const EisoArgs &a, int X, int Z) {
@@ -639,6 +646,22 @@ __global__ void __launch_bounds__(32 * W, MINB) eiso_slabg_kernel(const EisoArgs
 // velocities of the step; only the state the step stores is rounded.
 // ---------------------------------------------------------------------------
 #define EISO_EB 4
+// Source patches: near a source the wavefield is many times larger than
+// anywhere else and changes by orders of magnitude within a few cells, so the
+// rounding of 16-bit block storage there (2^-16 of the block's largest value
+// per step) radiates noise that dominates the traces of nearby receivers.
+// Block storage therefore keeps the cells around each source in FP32: a
+// patch of EISO_PR x rows (whole blocks, EISO_PB blocks on each side of the
+// source's block) by EISO_PC z columns centred on the source, one per source
+// (patches of a shot are disjoint; a source inside or next to another's patch
+// gets none).  The patch's values live in a side array of the buffer set;
+// the mantissas of those cells are written too (a state without its patches
+// is still a valid rounded state).
+#define EISO_PB 2
+#define EISO_PR (EISO_EB * (2 * EISO_PB + 1))
+#define EISO_PZ 4
+#define EISO_PC (2 * EISO_PZ + 1)
+#define EISO_PF (EISO_PR * EISO_PC)   // values per field of a patch
 
 struct EisoBMaps {
     CUtensorMap f;   // mantissas of the old set: (z, x, shot, field), box (BW, TX+2, 1, 5)
@@ -656,7 +679,8 @@ struct ESlabB {
     static_assert(BW <= 256 && BWE <= 256, "TMA box dimension");
     static constexpr size_t al(size_t x) { return (x + 127) / 128 * 128; }
     static constexpr size_t oE = al(5 * (size_t)RX * BW * 2);
-    static constexpr size_t oBar = oE + al(5 * (size_t)NB * BWE);
+    static constexpr size_t oStg = oE + al(5 * (size_t)NB * BWE);   // [5][EB][threads] floats
+    static constexpr size_t oBar = oStg + al(5 * (size_t)EISO_EB * 32 * W * 4);
     static constexpr size_t bytes = oBar + 16;
     static constexpr unsigned tx = (unsigned)(5 * RX * BW * 2 + 5 * NB * BWE);
 };
@@ -697,6 +721,22 @@ __device__ __forceinline__ void eiso_bslab_body(const EisoArgs &a, const CUtenso
     const long long sb = (long long)shot * a.sstride;
     const C zero = C(0);
     const int of = Z - zs, oe = Z - zse;
+    // this lane's source patch (the one whose columns hold Z and whose rows
+    // meet the box), -1 if none; cta_patch: the box meets any patch of the shot
+    int lp = -1, lpx = 0, lpz = 0;
+    bool cta_patch = false;
+    if (a.pfirst) {
+        for (int q = a.pfirst[shot]; q < a.pfirst[shot + 1]; ++q) {
+            const int px = a.pxz[2 * q], pz = a.pxz[2 * q + 1];
+            const bool rows = px <= X0 + TX && px + EISO_PR > X0 - 1;
+            cta_patch = cta_patch || (rows && pz <= Zc + 30 * W && pz + EISO_PC > Zc - 1);
+            if (rows && Z >= pz && Z < pz + EISO_PC) { lp = q; lpx = px; lpz = pz; }
+        }
+    }
+    auto in_patch = [&](int X) { return lp >= 0 && X >= lpx && X < lpx + EISO_PR; };
+    auto pidx = [&](int f, int X) {
+        return ((long long)lp * 5 + f) * EISO_PF + (X - lpx) * EISO_PC + (Z - lpz);
+    };
     // decoder of field f's block b of the box (0: the block holding row
     // X0-1; 1 .. TX/EB: the slab's own; TX/EB+1: the block holding X0+TX)
     auto DE = [&](int f, int b) -> BDec { return bfp_dec(ebox[(f * L::NB + b) * L::BWE + oe]); };
@@ -710,7 +750,7 @@ __device__ __forceinline__ void eiso_bslab_body(const EisoArgs &a, const CUtenso
         return __ldg(static_cast<const C *>(a.mat[m]) + (long long)x * a.pitch + Z);
     };
     const bool zint = (Z0 - 1 >= a.np) && (Z0 + 30 <= a.np + a.nz - 1);
-    const bool lean = zint && X0 >= a.np && X1 <= a.np + a.nx - 1;
+    const bool lean = zint && X0 >= a.np && X1 <= a.np + a.nx - 1 && !cta_patch;
     int16_t *const fo0 = static_cast<int16_t *>(a.fo[0]);
     const long long fso = static_cast<int16_t *>(a.fo[1]) - fo0;
     uint8_t *const eo0 = static_cast<uint8_t *>(a.feo) + (long long)shot * a.nxb * a.pitch + Z;
@@ -734,40 +774,56 @@ __device__ __forceinline__ void eiso_bslab_body(const EisoArgs &a, const CUtenso
     };
 
     if (lean) {
+        // the lean slab lies inside the grid (rows X0-1 .. X0+TX, every lane's
+        // column): materials by unchecked loads from row pointers
+        const long long mrow = (long long)(X0 - 1) * a.pitch + Z;
+        const C *mB = static_cast<const C *>(a.mat[M_B]) + mrow;
+        const C *mBM = static_cast<const C *>(a.mat[M_BM]) + mrow;
+        const C *mLA = static_cast<const C *>(a.mat[M_LA]) + mrow;
+        const C *mL2M = static_cast<const C *>(a.mat[M_L2M]) + mrow;
+        const C *mMU = static_cast<const C *>(a.mat[M_MU]) + mrow;
         C nb[TX], cbm[TX], cla[TX], cl2m[TX], cmu[TX];
-        const C b1 = M(1, M_B), bm0 = M(0, M_BM);
+        const C b1 = __ldg(mB + a.pitch), bm0 = __ldg(mBM);
 #pragma unroll
         for (int r = 0; r < TX; ++r) {
-            nb[r] = M(r + 2, M_B);
-            cbm[r] = M(r + 1, M_BM);
-            cla[r] = M(r + 1, M_LA);
-            cl2m[r] = M(r + 1, M_L2M);
-            cmu[r] = M(r + 1, M_MU);
+            nb[r] = __ldg(mB + (long long)(r + 2) * a.pitch);
+            cbm[r] = __ldg(mBM + (long long)(r + 1) * a.pitch);
+            cla[r] = __ldg(mLA + (long long)(r + 1) * a.pitch);
+            cl2m[r] = __ldg(mL2M + (long long)(r + 1) * a.pitch);
+            cmu[r] = __ldg(mMU + (long long)(r + 1) * a.pitch);
         }
         if (!__all_sync(full, mbar_wait(bar, 0, a.err, 9))) {
             mbar_wait(bar, 0, a.err, 9);
             return;
         }
+        // decoders of every block of the box, once; each value decoded once
+        BDec D[5][L::NB];
+#pragma unroll
+        for (int f = 0; f < 5; ++f)
+#pragma unroll
+            for (int b = 0; b < L::NB; ++b) D[f][b] = DE(f, b);
+        auto FV = [&](int rho, int f) -> C {
+            return bfp_val(fbox[(f * L::RX + rho) * L::BW + of], D[f][blk(rho)]);
+        };
         C vxc, vzp;
+        C c_txz = FV(1, F_TXZ), c_txx = FV(1, F_TXX);
         {
-            const C c_txz = F(1, F_TXZ), p_tzz = F(0, F_TZZ);
+            const C p_tzz = FV(0, F_TZZ);
             const C txz_zm = __shfl_up_sync(full, c_txz, 1);
             const C tzz_zp = __shfl_down_sync(full, p_tzz, 1);
-            vxc = r_fma(b1, r_add(r_sub(F(1, F_TXX), F(0, F_TXX)), r_sub(c_txz, txz_zm)), F(1, F_VX));
+            vxc = r_fma(b1, r_add(r_sub(c_txx, FV(0, F_TXX)), r_sub(c_txz, txz_zm)), FV(1, F_VX));
             vzp = zero;
             if (X0 - 1 >= a.np)
-                vzp = r_fma(bm0, r_add(r_sub(c_txz, F(0, F_TXZ)), r_sub(tzz_zp, p_tzz)), F(0, F_VZ));
-        }
-        if (X0 - 1 < a.np) {
-            ESplit<C> sp;
-            const EisoProf P{a.NX, a.NZ};
-            const C *pr = static_cast<const C *>(a.prof);
-            e_load_split<float, C>(a, sb, X0 - 1, Z, zin, sp);
-            const EZProf<C> zp{pr[P.azn() + Z], pr[P.bzn() + Z], pr[P.azh() + Z], pr[P.bzh() + Z]};
-            const C c_txz = F(1, F_TXZ), p_tzz = F(0, F_TZZ);
-            const C tzz_zp = __shfl_down_sync(full, p_tzz, 1);
-            vzp = e_vz<float, C>(a, sb, X0 - 1, Z, F(0, F_VZ), bm0, r_sub(c_txz, F(0, F_TXZ)),
-                                 r_sub(tzz_zp, p_tzz), sp.vz, zp, false);
+                vzp = r_fma(bm0, r_add(r_sub(c_txz, FV(0, F_TXZ)), r_sub(tzz_zp, p_tzz)), FV(0, F_VZ));
+            if (X0 - 1 < a.np) {
+                ESplit<C> sp;
+                const EisoProf P{a.NX, a.NZ};
+                const C *pr = static_cast<const C *>(a.prof);
+                e_load_split<float, C>(a, sb, X0 - 1, Z, zin, sp);
+                const EZProf<C> zp{pr[P.azn() + Z], pr[P.bzn() + Z], pr[P.azh() + Z], pr[P.bzh() + Z]};
+                vzp = e_vz<float, C>(a, sb, X0 - 1, Z, FV(0, F_VZ), bm0, r_sub(c_txz, FV(0, F_TXZ)),
+                                     r_sub(tzz_zp, p_tzz), sp.vz, zp, false);
+            }
         }
         const bool vm[EB] = {own, own, own, own};
         C bvx[EB], bvz[EB], btxx[EB], btzz[EB], btxz[EB];
@@ -775,9 +831,8 @@ __device__ __forceinline__ void eiso_bslab_body(const EisoArgs &a, const CUtenso
 #pragma unroll
         for (int r = 0; r < TX; ++r) {
             const int rc = r + 1;
-            const C n_txz = F(rc + 1, F_TXZ), c_txz = F(rc, F_TXZ), c_tzz = F(rc, F_TZZ);
-            const C c_txx = F(rc, F_TXX), n_txx = F(rc + 1, F_TXX);
-            const C n_vx = F(rc + 1, F_VX), c_vz = F(rc, F_VZ);
+            const C n_txz = FV(rc + 1, F_TXZ), n_txx = FV(rc + 1, F_TXX), n_vx = FV(rc + 1, F_VX);
+            const C c_tzz = FV(rc, F_TZZ), c_vz = FV(rc, F_VZ);
             const C txz_zm = __shfl_up_sync(full, n_txz, 1);
             const C tzz_zp = __shfl_down_sync(full, c_tzz, 1);
             const C ax = r_sub(n_txx, c_txx), az = r_sub(n_txz, txz_zm);
@@ -800,18 +855,49 @@ __device__ __forceinline__ void eiso_bslab_body(const EisoArgs &a, const CUtenso
                 store_block(F_TXX, q, btxx, vm);
                 store_block(F_TZZ, q, btzz, vm);
                 store_block(F_TXZ, q, btxz, vm);
+                bvx[0] = vxn;
             } else {
                 bvx[t + 1] = vxn;
             }
-            if (t == EB - 1 && r + 1 < TX) bvx[0] = vxn;
             vxc = vxn;
             vzp = vzn;
+            c_txz = n_txz;
+            c_txx = n_txx;
         }
         return;
     }
 
-    // general march (frame): unrolled over the slab's rows, rows past the
-    // grid's end masked; split parts FP32 as in the other precisions
+    // general march (the frame, the grid's ends and source patches): one
+    // row per iteration, not unrolled (the frame's code is long), the
+    // values of a block staged per thread in shared memory until the
+    // block's last row; split parts FP32 as in the other precisions; cells
+    // of a source patch read and write their FP32 values
+    float *stg = reinterpret_cast<float *>(smem + L::oStg) + threadIdx.x;
+    auto S_ = [&](int f, int t) -> float & { return stg[(f * EB + t) * 32 * W]; };
+    auto Fg = [&](int rho, int f) -> C {   // rho known at run time
+        const int X = X0 - 1 + rho;
+        if (in_patch(X)) return a.pv[pidx(f, X)];
+        return bfp_val(fbox[(f * L::RX + rho) * L::BW + of], DE(f, blk(rho)));
+    };
+    // the block of rows X0 + EB q .. (the first n of them in the grid) of
+    // every field, from the staged values
+    auto store_staged = [&](int q, int n) {
+        const int Xb = X0 + EB * q;
+        const bool pb = in_patch(Xb);
+#pragma unroll
+        for (int f = 0; f < 5; ++f) {
+            C v[EB];
+            bool vm[EB];
+#pragma unroll
+            for (int t = 0; t < EB; ++t) {
+                v[t] = S_(f, t);
+                vm[t] = own && t < n;
+            }
+            store_block(f, q, v, vm);
+            if (pb && own)
+                for (int t = 0; t < n; ++t) a.pvo[pidx(f, Xb + t)] = v[t];
+        }
+    };
     const C *pr = static_cast<const C *>(a.prof);
     const EisoProf P{a.NX, a.NZ};
     EZProf<C> zp{C(1), C(1), C(1), C(1)};
@@ -824,94 +910,82 @@ __device__ __forceinline__ void eiso_bslab_body(const EisoArgs &a, const CUtenso
     }
     C vxc, vzp;
     {
-        const C c_txz = F(1, F_TXZ), p_tzz = F(0, F_TZZ);
+        const C c_txz = Fg(1, F_TXZ), p_tzz = Fg(0, F_TZZ);
         const C txz_zm = __shfl_up_sync(full, c_txz, 1);
         const C tzz_zp = __shfl_down_sync(full, p_tzz, 1);
         // vx(X0) is this slab's row: its split parts are stored here
-        vxc = zin ? e_vx<float, C>(a, sb, X0, Z, F(1, F_VX), M(1, M_B), r_sub(F(1, F_TXX), F(0, F_TXX)),
-                                   r_sub(c_txz, txz_zm), sp.vx, zp, own)
+        vxc = zin ? e_vx<float, C>(a, sb, X0, Z, Fg(1, F_VX), M(1, M_B),
+                                   r_sub(Fg(1, F_TXX), Fg(0, F_TXX)), r_sub(c_txz, txz_zm), sp.vx,
+                                   zp, own)
                   : zero;
         vzp = zero;
         if (X0 >= 1 && zin)
-            vzp = e_vz<float, C>(a, sb, X0 - 1, Z, F(0, F_VZ), M(0, M_BM), r_sub(c_txz, F(0, F_TXZ)),
-                                 r_sub(tzz_zp, p_tzz), sp.vz, zp, false);
+            vzp = e_vz<float, C>(a, sb, X0 - 1, Z, Fg(0, F_VZ), M(0, M_BM),
+                                 r_sub(c_txz, Fg(0, F_TXZ)), r_sub(tzz_zp, p_tzz), sp.vz, zp,
+                                 false);
     }
+    S_(F_VX, 0) = vxc;
     e_load_split<float, C>(a, sb, X0, Z, zin, sp);
-    C bvx[EB], bvz[EB], btxx[EB], btzz[EB], btxz[EB];
-    bool vm[EB];
-    bvx[0] = vxc;
-#pragma unroll
-    for (int r = 0; r < TX; ++r) {
-        const int X = X0 + r;
-        const bool valid = X < X1;
-        const int rc = r + 1;
-        const int t = r % EB;
-        vm[t] = own && valid;
-        C vxn = zero, vzn = zero, txx = zero, tzz = zero, txz = zero;
-        if (valid) {   // uniform across the CTA
-            ESplit<C> sn;
-            e_load_split<float, C>(a, sb, X + 1, Z, zin && X + 1 < X1, sn);
-            const bool fast = zint && X >= a.np && X + 1 <= a.np + a.nx - 1;
-            const C n_b = M(rc + 1, M_B), c_bm = M(rc, M_BM);
-            const C la = M(rc, M_LA), l2m = M(rc, M_L2M), mu = M(rc, M_MU);
-            const C n_txz = F(rc + 1, F_TXZ), c_txz = F(rc, F_TXZ), c_tzz = F(rc, F_TZZ);
-            const C c_txx = F(rc, F_TXX);
-            const C txz_zm = __shfl_up_sync(full, n_txz, 1);
-            const C tzz_zp = __shfl_down_sync(full, c_tzz, 1);
-            const C ax = r_sub(F(rc + 1, F_TXX), c_txx), az = r_sub(n_txz, txz_zm);
-            const C bx_ = r_sub(n_txz, c_txz), bz = r_sub(tzz_zp, c_tzz);
-            if (fast) {
-                vxn = r_fma(n_b, r_add(ax, az), F(rc + 1, F_VX));
-                vzn = r_fma(c_bm, r_add(bx_, bz), F(rc, F_VZ));
-            } else {
-                // vx(X+1) belongs to this slab when X+1 < X1 (its split
-                // parts are stored then); the last row's is the next slab's
-                vxn = (X + 1 < a.NX && zin)
-                          ? e_vx<float, C>(a, sb, X + 1, Z, F(rc + 1, F_VX), n_b, ax, az, sp.vx, zp,
-                                           own && X + 1 < X1)
-                          : zero;
-                vzn = zin ? e_vz<float, C>(a, sb, X, Z, F(rc, F_VZ), c_bm, bx_, bz, sp.vz, zp, own)
-                          : zero;
-            }
-            const C vz_zm = __shfl_up_sync(full, vzn, 1);
-            const C vx_zp = __shfl_down_sync(full, vxc, 1);
-            const C sax = r_sub(vxn, vxc), saz = r_sub(vzn, vz_zm);
-            const C sbz = r_sub(vx_zp, vxc), sbx = r_sub(vzn, vzp);
-            if (fast || (zin && e_inside(a, X, Z))) {
-                txx = r_add(c_txx, r_fma(l2m, sax, r_mul(la, saz)));
-                tzz = r_add(c_tzz, r_fma(l2m, saz, r_mul(la, sax)));
-                txz = r_fma(mu, r_add(sbz, sbx), c_txz);
-            } else if (zin) {
-                const long long cc = sb + e_pml_index(a, X, Z);
-                const C Axh = pr[P.axh() + X], Bxh = pr[P.bxh() + X];
-                txx = e_frame<float, C>(a, F_TXX, cc, Axh, Bxh, zp.An, zp.Bn, sp.t[0], sp.t[1], l2m,
-                                        la, sax, saz, own);
-                tzz = e_frame<float, C>(a, F_TZZ, cc, Axh, Bxh, zp.An, zp.Bn, sp.t[2], sp.t[3], la,
-                                        l2m, sax, saz, own);
-                txz = e_frame<float, C>(a, F_TXZ, cc, pr[P.axn() + X], pr[P.bxn() + X], zp.Ah, zp.Bh,
-                                        sp.t[4], sp.t[5], mu, mu, sbx, sbz, own);
-            }
-            sp = sn;
-        }
-        bvz[t] = vzn;
-        btxx[t] = txx;
-        btzz[t] = tzz;
-        btxz[t] = txz;
-        if (t == EB - 1) {
-            const int q = r / EB;
-            if (X0 + EB * q < X1) {   // uniform across the CTA
-                store_block(F_VX, q, bvx, vm);
-                store_block(F_VZ, q, bvz, vm);
-                store_block(F_TXX, q, btxx, vm);
-                store_block(F_TZZ, q, btzz, vm);
-                store_block(F_TXZ, q, btxz, vm);
-            }
-            if (r + 1 < TX) bvx[0] = vxn;
+#pragma unroll 1
+    for (int X = X0; X < X1; ++X) {
+        const int r = X - X0, rc = r + 1, t = r % EB;
+        ESplit<C> sn;
+        e_load_split<float, C>(a, sb, X + 1, Z, zin && X + 1 < X1, sn);
+        const bool fast = zint && X >= a.np && X + 1 <= a.np + a.nx - 1;
+        const C n_b = M(rc + 1, M_B), c_bm = M(rc, M_BM);
+        const C la = M(rc, M_LA), l2m = M(rc, M_L2M), mu = M(rc, M_MU);
+        const C n_txz = Fg(rc + 1, F_TXZ), c_txz = Fg(rc, F_TXZ), c_tzz = Fg(rc, F_TZZ);
+        const C c_txx = Fg(rc, F_TXX);
+        const C txz_zm = __shfl_up_sync(full, n_txz, 1);
+        const C tzz_zp = __shfl_down_sync(full, c_tzz, 1);
+        const C ax = r_sub(Fg(rc + 1, F_TXX), c_txx), az = r_sub(n_txz, txz_zm);
+        const C bx_ = r_sub(n_txz, c_txz), bz = r_sub(tzz_zp, c_tzz);
+        C vxn, vzn;
+        if (fast) {
+            vxn = r_fma(n_b, r_add(ax, az), Fg(rc + 1, F_VX));
+            vzn = r_fma(c_bm, r_add(bx_, bz), Fg(rc, F_VZ));
         } else {
-            bvx[t + 1] = vxn;
+            // vx(X+1) belongs to this slab when X+1 < X1 (its split parts
+            // are stored then); the last row's is the next slab's
+            vxn = (X + 1 < a.NX && zin)
+                      ? e_vx<float, C>(a, sb, X + 1, Z, Fg(rc + 1, F_VX), n_b, ax, az, sp.vx, zp,
+                                       own && X + 1 < X1)
+                      : zero;
+            vzn = zin ? e_vz<float, C>(a, sb, X, Z, Fg(rc, F_VZ), c_bm, bx_, bz, sp.vz, zp, own)
+                      : zero;
+        }
+        const C vz_zm = __shfl_up_sync(full, vzn, 1);
+        const C vx_zp = __shfl_down_sync(full, vxc, 1);
+        const C sax = r_sub(vxn, vxc), saz = r_sub(vzn, vz_zm);
+        const C sbz = r_sub(vx_zp, vxc), sbx = r_sub(vzn, vzp);
+        C txx = zero, tzz = zero, txz = zero;
+        if (fast || (zin && e_inside(a, X, Z))) {
+            txx = r_add(c_txx, r_fma(l2m, sax, r_mul(la, saz)));
+            tzz = r_add(c_tzz, r_fma(l2m, saz, r_mul(la, sax)));
+            txz = r_fma(mu, r_add(sbz, sbx), c_txz);
+        } else if (zin) {
+            const long long cc = sb + e_pml_index(a, X, Z);
+            const C Axh = pr[P.axh() + X], Bxh = pr[P.bxh() + X];
+            txx = e_frame<float, C>(a, F_TXX, cc, Axh, Bxh, zp.An, zp.Bn, sp.t[0], sp.t[1], l2m, la,
+                                    sax, saz, own);
+            tzz = e_frame<float, C>(a, F_TZZ, cc, Axh, Bxh, zp.An, zp.Bn, sp.t[2], sp.t[3], la, l2m,
+                                    sax, saz, own);
+            txz = e_frame<float, C>(a, F_TXZ, cc, pr[P.axn() + X], pr[P.bxn() + X], zp.Ah, zp.Bh,
+                                    sp.t[4], sp.t[5], mu, mu, sbx, sbz, own);
+        }
+        S_(F_VZ, t) = vzn;
+        S_(F_TXX, t) = txx;
+        S_(F_TZZ, t) = tzz;
+        S_(F_TXZ, t) = txz;
+        if (t == EB - 1 || X + 1 == X1) {   // uniform across the CTA
+            store_staged(r / EB, t + 1);
+            S_(F_VX, 0) = vxn;   // the next block's first row
+        } else {
+            S_(F_VX, t + 1) = vxn;
         }
         vxc = vxn;
         vzp = vzn;
+        sp = sn;
     }
 }
 
@@ -1145,6 +1219,7 @@ struct SrcEntry {
     // grid, the source's row rs in it) and its exponent index qe, per shot
     long long qb, qe;
     int nb, rs;
+    long long pq;     // its cell's value (field 0) in the source patches, or -1
 };
 
 // add_src (src.c:170-184) for one shot, into the wavefields f just written
@@ -1190,6 +1265,7 @@ struct RecEntry {
     int group;         // sampling group
     long long out;     // offset of its first sample in the trace buffer
     long long qe;      // block storage: the exponent index of its block, per shot
+    long long pq;      // its cell's value (field 0) in the source patches, or -1
 };
 
 // one receiver's sample of step it, if the record's predicate takes it
@@ -1240,7 +1316,7 @@ __device__ __forceinline__ void eiso_binject(void *const *f, long long fstride, 
                                              long long estride, long long eshot, int pitch,
                                              long long it, const SrcEntry *src,
                                              const int *shot_first, const double *vals, int shot,
-                                             int *err) {
+                                             int *err, float *pv) {
     for (int e = shot_first[shot]; e < shot_first[shot + 1]; ++e) {
         const SrcEntry s = src[e];
         if (it >= s.len) continue;
@@ -1253,6 +1329,8 @@ __device__ __forceinline__ void eiso_binject(void *const *f, long long fstride, 
             if (fs[k] < 0) continue;
             eiso_badd(static_cast<int16_t *>(f[fs[k]]) + (long long)shot * fstride,
                       static_cast<uint8_t *>(fe) + fs[k] * estride + shot * eshot, s, pitch, v, err);
+            // the source's patch holds the cell in FP32: add there exactly
+            if (s.pq >= 0 && pv) pv[s.pq + fs[k] * EISO_PF] += v;
         }
     }
 }
@@ -1263,16 +1341,21 @@ __global__ void eiso_bsource_kernel(EisoArgs a, const SrcEntry *src, const int *
     const int shot = blockIdx.x * blockDim.x + threadIdx.x;
     if (shot >= nshots) return;
     eiso_binject(a.f, a.fstride, a.fe, a.estride, (long long)a.nxb * a.pitch, a.pitch, it, src,
-                 shot_first, vals, shot, a.err);
+                 shot_first, vals, shot, a.err, a.pfirst ? a.pv : nullptr);
 }
 
 __device__ __forceinline__ void eiso_bsample(void *const *f, long long fstride, const void *fe,
                                              long long estride, long long eshot, long long it,
                                              const RecEntry &e, const int32_t *table,
-                                             long long nsteps_max, double *traces) {
+                                             long long nsteps_max, double *traces,
+                                             const float *pv) {
     if (it >= nsteps_max) return;
     const int32_t slot = table[(long long)e.group * nsteps_max + it];
     if (slot < 0) return;
+    if (e.pq >= 0 && pv) {   // a cell of a source patch: its FP32 value
+        traces[e.out + slot] = static_cast<double>(pv[e.pq + e.field * EISO_PF]);
+        return;
+    }
     const int16_t m = static_cast<const int16_t *>(f[e.field])[(long long)e.shot * fstride + e.q];
     const unsigned e8 =
         static_cast<const uint8_t *>(fe)[e.field * estride + e.shot * eshot + e.qe];
@@ -1284,7 +1367,7 @@ __global__ void eiso_bgather_kernel(EisoArgs a, const RecEntry *rec, int nrec,
     const int r = blockIdx.x * blockDim.x + threadIdx.x;
     if (r >= nrec) return;
     eiso_bsample(a.f, a.fstride, a.fe, a.estride, (long long)a.nxb * a.pitch, *a.step - 1, rec[r],
-                 table, nsteps_max, traces);
+                 table, nsteps_max, traces, a.pfirst ? a.pv : nullptr);
 }
 
 // ---------------------------------------------------------------------------
@@ -1369,6 +1452,7 @@ struct EisoPost {
     long long estride, eshot;
     int pitch;
     int *err;
+    float *pv;   // source patches of the set just written (null: none)
 };
 
 struct EisoGroupPostParams {
@@ -1388,7 +1472,7 @@ __global__ void eiso_group_source_kernel(const __grid_constant__ EisoGroupPostPa
     const EisoPost &q = P.q[p];
     if constexpr (std::is_same<S, Bfp16>::value)
         eiso_binject(q.f, q.fstride, q.fe, q.estride, q.eshot, q.pitch, *q.step - 1, q.src,
-                     q.src_first, q.vals, t - P.first_src[p], q.err);
+                     q.src_first, q.vals, t - P.first_src[p], q.err, q.pv);
     else
         eiso_inject<S>(q.f, q.fstride, q.sc, q.isc, *q.step - 1, q.src, q.src_first, q.vals,
                        t - P.first_src[p]);
@@ -1403,7 +1487,7 @@ __global__ void eiso_group_gather_kernel(const __grid_constant__ EisoGroupPostPa
     const EisoPost &q = P.q[p];
     if constexpr (std::is_same<S, Bfp16>::value)
         eiso_bsample(q.f, q.fstride, q.fe, q.estride, q.eshot, *q.step - 1,
-                     q.rec[t - P.first_rec[p]], q.table, q.nsteps_max, q.traces);
+                     q.rec[t - P.first_rec[p]], q.table, q.nsteps_max, q.traces, q.pv);
     else
         eiso_sample<S>(q.f, q.fstride, q.isc, *q.step - 1, q.rec[t - P.first_rec[p]], q.table,
                        q.nsteps_max, q.traces);
@@ -1452,6 +1536,10 @@ struct sm_eiso {
     size_t nxb = 0;
     EisoBMaps bmaps[2];
     int bmap_key = -1;
+    // ... and its source patches (EISO_PR x EISO_PC cells in FP32 around
+    // each source): first row and column per patch, first patch per shot
+    std::vector<int> p_xz, p_first;
+    DevBuf d_pxz, d_pfirst, pside[2];
     DevBuf d_step;               // device step counter (EisoArgs::step)
     // CUDA graphs of graph_steps steps, one per parity of the starting
     // buffer set; captured again when graph_epoch moved since (new sources,
@@ -1503,6 +1591,8 @@ void eiso_bind(sm_eiso *h) {
     const int c = h->cur, o = 1 - h->cur;
     h->args.fe = h->fexp[c].p;
     h->args.feo = h->fexp[o].p;
+    h->args.pv = h->pside[c].as<float>();
+    h->args.pvo = h->pside[o].as<float>();
     for (int f = 0; f < 5; ++f) {
         h->args.f[f] = h->field(c, f);
         h->args.fx[f] = h->xpart[c][f].p;
@@ -1843,8 +1933,81 @@ int eiso_rescale(sm_eiso *h) {
     return rc;
 }
 
+// the patch holding padded cell (X, Z) of a shot, or -1
+int eiso_patch_of(const sm_eiso *h, size_t shot, long X, long Z) {
+    if (h->p_first.empty()) return -1;
+    for (int q = h->p_first[shot]; q < h->p_first[shot + 1]; ++q) {
+        const long px = h->p_xz[2 * q], pz = h->p_xz[2 * q + 1];
+        if (X >= px && X < px + EISO_PR && Z >= pz && Z < pz + EISO_PC) return q;
+    }
+    return -1;
+}
+
+long long eiso_patch_index(const sm_eiso *h, int q, long X, long Z) {
+    return (long long)q * 5 * EISO_PF + (X - h->p_xz[2 * q]) * EISO_PC + (Z - h->p_xz[2 * q + 1]);
+}
+
+// Source patches of block storage, from the shots' sources: one per source
+// whose rectangle keeps clear of the shot's earlier patches (rows apart by a
+// slab's reach, so a slab meets at most one patch per column); built only
+// for a handle at step 0 (the patches start from a zero state), dropped
+// otherwise.  Marks the receivers for upload (they look up their patch).
+int eiso_build_patches(sm_eiso *h) {
+    h->p_xz.clear();
+    h->p_first.assign(h->nshots + 1, 0);
+    h->args.pfirst = nullptr;
+    h->args.pxz = nullptr;
+    h->rec_dirty = 1;
+    if (h->it != 0) {
+        h->p_first.clear();
+        return SM_OK;
+    }
+    constexpr long kReach = 18;   // rows of the widest slab box
+    for (size_t s = 0; s < h->nshots; ++s) {
+        h->p_first[s] = (int)(h->p_xz.size() / 2);
+        for (SrcEntry &e : h->shot_src[s]) {
+            const long X = (long)(e.q / h->pitch), Z = (long)(e.q % h->pitch);
+            const long px = EISO_EB * (X / EISO_EB - EISO_PB), pz = Z - EISO_PZ;
+            bool clear = true;
+            for (int q = h->p_first[s]; q < (int)(h->p_xz.size() / 2); ++q) {
+                const long qx = h->p_xz[2 * q], qz = h->p_xz[2 * q + 1];
+                const bool zo = pz < qz + EISO_PC && qz < pz + EISO_PC;
+                const bool xo = px - kReach < qx + EISO_PR && qx - kReach < px + EISO_PR;
+                if (zo && xo) clear = false;
+            }
+            if (!clear) continue;
+            h->p_xz.push_back((int)px);
+            h->p_xz.push_back((int)pz);
+        }
+    }
+    const int np = (int)(h->p_xz.size() / 2);
+    h->p_first[h->nshots] = np;
+    if (np == 0) {
+        h->p_first.clear();
+        return SM_OK;
+    }
+    int rc;
+    if ((rc = h->d_pxz.alloc(h->p_xz.size() * sizeof(int)))) return rc;
+    if ((rc = h->d_pfirst.alloc(h->p_first.size() * sizeof(int)))) return rc;
+    for (int k = 0; k < 2; ++k) {
+        if ((rc = h->pside[k].alloc((size_t)np * 5 * EISO_PF * sizeof(float)))) return rc;
+        if ((rc = h->pside[k].zero(h->stream))) return rc;
+    }
+    SM_CUDA_TRY(cudaMemcpyAsync(h->d_pxz.p, h->p_xz.data(), h->p_xz.size() * sizeof(int),
+                                cudaMemcpyHostToDevice, h->stream));
+    SM_CUDA_TRY(cudaMemcpyAsync(h->d_pfirst.p, h->p_first.data(), h->p_first.size() * sizeof(int),
+                                cudaMemcpyHostToDevice, h->stream));
+    SM_CUDA_TRY(cudaStreamSynchronize(h->stream));
+    h->args.pfirst = h->d_pfirst.as<int>();
+    h->args.pxz = h->d_pxz.as<int>();
+    eiso_bind(h);
+    return SM_OK;
+}
+
 int upload_sources(sm_eiso *h) {
     h->graph_epoch++;
+    if (eiso_isb(h))
+        if (int rc = eiso_build_patches(h)) return rc;
     std::vector<SrcEntry> all;
     std::vector<int> first(h->nshots + 1, 0);
     std::vector<double> vals;
@@ -1853,6 +2016,10 @@ int upload_sources(sm_eiso *h) {
         long long base = (long long)vals.size();
         for (SrcEntry e : h->shot_src[s]) {
             e.voff += base;
+            e.pq = -1;
+            const long X = (long)(e.q / h->pitch), Z = (long)(e.q % h->pitch);
+            const int q = eiso_patch_of(h, s, X, Z);
+            if (q >= 0) e.pq = eiso_patch_index(h, q, X, Z);
             all.push_back(e);
         }
         vals.insert(vals.end(), h->shot_vals[s].begin(), h->shot_vals[s].end());
@@ -1906,6 +2073,10 @@ int upload_receivers(sm_eiso *h) {
             RecEntry e = sr.entries[r];
             e.group += gbase;
             e.out = out + (long long)r * (long long)sr.plan.max_samples;
+            e.pq = -1;
+            const long X = (long)(e.q / h->pitch), Z = (long)(e.q % h->pitch);
+            const int q = eiso_patch_of(h, s, X, Z);
+            if (q >= 0) e.pq = eiso_patch_index(h, q, X, Z);
             all.push_back(e);
         }
         out += (long long)sr.entries.size() * (long long)sr.plan.max_samples;
@@ -2058,6 +2229,7 @@ int eiso_source_entry(size_t nx, size_t nz, size_t np, size_t pitch, size_t inde
         e->nb = (int)std::min<size_t>(EISO_EB, NX - xb * EISO_EB);
         e->rs = (int)(X - xb * EISO_EB);
     }
+    e->pq = -1;
     e->type = type;
     e->voff = (long long)vals.size();
     e->len = (int)length;
@@ -2074,6 +2246,7 @@ int eiso_receiver_entry(size_t nx, size_t nz, size_t np, size_t pitch, size_t in
     *e = RecEntry{};
     e->q = (long long)(index / nz + np) * (long long)pitch + (long long)(index % nz + np);
     e->qe = (long long)((index / nz + np) / EISO_EB) * (long long)pitch + (long long)(index % nz + np);
+    e->pq = -1;
     e->field = f;
     e->group = group;
     return SM_OK;
@@ -2161,15 +2334,16 @@ extern "C" int sm_eiso_create(int device, size_t nx, size_t nz, size_t npml, dou
         h->args.estride = (long long)(nshots * h->nxb * (size_t)h->pitch);
     }
     for (int k = 0; k < 2; ++k) {
-        if ((rc = h->fset[k].alloc(5 * h->fset_stride))) return rc;
+        if ((rc = h->fset[k].alloc_pooled(5 * h->fset_stride, device))) return rc;
         for (int f = 0; f < 5; ++f) {
-            if ((rc = h->xpart[k][f].alloc(h->npml_cells * nshots * pelem))) return rc;
-            if ((rc = h->zpart[k][f].alloc(h->npml_cells * nshots * pelem))) return rc;
+            if ((rc = h->xpart[k][f].alloc_pooled(h->npml_cells * nshots * pelem, device))) return rc;
+            if ((rc = h->zpart[k][f].alloc_pooled(h->npml_cells * nshots * pelem, device))) return rc;
         }
-        if (precision == SM_BFP16 && (rc = h->fexp[k].alloc(5 * (size_t)h->args.estride)))
+        if (precision == SM_BFP16 &&
+            (rc = h->fexp[k].alloc_pooled(5 * (size_t)h->args.estride, device)))
             return rc;
     }
-    if ((rc = h->matbuf.alloc(5 * h->mat_stride))) return rc;
+    if ((rc = h->matbuf.alloc_pooled(5 * h->mat_stride, device))) return rc;
     EisoProf P{(int)NX, (int)NZ};
     if ((rc = h->prof.alloc((size_t)P.size() * cplx))) return rc;
     if ((rc = h->err.alloc(sizeof(int)))) return rc;
@@ -2240,6 +2414,7 @@ extern "C" int sm_eiso_reset(sm_eiso_t h) {
     for (int k = 0; k < 2; ++k) {
         if (int rc = h->fset[k].zero(h->stream)) return rc;
         if (int rc = h->fexp[k].zero(h->stream)) return rc;
+        if (int rc = h->pside[k].zero(h->stream)) return rc;
         for (int f = 0; f < 5; ++f) {
             if (int rc = h->xpart[k][f].zero(h->stream)) return rc;
             if (int rc = h->zpart[k][f].zero(h->stream)) return rc;
@@ -2489,6 +2664,7 @@ int eiso_group_step(sm_eiso *const *hs, int n, cudaStream_t st) {
         q.eshot = (long long)h->nxb * h->pitch;
         q.pitch = h->pitch;
         q.err = h->args.err;
+        q.pv = h->args.pfirst ? h->args.pv : nullptr;
         Q.first_src[k] = nsrc;
         Q.first_rec[k] = nrec;
         nsrc += h->d_src.bytes ? (int)h->nshots : 0;
@@ -2859,6 +3035,16 @@ extern "C" int sm_eiso_get_field(sm_eiso_t h, size_t shot, int comp, int part, d
                 for (size_t Z = 0; Z < NZ; ++Z)
                     out[X * NZ + Z] = bfp_value_host(m[X * h->pitch + Z],
                                                      ex[(X / EISO_EB) * h->pitch + Z]);
+            if (h->args.pfirst) {   // cells of source patches: their FP32 values
+                std::vector<float> pv(h->pside[h->cur].bytes / sizeof(float));
+                SM_CUDA_TRY(cudaMemcpy(pv.data(), h->pside[h->cur].p, h->pside[h->cur].bytes,
+                                       cudaMemcpyDeviceToHost));
+                for (int q = h->p_first[shot]; q < h->p_first[shot + 1]; ++q)
+                    for (long X = h->p_xz[2 * q]; X < h->p_xz[2 * q] + EISO_PR; ++X)
+                        for (long Z = h->p_xz[2 * q + 1]; Z < h->p_xz[2 * q + 1] + EISO_PC; ++Z)
+                            if (X >= 0 && X < (long)NX && Z >= 0 && Z < (long)NZ)
+                                out[X * NZ + Z] = pv[eiso_patch_index(h, q, X, Z) + f * EISO_PF];
+            }
             return SM_OK;
         }
         const DevBuf &src = part == SM_PART_X ? h->xpart[h->cur][f] : h->zpart[h->cur][f];
@@ -2943,6 +3129,18 @@ extern "C" int sm_eiso_set_field(sm_eiso_t h, size_t shot, int comp, int part, c
                                ex.data(), ex.size(), cudaMemcpyHostToDevice));
         SM_CUDA_TRY(cudaMemcpy(dpx, px.data(), px.size() * 4, cudaMemcpyHostToDevice));
         SM_CUDA_TRY(cudaMemcpy(dpz, pz.data(), pz.size() * 4, cudaMemcpyHostToDevice));
+        if (h->args.pfirst) {   // cells of source patches keep the FP32 totals
+            std::vector<float> pv(h->pside[h->cur].bytes / sizeof(float));
+            SM_CUDA_TRY(cudaMemcpy(pv.data(), h->pside[h->cur].p, h->pside[h->cur].bytes,
+                                   cudaMemcpyDeviceToHost));
+            for (int q = h->p_first[shot]; q < h->p_first[shot + 1]; ++q)
+                for (long X = h->p_xz[2 * q]; X < h->p_xz[2 * q] + EISO_PR; ++X)
+                    for (long Z = h->p_xz[2 * q + 1]; Z < h->p_xz[2 * q + 1] + EISO_PC; ++Z)
+                        if (X >= 0 && X < (long)NX && Z >= 0 && Z < (long)NZ)
+                            pv[eiso_patch_index(h, q, X, Z) + f * EISO_PF] = tot[X * NZ + Z];
+            SM_CUDA_TRY(cudaMemcpy(h->pside[h->cur].p, pv.data(), h->pside[h->cur].bytes,
+                                   cudaMemcpyHostToDevice));
+        }
         return SM_OK;
     }
     std::vector<unsigned char> tot(NX * (size_t)h->pitch * e), px(h->npml_cells * e),

@@ -61,6 +61,26 @@ def eiso_receivers(p):
     return out
 
 
+# the source patches of e_iso block storage: EISO_PR rows (whole blocks of
+# 4, two blocks on each side of the source's) by EISO_PC columns centred on
+# each source, in source order, a patch only where it keeps clear of the
+# shot's earlier ones (by 18 rows when their columns meet)
+EISO_PR, EISO_PC = 20, 9
+
+
+def eiso_source_patches(p, srcs):
+    out = []
+    for (idx, _, _) in srcs:
+        X, Z = idx // p.nz + p.npml, idx % p.nz + p.npml
+        px, pz = 4 * (X // 4 - 2), Z - 4
+        clear = all(not (pz < qz + EISO_PC and qz < pz + EISO_PC and
+                         px - 18 < qx + EISO_PR and qx - 18 < px + EISO_PR)
+                    for (qx, qz) in out)
+        if clear:
+            out.append((px, pz))
+    return out
+
+
 def run_eiso_oracle(p, shot=0, nsteps=None, fields_at=None, bfp_block=0, bfp_axis="x"):
     """FP64 oracle run.  Returns (traces list of np arrays, times list,
     optional dict of padded fields after the last step).  bfp_block > 0
@@ -72,6 +92,9 @@ def run_eiso_oracle(p, shot=0, nsteps=None, fields_at=None, bfp_block=0, bfp_axi
     if bfp_block:
         o.set_bfp(bfp_block, bfp_axis)
     srcs = eiso_sources(p, shot)
+    if bfp_block:
+        for (px, pz) in eiso_source_patches(p, srcs):
+            o.add_patch(px, pz, EISO_PR, EISO_PC)
     recs = eiso_receivers(p)
     tr = [[] for _ in recs]
     tt = [[] for _ in recs]
