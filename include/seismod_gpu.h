@@ -508,7 +508,7 @@ int sm_eiso_run_noalloc(int device, void *stream, const sm_eiso_request *r, doub
  * drop-in programs: the whole of e_iso / a_iso_3d main() on the device,
  * reading the reference's .par / model / source / output files and writing
  * its trc/<base>/<base>_<n>.trc files.  argv as the reference takes it
- * (io_utils.c:156-202: -p file.par, -v, -h); an added "-P fp32|fp64|fp16|bf16"
+ * (io_utils.c:156-202: -p file.par, -v, -h); an added "-P fp32|fp64|bfp16|fp16|bf16"
  * picks the storage precision (default fp32).  Returns 0 on success.
  * ====================================================================== */
 int sm_e_iso_main(int argc, char **argv);

@@ -1268,6 +1268,7 @@ static const int kA3NumConfigs = sizeof(kA3Configs) / sizeof(kA3Configs[0]);
 // block storage: every thread holds one block of A3_BJ rows
 static const A3Config kA3BConfigs[] = {
     {8, A3_BJ, 4, 2}, {4, A3_BJ, 4, 3}, {8, A3_BJ, 5, 1}, {4, A3_BJ, 6, 3}, {16, A3_BJ, 4, 1},
+    {8, A3_BJ, 4, 3}, {4, A3_BJ, 4, 5},
 };
 static const int kA3BNumConfigs = sizeof(kA3BConfigs) / sizeof(kA3BConfigs[0]);
 
@@ -1534,6 +1535,8 @@ size_t a3d_bconfig_smem(int config) {
     case 1: return a3d_bstep_smem<4 * A3_BJ, 4>();
     case 2: return a3d_bstep_smem<8 * A3_BJ, 5>();
     case 3: return a3d_bstep_smem<4 * A3_BJ, 6>();
+    case 5: return a3d_bstep_smem<8 * A3_BJ, 4>();
+    case 6: return a3d_bstep_smem<4 * A3_BJ, 4>();
     default: return a3d_bstep_smem<16 * A3_BJ, 4>();
     }
 }
@@ -1544,6 +1547,8 @@ int a3d_bready(sm_a3d *h) {
     case 1: return a3d_bready_cfg<4, 4, 3>(h);
     case 2: return a3d_bready_cfg<8, 5, 1>(h);
     case 3: return a3d_bready_cfg<4, 6, 3>(h);
+    case 5: return a3d_bready_cfg<8, 4, 3>(h);
+    case 6: return a3d_bready_cfg<4, 4, 5>(h);
     default: return a3d_bready_cfg<16, 4, 1>(h);
     }
 }
@@ -1554,6 +1559,8 @@ int a3d_blaunch_step(sm_a3d *h) {
     case 1: return a3d_blaunch_cfg<4, 4, 3>(h);
     case 2: return a3d_blaunch_cfg<8, 5, 1>(h);
     case 3: return a3d_blaunch_cfg<4, 6, 3>(h);
+    case 5: return a3d_blaunch_cfg<8, 4, 3>(h);
+    case 6: return a3d_blaunch_cfg<4, 4, 5>(h);
     default: return a3d_blaunch_cfg<16, 4, 1>(h);
     }
 }

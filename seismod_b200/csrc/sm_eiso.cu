@@ -756,6 +756,7 @@ __device__ __forceinline__ void eiso_bslab_body(const EisoArgs &a, const CUtenso
     uint8_t *const eo0 = static_cast<uint8_t *>(a.feo) + (long long)shot * a.nxb * a.pitch + Z;
     // store block q (rows X0 + EB q ..) of field f from v[EB]; rows past the
     // grid's end (vmask false) are left out of the exponent and not stored
+    bool overflow = false;   // a block beyond the format's range (reported once)
     auto store_block = [&](int f, int q, const C *v, const bool *vm) {
         unsigned mx = 0;
 #pragma unroll
@@ -767,10 +768,9 @@ __device__ __forceinline__ void eiso_bslab_body(const EisoArgs &a, const CUtenso
 #pragma unroll
         for (int t = 0; t < EB; ++t)
             if (vm[t]) o[(long long)t * a.pitch] = bfp_man(v[t], esc);
-        if (vm[0]) {   // a lane that owns the column and a block inside the grid
+        if (vm[0])   // a lane that owns the column and a block inside the grid
             eo0[(long long)f * a.estride + (long long)(xb0 + q) * a.pitch] = (uint8_t)e8;
-            if (over) atomicExch(a.err, 4);
-        }
+        overflow = overflow || (vm[0] && over);
     };
 
     if (lean) {
@@ -796,15 +796,12 @@ __device__ __forceinline__ void eiso_bslab_body(const EisoArgs &a, const CUtenso
             mbar_wait(bar, 0, a.err, 9);
             return;
         }
-        // decoders of every block of the box, once; each value decoded once
-        BDec D[5][L::NB];
-#pragma unroll
-        for (int f = 0; f < 5; ++f)
-#pragma unroll
-            for (int b = 0; b < L::NB; ++b) D[f][b] = DE(f, b);
-        auto FV = [&](int rho, int f) -> C {
-            return bfp_val(fbox[(f * L::RX + rho) * L::BW + of], D[f][blk(rho)]);
+        // each value decoded once; a field's decoder is taken when the march
+        // enters the block (TXZ, TXX, VX are read one row ahead of TZZ, VZ)
+        auto FVd = [&](int rho, int f, const BDec &d) -> C {
+            return bfp_val(fbox[(f * L::RX + rho) * L::BW + of], d);
         };
+        auto FV = [&](int rho, int f) -> C { return FVd(rho, f, DE(f, blk(rho))); };
         C vxc, vzp;
         C c_txz = FV(1, F_TXZ), c_txx = FV(1, F_TXX);
         {
@@ -828,11 +825,22 @@ __device__ __forceinline__ void eiso_bslab_body(const EisoArgs &a, const CUtenso
         const bool vm[EB] = {own, own, own, own};
         C bvx[EB], bvz[EB], btxx[EB], btzz[EB], btxz[EB];
         bvx[0] = vxc;
+        BDec dn[3], dc[2];   // decoders of TXZ, TXX, VX at row rc + 1; TZZ, VZ at row rc
 #pragma unroll
         for (int r = 0; r < TX; ++r) {
             const int rc = r + 1;
-            const C n_txz = FV(rc + 1, F_TXZ), n_txx = FV(rc + 1, F_TXX), n_vx = FV(rc + 1, F_VX);
-            const C c_tzz = FV(rc, F_TZZ), c_vz = FV(rc, F_VZ);
+            if (r == 0 || blk(rc + 1) != blk(rc)) {
+                dn[0] = DE(F_TXZ, blk(rc + 1));
+                dn[1] = DE(F_TXX, blk(rc + 1));
+                dn[2] = DE(F_VX, blk(rc + 1));
+            }
+            if (r == 0 || blk(rc) != blk(rc - 1)) {
+                dc[0] = DE(F_TZZ, blk(rc));
+                dc[1] = DE(F_VZ, blk(rc));
+            }
+            const C n_txz = FVd(rc + 1, F_TXZ, dn[0]), n_txx = FVd(rc + 1, F_TXX, dn[1]);
+            const C n_vx = FVd(rc + 1, F_VX, dn[2]);
+            const C c_tzz = FVd(rc, F_TZZ, dc[0]), c_vz = FVd(rc, F_VZ, dc[1]);
             const C txz_zm = __shfl_up_sync(full, n_txz, 1);
             const C tzz_zp = __shfl_down_sync(full, c_tzz, 1);
             const C ax = r_sub(n_txx, c_txx), az = r_sub(n_txz, txz_zm);
@@ -864,6 +872,7 @@ __device__ __forceinline__ void eiso_bslab_body(const EisoArgs &a, const CUtenso
             c_txz = n_txz;
             c_txx = n_txx;
         }
+        if (overflow) atomicExch(a.err, 4);
         return;
     }
 
@@ -987,6 +996,7 @@ __device__ __forceinline__ void eiso_bslab_body(const EisoArgs &a, const CUtenso
         vzp = vzn;
         sp = sn;
     }
+    if (overflow) atomicExch(a.err, 4);
 }
 
 template <int W, int TX, int MINB>
@@ -1622,7 +1632,8 @@ static const int kEisoNumConfigs = sizeof(kEisoConfigs) / sizeof(kEisoConfigs[0]
 struct EisoBConfig {
     int w, tx, minb;
 };
-static const EisoBConfig kEisoBConfigs[] = {{2, 8, 8}, {4, 8, 4}, {2, 4, 12}, {4, 4, 6}, {1, 8, 16}};
+static const EisoBConfig kEisoBConfigs[] = {{2, 8, 8}, {4, 8, 4}, {2, 4, 12}, {4, 4, 6}, {1, 8, 16},
+                                            {2, 8, 12}, {2, 4, 16}, {4, 8, 6}};
 static const int kEisoBNumConfigs = sizeof(kEisoBConfigs) / sizeof(kEisoBConfigs[0]);
 
 bool eiso_isb(const sm_eiso *h) { return h->precision == SM_BFP16; }
@@ -1772,9 +1783,9 @@ int launch_bslab_cfg(sm_eiso *h) {
 
 size_t eiso_bconfig_smem(int config) {
     switch (config) {
-    case 0: return ESlabB<2, 8>::bytes;
-    case 1: return ESlabB<4, 8>::bytes;
-    case 2: return ESlabB<2, 4>::bytes;
+    case 0: case 5: return ESlabB<2, 8>::bytes;
+    case 1: case 7: return ESlabB<4, 8>::bytes;
+    case 2: case 6: return ESlabB<2, 4>::bytes;
     case 3: return ESlabB<4, 4>::bytes;
     default: return ESlabB<1, 8>::bytes;
     }
@@ -1786,6 +1797,9 @@ int eiso_bready(sm_eiso *h) {
     case 1: return ready_bslab_cfg<4, 8, 4>(h);
     case 2: return ready_bslab_cfg<2, 4, 12>(h);
     case 3: return ready_bslab_cfg<4, 4, 6>(h);
+    case 5: return ready_bslab_cfg<2, 8, 12>(h);
+    case 6: return ready_bslab_cfg<2, 4, 16>(h);
+    case 7: return ready_bslab_cfg<4, 8, 6>(h);
     default: return ready_bslab_cfg<1, 8, 16>(h);
     }
 }
@@ -1796,6 +1810,9 @@ int eiso_blaunch(sm_eiso *h) {
     case 1: return launch_bslab_cfg<4, 8, 4>(h);
     case 2: return launch_bslab_cfg<2, 4, 12>(h);
     case 3: return launch_bslab_cfg<4, 4, 6>(h);
+    case 5: return launch_bslab_cfg<2, 8, 12>(h);
+    case 6: return launch_bslab_cfg<2, 4, 16>(h);
+    case 7: return launch_bslab_cfg<4, 8, 6>(h);
     default: return launch_bslab_cfg<1, 8, 16>(h);
     }
 }

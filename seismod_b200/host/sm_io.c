@@ -47,6 +47,7 @@ static int parse_precision(const char *s, int *out)
     else if (!strcmp(s, "fp64")) *out = SM_FP64;
     else if (!strcmp(s, "fp16")) *out = SM_FP16;
     else if (!strcmp(s, "bf16")) *out = SM_BF16;
+    else if (!strcmp(s, "bfp16")) *out = SM_BFP16;
     else return 0;
     return 1;
 }
