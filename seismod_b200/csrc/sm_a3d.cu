@@ -192,26 +192,33 @@ struct A3Maps {
 // read at run time; blockIdx.x numbers the ring's tiles.
 enum { A3_INNER = 0, A3_EDGE = 1 };
 
-// tile (kt, jt) of ring index e: rows below the rectangle, rows above it,
-// then the tiles left and right of it in its rows
-__device__ __forceinline__ void a3_edge_tile(const A3Args &a, int e, int &kt, int &jt) {
-    const int below = a.jt0 * a.nkt, above = (a.njt - a.jt1) * a.nkt;
-    if (e < below) {
-        jt = e / a.nkt; kt = e % a.nkt;
-    } else if (e < below + above) {
-        e -= below; jt = a.jt1 + e / a.nkt; kt = e % a.nkt;
-    } else {
-        e -= below + above;
-        const int m = a.nkt - (a.kt1 - a.kt0);
-        jt = a.jt0 + e / m;
-        const int c = e % m;
-        kt = c < a.kt0 ? c : a.kt1 + (c - a.kt0);
+// Tile (kt, jt) of ring index e, and its face: the ring is numbered by kind
+// so that CTAs running side by side mostly take the same code -- first the
+// tiles beside the interior rectangle in z (rows inside it: y is fast, face
+// A3_FACE_Z), then those beside it in y (columns inside it: z is fast, face
+// A3_FACE_Y), then the corners (both axes general, A3_FACE_GEN).
+enum { A3_FACE_GEN = 0, A3_FACE_Z = 1, A3_FACE_Y = 2 };
+__device__ __forceinline__ int a3_edge_tile(const A3Args &a, int e, int &kt, int &jt) {
+    const int nkin = a.kt1 - a.kt0, njin = a.jt1 - a.jt0;
+    const int nkout = a.nkt - nkin, njout = a.njt - njin;
+    auto kout = [&](int c) { return c < a.kt0 ? c : a.kt1 + (c - a.kt0); };
+    auto jout = [&](int c) { return c < a.jt0 ? c : a.jt1 + (c - a.jt0); };
+    if (e < nkout * njin) {
+        kt = kout(e % nkout); jt = a.jt0 + e / nkout;
+        return A3_FACE_Z;
     }
+    e -= nkout * njin;
+    if (e < nkin * njout) {
+        kt = a.kt0 + e % nkin; jt = jout(e / nkin);
+        return A3_FACE_Y;
+    }
+    e -= nkin * njout;
+    kt = kout(e % nkout); jt = jout(e / nkout);
+    return A3_FACE_GEN;
 }
 
-template <typename S, int W, int R, int D, int MINB, int CLS>
-__global__ void __launch_bounds__(32 * W, MINB)
-    a3d_step_kernel(const A3Args a, const __grid_constant__ A3Maps m) {
+template <typename S, int W, int R, int D, int CLS, int FACE>
+__device__ __forceinline__ void a3d_step_body(const A3Args &a, const A3Maps &m, int kt, int jt) {
     constexpr int TY = W * R;
     using C = typename Store<S>::C;
     using St = Store<S>;
@@ -230,13 +237,6 @@ __global__ void __launch_bounds__(32 * W, MINB)
 
     const int lane = threadIdx.x, w = threadIdx.y;
     const int tid = w * 32 + lane;
-    if (CLS == a.step_cls && (blockIdx.x | blockIdx.y | blockIdx.z | tid) == 0) ++*a.step;
-    int kt, jt;
-    if (CLS == A3_INNER) {
-        kt = a.kt0 + blockIdx.x; jt = a.jt0 + blockIdx.y;
-    } else {
-        a3_edge_tile(a, blockIdx.x, kt, jt);
-    }
     const int k0 = kt * 32, j0 = jt * TY;
     const int lo = a.np > 1 ? a.np : 1;
     const bool ytile = j0 >= lo && j0 + TY - 1 <= a.ny2 - 2 - a.np;
@@ -349,8 +349,8 @@ __global__ void __launch_bounds__(32 * W, MINB)
     // are compiled twice: with every axis fast (interior tiles on planes
     // clear of the x frame: straight-line code) and with the flags read at
     // run time.  The halo row and column always take the general update.
-    const bool yfast = CLS == A3_INNER || ytile;
-    const bool zfast = CLS == A3_INNER || ztile;
+    const bool yfast = CLS == A3_INNER || FACE == A3_FACE_Z || ytile;
+    const bool zfast = CLS == A3_INNER || FACE == A3_FACE_Y || ztile;
 
     // memory variables prefetched one plane ahead (loaded only for the
     // axes and planes that use them)
@@ -596,6 +596,24 @@ __global__ void __launch_bounds__(32 * W, MINB)
     }
 }
 
+// One launch per tile class; the ring's CTAs take the body compiled for
+// their face (one axis fast at compile time) or the general one.
+template <typename S, int W, int R, int D, int MINB, int CLS>
+__global__ void __launch_bounds__(32 * W, MINB)
+    a3d_step_kernel(const A3Args a, const __grid_constant__ A3Maps m) {
+    if (CLS == a.step_cls && (blockIdx.x | blockIdx.y | blockIdx.z | threadIdx.x | threadIdx.y) == 0)
+        ++*a.step;
+    if (CLS == A3_INNER) {
+        a3d_step_body<S, W, R, D, CLS, A3_FACE_GEN>(a, m, a.kt0 + blockIdx.x, a.jt0 + blockIdx.y);
+        return;
+    }
+    int kt, jt;
+    const int face = a3_edge_tile(a, blockIdx.x, kt, jt);
+    if (face == A3_FACE_Z) a3d_step_body<S, W, R, D, CLS, A3_FACE_Z>(a, m, kt, jt);
+    else if (face == A3_FACE_Y) a3d_step_body<S, W, R, D, CLS, A3_FACE_Y>(a, m, kt, jt);
+    else a3d_step_body<S, W, R, D, CLS, A3_FACE_GEN>(a, m, kt, jt);
+}
+
 template <typename S, int TY, int D>
 constexpr size_t a3d_step_smem() {
     return A3Lay<S, TY>::head + (size_t)D * A3Lay<S, TY>::stage;
@@ -648,9 +666,8 @@ struct A3BMaps {
     CUtensorMap P, eP, vx, eX, vy, eY, vz, eZ, rho, K;
 };
 
-template <int W, int D, int MINB, int CLS>
-__global__ void __launch_bounds__(32 * W, MINB)
-    a3d_bstep_kernel(const A3Args a, const __grid_constant__ A3BMaps m) {
+template <int W, int D, int CLS, int FACE>
+__device__ __forceinline__ void a3d_bstep_body(const A3Args &a, const A3BMaps &m, int kt, int jt) {
     constexpr int R = A3_BJ, TY = W * R;
     using C = float;
     using PSt = Store<float>;
@@ -669,13 +686,6 @@ __global__ void __launch_bounds__(32 * W, MINB)
 
     const int lane = threadIdx.x, w = threadIdx.y;
     const int tid = w * 32 + lane;
-    if (CLS == a.step_cls && (blockIdx.x | blockIdx.y | blockIdx.z | tid) == 0) ++*a.step;
-    int kt, jt;
-    if (CLS == A3_INNER) {
-        kt = a.kt0 + blockIdx.x; jt = a.jt0 + blockIdx.y;
-    } else {
-        a3_edge_tile(a, blockIdx.x, kt, jt);
-    }
     const int k0 = kt * 32, j0 = jt * TY, jb0 = jt * (TY / R);
     const int lo = a.np > 1 ? a.np : 1;
     const bool ytile = j0 >= lo && j0 + TY - 1 <= a.ny2 - 2 - a.np;
@@ -787,8 +797,8 @@ __global__ void __launch_bounds__(32 * W, MINB)
     const int hrow = w * R + lane;
     const bool hcol = lane < R && km >= 0 && j0 + hrow < ny2;
     const int kmh = (km >= 0) ? half_slab(km, nz2, np) : -1;
-    const bool yfast = CLS == A3_INNER || ytile;
-    const bool zfast = CLS == A3_INNER || ztile;
+    const bool yfast = CLS == A3_INNER || FACE == A3_FACE_Z || ytile;
+    const bool zfast = CLS == A3_INNER || FACE == A3_FACE_Y || ztile;
 
     // exponent byte of stage sb: P block b (0: rows above the tile), column
     // x = k - (k0 - 16); vx block w; vy block b (0: above); vz column x
@@ -1076,6 +1086,22 @@ __global__ void __launch_bounds__(32 * W, MINB)
         if (CLS == A3_INNER && ip >= lo && ip <= nx2 - 1 - np) pressure(ip, ip - i0, BoolT<true>{});
         else pressure(ip, ip - i0, BoolT<false>{});
     }
+}
+
+template <int W, int D, int MINB, int CLS>
+__global__ void __launch_bounds__(32 * W, MINB)
+    a3d_bstep_kernel(const A3Args a, const __grid_constant__ A3BMaps m) {
+    if (CLS == a.step_cls && (blockIdx.x | blockIdx.y | blockIdx.z | threadIdx.x | threadIdx.y) == 0)
+        ++*a.step;
+    if (CLS == A3_INNER) {
+        a3d_bstep_body<W, D, CLS, A3_FACE_GEN>(a, m, a.kt0 + blockIdx.x, a.jt0 + blockIdx.y);
+        return;
+    }
+    int kt, jt;
+    const int face = a3_edge_tile(a, blockIdx.x, kt, jt);
+    if (face == A3_FACE_Z) a3d_bstep_body<W, D, CLS, A3_FACE_Z>(a, m, kt, jt);
+    else if (face == A3_FACE_Y) a3d_bstep_body<W, D, CLS, A3_FACE_Y>(a, m, kt, jt);
+    else a3d_bstep_body<W, D, CLS, A3_FACE_GEN>(a, m, kt, jt);
 }
 
 template <int TY, int D>
@@ -2004,7 +2030,10 @@ int a3d_upload(sm_a3d *h) {
             if ((rc = h->d_table.alloc(std::max<size_t>(h->plan.table.size(), 1) * sizeof(int32_t))))
                 return rc;
             size_t nt = std::max<size_t>(h->rec.size() * h->plan.max_samples, 1);
-            if ((rc = h->d_traces.alloc(nt * sizeof(double)))) return rc;
+            // the trace buffer comes from the device cache: no step of this
+            // handle may still write the old one when it goes back
+            SM_CUDA_TRY(cudaStreamSynchronize(h->stream));
+            if ((rc = h->d_traces.alloc_pooled(nt * sizeof(double), h->device))) return rc;
             SM_CUDA_TRY(cudaMemcpyAsync(h->d_rec.p, h->rec.data(), h->rec.size() * sizeof(A3Rec),
                                         cudaMemcpyHostToDevice, h->stream));
             if (!h->plan.table.empty())

@@ -415,11 +415,29 @@ struct ESlabG {
     static constexpr unsigned tx = (unsigned)(5 * RX * BW * sizeof(S));
 };
 
+// the TMA load of slab (bx, by, shot) into a stage of ESlabG's layout,
+// completing on the stage's barrier (thread 0 only)
+template <typename S, int W, int TX>
+__device__ __forceinline__ void eiso_slabg_issue(const CUtensorMap *fmap, int bx, int by, int shot,
+                                                 unsigned char *smem) {
+    using L = ESlabG<S, W, TX>;
+    uint64_t *bar = reinterpret_cast<uint64_t *>(smem + L::oBar);
+    const int Zc = bx * W * 30;
+    const int zs = (Zc - 1 + L::HS) / L::HS * L::HS - L::HS;
+    fence_proxy_async();
+    mbar_expect_tx(bar, L::tx);
+    tma_load_4d(smem, fmap, zs, by * TX - 1, shot, 0, bar);
+}
+
 // the slab step of block (bx, by, shot) of one problem; fmap is the TMA map
-// of its old set (box (BW, TX+2, 1, 5)); smem holds ESlabG's layout
+// of its old set (box (BW, TX+2, 1, 5)); smem holds ESlabG's layout.
+// parity < 0: the slab's own launch (thread 0 initialises the barrier and
+// issues the load); parity >= 0: a persistent CTA that issued this stage's
+// load earlier and waits for that phase of its barrier
 template <typename S, int W, int TX>
 __device__ __forceinline__ void eiso_slabg_body(const EisoArgs &a, const CUtensorMap *fmap,
-                                                int bx, int by, int shot, unsigned char *smem) {
+                                                int bx, int by, int shot, unsigned char *smem,
+                                                int parity = -1) {
     using C = typename Store<S>::C;
     using St = Store<S>;
     using L = ESlabG<S, W, TX>;
@@ -432,13 +450,15 @@ __device__ __forceinline__ void eiso_slabg_body(const EisoArgs &a, const CUtenso
     const int X0 = by * TX;
     const int X1 = min(X0 + TX, a.NX);
     const int zs = (Zc - 1 + L::HS) / L::HS * L::HS - L::HS;
-    if (threadIdx.x == 0) {
-        mbar_init(bar, 1);
-        fence_proxy_async();
-        mbar_expect_tx(bar, L::tx);
-        tma_load_4d(smem, fmap, zs, X0 - 1, shot, 0, bar);
+    const unsigned ph = parity < 0 ? 0u : (unsigned)parity;
+    if (parity < 0) {
+        if (threadIdx.x == 0) {
+            mbar_init(bar, 1);
+            fence_proxy_async();
+            eiso_slabg_issue<S, W, TX>(fmap, bx, by, shot, smem);
+        }
+        __syncthreads();   // the barrier is initialised before anyone polls it
     }
-    __syncthreads();   // the barrier is initialised before anyone polls it
     const int Z0 = Zc + warp * 30;
     // warp 0 always has cells and keeps the CTA alive until the copy has
     // landed; later warps past the grid leave
@@ -479,8 +499,8 @@ __device__ __forceinline__ void eiso_slabg_body(const EisoArgs &a, const CUtenso
             cl2m[r] = M(r + 1, M_L2M);
             cmu[r] = M(r + 1, M_MU);
         }
-        if (!__all_sync(full, mbar_wait(bar, 0, a.err, 9))) {
-            mbar_wait(bar, 0, a.err, 9);
+        if (!__all_sync(full, mbar_wait(bar, ph, a.err, 9))) {
+            mbar_wait(bar, ph, a.err, 9);
             return;
         }
         C vxc, vzp;
@@ -547,8 +567,8 @@ __device__ __forceinline__ void eiso_slabg_body(const EisoArgs &a, const CUtenso
     if (zin) zp = EZProf<C>{pr[P.azn() + Z], pr[P.bzn() + Z], pr[P.azh() + Z], pr[P.bzh() + Z]};
     ESplit<C> sp;
     e_load_split<S, C>(a, sb, X0 - 1, Z, zin, sp);
-    if (!__all_sync(full, mbar_wait(bar, 0, a.err, 9))) {
-        mbar_wait(bar, 0, a.err, 9);
+    if (!__all_sync(full, mbar_wait(bar, ph, a.err, 9))) {
+        mbar_wait(bar, ph, a.err, 9);
         return;
     }
     C vxc, vzp;
@@ -631,6 +651,47 @@ __global__ void __launch_bounds__(32 * W, MINB) eiso_slabg_kernel(const EisoArgs
     eiso_slabg_body<S, W, TX>(a, &mp.f, blockIdx.x, blockIdx.y, blockIdx.z, smem);
 }
 
+// Persistent form of the slab step: a CTA per SM slot walks the slabs
+// s = blockIdx.x, + gridDim.x, ... (s -> bx fastest, then by, then shot)
+// through two shared-memory stages, the next slab's box in flight while the
+// current one computes.
+template <typename S, int W, int TX, int MINB>
+__global__ void __launch_bounds__(32 * W, MINB)
+    eiso_slabg_pkernel(const EisoArgs a, const __grid_constant__ EisoSlabMaps mp, int gx, int gy,
+                       int nslab) {
+    using L = ESlabG<S, W, TX>;
+    extern __shared__ __align__(128) unsigned char smem[];
+    unsigned char *stage[2] = {smem, smem + L::al(L::bytes)};
+    if (threadIdx.x == 0) {
+        mbar_init(reinterpret_cast<uint64_t *>(stage[0] + L::oBar), 1);
+        mbar_init(reinterpret_cast<uint64_t *>(stage[1] + L::oBar), 1);
+        fence_proxy_async();
+    }
+    __syncthreads();
+    auto coords = [&](int s, int &bx, int &by, int &shot) {
+        bx = s % gx;
+        const int r = s / gx;
+        by = r % gy;
+        shot = r / gy;
+    };
+    int bx, by, shot;
+    if (threadIdx.x == 0 && (int)blockIdx.x < nslab) {
+        coords(blockIdx.x, bx, by, shot);
+        eiso_slabg_issue<S, W, TX>(&mp.f, bx, by, shot, stage[0]);
+    }
+    int k = 0;
+    for (int s = blockIdx.x; s < nslab; s += gridDim.x, ++k) {
+        const int sn = s + gridDim.x;
+        if (threadIdx.x == 0 && sn < nslab) {   // its stage was released at the last sync
+            coords(sn, bx, by, shot);
+            eiso_slabg_issue<S, W, TX>(&mp.f, bx, by, shot, stage[(k + 1) & 1]);
+        }
+        coords(s, bx, by, shot);
+        eiso_slabg_body<S, W, TX>(a, &mp.f, bx, by, shot, stage[k & 1], (k >> 1) & 1);
+        __syncthreads();
+    }
+}
+
 // ---------------------------------------------------------------------------
 // Block-floating-point slab step (SM_BFP16).  The slab step above with the
 // five wavefields stored as 16-bit mantissas sharing one exponent byte per
@@ -685,10 +746,29 @@ struct ESlabB {
     static constexpr unsigned tx = (unsigned)(5 * RX * BW * 2 + 5 * NB * BWE);
 };
 
+// the two TMA loads of slab (bx, by, shot) into a stage of ESlabB's layout,
+// completing on the stage's barrier (thread 0 only)
+template <int W, int TX>
+__device__ __forceinline__ void eiso_bslab_issue(const CUtensorMap *fmap, const CUtensorMap *emap,
+                                                 int bx, int by, int shot, unsigned char *smem) {
+    using L = ESlabB<W, TX>;
+    uint64_t *bar = reinterpret_cast<uint64_t *>(smem + L::oBar);
+    const int Zc = bx * W * 30, X0 = by * TX;
+    const int zs = (Zc - 1 + L::HS) / L::HS * L::HS - L::HS;
+    const int zse = (Zc - 1 + 16) / 16 * 16 - 16;
+    fence_proxy_async();
+    mbar_expect_tx(bar, L::tx);
+    tma_load_4d(smem, fmap, zs, X0 - 1, shot, 0, bar);
+    tma_load_4d(smem + L::oE, emap, zse, X0 / EISO_EB - 1, shot, 0, bar);
+}
+
+// One slab.  parity < 0: the slab's own launch (thread 0 initialises the
+// barrier and issues the loads); parity >= 0: a persistent CTA that issued
+// this stage's loads earlier and waits for that phase of its barrier.
 template <int W, int TX>
 __device__ __forceinline__ void eiso_bslab_body(const EisoArgs &a, const CUtensorMap *fmap,
                                                 const CUtensorMap *emap, int bx, int by, int shot,
-                                                unsigned char *smem) {
+                                                unsigned char *smem, int parity = -1) {
     using C = float;
     using L = ESlabB<W, TX>;
     constexpr int EB = EISO_EB;
@@ -704,14 +784,15 @@ __device__ __forceinline__ void eiso_bslab_body(const EisoArgs &a, const CUtenso
     const int zs = (Zc - 1 + L::HS) / L::HS * L::HS - L::HS;
     const int zse = (Zc - 1 + 16) / 16 * 16 - 16;
     const int xb0 = X0 / EB;
-    if (threadIdx.x == 0) {
-        mbar_init(bar, 1);
-        fence_proxy_async();
-        mbar_expect_tx(bar, L::tx);
-        tma_load_4d(smem, fmap, zs, X0 - 1, shot, 0, bar);
-        tma_load_4d(smem + L::oE, emap, zse, xb0 - 1, shot, 0, bar);
+    const unsigned ph = parity < 0 ? 0u : (unsigned)parity;
+    if (parity < 0) {
+        if (threadIdx.x == 0) {
+            mbar_init(bar, 1);
+            fence_proxy_async();
+            eiso_bslab_issue<W, TX>(fmap, emap, bx, by, shot, smem);
+        }
+        __syncthreads();
     }
-    __syncthreads();
     const int Z0 = Zc + warp * 30;
     if (Z0 >= a.NZ) return;
     const int Z = Z0 - 1 + lane;
@@ -792,8 +873,8 @@ __device__ __forceinline__ void eiso_bslab_body(const EisoArgs &a, const CUtenso
             cl2m[r] = __ldg(mL2M + (long long)(r + 1) * a.pitch);
             cmu[r] = __ldg(mMU + (long long)(r + 1) * a.pitch);
         }
-        if (!__all_sync(full, mbar_wait(bar, 0, a.err, 9))) {
-            mbar_wait(bar, 0, a.err, 9);
+        if (!__all_sync(full, mbar_wait(bar, ph, a.err, 9))) {
+            mbar_wait(bar, ph, a.err, 9);
             return;
         }
         // each value decoded once; a field's decoder is taken when the march
@@ -913,8 +994,8 @@ __device__ __forceinline__ void eiso_bslab_body(const EisoArgs &a, const CUtenso
     if (zin) zp = EZProf<C>{pr[P.azn() + Z], pr[P.bzn() + Z], pr[P.azh() + Z], pr[P.bzh() + Z]};
     ESplit<C> sp;
     e_load_split<float, C>(a, sb, X0 - 1, Z, zin, sp);
-    if (!__all_sync(full, mbar_wait(bar, 0, a.err, 9))) {
-        mbar_wait(bar, 0, a.err, 9);
+    if (!__all_sync(full, mbar_wait(bar, ph, a.err, 9))) {
+        mbar_wait(bar, ph, a.err, 9);
         return;
     }
     C vxc, vzp;
@@ -1004,6 +1085,47 @@ __global__ void __launch_bounds__(32 * W, MINB) eiso_bslab_kernel(const EisoArgs
                                                                   const __grid_constant__ EisoBMaps mp) {
     extern __shared__ __align__(128) unsigned char smem[];
     eiso_bslab_body<W, TX>(a, &mp.f, &mp.e, blockIdx.x, blockIdx.y, blockIdx.z, smem);
+}
+
+// Persistent form: a CTA per SM slot walks the slabs s = blockIdx.x,
+// + gridDim.x, ... (s -> bx fastest, then by, then shot) through two shared-
+// memory stages: the next slab's boxes are in flight while the current slab
+// computes, so the load latency no longer stands between slabs.
+template <int W, int TX, int MINB>
+__global__ void __launch_bounds__(32 * W, MINB)
+    eiso_bslab_pkernel(const EisoArgs a, const __grid_constant__ EisoBMaps mp, int gx, int gy,
+                       int nslab) {
+    using L = ESlabB<W, TX>;
+    extern __shared__ __align__(128) unsigned char smem[];
+    unsigned char *stage[2] = {smem, smem + L::al(L::bytes)};
+    if (threadIdx.x == 0) {
+        mbar_init(reinterpret_cast<uint64_t *>(stage[0] + L::oBar), 1);
+        mbar_init(reinterpret_cast<uint64_t *>(stage[1] + L::oBar), 1);
+        fence_proxy_async();
+    }
+    __syncthreads();
+    auto coords = [&](int s, int &bx, int &by, int &shot) {
+        bx = s % gx;
+        const int r = s / gx;
+        by = r % gy;
+        shot = r / gy;
+    };
+    int bx, by, shot;
+    if (threadIdx.x == 0 && (int)blockIdx.x < nslab) {
+        coords(blockIdx.x, bx, by, shot);
+        eiso_bslab_issue<W, TX>(&mp.f, &mp.e, bx, by, shot, stage[0]);
+    }
+    int k = 0;
+    for (int s = blockIdx.x; s < nslab; s += gridDim.x, ++k) {
+        const int sn = s + gridDim.x;
+        if (threadIdx.x == 0 && sn < nslab) {   // its stage was released at the last sync
+            coords(sn, bx, by, shot);
+            eiso_bslab_issue<W, TX>(&mp.f, &mp.e, bx, by, shot, stage[(k + 1) & 1]);
+        }
+        coords(s, bx, by, shot);
+        eiso_bslab_body<W, TX>(a, &mp.f, &mp.e, bx, by, shot, stage[k & 1], (k >> 1) & 1);
+        __syncthreads();
+    }
 }
 
 // ---------------------------------------------------------------------------
@@ -1617,6 +1739,7 @@ void eiso_bind(sm_eiso *h) {
 //   slab, materials from global (kind 0): p = {warps per CTA, rows TX, min CTAs per SM}
 //   tile (kind 1): p = {TX, TZ, threads, min CTAs per SM}
 //   slab, materials by TMA (kind 2): p = {warps per CTA, rows TX, min CTAs per SM}
+//   persistent slab, materials from global (kind 3): p = {warps per CTA, rows TX, min CTAs per SM}
 // The minimum resident CTAs per SM caps the registers a thread may use.
 struct EisoConfig {
     int kind;
@@ -1625,15 +1748,18 @@ struct EisoConfig {
 static const EisoConfig kEisoConfigs[] = {
     {0, {2, 8, 8, 0}},  {0, {2, 4, 12, 0}},   {0, {4, 4, 6, 0}},    {0, {1, 8, 16, 0}},
     {0, {4, 8, 4, 0}},  {0, {2, 16, 4, 0}},   {1, {8, 32, 128, 6}}, {1, {16, 64, 256, 2}},
-    {1, {8, 64, 256, 3}}, {2, {2, 8, 8, 0}},  {2, {4, 8, 4, 0}},    {2, {1, 16, 12, 0}}};
+    {1, {8, 64, 256, 3}}, {2, {2, 8, 8, 0}},  {2, {4, 8, 4, 0}},    {2, {1, 16, 12, 0}},
+    {3, {2, 8, 8, 0}},  {3, {2, 8, 12, 0}},   {3, {4, 8, 6, 0}},    {3, {2, 4, 12, 0}}};
 static const int kEisoNumConfigs = sizeof(kEisoConfigs) / sizeof(kEisoConfigs[0]);
 // block storage: the slab step only, {warps per CTA, rows TX (whole blocks),
 // min CTAs per SM}
 struct EisoBConfig {
-    int w, tx, minb;
+    int w, tx, minb, persistent;
 };
-static const EisoBConfig kEisoBConfigs[] = {{2, 8, 8}, {4, 8, 4}, {2, 4, 12}, {4, 4, 6}, {1, 8, 16},
-                                            {2, 8, 12}, {2, 4, 16}, {4, 8, 6}};
+static const EisoBConfig kEisoBConfigs[] = {
+    {2, 8, 8, 0},  {4, 8, 4, 0},   {2, 4, 12, 0}, {4, 4, 6, 0}, {1, 8, 16, 0},
+    {2, 8, 12, 0}, {2, 4, 16, 0},  {4, 8, 6, 0},
+    {2, 8, 8, 1},  {2, 8, 12, 1},  {4, 8, 6, 1},  {2, 4, 16, 1}};
 static const int kEisoBNumConfigs = sizeof(kEisoBConfigs) / sizeof(kEisoBConfigs[0]);
 
 bool eiso_isb(const sm_eiso *h) { return h->precision == SM_BFP16; }
@@ -1766,6 +1892,36 @@ int launch_slabg_cfg(sm_eiso *h) {
     return SM_OK;
 }
 
+template <typename S, int W, int TX>
+constexpr size_t slabg_p_smem() {
+    return 2 * ESlabG<S, W, TX>::al(ESlabG<S, W, TX>::bytes);
+}
+
+template <typename S, int W, int TX, int MINB>
+int ready_slabg_p_cfg(sm_eiso *h) {
+    if (int rc = eiso_make_slab_maps<S, ESlabG<S, W, TX>, (1 << 20) + W * 4096 + TX>(h)) return rc;
+    return allow_smem(eiso_slabg_pkernel<S, W, TX, MINB>, slabg_p_smem<S, W, TX>(), h->device);
+}
+
+// as many CTAs as fit on the device at once, each walking its share of slabs
+template <typename S, int W, int TX, int MINB>
+int launch_slabg_p_cfg(sm_eiso *h) {
+    const int gx = ((h->NZ + 29) / 30 + W - 1) / W, gy = (h->NX + TX - 1) / TX;
+    const int nslab = gx * gy * (int)h->nshots;
+    static int occ[64] = {};
+    if (h->device >= 0 && h->device < 64 && occ[h->device] == 0) {
+        int n = 0;
+        SM_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+            &n, eiso_slabg_pkernel<S, W, TX, MINB>, 32 * W, slabg_p_smem<S, W, TX>()));
+        occ[h->device] = n > 0 ? n : 1;
+    }
+    const int per = (h->device >= 0 && h->device < 64) ? occ[h->device] : 1;
+    const int grid = std::min(nslab, h->sms * per);
+    eiso_slabg_pkernel<S, W, TX, MINB><<<grid, 32 * W, slabg_p_smem<S, W, TX>(), h->stream>>>(
+        h->args, h->slab_maps[h->cur], gx, gy, nslab);
+    return SM_OK;
+}
+
 template <int W, int TX, int MINB>
 int ready_bslab_cfg(sm_eiso *h) {
     if (int rc = eiso_make_bmaps<W, TX>(h)) return rc;
@@ -1781,12 +1937,45 @@ int launch_bslab_cfg(sm_eiso *h) {
     return SM_OK;
 }
 
+template <int W, int TX>
+constexpr size_t bslab_p_smem() {
+    return 2 * ESlabB<W, TX>::al(ESlabB<W, TX>::bytes);
+}
+
+template <int W, int TX, int MINB>
+int ready_bslab_p_cfg(sm_eiso *h) {
+    if (int rc = eiso_make_bmaps<W, TX>(h)) return rc;
+    return allow_smem(eiso_bslab_pkernel<W, TX, MINB>, bslab_p_smem<W, TX>(), h->device);
+}
+
+// as many CTAs as fit on the device at once (each walks its share of slabs)
+template <int W, int TX, int MINB>
+int launch_bslab_p_cfg(sm_eiso *h) {
+    const int gx = ((h->NZ + 29) / 30 + W - 1) / W, gy = (h->NX + TX - 1) / TX;
+    const int nslab = gx * gy * (int)h->nshots;
+    static int occ[64] = {};
+    if (h->device >= 0 && h->device < 64 && occ[h->device] == 0) {
+        int n = 0;
+        SM_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+            &n, eiso_bslab_pkernel<W, TX, MINB>, 32 * W, bslab_p_smem<W, TX>()));
+        occ[h->device] = n > 0 ? n : 1;
+    }
+    const int per = (h->device >= 0 && h->device < 64) ? occ[h->device] : 1;
+    const int grid = std::min(nslab, h->sms * per);
+    eiso_bslab_pkernel<W, TX, MINB><<<grid, 32 * W, bslab_p_smem<W, TX>(), h->stream>>>(
+        h->args, h->bmaps[h->cur], gx, gy, nslab);
+    return SM_OK;
+}
+
 size_t eiso_bconfig_smem(int config) {
     switch (config) {
     case 0: case 5: return ESlabB<2, 8>::bytes;
     case 1: case 7: return ESlabB<4, 8>::bytes;
     case 2: case 6: return ESlabB<2, 4>::bytes;
     case 3: return ESlabB<4, 4>::bytes;
+    case 8: case 9: return bslab_p_smem<2, 8>();
+    case 10: return bslab_p_smem<4, 8>();
+    case 11: return bslab_p_smem<2, 4>();
     default: return ESlabB<1, 8>::bytes;
     }
 }
@@ -1800,6 +1989,10 @@ int eiso_bready(sm_eiso *h) {
     case 5: return ready_bslab_cfg<2, 8, 12>(h);
     case 6: return ready_bslab_cfg<2, 4, 16>(h);
     case 7: return ready_bslab_cfg<4, 8, 6>(h);
+    case 8: return ready_bslab_p_cfg<2, 8, 8>(h);
+    case 9: return ready_bslab_p_cfg<2, 8, 12>(h);
+    case 10: return ready_bslab_p_cfg<4, 8, 6>(h);
+    case 11: return ready_bslab_p_cfg<2, 4, 16>(h);
     default: return ready_bslab_cfg<1, 8, 16>(h);
     }
 }
@@ -1813,6 +2006,10 @@ int eiso_blaunch(sm_eiso *h) {
     case 5: return launch_bslab_cfg<2, 8, 12>(h);
     case 6: return launch_bslab_cfg<2, 4, 16>(h);
     case 7: return launch_bslab_cfg<4, 8, 6>(h);
+    case 8: return launch_bslab_p_cfg<2, 8, 8>(h);
+    case 9: return launch_bslab_p_cfg<2, 8, 12>(h);
+    case 10: return launch_bslab_p_cfg<4, 8, 6>(h);
+    case 11: return launch_bslab_p_cfg<2, 4, 16>(h);
     default: return launch_bslab_cfg<1, 8, 16>(h);
     }
 }
@@ -1831,6 +2028,9 @@ size_t eiso_config_smem(int config) {
     case 8: return ETile<S, 8, 64>::bytes;
     case 9: return ESlab<S, 2, 8>::bytes;
     case 10: return ESlab<S, 4, 8>::bytes;
+    case 12: case 13: return slabg_p_smem<S, 2, 8>();
+    case 14: return slabg_p_smem<S, 4, 8>();
+    case 15: return slabg_p_smem<S, 2, 4>();
     default: return ESlab<S, 1, 16>::bytes;
     }
 }
@@ -1862,6 +2062,10 @@ int eiso_ready(sm_eiso *h) {
     case 8: return ready_tile_cfg<S, 8, 64, 256, 3>(h);
     case 9: return ready_slab_cfg<S, 2, 8, 8>(h);
     case 10: return ready_slab_cfg<S, 4, 8, 4>(h);
+    case 12: return ready_slabg_p_cfg<S, 2, 8, 8>(h);
+    case 13: return ready_slabg_p_cfg<S, 2, 8, 12>(h);
+    case 14: return ready_slabg_p_cfg<S, 4, 8, 6>(h);
+    case 15: return ready_slabg_p_cfg<S, 2, 4, 12>(h);
     default: return ready_slab_cfg<S, 1, 16, 12>(h);
     }
 }
@@ -1883,6 +2087,10 @@ int launch_step(sm_eiso *h) {
     case 8: rc = launch_tile_cfg<S, 8, 64, 256, 3>(h); break;
     case 9: rc = launch_slab_cfg<S, 2, 8, 8>(h); break;
     case 10: rc = launch_slab_cfg<S, 4, 8, 4>(h); break;
+    case 12: rc = launch_slabg_p_cfg<S, 2, 8, 8>(h); break;
+    case 13: rc = launch_slabg_p_cfg<S, 2, 8, 12>(h); break;
+    case 14: rc = launch_slabg_p_cfg<S, 4, 8, 6>(h); break;
+    case 15: rc = launch_slabg_p_cfg<S, 2, 4, 12>(h); break;
     default: rc = launch_slab_cfg<S, 1, 16, 12>(h); break;
     }
     if (rc) return rc;
@@ -2106,7 +2314,11 @@ int upload_receivers(sm_eiso *h) {
     int rc;
     if ((rc = h->d_rec.alloc(all.size() * sizeof(RecEntry)))) return rc;
     if ((rc = h->d_table.alloc(std::max<size_t>(table.size(), 1) * sizeof(int32_t)))) return rc;
-    if ((rc = h->d_traces.alloc(std::max<long long>(out, 1) * sizeof(double)))) return rc;
+    // the trace buffer comes from the device cache: no step of this handle
+    // may still write the old one when it goes back
+    SM_CUDA_TRY(cudaStreamSynchronize(h->stream));
+    if ((rc = h->d_traces.alloc_pooled(std::max<long long>(out, 1) * sizeof(double), h->device)))
+        return rc;
     SM_CUDA_TRY(cudaMemcpyAsync(h->d_rec.p, all.data(), all.size() * sizeof(RecEntry),
                                 cudaMemcpyHostToDevice, h->stream));
     if (!table.empty())
