@@ -198,6 +198,14 @@ enum { A3_INNER = 0, A3_EDGE = 1 };
 // A3_FACE_Z), then those beside it in y (columns inside it: z is fast, face
 // A3_FACE_Y), then the corners (both axes general, A3_FACE_GEN).
 enum { A3_FACE_GEN = 0, A3_FACE_Z = 1, A3_FACE_Y = 2 };
+// Whether the ring launch carries a body per face.  Measured on B200 at
+// 288^3: no gain over the one general body (0.268 against 0.266 ms per FP32
+// step; 0.327 against 0.326 in block storage), and three bodies triple the
+// ring kernel's code (instruction-fetch stalls in the capture), so the ring
+// takes the general body; the faces stay numbered for it.
+#ifndef SM_A3D_FACE_BODIES
+#define SM_A3D_FACE_BODIES 0
+#endif
 __device__ __forceinline__ int a3_edge_tile(const A3Args &a, int e, int &kt, int &jt) {
     const int nkin = a.kt1 - a.kt0, njin = a.jt1 - a.jt0;
     const int nkout = a.nkt - nkin, njout = a.njt - njin;
@@ -609,9 +617,13 @@ __global__ void __launch_bounds__(32 * W, MINB)
     }
     int kt, jt;
     const int face = a3_edge_tile(a, blockIdx.x, kt, jt);
+#if SM_A3D_FACE_BODIES
     if (face == A3_FACE_Z) a3d_step_body<S, W, R, D, CLS, A3_FACE_Z>(a, m, kt, jt);
     else if (face == A3_FACE_Y) a3d_step_body<S, W, R, D, CLS, A3_FACE_Y>(a, m, kt, jt);
-    else a3d_step_body<S, W, R, D, CLS, A3_FACE_GEN>(a, m, kt, jt);
+    else
+#endif
+    a3d_step_body<S, W, R, D, CLS, A3_FACE_GEN>(a, m, kt, jt);
+    (void)face;
 }
 
 template <typename S, int TY, int D>
@@ -1099,9 +1111,13 @@ __global__ void __launch_bounds__(32 * W, MINB)
     }
     int kt, jt;
     const int face = a3_edge_tile(a, blockIdx.x, kt, jt);
+#if SM_A3D_FACE_BODIES
     if (face == A3_FACE_Z) a3d_bstep_body<W, D, CLS, A3_FACE_Z>(a, m, kt, jt);
     else if (face == A3_FACE_Y) a3d_bstep_body<W, D, CLS, A3_FACE_Y>(a, m, kt, jt);
-    else a3d_bstep_body<W, D, CLS, A3_FACE_GEN>(a, m, kt, jt);
+    else
+#endif
+    a3d_bstep_body<W, D, CLS, A3_FACE_GEN>(a, m, kt, jt);
+    (void)face;
 }
 
 template <int TY, int D>

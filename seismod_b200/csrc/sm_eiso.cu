@@ -2558,6 +2558,7 @@ extern "C" int sm_eiso_create(int device, size_t nx, size_t nz, size_t npml, dou
     // block storage keeps the split parts in FP32
     const size_t pelem = precision == SM_BFP16 ? 4 : h->elem;
     if (precision == SM_BFP16) {
+        h->config = 5;   // block-storage slab 2 x 8, 12 CTAs per SM: the fastest measured
         h->nxb = (NX + EISO_EB - 1) / EISO_EB;
         h->args.nxb = (int)h->nxb;
         h->args.estride = (long long)(nshots * h->nxb * (size_t)h->pitch);
