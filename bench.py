@@ -489,8 +489,8 @@ def run_serve(args, local_rank):
         "data": "synthetic (seeded request stream of the named configuration)",
         "config": {"workload": desc, "precision": f"{args.precision} storage",
                    "server": "max_active 16, slices of 64 steps, CUDA graphs of %d steps%s"
-                             % (GRAPH or 0, ", e_iso requests stepped as one group"
-                                if args.group else "")},
+                             % (GRAPH or 0, ", e_iso and a_iso_3d requests each stepped as "
+                                "one group" if args.group else "")},
         "serving": {"shots_per_s": round(st["shots_per_s"], 4),
                     "latency_p50_s": round(st["latency_p50"], 4),
                     "latency_p99_s": round(st["latency_p99"], 4),
@@ -661,8 +661,8 @@ def main():
                     help="skip the batched / 512^3 / 400^2 comparison of the default run")
     ap.add_argument("--no-tune", action="store_true", help="default launch configuration")
     ap.add_argument("--group", action="store_true",
-                    help="serve workloads: running e_iso requests take their slices together "
-                         "(one launch per step over all their grids)")
+                    help="serve workloads: running requests of one program take their slices "
+                         "together (one launch per step over all their grids)")
     ap.add_argument("--no-graph", action="store_true", help="launch every kernel from the host")
     ap.add_argument("--size", type=int, default=None,
                     help="a3d only: interior edge length instead of 256 (profiling captures)")

@@ -269,6 +269,16 @@ int sm_a3d_set_sources(sm_a3d_t h, size_t nsrc, const size_t *index, const doubl
 int sm_a3d_set_receivers(sm_a3d_t h, size_t nrec, const size_t *index, const int *comp,
                          const double *t0, const double *rdt, size_t nsteps_max);
 int sm_a3d_run(sm_a3d_t h, size_t nsteps);
+/* Advance n handles of possibly different grid sizes and sources together
+ * by nsteps steps each (the same loop, a_iso_3d.c:593-741, for several
+ * models at once): each step is one launch over the tiles of all of them
+ * (up to 16 handles per launch), one for all their sources and one for all
+ * their receivers.  Every handle ends bit for bit where
+ * sm_a3d_run(handles[k], nsteps) would leave it.  Same device and precision
+ * for all; the work is queued on handles[0]'s stream after the work already
+ * queued on every handle's stream, and every handle's stream waits for it.
+ * Asynchronous like sm_a3d_run. */
+int sm_a3d_group_run(sm_a3d_t const *handles, int n, size_t nsteps);
 int sm_a3d_sync(sm_a3d_t h);
 int sm_a3d_step_count(sm_a3d_t h, size_t *it);
 int sm_a3d_read_traces(sm_a3d_t h, size_t rec0, size_t nrec, double *out, size_t ld,
@@ -453,10 +463,10 @@ typedef struct sm_server *sm_server_t;
  * (0 none; else as sm_eiso_set_graph). */
 int sm_server_create(int device, size_t hbm_budget, int max_active, int slice_steps,
                      int graph_steps, sm_server_t *out);
-/* on != 0: running e_iso requests of one precision take their slices
- * together, one sm_eiso_group_run call (one launch per step over all of
- * their grids) instead of one sm_eiso_run each; results are the same bits.
- * Call before the first submission. */
+/* on != 0: running requests of one program and precision take their
+ * slices together, one sm_eiso_group_run or sm_a3d_group_run call (one
+ * launch per step over all of their grids) instead of one run each; results
+ * are the same bits.  Call before the first submission. */
 int sm_server_set_group(sm_server_t s, int on);
 /* SM_EBUSY when the request alone exceeds the budget */
 int sm_server_submit_eiso(sm_server_t s, const sm_eiso_request *r, uint64_t *ticket);

@@ -80,6 +80,7 @@ _SIGS = {
     "sm_eiso_set_receivers": (C.c_int, [_vp, _sz, _sz, _szp, _ip, _dp, _dp, _sz]),
     "sm_eiso_run": (C.c_int, [_vp, _sz]),
     "sm_eiso_group_run": (C.c_int, [C.POINTER(_vp), C.c_int, _sz]),
+    "sm_a3d_group_run": (C.c_int, [C.POINTER(_vp), C.c_int, _sz]),
     "sm_eiso_sync": (C.c_int, [_vp]),
     "sm_eiso_step_count": (C.c_int, [_vp, _szp]),
     "sm_eiso_read_traces": (C.c_int, [_vp, _sz, _sz, _sz, _dp, _sz, _szp]),

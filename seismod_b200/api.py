@@ -400,6 +400,13 @@ def group_run(devs, n):
     L.check(L.load().sm_eiso_group_run(arr, len(devs), n))
 
 
+def a3d_group_run(devs, n):
+    """Advance several A3dDevice objects (any grid sizes, same precision) by
+    n steps together: one launch per step for all of them."""
+    arr = (C.c_void_p * len(devs))(*[d._h.value for d in devs])
+    L.check(L.load().sm_a3d_group_run(arr, len(devs), n))
+
+
 def a3d_index(p, x, y, z):
     nx2, ny2, nz2 = (n + 2 * p.npml for n in p.shape)
     i = c_round((x - p.origin[0]) / p.d[0]) + p.npml

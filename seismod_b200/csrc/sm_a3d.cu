@@ -16,6 +16,7 @@
 // Materials.  rho (for the staggered buoyancy dt*2/(rho_a + rho_b),
 // a_iso_3d.c:379-405, formed on the fly) and K = rho vp^2 dt (:407-409).
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstring>
 #include <map>
@@ -226,7 +227,8 @@ __device__ __forceinline__ int a3_edge_tile(const A3Args &a, int e, int &kt, int
 }
 
 template <typename S, int W, int R, int D, int CLS, int FACE>
-__device__ __forceinline__ void a3d_step_body(const A3Args &a, const A3Maps &m, int kt, int jt) {
+__device__ __forceinline__ void a3d_step_body(const A3Args &a, const A3Maps &m, int kt, int jt,
+                                              int ch) {
     constexpr int TY = W * R;
     using C = typename Store<S>::C;
     using St = Store<S>;
@@ -256,7 +258,7 @@ __device__ __forceinline__ void a3d_step_body(const A3Args &a, const A3Maps &m, 
         return;
     }
     const int k = k0 + lane;
-    const int i0 = blockIdx.z * a.chunk;
+    const int i0 = ch * a.chunk;
     const int i1 = min(i0 + a.chunk, a.nx2);
     const int nx2 = a.nx2, ny2 = a.ny2, nz2 = a.nz2, np = a.np, pitch = a.pitch;
     const int sx = a.sx, sy = a.sy;   // element strides (all indices fit 31 bits)
@@ -612,17 +614,18 @@ __global__ void __launch_bounds__(32 * W, MINB)
     if (CLS == a.step_cls && (blockIdx.x | blockIdx.y | blockIdx.z | threadIdx.x | threadIdx.y) == 0)
         ++*a.step;
     if (CLS == A3_INNER) {
-        a3d_step_body<S, W, R, D, CLS, A3_FACE_GEN>(a, m, a.kt0 + blockIdx.x, a.jt0 + blockIdx.y);
+        a3d_step_body<S, W, R, D, CLS, A3_FACE_GEN>(a, m, a.kt0 + blockIdx.x, a.jt0 + blockIdx.y,
+                                                    blockIdx.z);
         return;
     }
     int kt, jt;
     const int face = a3_edge_tile(a, blockIdx.x, kt, jt);
 #if SM_A3D_FACE_BODIES
-    if (face == A3_FACE_Z) a3d_step_body<S, W, R, D, CLS, A3_FACE_Z>(a, m, kt, jt);
-    else if (face == A3_FACE_Y) a3d_step_body<S, W, R, D, CLS, A3_FACE_Y>(a, m, kt, jt);
+    if (face == A3_FACE_Z) a3d_step_body<S, W, R, D, CLS, A3_FACE_Z>(a, m, kt, jt, blockIdx.z);
+    else if (face == A3_FACE_Y) a3d_step_body<S, W, R, D, CLS, A3_FACE_Y>(a, m, kt, jt, blockIdx.z);
     else
 #endif
-    a3d_step_body<S, W, R, D, CLS, A3_FACE_GEN>(a, m, kt, jt);
+    a3d_step_body<S, W, R, D, CLS, A3_FACE_GEN>(a, m, kt, jt, blockIdx.z);
     (void)face;
 }
 
@@ -679,7 +682,8 @@ struct A3BMaps {
 };
 
 template <int W, int D, int CLS, int FACE>
-__device__ __forceinline__ void a3d_bstep_body(const A3Args &a, const A3BMaps &m, int kt, int jt) {
+__device__ __forceinline__ void a3d_bstep_body(const A3Args &a, const A3BMaps &m, int kt, int jt,
+                                               int ch) {
     constexpr int R = A3_BJ, TY = W * R;
     using C = float;
     using PSt = Store<float>;
@@ -707,7 +711,7 @@ __device__ __forceinline__ void a3d_bstep_body(const A3Args &a, const A3BMaps &m
         return;
     }
     const int k = k0 + lane;
-    const int i0 = blockIdx.z * a.chunk;
+    const int i0 = ch * a.chunk;
     const int i1 = min(i0 + a.chunk, a.nx2);
     const int nx2 = a.nx2, ny2 = a.ny2, nz2 = a.nz2, np = a.np, pitch = a.pitch;
     const int sx = a.sx, sy = a.sy;
@@ -1106,17 +1110,17 @@ __global__ void __launch_bounds__(32 * W, MINB)
     if (CLS == a.step_cls && (blockIdx.x | blockIdx.y | blockIdx.z | threadIdx.x | threadIdx.y) == 0)
         ++*a.step;
     if (CLS == A3_INNER) {
-        a3d_bstep_body<W, D, CLS, A3_FACE_GEN>(a, m, a.kt0 + blockIdx.x, a.jt0 + blockIdx.y);
+        a3d_bstep_body<W, D, CLS, A3_FACE_GEN>(a, m, a.kt0 + blockIdx.x, a.jt0 + blockIdx.y, blockIdx.z);
         return;
     }
     int kt, jt;
     const int face = a3_edge_tile(a, blockIdx.x, kt, jt);
 #if SM_A3D_FACE_BODIES
-    if (face == A3_FACE_Z) a3d_bstep_body<W, D, CLS, A3_FACE_Z>(a, m, kt, jt);
-    else if (face == A3_FACE_Y) a3d_bstep_body<W, D, CLS, A3_FACE_Y>(a, m, kt, jt);
+    if (face == A3_FACE_Z) a3d_bstep_body<W, D, CLS, A3_FACE_Z>(a, m, kt, jt, blockIdx.z);
+    else if (face == A3_FACE_Y) a3d_bstep_body<W, D, CLS, A3_FACE_Y>(a, m, kt, jt, blockIdx.z);
     else
 #endif
-    a3d_bstep_body<W, D, CLS, A3_FACE_GEN>(a, m, kt, jt);
+    a3d_bstep_body<W, D, CLS, A3_FACE_GEN>(a, m, kt, jt, blockIdx.z);
     (void)face;
 }
 
@@ -1136,19 +1140,25 @@ struct A3Src {
     int nb, rs;
 };
 
+// the sources of one problem at the step just taken: one thread, in source
+// order, as a_iso_3d.c:689-693
 template <typename S>
-__global__ void a3d_source_kernel(A3Args a, const A3Src *src, int nsrc, const double *vals) {
+__device__ void a3d_inject(const A3Args &a, const A3Src *src, int nsrc, const double *vals) {
     using St = Store<S>;
     using C = typename Store<S>::C;
-    if (blockIdx.x != 0 || threadIdx.x != 0) return;
     const long long it = *a.step - 1;
-    // one thread, in source order, as a_iso_3d.c:689-693
     S *P = static_cast<S *>(a.f[A_P]);
     for (int e = 0; e < nsrc; ++e) {
         const A3Src s = src[e];
         if (it >= s.len) continue;
         St::st(P + s.q, St::ld(P + s.q, a.isc[A_P]) + static_cast<C>(vals[s.voff + it]), a.sc[A_P]);
     }
+}
+
+template <typename S>
+__global__ void a3d_source_kernel(A3Args a, const A3Src *src, int nsrc, const double *vals) {
+    if (blockIdx.x != 0 || threadIdx.x != 0) return;
+    a3d_inject<S>(a, src, nsrc, vals);
 }
 
 struct A3Rec {
@@ -1162,8 +1172,7 @@ struct A3Rec {
 // block storage: one thread adds the sources in order; each addition
 // decodes the source cell's block, adds, and stores the block again with
 // the exponent its new maximum takes (a_iso_3d.c:689-693)
-__global__ void a3d_bsource_kernel(A3Args a, const A3Src *src, int nsrc, const double *vals) {
-    if (blockIdx.x != 0 || threadIdx.x != 0) return;
+__device__ void a3d_binject(const A3Args &a, const A3Src *src, int nsrc, const double *vals) {
     const long long it = *a.step - 1;
     int16_t *P = static_cast<int16_t *>(a.f[A_P]);
     uint8_t *E = static_cast<uint8_t *>(a.fe[A_P]);
@@ -1187,31 +1196,159 @@ __global__ void a3d_bsource_kernel(A3Args a, const A3Src *src, int nsrc, const d
     }
 }
 
-__global__ void a3d_bgather_kernel(A3Args a, const A3Rec *rec, int nrec, const int32_t *table,
-                                   long long nsteps_max, double *traces) {
-    const int r = blockIdx.x * blockDim.x + threadIdx.x;
+__global__ void a3d_bsource_kernel(A3Args a, const A3Src *src, int nsrc, const double *vals) {
+    if (blockIdx.x != 0 || threadIdx.x != 0) return;
+    a3d_binject(a, src, nsrc, vals);
+}
+
+// receiver r of one problem at the step just taken (a_iso_3d.c:698-741)
+template <typename S>
+__device__ void a3d_sample(const A3Args &a, const A3Rec *rec, int r, const int32_t *table,
+                           long long nsteps_max, double *traces) {
     const long long it = *a.step - 1;
-    if (r >= nrec || it >= nsteps_max) return;
+    if (it >= nsteps_max) return;
     const A3Rec e = rec[r];
     const int32_t slot = table[(long long)e.group * nsteps_max + it];
     if (slot < 0) return;
-    const int16_t m = static_cast<const int16_t *>(a.f[e.field])[e.q];
-    const unsigned e8 = static_cast<const uint8_t *>(a.fe[e.field])[e.qe];
-    traces[e.out + slot] = static_cast<double>(bfp_val(m, bfp_dec(e8)));
+    if constexpr (std::is_same<S, Bfp16>::value) {
+        const int16_t m = static_cast<const int16_t *>(a.f[e.field])[e.q];
+        const unsigned e8 = static_cast<const uint8_t *>(a.fe[e.field])[e.qe];
+        traces[e.out + slot] = static_cast<double>(bfp_val(m, bfp_dec(e8)));
+    } else {
+        const S *p = static_cast<const S *>(a.f[e.field]) + e.q;
+        traces[e.out + slot] = static_cast<double>(Store<S>::ld(p, a.isc[e.field]));
+    }
+}
+
+__global__ void a3d_bgather_kernel(A3Args a, const A3Rec *rec, int nrec, const int32_t *table,
+                                   long long nsteps_max, double *traces) {
+    const int r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r < nrec) a3d_sample<Bfp16>(a, rec, r, table, nsteps_max, traces);
 }
 
 template <typename S>
 __global__ void a3d_gather_kernel(A3Args a, const A3Rec *rec, int nrec, const int32_t *table,
                                   long long nsteps_max, double *traces) {
-    using St = Store<S>;
     const int r = blockIdx.x * blockDim.x + threadIdx.x;
-    const long long it = *a.step - 1;
-    if (r >= nrec || it >= nsteps_max) return;
-    const A3Rec e = rec[r];
-    const int32_t slot = table[(long long)e.group * nsteps_max + it];
-    if (slot < 0) return;
-    const S *p = static_cast<const S *>(a.f[e.field]) + e.q;
-    traces[e.out + slot] = static_cast<double>(St::ld(p, a.isc[e.field]));
+    if (r < nrec) a3d_sample<S>(a, rec, r, table, nsteps_max, traces);
+}
+
+// ---------------------------------------------------------------------------
+// Several a_iso_3d problems (grids of different sizes) in one launch per
+// step: linear CTA b finds its problem in a prefix table of CTA counts; a
+// problem's CTAs are its ring tiles x chunks first, then its interior tiles
+// x chunks, and each runs the body the problem's own launches run for that
+// tile, so every problem gets the bits of its own step.  Each problem's TMA
+// maps are kernel parameters (read from parameter space like the
+// single-problem launches'); its other arguments are copied into shared
+// memory once per CTA.  Sources and receivers of all problems follow in one
+// launch each.
+// ---------------------------------------------------------------------------
+constexpr int kA3GroupMax = 16;
+
+template <typename M>
+struct A3GroupStepParams {
+    M m[kA3GroupMax];              // each problem's maps, old set as input
+    A3Args a[kA3GroupMax];         // its arguments for this step
+    int first[kA3GroupMax + 1];    // first linear CTA of each problem
+    int nedge[kA3GroupMax];        // its ring tiles
+    int n;
+};
+static_assert(sizeof(A3GroupStepParams<A3BMaps>) <= 32000, "kernel parameters are limited to 32 KB");
+static_assert(sizeof(A3Args) % 4 == 0, "A3Args is copied as 32-bit words");
+
+// problem, tile and chunk of linear CTA b; returns the tile's class
+template <typename M>
+__device__ __forceinline__ int a3_group_tile(const A3GroupStepParams<M> &P, A3Args &sa, int &kt,
+                                             int &jt, int &ch, int &p) {
+    const int b = blockIdx.x;
+    p = 0;
+    while (p + 1 < P.n && P.first[p + 1] <= b) ++p;
+    {
+        const int *src = reinterpret_cast<const int *>(&P.a[p]);
+        int *dst = reinterpret_cast<int *>(&sa);
+        const int tid = threadIdx.y * blockDim.x + threadIdx.x;
+        for (int i = tid; i < (int)(sizeof(A3Args) / 4); i += blockDim.x * blockDim.y) dst[i] = src[i];
+    }
+    __syncthreads();
+    int local = b - P.first[p];
+    if (local == 0 && threadIdx.x == 0 && threadIdx.y == 0) ++*sa.step;
+    const int ne = P.nedge[p];
+    const int nch = (sa.nx2 + sa.chunk - 1) / sa.chunk;
+    if (local < ne * nch) {
+        ch = local / ne;
+        a3_edge_tile(sa, local % ne, kt, jt);
+        return A3_EDGE;
+    }
+    local -= ne * nch;
+    const int nk = sa.kt1 - sa.kt0, nin = nk * (sa.jt1 - sa.jt0);
+    ch = local / nin;
+    kt = sa.kt0 + (local % nin) % nk;
+    jt = sa.jt0 + (local % nin) / nk;
+    return A3_INNER;
+}
+
+template <typename S, int W, int R, int D, int MINB>
+__global__ void __launch_bounds__(32 * W, MINB)
+    a3d_group_step_kernel(const __grid_constant__ A3GroupStepParams<A3Maps> P) {
+    __shared__ A3Args sa;
+    int kt, jt, ch, p;
+    if (a3_group_tile(P, sa, kt, jt, ch, p) == A3_EDGE)
+        a3d_step_body<S, W, R, D, A3_EDGE, A3_FACE_GEN>(sa, P.m[p], kt, jt, ch);
+    else
+        a3d_step_body<S, W, R, D, A3_INNER, A3_FACE_GEN>(sa, P.m[p], kt, jt, ch);
+}
+
+template <int W, int D, int MINB>
+__global__ void __launch_bounds__(32 * W, MINB)
+    a3d_bgroup_step_kernel(const __grid_constant__ A3GroupStepParams<A3BMaps> P) {
+    __shared__ A3Args sa;
+    int kt, jt, ch, p;
+    if (a3_group_tile(P, sa, kt, jt, ch, p) == A3_EDGE)
+        a3d_bstep_body<W, D, A3_EDGE, A3_FACE_GEN>(sa, P.m[p], kt, jt, ch);
+    else
+        a3d_bstep_body<W, D, A3_INNER, A3_FACE_GEN>(sa, P.m[p], kt, jt, ch);
+}
+
+// what the source and receiver kernels of one problem need after its step
+struct A3Post {
+    A3Args a;                 // bound to the state just written
+    const A3Src *src;
+    const double *vals;
+    const A3Rec *rec;
+    const int32_t *table;
+    long long nsteps_max;
+    double *traces;
+    int nsrc;
+};
+
+struct A3GroupPostParams {
+    A3Post q[kA3GroupMax];
+    int first_rec[kA3GroupMax + 1];   // prefix sums of the problems' receivers
+    int n;
+};
+static_assert(sizeof(A3GroupPostParams) <= 32000, "kernel parameters are limited to 32 KB");
+
+// block p adds problem p's sources (one thread, in source order)
+template <typename S>
+__global__ void a3d_group_source_kernel(const __grid_constant__ A3GroupPostParams P) {
+    if (threadIdx.x != 0 || (int)blockIdx.x >= P.n) return;
+    const A3Post &q = P.q[blockIdx.x];
+    if (q.nsrc == 0) return;
+    if constexpr (std::is_same<S, Bfp16>::value)
+        a3d_binject(q.a, q.src, q.nsrc, q.vals);
+    else
+        a3d_inject<S>(q.a, q.src, q.nsrc, q.vals);
+}
+
+template <typename S>
+__global__ void a3d_group_gather_kernel(const __grid_constant__ A3GroupPostParams P) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= P.first_rec[P.n]) return;
+    int p = 0;
+    while (p + 1 < P.n && P.first_rec[p + 1] <= t) ++p;
+    const A3Post &q = P.q[p];
+    a3d_sample<S>(q.a, q.rec, t - P.first_rec[p], q.table, q.nsteps_max, q.traces);
 }
 
 }  // namespace sm
@@ -1234,6 +1371,7 @@ struct sm_a3d {
     DevBuf f[2][4], psi[2][6], rho, K, coef;   // two buffer sets (ping-pong)
     int cur = 0;                               // set holding the current state
     int config = 6;                            // index into kA3Configs
+    uint64_t serial = 0;                       // unique per handle (grouped graphs' keys)
     int sms = 148;
     std::vector<A3Src> src;
     std::vector<double> vals;
@@ -1476,6 +1614,7 @@ int a3d_make_maps(sm_a3d *h, int ty) {
         if ((rc = make_map_3d(&m.K, h->K.p, dc, sizeof(C), n0, n1, n2, pt, 32, ty))) return rc;
     }
     h->maps_ty = ty;
+    h->graph_epoch++;   // maps are baked into captured graphs
     return SM_OK;
 }
 
@@ -1501,6 +1640,7 @@ int a3d_make_bmaps(sm_a3d *h, int ty) {
         if ((rc = make_map_3d(&m.K, h->K.p, f32, 4, n0, n1, n2, pt, 32, ty))) return rc;
     }
     h->maps_ty = ty;
+    h->graph_epoch++;   // maps are baked into captured graphs
     return SM_OK;
 }
 
@@ -1909,6 +2049,8 @@ extern "C" int sm_a3d_create(int device, size_t nx2, size_t ny2, size_t nz2, siz
     for (int p = 0; p < 6; ++p) { a.psc[p] = 1.f; a.pisc[p] = 1.f; }
     cudaDeviceGetAttribute(&h->sms, cudaDevAttrMultiProcessorCount, device);
     a.chunk = a3d_pick_chunk(nx2, ny2, nz2, h->sms, a3d_cfg(h.get(), h->config).ty());
+    static std::atomic<uint64_t> serials{1};
+    h->serial = serials.fetch_add(1);
     a3d_bind(h.get(), 0);
     a.rho = h->rho.p;
     a.K = h->K.p;
@@ -2149,6 +2291,290 @@ extern "C" int sm_a3d_run(sm_a3d_t h, size_t nsteps) {
     case SM_BFP16: rc = a3d_run_t<Bfp16>(h, nsteps); break;
     default: rc = a3d_run_t<float>(h, nsteps); break;
     }
+    if (rc) return rc;
+    SM_CUDA_TRY(cudaGetLastError());
+    return SM_OK;
+}
+
+namespace {
+
+// The grouped step's launch configuration: the default one of the storage
+// type (8 warps; FP32-like storage 2 rows per warp, block storage one block
+// of A3_BJ rows per thread).  Results do not depend on it.
+constexpr int kA3GW = 8, kA3GR = 2, kA3GD = 4, kA3GMinB = 3;
+constexpr int kA3GBD = 4, kA3GBMinB = 2;
+
+template <typename S>
+constexpr int a3d_group_ty() {
+    return std::is_same<S, Bfp16>::value ? kA3GW * A3_BJ : kA3GW * kA3GR;
+}
+
+template <typename S>
+size_t a3d_group_smem() {
+    if constexpr (std::is_same<S, Bfp16>::value)
+        return a3d_bstep_smem<kA3GW * A3_BJ, kA3GBD>();
+    else
+        return a3d_step_smem<S, kA3GW * kA3GR, kA3GD>();
+}
+
+template <typename S>
+int a3d_group_ready(int device) {
+    static std::mutex mu;
+    static bool done[64] = {};
+    if (device < 0 || device >= 64) return sm_fail(SM_EINVAL, "device %d", device);
+    std::lock_guard<std::mutex> lk(mu);
+    if (!done[device]) {
+        if constexpr (std::is_same<S, Bfp16>::value)
+            SM_CUDA_TRY(cudaFuncSetAttribute(a3d_bgroup_step_kernel<kA3GW, kA3GBD, kA3GBMinB>,
+                                             cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             (int)a3d_group_smem<S>()));
+        else
+            SM_CUDA_TRY(cudaFuncSetAttribute(a3d_group_step_kernel<S, kA3GW, kA3GR, kA3GD, kA3GMinB>,
+                                             cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             (int)a3d_group_smem<S>()));
+        done[device] = true;
+    }
+    return SM_OK;
+}
+
+// one grouped step of the problems hs[0..n) (n <= kA3GroupMax), on stream st
+template <typename S>
+int a3d_group_step(sm_a3d *const *hs, int n, cudaStream_t st) {
+    constexpr bool B = std::is_same<S, Bfp16>::value;
+    using M = std::conditional_t<B, A3BMaps, A3Maps>;
+    constexpr int TY = a3d_group_ty<S>();
+    static A3GroupStepParams<M> P;   // large: built in place, one caller at a time
+    static A3GroupPostParams Q;
+    static std::mutex mu;
+    std::lock_guard<std::mutex> lk(mu);
+    int total = 0;
+    for (int k = 0; k < n; ++k) {
+        sm_a3d *h = hs[k];
+        a3d_bind(h, h->cur);
+        a3d_tile_classes(h, TY);
+        const A3Args &a = h->args;
+        const int nch = (a.nx2 + a.chunk - 1) / a.chunk;
+        const int ninner = (a.kt1 - a.kt0) * (a.jt1 - a.jt0);
+        if constexpr (B) P.m[k] = h->bmaps[h->cur];
+        else P.m[k] = h->maps[h->cur];
+        P.a[k] = a;
+        P.nedge[k] = a.nkt * a.njt - ninner;
+        P.first[k] = total;
+        total += a.nkt * a.njt * nch;
+    }
+    P.first[n] = total;
+    P.n = n;
+    const dim3 blk(32, kA3GW, 1);
+    if constexpr (B)
+        a3d_bgroup_step_kernel<kA3GW, kA3GBD, kA3GBMinB><<<total, blk, a3d_group_smem<S>(), st>>>(P);
+    else
+        a3d_group_step_kernel<S, kA3GW, kA3GR, kA3GD, kA3GMinB><<<total, blk, a3d_group_smem<S>(), st>>>(P);
+    int nrec = 0;
+    bool src = false;
+    for (int k = 0; k < n; ++k) {
+        sm_a3d *h = hs[k];
+        h->cur = 1 - h->cur;
+        a3d_bind(h, h->cur);
+        A3Post &q = Q.q[k];
+        q.a = h->args;
+        q.src = h->d_src.as<A3Src>();
+        q.nsrc = (int)h->src.size();
+        q.vals = h->d_vals.as<double>();
+        q.rec = h->d_rec.as<A3Rec>();
+        q.table = h->d_table.as<int32_t>();
+        q.nsteps_max = (long long)h->plan.nsteps_max;
+        q.traces = h->d_traces.as<double>();
+        Q.first_rec[k] = nrec;
+        nrec += (int)h->rec.size();
+        src = src || !h->src.empty();
+    }
+    Q.first_rec[n] = nrec;
+    Q.n = n;
+    if (src) a3d_group_source_kernel<S><<<n, 32, 0, st>>>(Q);
+    if (nrec) a3d_group_gather_kernel<S><<<(nrec + 127) / 128, 128, 0, st>>>(Q);
+    hs[0]->timer.launches += 1 + (src ? 1 : 0) + (nrec ? 1 : 0);
+    SM_CUDA_TRY(cudaGetLastError());
+    return SM_OK;
+}
+
+template <typename S>
+int a3d_group_steps(sm_a3d *const *hs, int n, int steps) {
+    for (int s = 0; s < steps; ++s)
+        for (int k0 = 0; k0 < n; k0 += kA3GroupMax)
+            if (int rc = a3d_group_step<S>(hs + k0, std::min(kA3GroupMax, n - k0), hs[0]->stream))
+                return rc;
+    return SM_OK;
+}
+
+// CUDA graphs of kA3GroupGraphSteps grouped steps, cached per group: the key
+// holds each handle's serial, starting buffer set and graph epoch (sources,
+// receivers, scales, configuration), so a graph is only replayed on the
+// state it was captured for.  A few are kept, the least recently used
+// dropped.
+constexpr int kA3GroupGraphSteps = 16;
+constexpr size_t kA3GroupGraphCache = 8;
+
+struct A3GroupKey {
+    int device;
+    std::vector<std::tuple<uint64_t, int, unsigned, int>> members;
+    bool operator<(const A3GroupKey &o) const {
+        return std::tie(device, members) < std::tie(o.device, o.members);
+    }
+};
+struct A3GroupGraph {
+    cudaGraphExec_t exec = nullptr;
+    uint64_t used = 0;
+};
+std::mutex g_a3_group_mu;
+std::map<A3GroupKey, A3GroupGraph> g_a3_group_graphs;
+uint64_t g_a3_group_clock = 0;
+
+template <typename S>
+int a3d_group_graph(sm_a3d *const *hs, int n, cudaGraphExec_t *out) {
+    A3GroupKey key{hs[0]->device, {}};
+    for (int k = 0; k < n; ++k)
+        key.members.emplace_back(hs[k]->serial, hs[k]->cur, hs[k]->graph_epoch, hs[k]->args.chunk);
+    std::lock_guard<std::mutex> lk(g_a3_group_mu);
+    auto it = g_a3_group_graphs.find(key);
+    if (it != g_a3_group_graphs.end()) {
+        it->second.used = ++g_a3_group_clock;
+        *out = it->second.exec;
+        return SM_OK;
+    }
+    const size_t launches = hs[0]->timer.launches;
+    SM_CUDA_TRY(cudaStreamBeginCapture(hs[0]->stream, cudaStreamCaptureModeThreadLocal));
+    const int rc = a3d_group_steps<S>(hs, n, kA3GroupGraphSteps);
+    cudaGraph_t graph = nullptr;
+    cudaError_t e = cudaStreamEndCapture(hs[0]->stream, &graph);
+    hs[0]->timer.launches = launches;
+    for (int k = 0; k < n; ++k) a3d_bind(hs[k], hs[k]->cur);   // an even number of steps
+    if (rc) {
+        if (graph) cudaGraphDestroy(graph);
+        return rc;
+    }
+    if (e != cudaSuccess) return sm_fail(SM_ECUDA, "stream capture: %s", cudaGetErrorString(e));
+    cudaGraphExec_t exec = nullptr;
+    e = cudaGraphInstantiate(&exec, graph, 0);
+    cudaGraphDestroy(graph);
+    if (e != cudaSuccess) return sm_fail(SM_ECUDA, "cudaGraphInstantiate: %s", cudaGetErrorString(e));
+    if (g_a3_group_graphs.size() >= kA3GroupGraphCache) {
+        auto old = g_a3_group_graphs.begin();
+        for (auto i = g_a3_group_graphs.begin(); i != g_a3_group_graphs.end(); ++i)
+            if (i->second.used < old->second.used) old = i;
+        // some stream may still run it: wait before the executable goes
+        cudaDeviceSynchronize();
+        cudaGraphExecDestroy(old->second.exec);
+        g_a3_group_graphs.erase(old);
+    }
+    g_a3_group_graphs[key] = A3GroupGraph{exec, ++g_a3_group_clock};
+    *out = exec;
+    return SM_OK;
+}
+
+template <typename S>
+int a3d_group_run_t(sm_a3d *const *hs, int n, size_t nsteps) {
+    constexpr int TY = a3d_group_ty<S>();
+    for (int k = 0; k < n; ++k) {
+        sm_a3d *h = hs[k];
+        if (h->maps_ty == TY) continue;
+        int rc;
+        if constexpr (std::is_same<S, Bfp16>::value) rc = a3d_make_bmaps(h, TY);
+        else rc = a3d_make_maps<S>(h, TY);
+        if (rc) return rc;
+    }
+    if (int rc = a3d_group_ready<S>(hs[0]->device)) return rc;
+    const bool is16 = a3d_is16(hs[0]);
+    const size_t G = kA3GroupGraphSteps;
+    int per_step = 0;
+    for (int k0 = 0; k0 < n; k0 += kA3GroupMax) {
+        bool src = false, rec = false;
+        for (int k = k0; k < std::min(n, k0 + kA3GroupMax); ++k) {
+            src = src || !hs[k]->src.empty();
+            rec = rec || !hs[k]->rec.empty();
+        }
+        per_step += 1 + (src ? 1 : 0) + (rec ? 1 : 0);
+    }
+    while (nsteps > 0) {
+        // a graph of G steps when no handle rescales inside it
+        bool aligned = true;
+        for (int k = 0; k < n && is16; ++k) aligned = aligned && hs[k]->it % G == 0;
+        size_t done;
+        if (nsteps >= G && aligned) {
+            cudaGraphExec_t ex = nullptr;
+            if (int rc = a3d_group_graph<S>(hs, n, &ex)) return rc;
+            SM_CUDA_TRY(cudaGraphLaunch(ex, hs[0]->stream));
+            hs[0]->timer.launches += per_step * G;
+            done = G;
+        } else {
+            if (int rc = a3d_group_steps<S>(hs, n, 1)) return rc;
+            done = 1;
+        }
+        nsteps -= done;
+        for (int k = 0; k < n; ++k) {
+            sm_a3d *h = hs[k];
+            const size_t before = h->it;
+            h->it += done;
+            if (is16 && h->it / sm_a3d::kScalePeriod != before / sm_a3d::kScalePeriod)
+                if (int rc = a3d_rescale(h)) return rc;
+        }
+    }
+    return SM_OK;
+}
+
+}  // namespace
+
+// Several a_iso_3d handles of different grid sizes advanced together: every
+// step is one launch over all their tiles (up to 16 handles per launch), one
+// for all their sources and one for all their receivers.  Each handle ends
+// where sm_a3d_run(h, nsteps) would have left it, bit for bit.  The work
+// runs on the first handle's stream, ordered after the work already queued
+// on every handle's stream; every handle's stream waits for it to finish.
+extern "C" int sm_a3d_group_run(sm_a3d_t const *handles, int n, size_t nsteps) {
+    if (!handles || n <= 0) return sm_fail(SM_EINVAL, "sm_a3d_group_run: no handles");
+    for (int k = 0; k < n; ++k) {
+        if (int rc = a3d_check(handles[k])) return rc;
+        if (handles[k]->device != handles[0]->device ||
+            handles[k]->precision != handles[0]->precision)
+            return sm_fail(SM_EINVAL,
+                           "sm_a3d_group_run: handle %d differs in device or precision from "
+                           "handle 0", k);
+        for (int j = 0; j < k; ++j)
+            if (handles[j] == handles[k])
+                return sm_fail(SM_EINVAL, "sm_a3d_group_run: handle %d appears twice", k);
+    }
+    if (nsteps == 0) return SM_OK;
+    sm_a3d *const *hs = handles;
+    DeviceGuard g(hs[0]->device);
+    for (int k = 0; k < n; ++k) {
+        sm_a3d *h = hs[k];
+        if (!h->src_dirty && !h->rec_dirty) continue;
+        if (int rc = a3d_upload(h)) return rc;
+    }
+    // run every handle on the first handle's stream for the duration
+    const cudaStream_t st = hs[0]->stream;
+    std::vector<cudaStream_t> own(n);
+    cudaEvent_t ev = nullptr;
+    SM_CUDA_TRY(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+    for (int k = 1; k < n; ++k) {
+        cudaEventRecord(ev, hs[k]->stream);
+        cudaStreamWaitEvent(st, ev, 0);
+    }
+    for (int k = 0; k < n; ++k) {
+        own[k] = hs[k]->stream;
+        hs[k]->stream = st;
+    }
+    int rc;
+    switch (hs[0]->precision) {
+    case SM_FP64: rc = a3d_group_run_t<double>(hs, n, nsteps); break;
+    case SM_FP16: rc = a3d_group_run_t<__half>(hs, n, nsteps); break;
+    case SM_BF16: rc = a3d_group_run_t<__nv_bfloat16>(hs, n, nsteps); break;
+    case SM_BFP16: rc = a3d_group_run_t<Bfp16>(hs, n, nsteps); break;
+    default: rc = a3d_group_run_t<float>(hs, n, nsteps); break;
+    }
+    for (int k = 0; k < n; ++k) hs[k]->stream = own[k];
+    cudaEventRecord(ev, st);
+    for (int k = 1; k < n; ++k) cudaStreamWaitEvent(hs[k]->stream, ev, 0);
+    cudaEventDestroy(ev);
     if (rc) return rc;
     SM_CUDA_TRY(cudaGetLastError());
     return SM_OK;

@@ -70,7 +70,8 @@ struct sm_server {
     int device = 0;
     size_t budget = 0, used = 0, peak = 0;
     int max_active = 64, slice = 64, graph = 0;
-    bool group = false;   // e_iso requests stepped together (sm_eiso_group_run)
+    bool group = false;   // requests of one program and precision stepped together
+                          // (sm_eiso_group_run, sm_a3d_group_run)
     std::mutex mu;
     std::condition_variable cv;        // request finished / new request
     std::deque<std::shared_ptr<Req>> queue;
@@ -165,15 +166,22 @@ int feed(sm_server *s, Req &r) {
     return SM_OK;
 }
 
-// grouped mode: every running e_iso request of one precision that wants a
-// slice gets it from one sm_eiso_group_run call (one launch per step over
-// all of their grids); the slice is as long as the shortest remainder
+// grouped mode: every running request of one program and precision that
+// wants a slice gets it from one sm_eiso_group_run / sm_a3d_group_run call
+// (one launch per step over all of their grids); the slice is as long as the
+// shortest remainder
 int feed_group(sm_server *s, std::vector<Req *> &grp) {
     size_t k = (size_t)s->slice;
     for (Req *r : grp) k = std::min(k, r->nsteps - r->enqueued);
-    std::vector<sm_eiso_t> hs;
-    for (Req *r : grp) hs.push_back(r->he);
-    if (int rc = sm_eiso_group_run(hs.data(), (int)hs.size(), k)) return rc;
+    if (grp[0]->kind == 0) {
+        std::vector<sm_eiso_t> hs;
+        for (Req *r : grp) hs.push_back(r->he);
+        if (int rc = sm_eiso_group_run(hs.data(), (int)hs.size(), k)) return rc;
+    } else {
+        std::vector<sm_a3d_t> hs;
+        for (Req *r : grp) hs.push_back(r->ha);
+        if (int rc = sm_a3d_group_run(hs.data(), (int)hs.size(), k)) return rc;
+    }
     for (Req *r : grp) {
         cudaEvent_t ev = nullptr;
         if (cudaEventCreateWithFlags(&ev, cudaEventDisableTiming) != cudaSuccess ||
@@ -245,15 +253,15 @@ void work(sm_server *s) {
         }
         std::map<Req *, int> grc;   // grouped feed failures
         if (s->group) {
-            std::map<int, std::vector<Req *>> need;   // by precision
+            std::map<std::pair<int, int>, std::vector<Req *>> need;   // by program, precision
             for (auto &r : run) {
                 while (!r->slices.empty() && cudaEventQuery(r->slices.front()) == cudaSuccess) {
                     cudaEventDestroy(r->slices.front());
                     r->slices.pop_front();
                     progress = true;
                 }
-                if (r->kind == 0 && r->enqueued < r->nsteps && r->slices.size() < 2)
-                    need[r->e.precision].push_back(r.get());
+                if (r->enqueued < r->nsteps && r->slices.size() < 2)
+                    need[{r->kind, r->kind == 0 ? r->e.precision : r->a.precision}].push_back(r.get());
             }
             for (auto &g : need) {
                 const int rc = feed_group(s, g.second);
@@ -271,7 +279,7 @@ void work(sm_server *s) {
                 r->slices.pop_front();
                 progress = true;
             }
-            while (rc == SM_OK && !(s->group && r->kind == 0) && r->enqueued < r->nsteps &&
+            while (rc == SM_OK && !s->group && r->enqueued < r->nsteps &&
                    r->slices.size() < 2) {
                 rc = feed(s, *r);
                 progress = true;
