@@ -114,10 +114,16 @@ class Clocks:
 # workloads and algorithmic bytes
 # ----------------------------------------------------------------------------
 
+# bytes per stored value in block storage: a 16-bit mantissa and the share
+# of the block's exponent byte (a_iso_3d: blocks of 4 y rows; e_iso: 4 x rows)
+A3D_BFP_BYTES = 2.25
+EISO_BFP_BYTES = 2.25
+
+
 def a3d_bytes_per_step(p, s, m=4, psi=None):
     """Ncell (8 s + 2 m) + sum over axes of N_slab 4 p (state R+W, rho & K read
     once, both CPML memory variables R+W on their slabs).  Block storage:
-    s = 2 + 1/4 (a mantissa and a quarter of an exponent byte per value),
+    s = A3D_BFP_BYTES (a mantissa and a share of an exponent byte per value),
     p = 4 (FP32 memory variables)."""
     psi = s if psi is None else psi
     n2 = [n + 2 * p.npml for n in p.shape]
@@ -253,7 +259,8 @@ def run_ours(args, rank, world, local_rank, torch, dist):
     from seismod_b200 import api
     kind, p, desc = make_workload(args.workload, args.size)
     prec = args.precision
-    sbytes = {"fp32": 4, "fp64": 8, "fp16": 2, "bf16": 2, "bfp16": 2.25}[prec]
+    sbytes = {"fp32": 4, "fp64": 8, "fp16": 2, "bf16": 2,
+              "bfp16": A3D_BFP_BYTES if kind == "a3d" else EISO_BFP_BYTES}[prec]
     mbytes = 8 if prec == "fp64" else 4
     nshots = len(p.shots) if kind == "eiso" else 1
     if kind == "a3d":
@@ -381,7 +388,7 @@ def headline(local_rank, cfg1_precisions):
         ms, kms = timed_rate("eiso", p, prec, local_rank, 200)
         batch = api.run_eiso(p, prec, None, local_rank)
         err = max(trace_err(batch[s], ref[s]) for s in ref)
-        bps = eiso_bytes_per_step(p, nsh, 2.25 if prec == "bfp16" else 4.0, 4,
+        bps = eiso_bytes_per_step(p, nsh, EISO_BFP_BYTES if prec == "bfp16" else 4.0, 4,
                                   4.0 if prec == "bfp16" else None)
         sps = nsh / (ms * 1e-3 * n)
         e[f"batched_{prec}"] = {
@@ -406,7 +413,7 @@ def headline(local_rank, cfg1_precisions):
     for prec in ("fp32", "bfp16"):
         ms, kms = timed_rate("a3d", q, prec, local_rank, 100)
         err = trace_err(api.run_a3d(q, prec, local_rank), ref3)
-        sb = 2.25 if prec == "bfp16" else 4.0
+        sb = A3D_BFP_BYTES if prec == "bfp16" else 4.0
         bps = a3d_bytes_per_step(q, sb, 4, 4 if prec == "bfp16" else None)
         a[prec] = {"ms_per_step": round(ms, 5), "gcell_per_s": round(q.cells / (ms * 1e-3) / 1e9, 3),
                    "shots_per_s": round(1.0 / (ms * 1e-3 * 2000), 4),

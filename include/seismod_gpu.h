@@ -48,10 +48,11 @@ extern "C" {
  * FP32 and FP64 compute in their own type; FP16 and BF16 store 16-bit values
  * with one power-of-two scale per field and compute in FP32.  BFP16 (block
  * floating point) stores the wavefields as 16-bit integer mantissas sharing
- * one 8-bit exponent per block of cells (a_iso_3d: 8 consecutive y rows of a
- * z column; e_iso: 8 consecutive x rows of a z column), set from the block's
+ * one 8-bit exponent per block of cells (a_iso_3d: 4 consecutive y rows of a
+ * z column; e_iso: 4 consecutive x rows of a z column), set from the block's
  * largest value at every store, and computes in FP32; the CPML memory
- * variables and split parts stay FP32.  The reference stores FP64
+ * variables and split parts stay FP32, and e_iso keeps the 20 x 9 cells
+ * around each source in FP32 as well.  The reference stores FP64
  * (a_iso_3d.c:319-335, e_iso.c:384-411); BFP16 is the reduced-storage form
  * whose trace error stays below 1e-3 of FP64 on the benchmark shots. */
 #define SM_FP32 0

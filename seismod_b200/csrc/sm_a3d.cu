@@ -118,13 +118,15 @@ struct A3Lay {
     static constexpr size_t oZ = oY + al(bY), oK = oZ + al(bZ);
     static constexpr size_t stage = oK + al(bK);
     static constexpr unsigned tx = (unsigned)(bP + bR + bX + bY + bZ + bK);
-    // head: the stage mbarriers, two vy row buffers [TY+1][32], and the
-    // CPML coefficient tables of the chunk's planes, the tile's rows and columns
+    // head: the stage mbarriers, two vy row buffers [TY+1][32], the CPML
+    // coefficient tables of the chunk's planes, the tile's rows and columns,
+    // and two buffers [TY] of the halo column vz(k0-1)
     static constexpr size_t oVY = al(D_HEAD_BARS * 8);
     static constexpr size_t oCX = oVY + al((size_t)2 * (TY + 1) * 32 * sizeof(C));
     static constexpr size_t oCY = oCX + al((size_t)6 * (A3_CHMAX + 2) * sizeof(C));
     static constexpr size_t oCZ = oCY + al((size_t)6 * (TY + 1) * sizeof(C));
-    static constexpr size_t head = oCZ + al((size_t)6 * 33 * sizeof(C));
+    static constexpr size_t oVZ = oCZ + al((size_t)6 * 33 * sizeof(C));
+    static constexpr size_t head = oVZ + al((size_t)2 * TY * sizeof(C));
 };
 
 // one velocity component (a_iso_3d.c:605-651):
@@ -243,10 +245,17 @@ __device__ __forceinline__ void a3d_step_body(const A3Args &a, const A3Maps &m, 
     C(*CX)[NXT] = reinterpret_cast<C(*)[NXT]>(smem + L::oCX);     // [6][NXT]
     C(*CY)[TY + 1] = reinterpret_cast<C(*)[TY + 1]>(smem + L::oCY);  // [6][TY+1]
     C(*CZ)[33] = reinterpret_cast<C(*)[33]>(smem + L::oCZ);          // [6][33]
+    C(*VZH)[TY] = reinterpret_cast<C(*)[TY]>(smem + L::oVZ);         // [2][TY]
     unsigned char *ring = smem + L::head;
 
     const int lane = threadIdx.x, w = threadIdx.y;
     const int tid = w * 32 + lane;
+    // the TMA loads are issued by the last warp's lane 0, the halo row is
+    // computed by warp 0 and the halo column by warp HW (one lane per row),
+    // so the three per-plane extras fall to different warps
+    constexpr int HW = W > 2 ? 1 : 0;
+    static_assert(TY <= 32, "one halo-column lane per tile row");
+    const bool producer = tid == 32 * (W - 1);
     const int k0 = kt * 32, j0 = jt * TY;
     const int lo = a.np > 1 ? a.np : 1;
     const bool ytile = j0 >= lo && j0 + TY - 1 <= a.ny2 - 2 - a.np;
@@ -306,14 +315,14 @@ __device__ __forceinline__ void a3d_step_body(const A3Args &a, const A3Maps &m, 
         const bool ok = p >= 0 && p < (half ? nz2 - 1 : nz2);
         CZ[wch][e] = ok ? cf[a.cf.at(2, half ? 3 + wch : wch - 3) + p] : C(wch % 3 == 0 ? 0 : 1);
     }
-    if (tid == 0) {
+    if (producer) {
         for (int d = 0; d < D; ++d) mbar_init(&bars[d], 1);
         fence_proxy_async();
     }
 
     // ring of planes i0 .. min(i1, nx2-1), local index l = plane - i0
     const int nload = min(i1 + 1, nx2) - i0;
-    auto issue = [&](int l) {   // thread 0 only
+    auto issue = [&](int l) {   // the producer thread only
         if (l >= nload) return;
         unsigned char *b = ring + (size_t)(l % D) * L::stage;
         uint64_t *bar = &bars[l % D];
@@ -328,7 +337,7 @@ __device__ __forceinline__ void a3d_step_body(const A3Args &a, const A3Maps &m, 
         tma_load_3d(b + L::oK, &m.K, k0, j0, ip, bar);
     };
     __syncthreads();   // barriers initialised, tables filled
-    if (tid == 0)
+    if (producer)
         for (int l = 0; l < D - 2; ++l) issue(l);
 
     // per-row / per-column frame membership (fixed over the march)
@@ -346,8 +355,9 @@ __device__ __forceinline__ void a3d_step_body(const A3Args &a, const A3Maps &m, 
     const int kn = kin ? node_slab(k, nz2, np) : -1;
     const int jm = j0 - 1, km = k0 - 1;
     const int jmh = (jm >= 0) ? half_slab(jm, ny2, np) : -1;
-    const int hrow = w * R + lane;                 // halo-column row of lanes 0..R-1
-    const bool hcol = lane < R && km >= 0 && j0 + hrow < ny2;
+    const int hrow = lane;                         // halo-column row of warp HW's lane
+    const bool hwarp = w == HW && lane < TY;
+    const bool hcol = hwarp && km >= 0 && j0 + hrow < ny2;
     const int kmh = (km >= 0) ? half_slab(km, nz2, np) : -1;
     // Per-axis fast flags.  An axis is "fast" for a cell when neither its CPML
     // frame nor the grid edge touches it: the velocity component along the
@@ -414,9 +424,9 @@ __device__ __forceinline__ void a3d_step_body(const A3Args &a, const A3Maps &m, 
     };
 
     // per-thread state carried between planes, one entry per row
-    C vxa[R], vxb[R], vzp[R], vzhp[R];
+    C vxa[R], vxb[R], vzp[R];
 #pragma unroll
-    for (int r = 0; r < R; ++r) { vxa[r] = C(0); vxb[r] = C(0); vzp[r] = C(0); vzhp[r] = C(0); }
+    for (int r = 0; r < R; ++r) { vxa[r] = C(0); vxb[r] = C(0); vzp[r] = C(0); }
     // vx(i0-1) (direct loads, once per CTA): the pressure of plane i0 needs it
     if (i0 >= 1) {
         const int s = half_slab(i0 - 1, nx2, np);
@@ -449,8 +459,7 @@ __device__ __forceinline__ void a3d_step_body(const A3Args &a, const A3Maps &m, 
         for (int r = 0; r < R; ++r) {
             const int row = w * R + r, j = j0 + row;
             C vzm = __shfl_up_sync(0xffffffffu, vzp[r], 1);
-            const C hal = __shfl_sync(0xffffffffu, vzhp[r], r);
-            if (lane == 0) vzm = hal;
+            if (lane == 0) vzm = VZH[ip & 1][row];
             if (!rin[r]) continue;
             const C p_c = St::ld(pP + (row + 1) * WS + HS + lane, isP);
             C pn = p_c;
@@ -486,7 +495,7 @@ __device__ __forceinline__ void a3d_step_body(const A3Args &a, const A3Maps &m, 
 
     for (int i = i0; i < i1; ++i) {
         const int l = i - i0;
-        if (tid == 0) issue(l + D - 2);
+        if (producer) issue(l + D - 2);
         if (!mbar_wait(&bars[l % D], (l / D) & 1, a.err, 1)) return;
         if (i + 1 < nx2 && !mbar_wait(&bars[(l + 1) % D], ((l + 1) / D) & 1, a.err, 1)) return;
         const unsigned char *cbuf = ring + (size_t)(l % D) * L::stage;
@@ -509,7 +518,6 @@ __device__ __forceinline__ void a3d_step_body(const A3Args &a, const A3Maps &m, 
         // grid (from the zero fill): such values are neither stored nor
         // read by a cell inside the grid.
         C vxn[R], vzn[R];
-        C vzh = C(0);
         auto velocity = [&](auto AFt) {
         constexpr bool AF = decltype(AFt)::value;
         const bool fx = AF || xf, fy = AF || yfast, fz = AF || zfast;
@@ -571,13 +579,18 @@ __device__ __forceinline__ void a3d_step_body(const A3Args &a, const A3Maps &m, 
             }
             vyw[0][lane] = vyh;
         }
-        // halo column: vz(i, j, k0-1) of row w*R + lane, by lanes 0..R-1
-        if (hcol) {
-            const int cc = (hrow + 1) * WS + HS, rc = (hrow + 1) * WC + HC;
-            C psi_new;
-            vzh = a3_vel<C>(St::ld(cZ + hrow * WZ + HS - 1, isZ), St::ld(cP + cc - 1, isP),
-                            St::ld(cP + cc, isP), cR[rc - 1], cR[rc], idz, two_dt, kmh >= 0, CZ[0][0],
-                            CZ[1][0], CZ[2][0], fHz, psi_new);
+        // halo column: vz(i, j, k0-1) of row `lane`, by warp HW; read by
+        // the pressure of plane i (next iteration, after the barrier)
+        if (hwarp) {
+            C vzh = C(0);
+            if (hcol) {
+                const int cc = (hrow + 1) * WS + HS, rc = (hrow + 1) * WC + HC;
+                C psi_new;
+                vzh = a3_vel<C>(St::ld(cZ + hrow * WZ + HS - 1, isZ), St::ld(cP + cc - 1, isP),
+                                St::ld(cP + cc, isP), cR[rc - 1], cR[rc], idz, two_dt, kmh >= 0,
+                                CZ[0][0], CZ[1][0], CZ[2][0], fHz, psi_new);
+            }
+            VZH[i & 1][hrow] = vzh;
         }
         // memory variables for the next plane's velocities
         if (i + 1 < i1) load_vpsi(i + 1);
@@ -594,9 +607,7 @@ __device__ __forceinline__ void a3d_step_body(const A3Args &a, const A3Maps &m, 
             vxa[r] = vxn[r];
             vzp[r] = vzn[r];
         }
-#pragma unroll
-        for (int r = 0; r < R; ++r) vzhp[r] = (lane == r) ? vzh : vzhp[r];
-        __syncthreads();   // vy rows of plane i visible; the oldest stage may be refilled
+        __syncthreads();   // vy rows and halo column of plane i visible; the oldest stage may be refilled
     }
     // the last plane's pressure
     if (i1 > i0) {
@@ -698,10 +709,16 @@ __device__ __forceinline__ void a3d_bstep_body(const A3Args &a, const A3BMaps &m
     C(*CX)[NXT] = reinterpret_cast<C(*)[NXT]>(smem + HL::oCX);
     C(*CY)[TY + 1] = reinterpret_cast<C(*)[TY + 1]>(smem + HL::oCY);
     C(*CZ)[33] = reinterpret_cast<C(*)[33]>(smem + HL::oCZ);
+    C *VZH = reinterpret_cast<C *>(smem + HL::oVZ);   // [2][TY]: halo column by plane parity
     unsigned char *ring = smem + L::head;
 
     const int lane = threadIdx.x, w = threadIdx.y;
     const int tid = w * 32 + lane;
+    // TMA loads issued by the last warp's lane 0, the halo row computed by
+    // warp 0 and the halo column by warp HW (rows lane, lane + 32, ...)
+    constexpr int HW = W > 2 ? 1 : 0;
+    constexpr int NH = (TY + 31) / 32;
+    const bool producer = tid == 32 * (W - 1);
     const int k0 = kt * 32, j0 = jt * TY, jb0 = jt * (TY / R);
     const int lo = a.np > 1 ? a.np : 1;
     const bool ytile = j0 >= lo && j0 + TY - 1 <= a.ny2 - 2 - a.np;
@@ -765,13 +782,13 @@ __device__ __forceinline__ void a3d_bstep_body(const A3Args &a, const A3BMaps &m
         const bool ok = p >= 0 && p < (half ? nz2 - 1 : nz2);
         CZ[wch][e] = ok ? cf[a.cf.at(2, half ? 3 + wch : wch - 3) + p] : C(wch % 3 == 0 ? 0 : 1);
     }
-    if (tid == 0) {
+    if (producer) {
         for (int d = 0; d < D; ++d) mbar_init(&bars[d], 1);
         fence_proxy_async();
     }
 
     const int nload = min(i1 + 1, nx2) - i0;
-    auto issue = [&](int l) {   // thread 0 only
+    auto issue = [&](int l) {   // the producer thread only
         if (l >= nload) return;
         unsigned char *b = ring + (size_t)(l % D) * L::stage;
         uint64_t *bar = &bars[l % D];
@@ -790,7 +807,7 @@ __device__ __forceinline__ void a3d_bstep_body(const A3Args &a, const A3BMaps &m
         tma_load_3d(b + L::oK, &m.K, k0, j0, ip, bar);
     };
     __syncthreads();   // barriers initialised, tables filled
-    if (tid == 0)
+    if (producer)
         for (int l = 0; l < D - 2; ++l) issue(l);
 
     // rows of this thread: one block, rows j0 + w*R + r
@@ -810,8 +827,7 @@ __device__ __forceinline__ void a3d_bstep_body(const A3Args &a, const A3BMaps &m
     const int kn = kin ? node_slab(k, nz2, np) : -1;
     const int jm = j0 - 1, km = k0 - 1;
     const int jmh = (jm >= 0) ? half_slab(jm, ny2, np) : -1;
-    const int hrow = w * R + lane;
-    const bool hcol = lane < R && km >= 0 && j0 + hrow < ny2;
+    const bool hwarp = w == HW;
     const int kmh = (km >= 0) ? half_slab(km, nz2, np) : -1;
     const bool yfast = CLS == A3_INNER || FACE == A3_FACE_Z || ytile;
     const bool zfast = CLS == A3_INNER || FACE == A3_FACE_Y || ztile;
@@ -826,7 +842,9 @@ __device__ __forceinline__ void a3d_bstep_body(const A3Args &a, const A3BMaps &m
         return reinterpret_cast<const int16_t *>(sb + L::oP)[row * WP + x];
     };
 
-    C fPx[R], fPy[R], fPz[R], fVx[R], fVy[R], fVz[R], fHy = C(0), fHz = C(0);
+    C fPx[R], fPy[R], fPz[R], fVx[R], fVy[R], fVz[R], fHy = C(0), fHz[NH];
+#pragma unroll
+    for (int h = 0; h < NH; ++h) fHz[h] = C(0);
 #pragma unroll
     for (int r = 0; r < R; ++r) {
         fPx[r] = C(0); fPy[r] = C(0); fPz[r] = C(0);
@@ -851,7 +869,13 @@ __device__ __forceinline__ void a3d_bstep_body(const A3Args &a, const A3BMaps &m
             }
         }
         if (w == 0 && kin && jmh >= 0) fHy = psPy[(ip * 2 * np + jmh) * pitch + k];
-        if (hcol && kmh >= 0) fHz = psPz[(ip * ny2 + j0 + hrow) * 2 * np + kmh];
+        if (hwarp && km >= 0 && kmh >= 0) {
+#pragma unroll
+            for (int h = 0; h < NH; ++h) {
+                const int hr = lane + 32 * h;
+                if (hr < TY && j0 + hr < ny2) fHz[h] = psPz[(ip * ny2 + j0 + hr) * 2 * np + kmh];
+            }
+        }
     };
     auto load_ppsi = [&](int ip) {
         const int s = node_slab(ip, nx2, np);
@@ -874,7 +898,6 @@ __device__ __forceinline__ void a3d_bstep_body(const A3Args &a, const A3BMaps &m
     };
 
     C vxa[R], vxb[R], vzp[R];
-    C vzhp = C(0);    // lane r < R: the halo-column vz of row w*R + r, previous plane
     C pc[R], pp[R];   // decoded P of plane i (own cells) and of plane i-1
 #pragma unroll
     for (int r = 0; r < R; ++r) {
@@ -939,8 +962,7 @@ __device__ __forceinline__ void a3d_bstep_body(const A3Args &a, const A3BMaps &m
         for (int r = 0; r < R; ++r) {
             const int row = w * R + r, j = j0 + row;
             C vzm = __shfl_up_sync(0xffffffffu, vzp[r], 1);
-            const C hal = __shfl_sync(0xffffffffu, vzhp, r);
-            if (lane == 0) vzm = hal;
+            if (lane == 0) vzm = VZH[(ip & 1) * TY + row];
             const C p_c = pp[r];
             pn[r] = p_c;
             if (!rin[r]) continue;
@@ -975,7 +997,7 @@ __device__ __forceinline__ void a3d_bstep_body(const A3Args &a, const A3BMaps &m
 
     for (int i = i0; i < i1; ++i) {
         const int l = i - i0;
-        if (tid == 0) issue(l + D - 2);
+        if (producer) issue(l + D - 2);
         if (!mbar_wait(&bars[l % D], (l / D) & 1, a.err, 1)) return;
         if (i + 1 < nx2 && !mbar_wait(&bars[(l + 1) % D], ((l + 1) / D) & 1, a.err, 1)) return;
         const unsigned char *cbuf = ring + (size_t)(l % D) * L::stage;
@@ -1007,7 +1029,6 @@ __device__ __forceinline__ void a3d_bstep_body(const A3Args &a, const A3BMaps &m
 
         // ---- velocity half step at plane i (a_iso_3d.c:605-651) ----
         C vxn[R], vyn[R], vzn[R];
-        C vzh = C(0);
         auto velocity = [&](auto AFt) {
         constexpr bool AF = decltype(AFt)::value;
         const bool fx = AF || xf, fy = AF || yfast, fz = AF || zfast;
@@ -1069,15 +1090,27 @@ __device__ __forceinline__ void a3d_bstep_body(const A3Args &a, const A3BMaps &m
             }
             vyw[0][lane] = vyh;
         }
-        // halo column: vz(i, j, k0-1) of row w*R + lane, by lanes 0..R-1
-        if (hcol) {
-            const int rc = (hrow + 1) * WR + 4;
-            const BDec dP0 = bfp_dec(eP_(cbuf, w + 1, 15)), dP1 = bfp_dec(eP_(cbuf, w + 1, 16));
-            C psi_new;
-            vzh = a3_vel<C>(bfp_val(cZ[hrow * WZ + 7], bfp_dec(eZ_(cbuf, 15))),
-                            bfp_val(mP(cbuf, hrow + 1, 7), dP0), bfp_val(mP(cbuf, hrow + 1, 8), dP1),
-                            cR[rc - 1], cR[rc], idz, two_dt, kmh >= 0, CZ[0][0], CZ[1][0], CZ[2][0],
-                            fHz, psi_new);
+        // halo column: vz(i, j, k0-1) of rows lane, lane + 32, ..., by warp
+        // HW; read by the pressure of plane i (next iteration, after the
+        // barrier)
+        if (hwarp) {
+#pragma unroll
+            for (int h = 0; h < NH; ++h) {
+                const int hr = lane + 32 * h;
+                if (hr >= TY) continue;
+                C vzh = C(0);
+                if (km >= 0 && j0 + hr < ny2) {
+                    const int rc = (hr + 1) * WR + 4, hb = hr / R;
+                    const BDec dP0 = bfp_dec(eP_(cbuf, hb + 1, 15));
+                    const BDec dP1 = bfp_dec(eP_(cbuf, hb + 1, 16));
+                    const BDec dZh = bfp_dec(cbuf[L::oEZ + hb * WEZ + 15]);
+                    C psi_new;
+                    vzh = a3_vel<C>(bfp_val(cZ[hr * WZ + 7], dZh), bfp_val(mP(cbuf, hr + 1, 7), dP0),
+                                    bfp_val(mP(cbuf, hr + 1, 8), dP1), cR[rc - 1], cR[rc], idz,
+                                    two_dt, kmh >= 0, CZ[0][0], CZ[1][0], CZ[2][0], fHz[h], psi_new);
+                }
+                VZH[(i & 1) * TY + hr] = vzh;
+            }
         }
         if (i + 1 < i1) load_vpsi(i + 1);
         if (i > i0) {
@@ -1094,7 +1127,6 @@ __device__ __forceinline__ void a3d_bstep_body(const A3Args &a, const A3BMaps &m
             pp[r] = pc[r];
             pc[r] = pnx[r];
         }
-        vzhp = vzh;
         __syncthreads();
     }
     if (i1 > i0) {
@@ -1711,6 +1743,7 @@ size_t a3d_config_smem(int config) {
     }
 }
 
+// the block-storage configurations of kA3BConfigs as template arguments
 size_t a3d_bconfig_smem(int config) {
     switch (config) {
     case 0: return a3d_bstep_smem<8 * A3_BJ, 4>();
@@ -2301,7 +2334,11 @@ namespace {
 // The grouped step's launch configuration: the default one of the storage
 // type (8 warps; FP32-like storage 2 rows per warp, block storage one block
 // of A3_BJ rows per thread).  Results do not depend on it.
-constexpr int kA3GW = 8, kA3GR = 2, kA3GD = 4, kA3GMinB = 3;
+constexpr int kA3GW = 8, kA3GR = 2, kA3GD = 4;
+// resident CTAs the grouped kernel's registers are fitted to (both tile
+// bodies in one kernel: FP64 needs the larger budget to stay out of local memory)
+template <typename S>
+constexpr int a3d_group_minb() { return sizeof(S) == 8 ? 2 : 3; }
 constexpr int kA3GBD = 4, kA3GBMinB = 2;
 
 template <typename S>
@@ -2329,7 +2366,7 @@ int a3d_group_ready(int device) {
                                              cudaFuncAttributeMaxDynamicSharedMemorySize,
                                              (int)a3d_group_smem<S>()));
         else
-            SM_CUDA_TRY(cudaFuncSetAttribute(a3d_group_step_kernel<S, kA3GW, kA3GR, kA3GD, kA3GMinB>,
+            SM_CUDA_TRY(cudaFuncSetAttribute(a3d_group_step_kernel<S, kA3GW, kA3GR, kA3GD, a3d_group_minb<S>()>,
                                              cudaFuncAttributeMaxDynamicSharedMemorySize,
                                              (int)a3d_group_smem<S>()));
         done[device] = true;
@@ -2368,7 +2405,7 @@ int a3d_group_step(sm_a3d *const *hs, int n, cudaStream_t st) {
     if constexpr (B)
         a3d_bgroup_step_kernel<kA3GW, kA3GBD, kA3GBMinB><<<total, blk, a3d_group_smem<S>(), st>>>(P);
     else
-        a3d_group_step_kernel<S, kA3GW, kA3GR, kA3GD, kA3GMinB><<<total, blk, a3d_group_smem<S>(), st>>>(P);
+        a3d_group_step_kernel<S, kA3GW, kA3GR, kA3GD, a3d_group_minb<S>()><<<total, blk, a3d_group_smem<S>(), st>>>(P);
     int nrec = 0;
     bool src = false;
     for (int k = 0; k < n; ++k) {
