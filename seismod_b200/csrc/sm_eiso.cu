@@ -644,11 +644,59 @@ __device__ __forceinline__ void eiso_slabg_body(const EisoArgs &a, const CUtenso
     }
 }
 
+// Launch order of the slabs: the slab grid is gx (z) x gy (x) per shot, and
+// the rectangle [bx0, bx1) x [by0, by1) holds the slabs whose every warp is
+// clear of the PML frame (the lean path).  CTA b of the 1-D grid takes the
+// rectangle's slabs of every shot first, then the frame's, so the lean
+// loop and the frame's general path mostly run on the device at different
+// times (one loop's code in the instruction caches at a time).  The order
+// changes nothing else: each slab writes only its own cells.
+struct SlabOrder {
+    int gx, gy, bx0, bx1, by0, by1;
+};
+
+__device__ __forceinline__ void slab_of(const SlabOrder &o, int nshots, int b, int &bx, int &by,
+                                        int &shot) {
+    const int nix = o.bx1 - o.bx0, nin = nix * (o.by1 - o.by0);
+    if (b < nin * nshots) {
+        shot = b / nin;
+        const int r = b - shot * nin;
+        bx = o.bx0 + r % nix;
+        by = o.by0 + r / nix;
+        return;
+    }
+    b -= nin * nshots;
+    const int nring = o.gx * o.gy - nin;
+    shot = b / nring;
+    int e = b - shot * nring;
+    const int top = o.by0 * o.gx;   // rows of slabs before the rectangle
+    if (e < top) {
+        bx = e % o.gx;
+        by = e / o.gx;
+        return;
+    }
+    e -= top;
+    const int bot = (o.gy - o.by1) * o.gx;   // ... and after it
+    if (e < bot) {
+        bx = e % o.gx;
+        by = o.by1 + e / o.gx;
+        return;
+    }
+    e -= bot;
+    const int nox = o.gx - nix;   // the rectangle's rows: slabs left and right of it
+    by = o.by0 + e / nox;
+    const int c = e % nox;
+    bx = c < o.bx0 ? c : o.bx1 + (c - o.bx0);
+}
+
 template <typename S, int W, int TX, int MINB>
 __global__ void __launch_bounds__(32 * W, MINB) eiso_slabg_kernel(const EisoArgs a,
-                                                                  const __grid_constant__ EisoSlabMaps mp) {
+                                                                  const __grid_constant__ EisoSlabMaps mp,
+                                                                  const SlabOrder o) {
     extern __shared__ __align__(128) unsigned char smem[];
-    eiso_slabg_body<S, W, TX>(a, &mp.f, blockIdx.x, blockIdx.y, blockIdx.z, smem);
+    int bx, by, shot;
+    slab_of(o, a.nshots, blockIdx.x, bx, by, shot);
+    eiso_slabg_body<S, W, TX>(a, &mp.f, bx, by, shot, smem);
 }
 
 // Persistent form of the slab step: a CTA per SM slot walks the slabs
@@ -1082,9 +1130,12 @@ __device__ __forceinline__ void eiso_bslab_body(const EisoArgs &a, const CUtenso
 
 template <int W, int TX, int MINB>
 __global__ void __launch_bounds__(32 * W, MINB) eiso_bslab_kernel(const EisoArgs a,
-                                                                  const __grid_constant__ EisoBMaps mp) {
+                                                                  const __grid_constant__ EisoBMaps mp,
+                                                                  const SlabOrder o) {
     extern __shared__ __align__(128) unsigned char smem[];
-    eiso_bslab_body<W, TX>(a, &mp.f, &mp.e, blockIdx.x, blockIdx.y, blockIdx.z, smem);
+    int bx, by, shot;
+    slab_of(o, a.nshots, blockIdx.x, bx, by, shot);
+    eiso_bslab_body<W, TX>(a, &mp.f, &mp.e, bx, by, shot, smem);
 }
 
 // Persistent form: a CTA per SM slot walks the slabs s = blockIdx.x,
@@ -1883,12 +1934,39 @@ int ready_slabg_cfg(sm_eiso *h) {
     return allow_smem(eiso_slabg_kernel<S, W, TX, MINB>, ESlabG<S, W, TX>::bytes, h->device);
 }
 
+// the launch order of the slabs of W warps x TX rows (SlabOrder): the lean
+// rectangle first, or (lean_first false) every shot's slabs in grid order.
+// Measured on the 64-shot 1040 x 540 batch: block storage 0.514 against
+// 0.553 ms per step with the rectangle first; FP32 0.440 against 0.415, so
+// FP32 keeps the grid order.
+SlabOrder slab_order(const sm_eiso *h, int W, int TX, bool lean_first) {
+    const int wz = (int)((h->NZ + 29) / 30);
+    SlabOrder o{(wz + W - 1) / W, (int)((h->NX + TX - 1) / TX), 0, 0, 0, 0};
+    o.by0 = o.by1 = o.gy;   // no rectangle: grid order
+    if (!lean_first) return o;
+    const long long np = (long long)h->np, nx = (long long)h->nx, nz = (long long)h->nz;
+    // slab bx is lean in z when its first warp starts at Z0 - 1 >= np and its
+    // last warp ends at Z0 + 30 <= np + nz - 1; slab by when its rows lie in
+    // [np, np + nx - 1]
+    o.bx0 = (int)std::min<long long>(o.gx, (np + 1 + 30LL * W - 1) / (30LL * W));
+    o.bx1 = o.bx0;
+    while (o.bx1 < o.gx && 30LL * W * o.bx1 + 30LL * W <= np + nz - 1) ++o.bx1;
+    o.by0 = (int)std::min<long long>(o.gy, (np + TX - 1) / TX);
+    o.by1 = o.by0;
+    while (o.by1 < o.gy && (long long)TX * o.by1 + TX <= np + nx - 1) ++o.by1;
+    if (o.bx1 <= o.bx0 || o.by1 <= o.by0) {   // no rectangle: every slab in the ring
+        o.bx0 = o.bx1 = 0;
+        o.by0 = o.by1 = o.gy;
+    }
+    return o;
+}
+
 template <typename S, int W, int TX, int MINB>
 int launch_slabg_cfg(sm_eiso *h) {
-    const int wz = (h->NZ + 29) / 30;
-    dim3 grd((wz + W - 1) / W, (h->NX + TX - 1) / TX, (unsigned)h->nshots);
-    eiso_slabg_kernel<S, W, TX, MINB><<<grd, 32 * W, ESlabG<S, W, TX>::bytes, h->stream>>>(
-        h->args, h->slab_maps[h->cur]);
+    const SlabOrder o = slab_order(h, W, TX, false);
+    const unsigned n = (unsigned)(o.gx * o.gy) * (unsigned)h->nshots;
+    eiso_slabg_kernel<S, W, TX, MINB><<<n, 32 * W, ESlabG<S, W, TX>::bytes, h->stream>>>(
+        h->args, h->slab_maps[h->cur], o);
     return SM_OK;
 }
 
@@ -1930,10 +2008,10 @@ int ready_bslab_cfg(sm_eiso *h) {
 
 template <int W, int TX, int MINB>
 int launch_bslab_cfg(sm_eiso *h) {
-    const int wz = (h->NZ + 29) / 30;
-    dim3 grd((wz + W - 1) / W, (h->NX + TX - 1) / TX, (unsigned)h->nshots);
-    eiso_bslab_kernel<W, TX, MINB><<<grd, 32 * W, ESlabB<W, TX>::bytes, h->stream>>>(
-        h->args, h->bmaps[h->cur]);
+    const SlabOrder o = slab_order(h, W, TX, true);
+    const unsigned n = (unsigned)(o.gx * o.gy) * (unsigned)h->nshots;
+    eiso_bslab_kernel<W, TX, MINB><<<n, 32 * W, ESlabB<W, TX>::bytes, h->stream>>>(
+        h->args, h->bmaps[h->cur], o);
     return SM_OK;
 }
 
