@@ -271,7 +271,8 @@ __device__ __forceinline__ void a3d_step_body(const A3Args &a, const A3Maps &m, 
     const int i1 = min(i0 + a.chunk, a.nx2);
     const int nx2 = a.nx2, ny2 = a.ny2, nz2 = a.nz2, np = a.np, pitch = a.pitch;
     const int sx = a.sx, sy = a.sy;   // element strides (all indices fit 31 bits)
-    const bool kin = k < nz2;
+    // an interior tile lies inside the grid in y and z (checked above)
+    const bool kin = CLS == A3_INNER || k < nz2;
     const S *Pin = static_cast<const S *>(a.f[A_P]);
     const S *Vxin = static_cast<const S *>(a.f[A_VX]);
     S *Pout = static_cast<S *>(a.fo[A_P]);
@@ -346,7 +347,7 @@ __device__ __forceinline__ void a3d_step_body(const A3Args &a, const A3Maps &m, 
 #pragma unroll
     for (int r = 0; r < R; ++r) {
         const int j = j0 + w * R + r;
-        rin[r] = kin && j < ny2;
+        rin[r] = CLS == A3_INNER || (kin && j < ny2);
         jh[r] = j < ny2 ? half_slab(j, ny2, np) : -1;
         jn[r] = j < ny2 ? node_slab(j, ny2, np) : -1;
         joff[r] = j * sy + k;
@@ -357,7 +358,7 @@ __device__ __forceinline__ void a3d_step_body(const A3Args &a, const A3Maps &m, 
     const int jmh = (jm >= 0) ? half_slab(jm, ny2, np) : -1;
     const int hrow = lane;                         // halo-column row of warp HW's lane
     const bool hwarp = w == HW && lane < TY;
-    const bool hcol = hwarp && km >= 0 && j0 + hrow < ny2;
+    const bool hcol = hwarp && (CLS == A3_INNER || (km >= 0 && j0 + hrow < ny2));
     const int kmh = (km >= 0) ? half_slab(km, nz2, np) : -1;
     // Per-axis fast flags.  An axis is "fast" for a cell when neither its CPML
     // frame nor the grid edge touches it: the velocity component along the
@@ -496,7 +497,8 @@ __device__ __forceinline__ void a3d_step_body(const A3Args &a, const A3Maps &m, 
     for (int i = i0; i < i1; ++i) {
         const int l = i - i0;
         if (producer) issue(l + D - 2);
-        if (!mbar_wait(&bars[l % D], (l / D) & 1, a.err, 1)) return;
+        // plane l was waited for as the next plane of iteration l-1
+        if (l == 0 && !mbar_wait(&bars[0], 0, a.err, 1)) return;
         if (i + 1 < nx2 && !mbar_wait(&bars[(l + 1) % D], ((l + 1) / D) & 1, a.err, 1)) return;
         const unsigned char *cbuf = ring + (size_t)(l % D) * L::stage;
         const unsigned char *nbuf = ring + (size_t)((l + 1) % D) * L::stage;
@@ -571,7 +573,7 @@ __device__ __forceinline__ void a3d_step_body(const A3Args &a, const A3Maps &m, 
         // halo row: vy(i, j0-1, k), by warp 0
         if (w == 0) {
             C vyh = C(0);
-            if (jm >= 0 && kin) {
+            if (CLS == A3_INNER || (jm >= 0 && kin)) {
                 C psi_new;
                 vyh = a3_vel<C>(St::ld(cY + lane, isY), St::ld(cP + HS + lane, isP),
                                 St::ld(cP + WS + HS + lane, isP), cR[HC + lane], cR[WC + HC + lane],
@@ -733,7 +735,8 @@ __device__ __forceinline__ void a3d_bstep_body(const A3Args &a, const A3BMaps &m
     const int nx2 = a.nx2, ny2 = a.ny2, nz2 = a.nz2, np = a.np, pitch = a.pitch;
     const int sx = a.sx, sy = a.sy;
     const int ex = a.nyb * pitch;   // exponent bytes per x plane
-    const bool kin = k < nz2;
+    // an interior tile lies inside the grid in y and z (checked above)
+    const bool kin = CLS == A3_INNER || k < nz2;
     const int16_t *Pin = static_cast<const int16_t *>(a.f[A_P]);
     const int16_t *Vxin = static_cast<const int16_t *>(a.f[A_VX]);
     const uint8_t *EPin = static_cast<const uint8_t *>(a.fe[A_P]);
@@ -816,7 +819,7 @@ __device__ __forceinline__ void a3d_bstep_body(const A3Args &a, const A3BMaps &m
 #pragma unroll
     for (int r = 0; r < R; ++r) {
         const int j = j0 + w * R + r;
-        rin[r] = kin && j < ny2;
+        rin[r] = CLS == A3_INNER || (kin && j < ny2);
         jh[r] = j < ny2 ? half_slab(j, ny2, np) : -1;
         jn[r] = j < ny2 ? node_slab(j, ny2, np) : -1;
         joff[r] = j * sy + k;
@@ -998,7 +1001,8 @@ __device__ __forceinline__ void a3d_bstep_body(const A3Args &a, const A3BMaps &m
     for (int i = i0; i < i1; ++i) {
         const int l = i - i0;
         if (producer) issue(l + D - 2);
-        if (!mbar_wait(&bars[l % D], (l / D) & 1, a.err, 1)) return;
+        // plane l was waited for as the next plane of iteration l-1
+        if (l == 0 && !mbar_wait(&bars[0], 0, a.err, 1)) return;
         if (i + 1 < nx2 && !mbar_wait(&bars[(l + 1) % D], ((l + 1) / D) & 1, a.err, 1)) return;
         const unsigned char *cbuf = ring + (size_t)(l % D) * L::stage;
         const unsigned char *nbuf = ring + (size_t)((l + 1) % D) * L::stage;
@@ -1080,7 +1084,7 @@ __device__ __forceinline__ void a3d_bstep_body(const A3Args &a, const A3BMaps &m
         // halo row: vy(i, j0-1, k), by warp 0
         if (w == 0) {
             C vyh = C(0);
-            if (jm >= 0 && kin) {
+            if (CLS == A3_INNER || (jm >= 0 && kin)) {
                 C psi_new;
                 vyh = a3_vel<C>(bfp_val(cY[lane], bfp_dec(eY_(cbuf, 0))),
                                 bfp_val(mP(cbuf, 0, lane + 8), bfp_dec(eP_(cbuf, 0, lane + 16))),
@@ -1099,7 +1103,7 @@ __device__ __forceinline__ void a3d_bstep_body(const A3Args &a, const A3BMaps &m
                 const int hr = lane + 32 * h;
                 if (hr >= TY) continue;
                 C vzh = C(0);
-                if (km >= 0 && j0 + hr < ny2) {
+                if (CLS == A3_INNER || (km >= 0 && j0 + hr < ny2)) {
                     const int rc = (hr + 1) * WR + 4, hb = hr / R;
                     const BDec dP0 = bfp_dec(eP_(cbuf, hb + 1, 15));
                     const BDec dP1 = bfp_dec(eP_(cbuf, hb + 1, 16));
