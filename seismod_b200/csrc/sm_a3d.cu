@@ -228,7 +228,7 @@ __device__ __forceinline__ int a3_edge_tile(const A3Args &a, int e, int &kt, int
     return A3_FACE_GEN;
 }
 
-template <typename S, int W, int R, int D, int CLS, int FACE>
+template <typename S, int W, int R, int D, int CLS, int FACE, bool FULL = false>
 __device__ __forceinline__ void a3d_step_body(const A3Args &a, const A3Maps &m, int kt, int jt,
                                               int ch) {
     constexpr int TY = W * R;
@@ -271,8 +271,9 @@ __device__ __forceinline__ void a3d_step_body(const A3Args &a, const A3Maps &m, 
     const int i1 = min(i0 + a.chunk, a.nx2);
     const int nx2 = a.nx2, ny2 = a.ny2, nz2 = a.nz2, np = a.np, pitch = a.pitch;
     const int sx = a.sx, sy = a.sy;   // element strides (all indices fit 31 bits)
-    // an interior tile lies inside the grid in y and z (checked above)
-    const bool kin = CLS == A3_INNER || k < nz2;
+    // an interior tile, and a FULL one, lies inside the grid in y and z
+    constexpr bool INSIDE = CLS == A3_INNER || FULL;
+    const bool kin = INSIDE || k < nz2;
     const S *Pin = static_cast<const S *>(a.f[A_P]);
     const S *Vxin = static_cast<const S *>(a.f[A_VX]);
     S *Pout = static_cast<S *>(a.fo[A_P]);
@@ -347,7 +348,7 @@ __device__ __forceinline__ void a3d_step_body(const A3Args &a, const A3Maps &m, 
 #pragma unroll
     for (int r = 0; r < R; ++r) {
         const int j = j0 + w * R + r;
-        rin[r] = CLS == A3_INNER || (kin && j < ny2);
+        rin[r] = INSIDE || (kin && j < ny2);
         jh[r] = j < ny2 ? half_slab(j, ny2, np) : -1;
         jn[r] = j < ny2 ? node_slab(j, ny2, np) : -1;
         joff[r] = j * sy + k;
@@ -358,7 +359,7 @@ __device__ __forceinline__ void a3d_step_body(const A3Args &a, const A3Maps &m, 
     const int jmh = (jm >= 0) ? half_slab(jm, ny2, np) : -1;
     const int hrow = lane;                         // halo-column row of warp HW's lane
     const bool hwarp = w == HW && lane < TY;
-    const bool hcol = hwarp && (CLS == A3_INNER || (km >= 0 && j0 + hrow < ny2));
+    const bool hcol = hwarp && km >= 0 && (INSIDE || j0 + hrow < ny2);
     const int kmh = (km >= 0) ? half_slab(km, nz2, np) : -1;
     // Per-axis fast flags.  An axis is "fast" for a cell when neither its CPML
     // frame nor the grid edge touches it: the velocity component along the
@@ -638,7 +639,10 @@ __global__ void __launch_bounds__(32 * W, MINB)
     else if (face == A3_FACE_Y) a3d_step_body<S, W, R, D, CLS, A3_FACE_Y>(a, m, kt, jt, blockIdx.z);
     else
 #endif
-    a3d_step_body<S, W, R, D, CLS, A3_FACE_GEN>(a, m, kt, jt, blockIdx.z);
+    if (kt * 32 + 31 < a.nz2 && (jt + 1) * W * R <= a.ny2)
+        a3d_step_body<S, W, R, D, CLS, A3_FACE_GEN, true>(a, m, kt, jt, blockIdx.z);
+    else
+        a3d_step_body<S, W, R, D, CLS, A3_FACE_GEN, false>(a, m, kt, jt, blockIdx.z);
     (void)face;
 }
 
@@ -694,7 +698,7 @@ struct A3BMaps {
     CUtensorMap P, eP, vx, eX, vy, eY, vz, eZ, rho, K;
 };
 
-template <int W, int D, int CLS, int FACE>
+template <int W, int D, int CLS, int FACE, bool FULL = false>
 __device__ __forceinline__ void a3d_bstep_body(const A3Args &a, const A3BMaps &m, int kt, int jt,
                                                int ch) {
     constexpr int R = A3_BJ, TY = W * R;
@@ -735,8 +739,9 @@ __device__ __forceinline__ void a3d_bstep_body(const A3Args &a, const A3BMaps &m
     const int nx2 = a.nx2, ny2 = a.ny2, nz2 = a.nz2, np = a.np, pitch = a.pitch;
     const int sx = a.sx, sy = a.sy;
     const int ex = a.nyb * pitch;   // exponent bytes per x plane
-    // an interior tile lies inside the grid in y and z (checked above)
-    const bool kin = CLS == A3_INNER || k < nz2;
+    // an interior tile, and a FULL one, lies inside the grid in y and z
+    constexpr bool INSIDE = CLS == A3_INNER || FULL;
+    const bool kin = INSIDE || k < nz2;
     const int16_t *Pin = static_cast<const int16_t *>(a.f[A_P]);
     const int16_t *Vxin = static_cast<const int16_t *>(a.f[A_VX]);
     const uint8_t *EPin = static_cast<const uint8_t *>(a.fe[A_P]);
@@ -819,7 +824,7 @@ __device__ __forceinline__ void a3d_bstep_body(const A3Args &a, const A3BMaps &m
 #pragma unroll
     for (int r = 0; r < R; ++r) {
         const int j = j0 + w * R + r;
-        rin[r] = CLS == A3_INNER || (kin && j < ny2);
+        rin[r] = INSIDE || (kin && j < ny2);
         jh[r] = j < ny2 ? half_slab(j, ny2, np) : -1;
         jn[r] = j < ny2 ? node_slab(j, ny2, np) : -1;
         joff[r] = j * sy + k;
@@ -1103,7 +1108,7 @@ __device__ __forceinline__ void a3d_bstep_body(const A3Args &a, const A3BMaps &m
                 const int hr = lane + 32 * h;
                 if (hr >= TY) continue;
                 C vzh = C(0);
-                if (CLS == A3_INNER || (km >= 0 && j0 + hr < ny2)) {
+                if (km >= 0 && (INSIDE || j0 + hr < ny2)) {
                     const int rc = (hr + 1) * WR + 4, hb = hr / R;
                     const BDec dP0 = bfp_dec(eP_(cbuf, hb + 1, 15));
                     const BDec dP1 = bfp_dec(eP_(cbuf, hb + 1, 16));
@@ -1156,7 +1161,10 @@ __global__ void __launch_bounds__(32 * W, MINB)
     else if (face == A3_FACE_Y) a3d_bstep_body<W, D, CLS, A3_FACE_Y>(a, m, kt, jt, blockIdx.z);
     else
 #endif
-    a3d_bstep_body<W, D, CLS, A3_FACE_GEN>(a, m, kt, jt, blockIdx.z);
+    if (kt * 32 + 31 < a.nz2 && (jt + 1) * W * A3_BJ <= a.ny2)
+        a3d_bstep_body<W, D, CLS, A3_FACE_GEN, true>(a, m, kt, jt, blockIdx.z);
+    else
+        a3d_bstep_body<W, D, CLS, A3_FACE_GEN, false>(a, m, kt, jt, blockIdx.z);
     (void)face;
 }
 
