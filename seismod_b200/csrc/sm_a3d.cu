@@ -339,8 +339,11 @@ __device__ __forceinline__ void a3d_step_body(const A3Args &a, const A3Maps &m, 
         tma_load_3d(b + L::oK, &m.K, k0, j0, ip, bar);
     };
     __syncthreads();   // barriers initialised, tables filled
+    // the pressure of plane ip reads P and K of its plane from registers
+    // (kept by the velocity pass of plane ip), so the stage of plane l-1 is
+    // free in iteration l: the ring runs D-1 planes ahead
     if (producer)
-        for (int l = 0; l < D - 2; ++l) issue(l);
+        for (int l = 0; l < D - 1; ++l) issue(l);
 
     // per-row / per-column frame membership (fixed over the march)
     int jh[R], jn[R], joff[R];
@@ -426,9 +429,11 @@ __device__ __forceinline__ void a3d_step_body(const A3Args &a, const A3Maps &m, 
     };
 
     // per-thread state carried between planes, one entry per row
-    C vxa[R], vxb[R], vzp[R];
+    C vxa[R], vxb[R], vzp[R], pkp[R], kkp[R];   // ... and P, K of the previous plane
 #pragma unroll
-    for (int r = 0; r < R; ++r) { vxa[r] = C(0); vxb[r] = C(0); vzp[r] = C(0); }
+    for (int r = 0; r < R; ++r) {
+        vxa[r] = C(0); vxb[r] = C(0); vzp[r] = C(0); pkp[r] = C(0); kkp[r] = C(0);
+    }
     // vx(i0-1) (direct loads, once per CTA): the pressure of plane i0 needs it
     if (i0 >= 1) {
         const int s = half_slab(i0 - 1, nx2, np);
@@ -446,13 +451,10 @@ __device__ __forceinline__ void a3d_step_body(const A3Args &a, const A3Maps &m, 
     load_vpsi(i0);
 
     // ---- the lagged pressure half step of plane ip (a_iso_3d.c:659-683) ----
-    auto pressure = [&](int ip, int lp, auto AFt) {
+    auto pressure = [&](int ip, auto AFt) {
         constexpr bool AF = decltype(AFt)::value;
         const bool fx = AF || (ip >= lo && ip <= nx2 - 1 - np);
         const bool fy = AF || yfast, fz = AF || zfast;
-        const unsigned char *pb = ring + (size_t)(lp % D) * L::stage;
-        const S *pP = reinterpret_cast<const S *>(pb + L::oP);
-        const C *pK = reinterpret_cast<const C *>(pb + L::oK);
         const C(*vy)[32] = VYs[ip & 1];
         const int sxn = fx ? -1 : node_slab(ip, nx2, np);
         const int e = ip - (i0 - 1);
@@ -463,7 +465,7 @@ __device__ __forceinline__ void a3d_step_body(const A3Args &a, const A3Maps &m, 
             C vzm = __shfl_up_sync(0xffffffffu, vzp[r], 1);
             if (lane == 0) vzm = VZH[ip & 1][row];
             if (!rin[r]) continue;
-            const C p_c = St::ld(pP + (row + 1) * WS + HS + lane, isP);
+            const C p_c = pkp[r];
             C pn = p_c;
             // the reference leaves index 0 of every axis untouched
             bool upd = true;
@@ -487,7 +489,7 @@ __device__ __forceinline__ void a3d_step_body(const A3Args &a, const A3Maps &m, 
                     gz = a3_dv<C>(gz, CZ[3][lane + 1], CZ[4][lane + 1], CZ[5][lane + 1], fVz[r], psi_new);
                     St::st(poVz + (ip * ny2 + j) * 2 * np + kn, psi_new, a.psc[PS_VZ]);
                 }
-                pn = r_fma(-pK[row * 32 + lane], r_add(r_add(gx, gy), gz), p_c);
+                pn = r_fma(-kkp[r], r_add(r_add(gx, gy), gz), p_c);
             }
             // written whether updated or not: both buffers always hold a
             // complete state
@@ -497,7 +499,7 @@ __device__ __forceinline__ void a3d_step_body(const A3Args &a, const A3Maps &m, 
 
     for (int i = i0; i < i1; ++i) {
         const int l = i - i0;
-        if (producer) issue(l + D - 2);
+        if (producer) issue(l + D - 1);
         // plane l was waited for as the next plane of iteration l-1
         if (l == 0 && !mbar_wait(&bars[0], 0, a.err, 1)) return;
         if (i + 1 < nx2 && !mbar_wait(&bars[(l + 1) % D], ((l + 1) / D) & 1, a.err, 1)) return;
@@ -510,6 +512,7 @@ __device__ __forceinline__ void a3d_step_body(const A3Args &a, const A3Maps &m, 
         const S *cZ = reinterpret_cast<const S *>(cbuf + L::oZ);
         const S *nP = reinterpret_cast<const S *>(nbuf + L::oP);
         const C *nR = reinterpret_cast<const C *>(nbuf + L::oR);
+        const C *cK = reinterpret_cast<const C *>(cbuf + L::oK);
         C(*vyw)[32] = VYs[i & 1];
         const bool xf = i >= np && i <= nx2 - 2 - np;
         const int sxh = (i < nx2 - 1) ? half_slab(i, nx2, np) : -1;
@@ -520,7 +523,7 @@ __device__ __forceinline__ void a3d_step_body(const A3Args &a, const A3Maps &m, 
         // A component on a fast axis is updated even in cells outside the
         // grid (from the zero fill): such values are neither stored nor
         // read by a cell inside the grid.
-        C vxn[R], vzn[R];
+        C vxn[R], vzn[R], pkn[R], kkn[R];
         auto velocity = [&](auto AFt) {
         constexpr bool AF = decltype(AFt)::value;
         const bool fx = AF || xf, fy = AF || yfast, fz = AF || zfast;
@@ -562,6 +565,8 @@ __device__ __forceinline__ void a3d_step_body(const A3Args &a, const A3Maps &m, 
             vyw[row + 1][lane] = vy;
             vxn[r] = vx;
             vzn[r] = vz;
+            pkn[r] = p_c;
+            kkn[r] = cK[row * 32 + lane];
             if (rin[r]) {
                 St::st(ox + joff[r], vx, a.sc[A_VX]);
                 St::st(oy + joff[r], vy, a.sc[A_VY]);
@@ -600,8 +605,8 @@ __device__ __forceinline__ void a3d_step_body(const A3Args &a, const A3Maps &m, 
         // the pressure of the previous plane (its velocities are complete)
         if (i > i0) {
             const int ip = i - 1;
-            if (CLS == A3_INNER && ip >= lo && ip <= nx2 - 1 - np) pressure(ip, l - 1, BoolT<true>{});
-            else pressure(ip, l - 1, BoolT<false>{});
+            if (CLS == A3_INNER && ip >= lo && ip <= nx2 - 1 - np) pressure(ip, BoolT<true>{});
+            else pressure(ip, BoolT<false>{});
         }
         load_ppsi(i);
 #pragma unroll
@@ -609,14 +614,16 @@ __device__ __forceinline__ void a3d_step_body(const A3Args &a, const A3Maps &m, 
             vxb[r] = vxa[r];
             vxa[r] = vxn[r];
             vzp[r] = vzn[r];
+            pkp[r] = pkn[r];
+            kkp[r] = kkn[r];
         }
         __syncthreads();   // vy rows and halo column of plane i visible; the oldest stage may be refilled
     }
     // the last plane's pressure
     if (i1 > i0) {
         const int ip = i1 - 1;
-        if (CLS == A3_INNER && ip >= lo && ip <= nx2 - 1 - np) pressure(ip, ip - i0, BoolT<true>{});
-        else pressure(ip, ip - i0, BoolT<false>{});
+        if (CLS == A3_INNER && ip >= lo && ip <= nx2 - 1 - np) pressure(ip, BoolT<true>{});
+        else pressure(ip, BoolT<false>{});
     }
 }
 
@@ -634,12 +641,15 @@ __global__ void __launch_bounds__(32 * W, MINB)
     }
     int kt, jt;
     const int face = a3_edge_tile(a, blockIdx.x, kt, jt);
+    const bool full = kt * 32 + 31 < a.nz2 && (jt + 1) * W * R <= a.ny2;
 #if SM_A3D_FACE_BODIES
-    if (face == A3_FACE_Z) a3d_step_body<S, W, R, D, CLS, A3_FACE_Z>(a, m, kt, jt, blockIdx.z);
-    else if (face == A3_FACE_Y) a3d_step_body<S, W, R, D, CLS, A3_FACE_Y>(a, m, kt, jt, blockIdx.z);
+    if (full && face == A3_FACE_Z)
+        a3d_step_body<S, W, R, D, CLS, A3_FACE_Z, true>(a, m, kt, jt, blockIdx.z);
+    else if (full && face == A3_FACE_Y)
+        a3d_step_body<S, W, R, D, CLS, A3_FACE_Y, true>(a, m, kt, jt, blockIdx.z);
     else
 #endif
-    if (kt * 32 + 31 < a.nz2 && (jt + 1) * W * R <= a.ny2)
+    if (full)
         a3d_step_body<S, W, R, D, CLS, A3_FACE_GEN, true>(a, m, kt, jt, blockIdx.z);
     else
         a3d_step_body<S, W, R, D, CLS, A3_FACE_GEN, false>(a, m, kt, jt, blockIdx.z);
@@ -815,8 +825,10 @@ __device__ __forceinline__ void a3d_bstep_body(const A3Args &a, const A3BMaps &m
         tma_load_3d(b + L::oK, &m.K, k0, j0, ip, bar);
     };
     __syncthreads();   // barriers initialised, tables filled
+    // the pressure of plane ip takes P and K of its plane from registers,
+    // so the stage of plane l-1 is free in iteration l: D-1 planes ahead
     if (producer)
-        for (int l = 0; l < D - 2; ++l) issue(l);
+        for (int l = 0; l < D - 1; ++l) issue(l);
 
     // rows of this thread: one block, rows j0 + w*R + r
     int jh[R], jn[R], joff[R];
@@ -907,9 +919,10 @@ __device__ __forceinline__ void a3d_bstep_body(const A3Args &a, const A3BMaps &m
 
     C vxa[R], vxb[R], vzp[R];
     C pc[R], pp[R];   // decoded P of plane i (own cells) and of plane i-1
+    C kkp[R];         // K of plane i-1
 #pragma unroll
     for (int r = 0; r < R; ++r) {
-        vxa[r] = C(0); vxb[r] = C(0); vzp[r] = C(0); pc[r] = C(0); pp[r] = C(0);
+        vxa[r] = C(0); vxb[r] = C(0); vzp[r] = C(0); pc[r] = C(0); pp[r] = C(0); kkp[r] = C(0);
     }
     // vx(i0-1) (direct loads, once per CTA): the pressure of plane i0 needs it
     if (i0 >= 1 && bin) {
@@ -956,12 +969,10 @@ __device__ __forceinline__ void a3d_bstep_body(const A3Args &a, const A3BMaps &m
     };
 
     // ---- the lagged pressure half step of plane ip (a_iso_3d.c:659-683) ----
-    auto pressure = [&](int ip, int lp, auto AFt) {
+    auto pressure = [&](int ip, auto AFt) {
         constexpr bool AF = decltype(AFt)::value;
         const bool fx = AF || (ip >= lo && ip <= nx2 - 1 - np);
         const bool fy = AF || yfast, fz = AF || zfast;
-        const unsigned char *pb = ring + (size_t)(lp % D) * L::stage;
-        const C *pK = reinterpret_cast<const C *>(pb + L::oK);
         const C(*vy)[32] = VYs[ip & 1];
         const int sxn = fx ? -1 : node_slab(ip, nx2, np);
         const int e = ip - (i0 - 1);
@@ -995,7 +1006,7 @@ __device__ __forceinline__ void a3d_bstep_body(const A3Args &a, const A3BMaps &m
                     gz = a3_dv<C>(gz, CZ[3][lane + 1], CZ[4][lane + 1], CZ[5][lane + 1], fVz[r], psi_new);
                     poVz[(ip * ny2 + j) * 2 * np + kn] = psi_new;
                 }
-                pn[r] = r_fma(-pK[row * 32 + lane], r_add(r_add(gx, gy), gz), p_c);
+                pn[r] = r_fma(-kkp[r], r_add(r_add(gx, gy), gz), p_c);
             }
         }
         // written whether updated or not: both buffers always hold a
@@ -1005,7 +1016,7 @@ __device__ __forceinline__ void a3d_bstep_body(const A3Args &a, const A3BMaps &m
 
     for (int i = i0; i < i1; ++i) {
         const int l = i - i0;
-        if (producer) issue(l + D - 2);
+        if (producer) issue(l + D - 1);
         // plane l was waited for as the next plane of iteration l-1
         if (l == 0 && !mbar_wait(&bars[0], 0, a.err, 1)) return;
         if (i + 1 < nx2 && !mbar_wait(&bars[(l + 1) % D], ((l + 1) / D) & 1, a.err, 1)) return;
@@ -1013,6 +1024,7 @@ __device__ __forceinline__ void a3d_bstep_body(const A3Args &a, const A3BMaps &m
         const unsigned char *nbuf = ring + (size_t)((l + 1) % D) * L::stage;
         const C *cR = reinterpret_cast<const C *>(cbuf + L::oR);
         const C *nR = reinterpret_cast<const C *>(nbuf + L::oR);
+        const C *cK = reinterpret_cast<const C *>(cbuf + L::oK);
         const int16_t *cX = reinterpret_cast<const int16_t *>(cbuf + L::oX);
         const int16_t *cY = reinterpret_cast<const int16_t *>(cbuf + L::oY);
         const int16_t *cZ = reinterpret_cast<const int16_t *>(cbuf + L::oZ);
@@ -1124,8 +1136,8 @@ __device__ __forceinline__ void a3d_bstep_body(const A3Args &a, const A3BMaps &m
         if (i + 1 < i1) load_vpsi(i + 1);
         if (i > i0) {
             const int ip = i - 1;
-            if (CLS == A3_INNER && ip >= lo && ip <= nx2 - 1 - np) pressure(ip, l - 1, BoolT<true>{});
-            else pressure(ip, l - 1, BoolT<false>{});
+            if (CLS == A3_INNER && ip >= lo && ip <= nx2 - 1 - np) pressure(ip, BoolT<true>{});
+            else pressure(ip, BoolT<false>{});
         }
         load_ppsi(i);
 #pragma unroll
@@ -1135,13 +1147,14 @@ __device__ __forceinline__ void a3d_bstep_body(const A3Args &a, const A3BMaps &m
             vzp[r] = vzn[r];
             pp[r] = pc[r];
             pc[r] = pnx[r];
+            kkp[r] = cK[(w * R + r) * 32 + lane];
         }
         __syncthreads();
     }
     if (i1 > i0) {
         const int ip = i1 - 1;
-        if (CLS == A3_INNER && ip >= lo && ip <= nx2 - 1 - np) pressure(ip, ip - i0, BoolT<true>{});
-        else pressure(ip, ip - i0, BoolT<false>{});
+        if (CLS == A3_INNER && ip >= lo && ip <= nx2 - 1 - np) pressure(ip, BoolT<true>{});
+        else pressure(ip, BoolT<false>{});
     }
 }
 
@@ -1156,12 +1169,15 @@ __global__ void __launch_bounds__(32 * W, MINB)
     }
     int kt, jt;
     const int face = a3_edge_tile(a, blockIdx.x, kt, jt);
+    const bool full = kt * 32 + 31 < a.nz2 && (jt + 1) * W * A3_BJ <= a.ny2;
 #if SM_A3D_FACE_BODIES
-    if (face == A3_FACE_Z) a3d_bstep_body<W, D, CLS, A3_FACE_Z>(a, m, kt, jt, blockIdx.z);
-    else if (face == A3_FACE_Y) a3d_bstep_body<W, D, CLS, A3_FACE_Y>(a, m, kt, jt, blockIdx.z);
+    if (full && face == A3_FACE_Z)
+        a3d_bstep_body<W, D, CLS, A3_FACE_Z, true>(a, m, kt, jt, blockIdx.z);
+    else if (full && face == A3_FACE_Y)
+        a3d_bstep_body<W, D, CLS, A3_FACE_Y, true>(a, m, kt, jt, blockIdx.z);
     else
 #endif
-    if (kt * 32 + 31 < a.nz2 && (jt + 1) * W * A3_BJ <= a.ny2)
+    if (full)
         a3d_bstep_body<W, D, CLS, A3_FACE_GEN, true>(a, m, kt, jt, blockIdx.z);
     else
         a3d_bstep_body<W, D, CLS, A3_FACE_GEN, false>(a, m, kt, jt, blockIdx.z);
