@@ -951,6 +951,7 @@ __device__ __forceinline__ void a3d_bstep_body(const A3Args &a, const A3BMaps &m
 
     // encode and store one block (rows of this thread) of a field at plane
     // ip: mantissas where the row is in the grid, the exponent once
+    bool overflow = false;   // a block beyond the format's range (reported once, at the end)
     auto store_block = [&](int16_t *out, uint8_t *eout, int ip, const C *v) {
         unsigned mx = 0;
 #pragma unroll
@@ -962,10 +963,8 @@ __device__ __forceinline__ void a3d_bstep_body(const A3Args &a, const A3BMaps &m
 #pragma unroll
         for (int r = 0; r < R; ++r)
             if (rin[r]) o[joff[r]] = bfp_man(v[r], esc);
-        if (bin) {
-            eout[ip * ex + eoff] = (uint8_t)e8;
-            if (over) atomicExch(a.err, 4);
-        }
+        if (bin) eout[ip * ex + eoff] = (uint8_t)e8;
+        overflow = overflow || (bin && over);
     };
 
     // ---- the lagged pressure half step of plane ip (a_iso_3d.c:659-683) ----
@@ -1156,6 +1155,7 @@ __device__ __forceinline__ void a3d_bstep_body(const A3Args &a, const A3BMaps &m
         if (CLS == A3_INNER && ip >= lo && ip <= nx2 - 1 - np) pressure(ip, BoolT<true>{});
         else pressure(ip, BoolT<false>{});
     }
+    if (overflow) atomicExch(a.err, 4);
 }
 
 template <int W, int D, int MINB, int CLS>
