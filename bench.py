@@ -226,6 +226,7 @@ def trace_err(a, b):
 
 TUNE = True
 GRAPH = 16
+LAUNCH = {}   # (workload kind, precision) -> the autotuner's launch configuration
 
 
 def device_for(kind, p, precision, dev_id, shots=None):
@@ -237,7 +238,7 @@ def device_for(kind, p, precision, dev_id, shots=None):
     else:
         dev, n = api.eiso_device(p, precision, shots, dev_id)
     if TUNE:
-        dev.autotune()
+        LAUNCH[(kind, precision)] = dev.autotune()[:-1]
     if GRAPH:
         dev.set_graph(GRAPH)
     return dev, n
@@ -303,7 +304,8 @@ def run_ours(args, rank, world, local_rank, torch, dist):
         "config": {"workload": desc, "precision": f"{prec} storage",
                    "cells_per_shot": p.cells, "shots": nshots * world,
                    "parallelism": f"replicas x{world} (shot-parallel, no collective)",
-                   "l2": "inputs larger than L2 (state %.0f MB)" % (bps / 1e6)},
+                   "l2": "inputs larger than L2 (state %.0f MB)" % (bps / 1e6),
+                   "launch": {"autotuned": TUNE, "config_chunk": LAUNCH.get((kind, prec))}},
         "shots_per_s": round(nshots * world / (ms / K * 1e-3 * nsteps_shot), 3),
         "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": hbm,
                      "unit": "GB/s", "frac": round(achieved / hbm, 4),
