@@ -276,6 +276,10 @@ def run_ours(args, rank, world, local_rank, torch, dist):
     dev, nsteps_shot = device_for(kind, p, prec, local_rank)
     K, Wm = args.steps, args.warmup
     dev.run(Wm)
+    # one more untimed graph's worth of steps: the time loop's CUDA graph is
+    # captured here (a one-off cost of the handle, like the autotuning)
+    if GRAPH and kind != "ecyl":
+        dev.run(GRAPH)
     dev.sync()
     dev.kernel_stats(reset=True)
     if world > 1:
@@ -305,7 +309,9 @@ def run_ours(args, rank, world, local_rank, torch, dist):
                    "cells_per_shot": p.cells, "shots": nshots * world,
                    "parallelism": f"replicas x{world} (shot-parallel, no collective)",
                    "l2": "inputs larger than L2 (state %.0f MB)" % (bps / 1e6),
-                   "launch": {"autotuned": TUNE, "config_chunk": LAUNCH.get((kind, prec))}},
+                   "launch": {"autotuned": TUNE, "config_chunk": LAUNCH.get((kind, prec)),
+                              "graph_steps": GRAPH if kind != "ecyl" else 0,
+                              "untimed_graph_capture_steps": GRAPH if kind != "ecyl" else 0}},
         "shots_per_s": round(nshots * world / (ms / K * 1e-3 * nsteps_shot), 3),
         "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": hbm,
                      "unit": "GB/s", "frac": round(achieved / hbm, 4),
@@ -349,7 +355,7 @@ def timed_rate(kind, p, prec, dev_id, steps, shots=None):
     per-launch events around the step kernel."""
     import torch
     dev, _ = device_for(kind, p, prec, dev_id, shots)
-    dev.run(5)
+    dev.run(5 + GRAPH)   # warm-up, and the time loop's CUDA graph captured
     dev.sync()
     ms = time_steps(dev, steps, torch) / steps
     dev.set_timing(True)

@@ -2318,7 +2318,9 @@ int a3d_run_t(sm_a3d *h, size_t nsteps) {
     const size_t per_step =
         (size_t)a3d_step_kernels(h) + (h->src.empty() ? 0 : 1) + (h->rec.empty() ? 0 : 1);
     while (nsteps > 0) {
-        if (G && !h->timer.on && h->it % G == 0 && nsteps >= G) {
+        // graphs start anywhere, except in 16-bit storage, whose range
+        // checks fall on multiples of the scale period between graphs
+        if (G && !h->timer.on && nsteps >= G && (!a3d_is16(h) || h->it % G == 0)) {
             cudaGraphExec_t ex = nullptr;
             if (int rc = a3d_graph<S>(h, &ex)) return rc;
             SM_CUDA_TRY(cudaGraphLaunch(ex, h->stream));

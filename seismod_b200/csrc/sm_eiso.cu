@@ -691,12 +691,9 @@ __device__ __forceinline__ void slab_of(const SlabOrder &o, int nshots, int b, i
 
 template <typename S, int W, int TX, int MINB>
 __global__ void __launch_bounds__(32 * W, MINB) eiso_slabg_kernel(const EisoArgs a,
-                                                                  const __grid_constant__ EisoSlabMaps mp,
-                                                                  const SlabOrder o) {
+                                                                  const __grid_constant__ EisoSlabMaps mp) {
     extern __shared__ __align__(128) unsigned char smem[];
-    int bx, by, shot;
-    slab_of(o, a.nshots, blockIdx.x, bx, by, shot);
-    eiso_slabg_body<S, W, TX>(a, &mp.f, bx, by, shot, smem);
+    eiso_slabg_body<S, W, TX>(a, &mp.f, blockIdx.x, blockIdx.y, blockIdx.z, smem);
 }
 
 // Persistent form of the slab step: a CTA per SM slot walks the slabs
@@ -1938,7 +1935,7 @@ int ready_slabg_cfg(sm_eiso *h) {
 // rectangle first, or (lean_first false) every shot's slabs in grid order.
 // Measured on the 64-shot 1040 x 540 batch: block storage 0.514 against
 // 0.553 ms per step with the rectangle first; FP32 0.440 against 0.415, so
-// FP32 keeps the grid order.
+// the FP32 slab step keeps its 3-D grid in grid order.
 SlabOrder slab_order(const sm_eiso *h, int W, int TX, bool lean_first) {
     const int wz = (int)((h->NZ + 29) / 30);
     SlabOrder o{(wz + W - 1) / W, (int)((h->NX + TX - 1) / TX), 0, 0, 0, 0};
@@ -1963,10 +1960,10 @@ SlabOrder slab_order(const sm_eiso *h, int W, int TX, bool lean_first) {
 
 template <typename S, int W, int TX, int MINB>
 int launch_slabg_cfg(sm_eiso *h) {
-    const SlabOrder o = slab_order(h, W, TX, false);
-    const unsigned n = (unsigned)(o.gx * o.gy) * (unsigned)h->nshots;
-    eiso_slabg_kernel<S, W, TX, MINB><<<n, 32 * W, ESlabG<S, W, TX>::bytes, h->stream>>>(
-        h->args, h->slab_maps[h->cur], o);
+    const int wz = (h->NZ + 29) / 30;
+    dim3 grd((wz + W - 1) / W, (h->NX + TX - 1) / TX, (unsigned)h->nshots);
+    eiso_slabg_kernel<S, W, TX, MINB><<<grd, 32 * W, ESlabG<S, W, TX>::bytes, h->stream>>>(
+        h->args, h->slab_maps[h->cur]);
     return SM_OK;
 }
 
@@ -2874,7 +2871,9 @@ int eiso_run_t(sm_eiso *h, size_t nsteps) {
     const size_t G = (size_t)h->graph_steps;
     const size_t per_step = 1 + (h->d_src.bytes ? 1 : 0) + (h->n_rec_total ? 1 : 0);
     while (nsteps > 0) {
-        if (G && !h->timer.on && h->it % G == 0 && nsteps >= G) {
+        // graphs start anywhere, except in 16-bit storage, whose range
+        // checks fall on multiples of the scale period between graphs
+        if (G && !h->timer.on && nsteps >= G && (!eiso_is16(h) || h->it % G == 0)) {
             cudaGraphExec_t ex = nullptr;
             if (int rc = eiso_graph<S>(h, &ex)) return rc;
             SM_CUDA_TRY(cudaGraphLaunch(ex, h->stream));
