@@ -2902,7 +2902,8 @@ extern "C" int sm_a3d_stream(sm_a3d_t h, void **stream) {
 
 extern "C" int sm_a3d_set_timing(sm_a3d_t h, int on) {
     if (int rc = a3d_check(h)) return rc;
-    h->timer.on = on != 0;
+    DeviceGuard g(h->device);
+    h->timer.set(on != 0);
     return SM_OK;
 }
 

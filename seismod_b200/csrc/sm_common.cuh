@@ -276,6 +276,17 @@ struct KernelTimer {
         cudaEventCreate(&e);
         return e;
     }
+    // switch per-launch timing on or off; on: events for n timed launches are
+    // created up front, so no event creation falls inside a timed pass
+    void set(bool v, size_t n = 512) {
+        on = v;
+        if (!v) return;
+        while (pool.size() < 2 * n) {
+            cudaEvent_t e = nullptr;
+            if (cudaEventCreate(&e) != cudaSuccess) break;
+            pool.push_back(e);
+        }
+    }
     cudaEvent_t begin(cudaStream_t s) {
         if (!on) return nullptr;
         cudaEvent_t a = get();

@@ -850,7 +850,8 @@ extern "C" int sm_ecyl_stream(sm_ecyl_t h, void **stream) {
 
 extern "C" int sm_ecyl_set_timing(sm_ecyl_t h, int on) {
     if (int rc = ecyl_check(h)) return rc;
-    h->timer.on = on != 0;
+    DeviceGuard g(h->device);
+    h->timer.set(on != 0);
     return SM_OK;
 }
 

@@ -3527,7 +3527,8 @@ extern "C" int sm_eiso_get_config(sm_eiso_t h, int *config, int *nconfigs) {
 
 extern "C" int sm_eiso_set_timing(sm_eiso_t h, int on) {
     if (int rc = eiso_check(h)) return rc;
-    h->timer.on = on != 0;
+    DeviceGuard g(h->device);
+    h->timer.set(on != 0);
     return SM_OK;
 }
 
