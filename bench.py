@@ -239,10 +239,10 @@ def device_for(kind, p, precision, dev_id, shots=None):
         dev, n = api.a3d_device(p, precision, dev_id)
     else:
         dev, n = api.eiso_device(p, precision, shots, dev_id)
+    if GRAPH:
+        dev.set_graph(GRAPH)   # before the tuning, so its trials run as the steps will
     if TUNE:
         LAUNCH[(kind, precision)] = dev.autotune()[:-1]
-    if GRAPH:
-        dev.set_graph(GRAPH)
     return dev, n
 
 

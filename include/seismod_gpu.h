@@ -227,10 +227,11 @@ int sm_eiso_stream(sm_eiso_t h, void **stream);
 int sm_eiso_set_config(sm_eiso_t h, int config);
 int sm_eiso_get_config(sm_eiso_t h, int *config, int *nconfigs);
 /* Autotuner: times every launch configuration that fits for trial_steps
- * steps (<= 0: 20) from a zero state and keeps the fastest; results are
- * cached per (precision, grid, shots, device) for the process.  Call at step
- * 0 (or after sm_eiso_reset); the handle is left reset.  Any output pointer
- * may be NULL. */
+ * steps (<= 0: 32) from a zero state and keeps the fastest; with graphs set
+ * (sm_eiso_set_graph) the trials replay them, their capture untimed.
+ * Results are cached per (precision, grid, shots, device) for the process.
+ * Call at step 0 (or after sm_eiso_reset); the handle is left reset.  Any
+ * output pointer may be NULL. */
 int sm_eiso_autotune(sm_eiso_t h, int trial_steps, int *config, double *ms_per_step);
 /* Replay the time loop as CUDA graphs of `steps` steps (2, 4, 8 or 16; 0
  * launches every kernel from the host, the default).  Results are the same
@@ -296,7 +297,7 @@ int sm_a3d_set_config(sm_a3d_t h, int config);
 /* x planes each CTA marches through (<= 0: the library's choice) */
 int sm_a3d_set_chunk(sm_a3d_t h, int chunk);
 int sm_a3d_get_config(sm_a3d_t h, int *config, int *nconfigs);
-/* autotuner (over configurations and x-chunk lengths; trial_steps <= 0: 10)
+/* autotuner (over configurations and x-chunk lengths; trial_steps <= 0: 32)
  * and CUDA-graph replay, as sm_eiso_autotune / sm_eiso_set_graph */
 int sm_a3d_autotune(sm_a3d_t h, int trial_steps, int *config, int *chunk, double *ms_per_step);
 int sm_a3d_set_graph(sm_a3d_t h, int steps);

@@ -189,7 +189,7 @@ class EIsoDevice:
     def set_config(self, config):
         L.check(L.load().sm_eiso_set_config(self._h, int(config)))
 
-    def autotune(self, trial_steps=20):
+    def autotune(self, trial_steps=32):
         """Pick the fastest launch configuration (the handle is left reset).
         Returns (config, ms per step)."""
         c, ms = C.c_int(), C.c_double()
@@ -294,9 +294,10 @@ class A3DDevice:
     def set_chunk(self, chunk):
         L.check(L.load().sm_a3d_set_chunk(self._h, int(chunk)))
 
-    def autotune(self, trial_steps=10):
-        """Pick the fastest launch configuration (the handle is left reset).
-        Returns (config, chunk, ms per step)."""
+    def autotune(self, trial_steps=32):
+        """Pick the fastest launch configuration (the handle is left reset);
+        with graphs set (set_graph) the trials replay them.  Returns (config,
+        chunk, ms per step)."""
         c, k, ms = C.c_int(), C.c_int(), C.c_double()
         L.check(L.load().sm_a3d_autotune(self._h, int(trial_steps), C.byref(c), C.byref(k),
                                          C.byref(ms)))

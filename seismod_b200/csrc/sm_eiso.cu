@@ -3181,7 +3181,7 @@ extern "C" int sm_eiso_autotune(sm_eiso_t h, int trial_steps, int *config,
     if (int rc = eiso_check(h)) return rc;
     if (h->it != 0)
         return sm_fail(SM_ESTATE, "sm_eiso_autotune: call before the first step (or after reset)");
-    if (trial_steps <= 0) trial_steps = 20;
+    if (trial_steps <= 0) trial_steps = 32;
     DeviceGuard g(h->device);
     struct Key {
         int prec, NX, NZ, np;
@@ -3224,7 +3224,9 @@ extern "C" int sm_eiso_autotune(sm_eiso_t h, int trial_steps, int *config,
         h->config = c;
         h->graph_epoch++;
         if ((rc = sm_eiso_reset(h))) break;
-        if ((rc = sm_eiso_run(h, 2))) break;
+        // warm-up, and the time loop's graph (if the handle uses graphs)
+        // captured outside the timed trial
+        if ((rc = sm_eiso_run(h, 2 + (size_t)h->graph_steps))) break;
         cudaEventRecord(e0, h->stream);
         if ((rc = sm_eiso_run(h, (size_t)trial_steps))) break;
         cudaEventRecord(e1, h->stream);
