@@ -190,7 +190,7 @@ def make_workload(name, size=None):
 # which traffic follows), e_iso 64 x 1040 x 540 in FP32 and block storage,
 # and the velocity + stress launches of e_cyl_iso 2020 x 4040 FP32.
 MEASURED_TRAFFIC = {
-    ("a3d", 256, "fp32"): 1.116e9,
+    ("a3d", 256, "fp32"): 1.125e9,
     ("a3d", 256, "bfp16"): 0.809e9,
     ("eiso", 1000, "fp32"): 1.8375e9,
     ("eiso", 1000, "bfp16"): 1.1759e9,
