@@ -291,9 +291,12 @@ def run_ours(args, rank, world, local_rank, torch, dist):
         ms = time_steps(dev, K, torch)
     _, _, launches = dev.kernel_stats(reset=True)
     ms = max_over_ranks(ms, dist, f"cuda:{local_rank}")
-    # dominant-kernel duration: separate pass with per-launch events
+    # dominant-kernel duration: separate pass with per-launch events (event
+    # nodes inside the graph replays when the handle replays graphs)
     dev.set_timing(True)
     Kr = max(100, min(K, 400))   # at least 100 launches: the mean of a short pass is noisy
+    if GRAPH and kind != "ecyl":
+        Kr = -(-Kr // GRAPH) * GRAPH   # whole graphs only
     dev.run(Kr)
     upd_ms, upd_n, _ = dev.kernel_stats(reset=True)
     dev.set_timing(False)
@@ -370,7 +373,7 @@ def timed_rate(kind, p, prec, dev_id, steps, shots=None):
     dev.sync()
     ms = time_steps(dev, steps, torch) / steps
     dev.set_timing(True)
-    dev.run(steps)
+    dev.run(-(-steps // GRAPH) * GRAPH if GRAPH and kind != "ecyl" else steps)
     kms, kn, _ = dev.kernel_stats(reset=True)
     dev.set_timing(False)
     dev.close()

@@ -236,8 +236,9 @@ int sm_eiso_autotune(sm_eiso_t h, int trial_steps, int *config, double *ms_per_s
 /* Replay the time loop as CUDA graphs of `steps` steps (2, 4, 8 or 16; 0
  * launches every kernel from the host, the default).  Results are the same
  * either way.  Graphs are captured lazily and again after new sources,
- * receivers, configurations or 16-bit scales; per-kernel timing
- * (sm_eiso_set_timing) launches without graphs. */
+ * receivers, configurations or 16-bit scales.  With per-kernel timing on
+ * (sm_eiso_set_timing) the graphs are captured again with event nodes
+ * around each update launch, and the host waits for every replay. */
 int sm_eiso_set_graph(sm_eiso_t h, int steps);
 /* Per-kernel timing.  With timing on, every launch of the wavefield update
  * kernel(s) is bracketed by CUDA events on the handle's stream;

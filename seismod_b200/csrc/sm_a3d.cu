@@ -1461,10 +1461,17 @@ struct sm_a3d {
         cudaGraphExec_t exec = nullptr;
         unsigned epoch = 0;
         int steps = 0;
+        bool timed = false;      // captured with per-kernel timing on
+        EventPairs tev;          // the timed launches' event nodes
     } graphs[2];
     ~sm_a3d() {
-        for (Graph &g : graphs)
+        for (Graph &g : graphs) {
             if (g.exec) cudaGraphExecDestroy(g.exec);
+            for (auto &p : g.tev) {
+                cudaEventDestroy(p.first);
+                cudaEventDestroy(p.second);
+            }
+        }
     }
     // 16-bit storage: exponents of the 4 fields (A_*) and 6 memory
     // variables (4 + PS_*), stored = value * 2^expo
@@ -1890,17 +1897,26 @@ void a3d_launch(sm_a3d *h) {
 
 // x planes per CTA: enough CTAs for a few waves on the device, at least
 // 16 planes per chunk so the recomputed plane i0-1 and the pipeline fill stay
-// cheap
-int a3d_pick_chunk(size_t nx2, size_t ny2, size_t nz2, int sms, int ty) {
+// cheap.  Scalar storage (4 CTAs per SM) keeps chunks short, at most 20
+// planes, so a launch runs many waves and its last, partial one is short
+// (544^3 FP32: 1.22 ms per step with 16-20 planes, 1.38 with 64); block
+// storage (2 CTAs per SM, a costlier fill per chunk) aims at half the CTAs
+// and takes up to 64 planes (544^3: 1.23 ms with 48-64, 1.28 with 16).
+int a3d_pick_chunk(size_t nx2, size_t ny2, size_t nz2, int sms, int ty, bool block) {
     const size_t tiles = ((nz2 + 31) / 32) * ((ny2 + ty - 1) / ty);
-    const size_t want = (size_t)sms * 16;
+    const size_t want = (size_t)sms * (block ? 8 : 16);
     size_t nch = (want + tiles - 1) / tiles;
     if (nch < 1) nch = 1;
     size_t chunk = (nx2 + nch - 1) / nch;
+    const size_t cap = block ? A3_CHMAX : 20;
+    if (chunk > cap) chunk = (nx2 + (nx2 + cap - 1) / cap - 1) / ((nx2 + cap - 1) / cap);
     if (chunk < 16) chunk = 16;
-    if (chunk > A3_CHMAX) chunk = A3_CHMAX;
     if (chunk > nx2) chunk = nx2;
     return (int)chunk;
+}
+
+int a3d_default_chunk(const sm_a3d *h, int config) {
+    return a3d_pick_chunk(h->nx2, h->ny2, h->nz2, h->sms, a3d_cfg(h, config).ty(), a3d_isb(h));
 }
 
 int a3d_field_id(int comp) {
@@ -2116,7 +2132,7 @@ extern "C" int sm_a3d_create(int device, size_t nx2, size_t ny2, size_t nz2, siz
     for (int f = 0; f < 4; ++f) { a.sc[f] = 1.f; a.isc[f] = 1.f; }
     for (int p = 0; p < 6; ++p) { a.psc[p] = 1.f; a.pisc[p] = 1.f; }
     cudaDeviceGetAttribute(&h->sms, cudaDevAttrMultiProcessorCount, device);
-    a.chunk = a3d_pick_chunk(nx2, ny2, nz2, h->sms, a3d_cfg(h.get(), h->config).ty());
+    a.chunk = a3d_default_chunk(h.get(), h->config);
     static std::atomic<uint64_t> serials{1};
     h->serial = serials.fetch_add(1);
     a3d_bind(h.get(), 0);
@@ -2281,7 +2297,8 @@ namespace {
 template <typename S>
 int a3d_graph(sm_a3d *h, cudaGraphExec_t *out) {
     sm_a3d::Graph &gr = h->graphs[h->cur];
-    if (gr.exec && gr.epoch == h->graph_epoch && gr.steps == h->graph_steps) {
+    if (gr.exec && gr.epoch == h->graph_epoch && gr.steps == h->graph_steps &&
+        gr.timed == h->timer.on) {
         *out = gr.exec;
         return SM_OK;
     }
@@ -2289,12 +2306,16 @@ int a3d_graph(sm_a3d *h, cudaGraphExec_t *out) {
         cudaGraphExecDestroy(gr.exec);
         gr.exec = nullptr;
     }
+    h->timer.release(gr.tev);
     const size_t launches = h->timer.launches;
     const int cur = h->cur;
     SM_CUDA_TRY(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
+    gr.timed = h->timer.on;
+    h->timer.capture = gr.timed ? &gr.tev : nullptr;
     for (int k = 0; k < h->graph_steps; ++k) a3d_launch<S>(h);
     cudaGraph_t graph = nullptr;
     cudaError_t e = cudaStreamEndCapture(h->stream, &graph);
+    h->timer.capture = nullptr;
     h->timer.launches = launches;
     h->cur = cur;   // an even number of steps: back to the starting set
     a3d_bind(h, h->cur);
@@ -2327,10 +2348,11 @@ int a3d_run_t(sm_a3d *h, size_t nsteps) {
     while (nsteps > 0) {
         // graphs start anywhere, except in 16-bit storage, whose range
         // checks fall on multiples of the scale period between graphs
-        if (G && !h->timer.on && nsteps >= G && (!a3d_is16(h) || h->it % G == 0)) {
+        if (G && nsteps >= G && (!a3d_is16(h) || h->it % G == 0)) {
             cudaGraphExec_t ex = nullptr;
             if (int rc = a3d_graph<S>(h, &ex)) return rc;
             SM_CUDA_TRY(cudaGraphLaunch(ex, h->stream));
+            if (h->timer.on) h->timer.replayed(h->graphs[h->cur].tev);
             h->timer.launches += per_step * G;
             h->it += G;
             nsteps -= G;
@@ -2711,7 +2733,12 @@ extern "C" int sm_a3d_autotune(sm_a3d_t h, int trial_steps, int *config, int *ch
         h->timer.on = false;
         for (int c = 0; c < a3d_ncfg(h) && rc == SM_OK; ++c) {
             if (a3d_config_smem_prec(h->precision, c) > (size_t)lim) continue;
-            for (int ch : {0, 16, 32, 64}) {
+            if ((rc = sm_a3d_set_config(h, c))) break;
+            // the default chunk length, then other lengths it is not
+            std::vector<int> chunks{0};
+            for (int ch : {16, 20, 28, 32, 48, 64})
+                if (ch != a3d_default_chunk(h, c) && (size_t)ch <= h->nx2) chunks.push_back(ch);
+            for (int ch : chunks) {
                 if ((rc = sm_a3d_set_config(h, c)) || (rc = sm_a3d_set_chunk(h, ch))) break;
                 // warm-up, and the time loop's graph (if the handle uses
                 // graphs) captured outside the timed trial
@@ -2935,7 +2962,7 @@ extern "C" int sm_a3d_set_config(sm_a3d_t h, int config) {
                                   "in this precision (device limit %d)", config,
                        a3d_config_smem_prec(h->precision, config), maxsm);
     h->config = config;
-    h->args.chunk = a3d_pick_chunk(h->nx2, h->ny2, h->nz2, h->sms, a3d_cfg(h, config).ty());
+    h->args.chunk = a3d_default_chunk(h, config);
     h->graph_epoch++;
     // maps are rebuilt for the new tile height at the next run
     return SM_OK;
@@ -2944,7 +2971,7 @@ extern "C" int sm_a3d_set_config(sm_a3d_t h, int config) {
 extern "C" int sm_a3d_set_chunk(sm_a3d_t h, int chunk) {
     if (int rc = a3d_check(h)) return rc;
     if (chunk <= 0)
-        h->args.chunk = a3d_pick_chunk(h->nx2, h->ny2, h->nz2, h->sms, a3d_cfg(h, h->config).ty());
+        h->args.chunk = a3d_default_chunk(h, h->config);
     else
         h->args.chunk = chunk > A3_CHMAX ? A3_CHMAX : (chunk > (int)h->nx2 ? (int)h->nx2 : chunk);
     h->graph_epoch++;

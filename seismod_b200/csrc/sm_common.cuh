@@ -259,10 +259,17 @@ int upload_convert(void *dst, const double *src, size_t n, cudaStream_t s) {
 inline size_t round_up(size_t a, size_t b) { return (a + b - 1) / b * b; }
 
 // CUDA-event timing of the update kernel(s) plus launch counters
+// begin/end event pairs of the launches timed inside one captured CUDA graph
+using EventPairs = std::vector<std::pair<cudaEvent_t, cudaEvent_t>>;
+
 struct KernelTimer {
     bool on = false;
     std::vector<cudaEvent_t> pool;
-    std::vector<std::pair<cudaEvent_t, cudaEvent_t>> pending;
+    EventPairs pending;
+    // set while a graph is captured with timing on: begin() and end() then
+    // record external event nodes, which every replay of the graph records
+    // again, and the pairs go to the graph's list instead of `pending`
+    EventPairs *capture = nullptr;
     double ms = 0.0;
     size_t timed = 0;
     size_t launches = 0;        // every kernel this handle launched
@@ -290,15 +297,42 @@ struct KernelTimer {
     cudaEvent_t begin(cudaStream_t s) {
         if (!on) return nullptr;
         cudaEvent_t a = get();
-        cudaEventRecord(a, s);
+        if (capture) cudaEventRecordWithFlags(a, s, cudaEventRecordExternal);
+        else cudaEventRecord(a, s);
         return a;
     }
     void end(cudaEvent_t a, cudaStream_t s) {
         if (!a) return;
         cudaEvent_t b = get();
+        if (capture) {
+            cudaEventRecordWithFlags(b, s, cudaEventRecordExternal);
+            capture->emplace_back(a, b);
+            return;
+        }
         cudaEventRecord(b, s);
         pending.emplace_back(a, b);
         if (pending.size() > 4096) collect();
+    }
+    // one replay of a graph captured with timing was launched: wait for its
+    // last event (the next replay records the same events) and add the
+    // durations of its timed launches
+    void replayed(const EventPairs &ev) {
+        if (ev.empty()) return;
+        cudaEventSynchronize(ev.back().second);
+        for (auto &p : ev) {
+            float t = 0.f;
+            if (cudaEventElapsedTime(&t, p.first, p.second) != cudaSuccess) continue;
+            ms += t;
+            ++timed;
+        }
+    }
+    // a timed graph was destroyed: its events back to the pool
+    void release(EventPairs &ev) {
+        for (auto &p : ev) {
+            pool.push_back(p.first);
+            pool.push_back(p.second);
+        }
+        ev.clear();
     }
     void collect() {
         for (auto &p : pending) {

@@ -1730,10 +1730,17 @@ struct sm_eiso {
         cudaGraphExec_t exec = nullptr;
         unsigned epoch = 0;
         int steps = 0;
+        bool timed = false;      // captured with per-kernel timing on
+        EventPairs tev;          // the timed launches' event nodes
     } graphs[2];
     ~sm_eiso() {
-        for (Graph &g : graphs)
+        for (Graph &g : graphs) {
             if (g.exec) cudaGraphExecDestroy(g.exec);
+            for (auto &p : g.tev) {
+                cudaEventDestroy(p.first);
+                cudaEventDestroy(p.second);
+            }
+        }
     }
     int sms = 148;
     uint64_t serial = 0;   // unique per handle in the process (grouped graphs' keys)
@@ -2830,7 +2837,8 @@ int eiso_step_once(sm_eiso *h) {
 template <typename S>
 int eiso_graph(sm_eiso *h, cudaGraphExec_t *out) {
     sm_eiso::Graph &gr = h->graphs[h->cur];
-    if (gr.exec && gr.epoch == h->graph_epoch && gr.steps == h->graph_steps) {
+    if (gr.exec && gr.epoch == h->graph_epoch && gr.steps == h->graph_steps &&
+        gr.timed == h->timer.on) {
         *out = gr.exec;
         return SM_OK;
     }
@@ -2838,13 +2846,17 @@ int eiso_graph(sm_eiso *h, cudaGraphExec_t *out) {
         cudaGraphExecDestroy(gr.exec);
         gr.exec = nullptr;
     }
+    h->timer.release(gr.tev);
     const size_t launches = h->timer.launches;
     const int cur = h->cur;
     SM_CUDA_TRY(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
+    gr.timed = h->timer.on;
+    h->timer.capture = gr.timed ? &gr.tev : nullptr;
     int rc = SM_OK;
     for (int k = 0; k < h->graph_steps && rc == SM_OK; ++k) rc = eiso_step_once<S>(h);
     cudaGraph_t graph = nullptr;
     cudaError_t e = cudaStreamEndCapture(h->stream, &graph);
+    h->timer.capture = nullptr;
     h->timer.launches = launches;
     h->cur = cur;   // an even number of steps: back to the starting set
     eiso_bind(h);
@@ -2873,10 +2885,11 @@ int eiso_run_t(sm_eiso *h, size_t nsteps) {
     while (nsteps > 0) {
         // graphs start anywhere, except in 16-bit storage, whose range
         // checks fall on multiples of the scale period between graphs
-        if (G && !h->timer.on && nsteps >= G && (!eiso_is16(h) || h->it % G == 0)) {
+        if (G && nsteps >= G && (!eiso_is16(h) || h->it % G == 0)) {
             cudaGraphExec_t ex = nullptr;
             if (int rc = eiso_graph<S>(h, &ex)) return rc;
             SM_CUDA_TRY(cudaGraphLaunch(ex, h->stream));
+            if (h->timer.on) h->timer.replayed(h->graphs[h->cur].tev);
             h->timer.launches += per_step * G;
             h->it += G;
             nsteps -= G;
