@@ -322,6 +322,10 @@ def run_ours(args, rank, world, local_rank, torch, dist):
                      "unit": "GB/s", "frac": round(achieved / hbm, 4),
                      "traffic": measured_traffic(kind, p, prec),
                      "peak_source": how, "algorithmic_bytes_per_step": bps,
+                     "duration": "mean of %d update launches, CUDA events on the library's "
+                                 "stream%s, right after the timed region"
+                                 % (upd_n, " recorded as event nodes of the replayed graphs"
+                                    if GRAPH and kind != "ecyl" else ""),
                      "kernel": "wavefield update (velocity + stress/pressure, PML/CPML)"},
         "gpu_launches": int(launches),
         "clocks": clk.summary(),
