@@ -548,12 +548,14 @@ def e2e(kind, p, K, local_rank):
     """Whole user call through the public API from host arrays: set-up and
     upload, K steps, traces back to the host, teardown."""
     from seismod_b200 import api
+    import gc
+    gc.collect()   # the earlier legs' garbage is not this call's to collect
     marks = [("start", time.perf_counter())]
     if kind == "a3d":   # the steps of api.a3d_device, timed one by one
-        q = api.a3d_inputs(p)
+        q = api.a3d_inputs(p, pad=False)   # padded as it is staged
         marks.append(("host_inputs", time.perf_counter()))
         dev = api.A3DDevice(q["vp"], q["rho"], q["npml"], q["d"], q["dt"], q["coef"], "fp32",
-                            local_rank)
+                            local_rank, padded=False)
         dev.set_sources(*q["src"], q["src_scale"])
         dev.set_receivers(*q["rec"], q["nsteps"])
         marks.append(("create_upload", time.perf_counter()))

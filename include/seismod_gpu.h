@@ -147,6 +147,9 @@ int sm_eiso_profiles(size_t np, double h, size_t ncell, const double *vp,
 int sm_a3d_pad_model(size_t nx, size_t ny, size_t nz, size_t np,
                      const double *vp, const double *rho, double *vp_pad, double *rho_pad);
 double sm_a3d_cfl_vpmax(size_t nx, size_t nz, const double *vp_pad);
+/* the same maximum from the unpadded nx x ny x nz model (no reference
+ * counterpart: sm_a3d_cfl_vpmax of sm_a3d_pad_model's output, without it) */
+double sm_a3d_cfl_vpmax_unpadded(size_t nx, size_t ny, size_t nz, size_t np, const double *vp);
 int sm_a3d_cpml(size_t np, size_t nx2, size_t ny2, size_t nz2,
                 double dx, double dy, double dz, double dt,
                 double pml_order, double vmax, double Rc, double kappa_max,
@@ -264,6 +267,15 @@ int sm_a3d_create(int device, size_t nx2, size_t ny2, size_t nz2, size_t np,
                   double dx, double dy, double dz, double dt,
                   const double *vp, const double *rho, const double *const *coef,
                   int precision, sm_a3d_t *out);
+/* sm_a3d_create from the unpadded nx x ny x nz model: the padded nodes take
+ * the value of the nearest interior node (io_utils.c:1096-1143) as the
+ * materials are staged, so no padded copy is made on the host.  The handle
+ * equals sm_a3d_create's on sm_a3d_pad_model's output bit for bit; coef is
+ * for the padded grid (nx + 2 np, ...).  No reference counterpart. */
+int sm_a3d_create_unpadded(int device, size_t nx, size_t ny, size_t nz, size_t np,
+                           double dx, double dy, double dz, double dt,
+                           const double *vp, const double *rho, const double *const *coef,
+                           int precision, sm_a3d_t *out);
 /* a_iso_3d.c:689-693: P[index[s]] += scale * fct[s*stride + it] while
  * it < length[s]; the reference uses scale = dt * 1e6 for every source type */
 int sm_a3d_set_sources(sm_a3d_t h, size_t nsrc, const size_t *index, const double *fct,

@@ -52,6 +52,7 @@ _SIGS = {
     "sm_eiso_profiles": (C.c_int, [_sz, C.c_double, _sz, _dp, _dp, _dp, _dp]),
     "sm_a3d_pad_model": (C.c_int, [_sz, _sz, _sz, _sz, _dp, _dp, _dp, _dp]),
     "sm_a3d_cfl_vpmax": (C.c_double, [_sz, _sz, _dp]),
+    "sm_a3d_cfl_vpmax_unpadded": (C.c_double, [_sz, _sz, _sz, _sz, _dp]),
     "sm_a3d_cpml": (C.c_int, [_sz, _sz, _sz, _sz] + [C.c_double] * 8 +
                     [C.c_int, C.c_double, C.POINTER(_dp)]),
     "sm_ecyl_pad_model": (C.c_int, [_sz, _sz, _sz] + [_dp] * 6),
@@ -90,6 +91,8 @@ _SIGS = {
     "sm_eiso_destroy": (C.c_int, [_vp]),
     "sm_a3d_create": (C.c_int, [C.c_int, _sz, _sz, _sz, _sz] + [C.c_double] * 4 +
                       [_dp, _dp, C.POINTER(_dp), C.c_int, C.POINTER(_vp)]),
+    "sm_a3d_create_unpadded": (C.c_int, [C.c_int, _sz, _sz, _sz, _sz] + [C.c_double] * 4 +
+                               [_dp, _dp, C.POINTER(_dp), C.c_int, C.POINTER(_vp)]),
     "sm_a3d_set_sources": (C.c_int, [_vp, _sz, _szp, _dp, _szp, _sz, C.c_double]),
     "sm_a3d_set_receivers": (C.c_int, [_vp, _sz, _szp, _ip, _dp, _dp, _sz]),
     "sm_a3d_run": (C.c_int, [_vp, _sz]),

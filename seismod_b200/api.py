@@ -83,6 +83,12 @@ def a3d_cfl_vpmax(nx, nz, vp_pad):
     return L.load().sm_a3d_cfl_vpmax(nx, nz, L.dptr(_f64(vp_pad)))
 
 
+def a3d_cfl_vpmax_unpadded(vp, npml):
+    """a3d_cfl_vpmax of the padded model, read from the unpadded one."""
+    nx, ny, nz = vp.shape
+    return L.load().sm_a3d_cfl_vpmax_unpadded(nx, ny, nz, npml, L.dptr(_f64(vp)))
+
+
 def a3d_cpml(npml, shape2, d, dt, pml_order=2.0, vmax=5000.0, Rc=1e-5, kappa_max=1.0,
              alpha_max_flag=1, f0=0.0):
     n2 = list(shape2)
@@ -218,18 +224,23 @@ class EIsoDevice:
 class A3DDevice:
     """An a_iso_3d state on the GPU."""
 
-    def __init__(self, vp_pad, rho_pad, npml, d, dt, coef, precision="fp32", device=0):
+    def __init__(self, vp_pad, rho_pad, npml, d, dt, coef, precision="fp32", device=0,
+                 padded=True):
+        """vp_pad, rho_pad: the padded model (sm_a3d_create), or with
+        padded=False the unpadded one, edge-replicated as it is staged
+        (sm_a3d_create_unpadded)."""
         lib = L.load()
-        self.shape = vp_pad.shape
+        n = vp_pad.shape
+        self.shape = n if padded else tuple(x + 2 * npml for x in n)
         self.npml, self.d, self.dt, self.precision = npml, d, dt, precision
         vp_pad, rho_pad = _f64(vp_pad), _f64(rho_pad)
         cf = [_f64(c) for c in coef]
         P = (L._dp * 18)(*[L.dptr(c) for c in cf])
         hnd = C.c_void_p()
-        n = self.shape
-        L.check(lib.sm_a3d_create(device, n[0], n[1], n[2], npml, d[0], d[1], d[2], dt,
-                                  L.dptr(vp_pad), L.dptr(rho_pad), P, L.PRECISIONS[precision],
-                                  C.byref(hnd)))
+        create = lib.sm_a3d_create if padded else lib.sm_a3d_create_unpadded
+        L.check(create(device, n[0], n[1], n[2], npml, d[0], d[1], d[2], dt,
+                       L.dptr(vp_pad), L.dptr(rho_pad), P, L.PRECISIONS[precision],
+                       C.byref(hnd)))
         self._h = hnd
         self.nrec = 0
 
@@ -429,32 +440,41 @@ def _a3d_index_many(p, xyz):
     return ((i * ny2 + j) * nz2 + k).tolist()
 
 
-def a3d_inputs(p):
+def a3d_inputs(p, pad=True):
     """Everything sm_a3d_create and the source / receiver set-up take for
-    problem p (host arrays), as a_iso_3d.c:317-590 prepares it."""
+    problem p (host arrays), as a_iso_3d.c:317-590 prepares it.  pad=False
+    leaves the model unpadded, for A3DDevice(..., padded=False)."""
     nx, ny, nz = p.shape
-    vpp, rhop = a3d_pad_model(p.vp, p.rho, p.npml)
     dt = p.dt
-    vpmax = a3d_cfl_vpmax(nx, nz, vpp)
+    if pad:
+        vpp, rhop = a3d_pad_model(p.vp, p.rho, p.npml)
+        vpmax = a3d_cfl_vpmax(nx, nz, vpp)
+    else:
+        vpp, rhop = _f64(p.vp), _f64(p.rho)
+        vpmax = a3d_cfl_vpmax_unpadded(vpp, p.npml)
+    shape2 = tuple(n + 2 * p.npml for n in p.shape)
     dx, dy, dz = p.d
     if dt * vpmax * math.sqrt(1. / dx ** 2 + 1. / dy ** 2 + 1. / dz ** 2) > 1.:
         raise L.SeismodError(L.SM_ECFL, "time step too large (a_iso_3d.c:411-417)")
-    coef = a3d_cpml(p.npml, vpp.shape, p.d, dt, 2.0, 5000.0, p.Rc, p.kappa_max, p.alpha_max,
+    coef = a3d_cpml(p.npml, shape2, p.d, dt, 2.0, 5000.0, p.Rc, p.kappa_max, p.alpha_max,
                     p.sources[0][2])
     fct, ln = ricker([q[1] for q in p.sources], [q[2] for q in p.sources], dt)
     idx = [a3d_index(p, q[3], q[4], q[5]) for q in p.sources]
     rxyz = np.array([r[1:4] for r in p.receivers], dtype=np.float64).reshape(-1, 3)
     ridx = _a3d_index_many(p, rxyz)
     comps = [L.SM_COMP[c.lower()] for (c, _, _, _, _, _) in p.receivers]
-    return dict(vp=vpp, rho=rhop, npml=p.npml, d=p.d, dt=dt, coef=coef,
+    return dict(vp=vpp, rho=rhop, padded=pad, npml=p.npml, d=p.d, dt=dt, coef=coef,
                 src=(idx, fct, ln), src_scale=dt * 1e6,
                 rec=(ridx, comps, [r[4] for r in p.receivers], [r[5] * 1e-3 for r in p.receivers]),
                 nsteps=nsteps(p.duration, dt))
 
 
-def a3d_device(p, precision="fp32", device=0):
-    q = a3d_inputs(p)
-    dev = A3DDevice(q["vp"], q["rho"], q["npml"], q["d"], q["dt"], q["coef"], precision, device)
+def a3d_device(p, precision="fp32", device=0, pad_on_host=False):
+    """A handle for problem p; the model is padded as it is staged unless
+    pad_on_host (the padded model through sm_a3d_create, the same bits)."""
+    q = a3d_inputs(p, pad=pad_on_host)
+    dev = A3DDevice(q["vp"], q["rho"], q["npml"], q["d"], q["dt"], q["coef"], precision, device,
+                    padded=pad_on_host)
     n = q["nsteps"]
     dev.set_sources(*q["src"], q["src_scale"])
     dev.set_receivers(*q["rec"], n)

@@ -1972,27 +1972,44 @@ extern "C" int sm_a3d_device_bytes(size_t nx2, size_t ny2, size_t nz2, size_t np
     return SM_OK;
 }
 
+// The model a handle is made from: the padded volume (pad = 0, extents
+// nx2 x ny2 x nz2), or the unpadded one (extents nx x ny x nz) whose padded
+// nodes take the value of the nearest interior node (io_utils.c:1096-1143),
+// gathered as the materials are staged.
+struct A3Model {
+    const double *vp, *rho;
+    size_t nx, ny, nz, pad;
+    static size_t clamp(size_t n, size_t pad, size_t ext) {
+        return n < pad ? 0 : (n - pad >= ext ? ext - 1 : n - pad);
+    }
+    // offset of the source row of padded row (i, j)
+    size_t row(size_t i, size_t j) const { return (clamp(i, pad, nx) * ny + clamp(j, pad, ny)) * nz; }
+    size_t col(size_t k) const { return clamp(k, pad, nz); }
+};
+
 // pitched rho and K = rho vp^2 dt (a_iso_3d.c:407-409) in the compute type,
 // filled by a few host threads straight into the upload buffers (the model
 // of a large grid is hundreds of MB).  Pitch padding: rho repeats the last
 // real value so the on-the-fly buoyancy never divides by zero there (those
 // cells are not updated), K is zero.
 template <typename C>
-int a3d_upload_materials(sm_a3d *h, const double *rho, const double *vp, double dt, size_t nx2,
-                         size_t ny2, size_t nz2) {
+int a3d_upload_materials(sm_a3d *h, const A3Model &m, double dt, size_t nx2, size_t ny2,
+                         size_t nz2) {
     const size_t pitch = (size_t)h->pitch, ncell = nx2 * ny2 * pitch;
     // pinned staging (cached across handles): the copies run at full link speed
     PinnedBuf rb, kb;
     if (int rc = rb.get(ncell * sizeof(C))) return rc;
     if (int rc = kb.get(ncell * sizeof(C))) return rc;
     C *r = rb.as<C>(), *kk = kb.as<C>();
+    const double *rho = m.rho, *vp = m.vp;
     auto fill = [&](size_t ib, size_t ie) {
         for (size_t i = ib; i < ie; ++i)
             for (size_t j = 0; j < ny2; ++j) {
-                const size_t s0 = (i * ny2 + j) * nz2, d0 = (i * ny2 + j) * pitch;
+                const size_t s0 = m.row(i, j), d0 = (i * ny2 + j) * pitch;
                 for (size_t k = 0; k < nz2; ++k) {
-                    r[d0 + k] = static_cast<C>(rho[s0 + k]);
-                    kk[d0 + k] = static_cast<C>(rho[s0 + k] * vp[s0 + k] * vp[s0 + k] * dt);
+                    const size_t sk = s0 + m.col(k);
+                    r[d0 + k] = static_cast<C>(rho[sk]);
+                    kk[d0 + k] = static_cast<C>(rho[sk] * vp[sk] * vp[sk] * dt);
                 }
                 for (size_t k = nz2; k < pitch; ++k) {
                     r[d0 + k] = r[d0 + nz2 - 1];
@@ -2013,15 +2030,16 @@ int a3d_upload_materials(sm_a3d *h, const double *rho, const double *vp, double 
     return SM_OK;
 }
 
-extern "C" int sm_a3d_create(int device, size_t nx2, size_t ny2, size_t nz2, size_t np,
-                             double dx, double dy, double dz, double dt, const double *vp,
-                             const double *rho, const double *const *coef, int precision,
-                             sm_a3d_t *out) {
+namespace {
+
+int a3d_create(int device, size_t nx2, size_t ny2, size_t nz2, size_t np, double dx, double dy,
+               double dz, double dt, const A3Model &m, const double *const *coef, int precision,
+               sm_a3d_t *out) {
     if (!out) return sm_fail(SM_EINVAL, "sm_a3d_create: out is NULL");
     *out = nullptr;
     if (nx2 < 2 * np + 2 || ny2 < 2 * np + 2 || nz2 < 2 * np + 2)
         return sm_fail(SM_EINVAL, "sm_a3d_create: grid smaller than the CPML frame");
-    if (!vp || !rho || !coef) return sm_fail(SM_EINVAL, "sm_a3d_create: NULL array");
+    if (!m.vp || !m.rho || !coef) return sm_fail(SM_EINVAL, "sm_a3d_create: NULL array");
     for (int c = 0; c < 18; ++c)
         if (!coef[c]) return sm_fail(SM_EINVAL, "sm_a3d_create: NULL coefficient array");
     if (!(dx > 0) || !(dy > 0) || !(dz > 0) || !(dt > 0))
@@ -2084,8 +2102,8 @@ extern "C" int sm_a3d_create(int device, size_t nx2, size_t ny2, size_t nz2, siz
     }
     if ((rc = h->rho.alloc_pooled(ncell * cb, device))) return rc;
     if ((rc = h->K.alloc_pooled(ncell * cb, device))) return rc;
-    rc = precision == SM_FP64 ? a3d_upload_materials<double>(h.get(), rho, vp, dt, nx2, ny2, nz2)
-                              : a3d_upload_materials<float>(h.get(), rho, vp, dt, nx2, ny2, nz2);
+    rc = precision == SM_FP64 ? a3d_upload_materials<double>(h.get(), m, dt, nx2, ny2, nz2)
+                              : a3d_upload_materials<float>(h.get(), m, dt, nx2, ny2, nz2);
     if (rc) return rc;
     A3Coef cf{{(int)nx2, (int)ny2, (int)nz2}};
     {
@@ -2114,12 +2132,13 @@ extern "C" int sm_a3d_create(int device, size_t nx2, size_t ny2, size_t nz2, siz
     a.nyb = (int)h->nyb;
     if (precision == SM_FP16 || precision == SM_BF16) {
         if ((rc = h->scaler.init(10, 10))) return rc;
-        const size_t N = nx2 * ny2 * nz2;
-        h->rho_min = rho[0];
-        h->vp_min = vp[0];
+        // the padded nodes repeat interior values: the source's minima
+        const size_t N = m.nx * m.ny * m.nz;
+        h->rho_min = m.rho[0];
+        h->vp_min = m.vp[0];
         for (size_t q = 1; q < N; ++q) {
-            if (rho[q] < h->rho_min) h->rho_min = rho[q];
-            if (vp[q] < h->vp_min) h->vp_min = vp[q];
+            if (m.rho[q] < h->rho_min) h->rho_min = m.rho[q];
+            if (m.vp[q] < h->vp_min) h->vp_min = m.vp[q];
         }
         h->hmin = std::min(dx, std::min(dy, dz));
         h->expo0.assign(10, 0);
@@ -2146,6 +2165,27 @@ extern "C" int sm_a3d_create(int device, size_t nx2, size_t ny2, size_t nz2, siz
     if ((rc = sm_a3d_reset(h.get()))) return rc;
     *out = h.release();
     return SM_OK;
+}
+
+}  // namespace
+
+extern "C" int sm_a3d_create(int device, size_t nx2, size_t ny2, size_t nz2, size_t np,
+                             double dx, double dy, double dz, double dt, const double *vp,
+                             const double *rho, const double *const *coef, int precision,
+                             sm_a3d_t *out) {
+    return a3d_create(device, nx2, ny2, nz2, np, dx, dy, dz, dt,
+                      A3Model{vp, rho, nx2, ny2, nz2, 0}, coef, precision, out);
+}
+
+extern "C" int sm_a3d_create_unpadded(int device, size_t nx, size_t ny, size_t nz, size_t np,
+                                      double dx, double dy, double dz, double dt,
+                                      const double *vp, const double *rho,
+                                      const double *const *coef, int precision, sm_a3d_t *out) {
+    if (!out) return sm_fail(SM_EINVAL, "sm_a3d_create_unpadded: out is NULL");
+    *out = nullptr;
+    if (!nx || !ny || !nz) return sm_fail(SM_EINVAL, "sm_a3d_create_unpadded: empty model");
+    return a3d_create(device, nx + 2 * np, ny + 2 * np, nz + 2 * np, np, dx, dy, dz, dt,
+                      A3Model{vp, rho, nx, ny, nz, np}, coef, precision, out);
 }
 
 extern "C" int sm_a3d_reset(sm_a3d_t h) {

@@ -209,6 +209,26 @@ double sm_a3d_cfl_vpmax(size_t nx, size_t nz, const double *vp_pad)
     return v;
 }
 
+double sm_a3d_cfl_vpmax_unpadded(size_t nx, size_t ny, size_t nz, size_t np, const double *vp)
+{
+    /* sm_a3d_cfl_vpmax on the padded model that sm_a3d_pad_model would
+     * make: the same padded indices i*nz + j, each mapped to the interior
+     * node whose value edge replication copies there */
+    const size_t ny2 = ny + 2 * np, nz2 = nz + 2 * np;
+    double v = 0.0;
+    for (size_t i = 0; i < nx; ++i)
+        for (size_t j = 0; j < nz; ++j) {
+            const size_t q = i * nz + j;
+            const size_t x = q / (ny2 * nz2), y = q / nz2 % ny2, z = q % nz2;
+            const size_t cx = x < np ? 0 : (x - np >= nx ? nx - 1 : x - np);
+            const size_t cy = y < np ? 0 : (y - np >= ny ? ny - 1 : y - np);
+            const size_t cz = z < np ? 0 : (z - np >= nz ? nz - 1 : z - np);
+            const double a = vp[(cx * ny + cy) * nz + cz];
+            if (a > v) v = a;
+        }
+    return v;
+}
+
 int sm_a3d_cpml(size_t np, size_t nx2, size_t ny2, size_t nz2,
                 double dx, double dy, double dz, double dt,
                 double pml_order, double vmax, double Rc, double kappa_max,

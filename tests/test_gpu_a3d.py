@@ -223,3 +223,35 @@ def test_bfp16_shot_within_gate_and_as_the_rounding_oracle_predicts():
     again = api.run_a3d(p, "bfp16")
     for a, b in zip(got, again):
         np.testing.assert_array_equal(a, b)
+
+
+@pytest.mark.parametrize("precision", ["fp32", "fp64", "bfp16", "fp16"])
+def test_unpadded_create_equals_the_padded_one(precision):
+    """sm_a3d_create_unpadded pads the model as it stages the materials:
+    the same handle, bit for bit, as sm_a3d_create on the padded model
+    (traces and the whole state), on a grid whose padding is uneven in
+    every axis."""
+    rng = np.random.default_rng(77)
+    shape = (23, 31, 45)
+    vp = 1500 + 3000 * rng.random(shape)
+    rho = 1800 + 600 * rng.random(shape)
+    d = (4.0, 5.0, 3.0)
+    dt_ms = 0.5 / (vp.max() * np.sqrt(sum(1 / h ** 2 for h in d))) * 1e3
+    rec = [(c, float(rng.integers(0, shape[0])) * d[0], float(rng.integers(0, shape[1])) * d[1],
+            float(rng.integers(0, shape[2])) * d[2], 0.0, dt_ms)
+           for c in ("Vx", "Vy", "Vz", "P")]
+    p = W.A3DProblem(vp, rho, d, 6, dt_ms, W.steps_duration(60, dt_ms),
+                     [("Bulk", 1.0, 40.0, 11 * d[0], 7 * d[1], 20 * d[2])], rec,
+                     Rc=1e-3, kappa_max=2.0, alpha_max=1)
+    a, n = api.a3d_device(p, precision, pad_on_host=True)
+    b, _ = api.a3d_device(p, precision)
+    assert a.shape == b.shape
+    for d in (a, b):
+        d.run(n)
+        d.sync()
+    for x, y in zip(a.traces(), b.traces()):
+        np.testing.assert_array_equal(x, y)
+    for f in ("p", "vx", "vy", "vz"):
+        np.testing.assert_array_equal(a.get_field(f), b.get_field(f))
+    a.close()
+    b.close()

@@ -81,6 +81,24 @@ def test_a3d_pad_model_split_over_threads_equals_the_oracle():
         np.testing.assert_array_equal(a[1], b[1])
 
 
+def test_a3d_cfl_vpmax_from_the_unpadded_model_equals_the_padded_scan():
+    # the reference scans padded indices i*nz + j (i < nx, j < nz); read
+    # from the unpadded model they must land on the nodes padding copies
+    # there, including the first planes' padded rows and columns
+    rng = np.random.default_rng(6)
+    for shape, npml in [((6, 7, 8), 1), ((6, 7, 8), 3), ((40, 3, 50), 16), ((9, 30, 2), 4),
+                        ((2, 2, 2), 0)]:
+        for trial in range(3):
+            vp = 1500 + 3000 * rng.random(shape)
+            if trial == 1:   # the maximum on an edge that padding replicates
+                vp[0, 0, :] += 5000
+            elif trial == 2:
+                vp[:, -1, -1] += 5000
+            vpp, _ = O.a3d_pad_model(vp, vp, npml)
+            nx, _, nz = shape
+            assert api.a3d_cfl_vpmax_unpadded(vp, npml) == O.a3d_cfl_vpmax(nx, nz, vpp)
+
+
 def test_sampling_and_nsteps_match_oracle():
     for dt in (8.838834764831844e-05, 1e-4, 1.7e-4):
         for (t0, rdt) in [(0.0, dt), (0.0, 3 * dt), (2e-3, dt), (5 * dt, 0.0), (0.0, 2.5 * dt)]:
