@@ -460,12 +460,16 @@ def a3d_inputs(p, pad=True):
                     p.sources[0][2])
     fct, ln = ricker([q[1] for q in p.sources], [q[2] for q in p.sources], dt)
     idx = [a3d_index(p, q[3], q[4], q[5]) for q in p.sources]
-    rxyz = np.array([r[1:4] for r in p.receivers], dtype=np.float64).reshape(-1, 3)
+    # receivers (component, x, y, z, t0, dt) transposed once: a large grid
+    # of receivers is tens of thousands of tuples
+    cols = list(zip(*p.receivers)) if p.receivers else [()] * 6
+    rxyz = np.array(cols[1:4], dtype=np.float64).reshape(3, -1).T
     ridx = _a3d_index_many(p, rxyz)
-    comps = [L.SM_COMP[c.lower()] for (c, _, _, _, _, _) in p.receivers]
+    code = {c: L.SM_COMP[c.lower()] for c in set(cols[0])}
+    comps = [code[c] for c in cols[0]]
     return dict(vp=vpp, rho=rhop, padded=pad, npml=p.npml, d=p.d, dt=dt, coef=coef,
                 src=(idx, fct, ln), src_scale=dt * 1e6,
-                rec=(ridx, comps, [r[4] for r in p.receivers], [r[5] * 1e-3 for r in p.receivers]),
+                rec=(ridx, comps, list(cols[4]), (np.array(cols[5], dtype=np.float64) * 1e-3).tolist()),
                 nsteps=nsteps(p.duration, dt))
 
 

@@ -2017,16 +2017,38 @@ int a3d_upload_materials(sm_a3d *h, const A3Model &m, double dt, size_t nx2, siz
                 }
             }
     };
+    // each thread fills its x planes in a few pieces and queues the copy of
+    // a piece as soon as it is filled, so the link carries the first pieces
+    // while the later ones are filled
+    const size_t plane = ny2 * pitch;
+    const int device = h->device;
+    cudaStream_t st = h->stream;
+    std::atomic<int> failed{0};
+    auto part = [&](size_t ib, size_t ie) {
+        cudaSetDevice(device);
+        constexpr size_t kPieces = 4;
+        for (size_t p = 0; p < kPieces; ++p) {
+            const size_t pb = ib + (ie - ib) * p / kPieces, pe = ib + (ie - ib) * (p + 1) / kPieces;
+            if (pb == pe) continue;
+            fill(pb, pe);
+            const size_t off = pb * plane, n = (pe - pb) * plane * sizeof(C);
+            if (cudaMemcpyAsync(h->rho.as<C>() + off, r + off, n, cudaMemcpyHostToDevice, st) !=
+                    cudaSuccess ||
+                cudaMemcpyAsync(h->K.as<C>() + off, kk + off, n, cudaMemcpyHostToDevice, st) !=
+                    cudaSuccess)
+                failed = 1;
+        }
+    };
     const size_t nt = std::min<size_t>(std::max(1u, std::thread::hardware_concurrency()), 16);
     std::vector<std::thread> pool;
     for (size_t t = 0; t < nt; ++t) {
         const size_t ib = nx2 * t / nt, ie = nx2 * (t + 1) / nt;
-        if (ib < ie) pool.emplace_back(fill, ib, ie);
+        if (ib < ie) pool.emplace_back(part, ib, ie);
     }
     for (auto &th : pool) th.join();
-    SM_CUDA_TRY(cudaMemcpyAsync(h->rho.p, r, ncell * sizeof(C), cudaMemcpyHostToDevice, h->stream));
-    SM_CUDA_TRY(cudaMemcpyAsync(h->K.p, kk, ncell * sizeof(C), cudaMemcpyHostToDevice, h->stream));
-    SM_CUDA_TRY(cudaStreamSynchronize(h->stream));   // the staging goes back to the cache
+    // the staging goes back to the cache only after every copy has run
+    SM_CUDA_TRY(cudaStreamSynchronize(h->stream));
+    if (failed) return sm_fail(SM_ECUDA, "sm_a3d_create: material upload failed");
     return SM_OK;
 }
 
