@@ -577,8 +577,8 @@ def e2e(kind, p, K, local_rank):
         tr = dev.traces()
         d2h = sum(len(x) for x in tr) * 8
     else:
-        tr = [dev.traces(s) for s in range(dev.nshots)]
-        d2h = sum(sum(len(x) for x in t) for t in tr) * 8
+        tr = [dev.traces_array(s) for s in range(dev.nshots)]
+        d2h = sum(t.size for t in tr) * 8
     marks.append(("traces_back", time.perf_counter()))
     dev.close()
     marks.append(("teardown", time.perf_counter()))

@@ -170,6 +170,19 @@ class EIsoDevice:
                                                  L.szptr(counts)))
         return [out[r, :int(counts[r])].copy() for r in range(n)]
 
+    def traces_array(self, shot=0):
+        """Traces of one shot as one [nrec, nsamples] array, one copy from
+        the device (receivers with fewer samples are zero-padded)."""
+        n = self.nrec[shot]
+        counts = np.zeros(n, dtype=np.uintp)
+        L.check(L.load().sm_eiso_read_traces(self._h, shot, 0, n, None, 0, L.szptr(counts)))
+        ld = int(counts.max()) if n else 0
+        out = np.zeros((n, max(ld, 1)))
+        if n and ld:
+            L.check(L.load().sm_eiso_read_traces(self._h, shot, 0, n, L.dptr(out), ld,
+                                                 L.szptr(counts)))
+        return out
+
     def get_field(self, comp, shot=0, part="total"):
         out = np.zeros((self.NX, self.NZ))
         L.check(L.load().sm_eiso_get_field(self._h, shot, L.SM_COMP[comp], L.SM_PART[part],

@@ -313,3 +313,20 @@ def test_bfp16_shot_within_gate_and_as_the_rounding_oracle_predicts():
     pred, _, _ = H.run_eiso_oracle(p, bfp_block=BFP_BLOCK, bfp_axis="x")
     predicted = H.rel_l2(pred, plain)
     assert 0.5 * predicted < err < 2.0 * predicted, (err, predicted)
+
+
+def test_traces_array_equals_the_per_receiver_traces():
+    """EIsoDevice.traces_array(shot): one [nrec, nsamples] copy per shot,
+    the same samples as the per-receiver read, mid-run and at the end."""
+    p = W.cfg2(nx=120, nz=80, npml=10, nsteps=120, nshots=3, nrec=12)
+    dev, n = api.eiso_device(p, "fp32")
+    for steps in (n // 3, n - n // 3):
+        dev.run(steps)
+        for s in range(3):
+            a = dev.traces_array(s)
+            rows = dev.traces(s)
+            assert a.shape[0] == len(rows)
+            for r, x in enumerate(rows):
+                np.testing.assert_array_equal(a[r, :len(x)], x)
+                assert not a[r, len(x):].any()
+    dev.close()
