@@ -133,6 +133,18 @@ def test_argument_errors_are_status_codes():
     f = np.array([50.0])
     rc = lib.sm_ricker(1, L.dptr(A), L.dptr(f), 1e-4, 1.0, 4, L.dptr(fct), L.szptr(ln))
     assert rc == L.SM_EINVAL
+    # the unpadded a_iso_3d create: an empty model, a NULL array, no handle
+    # pointer (all refused before any device is touched)
+    cf = (L._dp * 18)(*[L.dptr(z)] * 18)
+    rc = lib.sm_a3d_create_unpadded(0, 0, 4, 4, 1, 1.0, 1.0, 1.0, 1e-4, L.dptr(z), L.dptr(z),
+                                    cf, 0, C.byref(h))
+    assert rc == L.SM_EINVAL and b"empty" in lib.sm_last_error()
+    rc = lib.sm_a3d_create_unpadded(0, 4, 4, 4, 1, 1.0, 1.0, 1.0, 1e-4, None, L.dptr(z),
+                                    cf, 0, C.byref(h))
+    assert rc == L.SM_EINVAL and b"NULL" in lib.sm_last_error()
+    rc = lib.sm_a3d_create_unpadded(0, 4, 4, 4, 1, 1.0, 1.0, 1.0, 1e-4, L.dptr(z), L.dptr(z),
+                                    cf, 0, None)
+    assert rc == L.SM_EINVAL
 
 
 def test_a3d_rejects_coefficients_that_are_not_reference_defaults_inside():
