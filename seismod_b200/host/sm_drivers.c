@@ -251,7 +251,7 @@ int sm_a_iso_3d_main(int argc, char **argv)
     const char *prog = "a_iso_3d_gpu";
     sm_params p;
     sm_grid g;
-    double *vp = NULL, *rho = NULL, *vpp = NULL, *rhop = NULL, *fct = NULL, *vals = NULL;
+    double *vp = NULL, *rho = NULL, *fct = NULL, *vals = NULL;
     double *coef[18] = {0};
     size_t *len = NULL, *counts = NULL;
     sm_source *src = NULL;
@@ -269,12 +269,10 @@ int sm_a_iso_3d_main(int argc, char **argv)
     const size_t np = p.np, nx2 = g.nx + 2 * np, ny2 = g.ny + 2 * np, nz2 = g.nz + 2 * np;
     const size_t n3 = nx2 * ny2 * nz2;
     const double dt = p.dt;
-    vpp = malloc(n3 * sizeof(double));
-    rhop = malloc(n3 * sizeof(double));
-    if (!vpp || !rhop) { rc = sm_fail(SM_ENOMEM, "out of host memory"); goto out; }
-    if ((rc = sm_a3d_pad_model(g.nx, g.ny, g.nz, np, vp, rho, vpp, rhop))) goto out;
+    /* the model stays unpadded on the host: the library replicates its edges
+     * (io_utils.c:1096-1143) as it stages the materials */
     {   /* a_iso_3d.c:368-374 and 411-417 */
-        double vpmax = sm_a3d_cfl_vpmax(g.nx, g.nz, vpp);
+        double vpmax = sm_a3d_cfl_vpmax_unpadded(g.nx, g.ny, g.nz, np, vp);
         if (dt * vpmax * sqrt(1. / (g.dx * g.dx) + 1. / (g.dy * g.dy) + 1. / (g.dz * g.dz)) > 1.) {
             rc = sm_fail(SM_ECFL, "Time step too large");
             goto out;
@@ -292,8 +290,8 @@ int sm_a_iso_3d_main(int argc, char **argv)
             goto out;
     }
     const size_t nsteps = sm_nsteps(p.duration, dt);
-    if ((rc = sm_a3d_create(0, nx2, ny2, nz2, np, g.dx, g.dy, g.dz, dt, vpp, rhop,
-                            (const double *const *)coef, p.precision, &h)))
+    if ((rc = sm_a3d_create_unpadded(0, g.nx, g.ny, g.nz, np, g.dx, g.dy, g.dz, dt, vp, rho,
+                                     (const double *const *)coef, p.precision, &h)))
         goto out;
     {   /* a_iso_3d.c:689-693: P += dt fct 1e6 for every source type */
         size_t *idx = malloc(nsrc * sizeof(size_t));
@@ -387,7 +385,7 @@ int sm_a_iso_3d_main(int argc, char **argv)
     if (p.verbose) fprintf(stdout, "\nEnd of computation\n");
 out:
     sm_a3d_destroy(h);
-    free(vp); free(rho); free(vpp); free(rhop); free(fct); free(len); free(src); free(rec);
+    free(vp); free(rho); free(fct); free(len); free(src); free(rec);
     free(vals); free(counts);
     for (int c = 0; c < 18; ++c) free(coef[c]);
     rec_plan_free(&rp);
